@@ -1,0 +1,309 @@
+/*
+ * hvdg.h -- C ABI of the B200 (sm_100a) holographic-variational Y/C separator.
+ *
+ * Plain C: no C++ or torch types cross this boundary, only pointers, sizes
+ * and POD structs. Every entry point returns an hvdg_status; none throws.
+ *
+ * Reference interfaces replaced (paths relative to the hvd-cvbs-decoding
+ * project; each declaration below cites the one it stands in for):
+ *
+ *   hvd-core/src/frame_bridge.h:196-199   hvd::DecodeFrameSequenceWindow
+ *   hvd-core/src/engine/engine.h:112-114  HvdEngine::DecodeSequenceWindow
+ *   hvd-core/src/engine/sequence.h:60-61  PrepareFieldObs
+ *   hvd-core/src/engine/sequence.h:98-101 DecodeFieldWindow
+ *   hvd-core/src/engine/lockin.h:31-59    BurstLockinPhase / BurstLockinPhasePal
+ *   hvd-core/src/engine/lockin.h:36       BurstAmplitudeIre
+ *   hvd-core/src/engine/holographic_init.h:221-223  HolographicInit
+ *   hvd-core/src/engine/variational.h:76-78         VariationalRefine
+ *   hvd-core/src/engine/motion.h:49-50              EstimateMotion
+ *
+ * Units and layouts follow the reference: planes are row-major float32,
+ * index (y, x) -> y * width + x; complex planes are interleaved (re, im)
+ * float pairs, chi = V - iU in IRE; composite samples are IRE referenced to
+ * blanking (ntsc_geometry.h:225-228).
+ *
+ * Where the reference passes a carrier plane exp(i*phi) (FieldObs::carrier),
+ * this ABI passes the per-line burst-locked phase theta[] plus the PAL
+ * V-switch vswitch[] and rebuilds the carrier exactly as MakeCarrier /
+ * MakeCarrierPal do (ntsc_geometry.cpp:29-47, 75-93): the device never
+ * stores a carrier plane.
+ *
+ * Threading: one hvdg_ctx per host thread (same contract as one HvdEngine
+ * per thread, frame_bridge.h:137-140). Calls on one context are serialised
+ * on that context's CUDA stream and are synchronous unless named *_async.
+ */
+#ifndef HVDG_H_
+#define HVDG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HVDG_ABI_VERSION 1
+
+typedef enum hvdg_status {
+  HVDG_OK = 0,
+  HVDG_ERR_BAD_ARGUMENT = 1,    /* null pointer, n < 0, bad enum value */
+  HVDG_ERR_BAD_GEOMETRY = 2,    /* active window / burst window out of range, h or w < 2 */
+  HVDG_ERR_NONFINITE_INPUT = 3, /* NaN / Inf among the input samples */
+  HVDG_ERR_DEVICE_TIMEOUT = 4,  /* a bounded device-side wait expired */
+  HVDG_ERR_CUDA = 5,            /* a CUDA runtime call failed (see hvdg_last_error) */
+  HVDG_ERR_OUT_OF_MEMORY = 6,   /* device or pinned allocation failed */
+  HVDG_ERR_UNSUPPORTED = 7,     /* a configuration this build does not implement */
+  HVDG_ERR_NO_DEVICE = 8        /* no CUDA device / wrong architecture */
+} hvdg_status;
+
+typedef enum hvdg_standard {
+  HVDG_STD_NTSC = 0,  /* VideoStandard::kNtsc  (ntsc_geometry.h:137) */
+  HVDG_STD_PAL = 1,   /* VideoStandard::kPal   */
+  HVDG_STD_PAL_M = 2  /* VideoStandard::kPalM  */
+} hvdg_standard;
+
+typedef enum hvdg_sample_type {
+  HVDG_SAMPLES_F32_IRE = 0, /* float, already IRE (FieldInput::samples) */
+  HVDG_SAMPLES_U16 = 1,     /* uint16 codes; IRE = (s - blanking) / ((white - blanking) / 100) */
+  HVDG_SAMPLES_S16 = 2      /* int16 codes (the plugin's 10-bit frame buffers), same level map */
+} hvdg_sample_type;
+
+/* Mirror of hvd::FieldGeometry (ntsc_geometry.h:66-191). */
+typedef struct hvdg_geometry {
+  int32_t field_width;             /* samples per line incl. blanking (910 NTSC, 1135 PAL) */
+  int32_t field_height;            /* lines per field (263 NTSC, 313 PAL) */
+  int32_t active_video_start;      /* first active sample (inclusive) */
+  int32_t active_video_end;        /* one past the last active sample */
+  int32_t colour_burst_start;      /* burst window start (inclusive) */
+  int32_t colour_burst_end;        /* burst window end (exclusive) */
+  int32_t first_active_field_line; /* first active line */
+  int32_t last_active_field_line;  /* one past the last active line; 0 => field_height */
+  double sample_rate;              /* Hz */
+  int32_t standard;                /* hvdg_standard */
+  int32_t reserved0;
+  double subcarrier_hz;            /* 0 => the standard's nominal fsc */
+} hvdg_geometry;
+
+/* Mirror of hvd::HvdConfig (hvd_config.h:21-419), hot-path fields only, same
+ * defaults (hvdg_config_default). */
+typedef struct hvdg_config {
+  float lambda_c;            /* 1.0  */
+  float chroma_aniso;        /* 0.0 = auto (variational.cpp:130-196) */
+  float charbonnier_eps;     /* 0.5  */
+  float chroma_eps;          /* 1.0  */
+  float structure_coupling;  /* 0.25 */
+  float diag_prior;          /* 0.0; > 0 is HVDG_ERR_UNSUPPORTED on the device path */
+  int32_t cg_iterations;     /* 2    */
+  int32_t irls_outer;        /* 4    */
+  float cg_tol;              /* 0 = auto (0.02 slow / 0.10 fast) */
+  int32_t fast;              /* 1    */
+  int32_t parallel_across_fields; /* 1 (CPU-baseline knob; the device path always batches) */
+  int32_t symmetry_variant;  /* 0; 1 is HVDG_ERR_UNSUPPORTED on the device path */
+  int32_t acc;               /* 1    */
+  float chroma_gain;         /* 1.0  */
+  int32_t monochrome;        /* 0    */
+  float chroma_phase_deg;    /* 0.0  */
+  int32_t field_order;       /* 0 = auto, 1 = field 1 top, 2 = field 1 bottom */
+  float temporal_strength;   /* 0 = adaptive, < 0 = 3-D off, > 0 = fixed */
+  int32_t bidirectional;     /* 1    */
+  int32_t passes;            /* 2    */
+  float temporal_eps;        /* 0 = auto clip(7 sigma, 4, 20) */
+  float nr_anchor;           /* 1.0  */
+  float nr_eps;              /* 0 = auto clip(3 sigma, 3, 12) */
+  int32_t nr_radius;         /* 2    */
+  int32_t mc_tile;           /* 32   */
+  int32_t mc_search;         /* 16   */
+  int32_t trajectory_fit;    /* 1    */
+  int32_t extended_temporal; /* 1    */
+  float coherence_gate;      /* 0.6  */
+  float odd_gate_floor;      /* 0.35 */
+  int32_t output_fidelity;   /* 1    */
+  int32_t psi_init;          /* 0    */
+  /* ---- B200 build extensions (no HvdConfig counterpart) ---- */
+  int32_t me_mode;           /* 0 = reference float-SSD pyramid (motion.cpp:397-488),
+                                1 = exhaustive integer SAD on uint16-quantised luma */
+  int32_t me_block;          /* block size for me_mode 1 (16) */
+  int32_t me_range;          /* +/- search range for me_mode 1 (16) */
+  int32_t reserved[5];
+} hvdg_config;
+
+/* Mirror of hvd::FrameParams (frame_bridge.h:40-101). */
+#define HVDG_MAX_EXTRA_SAMPLE_LINES 8
+typedef struct hvdg_frame_params {
+  int32_t standard;
+  int32_t frame_width;
+  int32_t frame_height;
+  int32_t field1_lines;
+  int32_t active_video_start;
+  int32_t active_video_end;
+  int32_t colour_burst_start;
+  int32_t colour_burst_end;
+  int32_t first_active_frame_line;
+  int32_t last_active_frame_line;
+  float black_level;
+  float white_level;
+  float blanking_level;
+  float chroma_dc;
+  double sample_rate;
+  double subcarrier_hz;
+  int32_t extra_sample_lines[HVDG_MAX_EXTRA_SAMPLE_LINES];
+  int32_t extra_sample_line_count;
+  int32_t reserved0;
+} hvdg_frame_params;
+
+/* One composite field in (FieldInput + the parity FieldObs carries). */
+typedef struct hvdg_field_in {
+  const void* samples;        /* field_height x field_width, see sample_type */
+  int32_t sample_type;        /* hvdg_sample_type */
+  int32_t parity;             /* 0 = top field, 1 = bottom (FieldObs::parity) */
+  float blanking_level;       /* used for U16 / S16 samples */
+  float white_level;          /* used for U16 / S16 samples */
+  const hvdg_geometry* geometry; /* per-field geometry (mixed NTSC/PAL batches) */
+  int32_t irls_outer;         /* <= 0: cfg->irls_outer   (per-field solver budget) */
+  int32_t cg_iterations;      /* <  0: cfg->cg_iterations */
+} hvdg_field_in;
+
+/* One decoded field out (DecodedField, sequence.h:64-69). Caller-owned. */
+typedef struct hvdg_field_out {
+  float* luma;     /* active_lines x active_width, IRE */
+  float* chroma;   /* active_lines x active_width x 2 (re, im), chi = V - iU, IRE */
+  float* theta;    /* optional (may be NULL): field_height carrier phases after the trim */
+  int8_t* vswitch; /* optional (may be NULL): field_height V-switch senses (+1 / -1) */
+} hvdg_field_out;
+
+/* One decoded frame (YcFrameS16, frame_bridge.h:123-131). Caller-owned,
+ * frame_width * frame_height elements each. */
+typedef struct hvdg_yc_frame {
+  int16_t* luma;
+  int16_t* chroma;
+  double* u_plane;
+  double* v_plane;
+} hvdg_yc_frame;
+
+/* Per-call timing / diagnostics (SequenceDiagnostics, sequence.h:75-81, plus
+ * device timings). Optional everywhere. */
+typedef struct hvdg_diag {
+  float resolved_strength;
+  float ambiguity_ire;
+  float sigma_ire;
+  float temporal_eps;
+  float nr_eps;
+  float acc_gain;
+  float ms_total;       /* device time of the whole call (CUDA events) */
+  float ms_solver;      /* device time of the IRLS + CG persistent kernel(s) */
+  float ms_init;        /* device time of lock-in + holographic init */
+  float ms_motion;      /* device time of motion estimation + warps */
+  int64_t cg_iterations_run;   /* sum over fields of CG iterations executed */
+  int64_t solver_pixel_iters;  /* sum over fields of active px * CG iterations */
+  int64_t solver_pixel_outers; /* sum over fields of active px * IRLS outers */
+  int32_t kernel_launches;     /* kernels this call launched */
+  int32_t reserved;
+} hvdg_diag;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+
+int hvdg_abi_version(void);
+const char* hvdg_status_string(hvdg_status s);
+void hvdg_config_default(hvdg_config* cfg);
+/* NTSC 4fsc / PAL 4fsc default geometries (ntsc_geometry.h:66-74;
+ * research/reference-pal/hvd_pal/tbc.py:34-50). */
+void hvdg_geometry_default(int standard, hvdg_geometry* g);
+
+typedef struct hvdg_ctx hvdg_ctx;
+/* Owns the device arena, the stream, the CUDA-graph cache and the tuning
+ * table (HvdEngine, engine.h:70-128, owns the FFT plan cache). */
+hvdg_status hvdg_create(int device, hvdg_ctx** out);
+void hvdg_destroy(hvdg_ctx* ctx);
+/* Last error text for this context (static storage, valid until next call). */
+const char* hvdg_last_error(const hvdg_ctx* ctx);
+/* 0 = plain path (one field per launch sequence), 1 = batched persistent
+ * launch (default). Exists for the batched-vs-plain comparison. */
+hvdg_status hvdg_set_batching(hvdg_ctx* ctx, int batched);
+/* Solver tiling: band height (rows per work unit; 0 = autotuned). */
+hvdg_status hvdg_set_tuning(hvdg_ctx* ctx, int band_rows, int ctas_per_sm);
+
+/* ------------------------------------------------------------------------ */
+/* Engine level                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* PrepareFieldObs x n + DecodeFieldWindow (sequence.cpp:229-281, 423-1116):
+ * burst lock-in, active crop, carrier, holographic init, (3-D neighbour
+ * terms when cfg->temporal_strength > 0), IRLS + CG, output-fidelity luma.
+ * All fields must share fields[0].geometry (the reference's window contract). */
+hvdg_status hvdg_decode_field_window(hvdg_ctx* ctx, const hvdg_field_in* fields,
+                                     int n_fields, const hvdg_config* cfg,
+                                     hvdg_field_out* out, hvdg_diag* diag);
+
+/* Independent 2-D fields of mixed geometry and per-field solver budgets in
+ * one batched persistent launch (the reference decodes these one by one:
+ * sequence.cpp:1076-1084 with temporal off). Host buffers in and out. */
+hvdg_status hvdg_decode_fields(hvdg_ctx* ctx, const hvdg_field_in* fields,
+                               int n_fields, const hvdg_config* cfg,
+                               hvdg_field_out* out, hvdg_diag* diag);
+
+/* Same as hvdg_decode_fields with every samples / luma / chroma / theta /
+ * vswitch pointer a DEVICE pointer on the context's device; no host copies.
+ * Returns after the work is enqueued on `stream` (0 = the context stream)
+ * and completed (synchronous). */
+hvdg_status hvdg_decode_fields_device(hvdg_ctx* ctx, const hvdg_field_in* fields,
+                                      int n_fields, const hvdg_config* cfg,
+                                      hvdg_field_out* out, hvdg_diag* diag);
+
+/* hvd::DecodeFrameSequenceWindow (frame_bridge.cpp:722-947): split each
+ * int16 frame into fields, ACC, field-order vote, window decode, weave and
+ * 10-bit requantise. `out` has core_end - core_begin entries. Returns
+ * HVDG_ERR_BAD_ARGUMENT where the reference returns an empty vector. */
+hvdg_status hvdg_decode_frame_sequence_window(
+    hvdg_ctx* ctx, const int16_t* const* frames, int n_frames, int core_begin,
+    int core_end, const hvdg_frame_params* fp, const hvdg_config* cfg,
+    hvdg_yc_frame* out, hvdg_diag* diag);
+
+/* ------------------------------------------------------------------------ */
+/* Kernel level (host buffers)                                               */
+/* ------------------------------------------------------------------------ */
+
+/* BurstLockinPhase (lockin.cpp:169-254) on NTSC, BurstLockinPhasePal
+ * (lockin.cpp:325-417) on the PAL family. `field_ire` is field_height x
+ * field_width IRE; theta/vswitch have field_height entries (vswitch is
+ * filled with +1 on NTSC and may be NULL there). */
+hvdg_status hvdg_burst_lockin(hvdg_ctx* ctx, const float* field_ire,
+                              const hvdg_geometry* g, float* theta,
+                              int8_t* vswitch);
+
+/* BurstAmplitudeIre (lockin.cpp:256-323). */
+hvdg_status hvdg_burst_amplitude(hvdg_ctx* ctx, const float* field_ire,
+                                 const hvdg_geometry* g, float* amplitude_ire);
+
+/* HolographicInit (holographic_init.cpp:427-544) on the active picture
+ * `s` (active_lines x active_width); carrier from theta/vswitch (active
+ * lines only). Outputs luma0 (h x w) and chi0 (h x w x 2). */
+hvdg_status hvdg_holographic_init(hvdg_ctx* ctx, const float* s,
+                                  const float* theta_active,
+                                  const int8_t* vswitch_active,
+                                  const hvdg_geometry* g, const hvdg_config* cfg,
+                                  float* luma0, float* chi0);
+
+/* VariationalRefine (variational.cpp:198-556), 2-D (no neighbours). */
+hvdg_status hvdg_variational_refine(hvdg_ctx* ctx, const float* s,
+                                    const float* theta_active,
+                                    const int8_t* vswitch_active,
+                                    const float* chi0, const hvdg_geometry* g,
+                                    const hvdg_config* cfg, float* luma,
+                                    float* chi);
+
+/* EstimateMotion (motion.cpp:397-488): per-tile (dy, dx, confidence) from
+ * y_ref to y_cur (both h x w); outputs are ceil(h/tile) x ceil(w/tile).
+ * me_mode selects the cost (see hvdg_config::me_mode); for me_mode 1 the
+ * block size and range come from `tile` and `search`. */
+hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref,
+                                 const float* y_cur, int h, int w, int tile,
+                                 int search, int me_mode, float* dy, float* dx,
+                                 float* confidence);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* HVDG_H_ */
