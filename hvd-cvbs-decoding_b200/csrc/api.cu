@@ -1,0 +1,1162 @@
+// api.cu -- the C ABI (include/hvdg.h): context, device arena, batch
+// planning, host-side tables, and the decode pipelines.
+//
+// Host orchestration replaces hvd-core's HvdEngine / DecodeFieldWindow
+// driver (hvd-core/src/engine/engine.cpp:133-137,
+// hvd-core/src/engine/sequence.cpp:229-281, 423-1116): instead of one OpenMP
+// solve per field, a batch of fields is laid out in one device arena and
+// every stage runs as one launch over all fields.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "hvdg.h"
+#include "hvdg_internal.h"
+#include "hvdg_host.h"
+#include "k_init.h"
+#include "k_prep.h"
+#include "k_solver.h"
+
+using hvdg::FieldCtl;
+using hvdg::FieldDesc;
+using hvdg::GeomDesc;
+using hvdg::Unit;
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------------------
+// Geometry helpers (mirror FieldGeometry, ntsc_geometry.h:142-267)
+// ---------------------------------------------------------------------------
+bool uses_vswitch(const hvdg_geometry& g) {
+  return g.standard == HVDG_STD_PAL || g.standard == HVDG_STD_PAL_M;
+}
+int last_active_line(const hvdg_geometry& g) {
+  return g.last_active_field_line != 0 ? g.last_active_field_line : g.field_height;
+}
+double phase_per_sample(const hvdg_geometry& g) {
+  if (g.subcarrier_hz <= 0.0) return 0.5 * kPi;
+  return 2.0 * kPi * g.subcarrier_hz / g.sample_rate;
+}
+double line_advance(const hvdg_geometry& g) {
+  if (g.subcarrier_hz <= 0.0) {
+    if (g.standard == HVDG_STD_PAL) return 2.0 * kPi * 0.7516;
+    if (g.standard == HVDG_STD_PAL_M) return 0.5 * kPi;
+    return kPi;
+  }
+  const double cycles = g.subcarrier_hz * (double)g.field_width / g.sample_rate;
+  return 2.0 * kPi * (cycles - std::floor(cycles));
+}
+float nominal_burst(const hvdg_geometry& g) {
+  return g.standard == HVDG_STD_PAL ? 21.43f : 20.0f;
+}
+
+hvdg_status check_geometry(const hvdg_geometry* g) {
+  if (!g) return HVDG_ERR_BAD_ARGUMENT;
+  if (g->standard < 0 || g->standard > 2) return HVDG_ERR_BAD_ARGUMENT;
+  const int lal = last_active_line(*g);
+  if (g->field_width < 1 || g->field_height < 1) return HVDG_ERR_BAD_GEOMETRY;
+  if (g->active_video_start < 0 || g->active_video_end > g->field_width ||
+      g->active_video_end - g->active_video_start < 2)
+    return HVDG_ERR_BAD_GEOMETRY;
+  if (g->first_active_field_line < 0 || lal > g->field_height ||
+      lal - g->first_active_field_line < 2)
+    return HVDG_ERR_BAD_GEOMETRY;
+  if (g->colour_burst_start < 0 || g->colour_burst_end > g->field_width ||
+      g->colour_burst_end < g->colour_burst_start)
+    return HVDG_ERR_BAD_GEOMETRY;
+  if (!(g->sample_rate > 0.0)) return HVDG_ERR_BAD_GEOMETRY;
+  // device-path limits (documented in include/hvdg.h)
+  if (g->field_height > hvdg::kMaxLines) return HVDG_ERR_UNSUPPORTED;
+  const int w = g->active_video_end - g->active_video_start;
+  const int h = lal - g->first_active_field_line;
+  const int pad = std::min(hvdg::kInitPad, h - 1);
+  if (2 * w - 1 > hvdg::kRowFft || 2 * (h + 2 * pad) - 1 > hvdg::kColFft) return HVDG_ERR_UNSUPPORTED;
+  if (g->colour_burst_end - g->colour_burst_start > 64 + 3) return HVDG_ERR_UNSUPPORTED;
+  return HVDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side init tables (double precision, cached per geometry).
+// ---------------------------------------------------------------------------
+using cd = std::complex<double>;
+
+// numpy.fft.fftfreq(n, d) (holographic_init.cpp:20-30)
+double fftfreq(int i, int n, double d) {
+  const int half = (n % 2 == 0) ? n / 2 : (n + 1) / 2;
+  const int k = i < half ? i : i - n;
+  return k / (n * d);
+}
+
+// Spectrum (length M, scaled by `scale` / M) of the circular kernel
+// k = IDFT_n(mask), embedded for a cyclic convolution of length M >= 2n - 1.
+std::vector<cd> kernel_spectrum(const std::vector<double>& mask, int M, double scale) {
+  const int n = (int)mask.size();
+  std::vector<cd> k(n);
+  std::vector<cd> twn(n);
+  for (int j = 0; j < n; ++j) twn[j] = cd(std::cos(2 * kPi * j / n), std::sin(2 * kPi * j / n));
+  for (int j = 0; j < n; ++j) {
+    cd acc = 0.0;
+    for (int q = 0; q < n; ++q) acc += mask[q] * twn[(int64_t)j * q % n];
+    k[j] = acc / (double)n;
+  }
+  std::vector<cd> emb(M, cd(0, 0));
+  for (int j = -(n - 1); j <= n - 1; ++j) emb[((j % M) + M) % M] = k[((j % n) + n) % n];
+  std::vector<cd> twm(M);
+  for (int j = 0; j < M; ++j) twm[j] = cd(std::cos(2 * kPi * j / M), -std::sin(2 * kPi * j / M));
+  std::vector<cd> out(M);
+  for (int m = 0; m < M; ++m) {
+    cd acc = 0.0;
+    for (int j = 0; j < M; ++j) {
+      if (emb[j] == cd(0, 0)) continue;
+      acc += emb[j] * twm[(int64_t)j * m % M];
+    }
+    out[m] = acc * (scale / M);
+  }
+  return out;
+}
+
+struct GeomTables {
+  int w, h, hp, pad;
+  std::vector<float2> khat_row;  // 2 * kRowFft
+  std::vector<float2> khat_col;  // 2 * kColFft
+  std::vector<float2> col_phasor;
+};
+
+// The two crop variants of HolographicInit (holographic_init.cpp:236).
+const double kVariants[2][2] = {{0.8, 120.0}, {1.8, 30.0}};
+
+GeomTables make_geom_tables(const hvdg_geometry& g) {
+  GeomTables t;
+  t.w = g.active_video_end - g.active_video_start;
+  t.h = last_active_line(g) - g.first_active_field_line;
+  t.pad = std::min(hvdg::kInitPad, t.h > 1 ? t.h - 1 : 0);
+  t.hp = t.h + 2 * t.pad;
+  for (int v = 0; v < 2; ++v) {
+    std::vector<double> gx(t.w), gy(t.hp);
+    const double cx = kVariants[v][0] * 1.0e6;
+    const double cy = kVariants[v][1] / (2.0 * t.h);  // against the REAL height
+    for (int i = 0; i < t.w; ++i) {
+      const double r = fftfreq(i, t.w, 1.0 / g.sample_rate) / cx;
+      gx[i] = std::exp(-0.5 * r * r);
+    }
+    for (int i = 0; i < t.hp; ++i) {
+      const double r = fftfreq(i, t.hp, 1.0) / cy;
+      gy[i] = std::exp(-0.5 * r * r);
+    }
+    for (const cd& c : kernel_spectrum(gx, hvdg::kRowFft, 1.0))
+      t.khat_row.push_back(make_float2((float)c.real(), (float)c.imag()));
+    // x2 of the init (holographic_init.cpp:247-251) folded into the column pass
+    for (const cd& c : kernel_spectrum(gy, hvdg::kColFft, 2.0))
+      t.khat_col.push_back(make_float2((float)c.real(), (float)c.imag()));
+  }
+  const double w0 = phase_per_sample(g);
+  const bool quad = g.subcarrier_hz <= 0.0;
+  for (int x = 0; x < t.w; ++x) {
+    const int s = g.active_video_start + x;
+    if (quad) {
+      static const float2 q[4] = {{1.f, 0.f}, {0.f, 1.f}, {-1.f, 0.f}, {0.f, -1.f}};
+      t.col_phasor.push_back(q[s & 3]);
+    } else {
+      t.col_phasor.push_back(make_float2((float)std::cos(w0 * s), (float)std::sin(w0 * s)));
+    }
+  }
+  return t;
+}
+
+using GeomKey = std::tuple<int, int, int, int, int, int, double, double>;
+GeomKey geom_key(const hvdg_geometry& g) {
+  return GeomKey(g.active_video_start, g.active_video_end, g.first_active_field_line,
+                 last_active_line(g), g.standard, g.field_width, g.sample_rate, g.subcarrier_hz);
+}
+
+std::vector<float2> twiddles(int M) {
+  std::vector<float2> t(M);
+  for (int k = 0; k < M; ++k) {
+    const double a = -2.0 * kPi * k / M;
+    t[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct hvdg_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  std::string last_error;
+  int batched = 1;
+  int band_rows = 0;
+  int ctas_per_sm = 0;
+  hvdg::DeviceArena arena;
+  hvdg::PinnedArena pinned;
+  std::map<GeomKey, GeomTables> geoms;
+};
+
+namespace hvdg {
+
+hvdg_status cuda_fail(hvdg_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return HVDG_OK;
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  ctx->last_error = buf;
+  cudaGetLastError();
+  return e == cudaErrorMemoryAllocation ? HVDG_ERR_OUT_OF_MEMORY : HVDG_ERR_CUDA;
+}
+
+hvdg_status DeviceArena::reserve(size_t bytes) {
+  if (bytes <= capacity) return HVDG_OK;
+  if (base) cudaFree(base);
+  base = nullptr;
+  capacity = 0;
+  const size_t want = bytes + bytes / 8;
+  if (cudaMalloc(&base, want) != cudaSuccess) {
+    cudaGetLastError();
+    return HVDG_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemset(base, 0, want);
+  capacity = want;
+  return HVDG_OK;
+}
+DeviceArena::~DeviceArena() {
+  if (base) cudaFree(base);
+}
+hvdg_status PinnedArena::reserve(size_t bytes) {
+  if (bytes <= capacity) return HVDG_OK;
+  if (base) cudaFreeHost(base);
+  base = nullptr;
+  capacity = 0;
+  if (cudaMallocHost(&base, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return HVDG_ERR_OUT_OF_MEMORY;
+  }
+  capacity = bytes;
+  return HVDG_OK;
+}
+PinnedArena::~PinnedArena() {
+  if (base) cudaFreeHost(base);
+}
+
+}  // namespace hvdg
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Batch planning
+// ---------------------------------------------------------------------------
+struct FieldPlan {
+  const hvdg_geometry* g;
+  int h, w, pitch, fh, fw;
+  int64_t px_off;
+  int line_off, theta_off, geom_slot;
+  int64_t raw_off, raw_bytes;
+  int hp;
+  int64_t rowbuf_off;
+};
+
+struct Layout {
+  // byte offsets into the arena
+  size_t o_raw, o_prep, o_fields, o_geoms, o_ctl, o_units, o_partials, o_done, o_arrive,
+      o_flags, o_queue, o_lineph, o_theta, o_theta64, o_vsw, o_colph, o_khat, o_twr, o_twc,
+      o_S, o_Y, o_X0, o_X1, o_G0, o_G1, o_D0, o_D1, o_Q0, o_Q1, o_W, o_rowbuf, o_itab, o_amp;
+  size_t total;
+  int64_t total_px, total_rowbuf;
+  int total_lines, total_theta, total_units, total_prows, total_cgroups, total_btiles;
+  int ncol, nkhat;
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Batch {
+  std::vector<FieldPlan> fp;
+  std::vector<hvdg::PrepDesc> prep;
+  std::vector<FieldDesc> fields;
+  std::vector<GeomDesc> geoms;
+  std::vector<const GeomTables*> gtabs;
+  std::vector<int> gcol_off;
+  std::vector<Unit> units;
+  std::vector<int> itab;  // prow_field | prow_first | cgrp_field | cgrp_first | btile_field | btile_first
+  int it_prow_field, it_prow_first, it_cgrp_field, it_cgrp_first, it_btile_field, it_btile_first;
+  std::vector<int64_t> rowbuf_offs;
+  std::vector<int> crop_row_field, crop_row_first;
+  std::vector<int64_t> px_offs;
+  std::vector<int> pitches;
+  Layout L;
+  int max_phases = 0;
+};
+
+int elem_size(int sample_type) { return sample_type == HVDG_SAMPLES_F32_IRE ? 4 : 2; }
+
+hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
+                       int band_rows, Batch& b) {
+  b = Batch();
+  std::map<GeomKey, int> slot;
+  int64_t px = 0, rawb = 0, rowb = 0;
+  int lines = 0, theta = 0;
+  for (int i = 0; i < n; ++i) {
+    const hvdg_geometry& g = *in[i].geometry;
+    const GeomKey key = geom_key(g);
+    auto it = ctx->geoms.find(key);
+    if (it == ctx->geoms.end()) it = ctx->geoms.emplace(key, make_geom_tables(g)).first;
+    int gs;
+    auto sit = slot.find(key);
+    if (sit == slot.end()) {
+      gs = (int)b.gtabs.size();
+      slot.emplace(key, gs);
+      b.gtabs.push_back(&it->second);
+    } else {
+      gs = sit->second;
+    }
+    FieldPlan p;
+    p.g = in[i].geometry;
+    p.fh = g.field_height;
+    p.fw = g.field_width;
+    p.h = last_active_line(g) - g.first_active_field_line;
+    p.w = g.active_video_end - g.active_video_start;
+    p.pitch = (p.w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
+    p.px_off = px;
+    px += (int64_t)p.h * p.pitch;
+    p.line_off = lines;
+    lines += p.h;
+    p.theta_off = theta;
+    theta += p.fh;
+    p.geom_slot = gs;
+    p.raw_bytes = (int64_t)p.fh * p.fw * elem_size(in[i].sample_type);
+    p.raw_off = rawb;
+    rawb += align_up(p.raw_bytes, 256);
+    p.hp = it->second.hp;
+    p.rowbuf_off = rowb;
+    rowb += 2LL * p.hp * p.pitch;
+    b.fp.push_back(p);
+  }
+  // geometry descriptors + packed tables
+  int ncol = 0, nkhat = 0;
+  for (size_t s = 0; s < b.gtabs.size(); ++s) {
+    const GeomTables& t = *b.gtabs[s];
+    GeomDesc gd;
+    gd.w = t.w;
+    gd.h = t.h;
+    gd.hp = t.hp;
+    gd.pad = t.pad;
+    gd.khat_row_off = nkhat;
+    nkhat += 2 * hvdg::kRowFft;
+    gd.khat_col_off = nkhat;
+    nkhat += 2 * hvdg::kColFft;
+    b.geoms.push_back(gd);
+    b.gcol_off.push_back(ncol);
+    ncol += t.w;
+  }
+  // per-field descriptors, units
+  const int band = band_rows > 0 ? band_rows : 32;
+  for (int i = 0; i < n; ++i) {
+    const FieldPlan& p = b.fp[i];
+    const hvdg_geometry& g = *p.g;
+    FieldDesc f;
+    std::memset(&f, 0, sizeof(f));
+    f.h = p.h;
+    f.w = p.w;
+    f.pitch = p.pitch;
+    f.fh = p.fh;
+    f.fw = p.fw;
+    f.px_off = p.px_off;
+    f.line_off = p.line_off;
+    f.col_off = b.gcol_off[p.geom_slot];
+    f.geom = p.geom_slot;
+    f.is_pal = uses_vswitch(g) ? 1 : 0;
+    // solver budget (variational.cpp:224-230)
+    const int outer_cfg = in[i].irls_outer > 0 ? in[i].irls_outer : cfg->irls_outer;
+    const int cg_cfg = in[i].cg_iterations >= 0 ? in[i].cg_iterations : cfg->cg_iterations;
+    f.n_outer = std::max(1, outer_cfg);
+    const int cg_total = cfg->fast ? cg_cfg * 2 / 3 : cg_cfg;
+    f.n_inner = std::max(1, cg_total / f.n_outer);
+    f.cg_tol = cfg->cg_tol > 0.0f ? cfg->cg_tol : (cfg->fast ? 0.10f : 0.02f);
+    f.eps = cfg->charbonnier_eps;
+    f.eps_c = cfg->chroma_eps;
+    f.k_coupling = cfg->structure_coupling;
+    f.lambda_c = cfg->lambda_c;
+    f.aniso_cfg = cfg->chroma_aniso;
+    f.mu_h = cfg->lambda_c;
+    f.mu_v = cfg->lambda_c;
+    f.plane_px = (int64_t)p.h * p.pitch;
+    f.unit_begin = (int)b.units.size();
+    for (int x0 = 0; x0 < p.w; x0 += hvdg::kStrip)
+      for (int y0 = 0; y0 < p.h; y0 += band) b.units.push_back(Unit{i, x0, y0, std::min(p.h, y0 + band)});
+    f.unit_count = (int)b.units.size() - f.unit_begin;
+    f.n_phases = f.n_outer * (2 + f.n_inner) + 1;
+    b.max_phases = std::max(b.max_phases, f.n_phases);
+    b.fields.push_back(f);
+
+    hvdg::PrepDesc pd;
+    std::memset(&pd, 0, sizeof(pd));
+    pd.sample_type = in[i].sample_type;
+    pd.quadrant = g.subcarrier_hz <= 0.0 ? 1 : 0;
+    pd.blank = in[i].blanking_level;
+    pd.codes_per_ire = (in[i].white_level - in[i].blanking_level) / 100.0f;
+    pd.fh = p.fh;
+    pd.fw = p.fw;
+    pd.bx0 = g.colour_burst_start;
+    pd.bx1 = g.colour_burst_end;
+    pd.fal = g.first_active_field_line;
+    pd.lal = last_active_line(g);
+    pd.a0 = g.active_video_start;
+    pd.a1 = g.active_video_end;
+    pd.vswitch_family = uses_vswitch(g) ? 1 : 0;
+    pd.nominal_burst = nominal_burst(g);
+    pd.w0 = phase_per_sample(g);
+    pd.adv = line_advance(g);
+    pd.chroma_phase_off = -cfg->chroma_phase_deg * 3.14159265358979323846f / 180.0f;
+    pd.theta_off = p.theta_off;
+    pd.line_off = p.line_off;
+    b.prep.push_back(pd);
+    b.px_offs.push_back(p.px_off);
+    b.pitches.push_back(p.pitch);
+    b.rowbuf_offs.push_back(p.rowbuf_off);
+    for (int y = 0; y < p.h; ++y) {
+      b.crop_row_field.push_back(i);
+    }
+    b.crop_row_first.push_back(p.line_off);
+  }
+  // init tables
+  std::vector<int> prow_field, prow_first, cgrp_field, cgrp_first, btile_field, btile_first;
+  const int cg = hvdg::init_col_group(), bt = hvdg::init_blend_tile();
+  for (int i = 0; i < n; ++i) {
+    const FieldPlan& p = b.fp[i];
+    prow_first.push_back((int)prow_field.size());
+    for (int y = 0; y < p.hp; ++y) prow_field.push_back(i);
+    cgrp_first.push_back((int)cgrp_field.size());
+    for (int x = 0; x < p.w; x += cg) cgrp_field.push_back(i);
+    btile_first.push_back((int)btile_field.size());
+    const int nt = ((p.h + bt - 1) / bt) * ((p.w + bt - 1) / bt);
+    for (int t = 0; t < nt; ++t) btile_field.push_back(i);
+  }
+  auto append = [&](const std::vector<int>& v) {
+    const int off = (int)b.itab.size();
+    b.itab.insert(b.itab.end(), v.begin(), v.end());
+    return off;
+  };
+  b.it_prow_field = append(prow_field);
+  b.it_prow_first = append(prow_first);
+  b.it_cgrp_field = append(cgrp_field);
+  b.it_cgrp_first = append(cgrp_first);
+  b.it_btile_field = append(btile_field);
+  b.it_btile_first = append(btile_first);
+  // crop tables appended to itab too
+  Layout& L = b.L;
+  L.total_px = px;
+  L.total_rowbuf = rowb;
+  L.total_lines = lines;
+  L.total_theta = theta;
+  L.total_units = (int)b.units.size();
+  L.total_prows = (int)prow_field.size();
+  L.total_cgroups = (int)cgrp_field.size();
+  L.total_btiles = (int)btile_field.size();
+  L.ncol = ncol;
+  L.nkhat = nkhat;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes, 256);
+    return r;
+  };
+  L.o_raw = take(rawb);
+  L.o_prep = take(sizeof(hvdg::PrepDesc) * n);
+  L.o_fields = take(sizeof(FieldDesc) * n);
+  L.o_geoms = take(sizeof(GeomDesc) * b.geoms.size());
+  L.o_ctl = take(sizeof(FieldCtl) * n);
+  L.o_units = take(sizeof(Unit) * b.units.size());
+  L.o_partials = take(sizeof(double) * 5 * b.units.size());
+  L.o_done = take(sizeof(int) * n);
+  L.o_arrive = take(sizeof(int) * n);
+  L.o_flags = take(sizeof(int) * 4);
+  L.o_queue = take(sizeof(unsigned long long));
+  L.o_lineph = take(sizeof(float4) * lines);
+  L.o_theta = take(sizeof(float) * theta);
+  L.o_theta64 = take(sizeof(double) * theta);
+  L.o_vsw = take(theta);
+  L.o_colph = take(sizeof(float2) * ncol);
+  L.o_khat = take(sizeof(float2) * nkhat);
+  L.o_twr = take(sizeof(float2) * hvdg::kRowFft);
+  L.o_twc = take(sizeof(float2) * hvdg::kColFft);
+  L.o_amp = take(sizeof(float) * n);
+  // crop tables: crop_row_field | crop_row_first | px_offs(int64) | pitches
+  L.o_itab = take(sizeof(int) * (b.itab.size() + b.crop_row_field.size() + b.crop_row_first.size() +
+                                 b.pitches.size()) +
+                  sizeof(int64_t) * (b.px_offs.size() + b.rowbuf_offs.size()) + 64);
+  L.o_S = take(sizeof(float) * px);
+  L.o_Y = take(sizeof(float) * px);
+  L.o_X0 = take(sizeof(float2) * px);
+  L.o_X1 = take(sizeof(float2) * px);
+  L.o_G0 = take(sizeof(float2) * px);
+  L.o_G1 = take(sizeof(float2) * px);
+  L.o_D0 = take(sizeof(float2) * px);
+  L.o_D1 = take(sizeof(float2) * px);
+  L.o_Q0 = take(sizeof(float2) * px);
+  L.o_Q1 = take(sizeof(float2) * px);
+  L.o_W = take(sizeof(float4) * px);
+  L.o_rowbuf = take(sizeof(float2) * rowb);
+  L.total = o;
+  return HVDG_OK;
+}
+
+template <typename T>
+T* at(hvdg_ctx* ctx, size_t off) {
+  return reinterpret_cast<T*>(static_cast<char*>(ctx->arena.base) + off);
+}
+
+struct RunOpts {
+  bool device_io = false;  // samples / outputs are device pointers
+  bool do_lockin = true;   // false: line phasors from theta_in / vswitch_in
+  bool do_init = true;     // false: chi0 from chi0_in
+  bool do_solve = true;    // false: outputs are the init (Y0, chi0)
+  const float* s_in = nullptr;       // active S (dense h x w), replaces the crop
+  const float* theta_in = nullptr;   // active-line theta
+  const int8_t* vswitch_in = nullptr;
+  const float* chi0_in = nullptr;    // dense h x w x 2
+};
+
+// The 2-D pipeline over one batch: lock-in, crop, init, aniso, solver.
+hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
+                      hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt) {
+  Batch b;
+  hvdg_status st = plan_batch(ctx, in, n, cfg, ctx->band_rows, b);
+  if (st != HVDG_OK) return st;
+  const Layout& L = b.L;
+  st = ctx->arena.reserve(L.total);
+  if (st != HVDG_OK) {
+    ctx->last_error = "device arena allocation failed";
+    return st;
+  }
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  // ---- tables to the device (one staging copy) ----
+  std::vector<char> host(L.o_S - L.o_prep, 0);
+  auto put = [&](size_t off, const void* src, size_t bytes) {
+    if (bytes) std::memcpy(host.data() + (off - L.o_prep), src, bytes);
+  };
+  for (int i = 0; i < n; ++i) {
+    b.prep[i].samples = opt.device_io ? in[i].samples : (const void*)(at<char>(ctx, L.o_raw) + b.fp[i].raw_off);
+  }
+  put(L.o_prep, b.prep.data(), sizeof(hvdg::PrepDesc) * n);
+  put(L.o_fields, b.fields.data(), sizeof(FieldDesc) * n);
+  put(L.o_geoms, b.geoms.data(), sizeof(GeomDesc) * b.geoms.size());
+  put(L.o_units, b.units.data(), sizeof(Unit) * b.units.size());
+  {
+    std::vector<int> done(n, -1);
+    put(L.o_done, done.data(), sizeof(int) * n);
+  }
+  {
+    std::vector<float2> col, kh;
+    for (size_t g = 0; g < b.gtabs.size(); ++g) {
+      col.insert(col.end(), b.gtabs[g]->col_phasor.begin(), b.gtabs[g]->col_phasor.end());
+      kh.insert(kh.end(), b.gtabs[g]->khat_row.begin(), b.gtabs[g]->khat_row.end());
+      kh.insert(kh.end(), b.gtabs[g]->khat_col.begin(), b.gtabs[g]->khat_col.end());
+    }
+    put(L.o_colph, col.data(), sizeof(float2) * col.size());
+    put(L.o_khat, kh.data(), sizeof(float2) * kh.size());
+    static const std::vector<float2> twr = twiddles(hvdg::kRowFft), twc = twiddles(hvdg::kColFft);
+    put(L.o_twr, twr.data(), sizeof(float2) * twr.size());
+    put(L.o_twc, twc.data(), sizeof(float2) * twc.size());
+  }
+  size_t it = L.o_itab;
+  const size_t it_itab = it;
+  put(it, b.itab.data(), sizeof(int) * b.itab.size());
+  it += sizeof(int) * b.itab.size();
+  const size_t it_crf = it;
+  put(it, b.crop_row_field.data(), sizeof(int) * b.crop_row_field.size());
+  it += sizeof(int) * b.crop_row_field.size();
+  const size_t it_crfirst = it;
+  put(it, b.crop_row_first.data(), sizeof(int) * b.crop_row_first.size());
+  it += sizeof(int) * b.crop_row_first.size();
+  const size_t it_pitch = it;
+  put(it, b.pitches.data(), sizeof(int) * b.pitches.size());
+  it += sizeof(int) * b.pitches.size();
+  it = align_up(it, 8);
+  const size_t it_pxoff = it;
+  put(it, b.px_offs.data(), sizeof(int64_t) * b.px_offs.size());
+  it += sizeof(int64_t) * b.px_offs.size();
+  const size_t it_rbo = it;
+  put(it, b.rowbuf_offs.data(), sizeof(int64_t) * b.rowbuf_offs.size());
+
+  cudaEventRecord(ctx->ev[0], s);
+  // raw samples
+  if (!opt.device_io && opt.do_lockin) {
+    for (int i = 0; i < n; ++i) {
+      e = cudaMemcpyAsync(at<char>(ctx, L.o_raw) + b.fp[i].raw_off, in[i].samples,
+                          (size_t)b.fp[i].raw_bytes, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D samples");
+    }
+  }
+  e = cudaMemcpyAsync(at<char>(ctx, L.o_prep), host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D tables");
+  cudaMemsetAsync(at<char>(ctx, L.o_ctl), 0, sizeof(FieldCtl) * n, s);
+  cudaMemsetAsync(at<char>(ctx, L.o_arrive), 0, sizeof(int) * n, s);
+  cudaMemsetAsync(at<char>(ctx, L.o_flags), 0, sizeof(int) * 4, s);
+  cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
+  int launches = 0;
+
+  // ---- lock-in + crop ----
+  cudaEventRecord(ctx->ev[1], s);
+  hvdg::LockinOut lo;
+  lo.theta = at<float>(ctx, L.o_theta);
+  lo.theta64 = nullptr;
+  lo.vswitch = at<signed char>(ctx, L.o_vsw);
+  lo.line_phasor = at<float4>(ctx, L.o_lineph);
+  std::vector<float4> lph_host;
+  if (opt.do_lockin) {
+    hvdg::launch_burst_lockin(at<hvdg::PrepDesc>(ctx, L.o_prep), n, lo, s);
+    launches += 1;
+  } else {
+    // caller-supplied active-line phases (one field): exp(i theta) in FP64
+    const FieldPlan& p = b.fp[0];
+    lph_host.resize(p.h);
+    for (int y = 0; y < p.h; ++y) {
+      const double th = (double)opt.theta_in[y];
+      const bool sw = uses_vswitch(*p.g) && opt.vswitch_in && opt.vswitch_in[y] < 0;
+      lph_host[y] = make_float4((float)std::cos(th), (float)std::sin(th), sw ? -1.f : 1.f, 0.f);
+    }
+    e = cudaMemcpyAsync(at<float4>(ctx, L.o_lineph), lph_host.data(), sizeof(float4) * p.h,
+                        cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D line phasors");
+  }
+  if (opt.s_in) {
+    const FieldPlan& p = b.fp[0];
+    e = cudaMemcpy2DAsync(at<float>(ctx, L.o_S) + p.px_off, sizeof(float) * p.pitch, opt.s_in,
+                          sizeof(float) * p.w, sizeof(float) * p.w, p.h, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D S");
+  } else {
+    hvdg::launch_crop(at<hvdg::PrepDesc>(ctx, L.o_prep), at<int>(ctx, it_crf),
+                      at<int>(ctx, it_crfirst), L.total_lines, at<float>(ctx, L.o_S),
+                      at<int64_t>(ctx, it_pxoff), at<int>(ctx, it_pitch),
+                      at<int>(ctx, L.o_flags) + 1, s);
+    launches += 1;
+  }
+  if (opt.chi0_in) {
+    const FieldPlan& p = b.fp[0];
+    e = cudaMemcpy2DAsync(at<float2>(ctx, L.o_X0) + p.px_off, sizeof(float2) * p.pitch, opt.chi0_in,
+                          sizeof(float2) * p.w, sizeof(float2) * p.w, p.h, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D chi0");
+  }
+  // ---- holographic init ----
+  hvdg::InitArgs ia;
+  ia.fields = at<FieldDesc>(ctx, L.o_fields);
+  ia.geoms = at<GeomDesc>(ctx, L.o_geoms);
+  ia.S = at<float>(ctx, L.o_S);
+  ia.line_phasor = at<float4>(ctx, L.o_lineph);
+  ia.col_phasor = at<float2>(ctx, L.o_colph);
+  ia.khat = at<float2>(ctx, L.o_khat);
+  ia.tw_row = at<float2>(ctx, L.o_twr);
+  ia.tw_col = at<float2>(ctx, L.o_twc);
+  ia.rowbuf = at<float2>(ctx, L.o_rowbuf);
+  ia.rowbuf_off = at<int64_t>(ctx, it_rbo);
+  ia.chi1 = at<float2>(ctx, L.o_G0);
+  ia.chi2 = at<float2>(ctx, L.o_D0);
+  ia.chi0 = at<float2>(ctx, L.o_X0);
+  ia.Y = at<float>(ctx, L.o_Y);
+  const int* itb = at<int>(ctx, it_itab);
+  ia.prow_field = itb + b.it_prow_field;
+  ia.prow_first = itb + b.it_prow_first;
+  ia.cgrp_field = itb + b.it_cgrp_field;
+  ia.cgrp_first = itb + b.it_cgrp_first;
+  ia.btile_field = itb + b.it_btile_field;
+  ia.btile_first = itb + b.it_btile_first;
+  if (opt.do_init) {
+    hvdg::launch_init(ia, L.total_prows, L.total_cgroups, L.total_btiles, s);
+    launches += 3;
+  }
+  if (opt.do_solve) {
+    hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), n, at<float2>(ctx, L.o_X0), s);
+    launches += 1;
+  }
+  cudaEventRecord(ctx->ev[2], s);
+  // ---- solver ----
+  hvdg::SolverArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.fields = at<FieldDesc>(ctx, L.o_fields);
+  sa.ctl = at<FieldCtl>(ctx, L.o_ctl);
+  sa.units = at<Unit>(ctx, L.o_units);
+  sa.n_units = L.total_units;
+  sa.n_phases = b.max_phases;
+  sa.queue = at<unsigned long long>(ctx, L.o_queue);
+  sa.done_phase = at<int>(ctx, L.o_done);
+  sa.arrive = at<int>(ctx, L.o_arrive);
+  sa.partials = at<double>(ctx, L.o_partials);
+  sa.err = at<int>(ctx, L.o_flags);
+  sa.S = at<float>(ctx, L.o_S);
+  sa.X[0] = at<float2>(ctx, L.o_X0);
+  sa.X[1] = at<float2>(ctx, L.o_X1);
+  sa.G[0] = at<float2>(ctx, L.o_G0);
+  sa.G[1] = at<float2>(ctx, L.o_G1);
+  sa.D[0] = at<float2>(ctx, L.o_D0);
+  sa.D[1] = at<float2>(ctx, L.o_D1);
+  sa.Q[0] = at<float2>(ctx, L.o_Q0);
+  sa.Q[1] = at<float2>(ctx, L.o_Q1);
+  sa.W = at<float4>(ctx, L.o_W);
+  sa.Y = at<float>(ctx, L.o_Y);
+  sa.line_phasor = at<float4>(ctx, L.o_lineph);
+  sa.col_phasor = at<float2>(ctx, L.o_colph);
+  const int per_sm = ctx->ctas_per_sm > 0 ? ctx->ctas_per_sm
+                                          : std::max(1, hvdg::solver_max_blocks_per_sm());
+  int grid = ctx->sm_count * per_sm;
+  // never more warps than the first phase can use
+  grid = std::max(1, std::min(grid, (L.total_units + (hvdg::kSolverThreads / 32) - 1) /
+                                        (hvdg::kSolverThreads / 32)));
+  if (opt.do_solve) {
+    e = hvdg::launch_solver(sa, grid, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
+    launches += 1;
+  }
+  cudaEventRecord(ctx->ev[3], s);
+  // ---- outputs ----
+  const cudaMemcpyKind kind = opt.device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  for (int i = 0; i < n; ++i) {
+    const FieldPlan& p = b.fp[i];
+    if (out[i].luma) {
+      e = cudaMemcpy2DAsync(out[i].luma, sizeof(float) * p.w, at<float>(ctx, L.o_Y) + p.px_off,
+                            sizeof(float) * p.pitch, sizeof(float) * p.w, p.h, kind, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy luma");
+    }
+    if (out[i].chroma) {
+      e = cudaMemcpy2DAsync(out[i].chroma, sizeof(float2) * p.w, at<float2>(ctx, L.o_X0) + p.px_off,
+                            sizeof(float2) * p.pitch, sizeof(float2) * p.w, p.h, kind, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy chroma");
+    }
+    if (out[i].theta) {
+      e = cudaMemcpyAsync(out[i].theta, at<float>(ctx, L.o_theta) + p.theta_off, sizeof(float) * p.fh,
+                          kind, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy theta");
+    }
+    if (out[i].vswitch) {
+      e = cudaMemcpyAsync(out[i].vswitch, at<signed char>(ctx, L.o_vsw) + p.theta_off, p.fh, kind, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy vswitch");
+    }
+  }
+  int flags[4] = {0, 0, 0, 0};
+  e = cudaMemcpyAsync(flags, at<int>(ctx, L.o_flags), sizeof(flags), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy flags");
+  std::vector<FieldCtl> ctl(n);
+  if (diag) cudaMemcpyAsync(ctl.data(), at<FieldCtl>(ctx, L.o_ctl), sizeof(FieldCtl) * n,
+                            cudaMemcpyDeviceToHost, s);
+  cudaEventRecord(ctx->ev[4], s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "stream sync");
+  if (diag) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[4]);
+    diag->ms_total += ms;
+    cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+    diag->ms_solver += ms;
+    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+    diag->ms_init += ms;
+    for (int i = 0; i < n; ++i) {
+      diag->cg_iterations_run += ctl[i].cg_iters;
+      diag->solver_pixel_iters += (int64_t)ctl[i].cg_iters * b.fp[i].h * b.fp[i].w;
+      diag->solver_pixel_outers += (int64_t)b.fields[i].n_outer * b.fp[i].h * b.fp[i].w;
+    }
+    diag->kernel_launches += launches;
+  }
+  if (flags[1]) {
+    ctx->last_error = "non-finite input samples";
+    return HVDG_ERR_NONFINITE_INPUT;
+  }
+  if (flags[0]) {
+    ctx->last_error = "device-side bounded wait expired in the solver";
+    return HVDG_ERR_DEVICE_TIMEOUT;
+  }
+  return HVDG_OK;
+}
+
+hvdg_status validate_fields(const hvdg_field_in* fields, int n, const hvdg_config* cfg,
+                            hvdg_field_out* out) {
+  if (n < 0 || (n > 0 && (!fields || !out)) || !cfg) return HVDG_ERR_BAD_ARGUMENT;
+  if (cfg->diag_prior > 0.0f || cfg->symmetry_variant) return HVDG_ERR_UNSUPPORTED;
+  for (int i = 0; i < n; ++i) {
+    if (!fields[i].samples || !fields[i].geometry) return HVDG_ERR_BAD_ARGUMENT;
+    if (fields[i].sample_type < 0 || fields[i].sample_type > 2) return HVDG_ERR_BAD_ARGUMENT;
+    if (fields[i].sample_type != HVDG_SAMPLES_F32_IRE &&
+        !(fields[i].white_level != fields[i].blanking_level))
+      return HVDG_ERR_BAD_ARGUMENT;
+    const hvdg_status s = check_geometry(fields[i].geometry);
+    if (s != HVDG_OK) return s;
+  }
+  return HVDG_OK;
+}
+
+// DecodeFieldWindow (sequence.cpp:270-281, 423-1116) over one window of one
+// geometry. With the temporal terms off every field is independent (the
+// stride-1 sweep, sequence.cpp:1076-1084) and the window is one batch.
+hvdg_status decode_window_impl(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                               const hvdg_config* cfg, hvdg_field_out* out, hvdg_diag* diag) {
+  const hvdg_geometry& g = *fields[0].geometry;
+  const int amb_stride = uses_vswitch(g) ? 4 : 2;
+  const bool scan = cfg->temporal_strength == 0.0f && cfg->cg_iterations > 0 && n > amb_stride;
+  if (scan || cfg->temporal_strength > 0.0f) {
+    ctx->last_error = "temporal (3-D) window decode is not available in this build";
+    return HVDG_ERR_UNSUPPORTED;
+  }
+  cudaSetDevice(ctx->device);
+  if (diag) std::memset(diag, 0, sizeof(*diag));
+  RunOpts opt;
+  if (ctx->batched) return run_batch(ctx, fields, n, cfg, out, diag, opt);
+  for (int i = 0; i < n; ++i) {
+    const hvdg_status st = run_batch(ctx, fields + i, 1, cfg, out + i, diag, opt);
+    if (st != HVDG_OK) return st;
+  }
+  return HVDG_OK;
+}
+
+// Lock-in / burst amplitude of one IRE field (kernel-level entry points).
+hvdg_status lockin_one(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometry* g, float* theta,
+                       int8_t* vswitch, float* amp) {
+  hvdg_status st = check_geometry(g);
+  if (st != HVDG_OK) return st;
+  cudaSetDevice(ctx->device);
+  const size_t fbytes = sizeof(float) * g->field_width * g->field_height;
+  const size_t o_field = 0;
+  const size_t o_desc = align_up(fbytes, 256);
+  const size_t o_theta = align_up(o_desc + sizeof(hvdg::PrepDesc), 256);
+  const size_t o_vsw = align_up(o_theta + sizeof(float) * g->field_height, 256);
+  const size_t o_amp = align_up(o_vsw + g->field_height, 256);
+  const size_t o_lph = align_up(o_amp + sizeof(float), 256);
+  const size_t total = align_up(o_lph + sizeof(float4) * g->field_height, 256);
+  st = ctx->arena.reserve(total);
+  if (st != HVDG_OK) return st;
+  char* base = static_cast<char*>(ctx->arena.base);
+  hvdg::PrepDesc pd;
+  std::memset(&pd, 0, sizeof(pd));
+  pd.samples = base + o_field;
+  pd.sample_type = HVDG_SAMPLES_F32_IRE;
+  pd.quadrant = g->subcarrier_hz <= 0.0 ? 1 : 0;
+  pd.fh = g->field_height;
+  pd.fw = g->field_width;
+  pd.bx0 = g->colour_burst_start;
+  pd.bx1 = g->colour_burst_end;
+  pd.fal = g->first_active_field_line;
+  pd.lal = last_active_line(*g);
+  pd.a0 = g->active_video_start;
+  pd.a1 = g->active_video_end;
+  pd.vswitch_family = uses_vswitch(*g) ? 1 : 0;
+  pd.nominal_burst = nominal_burst(*g);
+  pd.w0 = phase_per_sample(*g);
+  pd.adv = line_advance(*g);
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(base + o_field, field_ire, fbytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D field");
+  e = cudaMemcpyAsync(base + o_desc, &pd, sizeof(pd), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D desc");
+  const hvdg::PrepDesc* dd = reinterpret_cast<const hvdg::PrepDesc*>(base + o_desc);
+  if (theta) {
+    hvdg::LockinOut lo;
+    lo.theta = reinterpret_cast<float*>(base + o_theta);
+    lo.theta64 = nullptr;
+    lo.vswitch = reinterpret_cast<signed char*>(base + o_vsw);
+    lo.line_phasor = reinterpret_cast<float4*>(base + o_lph);
+    hvdg::launch_burst_lockin(dd, 1, lo, s);
+    cudaMemcpyAsync(theta, base + o_theta, sizeof(float) * g->field_height, cudaMemcpyDeviceToHost, s);
+    if (vswitch) cudaMemcpyAsync(vswitch, base + o_vsw, g->field_height, cudaMemcpyDeviceToHost, s);
+  }
+  if (amp) {
+    hvdg::launch_burst_amplitude(dd, 1, reinterpret_cast<float*>(base + o_amp), s);
+    cudaMemcpyAsync(amp, base + o_amp, sizeof(float), cudaMemcpyDeviceToHost, s);
+  }
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "lock-in");
+  return HVDG_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int hvdg_abi_version(void) { return HVDG_ABI_VERSION; }
+
+const char* hvdg_status_string(hvdg_status s) {
+  switch (s) {
+    case HVDG_OK: return "HVDG_OK";
+    case HVDG_ERR_BAD_ARGUMENT: return "HVDG_ERR_BAD_ARGUMENT";
+    case HVDG_ERR_BAD_GEOMETRY: return "HVDG_ERR_BAD_GEOMETRY";
+    case HVDG_ERR_NONFINITE_INPUT: return "HVDG_ERR_NONFINITE_INPUT";
+    case HVDG_ERR_DEVICE_TIMEOUT: return "HVDG_ERR_DEVICE_TIMEOUT";
+    case HVDG_ERR_CUDA: return "HVDG_ERR_CUDA";
+    case HVDG_ERR_OUT_OF_MEMORY: return "HVDG_ERR_OUT_OF_MEMORY";
+    case HVDG_ERR_UNSUPPORTED: return "HVDG_ERR_UNSUPPORTED";
+    case HVDG_ERR_NO_DEVICE: return "HVDG_ERR_NO_DEVICE";
+  }
+  return "HVDG_ERR_UNKNOWN";
+}
+
+void hvdg_config_default(hvdg_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->lambda_c = 1.0f;
+  c->chroma_aniso = 0.0f;
+  c->charbonnier_eps = 0.5f;
+  c->chroma_eps = 1.0f;
+  c->structure_coupling = 0.25f;
+  c->diag_prior = 0.0f;
+  c->cg_iterations = 2;
+  c->irls_outer = 4;
+  c->cg_tol = 0.0f;
+  c->fast = 1;
+  c->parallel_across_fields = 1;
+  c->symmetry_variant = 0;
+  c->acc = 1;
+  c->chroma_gain = 1.0f;
+  c->monochrome = 0;
+  c->chroma_phase_deg = 0.0f;
+  c->field_order = 0;
+  c->temporal_strength = 0.0f;
+  c->bidirectional = 1;
+  c->passes = 2;
+  c->temporal_eps = 0.0f;
+  c->nr_anchor = 1.0f;
+  c->nr_eps = 0.0f;
+  c->nr_radius = 2;
+  c->mc_tile = 32;
+  c->mc_search = 16;
+  c->trajectory_fit = 1;
+  c->extended_temporal = 1;
+  c->coherence_gate = 0.6f;
+  c->odd_gate_floor = 0.35f;
+  c->output_fidelity = 1;
+  c->psi_init = 0;
+  c->me_mode = 0;
+  c->me_block = 16;
+  c->me_range = 16;
+}
+
+void hvdg_geometry_default(int standard, hvdg_geometry* g) {
+  if (!g) return;
+  std::memset(g, 0, sizeof(*g));
+  if (standard == HVDG_STD_PAL) {
+    g->field_width = 1135;
+    g->field_height = 313;
+    g->active_video_start = 185;
+    g->active_video_end = 1107;
+    g->colour_burst_start = 98;
+    g->colour_burst_end = 138;
+    g->first_active_field_line = 22;
+    g->sample_rate = 4.0 * 4433618.75;
+  } else {
+    g->field_width = 910;
+    g->field_height = 263;
+    g->active_video_start = 134;
+    g->active_video_end = 894;
+    g->colour_burst_start = 78;
+    g->colour_burst_end = 110;
+    g->first_active_field_line = 21;
+    g->sample_rate = 4.0 * 315.0e6 / 88.0;
+  }
+  g->last_active_field_line = 0;
+  g->standard = standard;
+  g->subcarrier_hz = 0.0;
+}
+
+hvdg_status hvdg_create(int device, hvdg_ctx** out) {
+  if (!out) return HVDG_ERR_BAD_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0 || device < 0 || device >= n) {
+    cudaGetLastError();
+    return HVDG_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+    cudaGetLastError();
+    return HVDG_ERR_NO_DEVICE;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return HVDG_ERR_NO_DEVICE;
+  }
+  hvdg_ctx* ctx = new hvdg_ctx();
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    cudaGetLastError();
+    return HVDG_ERR_CUDA;
+  }
+  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  *out = ctx;
+  return HVDG_OK;
+}
+
+void hvdg_destroy(hvdg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* hvdg_last_error(const hvdg_ctx* ctx) {
+  return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+hvdg_status hvdg_set_batching(hvdg_ctx* ctx, int batched) {
+  if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  ctx->batched = batched ? 1 : 0;
+  return HVDG_OK;
+}
+
+hvdg_status hvdg_set_tuning(hvdg_ctx* ctx, int band_rows, int ctas_per_sm) {
+  if (!ctx || band_rows < 0 || ctas_per_sm < 0) return HVDG_ERR_BAD_ARGUMENT;
+  ctx->band_rows = band_rows;
+  ctx->ctas_per_sm = ctas_per_sm;
+  return HVDG_OK;
+}
+
+static hvdg_status decode_fields_impl(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                                      const hvdg_config* cfg, hvdg_field_out* out,
+                                      hvdg_diag* diag, bool device_io) {
+  if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  hvdg_status st = validate_fields(fields, n, cfg, out);
+  if (st != HVDG_OK) return st;
+  if (n == 0) return HVDG_OK;
+  cudaSetDevice(ctx->device);
+  if (diag) std::memset(diag, 0, sizeof(*diag));
+  RunOpts opt;
+  opt.device_io = device_io;
+  if (ctx->batched) return run_batch(ctx, fields, n, cfg, out, diag, opt);
+  for (int i = 0; i < n; ++i) {
+    st = run_batch(ctx, fields + i, 1, cfg, out + i, diag, opt);
+    if (st != HVDG_OK) return st;
+  }
+  return HVDG_OK;
+}
+
+hvdg_status hvdg_decode_fields(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                               const hvdg_config* cfg, hvdg_field_out* out, hvdg_diag* diag) {
+  return decode_fields_impl(ctx, fields, n, cfg, out, diag, false);
+}
+
+hvdg_status hvdg_decode_fields_device(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                                      const hvdg_config* cfg, hvdg_field_out* out,
+                                      hvdg_diag* diag) {
+  return decode_fields_impl(ctx, fields, n, cfg, out, diag, true);
+}
+
+hvdg_status hvdg_decode_field_window(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                                     const hvdg_config* cfg, hvdg_field_out* out,
+                                     hvdg_diag* diag) {
+  if (!ctx || !cfg) return HVDG_ERR_BAD_ARGUMENT;
+  hvdg_status st = validate_fields(fields, n, cfg, out);
+  if (st != HVDG_OK) return st;
+  if (n == 0) return HVDG_OK;
+  for (int i = 1; i < n; ++i)
+    if (geom_key(*fields[i].geometry) != geom_key(*fields[0].geometry)) return HVDG_ERR_BAD_GEOMETRY;
+  return decode_window_impl(ctx, fields, n, cfg, out, diag);
+}
+
+hvdg_status hvdg_burst_lockin(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometry* g,
+                              float* theta, int8_t* vswitch) {
+  if (!ctx || !field_ire || !g || !theta) return HVDG_ERR_BAD_ARGUMENT;
+  if (uses_vswitch(*g) && !vswitch) return HVDG_ERR_BAD_ARGUMENT;
+  return lockin_one(ctx, field_ire, g, theta, vswitch, nullptr);
+}
+
+hvdg_status hvdg_burst_amplitude(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometry* g,
+                                 float* amplitude_ire) {
+  if (!ctx || !field_ire || !g || !amplitude_ire) return HVDG_ERR_BAD_ARGUMENT;
+  return lockin_one(ctx, field_ire, g, nullptr, nullptr, amplitude_ire);
+}
+
+hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref, const float* y_cur, int h,
+                                 int w, int tile, int search, int me_mode, float* dy, float* dx,
+                                 float* confidence) {
+  if (!ctx || !y_ref || !y_cur || !dy || !dx || !confidence || h < 1 || w < 1 || tile < 1 ||
+      search < 0 || me_mode < 0 || me_mode > 1)
+    return HVDG_ERR_BAD_ARGUMENT;
+  ctx->last_error = "motion estimation is not available in this build";
+  return HVDG_ERR_UNSUPPORTED;
+}
+
+hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* const* frames,
+                                              int n_frames, int core_begin, int core_end,
+                                              const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                              hvdg_yc_frame* out, hvdg_diag* diag) {
+  if (!ctx || !fp || !cfg) return HVDG_ERR_BAD_ARGUMENT;
+  (void)frames; (void)n_frames; (void)core_begin; (void)core_end; (void)out; (void)diag;
+  ctx->last_error = "frame bridge is not available in this build";
+  return HVDG_ERR_UNSUPPORTED;
+}
+
+hvdg_status hvdg_holographic_init(hvdg_ctx* ctx, const float* s, const float* theta_active,
+                                  const int8_t* vswitch_active, const hvdg_geometry* g,
+                                  const hvdg_config* cfg, float* luma0, float* chi0) {
+  if (!ctx || !s || !theta_active || !g || !cfg || !luma0 || !chi0) return HVDG_ERR_BAD_ARGUMENT;
+  hvdg_status st = check_geometry(g);
+  if (st != HVDG_OK) return st;
+  if (uses_vswitch(*g) && !vswitch_active) return HVDG_ERR_BAD_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  hvdg_field_in fi;
+  std::memset(&fi, 0, sizeof(fi));
+  fi.samples = s;
+  fi.sample_type = HVDG_SAMPLES_F32_IRE;
+  fi.geometry = g;
+  fi.irls_outer = 0;
+  fi.cg_iterations = -1;
+  hvdg_field_out fo;
+  std::memset(&fo, 0, sizeof(fo));
+  fo.luma = luma0;
+  fo.chroma = chi0;
+  RunOpts opt;
+  opt.do_lockin = false;
+  opt.do_solve = false;
+  opt.s_in = s;
+  opt.theta_in = theta_active;
+  opt.vswitch_in = vswitch_active;
+  return run_batch(ctx, &fi, 1, cfg, &fo, nullptr, opt);
+}
+
+hvdg_status hvdg_variational_refine(hvdg_ctx* ctx, const float* s, const float* theta_active,
+                                    const int8_t* vswitch_active, const float* chi0,
+                                    const hvdg_geometry* g, const hvdg_config* cfg, float* luma,
+                                    float* chi) {
+  if (!ctx || !s || !theta_active || !chi0 || !g || !cfg || !luma || !chi)
+    return HVDG_ERR_BAD_ARGUMENT;
+  hvdg_status st = check_geometry(g);
+  if (st != HVDG_OK) return st;
+  if (cfg->diag_prior > 0.0f) return HVDG_ERR_UNSUPPORTED;
+  if (uses_vswitch(*g) && !vswitch_active) return HVDG_ERR_BAD_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  hvdg_field_in fi;
+  std::memset(&fi, 0, sizeof(fi));
+  fi.samples = s;
+  fi.sample_type = HVDG_SAMPLES_F32_IRE;
+  fi.geometry = g;
+  fi.irls_outer = 0;
+  fi.cg_iterations = -1;
+  hvdg_field_out fo;
+  std::memset(&fo, 0, sizeof(fo));
+  fo.luma = luma;
+  fo.chroma = chi;
+  RunOpts opt;
+  opt.do_lockin = false;
+  opt.do_init = false;
+  opt.s_in = s;
+  opt.theta_in = theta_active;
+  opt.vswitch_in = vswitch_active;
+  opt.chi0_in = chi0;
+  return run_batch(ctx, &fi, 1, cfg, &fo, nullptr, opt);
+}
+
+}  // extern "C"

@@ -1,0 +1,122 @@
+// hvdg_common.cuh -- device helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hvdg_internal.h"
+
+namespace hvdg {
+
+// ---- complex float2 arithmetic --------------------------------------------
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return make_float2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) {
+  return make_float2(a.x * s, a.y * s);
+}
+__device__ __forceinline__ float cnorm(float2 a) { return a.x * a.x + a.y * a.y; }
+// Re[a * b]
+__device__ __forceinline__ float re_mul(float2 a, float2 b) { return a.x * b.x - a.y * b.y; }
+
+// Carrier at (line phasor, column phasor, V-switch sign): c = L * P, and
+// -conj(c) on switched lines (MakeCarrierPal, ntsc_geometry.cpp:438-456).
+__device__ __forceinline__ float2 carrier(float2 L, float2 P, float sw) {
+  float2 c = cmul(L, P);
+  return sw < 0.0f ? make_float2(-c.x, c.y) : c;
+}
+
+// ---- warp reductions --------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;  // valid in lane 0
+}
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_allmax(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Order-preserving map float -> uint32 (for radix selection).
+__device__ __forceinline__ uint32_t float_key(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  return __uint_as_float(u);
+}
+
+// Exact k-th smallest (0-based) of n floats in shared memory by the whole
+// block: 4-pass 8-bit radix select on order-preserving keys. `hist` is
+// 256 unsigned ints of shared scratch, `bcast` 2 unsigned ints. All threads
+// must call. Equivalent to std::nth_element(v, v + k, v + n); v[k].
+__device__ inline float block_select_kth(const float* v, int n, int k, unsigned* hist,
+                                         unsigned* bcast) {
+  uint32_t prefix = 0, mask = 0;
+  int kk = k;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t key = float_key(v[i]);
+      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned acc = 0;
+      int b = 0;
+      for (; b < 256; ++b) {
+        if (acc + hist[b] > (unsigned)kk) break;
+        acc += hist[b];
+      }
+      bcast[0] = (unsigned)b;
+      bcast[1] = acc;
+    }
+    __syncthreads();
+    const uint32_t b = bcast[0];
+    kk -= (int)bcast[1];
+    prefix |= b << shift;
+    mask |= 255u << shift;
+    __syncthreads();
+  }
+  return key_float(prefix);
+}
+
+// Bounded spin on a device-scope flag: returns true when *flag >= target
+// within the iteration budget, false on timeout (caller reports an error;
+// nothing traps or spins forever).
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+constexpr long long kSpinLimit = 4000000;  // x ~0.5 us sleeps ~= 2 s
+__device__ __forceinline__ bool wait_at_least(const int* flag, int target) {
+  long long n = 0;
+  while (ld_acquire(flag) < target) {
+    if (++n > kSpinLimit) return false;
+    __nanosleep(256);
+  }
+  return true;
+}
+
+}  // namespace hvdg

@@ -1,0 +1,33 @@
+// hvdg_host.h -- host-side helpers shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "hvdg.h"
+
+struct hvdg_ctx;
+
+namespace hvdg {
+
+// Grow-only device arena (one allocation per context; zeroed when grown).
+struct DeviceArena {
+  void* base = nullptr;
+  size_t capacity = 0;
+  hvdg_status reserve(size_t bytes);
+  ~DeviceArena();
+};
+
+// Grow-only pinned host staging buffer.
+struct PinnedArena {
+  void* base = nullptr;
+  size_t capacity = 0;
+  hvdg_status reserve(size_t bytes);
+  ~PinnedArena();
+};
+
+// Records a CUDA failure in the context and maps it to a status.
+hvdg_status cuda_fail(hvdg_ctx* ctx, cudaError_t e, const char* what);
+
+}  // namespace hvdg

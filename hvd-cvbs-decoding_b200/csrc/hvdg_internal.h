@@ -1,0 +1,83 @@
+// hvdg_internal.h -- host/device shared layouts of the batched field solver.
+//
+// Device memory holds a BATCH of fields. Every per-pixel plane of a field is
+// stored row-major with a row pitch that is a multiple of 64 elements (one
+// solver strip), at offset `px_off` (in pixels) inside one batch-wide array
+// per plane kind. Per-line and per-column carrier phasors replace the
+// reference's stored carrier plane (FieldObs::carrier, sequence.h:52-56):
+//   c(y, x) = L[y] * P[x],  L[y] = exp(i theta[y]),  P[x] = exp(i w0 (a0 + x))
+// and c -> -conj(c) on V-switched lines (MakeCarrierPal,
+// ntsc_geometry.cpp:438-456).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace hvdg {
+
+constexpr int kStrip = 64;        // solver strip width (columns per warp unit)
+constexpr int kMaxLines = 1024;   // max field lines handled by the lock-in kernel
+constexpr int kRowFft = 2048;     // init: row cyclic-convolution length
+constexpr int kColFft = 1024;     // init: column cyclic-convolution length
+constexpr int kInitPad = 16;      // init: reflect-101 row pad (holographic_init.cpp:214-222)
+
+// Per-field descriptor (device copy is read-only during a launch except the
+// fields marked "written by").
+struct FieldDesc {
+  int h, w;            // active lines / active width
+  int pitch;           // row pitch (elements), multiple of kStrip
+  int fh, fw;          // full field height / width
+  int64_t px_off;      // plane offset of this field (pixels)
+  int line_off;        // offset into per-line tables (active lines)
+  int col_off;         // offset into the column-phasor table (per geometry)
+  int geom;            // geometry slot (init kernels, column phasors)
+  int is_pal;          // V-switch family (aniso 4-line groups)
+  int n_outer;         // IRLS outer passes (>= 1)
+  int n_inner;         // CG iterations per outer (>= 1)
+  float cg_tol;        // relative gradient-norm exit
+  float eps, eps_c, k_coupling;  // Charbonnier scales, structure coupling
+  float lambda_c, aniso_cfg;     // lambda_c, fixed aniso (> 0) or 0 = auto
+  float mu_h, mu_v;    // written by the aniso kernel
+  float nu;            // temporal strength (0 = 2-D)
+  float eps_t;         // temporal robust scale
+  int has_nbr;         // 3-D neighbour terms present (M / b planes valid)
+  int n_nbr;           // neighbour planes
+  int64_t nbr_off;     // offset (float4) of this field's neighbour planes
+  int64_t plane_px;    // h * pitch (one plane of this field)
+  int unit_begin;      // first solver unit of this field
+  int unit_count;      // number of solver units
+  int n_phases;        // n_outer * (2 + n_inner) + 1
+  int pad0;
+};
+
+// Per-geometry init tables.
+struct GeomDesc {
+  int w, h, hp;        // active width, active lines, padded lines (h + 2 pad)
+  int pad;             // row pad
+  int khat_row_off;    // offset (float2) of the 2 row kernels' spectra (2 * kRowFft)
+  int khat_col_off;    // offset (float2) of the 2 column kernels' spectra (2 * kColFft)
+};
+
+// Solver control block, one per field (written by the last arriver of each
+// phase, read by every unit of the next phase).
+struct FieldCtl {
+  double gg;           // ||g_k||^2 (exact, of the stored residual)
+  double gg0;          // ||g_0||^2 of the current outer pass
+  double gg_next;      // ||g_{k+1}||^2 predicted by the recurrence
+  float alpha;         // pending step to apply (chi += alpha d, g += alpha q)
+  float beta;          // direction update factor for the next iteration
+  int pending;         // 1 => alpha/beta pending from the previous I phase
+  int cg_iters;        // CG iterations executed (stats)
+  int sel;             // which of the double-buffered g / d / q planes is current
+  int xsel;            // which of the double-buffered chi planes is current
+};
+
+// One solver work unit: a kStrip-wide strip x `band` rows of one field.
+struct Unit {
+  int field;
+  int x0;
+  int y0;
+  int y1;
+};
+
+}  // namespace hvdg

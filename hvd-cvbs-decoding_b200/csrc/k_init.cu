@@ -1,0 +1,366 @@
+// k_init.cu -- holographic initialisation (kernel b) and the auto chroma
+// anisotropy (variational.cpp:130-196).
+//
+// Reference: HolographicInit (hvd-core/src/engine/holographic_init.cpp:200-317):
+// demodulate S by conj(carrier), reflect-101 pad 16 rows, 2-D FFT, two
+// separable Gaussian sideband crops {0.8 MHz, 120 c/ph} and {1.8 MHz, 30 c/ph},
+// inverse FFT, crop, x2, edge-energy blend w = 1 / (BoxBlur_3(|Dx Y|+|Dy Y|) + 0.5).
+//
+// Because each crop mask is separable (gy[y] * gx[x]) the 2-D
+// "FFT -> mask -> inverse FFT" equals a circular convolution along rows with
+// k_x = IDFT_w(gx) followed by one along columns with k_y = IDFT_hp(gy). Each
+// circular convolution of length n runs as a cyclic convolution of
+// power-of-two length M >= 2n - 1 (rows: 2048, columns: 1024) with the
+// kernel's FFT precomputed on the host: forward radix-4/2 Stockham FFT in
+// shared memory, mask multiply fused in shared memory, inverse FFT, write.
+//   k_init_rows : one CTA per padded row -> both row-filtered variants
+//   k_init_cols : one CTA per 8-column group -> chi_1, chi_2 (x2 folded in)
+//   k_init_blend: edge-energy blend -> chi0, Y0
+#include <cuda_runtime.h>
+
+#include "hvdg_common.cuh"
+#include "k_init.h"
+
+namespace hvdg {
+
+// ---- Stockham autosort FFT (radix 4, one radix-2 stage when needed) --------
+// Length M (power of two). `tw` = exp(-2 pi i k / M), k in [0, M). Threads
+// [tid, nt) of the cooperating group call it together; `sync` separates the
+// stages. Returns the buffer (a or b) holding the result.
+template <int M, bool INV, typename Sync>
+__device__ __forceinline__ float2* fft_stockham(float2* a, float2* b,
+                                                const float2* __restrict__ tw, int tid,
+                                                int nt, Sync sync) {
+  float2* src = a;
+  float2* dst = b;
+#pragma unroll 1
+  for (int Ns = 1; Ns < M;) {
+    const int R = ((M / Ns) % 4 == 0) ? 4 : 2;
+    const int nb = M / R;
+    const int st = M / (Ns * R);
+    if (R == 4) {
+      for (int j = tid; j < nb; j += nt) {
+        const int k = j & (Ns - 1);
+        float2 v0 = src[j], v1 = src[j + nb], v2 = src[j + 2 * nb], v3 = src[j + 3 * nb];
+        if (k) {
+          float2 w1 = __ldg(tw + k * st), w2 = __ldg(tw + 2 * k * st), w3 = __ldg(tw + 3 * k * st);
+          if (INV) {
+            w1.y = -w1.y;
+            w2.y = -w2.y;
+            w3.y = -w3.y;
+          }
+          v1 = cmul(v1, w1);
+          v2 = cmul(v2, w2);
+          v3 = cmul(v3, w3);
+        }
+        const float2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = csub(v1, v3);
+        const float2 t3r = INV ? make_float2(-t3.y, t3.x) : make_float2(t3.y, -t3.x);
+        const int base = (j / Ns) * Ns * 4 + k;
+        dst[base] = cadd(t0, t2);
+        dst[base + Ns] = cadd(t1, t3r);
+        dst[base + 2 * Ns] = csub(t0, t2);
+        dst[base + 3 * Ns] = csub(t1, t3r);
+      }
+    } else {
+      for (int j = tid; j < nb; j += nt) {
+        const int k = j & (Ns - 1);
+        float2 v0 = src[j], v1 = src[j + nb];
+        if (k) {
+          float2 w1 = __ldg(tw + k * st);
+          if (INV) w1.y = -w1.y;
+          v1 = cmul(v1, w1);
+        }
+        const int base = (j / Ns) * Ns * 2 + k;
+        dst[base] = cadd(v0, v1);
+        dst[base + Ns] = csub(v0, v1);
+      }
+    }
+    sync();
+    float2* t = src;
+    src = dst;
+    dst = t;
+    Ns *= R;
+  }
+  return src;
+}
+
+struct BlockSync {
+  __device__ void operator()() const { __syncthreads(); }
+};
+struct WarpSync {
+  __device__ void operator()() const { __syncwarp(); }
+};
+
+__device__ __forceinline__ int mirror_row(int y, int h) {
+  // reflect-101 (holographic_init.cpp:126-131)
+  if (h <= 1) return 0;
+  const int period = 2 * h - 2;
+  y = ((y % period) + period) % period;
+  return y < h ? y : period - y;
+}
+
+__device__ __forceinline__ float2 carrier_at(const InitArgs& a, const FieldDesc& f, int y,
+                                             int x) {
+  const float4 L = __ldg(a.line_phasor + f.line_off + y);
+  const float2 P = __ldg(a.col_phasor + f.col_off + x);
+  return carrier(make_float2(L.x, L.y), P, L.z);
+}
+
+// ---- rows ------------------------------------------------------------------
+// grid = total padded rows; block = 256; dynamic smem = 3 * kRowFft float2.
+__global__ void __launch_bounds__(256) k_init_rows(InitArgs a) {
+  extern __shared__ float2 sm_rows[];
+  float2* X = sm_rows;
+  float2* P = X + kRowFft;
+  float2* Q = P + kRowFft;
+  const int r = blockIdx.x;
+  const int f_idx = a.prow_field[r];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  const int yp = r - a.prow_first[f_idx];
+  const int sy = mirror_row(yp - gd.pad, f.h);
+  const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
+  for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) {
+    float2 v = make_float2(0.f, 0.f);
+    if (i < f.w) {
+      const float s = S[i];
+      const float2 c = carrier_at(a, f, sy, i);
+      v = make_float2(s * c.x, -s * c.y);  // S * conj(c)
+    }
+    P[i] = v;
+  }
+  __syncthreads();
+  float2* spec = fft_stockham<kRowFft, false>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+  for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) X[i] = spec[i];
+  __syncthreads();
+  for (int v = 0; v < 2; ++v) {
+    const float2* kh = a.khat + gd.khat_row_off + v * kRowFft;
+    for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) P[i] = cmul(X[i], __ldg(kh + i));
+    __syncthreads();
+    float2* res = fft_stockham<kRowFft, true>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+    float2* out = a.rowbuf + a.rowbuf_off[f_idx] + ((int64_t)v * gd.hp + yp) * f.pitch;
+    for (int i = threadIdx.x; i < f.pitch; i += blockDim.x)
+      out[i] = i < f.w ? res[i] : make_float2(0.f, 0.f);
+    __syncthreads();
+  }
+}
+
+// ---- columns ---------------------------------------------------------------
+// grid = (column groups of 8, over all fields); block = 256 (8 warps, one
+// column each); dynamic smem = 8 * 2 * kColFft float2.
+constexpr int kColGroup = 8;
+__global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
+  extern __shared__ float2 sm_cols[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gidx = blockIdx.x;
+  const int f_idx = a.cgrp_field[gidx];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
+  float2* A = sm_cols + warp * 2 * kColFft;
+  float2* B = A + kColFft;
+  for (int v = 0; v < 2; ++v) {
+    const float2* src = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
+    // cooperative coalesced load: thread -> (row, column-in-group)
+    for (int i = threadIdx.x; i < kColFft * kColGroup; i += blockDim.x) {
+      const int row = i / kColGroup, c = i % kColGroup;
+      float2 val = make_float2(0.f, 0.f);
+      if (row < gd.hp && x0 + c < f.w) val = src[(int64_t)row * f.pitch + x0 + c];
+      sm_cols[c * 2 * kColFft + row] = val;
+    }
+    __syncthreads();
+    float2* spec = fft_stockham<kColFft, false>(A, B, a.tw_col, lane, 32, WarpSync());
+    const float2* kh = a.khat + gd.khat_col_off + v * kColFft;
+    float2* other = spec == A ? B : A;
+    for (int i = lane; i < kColFft; i += 32) other[i] = cmul(spec[i], __ldg(kh + i));
+    __syncwarp();
+    float2* res = fft_stockham<kColFft, true>(other, spec, a.tw_col, lane, 32, WarpSync());
+    // result must land where the cooperative store reads it: column c at A_c
+    if (res != A)
+      for (int i = lane; i < kColFft; i += 32) A[i] = res[i];
+    __syncthreads();
+    float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
+    for (int i = threadIdx.x; i < f.h * kColGroup; i += blockDim.x) {
+      const int y = i / kColGroup, c = i % kColGroup;
+      if (x0 + c < f.w)
+        dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * kColFft + y + gd.pad];
+    }
+    __syncthreads();
+  }
+}
+
+// ---- blend -----------------------------------------------------------------
+// Edge-energy blend (holographic_init.cpp:240-316). 32 x 32 output tile per
+// CTA; y_v on the tile + 4 halo (forward difference + box radius 3); the box
+// blur is zero-padded at the field border with constant 1/7 normalisation.
+constexpr int kBT = 32;
+constexpr int kBH = kBT + 8;  // y_v tile incl. halo [-3, +4]
+__global__ void __launch_bounds__(256) k_init_blend(InitArgs a) {
+  const int f_idx = a.btile_field[blockIdx.x];
+  const FieldDesc f = a.fields[f_idx];
+  const int t = blockIdx.x - a.btile_first[f_idx];
+  const int ntx = (f.w + kBT - 1) / kBT;
+  const int ty0 = (t / ntx) * kBT, tx0 = (t % ntx) * kBT;
+  __shared__ float yv[kBH][kBH + 1];
+  __shared__ float ev[kBH][kBH + 1];
+  __shared__ float vb[kBT][kBH + 1];
+  __shared__ float wsum[kBT][kBT];
+  __shared__ float2 num[kBT][kBT];
+  const float* S = a.S + f.px_off;
+  for (int v = 0; v < 2; ++v) {
+    const float2* chi = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
+    // residual luma on [ty0-3, ty0+kBT+5) x [tx0-3, ...)
+    for (int i = threadIdx.x; i < kBH * kBH; i += blockDim.x) {
+      const int ly = i / kBH, lx = i % kBH;
+      const int y = ty0 - 3 + ly, x = tx0 - 3 + lx;
+      float val = 0.f;
+      if (y >= 0 && y < f.h && x >= 0 && x < f.w) {
+        const int64_t o = (int64_t)y * f.pitch + x;
+        val = S[o] - re_mul(chi[o], carrier_at(a, f, y, x));
+      }
+      yv[ly][lx] = val;
+    }
+    __syncthreads();
+    // e = |Dx y| + |Dy y| (forward, zero on the last column / row), zero
+    // outside the field (the box blur's zero padding).
+    for (int i = threadIdx.x; i < (kBH - 1) * (kBH - 1); i += blockDim.x) {
+      const int ly = i / (kBH - 1), lx = i % (kBH - 1);
+      const int y = ty0 - 3 + ly, x = tx0 - 3 + lx;
+      float e = 0.f;
+      if (y >= 0 && y < f.h && x >= 0 && x < f.w) {
+        const float dx = (x + 1 < f.w) ? yv[ly][lx + 1] - yv[ly][lx] : 0.f;
+        const float dy = (y + 1 < f.h) ? yv[ly + 1][lx] - yv[ly][lx] : 0.f;
+        e = fabsf(dx) + fabsf(dy);
+      }
+      ev[ly][lx] = e;
+    }
+    __syncthreads();
+    // vertical box (rows of the tile, all halo columns)
+    for (int i = threadIdx.x; i < kBT * (kBT + 6); i += blockDim.x) {
+      const int ly = i / (kBT + 6), lx = i % (kBT + 6);
+      float acc = 0.f;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) acc += ev[ly + k][lx];
+      vb[ly][lx] = acc * (1.0f / 7.0f);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kBT * kBT; i += blockDim.x) {
+      const int ly = i / kBT, lx = i % kBT;
+      const int y = ty0 + ly, x = tx0 + lx;
+      float acc = 0.f;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) acc += vb[ly][lx + k];
+      const float E = acc * (1.0f / 7.0f);
+      const float wt = 1.0f / (E + 0.5f);
+      float2 cv = make_float2(0.f, 0.f);
+      if (y < f.h && x < f.w) cv = chi[(int64_t)y * f.pitch + x];
+      if (v == 0) {
+        num[ly][lx] = cscale(cv, wt);
+        wsum[ly][lx] = wt;
+      } else {
+        num[ly][lx] = cadd(num[ly][lx], cscale(cv, wt));
+        wsum[ly][lx] += wt;
+      }
+    }
+    __syncthreads();
+  }
+  float2* X = a.chi0 + f.px_off;
+  float* Y = a.Y + f.px_off;
+  for (int i = threadIdx.x; i < kBT * kBT; i += blockDim.x) {
+    const int ly = i / kBT, lx = i % kBT;
+    const int y = ty0 + ly, x = tx0 + lx;
+    if (y < f.h && x < f.w) {
+      const float2 c0 = make_float2(num[ly][lx].x / wsum[ly][lx], num[ly][lx].y / wsum[ly][lx]);
+      const int64_t o = (int64_t)y * f.pitch + x;
+      X[o] = c0;
+      Y[o] = S[o] - re_mul(c0, carrier_at(a, f, y, x));
+    }
+  }
+}
+
+// ---- auto chroma anisotropy (variational.cpp:130-196) ----------------------
+// One CTA (1024 threads) per field: p98 of |delta| of 2-line (NTSC) / 4-line
+// (PAL) group averages, sampled at odd group rows and every 3rd column,
+// exact k-th element by radix select.
+constexpr int kAnisoMax = 24576;
+__global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2* __restrict__ chi0) {
+  extern __shared__ float sm_an[];
+  __shared__ unsigned hist[256];
+  __shared__ unsigned bc[2];
+  FieldDesc& f = fields[blockIdx.x];
+  float aniso = f.aniso_cfg;
+  if (!(aniso > 0.0f)) {
+    const int group = f.is_pal ? 4 : 2;
+    const int Hh = f.h / group;
+    const int nt = Hh / 2;                // t = 1, 3, 5, ... < Hh
+    const int nx = (f.w - 1 + 2) / 3;     // x = 1, 4, 7, ... < w
+    int n = nt * nx;
+    if (n > kAnisoMax) n = kAnisoMax;     // geometry guard (host rejects larger)
+    float* gx = sm_an;
+    float* gy = sm_an + kAnisoMax;
+    const float2* c = chi0 + f.px_off;
+    const float inv = 1.0f / (float)group;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int ti = i / nx, xi = i % nx;
+      const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
+      float2 p = make_float2(0.f, 0.f), pl = p, pu = p;
+      for (int k = 0; k < group; ++k) {
+        p = cadd(p, c[(int64_t)(group * tt + k) * f.pitch + x]);
+        pl = cadd(pl, c[(int64_t)(group * tt + k) * f.pitch + x - 1]);
+        pu = cadd(pu, c[(int64_t)(group * (tt - 1) + k) * f.pitch + x]);
+      }
+      p = cscale(p, inv);
+      pl = cscale(pl, inv);
+      pu = cscale(pu, inv);
+      gx[i] = sqrtf(cnorm(csub(p, pl)));
+      gy[i] = sqrtf(cnorm(csub(p, pu)));
+    }
+    __syncthreads();
+    float px = 0.f, py = 0.f;
+    if (n > 0) {
+      const int k = n - 1 - n / 50;
+      px = block_select_kth(gx, n, k, hist, bc);
+      py = block_select_kth(gy, n, k, hist, bc);
+    }
+    const float r = py / fmaxf(px, 1e-6f);
+    if (f.is_pal)
+      aniso = fminf(fmaxf(0.7f + 0.9f * (r - 1.3f), 0.55f), 1.0f);
+    else
+      aniso = fminf(fmaxf(0.5f + 1.1f * (r - 1.3f), 0.5f), 1.0f);
+  }
+  if (threadIdx.x == 0) {
+    f.mu_h = f.lambda_c * aniso;
+    f.mu_v = f.lambda_c;
+  }
+}
+
+void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
+                 cudaStream_t st) {
+  static bool configured = false;
+  const int row_smem = 3 * kRowFft * sizeof(float2);
+  const int col_smem = kColGroup * 2 * kColFft * sizeof(float2);
+  if (!configured) {
+    cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem);
+    cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem);
+    configured = true;
+  }
+  if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
+  if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
+  if (total_btiles > 0) k_init_blend<<<total_btiles, 256, 0, st>>>(a);
+}
+
+void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {
+  static bool configured = false;
+  const int smem = 2 * kAnisoMax * sizeof(float);
+  if (!configured) {
+    cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    configured = true;
+  }
+  if (n_fields > 0) k_aniso<<<n_fields, 1024, smem, st>>>(d_fields, chi0);
+}
+
+int aniso_max_samples() { return kAnisoMax; }
+int init_col_group() { return kColGroup; }
+int init_blend_tile() { return kBT; }
+
+}  // namespace hvdg

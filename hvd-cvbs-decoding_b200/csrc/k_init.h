@@ -1,0 +1,41 @@
+// k_init.h -- launchers of the holographic-init and aniso kernels (k_init.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hvdg_internal.h"
+
+namespace hvdg {
+
+struct InitArgs {
+  const FieldDesc* fields;
+  const GeomDesc* geoms;
+  const float* S;              // active composite planes
+  const float4* line_phasor;   // per active line (cos, sin, sign, 0)
+  const float2* col_phasor;    // per geometry column exp(i w0 (a0 + x))
+  const float2* khat;          // kernel spectra (row / column, 2 variants each)
+  const float2* tw_row;        // exp(-2 pi i k / kRowFft)
+  const float2* tw_col;        // exp(-2 pi i k / kColFft)
+  float2* rowbuf;              // row-filtered variants: per field 2 x hp x pitch
+  const int64_t* rowbuf_off;   // per field offset into rowbuf (float2)
+  float2* chi1;                // variant outputs (pitched like the planes)
+  float2* chi2;
+  float2* chi0;                // blended init chi0
+  float* Y;                    // init luma Y0
+  const int* prow_field;       // padded row -> field
+  const int* prow_first;       // field -> first padded row index
+  const int* cgrp_field;       // column group -> field
+  const int* cgrp_first;       // field -> first column group
+  const int* btile_field;      // blend tile -> field
+  const int* btile_first;      // field -> first blend tile
+};
+
+void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
+                 cudaStream_t st);
+void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st);
+int aniso_max_samples();
+int init_col_group();
+int init_blend_tile();
+
+}  // namespace hvdg

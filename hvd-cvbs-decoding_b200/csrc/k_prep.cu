@@ -1,0 +1,368 @@
+// k_prep.cu -- field preparation: level conversion + active crop, burst
+// lock-in (kernel a), burst amplitude (ACC), carrier phasor tables.
+//
+// Reference: PrepareFieldObs (hvd-core/src/engine/sequence.cpp:229-268),
+// BurstLockin / BurstLockinPhase / BurstLockinPhasePal / BurstAmplitudeIre
+// (engine/lockin.cpp:103-417), SampleToIre (engine/ntsc_geometry.h:301-304),
+// ApplyChromaPhase (ntsc_geometry.h:341-352).
+//
+// One CTA per field for the lock-in: the per-line quadrature demodulation is
+// a warp-shuffle reduction over the burst window accumulated in FP64; the
+// per-field trajectory smoothing (two Thomas solves over <= 1024 lines) is a
+// short serial section.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "hvdg_common.cuh"
+#include "k_prep.h"
+
+namespace hvdg {
+
+__device__ __forceinline__ float sample_ire(const PrepDesc& p, int64_t idx) {
+  float s;
+  if (p.sample_type == 1) {
+    s = (float)__ldg(reinterpret_cast<const uint16_t*>(p.samples) + idx);
+  } else if (p.sample_type == 2) {
+    s = (float)__ldg(reinterpret_cast<const int16_t*>(p.samples) + idx);
+  } else {
+    return __ldg(reinterpret_cast<const float*>(p.samples) + idx);
+  }
+  // (s - blanking) / ((white - blanking) / 100): same float operations as
+  // SampleToIre / CodesPerIre.
+  return __fdiv_rn(__fsub_rn(s, p.blank), p.codes_per_ire);
+}
+
+// exp(-i w0 x) in FP64; exact quadrants when w0 == pi/2.
+__device__ __forceinline__ double2 lo_phasor(const PrepDesc& p, int x) {
+  if (p.quadrant) {
+    switch (x & 3) {
+      case 0: return make_double2(1.0, 0.0);
+      case 1: return make_double2(0.0, -1.0);
+      case 2: return make_double2(-1.0, 0.0);
+      default: return make_double2(0.0, 1.0);
+    }
+  }
+  double s, c;
+  sincos(p.w0 * (double)x, &s, &c);
+  return make_double2(c, -s);
+}
+
+__device__ __forceinline__ double wrap_pi(double a) { return atan2(sin(a), cos(a)); }
+
+// k-th smallest (0-based) among v[0..n) (doubles in shared memory), exact,
+// by rank counting; all threads call; result broadcast through *out.
+__device__ void block_rank_select(const double* v, int n, int k, double* out) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double vi = v[i];
+    int less = 0, eq = 0;
+    for (int j = 0; j < n; ++j) {
+      const double vj = v[j];
+      less += vj < vi;
+      eq += vj == vi;
+    }
+    if (less <= k && k < less + eq) *out = vi;  // every writer writes the same value
+  }
+  __syncthreads();
+}
+
+// Thomas algorithm for (diag(a) + lam L) x = a d (TridiagSmooth,
+// lockin.cpp:133-167). Serial; called by one thread.
+__device__ void tridiag_smooth(const double* d, const double* a, int n, double lam,
+                               double* x, double* c, double* dd) {
+  if (n == 0) return;
+  if (n == 1) {
+    x[0] = a[0] > 0.0 ? d[0] : 0.0;
+    return;
+  }
+  const double off = -lam;
+  auto diag = [&](int i) {
+    double v = a[i] + 2.0 * lam;
+    if (i == 0 || i == n - 1) v -= lam;
+    return v;
+  };
+  c[0] = off / diag(0);
+  dd[0] = a[0] * d[0] / diag(0);
+  for (int i = 1; i < n; ++i) {
+    const double m = diag(i) - off * c[i - 1];
+    if (i < n - 1) c[i] = off / m;
+    dd[i] = (a[i] * d[i] - off * dd[i - 1]) / m;
+  }
+  x[n - 1] = dd[n - 1];
+  for (int i = n - 2; i >= 0; --i) x[i] = dd[i] - c[i] * x[i + 1];
+}
+
+// One CTA per field. blockDim = 256.
+__global__ void __launch_bounds__(256) k_burst_lockin(const PrepDesc* __restrict__ descs,
+                                                      LockinOut out) {
+  const PrepDesc p = descs[blockIdx.x];
+  const int h = p.fh;
+  extern __shared__ double lk_smem[];
+  double* zr = lk_smem;
+  double* zi = zr + kMaxLines;
+  double* amp = zi + kMaxLines;
+  double* d = amp + kMaxLines;
+  double* a = d + kMaxLines;
+  double* x = a + kMaxLines;
+  double* model = x + kMaxLines;
+  double* tc = model + kMaxLines;
+  double* tdd = tc + kMaxLines;
+  double* gbuf = tdd + kMaxLines;
+  signed char* good = reinterpret_cast<signed char*>(gbuf + kMaxLines);
+  signed char* sw = good + kMaxLines;
+  __shared__ double s_amax, s_med, s_score[2];
+  __shared__ int s_fg, s_ngood;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int x0 = p.bx0, x1 = p.bx1, n = max(0, x1 - x0);
+  // ---- per-line lock-in: z = mean((seg - mean) * exp(-i w0 x)) -------------
+  for (int y = warp; y < h; y += nwarps) {
+    double sum = 0.0;
+    for (int xx = x0 + lane; xx < x1; xx += 32) sum += (double)sample_ire(p, (int64_t)y * p.fw + xx);
+    sum = warp_allsum(sum);
+    const double mean = n > 0 ? sum / n : 0.0;
+    double ar = 0.0, ai = 0.0;
+    for (int xx = x0 + lane; xx < x1; xx += 32) {
+      const double v = (double)sample_ire(p, (int64_t)y * p.fw + xx) - mean;
+      const double2 ph = lo_phasor(p, xx);
+      ar += v * ph.x;
+      ai += v * ph.y;
+    }
+    ar = warp_allsum(ar);
+    ai = warp_allsum(ai);
+    if (lane == 0) {
+      zr[y] = n > 0 ? ar / n : 0.0;
+      zi[y] = n > 0 ? ai / n : 0.0;
+      amp[y] = sqrt(zr[y] * zr[y] + zi[y] * zi[y]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int y = 0; y < h; ++y) m = fmax(m, amp[y]);
+    s_amax = m;
+    const double thr = m > 0.0 ? m * 0.2 : 1.0;
+    int fg = -1, ng = 0;
+    for (int y = 0; y < h; ++y) {
+      good[y] = amp[y] > thr;
+      if (good[y]) {
+        if (fg < 0) fg = y;
+        gbuf[ng++] = amp[y];
+      }
+    }
+    s_fg = fg;
+    s_ngood = ng;
+  }
+  __syncthreads();
+  const int fg = s_fg;
+  const double adv = p.adv;
+  const double hpi = 0.5 * CUDART_PI;
+  const double qpi = 0.25 * CUDART_PI;
+  double* theta = model;  // reuse: final theta is written over model at the end
+
+  if (fg < 0) {
+    // No burst anywhere: NTSC keeps the raw angles (lockin.cpp:211); PAL uses
+    // the model phase with alternating parity (lockin.cpp:348-355).
+    for (int y = threadIdx.x; y < h; y += blockDim.x) {
+      if (p.vswitch_family) {
+        x[y] = adv * y;
+        sw[y] = (y % 2 == 0) ? 1 : -1;
+      } else {
+        x[y] = atan2(zi[y], zr[y]) - hpi;
+        sw[y] = 1;
+      }
+    }
+    __syncthreads();
+  } else {
+    if (!p.vswitch_family) {
+      // NTSC (lockin.cpp:198-228)
+      const double th_fg = atan2(zi[fg], zr[fg]) - hpi;
+      for (int y = threadIdx.x; y < h; y += blockDim.x) {
+        const double th = atan2(zi[y], zr[y]) - hpi;
+        model[y] = th_fg + adv * (double)(y - fg);
+        d[y] = wrap_pi(th - model[y]);
+        sw[y] = 1;
+      }
+    } else {
+      // PAL family: two parity hypotheses (lockin.cpp:360-397)
+      const double a_fg = atan2(zi[fg], zr[fg]);
+      for (int hyp = 0; hyp < 2; ++hyp) {
+        const double s_ref = hyp == 0 ? 1.0 : -1.0;
+        const double theta_ref = a_fg - hpi + s_ref * qpi;
+        double acc = 0.0;
+        for (int y = threadIdx.x; y < h; y += blockDim.x) {
+          if (!good[y]) continue;
+          const double m = theta_ref + adv * (double)(y - fg);
+          const bool same = ((y - fg) % 2) == 0;
+          const double sy = same ? s_ref : -s_ref;
+          const double dev = wrap_pi(atan2(zi[y], zr[y]) - (m + hpi - sy * qpi));
+          acc += cos(dev) * amp[y];
+        }
+        acc = warp_allsum(acc);
+        __shared__ double red[32];
+        if (lane == 0) red[warp] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double t = 0.0;
+          for (int w = 0; w < nwarps; ++w) t += red[w];
+          s_score[hyp] = t;
+        }
+        __syncthreads();
+      }
+      // hypothesis 0 wins ties (strict > against an initial -1e30)
+      const double s_ref = (s_score[1] > s_score[0]) ? -1.0 : 1.0;
+      const double theta_ref = a_fg - hpi + s_ref * qpi;
+      for (int y = threadIdx.x; y < h; y += blockDim.x) {
+        const double m = theta_ref + adv * (double)(y - fg);
+        const bool same = ((y - fg) % 2) == 0;
+        const double sy = same ? s_ref : -s_ref;
+        model[y] = m;
+        sw[y] = sy > 0 ? 1 : -1;
+        const double theta_meas = atan2(zi[y], zr[y]) - hpi + sy * qpi;
+        d[y] = wrap_pi(theta_meas - m);
+      }
+    }
+    __syncthreads();
+    // median good amplitude (upper median, lockin.cpp:85-90) + weights
+    block_rank_select(gbuf, s_ngood, s_ngood / 2, &s_med);
+    const double med = s_med + 1e-9;
+    for (int y = threadIdx.x; y < h; y += blockDim.x)
+      a[y] = good[y] ? fmin(fmax(amp[y] / med, 0.0), 2.0) : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tridiag_smooth(d, a, h, 25.0, x, tc, tdd);
+      for (int y = 0; y < h; ++y) {
+        const double r = fabs(d[y] - x[y]);
+        a[y] = a[y] * 0.15 / fmax(r, 0.15);
+      }
+      tridiag_smooth(d, a, h, 25.0, x, tc, tdd);
+      for (int y = 0; y < h; ++y) x[y] = model[y] + x[y];
+    }
+    __syncthreads();
+  }
+  // x[] now holds theta. Chroma-phase trim (ApplyChromaPhase).
+  for (int y = threadIdx.x; y < h; y += blockDim.x) {
+    double th = x[y];
+    if (p.chroma_phase_off != 0.0f) {
+      const double off = (double)p.chroma_phase_off;
+      th += (p.vswitch_family && sw[y] < 0) ? -off : off;
+    }
+    if (out.theta) out.theta[p.theta_off + y] = (float)th;
+    if (out.theta64) out.theta64[p.theta_off + y] = th;
+    if (out.vswitch) out.vswitch[p.theta_off + y] = sw[y];
+    if (out.line_phasor && y >= p.fal && y < p.lal) {
+      double s, c;
+      sincos(th, &s, &c);
+      out.line_phasor[p.line_off + (y - p.fal)] =
+          make_float4((float)c, (float)s, sw[y] < 0 ? -1.0f : 1.0f, 0.0f);
+    }
+  }
+  (void)theta;
+}
+
+// BurstAmplitudeIre (lockin.cpp:256-323). One CTA per field.
+__global__ void __launch_bounds__(256) k_burst_amplitude(const PrepDesc* __restrict__ descs,
+                                                         float* __restrict__ amp_out) {
+  const PrepDesc p = descs[blockIdx.x];
+  const int h = p.fh;
+  const int x0 = p.bx0, x1 = p.bx1;
+  __shared__ double per_line[kMaxLines];
+  __shared__ double env[8][64];
+  __shared__ double s_m;
+  __shared__ double good[kMaxLines];
+  __shared__ int s_ng;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  if (x1 - x0 < 4) {
+    if (threadIdx.x == 0) amp_out[blockIdx.x] = p.nominal_burst;
+    return;
+  }
+  const int nenv = min(x1 - x0 - 3, 64);
+  for (int y = warp; y < h; y += nwarps) {
+    for (int s = lane; s < nenv; s += 32) {
+      double ar = 0.0, ai = 0.0;
+      for (int k = 0; k < 4; ++k) {
+        const int xx = x0 + s + k;
+        const double v = (double)sample_ire(p, (int64_t)y * p.fw + xx);
+        const double2 ph = lo_phasor(p, xx);
+        ar += v * ph.x;
+        ai += v * ph.y;
+      }
+      env[warp][s] = 2.0 * sqrt(ar * ar + ai * ai) * 0.25;
+    }
+    __syncwarp();
+    // upper median of env[warp][0..nenv) by rank counting within the warp
+    const int kq = nenv / 2;
+    for (int i = lane; i < nenv; i += 32) {
+      const double vi = env[warp][i];
+      int less = 0, eq = 0;
+      for (int j = 0; j < nenv; ++j) {
+        less += env[warp][j] < vi;
+        eq += env[warp][j] == vi;
+      }
+      if (less <= kq && kq < less + eq) per_line[y] = vi;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  block_rank_select(per_line, h, h / 2, &s_m);
+  if (threadIdx.x == 0) {
+    const double thr = 0.25 * s_m;
+    int ng = 0;
+    for (int y = 0; y < h; ++y)
+      if (per_line[y] > thr) good[ng++] = per_line[y];
+    s_ng = ng;
+  }
+  __syncthreads();
+  if (s_ng == 0) {
+    if (threadIdx.x == 0) amp_out[blockIdx.x] = p.nominal_burst;
+    return;
+  }
+  block_rank_select(good, s_ng, s_ng / 2, &s_m);
+  if (threadIdx.x == 0) amp_out[blockIdx.x] = (float)s_m;
+}
+
+// Active crop + level conversion into the pitched S plane; zero fill of the
+// pitch padding; non-finite detection. grid = (rows of all fields).
+__global__ void k_crop(const PrepDesc* __restrict__ descs, const int* __restrict__ row_field,
+                       const int* __restrict__ row_first, float* __restrict__ S,
+                       const int64_t* __restrict__ px_off, const int* __restrict__ pitch,
+                       int* __restrict__ nonfinite) {
+  const int r = blockIdx.x;
+  const int f = row_field[r];
+  const int y = r - row_first[f];
+  const PrepDesc p = descs[f];
+  const int w = p.a1 - p.a0;
+  float* dst = S + px_off[f] + (int64_t)y * pitch[f];
+  const int64_t src = (int64_t)(p.fal + y) * p.fw + p.a0;
+  for (int x = threadIdx.x; x < pitch[f]; x += blockDim.x) {
+    float v = 0.0f;
+    if (x < w) {
+      v = sample_ire(p, src + x);
+      if (!isfinite(v)) atomicOr(nonfinite, 1);
+    }
+    dst[x] = v;
+  }
+}
+
+constexpr size_t kLockinSmem = 10 * kMaxLines * sizeof(double) + 2 * kMaxLines;
+
+void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_burst_lockin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kLockinSmem);
+    configured = true;
+  }
+  if (n > 0) k_burst_lockin<<<n, 256, kLockinSmem, st>>>(d_descs, out);
+}
+void launch_burst_amplitude(const PrepDesc* d_descs, int n, float* d_amp, cudaStream_t st) {
+  if (n > 0) k_burst_amplitude<<<n, 256, 0, st>>>(d_descs, d_amp);
+}
+void launch_crop(const PrepDesc* d_descs, const int* d_row_field, const int* d_row_first,
+                 int total_rows, float* d_S, const int64_t* d_px_off, const int* d_pitch,
+                 int* d_nonfinite, cudaStream_t st) {
+  if (total_rows > 0)
+    k_crop<<<total_rows, 256, 0, st>>>(d_descs, d_row_field, d_row_first, d_S, d_px_off,
+                                       d_pitch, d_nonfinite);
+}
+
+}  // namespace hvdg

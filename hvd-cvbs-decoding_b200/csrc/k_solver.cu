@@ -1,0 +1,614 @@
+// k_solver.cu -- persistent IRLS + conjugate-gradient Y/C arbitration
+// (kernel c) over a batch of fields of any geometry.
+//
+// Reference: VariationalRefine (hvd-core/src/engine/variational.cpp:198-556):
+// per IRLS outer pass, Charbonnier / coupled diffusivities at the current
+// chi (:406-433), then CG on the fixed-weight quadratic with
+//   alpha = -0.5 <g,d> / curv(d),  beta = ||g'||^2 / ||g||^2  (:519-549),
+// the gradient g(chi) = -2[DxT(wx Dx Yc) + DyT(wy Dy Yc)] conj(c)
+//                       + 2[mu_h DxT(wcx Dx chi) + mu_v DyT(wcy Dy chi)]
+// (:286-347), FP64 inner products (:72-95), early exits (:530, :547-548).
+//
+// B200 formulation (same iterates in exact arithmetic):
+//  * The gradient is affine in chi, so g(chi + a d) = g(chi) + a q with
+//    q = g(d) - g(0) (the stencil applied to d with S = 0), and
+//    curv(d) = sum wx (Dx dY)^2 + ... is computed from the same differences.
+//    One CG iteration is ONE fused sweep: apply the pending step
+//    (chi += a d, g += a q), form d = -g + b d, compute q = A d, and
+//    accumulate <curv>, <g,d>, <g,q>, <q,q>, <g,g> in FP64. The next ||g||^2
+//    follows from ||g + a q||^2 = gg + 2a gq + a^2 qq, so each iteration
+//    needs one reduction point instead of two; gg itself is re-measured
+//    exactly every sweep.
+//  * Work is split into units (64-column strip x band of rows, one warp).
+//    Units of all fields and all phases form one ordered queue; a warp takes
+//    the next item, waits (bounded) until its field completed the previous
+//    phase, and the last unit to finish a phase reduces the field's partials
+//    in a fixed order and publishes the field's scalars. Fields therefore
+//    progress independently with no grid-wide barrier, and the reduction is
+//    deterministic.
+//  * Planes read with a halo are double-buffered (chi, g, d, q) so a unit
+//    never reads a neighbour's freshly written rows.
+//  * Each lane owns two adjacent pixels (128-bit loads of complex pairs);
+//    horizontal neighbours come from warp shuffles, vertical neighbours from
+//    a rolling window of rows kept in registers.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "hvdg_common.cuh"
+#include "k_solver.h"
+
+namespace hvdg {
+
+constexpr int kNPart = 5;
+
+__device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
+  const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
+  a = make_float2(v.x, v.y);
+  b = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void st_pair(float2* p, float2 a, float2 b, bool va, bool vb) {
+  if (va && vb) {
+    __stcg(reinterpret_cast<float4*>(p), make_float4(a.x, a.y, b.x, b.y));
+  } else {
+    if (va) __stcg(p, a);
+    if (vb) __stcg(p + 1, b);
+  }
+}
+__device__ __forceinline__ void ld_pairf(const float* p, float& a, float& b) {
+  const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+  a = v.x;
+  b = v.y;
+}
+
+struct Lanes {
+  int xa, xb, hx;
+  bool va, vb, hv;
+  float2 Pa, Pb, Ph;
+};
+
+__device__ __forceinline__ Lanes make_lanes(const SolverArgs& A, const FieldDesc& f, int x0,
+                                            int lane) {
+  Lanes l;
+  l.xa = x0 + 2 * lane;
+  l.xb = l.xa + 1;
+  l.va = l.xa < f.w;
+  l.vb = l.xb < f.w;
+  l.hx = lane == 0 ? x0 - 1 : x0 + kStrip;
+  l.hv = (lane == 0 && x0 > 0) || (lane == 31 && x0 + kStrip < f.w);
+  const float2* P = A.col_phasor + f.col_off;
+  l.Pa = l.va ? __ldg(P + l.xa) : make_float2(0.f, 0.f);
+  l.Pb = l.vb ? __ldg(P + l.xb) : make_float2(0.f, 0.f);
+  l.Ph = l.hv ? __ldg(P + l.hx) : make_float2(0.f, 0.f);
+  return l;
+}
+
+// ---------------------------------------------------------------------------
+// R phase: apply the pending step, recompute the IRLS weights (lagged
+// diffusivity, variational.cpp:406-433) and, with neighbours, their robust
+// weights, prior renormalisation and the pointwise 2x2 data term.
+// ---------------------------------------------------------------------------
+struct RRow {
+  float2 ca, cb, xa_, xb_, xh;
+  float ya, yb, yh;
+  float Sa, Sb;
+};
+
+__device__ __forceinline__ void r_form(const SolverArgs& A, const FieldDesc& f, const Lanes& l,
+                                       const float2* X, const float2* D, const float* S,
+                                       bool pend, float alpha, int y, RRow& r) {
+  const int64_t o = (int64_t)y * f.pitch + l.xa;
+  const float4 L = __ldg(A.line_phasor + f.line_off + y);
+  const float2 Lc = make_float2(L.x, L.y);
+  r.ca = carrier(Lc, l.Pa, L.z);
+  r.cb = carrier(Lc, l.Pb, L.z);
+  ld_pair(X + o, r.xa_, r.xb_);
+  if (pend) {
+    float2 da, db;
+    ld_pair(D + o, da, db);
+    r.xa_ = cadd(r.xa_, cscale(da, alpha));
+    r.xb_ = cadd(r.xb_, cscale(db, alpha));
+  }
+  ld_pairf(S + o, r.Sa, r.Sb);
+  r.ya = l.va ? r.Sa - re_mul(r.xa_, r.ca) : 0.f;
+  r.yb = l.vb ? r.Sb - re_mul(r.xb_, r.cb) : 0.f;
+  if (!l.va) r.xa_ = make_float2(0.f, 0.f);
+  if (!l.vb) r.xb_ = make_float2(0.f, 0.f);
+  r.xh = make_float2(0.f, 0.f);
+  r.yh = 0.f;
+  if (l.hv) {  // right halo (lane 31) -- lane 0's left halo is loaded but unused
+    const int64_t oh = (int64_t)y * f.pitch + l.hx;
+    float2 xv = __ldcg(X + oh);
+    if (pend) xv = cadd(xv, cscale(__ldcg(D + oh), alpha));
+    r.xh = xv;
+    r.yh = __ldcg(S + oh) - re_mul(xv, carrier(Lc, l.Ph, L.z));
+  }
+}
+
+__device__ void phase_reweight(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
+                               const FieldCtl& c) {
+  const Lanes l = make_lanes(A, f, u.x0, lane);
+  const int64_t base = f.px_off;
+  const float2* X = A.X[c.xsel] + base;
+  float2* Xo = A.X[c.xsel ^ 1] + base;
+  const float2* D = A.D[c.sel] + base;
+  const float* S = A.S + base;
+  float4* W = A.W + base;
+  const bool pend = c.pending != 0;
+  const float alpha = c.alpha;
+  const float eps = f.eps, epsc = f.eps_c, k = f.k_coupling;
+  const float e2 = eps * eps, ec2 = epsc * epsc;
+  RRow cur, nxt;
+  r_form(A, f, l, X, D, S, pend, alpha, u.y0, cur);
+  for (int y = u.y0; y < u.y1; ++y) {
+    const bool hn = y + 1 < f.h;
+    if (hn) r_form(A, f, l, X, D, S, pend, alpha, y + 1, nxt);
+    float y_r = __shfl_down_sync(0xffffffffu, cur.ya, 1);
+    float2 x_r = make_float2(__shfl_down_sync(0xffffffffu, cur.xa_.x, 1),
+                             __shfl_down_sync(0xffffffffu, cur.xa_.y, 1));
+    if (lane == 31) {
+      y_r = cur.yh;
+      x_r = cur.xh;
+    }
+    const float gxa = (l.xa < f.w - 1) ? cur.yb - cur.ya : 0.f;
+    const float gxb = (l.xb < f.w - 1) ? y_r - cur.yb : 0.f;
+    const float gya = hn ? nxt.ya - cur.ya : 0.f;
+    const float gyb = hn ? nxt.yb - cur.yb : 0.f;
+    const float2 dxa = (l.xa < f.w - 1) ? csub(cur.xb_, cur.xa_) : make_float2(0.f, 0.f);
+    const float2 dxb = (l.xb < f.w - 1) ? csub(x_r, cur.xb_) : make_float2(0.f, 0.f);
+    const float2 dya = hn ? csub(nxt.xa_, cur.xa_) : make_float2(0.f, 0.f);
+    const float2 dyb = hn ? csub(nxt.xb_, cur.xb_) : make_float2(0.f, 0.f);
+    const float mxa = sqrtf(cnorm(dxa)), mxb = sqrtf(cnorm(dxb));
+    const float mya = sqrtf(cnorm(dya)), myb = sqrtf(cnorm(dyb));
+    float4 wa, wb;
+    wa.x = eps / sqrtf(gxa * gxa + e2);
+    wa.y = eps / sqrtf(gya * gya + e2);
+    wa.z = epsc / sqrtf(mxa * mxa + k * gxa * gxa + ec2);
+    wa.w = epsc / sqrtf(mya * mya + k * gya * gya + ec2);
+    wb.x = eps / sqrtf(gxb * gxb + e2);
+    wb.y = eps / sqrtf(gyb * gyb + e2);
+    wb.z = epsc / sqrtf(mxb * mxb + k * gxb * gxb + ec2);
+    wb.w = epsc / sqrtf(myb * myb + k * gyb * gyb + ec2);
+    const int64_t o = (int64_t)y * f.pitch + l.xa;
+    if (f.has_nbr) {
+      // neighbour robust weights (variational.cpp:452-462), prior
+      // renormalisation (:493-516) and the pointwise data term written as
+      // M = 2 nu sum wt u u^T, b = 2 nu sum wt (S_w - S) u, u = (Re dc, -Im dc).
+      const float nu = f.nu, et2 = f.eps_t * f.eps_t;
+      float psa = 1.f, psb = 1.f;
+      float4 Ma = make_float4(0.f, 0.f, 0.f, 0.f), Mb = Ma;
+      float2 ba = make_float2(0.f, 0.f), bb = ba;
+      for (int j = 0; j < f.n_nbr; ++j) {
+        const float4* NB = A.nbr + f.nbr_off + (int64_t)j * f.plane_px;
+        const float4 na = __ldcg(NB + o);
+        const float4 nbv = __ldcg(NB + o + 1);
+        // na = (S_w - S, dc.x, dc.y, conf)
+        const float rta = na.x + (cur.xa_.x * na.y - cur.xa_.y * na.z);
+        const float rtb = nbv.x + (cur.xb_.x * nbv.y - cur.xb_.y * nbv.z);
+        const float wta = na.w * et2 / (rta * rta + et2);
+        const float wtb = nbv.w * et2 / (rtb * rtb + et2);
+        psa += nu * wta * (na.y * na.y + na.z * na.z);
+        psb += nu * wtb * (nbv.y * nbv.y + nbv.z * nbv.z);
+        const float sa = 2.f * nu * wta, sb = 2.f * nu * wtb;
+        Ma.x += sa * na.y * na.y;
+        Ma.y -= sa * na.y * na.z;
+        Ma.z += sa * na.z * na.z;
+        Mb.x += sb * nbv.y * nbv.y;
+        Mb.y -= sb * nbv.y * nbv.z;
+        Mb.z += sb * nbv.z * nbv.z;
+        ba.x += sa * na.x * na.y;
+        ba.y -= sa * na.x * na.z;
+        bb.x += sb * nbv.x * nbv.y;
+        bb.y -= sb * nbv.x * nbv.z;
+      }
+      wa.x *= psa; wa.y *= psa; wa.z *= psa; wa.w *= psa;
+      wb.x *= psb; wb.y *= psb; wb.z *= psb; wb.w *= psb;
+      if (l.va) __stcg(A.M + base + o, Ma);
+      if (l.vb) __stcg(A.M + base + o + 1, Mb);
+      st_pair(A.B + base + o, ba, bb, l.va, l.vb);
+    }
+    if (l.va) __stcg(W + o, wa);
+    if (l.vb) __stcg(W + o + 1, wb);
+    st_pair(Xo + o, cur.xa_, cur.xb_, l.va, l.vb);
+    cur = nxt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stencil phases: G (gradient at chi, with S) and I (one fused CG sweep).
+// ---------------------------------------------------------------------------
+struct SRow {
+  float2 ca, cb;
+  float2 ua, ub, uh;   // operand (chi for G, d_k for I), halo
+  float ya, yb, yh;    // S - Re[u c] (G) or -Re[u c] (I)
+  float2 gka, gkb;     // I: g_k
+  float2 doa, dob;     // I: d_{k-1} (pending chi step)
+};
+
+template <bool MODE_I>
+__device__ __forceinline__ void s_form(const SolverArgs& A, const FieldDesc& f, const Lanes& l,
+                                       const FieldCtl& c, bool first, int y, SRow& r) {
+  const int64_t base = f.px_off;
+  const int64_t o = (int64_t)y * f.pitch + l.xa;
+  const float4 L = __ldg(A.line_phasor + f.line_off + y);
+  const float2 Lc = make_float2(L.x, L.y);
+  r.ca = carrier(Lc, l.Pa, L.z);
+  r.cb = carrier(Lc, l.Pb, L.z);
+  const float2 z = make_float2(0.f, 0.f);
+  if (!MODE_I) {
+    const float2* X = A.X[c.xsel] + base;
+    float Sa, Sb;
+    ld_pair(X + o, r.ua, r.ub);
+    ld_pairf(A.S + base + o, Sa, Sb);
+    if (!l.va) r.ua = z;
+    if (!l.vb) r.ub = z;
+    r.ya = l.va ? Sa - re_mul(r.ua, r.ca) : 0.f;
+    r.yb = l.vb ? Sb - re_mul(r.ub, r.cb) : 0.f;
+    r.uh = z;
+    r.yh = 0.f;
+    if (l.hv) {
+      const int64_t oh = (int64_t)y * f.pitch + l.hx;
+      r.uh = __ldcg(X + oh);
+      r.yh = __ldcg(A.S + base + oh) - re_mul(r.uh, carrier(Lc, l.Ph, L.z));
+    }
+  } else {
+    const float2* G = A.G[c.sel] + base;
+    const float2* Q = A.Q[c.sel] + base;
+    const float2* D = A.D[c.sel] + base;
+    float2 ga, gb;
+    ld_pair(G + o, ga, gb);
+    if (first) {
+      r.gka = ga;
+      r.gkb = gb;
+      r.ua = make_float2(-ga.x, -ga.y);
+      r.ub = make_float2(-gb.x, -gb.y);
+      r.doa = z;
+      r.dob = z;
+    } else {
+      float2 qa, qb, da, db;
+      ld_pair(Q + o, qa, qb);
+      ld_pair(D + o, da, db);
+      r.gka = cadd(ga, cscale(qa, c.alpha));
+      r.gkb = cadd(gb, cscale(qb, c.alpha));
+      r.ua = cadd(make_float2(-r.gka.x, -r.gka.y), cscale(da, c.beta));
+      r.ub = cadd(make_float2(-r.gkb.x, -r.gkb.y), cscale(db, c.beta));
+      r.doa = da;
+      r.dob = db;
+    }
+    if (!l.va) { r.ua = z; r.gka = z; }
+    if (!l.vb) { r.ub = z; r.gkb = z; }
+    r.ya = -re_mul(r.ua, r.ca);
+    r.yb = -re_mul(r.ub, r.cb);
+    r.uh = z;
+    r.yh = 0.f;
+    if (l.hv) {
+      const int64_t oh = (int64_t)y * f.pitch + l.hx;
+      const float2 gh = __ldcg(G + oh);
+      float2 dh;
+      if (first) {
+        dh = make_float2(-gh.x, -gh.y);
+      } else {
+        const float2 gkh = cadd(gh, cscale(__ldcg(Q + oh), c.alpha));
+        dh = cadd(make_float2(-gkh.x, -gkh.y), cscale(__ldcg(D + oh), c.beta));
+      }
+      r.uh = dh;
+      r.yh = -re_mul(dh, carrier(Lc, l.Ph, L.z));
+    }
+  }
+}
+
+template <bool MODE_I>
+__device__ void phase_stencil(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
+                              const FieldCtl& c, bool first, double* part) {
+  const Lanes l = make_lanes(A, f, u.x0, lane);
+  const int64_t base = f.px_off;
+  const float4* W = A.W + base;
+  const float mu_h = f.mu_h, mu_v = f.mu_v;
+  const float2 z = make_float2(0.f, 0.f);
+  double pH = 0.0, pgd = 0.0, pgq = 0.0, pqq = 0.0, pgg = 0.0;
+  SRow cur, nxt;
+  float aypa = 0.f, aypb = 0.f;
+  float2 bypa = z, bypb = z;
+  s_form<MODE_I>(A, f, l, c, first, u.y0, cur);
+  if (u.y0 > 0) {
+    SRow prv;
+    s_form<MODE_I>(A, f, l, c, first, u.y0 - 1, prv);
+    const int64_t op = (int64_t)(u.y0 - 1) * f.pitch + l.xa;
+    const float4 wpa = __ldcg(W + op), wpb = __ldcg(W + op + 1);
+    aypa = wpa.y * (cur.ya - prv.ya);
+    aypb = wpb.y * (cur.yb - prv.yb);
+    bypa = cscale(csub(cur.ua, prv.ua), wpa.w);
+    bypb = cscale(csub(cur.ub, prv.ub), wpb.w);
+  }
+  for (int y = u.y0; y < u.y1; ++y) {
+    const bool hn = y + 1 < f.h;
+    if (hn) s_form<MODE_I>(A, f, l, c, first, y + 1, nxt);
+    const int64_t o = (int64_t)y * f.pitch + l.xa;
+    const float4 wa = __ldcg(W + o), wb = __ldcg(W + o + 1);
+    float4 wh = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (l.hv && lane == 0) wh = __ldcg(W + (int64_t)y * f.pitch + l.hx);
+    // horizontal neighbours
+    float y_r = __shfl_down_sync(0xffffffffu, cur.ya, 1);
+    float2 u_r = make_float2(__shfl_down_sync(0xffffffffu, cur.ua.x, 1),
+                             __shfl_down_sync(0xffffffffu, cur.ua.y, 1));
+    if (lane == 31) {
+      y_r = cur.yh;
+      u_r = cur.uh;
+    }
+    const bool ia = l.xa < f.w - 1, ib = l.xb < f.w - 1;
+    const float dxya = ia ? cur.yb - cur.ya : 0.f;
+    const float dxyb = ib ? y_r - cur.yb : 0.f;
+    const float2 dxua = ia ? csub(cur.ub, cur.ua) : z;
+    const float2 dxub = ib ? csub(u_r, cur.ub) : z;
+    const float axa = wa.x * dxya, axb = wb.x * dxyb;
+    const float2 bxa = cscale(dxua, wa.z), bxb = cscale(dxub, wb.z);
+    // left neighbour of pixel a: lane - 1's pixel b, or lane 0's halo
+    float axl = __shfl_up_sync(0xffffffffu, axb, 1);
+    float2 bxl = make_float2(__shfl_up_sync(0xffffffffu, bxb.x, 1),
+                             __shfl_up_sync(0xffffffffu, bxb.y, 1));
+    if (lane == 0) {
+      if (l.hv && l.hx < f.w - 1) {
+        axl = wh.x * (cur.ya - cur.yh);
+        bxl = cscale(csub(cur.ua, cur.uh), wh.z);
+      } else {
+        axl = 0.f;
+        bxl = z;
+      }
+    }
+    // vertical
+    const float dyya = hn ? nxt.ya - cur.ya : 0.f;
+    const float dyyb = hn ? nxt.yb - cur.yb : 0.f;
+    const float2 dyua = hn ? csub(nxt.ua, cur.ua) : z;
+    const float2 dyub = hn ? csub(nxt.ub, cur.ub) : z;
+    const float aya = wa.y * dyya, ayb = wb.y * dyyb;
+    const float2 bya = cscale(dyua, wa.w), byb = cscale(dyub, wb.w);
+    // operator: -2[(ax(x-1) - ax) + (ay(y-1) - ay)] conj(c) + 2[mu_h (..) + mu_v (..)]
+    const float ima = 2.f * ((axl - axa) + (aypa - aya));
+    const float imb = 2.f * ((axa - axb) + (aypb - ayb));
+    float2 oa = make_float2(-ima * cur.ca.x, ima * cur.ca.y);
+    float2 ob = make_float2(-imb * cur.cb.x, imb * cur.cb.y);
+    oa = cadd(oa, cscale(cadd(cscale(csub(bxl, bxa), mu_h), cscale(csub(bypa, bya), mu_v)), 2.f));
+    ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
+    if (f.has_nbr) {
+      const float4 Ma = __ldcg(A.M + base + o), Mb = __ldcg(A.M + base + o + 1);
+      // M u with u as the real 2-vector (Re, Im)
+      oa.x += Ma.x * cur.ua.x + Ma.y * cur.ua.y;
+      oa.y += Ma.y * cur.ua.x + Ma.z * cur.ua.y;
+      ob.x += Mb.x * cur.ub.x + Mb.y * cur.ub.y;
+      ob.y += Mb.y * cur.ub.x + Mb.z * cur.ub.y;
+      if (!MODE_I) {
+        float2 ba, bb;
+        ld_pair(A.B + base + o, ba, bb);
+        oa = cadd(oa, ba);
+        ob = cadd(ob, bb);
+      }
+      if (MODE_I) {
+        pH += 0.5 * (double)(Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
+                             Ma.z * cur.ua.y * cur.ua.y) * l.va;
+        pH += 0.5 * (double)(Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
+                             Mb.z * cur.ub.y * cur.ub.y) * l.vb;
+      }
+    }
+    if (!l.va) oa = z;
+    if (!l.vb) ob = z;
+    if (!MODE_I) {
+      st_pair(A.G[0] + base + o, oa, ob, l.va, l.vb);
+      pgg += (double)cnorm(oa) + (double)cnorm(ob);
+    } else {
+      if (l.va)
+        pH += (double)wa.x * dxya * dxya + (double)wa.y * dyya * dyya +
+              (double)mu_h * wa.z * cnorm(dxua) + (double)mu_v * wa.w * cnorm(dyua);
+      if (l.vb)
+        pH += (double)wb.x * dxyb * dxyb + (double)wb.y * dyyb * dyyb +
+              (double)mu_h * wb.z * cnorm(dxub) + (double)mu_v * wb.w * cnorm(dyub);
+      pgd += (double)cur.gka.x * cur.ua.x + (double)cur.gka.y * cur.ua.y +
+             (double)cur.gkb.x * cur.ub.x + (double)cur.gkb.y * cur.ub.y;
+      pgq += (double)cur.gka.x * oa.x + (double)cur.gka.y * oa.y + (double)cur.gkb.x * ob.x +
+             (double)cur.gkb.y * ob.y;
+      pqq += (double)cnorm(oa) + (double)cnorm(ob);
+      pgg += (double)cnorm(cur.gka) + (double)cnorm(cur.gkb);
+      const int s2 = c.sel ^ 1;
+      st_pair(A.G[s2] + base + o, cur.gka, cur.gkb, l.va, l.vb);
+      st_pair(A.D[s2] + base + o, cur.ua, cur.ub, l.va, l.vb);
+      st_pair(A.Q[s2] + base + o, oa, ob, l.va, l.vb);
+      if (!first) {
+        float2* X = A.X[c.xsel] + base;
+        float2 xa, xb;
+        ld_pair(X + o, xa, xb);
+        xa = cadd(xa, cscale(cur.doa, c.alpha));
+        xb = cadd(xb, cscale(cur.dob, c.alpha));
+        st_pair(X + o, xa, xb, l.va, l.vb);
+      }
+    }
+    aypa = aya;
+    aypb = ayb;
+    bypa = bya;
+    bypb = byb;
+    cur = nxt;
+  }
+  part[0] = MODE_I ? pH : pgg;
+  part[1] = pgd;
+  part[2] = pgq;
+  part[3] = pqq;
+  part[4] = pgg;
+}
+
+// F phase: apply the pending step, output-fidelity luma Y = S - Re[chi c]
+// (variational.cpp:552-555, sequence.cpp:1102-1114); final chi -> X[0].
+__device__ void phase_final(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
+                            const FieldCtl& c) {
+  const Lanes l = make_lanes(A, f, u.x0, lane);
+  const int64_t base = f.px_off;
+  const float2* X = A.X[c.xsel] + base;
+  const float2* D = A.D[c.sel] + base;
+  float2* Xo = A.X[0] + base;
+  for (int y = u.y0; y < u.y1; ++y) {
+    const int64_t o = (int64_t)y * f.pitch + l.xa;
+    const float4 L = __ldg(A.line_phasor + f.line_off + y);
+    const float2 Lc = make_float2(L.x, L.y);
+    float2 xa, xb;
+    ld_pair(X + o, xa, xb);
+    if (c.pending) {
+      float2 da, db;
+      ld_pair(D + o, da, db);
+      xa = cadd(xa, cscale(da, c.alpha));
+      xb = cadd(xb, cscale(db, c.alpha));
+    }
+    float Sa, Sb;
+    ld_pairf(A.S + base + o, Sa, Sb);
+    const float ya = Sa - re_mul(xa, carrier(Lc, l.Pa, L.z));
+    const float yb = Sb - re_mul(xb, carrier(Lc, l.Pb, L.z));
+    st_pair(Xo + o, xa, xb, l.va, l.vb);
+    if (l.va && l.vb) {
+      __stcg(reinterpret_cast<float2*>(A.Y + base + o), make_float2(ya, yb));
+    } else if (l.va) {
+      __stcg(A.Y + base + o, ya);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Field-level completion: fixed-order reduction of the unit partials and the
+// CG scalar logic (variational.cpp:519-549).
+// ---------------------------------------------------------------------------
+__device__ void complete_phase(const SolverArgs& A, const FieldDesc& f, int fi, int kind, int k,
+                               int p, int lane) {
+  FieldCtl* c = A.ctl + fi;
+  double s[kNPart];
+#pragma unroll
+  for (int i = 0; i < kNPart; ++i) s[i] = 0.0;
+  if (kind == kPhaseG || kind == kPhaseI) {
+    for (int uu = f.unit_begin + lane; uu < f.unit_begin + f.unit_count; uu += 32) {
+#pragma unroll
+      for (int i = 0; i < kNPart; ++i) s[i] += __ldcg(A.partials + (int64_t)uu * kNPart + i);
+    }
+#pragma unroll
+    for (int i = 0; i < kNPart; ++i) s[i] = warp_allsum(s[i]);
+  }
+  int publish = p;
+  if (lane == 0) {
+    const int B = 2 + f.n_inner;
+    if (kind == kPhaseR) {
+      c->pending = 0;
+      c->xsel ^= 1;
+    } else if (kind == kPhaseG) {
+      c->gg0 = s[0];
+      c->gg = s[0];
+      c->pending = 0;
+      c->sel = 0;
+    } else if (kind == kPhaseI) {
+      const double H = s[0], gd = s[1], gq = s[2], qq = s[3], ggk = s[4];
+      c->sel ^= 1;
+      c->gg = ggk;
+      const int o = p / B;
+      const int last_i = o * B + 1 + f.n_inner;
+      if (H <= 1e-12) {
+        c->pending = 0;
+        publish = last_i;
+      } else {
+        const float alpha = (float)(-0.5 * gd / H);
+        const double gn = ggk + 2.0 * (double)alpha * gq + (double)alpha * (double)alpha * qq;
+        c->alpha = alpha;
+        c->beta = (float)(gn / fmax(ggk, 1e-30));
+        c->gg_next = gn;
+        c->pending = 1;
+        c->cg_iters += 1;
+        const double tol = (double)f.cg_tol;
+        if (gn < tol * tol * c->gg0 || gn < 1e-10 * (double)f.h * (double)f.w) publish = last_i;
+      }
+    } else {
+      c->pending = 0;
+    }
+    (void)k;
+    __threadfence();
+    st_release(A.done_phase + fi, publish);
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kSolverThreads, 3) k_solver(SolverArgs A) {
+  const int lane = threadIdx.x & 31;
+  const long long total = (long long)A.n_units * A.n_phases;
+  for (;;) {
+    long long item = 0;
+    if (lane == 0) item = (long long)atomicAdd(A.queue, 1ULL);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= total) break;
+    const int p = (int)(item / A.n_units);
+    const int ui = (int)(item % A.n_units);
+    const Unit u = A.units[ui];
+    const FieldDesc f = A.fields[u.field];
+    if (p >= f.n_phases) continue;
+    int ok = 1, dp = 0;
+    if (lane == 0) {
+      ok = wait_at_least(A.done_phase + u.field, p - 1);
+      dp = ld_acquire(A.done_phase + u.field);
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    dp = __shfl_sync(0xffffffffu, dp, 0);
+    if (!ok) {
+      if (lane == 0) atomicOr(A.err, 1);
+      break;
+    }
+    if (dp >= p) continue;  // phase skipped by an early CG exit
+    __syncwarp();
+    FieldCtl c;
+    {
+      const FieldCtl* vc = A.ctl + u.field;
+      c.alpha = __ldcg(&vc->alpha);
+      c.beta = __ldcg(&vc->beta);
+      c.pending = __ldcg(&vc->pending);
+      c.sel = __ldcg(&vc->sel);
+      c.xsel = __ldcg(&vc->xsel);
+    }
+    const int B = 2 + f.n_inner;
+    int kind, k = 0;
+    if (p == f.n_outer * B) {
+      kind = kPhaseF;
+    } else {
+      const int r = p % B;
+      kind = r == 0 ? kPhaseR : (r == 1 ? kPhaseG : kPhaseI);
+      k = r - 2;
+    }
+    double part[kNPart] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (kind == kPhaseR) {
+      phase_reweight(A, f, u, lane, c);
+    } else if (kind == kPhaseG) {
+      phase_stencil<false>(A, f, u, lane, c, false, part);
+    } else if (kind == kPhaseI) {
+      phase_stencil<true>(A, f, u, lane, c, k == 0, part);
+    } else {
+      phase_final(A, f, u, lane, c);
+    }
+    if (kind == kPhaseG || kind == kPhaseI) {
+#pragma unroll
+      for (int i = 0; i < kNPart; ++i) {
+        const double v = warp_sum(part[i]);
+        if (lane == 0) __stcg(A.partials + (int64_t)ui * kNPart + i, v);
+      }
+    }
+    __threadfence();
+    int last = 0;
+    if (lane == 0) last = atomicAdd(A.arrive + u.field, 1) == f.unit_count - 1;
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+      if (lane == 0) A.arrive[u.field] = 0;
+      __threadfence();
+      complete_phase(A, f, u.field, kind, k, p, lane);
+    }
+  }
+}
+
+int solver_max_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solver, kSolverThreads, 0);
+  return n;
+}
+
+cudaError_t launch_solver(const SolverArgs& args, int grid, cudaStream_t st) {
+  SolverArgs a = args;
+  void* params[] = {&a};
+  return cudaLaunchCooperativeKernel((const void*)k_solver, dim3(grid), dim3(kSolverThreads),
+                                     params, 0, st);
+}
+
+}  // namespace hvdg

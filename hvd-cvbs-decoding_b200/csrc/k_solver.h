@@ -1,0 +1,42 @@
+// k_solver.h -- launcher of the persistent IRLS + CG kernel (k_solver.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hvdg_internal.h"
+
+namespace hvdg {
+
+constexpr int kSolverThreads = 256;
+enum PhaseKind { kPhaseR = 0, kPhaseG = 1, kPhaseI = 2, kPhaseF = 3 };
+
+struct SolverArgs {
+  const FieldDesc* fields;
+  FieldCtl* ctl;
+  const Unit* units;
+  int n_units;                  // units per phase (all fields)
+  int n_phases;                 // max phases over fields
+  unsigned long long* queue;    // work counter (zeroed before launch)
+  int* done_phase;              // per field, -1 before launch
+  int* arrive;                  // per field, 0 before launch
+  double* partials;             // per unit x 5
+  int* err;                     // set on a bounded-wait timeout
+  const float* S;
+  float2* X[2];                 // chi (double-buffered; final chi in X[0])
+  float2* G[2];
+  float2* D[2];
+  float2* Q[2];
+  float4* W;                    // (wx, wy, wcx, wcy)
+  float* Y;                     // output-fidelity luma
+  float4* M;                    // neighbour 2x2 data term (m11, m12, m22, -)
+  float2* B;                    // neighbour constant term
+  const float4* nbr;            // neighbour planes (S_w - S, Re dc, Im dc, conf)
+  const float4* line_phasor;
+  const float2* col_phasor;
+};
+
+int solver_max_blocks_per_sm();
+cudaError_t launch_solver(const SolverArgs& args, int grid, cudaStream_t st);
+
+}  // namespace hvdg

@@ -1,0 +1,234 @@
+"""Python mirror of the engine interface, over the C ABI (include/hvdg.h).
+
+Names and argument meanings follow hvd-core: decode_field_window ~
+PrepareFieldObs + DecodeFieldWindow (sequence.h:60-101), burst_lockin ~
+BurstLockinPhase[Pal] (lockin.h:31-59), holographic_init ~ HolographicInit,
+variational_refine ~ VariationalRefine, estimate_motion ~ EstimateMotion,
+decode_frame_sequence_window ~ hvd::DecodeFrameSequenceWindow. Errors are
+raised as HvdgError carrying the C status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _cabi
+from ._cabi import Config, Diag, FieldIn, FieldOut, Geometry
+
+
+class HvdgError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"{_cabi.STATUS_NAMES.get(status, status)}: {msg}")
+
+
+@dataclass
+class Field:
+    """One composite field in (FieldInput + parity + per-field budget)."""
+    samples: np.ndarray             # (field_height, field_width) uint16 / int16 / float32 IRE
+    geometry: Geometry
+    parity: int = 0
+    blanking_level: float = 16384.0
+    white_level: float = 51200.0
+    irls_outer: int = 0             # <= 0: config value
+    cg_iterations: int = -1         # < 0: config value
+
+
+@dataclass
+class Decoded:
+    luma: np.ndarray                # (active_lines, active_width) float32
+    chroma: np.ndarray              # (active_lines, active_width) complex64, chi = V - iU
+    theta: np.ndarray | None = None
+    vswitch: np.ndarray | None = None
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a)
+
+
+_SAMPLE_TYPES = {np.dtype(np.uint16): _cabi.SAMPLES_U16, np.dtype(np.int16): _cabi.SAMPLES_S16,
+                 np.dtype(np.float32): _cabi.SAMPLES_F32_IRE}
+
+
+class Context:
+    """hvdg_ctx: one per thread (same contract as one HvdEngine per thread)."""
+
+    def __init__(self, device: int = 0, lib_path=None):
+        self.lib = _cabi.load_library(lib_path)
+        h = C.c_void_p()
+        st = self.lib.hvdg_create(int(device), C.byref(h))
+        if st != _cabi.OK:
+            raise HvdgError(st, "hvdg_create")
+        self._h = h
+        self.last_diag = Diag()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.hvdg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != _cabi.OK:
+            err = self.lib.hvdg_last_error(self._h)
+            raise HvdgError(st, f"{what}: {err.decode() if err else ''}")
+
+    def set_batching(self, batched: bool):
+        self._check(self.lib.hvdg_set_batching(self._h, int(bool(batched))), "set_batching")
+
+    def set_tuning(self, band_rows: int = 0, ctas_per_sm: int = 0):
+        self._check(self.lib.hvdg_set_tuning(self._h, int(band_rows), int(ctas_per_sm)), "set_tuning")
+
+    # ---- engine level ----------------------------------------------------
+    def _build_fields(self, fields):
+        n = len(fields)
+        arr = (FieldIn * max(n, 1))()
+        keep = []
+        for i, f in enumerate(fields):
+            s = np.ascontiguousarray(f.samples)
+            st = _SAMPLE_TYPES.get(s.dtype)
+            if st is None:
+                s = np.ascontiguousarray(s, dtype=np.float32)
+                st = _cabi.SAMPLES_F32_IRE
+            g = f.geometry
+            if s.shape != (g.field_height, g.field_width):
+                raise ValueError(f"field {i}: samples {s.shape} != geometry "
+                                 f"({g.field_height}, {g.field_width})")
+            keep.append(s)
+            arr[i].samples = s.ctypes.data
+            arr[i].sample_type = st
+            arr[i].parity = int(f.parity)
+            arr[i].blanking_level = float(f.blanking_level)
+            arr[i].white_level = float(f.white_level)
+            arr[i].geometry = C.pointer(g)
+            arr[i].irls_outer = int(f.irls_outer)
+            arr[i].cg_iterations = int(f.cg_iterations)
+            keep.append(arr[i].geometry)
+        return arr, keep
+
+    def _alloc_out(self, fields, want_theta: bool):
+        outs, res = (FieldOut * max(len(fields), 1))(), []
+        for i, f in enumerate(fields):
+            g = f.geometry
+            d = Decoded(np.zeros((g.active_lines, g.active_width), np.float32),
+                        np.zeros((g.active_lines, g.active_width), np.complex64))
+            outs[i].luma = d.luma.ctypes.data
+            outs[i].chroma = d.chroma.ctypes.data
+            if want_theta:
+                d.theta = np.zeros(g.field_height, np.float32)
+                d.vswitch = np.zeros(g.field_height, np.int8)
+                outs[i].theta = d.theta.ctypes.data
+                outs[i].vswitch = d.vswitch.ctypes.data
+            res.append(d)
+        return outs, res
+
+    def decode_fields(self, fields, cfg: Config, want_theta: bool = False) -> list[Decoded]:
+        """Independent 2-D fields (mixed geometry / budget) in one batch."""
+        arr, keep = self._build_fields(fields)
+        outs, res = self._alloc_out(fields, want_theta)
+        self.last_diag = Diag()
+        st = self.lib.hvdg_decode_fields(self._h, arr, len(fields), C.byref(cfg), outs,
+                                         C.byref(self.last_diag))
+        self._check(st, "hvdg_decode_fields")
+        del keep
+        return res
+
+    def decode_field_window(self, fields, cfg: Config, want_theta: bool = False) -> list[Decoded]:
+        """PrepareFieldObs x n + DecodeFieldWindow (one geometry per window)."""
+        arr, keep = self._build_fields(fields)
+        outs, res = self._alloc_out(fields, want_theta)
+        self.last_diag = Diag()
+        st = self.lib.hvdg_decode_field_window(self._h, arr, len(fields), C.byref(cfg), outs,
+                                               C.byref(self.last_diag))
+        self._check(st, "hvdg_decode_field_window")
+        del keep
+        return res
+
+    def decode_fields_device(self, fields_in, outs, n, cfg: Config) -> Diag:
+        """Device-resident variant: `fields_in` / `outs` are prepared FieldIn /
+        FieldOut arrays holding DEVICE pointers (e.g. torch tensor data_ptr)."""
+        d = Diag()
+        st = self.lib.hvdg_decode_fields_device(self._h, fields_in, int(n), C.byref(cfg), outs,
+                                                C.byref(d))
+        self._check(st, "hvdg_decode_fields_device")
+        return d
+
+    # ---- kernel level --------------------------------------------------------
+    def burst_lockin(self, field_ire: np.ndarray, g: Geometry):
+        f = np.ascontiguousarray(field_ire, dtype=np.float32)
+        th = np.zeros(g.field_height, np.float32)
+        sw = np.zeros(g.field_height, np.int8)
+        self._check(self.lib.hvdg_burst_lockin(self._h, f.ctypes.data, C.byref(g), th.ctypes.data,
+                                               sw.ctypes.data), "hvdg_burst_lockin")
+        return th, sw
+
+    def burst_amplitude(self, field_ire: np.ndarray, g: Geometry) -> float:
+        f = np.ascontiguousarray(field_ire, dtype=np.float32)
+        v = C.c_float()
+        self._check(self.lib.hvdg_burst_amplitude(self._h, f.ctypes.data, C.byref(g), C.byref(v)),
+                    "hvdg_burst_amplitude")
+        return float(v.value)
+
+    def holographic_init(self, s, theta_active, vswitch_active, g: Geometry, cfg: Config):
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        th = np.ascontiguousarray(theta_active, dtype=np.float32)
+        sw = np.ascontiguousarray(vswitch_active, dtype=np.int8)
+        y0 = np.zeros_like(s)
+        chi0 = np.zeros(s.shape, np.complex64)
+        self._check(self.lib.hvdg_holographic_init(self._h, s.ctypes.data, th.ctypes.data,
+                                                   sw.ctypes.data, C.byref(g), C.byref(cfg),
+                                                   y0.ctypes.data, chi0.ctypes.data),
+                    "hvdg_holographic_init")
+        return y0, chi0
+
+    def variational_refine(self, s, theta_active, vswitch_active, chi0, g: Geometry, cfg: Config):
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        th = np.ascontiguousarray(theta_active, dtype=np.float32)
+        sw = np.ascontiguousarray(vswitch_active, dtype=np.int8)
+        x0 = np.ascontiguousarray(chi0, dtype=np.complex64)
+        y = np.zeros_like(s)
+        chi = np.zeros(s.shape, np.complex64)
+        self._check(self.lib.hvdg_variational_refine(self._h, s.ctypes.data, th.ctypes.data,
+                                                     sw.ctypes.data, x0.ctypes.data, C.byref(g),
+                                                     C.byref(cfg), y.ctypes.data, chi.ctypes.data),
+                    "hvdg_variational_refine")
+        return y, chi
+
+    def estimate_motion(self, y_ref, y_cur, tile: int = 32, search: int = 16, me_mode: int = 0):
+        a = np.ascontiguousarray(y_ref, dtype=np.float32)
+        b = np.ascontiguousarray(y_cur, dtype=np.float32)
+        h, w = a.shape
+        th, tw = -(-h // tile), -(-w // tile)
+        dy = np.zeros((th, tw), np.float32)
+        dx = np.zeros_like(dy)
+        cf = np.zeros_like(dy)
+        self._check(self.lib.hvdg_estimate_motion(self._h, a.ctypes.data, b.ctypes.data, h, w,
+                                                  tile, search, me_mode, dy.ctypes.data,
+                                                  dx.ctypes.data, cf.ctypes.data),
+                    "hvdg_estimate_motion")
+        return dy, dx, cf
+
+
+def default_config(**kw) -> Config:
+    return _cabi.config_copy(_cabi.default_config(), **kw)
+
+
+def default_geometry(standard: int) -> Geometry:
+    return _cabi.default_geometry(standard)

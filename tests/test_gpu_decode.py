@@ -1,0 +1,51 @@
+"""GPU parity of the 2-D field decode (lock-in -> init -> IRLS + CG) against
+the FP64 oracle (oracle/hvd_oracle.py) and, where built, the compiled
+reference engine. Tolerances: PSNR against ground truth within 0.05 dB of
+the oracle's; max |dY|, |dC| small in IRE."""
+import numpy as np
+import pytest
+
+from hvdg import _cabi, api, synth
+from oracle import hvd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def psnr(a, b, peak=100.0):
+    d = np.asarray(a) - np.asarray(b)
+    return 10 * np.log10(peak ** 2 / np.mean(np.abs(d.astype(np.complex128)) ** 2))
+
+
+def _cfg(**kw):
+    base = dict(irls_outer=5, cg_iterations=150, fast=0, cg_tol=1e-6, temporal_strength=-1.0)
+    base.update(kw)
+    return api.default_config(**base)
+
+
+@pytest.mark.parametrize("std", [_cabi.STD_NTSC, _cabi.STD_PAL])
+def test_decode_field_matches_oracle(ctx, std):
+    g = _cabi.default_geometry(std)
+    f = synth.make_field(11 + std, std, noise_sigma=0.5)
+    cfg = _cfg()
+    out = ctx.decode_fields([api.Field(f.samples, g, parity=0)], cfg, want_theta=True)[0]
+    ire = synth.to_ire(f.samples)
+    (yo, chio, obs), = O.decode_fields_2d([ire], [0], g, cfg)
+    # lock-in phases (FP64 on both sides)
+    dth = np.abs(np.angle(np.exp(1j * (out.theta.astype(np.float64) - obs.theta))))
+    assert dth.max() < 1e-4
+    if std == _cabi.STD_PAL:
+        assert (out.vswitch == obs.vswitch).all()
+    dY = np.abs(out.luma - yo).max()
+    dC = np.abs(out.chroma - chio).max()
+    p_gpu = psnr(out.luma, f.y_true)
+    p_orc = psnr(yo, f.y_true)
+    pc_gpu = psnr(out.chroma, f.chi_true)
+    pc_orc = psnr(chio, f.chi_true)
+    print(f"std={std} maxdY={dY:.4g} maxdC={dC:.4g} PSNR Y gpu={p_gpu:.3f} oracle={p_orc:.3f} "
+          f"C gpu={pc_gpu:.3f} oracle={pc_orc:.3f} vs-oracle={psnr(out.luma, yo):.1f} dB")
+    assert abs(p_gpu - p_orc) < 0.05
+    assert abs(pc_gpu - pc_orc) < 0.05
+    assert dY < 0.05 and dC < 0.05
+    # lossless split: Y + Re[chi c] == S
+    s = obs.s
+    assert np.abs(out.luma + np.real(out.chroma * obs.carrier) - s).max() < 2e-3
