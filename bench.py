@@ -1,0 +1,356 @@
+"""Benchmark: batched 2-D field decode on B200 (fields/s).
+
+Workload (one step): 64 composite fields in one batch -- 40 NTSC 910x263
+and 24 PAL 1135x313 uint16 fields in seeded random order, per-field noise
+sigma ~ U[0.2, 2] IRE, per-field IRLS outer count ~ U{4..12} with 50 CG
+iterations per outer, fixed iteration counts (cg_tol 1e-6, fast off),
+temporal terms off. Synthetic data (hvdg.synth), seeded per rank.
+
+  value     : fields/s with the inputs already resident in HBM
+              (hvdg_decode_fields_device), device time from CUDA events on
+              the library's stream, L2 flushed between steps.
+  e2e       : the same through the host-buffer C ABI (hvdg_decode_fields),
+              pinned uint16 inputs in, float Y/chi out, copies included,
+              wall clock of the synchronous call.
+  plain     : the one-field-per-launch path (hvdg_set_batching(ctx, 0)).
+  roofline  : the IRLS+CG solver kernel, algorithmic bytes (92 B per active
+              px per CG iteration + 80 B per active px per IRLS outer) over
+              its event-timed duration, against the measured HBM copy peak.
+  cpu_baseline : the reference engine (oracle/_ref, compiled from the
+              reference sources) on a bounded sample of the same workload on
+              the host cores.
+
+--impl reference times the reference engine alone (rank 0), same metric.
+Multi-GPU (torchrun): each rank decodes its own 64-field batch (fields are
+independent; no collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "hvd-cvbs-decoding_b200"))
+sys.path.insert(0, str(REPO))
+
+METRIC = "fields/s on 1 B200, batched FP32 vs plain per-field GPU, at <=0.05 dB PSNR delta"
+N_NTSC, N_PAL = 40, 24
+ALG_BYTES_ITER = 92.0    # per active px per CG iteration
+ALG_BYTES_OUTER = 80.0   # per active px per IRLS outer
+
+
+def workload(seed: int):
+    from hvdg import synth
+    return synth.mixed_batch(seed, N_NTSC, N_PAL)
+
+
+def solver_config():
+    from hvdg import api
+    return api.default_config(fast=0, cg_tol=1e-6, temporal_strength=-1.0)
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM traffic of the solver on this workload, from the
+    committed ncu summary (profiles/solver_traffic.json), or None."""
+    p = REPO / "profiles" / "solver_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"hvdg_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(fields, threads: int) -> float:
+    """Decode `fields` with the reference engine (OpenMP across fields, as
+    parallel_across_fields does); returns seconds."""
+    from hvdg import _cabi, synth
+    from oracle import ref
+    ref.set_threads(threads)
+    base = _cabi.config_copy(solver_config())
+    geoms = [_cabi.default_geometry(f.standard) for f in fields]
+    cfgs = [_cabi.config_copy(base, irls_outer=f.irls_outer, cg_iterations=f.cg_iterations)
+            for f in fields]
+    ires = [synth.to_ire(f.samples) for f in fields]
+    t = time.perf_counter()
+    ref.decode_fields(ires, [f.parity for f in fields], geoms, cfgs, across_fields=True)
+    return time.perf_counter() - t
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    fields = workload(1000)
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference engine library oracle/_ref/libhvdref.so was not built"}))
+        return 0
+    sample = fields[:max(8, min(threads, len(fields)))]
+    for _ in range(args.warmup):
+        run_reference(sample[:max(2, threads // 4)], threads)
+    times = [run_reference(sample, threads) for _ in range(args.steps)]
+    total = float(sum(times))
+    v = len(sample) * args.steps / total
+    desc = (f"{len(sample)} of the 64 workload fields per step "
+            f"({sum(f.standard == 0 for f in sample)} NTSC, {sum(f.standard == 1 for f in sample)} PAL), "
+            f"OpenMP across fields, {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "fields/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded hvdg.synth mixed NTSC/PAL batch)",
+        "config": {"workload": "mixed-64: 40 NTSC 910x263 + 24 PAL 1135x313 uint16, irls U{4..12} x 50 CG",
+                   "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "fields/s", "cores": threads, "kind": "reference",
+                         "sample": desc},
+        "e2e": {"value": v, "unit": "fields/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+
+    from hvdg import _cabi, api
+    cfg = solver_config()
+    fields = workload(1000 + rank)
+    ctx = api.Context(local)
+
+    # ---- device-resident inputs / outputs ----
+    n = len(fields)
+    geoms = [_cabi.default_geometry(f.standard) for f in fields]
+    d_in = [torch.from_numpy(f.samples.view(np.int16)).cuda() for f in fields]
+    d_y = [torch.empty((g.active_lines, g.active_width), dtype=torch.float32, device="cuda")
+           for g in geoms]
+    d_c = [torch.empty((g.active_lines, g.active_width, 2), dtype=torch.float32, device="cuda")
+           for g in geoms]
+    fin = (_cabi.FieldIn * n)()
+    fout = (_cabi.FieldOut * n)()
+    for i, f in enumerate(fields):
+        fin[i].samples = d_in[i].data_ptr()
+        fin[i].sample_type = _cabi.SAMPLES_U16
+        fin[i].parity = f.parity
+        fin[i].blanking_level = 16384.0
+        fin[i].white_level = 51200.0
+        fin[i].geometry = C.pointer(geoms[i])
+        fin[i].irls_outer = f.irls_outer
+        fin[i].cg_iterations = f.cg_iterations
+        fout[i].luma = d_y[i].data_ptr()
+        fout[i].chroma = d_c[i].data_ptr()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        ctx.decode_fields_device(fin, fout, n, cfg)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ms_total = ms_solver = 0.0
+    pix_iters = pix_outers = 0
+    launches = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        d = ctx.decode_fields_device(fin, fout, n, cfg)
+        ms_total += d.ms_total
+        ms_solver += d.ms_solver
+        pix_iters += d.solver_pixel_iters
+        pix_outers += d.solver_pixel_outers
+        launches += d.kernel_launches
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    if dist is not None:
+        t = torch.tensor([ms_total, ms_solver], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total, ms_solver = float(t[0]), float(t[1])
+        dist.barrier()
+
+    # ---- e2e through the host-buffer API (pinned in/out) ----
+    pin_in = []
+    for f in fields:
+        t = torch.empty(f.samples.shape, dtype=torch.int16, pin_memory=True)
+        t.numpy()[...] = f.samples.view(np.int16)
+        pin_in.append(t)
+    host_fields = [api.Field(pin_in[i].numpy().view(np.uint16), geoms[i], parity=f.parity,
+                             irls_outer=f.irls_outer, cg_iterations=f.cg_iterations)
+                   for i, f in enumerate(fields)]
+    ctx.decode_fields(host_fields, cfg)  # warm
+    e2e_t = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = ctx.decode_fields(host_fields, cfg)
+        e2e_t += time.perf_counter() - t
+    h2d = sum(f.samples.nbytes for f in fields)
+    d2h = sum(o.luma.nbytes + o.chroma.nbytes for o in out)
+    if dist is not None:
+        tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt[0])
+
+    # ---- plain one-field-per-launch path ----
+    plain = None
+    if not args.no_plain:
+        ctx.set_batching(False)
+        ctx.decode_fields_device(fin, fout, n, cfg)
+        pt = 0.0
+        psteps = max(1, min(args.steps, 2))
+        for _ in range(psteps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            pt += ctx.decode_fields_device(fin, fout, n, cfg).ms_total
+        ctx.set_batching(True)
+        if dist is not None:
+            tt = torch.tensor([pt], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            pt = float(tt[0])
+        plain = {"value": n * psteps * world / (pt / 1000.0), "unit": "fields/s",
+                 "ms_per_step": pt / psteps}
+
+    value = n * args.steps * world / (ms_total / 1000.0)
+    peak, peak_kind = measured_peaks()
+    alg_bytes_per_launch = (ALG_BYTES_ITER * pix_iters + ALG_BYTES_OUTER * pix_outers) / args.steps
+    solver_s = ms_solver / 1000.0 / args.steps
+    achieved = alg_bytes_per_launch / solver_s / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": profile_traffic(), "peak_kind": peak_kind,
+            "kernel": "k_solver (persistent IRLS + CG)",
+            "alg_bytes_per_launch": alg_bytes_per_launch, "ms_per_launch": 1000 * solver_s}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "fields/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded hvdg.synth mixed NTSC/PAL batch)",
+        "config": {"workload": "mixed-64: 40 NTSC 910x263 + 24 PAL 1135x313 uint16, irls U{4..12} x 50 CG",
+                   "solver": "FP32 planes, FP64 reductions, fixed iterations (cg_tol 1e-6, fast off)",
+                   "l2": "flushed between steps (256 MiB write, outside the timed events)",
+                   "parallelism": f"fields sharded per rank x{world}, no data-path collective"},
+        "e2e": {"value": n * args.steps * world / e2e_t, "unit": "fields/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "clocks": clocks,
+        "plain": plain,
+        "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            threads = os.cpu_count() or 1
+            sample = fields[:max(8, min(threads, n))]
+            run_reference(sample[:2], threads)
+            ts = run_reference(sample, threads)
+            line["cpu_baseline"] = {
+                "value": len(sample) / ts, "unit": "fields/s", "cores": threads, "kind": "reference",
+                "sample": f"{len(sample)} of the 64 workload fields, reference engine "
+                          f"(oracle/_ref) OpenMP across fields"}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
