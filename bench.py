@@ -47,9 +47,24 @@ ALG_BYTES_ITER = 92.0    # per active px per CG iteration
 ALG_BYTES_OUTER = 80.0   # per active px per IRLS outer
 
 
-def workload(seed: int):
+WORKLOADS = {
+    # name: (n_ntsc, n_pal, irls range, CG per outer)
+    "mixed64": (N_NTSC, N_PAL, (4, 12), 50),
+    # profiling case: same kernels, working set (~260 MB) above L2, short solve
+    "small16": (16, 0, (2, 2), 10),
+}
+
+
+WORKLOAD_DESC = {
+    "mixed64": "mixed-64: 40 NTSC 910x263 + 24 PAL 1135x313 uint16, irls U{4..12} x 50 CG",
+    "small16": "small-16 (profiling): 16 NTSC 910x263 uint16, irls 2 x 10 CG",
+}
+
+
+def workload(seed: int, name: str = "mixed64"):
     from hvdg import synth
-    return synth.mixed_batch(seed, N_NTSC, N_PAL)
+    nn, npal, outer, cg = WORKLOADS[name]
+    return synth.mixed_batch(seed, nn, npal, outer_range=outer, cg_per_outer=cg)
 
 
 def solver_config():
@@ -148,7 +163,7 @@ def reference_arm(args, rank, world):
         return 0
     from oracle import ref
     threads = os.cpu_count() or 1
-    fields = workload(1000)
+    fields = workload(1000, args.workload)
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference engine library oracle/_ref/libhvdref.so was not built"}))
@@ -167,8 +182,7 @@ def reference_arm(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded hvdg.synth mixed NTSC/PAL batch)",
-        "config": {"workload": "mixed-64: 40 NTSC 910x263 + 24 PAL 1135x313 uint16, irls U{4..12} x 50 CG",
-                   "sample": desc},
+        "config": {"workload": WORKLOAD_DESC[args.workload], "sample": desc},
         "cpu_baseline": {"value": v, "unit": "fields/s", "cores": threads, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": v, "unit": "fields/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -185,6 +199,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -205,7 +220,7 @@ def main():
 
     from hvdg import _cabi, api
     cfg = solver_config()
-    fields = workload(1000 + rank)
+    fields = workload(1000 + rank, args.workload)
     ctx = api.Context(local)
 
     # ---- device-resident inputs / outputs ----
@@ -321,7 +336,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded hvdg.synth mixed NTSC/PAL batch)",
-        "config": {"workload": "mixed-64: 40 NTSC 910x263 + 24 PAL 1135x313 uint16, irls U{4..12} x 50 CG",
+        "config": {"workload": WORKLOAD_DESC[args.workload],
                    "solver": "FP32 planes, FP64 reductions, fixed iterations (cg_tol 1e-6, fast off)",
                    "l2": "flushed between steps (256 MiB write, outside the timed events)",
                    "parallelism": f"fields sharded per rank x{world}, no data-path collective"},

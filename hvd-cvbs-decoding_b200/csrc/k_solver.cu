@@ -40,6 +40,7 @@
 namespace hvdg {
 
 constexpr int kNPart = 5;
+constexpr int kNS = 4;  // ring slots per warp (I phase)
 
 __device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
   const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
@@ -432,6 +433,264 @@ __device__ void phase_stencil(const SolverArgs& A, const FieldDesc& f, const Uni
   part[4] = pgg;
 }
 
+// ---------------------------------------------------------------------------
+// I phase with TMA-staged rows. Each warp owns a ring of kNS row slots in
+// shared memory; lane 0 fills them with 1-D bulk copies (cp.async.bulk,
+// mbarrier-tracked) of the g / q / d row segments (strip + 2-pixel halo
+// each side), the chi row segment and the weight row segment (strip + left
+// halo), so up to kNS - 1 rows are in flight per warp without holding
+// registers. Rows of one unit: [max(y0 - 1, 0), min(y1, h - 1)].
+// ---------------------------------------------------------------------------
+constexpr int kSlotG = (kStrip + 4) * 8;        // 544 B: columns x0-2 .. x0+65
+constexpr int kSlotX = kStrip * 8;              // 512 B: columns x0 .. x0+63
+constexpr int kSlotW = (kStrip + 1) * 16;       // 1040 B: columns x0-1 .. x0+63
+constexpr int kOffQ = kSlotG, kOffD = 2 * kSlotG, kOffX = 3 * kSlotG, kOffW = 3 * kSlotG + kSlotX;
+constexpr int kSlotBytes = kOffW + kSlotW;      // 3184 B
+constexpr int kWarpRingBytes = kNS * kSlotBytes + kNS * 8;
+
+struct Ring {
+  char* slots;
+  uint64_t* bar;
+  uint32_t bits;  // per-slot phase parity
+};
+
+__device__ __forceinline__ void ring_issue(Ring& r, int slot, const SolverArgs& A,
+                                           const FieldDesc& f, const FieldCtl& c, int x0, int y,
+                                           bool first, bool need_x) {
+  char* dst = r.slots + slot * kSlotBytes;
+  uint64_t* bar = r.bar + slot;
+  const int64_t row = f.px_off + (int64_t)y * f.pitch;
+  const int gs = max(x0 - 2, 0), ge = min(x0 + kStrip + 2, f.pitch);
+  const uint32_t gb = (uint32_t)(ge - gs) * 8u;
+  const int goff = (gs - (x0 - 2)) * 8;
+  const int ws = max(x0 - 1, 0), we = min(x0 + kStrip, f.pitch);
+  const uint32_t wb = (uint32_t)(we - ws) * 16u;
+  const int woff = (ws - (x0 - 1)) * 16;
+  const bool qd = !first;
+  const bool xx = need_x && !first;
+  const uint32_t total = gb + wb + (qd ? 2 * gb : 0u) + (xx ? (uint32_t)kSlotX : 0u);
+  mbar_expect_tx(bar, total);
+  bulk_g2s(dst + goff, A.G[c.sel] + row + gs, gb, bar);
+  if (qd) {
+    bulk_g2s(dst + kOffQ + goff, A.Q[c.sel] + row + gs, gb, bar);
+    bulk_g2s(dst + kOffD + goff, A.D[c.sel] + row + gs, gb, bar);
+  }
+  if (xx) bulk_g2s(dst + kOffX, A.X[c.xsel] + row + x0, kSlotX, bar);
+  bulk_g2s(dst + kOffW + woff, A.W + row + ws, wb, bar);
+}
+
+__device__ __forceinline__ bool ring_wait(Ring& r, int slot) {
+  const bool ok = mbar_wait(r.bar + slot, (r.bits >> slot) & 1u);
+  r.bits ^= 1u << slot;
+  return ok;
+}
+
+// Form g_k, d_k, dY for one row from a ring slot (I phase).
+__device__ __forceinline__ void ring_form(const char* slot, const SolverArgs& A,
+                                          const FieldDesc& f, const Lanes& l, const FieldCtl& c,
+                                          bool first, int lane, int y, SRow& r) {
+  const float4 L = __ldg(A.line_phasor + f.line_off + y);
+  const float2 Lc = make_float2(L.x, L.y);
+  r.ca = carrier(Lc, l.Pa, L.z);
+  r.cb = carrier(Lc, l.Pb, L.z);
+  const float2 z = make_float2(0.f, 0.f);
+  const float4 g4 = *reinterpret_cast<const float4*>(slot + 16 + 16 * lane);
+  const float2 ga = make_float2(g4.x, g4.y), gb = make_float2(g4.z, g4.w);
+  if (first) {
+    r.gka = ga;
+    r.gkb = gb;
+    r.ua = make_float2(-ga.x, -ga.y);
+    r.ub = make_float2(-gb.x, -gb.y);
+    r.doa = z;
+    r.dob = z;
+  } else {
+    const float4 q4 = *reinterpret_cast<const float4*>(slot + kOffQ + 16 + 16 * lane);
+    const float4 d4 = *reinterpret_cast<const float4*>(slot + kOffD + 16 + 16 * lane);
+    r.gka = cadd(ga, cscale(make_float2(q4.x, q4.y), c.alpha));
+    r.gkb = cadd(gb, cscale(make_float2(q4.z, q4.w), c.alpha));
+    r.doa = make_float2(d4.x, d4.y);
+    r.dob = make_float2(d4.z, d4.w);
+    r.ua = cadd(make_float2(-r.gka.x, -r.gka.y), cscale(r.doa, c.beta));
+    r.ub = cadd(make_float2(-r.gkb.x, -r.gkb.y), cscale(r.dob, c.beta));
+  }
+  if (!l.va) { r.ua = z; r.gka = z; }
+  if (!l.vb) { r.ub = z; r.gkb = z; }
+  r.ya = -re_mul(r.ua, r.ca);
+  r.yb = -re_mul(r.ub, r.cb);
+  r.uh = z;
+  r.yh = 0.f;
+  if (l.hv) {
+    const int hl = lane == 0 ? 1 : kStrip + 2;  // local column of x0-1 / x0+64
+    const float2 gh = *reinterpret_cast<const float2*>(slot + 8 * hl);
+    float2 dh;
+    if (first) {
+      dh = make_float2(-gh.x, -gh.y);
+    } else {
+      const float2 qh = *reinterpret_cast<const float2*>(slot + kOffQ + 8 * hl);
+      const float2 dd = *reinterpret_cast<const float2*>(slot + kOffD + 8 * hl);
+      const float2 gkh = cadd(gh, cscale(qh, c.alpha));
+      dh = cadd(make_float2(-gkh.x, -gkh.y), cscale(dd, c.beta));
+    }
+    r.uh = dh;
+    r.yh = -re_mul(dh, carrier(Lc, l.Ph, L.z));
+  }
+}
+
+__device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
+                           const FieldCtl& c, bool first, Ring& ring, double* part) {
+  const Lanes l = make_lanes(A, f, u.x0, lane);
+  const int64_t base = f.px_off;
+  const float mu_h = f.mu_h, mu_v = f.mu_v;
+  const float2 z = make_float2(0.f, 0.f);
+  const int ybeg = max(u.y0 - 1, 0), yend = min(u.y1, f.h - 1);
+  const int nrows = yend - ybeg + 1;
+  double pH = 0.0, pgd = 0.0, pgq = 0.0, pqq = 0.0, pgg = 0.0;
+  bool ok = true;
+  __syncwarp();
+  if (lane == 0) {
+    fence_proxy_async_global();
+    fence_proxy_async_smem();
+    for (int i = 0; i < min(kNS, nrows); ++i) {
+      const int y = ybeg + i;
+      ring_issue(ring, i % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
+    }
+  }
+  auto slot_ptr = [&](int i) { return ring.slots + (i % kNS) * kSlotBytes; };
+  auto issue_after = [&](int i_free) {
+    __syncwarp();
+    const int inext = i_free + kNS;
+    if (lane == 0 && inext < nrows) {
+      fence_proxy_async_smem();
+      const int y = ybeg + inext;
+      ring_issue(ring, inext % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
+    }
+  };
+  SRow cur, nxt;
+  float aypa = 0.f, aypb = 0.f;
+  float2 bypa = z, bypb = z;
+  int icur = 0;
+  if (u.y0 > 0) {
+    SRow prv;
+    ok &= ring_wait(ring, 0);
+    ring_form(slot_ptr(0), A, f, l, c, first, lane, u.y0 - 1, prv);
+    ok &= ring_wait(ring, 1 % kNS);
+    ring_form(slot_ptr(1), A, f, l, c, first, lane, u.y0, cur);
+    const char* w0 = slot_ptr(0) + kOffW;
+    const float4 wpa = *reinterpret_cast<const float4*>(w0 + 16 * (1 + 2 * lane));
+    const float4 wpb = *reinterpret_cast<const float4*>(w0 + 16 * (2 + 2 * lane));
+    aypa = wpa.y * (cur.ya - prv.ya);
+    aypb = wpb.y * (cur.yb - prv.yb);
+    bypa = cscale(csub(cur.ua, prv.ua), wpa.w);
+    bypb = cscale(csub(cur.ub, prv.ub), wpb.w);
+    issue_after(0);
+    icur = 1;
+  } else {
+    ok &= ring_wait(ring, 0);
+    ring_form(slot_ptr(0), A, f, l, c, first, lane, u.y0, cur);
+  }
+  const int s2 = c.sel ^ 1;
+  for (int y = u.y0; y < u.y1; ++y) {
+    const bool hn = y + 1 < f.h;
+    if (hn) {
+      ok &= ring_wait(ring, (icur + 1) % kNS);
+      ring_form(slot_ptr(icur + 1), A, f, l, c, first, lane, y + 1, nxt);
+    }
+    const char* sl = slot_ptr(icur);
+    const float4 wa = *reinterpret_cast<const float4*>(sl + kOffW + 16 * (1 + 2 * lane));
+    const float4 wb = *reinterpret_cast<const float4*>(sl + kOffW + 16 * (2 + 2 * lane));
+    float4 wh = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (l.hv && lane == 0) wh = *reinterpret_cast<const float4*>(sl + kOffW);
+    float y_r = __shfl_down_sync(0xffffffffu, cur.ya, 1);
+    float2 u_r = make_float2(__shfl_down_sync(0xffffffffu, cur.ua.x, 1),
+                             __shfl_down_sync(0xffffffffu, cur.ua.y, 1));
+    if (lane == 31) {
+      y_r = cur.yh;
+      u_r = cur.uh;
+    }
+    const bool ia = l.xa < f.w - 1, ib = l.xb < f.w - 1;
+    const float dxya = ia ? cur.yb - cur.ya : 0.f;
+    const float dxyb = ib ? y_r - cur.yb : 0.f;
+    const float2 dxua = ia ? csub(cur.ub, cur.ua) : z;
+    const float2 dxub = ib ? csub(u_r, cur.ub) : z;
+    const float axa = wa.x * dxya, axb = wb.x * dxyb;
+    const float2 bxa = cscale(dxua, wa.z), bxb = cscale(dxub, wb.z);
+    float axl = __shfl_up_sync(0xffffffffu, axb, 1);
+    float2 bxl = make_float2(__shfl_up_sync(0xffffffffu, bxb.x, 1),
+                             __shfl_up_sync(0xffffffffu, bxb.y, 1));
+    if (lane == 0) {
+      if (l.hv && l.hx < f.w - 1) {
+        axl = wh.x * (cur.ya - cur.yh);
+        bxl = cscale(csub(cur.ua, cur.uh), wh.z);
+      } else {
+        axl = 0.f;
+        bxl = z;
+      }
+    }
+    const float dyya = hn ? nxt.ya - cur.ya : 0.f;
+    const float dyyb = hn ? nxt.yb - cur.yb : 0.f;
+    const float2 dyua = hn ? csub(nxt.ua, cur.ua) : z;
+    const float2 dyub = hn ? csub(nxt.ub, cur.ub) : z;
+    const float aya = wa.y * dyya, ayb = wb.y * dyyb;
+    const float2 bya = cscale(dyua, wa.w), byb = cscale(dyub, wb.w);
+    const float ima = 2.f * ((axl - axa) + (aypa - aya));
+    const float imb = 2.f * ((axa - axb) + (aypb - ayb));
+    float2 oa = make_float2(-ima * cur.ca.x, ima * cur.ca.y);
+    float2 ob = make_float2(-imb * cur.cb.x, imb * cur.cb.y);
+    oa = cadd(oa, cscale(cadd(cscale(csub(bxl, bxa), mu_h), cscale(csub(bypa, bya), mu_v)), 2.f));
+    ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
+    const int64_t o = (int64_t)y * f.pitch + l.xa;
+    if (f.has_nbr) {
+      const float4 Ma = __ldcg(A.M + base + o), Mb = __ldcg(A.M + base + o + 1);
+      oa.x += Ma.x * cur.ua.x + Ma.y * cur.ua.y;
+      oa.y += Ma.y * cur.ua.x + Ma.z * cur.ua.y;
+      ob.x += Mb.x * cur.ub.x + Mb.y * cur.ub.y;
+      ob.y += Mb.y * cur.ub.x + Mb.z * cur.ub.y;
+      if (l.va)
+        pH += 0.5 * (double)(Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
+                             Ma.z * cur.ua.y * cur.ua.y);
+      if (l.vb)
+        pH += 0.5 * (double)(Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
+                             Mb.z * cur.ub.y * cur.ub.y);
+    }
+    if (!l.va) oa = z;
+    if (!l.vb) ob = z;
+    if (l.va)
+      pH += (double)wa.x * dxya * dxya + (double)wa.y * dyya * dyya +
+            (double)mu_h * wa.z * cnorm(dxua) + (double)mu_v * wa.w * cnorm(dyua);
+    if (l.vb)
+      pH += (double)wb.x * dxyb * dxyb + (double)wb.y * dyyb * dyyb +
+            (double)mu_h * wb.z * cnorm(dxub) + (double)mu_v * wb.w * cnorm(dyub);
+    pgd += (double)cur.gka.x * cur.ua.x + (double)cur.gka.y * cur.ua.y +
+           (double)cur.gkb.x * cur.ub.x + (double)cur.gkb.y * cur.ub.y;
+    pgq += (double)cur.gka.x * oa.x + (double)cur.gka.y * oa.y + (double)cur.gkb.x * ob.x +
+           (double)cur.gkb.y * ob.y;
+    pqq += (double)cnorm(oa) + (double)cnorm(ob);
+    pgg += (double)cnorm(cur.gka) + (double)cnorm(cur.gkb);
+    st_pair(A.G[s2] + base + o, cur.gka, cur.gkb, l.va, l.vb);
+    st_pair(A.D[s2] + base + o, cur.ua, cur.ub, l.va, l.vb);
+    st_pair(A.Q[s2] + base + o, oa, ob, l.va, l.vb);
+    if (!first) {
+      const float4 x4 = *reinterpret_cast<const float4*>(sl + kOffX + 16 * lane);
+      const float2 xa = cadd(make_float2(x4.x, x4.y), cscale(cur.doa, c.alpha));
+      const float2 xb = cadd(make_float2(x4.z, x4.w), cscale(cur.dob, c.alpha));
+      st_pair(A.X[c.xsel] + base + o, xa, xb, l.va, l.vb);
+    }
+    issue_after(icur);
+    aypa = aya;
+    aypb = ayb;
+    bypa = bya;
+    bypb = byb;
+    cur = nxt;
+    icur += 1;
+  }
+  part[0] = pH;
+  part[1] = pgd;
+  part[2] = pgq;
+  part[3] = pqq;
+  part[4] = pgg;
+  return ok;
+}
+
 // F phase: apply the pending step, output-fidelity luma Y = S - Re[chi c]
 // (variational.cpp:552-555, sequence.cpp:1102-1114); final chi -> X[0].
 __device__ void phase_final(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
@@ -525,8 +784,22 @@ __device__ void complete_phase(const SolverArgs& A, const FieldDesc& f, int fi, 
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kSolverThreads, 3) k_solver(SolverArgs A) {
+__global__ void __launch_bounds__(kSolverThreads, 2) k_solver(SolverArgs A) {
   const int lane = threadIdx.x & 31;
+  extern __shared__ __align__(16) char solver_smem[];
+  Ring ring;
+  {
+    char* wbase = solver_smem + (threadIdx.x >> 5) * kWarpRingBytes;
+    ring.slots = wbase;
+    ring.bar = reinterpret_cast<uint64_t*>(wbase + kNS * kSlotBytes);
+    ring.bits = 0;
+    if (lane == 0) {
+      for (int i = 0; i < kNS; ++i) mbar_init(ring.bar + i, 1);
+      fence_mbar_init();
+      fence_proxy_async_smem();
+    }
+    __syncwarp();
+  }
   const long long total = (long long)A.n_units * A.n_phases;
   for (;;) {
     long long item = 0;
@@ -575,7 +848,10 @@ __global__ void __launch_bounds__(kSolverThreads, 3) k_solver(SolverArgs A) {
     } else if (kind == kPhaseG) {
       phase_stencil<false>(A, f, u, lane, c, false, part);
     } else if (kind == kPhaseI) {
-      phase_stencil<true>(A, f, u, lane, c, k == 0, part);
+      if (!phase_iter(A, f, u, lane, c, k == 0, ring, part)) {
+        if (lane == 0) atomicOr(A.err, 2);
+        break;
+      }
     } else {
       phase_final(A, f, u, lane, c);
     }
@@ -598,17 +874,29 @@ __global__ void __launch_bounds__(kSolverThreads, 3) k_solver(SolverArgs A) {
   }
 }
 
+constexpr int kSolverSmem = (kSolverThreads / 32) * kWarpRingBytes;
+
+static void configure_solver() {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolverSmem);
+    done = true;
+  }
+}
+
 int solver_max_blocks_per_sm() {
+  configure_solver();
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solver, kSolverThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solver, kSolverThreads, kSolverSmem);
   return n;
 }
 
 cudaError_t launch_solver(const SolverArgs& args, int grid, cudaStream_t st) {
+  configure_solver();
   SolverArgs a = args;
   void* params[] = {&a};
   return cudaLaunchCooperativeKernel((const void*)k_solver, dim3(grid), dim3(kSolverThreads),
-                                     params, 0, st);
+                                     params, kSolverSmem, st);
 }
 
 }  // namespace hvdg
