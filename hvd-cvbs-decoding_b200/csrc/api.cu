@@ -209,6 +209,21 @@ struct hvdg_ctx {
 
 namespace hvdg {
 
+// Init tables of one geometry (the same tables run_batch uploads), for
+// translation units that launch the init kernels on their own memory.
+void init_tables_for(const hvdg_geometry& g, std::vector<float2>* khat_row_col,
+                     std::vector<float2>* col_phasor, std::vector<float2>* tw_row,
+                     std::vector<float2>* tw_col, int* hp, int* pad) {
+  const GeomTables t = make_geom_tables(g);
+  khat_row_col->assign(t.khat_row.begin(), t.khat_row.end());
+  khat_row_col->insert(khat_row_col->end(), t.khat_col.begin(), t.khat_col.end());
+  *col_phasor = t.col_phasor;
+  *tw_row = twiddles(kRowFft);
+  *tw_col = twiddles(kColFft);
+  *hp = t.hp;
+  *pad = t.pad;
+}
+
 hvdg_status cuda_fail(hvdg_ctx* ctx, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return HVDG_OK;
   char buf[256];

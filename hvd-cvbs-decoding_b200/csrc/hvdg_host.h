@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <vector>
 
 #include "hvdg.h"
 
@@ -26,6 +27,12 @@ struct PinnedArena {
   hvdg_status reserve(size_t bytes);
   ~PinnedArena();
 };
+
+// Host-side init tables of one geometry (kernel spectra, column phasors,
+// FFT twiddles), as uploaded by the batched pipeline.
+void init_tables_for(const hvdg_geometry& g, std::vector<float2>* khat_row_col,
+                     std::vector<float2>* col_phasor, std::vector<float2>* tw_row,
+                     std::vector<float2>* tw_col, int* hp, int* pad);
 
 // Records a CUDA failure in the context and maps it to a status.
 hvdg_status cuda_fail(hvdg_ctx* ctx, cudaError_t e, const char* what);
