@@ -210,7 +210,7 @@ def make_field(seed: int, standard: int = _cabi.STD_NTSC, noise_sigma: float = 0
     # active picture
     ire[fal:lal, a0:a1] = luma + np.real(chi * car[fal:lal, a0:a1])
     # sync pulse (4.7 us)
-    sync_len = int(round(4.7e-6 * fs))
+    sync_len = min(int(round(4.7e-6 * fs)), max(0, g.colour_burst_start - 8))
     ire[:, :sync_len] = -40.0
     # burst: 9 (NTSC) / 10 (PAL) cycles centred on the burst window
     b0, b1 = g.colour_burst_start, g.colour_burst_end

@@ -1,0 +1,277 @@
+"""Pins of the FP64 oracle (oracle/hvd_oracle.py), CPU only:
+
+1. the reference's own analytic tests, restated (file:line of each);
+2. the golden fixtures in tests/golden/ -- outputs of the reference engine
+   itself, compiled from its own sources and run on seeded inputs
+   (tests/golden/make_golden.py);
+3. the algebra the device kernels rely on (cyclic-convolution form of the
+   FFT crop, the single-reduction CG recurrence), checked in FP64.
+"""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from hvdg import _cabi
+from oracle import hvd_oracle as O
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def wrap(a):
+    return np.arctan2(np.sin(a), np.cos(a))
+
+
+def geom_from(arr, sr):
+    g = _cabi.Geometry()
+    (g.field_width, g.field_height, g.active_video_start, g.active_video_end,
+     g.colour_burst_start, g.colour_burst_end, g.first_active_field_line,
+     g.last_active_field_line, g.standard) = [int(v) for v in arr]
+    g.sample_rate = float(sr)
+    return g
+
+
+def cfg_from(arr):
+    c = _cabi.default_config()
+    c.irls_outer, c.cg_iterations, c.fast = int(arr[0]), int(arr[1]), int(arr[2])
+    c.cg_tol, c.temporal_strength, c.chroma_aniso, c.lambda_c = map(float, arr[3:7])
+    return c
+
+
+# ---------------------------------------------------------------------------
+# 1. restated reference tests
+# ---------------------------------------------------------------------------
+
+def test_lockin_ntsc_recovers_phase_and_amplitude():
+    """lockin_test.cpp:28-67: a -A sin(phi) burst on 30 lines of 200 samples,
+    theta recovered to 0.05 rad, amplitude 20 +/- 1, TridiagSmooth's low-lambda
+    limit returns the data."""
+    g = _cabi.geometry_copy(_cabi.default_geometry(_cabi.STD_NTSC), field_width=200,
+                            colour_burst_start=20, colour_burst_end=60)
+    h = 30
+    field = np.zeros((h, 200))
+    ys = np.arange(h)
+    tt = 0.3 + math.pi * ys + 0.05 * np.sin(0.2 * ys)
+    x = np.arange(20, 60)
+    field[:, 20:60] = -20.0 * np.sin(tt[:, None] + 0.5 * math.pi * x[None, :])
+    th = O.burst_lockin_phase(field, g)
+    assert np.abs(wrap(th[2:h - 2] - tt[2:h - 2])).max() < 0.05
+    assert abs(O.burst_amplitude_ire(field, g) - 20.0) < 1.0
+    xs = O.tridiag_smooth([1, 2, 3, 4], [1, 1, 1, 1], 1e-6)
+    assert np.allclose(xs, [1, 2, 3, 4], atol=1e-3)
+
+
+def _pal_field(g, theta, sw, Y, U, V, burst):
+    """pal_lockin_test.cpp:44-62."""
+    h = len(theta)
+    x = np.arange(g.field_width)
+    phi = theta[:, None] + 0.5 * math.pi * x[None, :]
+    s = np.where(np.asarray(sw) > 0, 1.0, -1.0)[:, None]
+    bs = burst / math.sqrt(2.0)
+    f = np.zeros((h, g.field_width))
+    bm = (x >= g.colour_burst_start) & (x < g.colour_burst_end)
+    am = (x >= g.active_video_start) & (x < g.active_video_end)
+    f[:, bm] = (-bs * np.sin(phi) + s * bs * np.cos(phi))[:, bm]
+    f[:, am] = (Y + U * np.sin(phi) + s * V * np.cos(phi))[:, am]
+    return f
+
+
+def test_lockin_pal_joint_phase_and_parity():
+    """pal_lockin_test.cpp:75-155: exact parity, 0.03 rad clean, 0.08 rad with
+    8 bursts destroyed; effective-carrier identity < 1e-3; line advance
+    2 pi * 0.7516."""
+    g = _cabi.geometry_copy(_cabi.default_geometry(_cabi.STD_PAL), field_width=300,
+                            colour_burst_start=20, colour_burst_end=60, active_video_start=80,
+                            active_video_end=280, first_active_field_line=0,
+                            last_active_field_line=0, field_height=40)
+    h = 40
+    ys = np.arange(h)
+    adv = 2 * math.pi * 0.7516
+    tt = 0.4 + adv * ys + 0.05 * np.sin(0.15 * ys)
+    sw = np.where(ys % 2 == 0, 1, -1)
+    field = _pal_field(g, tt, sw, 50.0, -12.0, 20.0, 21.43)
+    th, vs = O.burst_lockin_phase_pal(field, g)
+    assert (vs == sw).all()
+    assert np.abs(wrap(th - tt)).max() < 0.03
+    dmg = field.copy()
+    dmg[12:20, 20:60] = 0.0
+    th2, vs2 = O.burst_lockin_phase_pal(dmg, g)
+    assert (vs2 == sw).all()
+    assert np.abs(wrap(th2 - tt)).max() < 0.08
+    c = O.make_carrier(tt, sw, g)
+    chi = 20.0 - 1j * (-12.0)
+    recon = 50.0 + np.real(chi * c)
+    assert np.abs(recon - field[:, 80:280]).max() < 1e-3
+    cyc = 4433618.75 / 15625.0
+    assert abs(O.line_advance(g) - 2 * math.pi * (cyc - math.floor(cyc))) < 1e-5
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 8), (8, 1), (17, 23), (64, 48)])
+def test_gradient_adjoints(shape):
+    """gradients_test.cpp:40-67: <Da, b> == <a, D^T b> for Dx, Dy (real and
+    complex planes)."""
+    rng = np.random.default_rng(3)
+    a = rng.uniform(-1, 1, shape)
+    b = rng.uniform(-1, 1, shape)
+    assert abs(np.sum(O.Dx(a) * b) - np.sum(a * O.DxT(b))) < 1e-12
+    assert abs(np.sum(O.Dy(a) * b) - np.sum(a * O.DyT(b))) < 1e-12
+    ac = a + 1j * rng.uniform(-1, 1, shape)
+    bc = b + 1j * rng.uniform(-1, 1, shape)
+    assert abs(np.vdot(O.Dx(ac), bc) - np.vdot(ac, O.DxT(bc))) < 1e-12
+
+
+def test_box_blur_equals_naive_convolution():
+    """motion_v2_test.cpp: BoxBlur == zero-padded 'same' convolution with a
+    constant 1/(2r+1) kernel per axis."""
+    rng = np.random.default_rng(5)
+    a = rng.normal(size=(23, 31))
+    for r in (1, 2, 3, 8):
+        k = np.ones(2 * r + 1) / (2 * r + 1)
+        rows = np.array([np.convolve(a[:, x], k, mode="same") for x in range(a.shape[1])]).T
+        naive = np.array([np.convolve(rows[y], k, mode="same") for y in range(a.shape[0])])
+        assert np.abs(O.box_blur_same(a, r) - naive).max() < 1e-12
+
+
+def test_motion_recovers_shift():
+    """motion_test.cpp:78-127 (own texture): a (3, -2) shift of a textured
+    128 x 128 plane is recovered within 0.6 px on confident interior tiles,
+    and unconfident tiles are flagged."""
+    rng = np.random.default_rng(11)
+    h = w = 128
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    blocks = rng.uniform(-15, 15, size=(h // 4, w // 4))
+    tex = (40 * np.sin(yy * 0.31) * np.cos(xx * 0.27) + 15 * np.sin(xx * 0.23 + yy * 0.17)
+           + blocks[(yy // 4).astype(int), (xx // 4).astype(int)])
+    cur = tex[np.clip(np.arange(h) - 3, 0, h - 1)][:, np.clip(np.arange(w) + 2, 0, w - 1)]
+    dy, dx, cf = O.estimate_motion(tex, cur, 32, 8)
+    inner = (slice(1, -1), slice(1, -1))
+    conf = cf[inner] > 0.15
+    assert conf.sum() >= 1
+    assert np.abs(dy[inner][conf] - 3).max() <= 0.6
+    assert np.abs(dx[inner][conf] + 2).max() <= 0.6
+
+
+def test_lossless_identity():
+    """lossless_identity_test.cpp:40-101: init and refine keep
+    |S - Y - Re[chi c]| < 1e-3."""
+    d = np.load(GOLD / "field_ntsc_small.npz")
+    g = geom_from(d["geometry"], d["sample_rate"])
+    cfg = cfg_from(d["cfg"])
+    s, c = d["s"].astype(np.float64), d["carrier"].astype(np.complex128)
+    y0, chi0 = O.holographic_init(s, c, g)
+    assert np.abs(s - y0 - np.real(chi0 * c)).max() < 1e-3
+    y, chi = O.variational_refine(s, c, chi0, cfg)
+    assert np.abs(s - y - np.real(chi * c)).max() < 1e-3
+
+
+# ---------------------------------------------------------------------------
+# 2. golden fixtures (the reference engine's own outputs)
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("tag", ["ntsc", "pal"])
+def test_oracle_matches_reference_golden(tag):
+    d = np.load(GOLD / f"field_{tag}_small.npz")
+    g = geom_from(d["geometry"], d["sample_rate"])
+    cfg = cfg_from(d["cfg"])
+    ire = ((d["samples"].astype(np.float32) - np.float32(16384.0)) /
+           np.float32((51200.0 - 16384.0) / 100.0)).astype(np.float64)
+    if O.uses_vswitch(g):
+        th, vs = O.burst_lockin_phase_pal(ire, g)
+        assert (vs == d["vswitch"]).all()
+    else:
+        th = O.burst_lockin_phase(ire, g)
+    assert np.abs(wrap(th - d["theta"])).max() < 2e-3
+    assert abs(O.burst_amplitude_ire(ire, g) - float(d["amplitude"])) < 1e-3
+    # init / refine from the reference's own prepared field
+    s, c = d["s"].astype(np.float64), d["carrier"].astype(np.complex128)
+    y0, chi0 = O.holographic_init(s, c, g)
+    assert np.abs(chi0 - d["chi0"]).max() < 5e-3
+    assert np.abs(y0 - d["y0"]).max() < 5e-3
+    y, chi = O.variational_refine(s, c, d["chi0"].astype(np.complex128), cfg,
+                                  is_pal=O.uses_vswitch(g))
+    assert np.abs(chi - d["chi_refine"]).max() < 5e-3
+    assert np.abs(y - d["y_refine"]).max() < 5e-3
+    # whole 2-D field decode from the raw samples
+    (yd, chid, _), = O.decode_fields_2d([ire], [0], g, cfg)
+    assert np.abs(yd - d["y_decode"]).max() < 2e-2
+    assert np.abs(chid - d["chi_decode"]).max() < 2e-2
+
+
+def test_oracle_motion_matches_reference_golden():
+    d = np.load(GOLD / "motion_small.npz")
+    dy, dx, cf = O.estimate_motion(d["y_ref"], d["y_cur"], int(d["tile"]), int(d["search"]))
+    # same integer vectors and sub-pel fits (FP64 vs the reference's FP32)
+    assert np.abs(dy - d["dy"]).max() < 1e-4 and np.abs(dx - d["dx"]).max() < 1e-4
+    assert np.abs(cf - d["conf"]).max() < 1e-4
+
+
+# ---------------------------------------------------------------------------
+# 3. algebra behind the device kernels
+# ---------------------------------------------------------------------------
+
+def _khat(k, n, M, scale=1.0):
+    kt = np.zeros(M, np.complex128)
+    for j in range(-(n - 1), n):
+        kt[j % M] = k[j % n]
+    return np.fft.fft(kt) * scale / M
+
+
+def test_init_cyclic_convolution_equals_fft_crop():
+    """k_init_rows / k_init_cols: IDFT(gy gx DFT(x)) on the padded field equals
+    a row cyclic convolution (length 2048) followed by a column one (length
+    1024) with the kernels' spectra."""
+    d = np.load(GOLD / "field_pal_small.npz")
+    g = geom_from(d["geometry"], d["sample_rate"])
+    s, c = d["s"].astype(np.float64), d["carrier"].astype(np.complex128)
+    h, w = s.shape
+    pad = min(16, h - 1)
+    hp = h + 2 * pad
+    X = (s * np.conj(c))[O.mirror_row(np.arange(hp) - pad, h)]
+    for (mhz, cph) in O.INIT_VARIANTS:
+        gy, gx = O.gaussian_lpf(hp, w, g, mhz, cph, h)
+        want = np.fft.ifft2(np.fft.fft2(X) * gy[:, None] * gx[None, :])
+        xp = np.zeros((hp, 2048), complex)
+        xp[:, :w] = X
+        R = np.fft.ifft(np.fft.fft(xp, axis=1) * _khat(np.fft.ifft(gx), w, 2048)[None, :],
+                        axis=1)[:, :w] * 2048
+        cp = np.zeros((1024, w), complex)
+        cp[:hp] = R
+        got = np.fft.ifft(np.fft.fft(cp, axis=0) * _khat(np.fft.ifft(gy), hp, 1024)[:, None],
+                          axis=0)[:hp] * 1024
+        assert np.abs(got - want).max() < 1e-10
+
+
+def test_single_reduction_cg_recurrence():
+    """k_solver: with q = g(d) - g(0), g(chi + a d) = g(chi) + a q and
+    curv(d) = <d, q> / 2, so ||g + a q||^2 = gg + 2 a <g,q> + a^2 <q,q>
+    reproduces the reference's recomputed residual norm."""
+    d = np.load(GOLD / "field_ntsc_small.npz")
+    cfg = cfg_from(d["cfg"])
+    s, c = d["s"].astype(np.float64), d["carrier"].astype(np.complex128)
+    chi = d["chi0"].astype(np.complex128)
+    _, _, W = O.variational_refine(s, c, chi, _cabi.config_copy(cfg, irls_outer=1, cg_iterations=1),
+                                   return_weights=True)
+    mu_h = cfg.lambda_c * O.resolve_chroma_aniso(chi, cfg, False)
+    mu_v = cfg.lambda_c
+
+    def grad(ch, ss):
+        yc = ss - np.real(ch * c)
+        img = 2 * (O.DxT(W["wx"] * O.Dx(yc)) + O.DyT(W["wy"] * O.Dy(yc)))
+        return -img * np.conj(c) + 2 * (mu_h * O.DxT(W["wcx"] * O.Dx(ch)) +
+                                        mu_v * O.DyT(W["wcy"] * O.Dy(ch)))
+    rng = np.random.default_rng(1)
+    dd = rng.normal(size=s.shape) + 1j * rng.normal(size=s.shape)
+    g0 = grad(chi, s)
+    q = grad(dd, np.zeros_like(s))
+    a = 0.37
+    g1 = grad(chi + a * dd, s)
+    assert np.abs(g1 - (g0 + a * q)).max() < 1e-9
+    dy = -np.real(dd * c)
+    curv = (np.sum(W["wx"] * O.Dx(dy) ** 2) + np.sum(W["wy"] * O.Dy(dy) ** 2) +
+            mu_h * np.sum(W["wcx"] * np.abs(O.Dx(dd)) ** 2) +
+            mu_v * np.sum(W["wcy"] * np.abs(O.Dy(dd)) ** 2))
+    assert abs(curv - 0.5 * np.real(np.vdot(dd, q))) < 1e-8 * abs(curv)
+    gg = np.vdot(g0, g0).real
+    pred = gg + 2 * a * np.real(np.vdot(g0, q)) + a * a * np.vdot(q, q).real
+    assert abs(pred - np.vdot(g1, g1).real) < 1e-9 * gg
