@@ -22,6 +22,7 @@
 #include "hvdg_internal.h"
 #include "hvdg_host.h"
 #include "k_init.h"
+#include "k_motion.h"
 #include "k_prep.h"
 #include "k_solver.h"
 
@@ -1100,8 +1101,87 @@ hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref, const float*
   if (!ctx || !y_ref || !y_cur || !dy || !dx || !confidence || h < 1 || w < 1 || tile < 1 ||
       search < 0 || me_mode < 0 || me_mode > 1)
     return HVDG_ERR_BAD_ARGUMENT;
-  ctx->last_error = "motion estimation is not available in this build";
-  return HVDG_ERR_UNSUPPORTED;
+  if (me_mode == 1) {
+    ctx->last_error = "integer-SAD motion mode is not available in this build";
+    return HVDG_ERR_UNSUPPORTED;
+  }
+  if (4 * tile > 4096 || search > 64) return HVDG_ERR_UNSUPPORTED;
+  cudaSetDevice(ctx->device);
+  const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
+  const int dpitch = pitch / 4;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const int ct = std::max(4, tile / 4);
+  const int cth = (h / 4 + ct - 1) / ct, ctw = (w / 4 + ct - 1) / ct;
+  const size_t plane = (size_t)h * pitch;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes, 256);
+    return r;
+  };
+  const size_t o_f = take(sizeof(hvdg::MeField) * 2);
+  const size_t o_p = take(sizeof(hvdg::MePair));
+  const size_t o_l = take(sizeof(float) * 2 * plane);
+  const size_t o_t = take(sizeof(float) * 2 * plane);
+  const size_t o_b = take(sizeof(float) * 2 * plane);
+  const size_t o_d = take(sizeof(float) * 2 * (size_t)(h / 4 + 1) * dpitch);
+  const size_t nct = (size_t)std::max(1, cth * ctw), nt = (size_t)th * tw;
+  const size_t o_cdy = take(sizeof(float) * nct), o_cdx = take(sizeof(float) * nct);
+  size_t ot[8];
+  for (int i = 0; i < 8; ++i) ot[i] = take(sizeof(float) * nt);
+  hvdg_status st = ctx->arena.reserve(o);
+  if (st != HVDG_OK) return st;
+  char* base = static_cast<char*>(ctx->arena.base);
+  hvdg::MeField mf[2];
+  for (int i = 0; i < 2; ++i) {
+    mf[i].h = h;
+    mf[i].w = w;
+    mf[i].pitch = pitch;
+    mf[i].dpitch = dpitch;
+    mf[i].y_off = mf[i].t_off = mf[i].b_off = (int64_t)i * plane;
+    mf[i].d_off = (int64_t)i * (h / 4 + 1) * dpitch;
+  }
+  hvdg::MePair pr{0, 1};
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(base + o_f, mf, sizeof(mf), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_p, &pr, sizeof(pr), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(base + o_l, sizeof(float) * pitch, y_ref, sizeof(float) * w,
+                          sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(base + o_l + sizeof(float) * plane, sizeof(float) * pitch, y_cur,
+                          sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D motion inputs");
+  hvdg::MeArgs a;
+  a.tile = tile;
+  a.search = search;
+  a.coarse_off = (int)nct;
+  a.tiles_off = (int)nt;
+  hvdg::MeBuffers mb;
+  mb.luma = reinterpret_cast<const float*>(base + o_l);
+  mb.tmp = reinterpret_cast<float*>(base + o_t);
+  mb.blur = reinterpret_cast<float*>(base + o_b);
+  mb.dec = reinterpret_cast<float*>(base + o_d);
+  mb.cdy = reinterpret_cast<float*>(base + o_cdy);
+  mb.cdx = reinterpret_cast<float*>(base + o_cdx);
+  mb.mdy = reinterpret_cast<float*>(base + ot[0]);
+  mb.mdx = reinterpret_cast<float*>(base + ot[1]);
+  mb.sdy = reinterpret_cast<float*>(base + ot[2]);
+  mb.sdx = reinterpret_cast<float*>(base + ot[3]);
+  mb.best = reinterpret_cast<float*>(base + ot[4]);
+  mb.dy = reinterpret_cast<float*>(base + ot[5]);
+  mb.dx = reinterpret_cast<float*>(base + ot[6]);
+  mb.conf = reinterpret_cast<float*>(base + ot[7]);
+  hvdg::launch_motion(reinterpret_cast<const hvdg::MeField*>(base + o_f), 2, h, w,
+                      reinterpret_cast<const hvdg::MePair*>(base + o_p), 1, a, mb, s);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, mb.dy, sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dx, mb.dx, sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(confidence, mb.conf, sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "motion estimation");
+  return HVDG_OK;
 }
 
 hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* const* frames,

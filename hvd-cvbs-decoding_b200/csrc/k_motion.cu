@@ -1,0 +1,574 @@
+// k_motion.cu -- block-matching motion estimation (kernel d) and the
+// per-pixel vector field / warps / confidence upsampling that turn it into
+// neighbour terms.
+//
+// Reference: EstimateMotion (hvd-core/src/engine/motion.cpp:397-488) with
+// BoxBlur (:21-55, 391-395), Decimate (:59-78), BmPass (:105-260),
+// RangeFromCentre (:286-298), CostAt (:309-315), MotionConfidence (:321-387);
+// VectorsPerPixel / WarpByTiles / UpsampleConfidence[Fast]
+// (engine/temporal.cpp:45-254).
+//
+// Bit-exact to the reference's float arithmetic: this file is compiled with
+// FMA contraction off (--fmad=false), every float / double operation is
+// issued in the reference's order, and each (pair, tile) is one thread that
+// visits the candidates in the reference's centre-out order with the same
+// partial-distortion bail-out and strict-less update, so the selected
+// vectors, sub-pel fits and confidences equal the reference's bit for bit.
+#include <cuda_runtime.h>
+
+#include "hvdg_common.cuh"
+#include "k_motion.h"
+
+namespace hvdg {
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---- BoxBlur (motion.cpp:21-55): double prefix sums, constant 1/(2r+1) ----
+// Vertical pass: one thread per (field, column).
+__global__ void k_blur_v(const MeField* __restrict__ mf, int nf, const float* __restrict__ src,
+                         float* __restrict__ dst, int r, int src_sel) {
+  const int f = blockIdx.y;
+  if (f >= nf) return;
+  const MeField m = mf[f];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= m.w) return;
+  const int64_t sb = src_sel == 0 ? m.y_off : m.b_off;
+  const float* s = src + sb;
+  float* d = dst + m.t_off;
+  const double norm = (double)(1.0f / (float)(2 * r + 1));
+  // ring of prefix sums c[y] for y in [y - r, y + r + 1]
+  double ring[32];
+  const int R = 2 * r + 2;
+  double c = 0.0;
+  ring[0] = 0.0;
+  int next = 1;  // index of the next prefix value to produce (c[next])
+  for (int y = 0; y < m.h; ++y) {
+    const int y0 = y - r < 0 ? 0 : y - r;
+    const int y1 = y + r + 1 > m.h ? m.h : y + r + 1;
+    while (next <= y1) {
+      c = c + (double)s[(int64_t)(next - 1) * m.pitch + x];
+      ring[next % R] = c;
+      ++next;
+    }
+    d[(int64_t)y * m.pitch + x] = (float)((ring[y1 % R] - ring[y0 % R]) * norm);
+  }
+}
+
+// Horizontal pass: one thread per (field, row).
+__global__ void k_blur_h(const MeField* __restrict__ mf, int nf, const float* __restrict__ src,
+                         float* __restrict__ dst, int r) {
+  const int f = blockIdx.y;
+  if (f >= nf) return;
+  const MeField m = mf[f];
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= m.h) return;
+  const float* s = src + m.t_off + (int64_t)y * m.pitch;
+  float* d = dst + m.b_off + (int64_t)y * m.pitch;
+  const double norm = (double)(1.0f / (float)(2 * r + 1));
+  double ring[32];
+  const int R = 2 * r + 2;
+  double c = 0.0;
+  ring[0] = 0.0;
+  int next = 1;
+  for (int x = 0; x < m.w; ++x) {
+    const int x0 = x - r < 0 ? 0 : x - r;
+    const int x1 = x + r + 1 > m.w ? m.w : x + r + 1;
+    while (next <= x1) {
+      c = c + (double)s[next - 1];
+      ring[next % R] = c;
+      ++next;
+    }
+    d[x] = (float)((ring[x1 % R] - ring[x0 % R]) * norm);
+  }
+}
+
+// ---- Decimate (motion.cpp:59-78): 4 x 4 block mean ---------------------------
+__global__ void k_decimate(const MeField* __restrict__ mf, int nf, const float* __restrict__ blur,
+                           float* __restrict__ dec) {
+  const int f = blockIdx.y;
+  if (f >= nf) return;
+  const MeField m = mf[f];
+  const int hd = m.h / 4, wd = m.w / 4;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= hd * wd) return;
+  const int y = i / wd, x = i % wd;
+  const float* b = blur + m.b_off;
+  float acc = 0.0f;
+  for (int dy = 0; dy < 4; ++dy)
+    for (int dx = 0; dx < 4; ++dx) acc += b[(int64_t)(y * 4 + dy) * m.pitch + x * 4 + dx];
+  dec[m.d_off + (int64_t)y * m.dpitch + x] = acc * (1.0f / 16.0f);
+}
+
+// Sum of squared differences over one tile, rows in order, with the
+// reference's per-row partial-distortion bail-out (acc >= kill).
+__device__ __forceinline__ float tile_ssd(const float* A, const float* B, int pitch, int h, int w,
+                                          int ty0, int ty1, int tx0, int tx1, int sy, int sx,
+                                          float kill) {
+  float acc = 0.0f;
+  for (int y = ty0; y < ty1; ++y) {
+    const float* arow = A + (int64_t)y * pitch;
+    const float* brow = B + (int64_t)clampi(y - sy, 0, h - 1) * pitch;
+    for (int x = tx0; x < tx1; ++x) {
+      const float diff = arow[x] - brow[clampi(x - sx, 0, w - 1)];
+      acc += diff * diff;
+    }
+    if (acc >= kill) break;
+  }
+  return acc;
+}
+
+// centre-out candidate order (RangeFromCentre, motion.cpp:286-298) for a
+// symmetric range [-r, r]: 0, -1, 1, -2, 2, ...
+__device__ __forceinline__ int centre_out(int i) { return (i & 1) ? -((i + 1) >> 1) : (i >> 1); }
+
+// ---- coarse absolute pass on the 4x-decimated planes (motion.cpp:406-413) --
+__global__ void k_me_coarse(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                            int npairs, const float* __restrict__ dec, MeArgs a,
+                            float* __restrict__ cdy, float* __restrict__ cdx) {
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int hd = mc.h / 4, wd = mc.w / 4;
+  const int ct = a.tile / 4 > 4 ? a.tile / 4 : 4;
+  const int th = (hd + ct - 1) / ct, tw = (wd + ct - 1) / ct;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= th * tw) return;
+  const int ty = t / tw, tx = t % tw;
+  const int cs = (a.search + 3) / 4 > 1 ? (a.search + 3) / 4 : 1;
+  const float* A = dec + mc.d_off;
+  const float* B = dec + mr.d_off;
+  const int y0 = ty * ct, y1 = min((ty + 1) * ct, hd);
+  const int x0 = tx * ct, x1 = min((tx + 1) * ct, wd);
+  float best = __int_as_float(0x7f800000);
+  float bdy = 0.0f, bdx = 0.0f;
+  const int n = 2 * cs + 1;
+  for (int i = 0; i < n; ++i) {
+    const int dy = centre_out(i);
+    for (int j = 0; j < n; ++j) {
+      const int dx = centre_out(j);
+      const float bias = 1.0f + 0.02f * (float)(abs(dy) + abs(dx));
+      const float inv_bias = 1.0f / bias;
+      const bool exact = dy == 0 && dx == 0;  // cost0 needs the full sum
+      const float kill = exact ? __int_as_float(0x7f800000) : best * inv_bias;
+      const float se = tile_ssd(A, B, mc.dpitch, hd, wd, y0, y1, x0, x1, dy, dx, kill);
+      const float cost = se * bias;
+      if (cost < best) {
+        best = cost;
+        bdy = (float)dy;
+        bdx = (float)dx;
+      }
+    }
+  }
+  cdy[a.coarse_off * p + t] = bdy;
+  cdx[a.coarse_off * p + t] = bdx;
+}
+
+// ---- full-res refinement, sub-pel fit, zero / margin rule (motion.cpp:415-473)
+__global__ void k_me_refine(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                            int npairs, const float* __restrict__ blur, MeArgs a,
+                            const float* __restrict__ cdy, const float* __restrict__ cdx,
+                            float* __restrict__ out_mdy, float* __restrict__ out_mdx,
+                            float* __restrict__ out_sdy, float* __restrict__ out_sdx,
+                            float* __restrict__ out_best) {
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int h = mc.h, w = mc.w, tile = a.tile;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= th * tw) return;
+  const int ty = t / tw, tx = t % tw;
+  const int hd = h / 4, wd = w / 4;
+  const int ct = tile / 4 > 4 ? tile / 4 : 4;
+  const int hh = (hd + ct - 1) / ct, ww = (wd + ct - 1) / ct;
+  const int gy = min((ty * hh) / th, hh - 1), gx = min((tx * ww) / tw, ww - 1);
+  const float base_dy = cdy[a.coarse_off * p + gy * ww + gx] * 4.0f;
+  const float base_dx = cdx[a.coarse_off * p + gy * ww + gx] * 4.0f;
+  const float* A = blur + mc.b_off;
+  const float* B = blur + mr.b_off;
+  const int y0 = ty * tile, y1 = min((ty + 1) * tile, h);
+  const int x0 = tx * tile, x1 = min((tx + 1) * tile, w);
+  const float inf = __int_as_float(0x7f800000);
+  // refine: relative candidates RangeFromCentre(-3, 3)^2, no cost0
+  const int rby = (int)lroundf(base_dy), rbx = (int)lroundf(base_dx);
+  float best = inf, mdy = 0.0f, mdx = 0.0f;
+  for (int i = 0; i < 7; ++i) {
+    const int dy = centre_out(i);
+    for (int j = 0; j < 7; ++j) {
+      const int dx = centre_out(j);
+      const float bias = 1.0f + 0.02f * (float)(abs(dy) + abs(dx));
+      const float inv_bias = 1.0f / bias;
+      const float kill = best * inv_bias;
+      const float se = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, rby + dy, rbx + dx, kill);
+      const float cost = se * bias;
+      if (cost < best) {
+        best = cost;
+        mdy = base_dy + (float)dy;
+        mdx = base_dx + (float)dx;
+      }
+    }
+  }
+  // CostAt at (+-1, 0), (0, +-1): single relative candidate, full sum, bias 1
+  const int iy = (int)lroundf(mdy), ix = (int)lroundf(mdx);
+  const float cym = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1,
+                             (int)lroundf(mdy + -1.0f), ix, inf) * 1.0f;
+  const float cyp = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1,
+                             (int)lroundf(mdy + 1.0f), ix, inf) * 1.0f;
+  const float cxm = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, iy,
+                             (int)lroundf(mdx + -1.0f), inf) * 1.0f;
+  const float cxp = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, iy,
+                             (int)lroundf(mdx + 1.0f), inf) * 1.0f;
+  auto parabolic = [](float cm, float c0, float cp) {
+    const float den = cm - 2.0f * c0 + cp;
+    float sub = 0.0f;
+    if (den > 1e-9f) sub = 0.5f * (cm - cp) / fmaxf(den, 1e-9f);
+    return fminf(fmaxf(sub, -0.5f), 0.5f);
+  };
+  float sdy = parabolic(cym, best, cyp);
+  float sdx = parabolic(cxm, best, cxp);
+  // explicit zero-motion evaluation + "prefer zero" margin rule
+  const float cost0 = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, 0, 0, inf);
+  const float best0 = cost0 * 1.0f;
+  if (best0 < best) {
+    mdy = 0.0f;
+    mdx = 0.0f;
+    best = best0;
+  }
+  if (best > 0.85f * cost0) {
+    mdy = 0.0f;
+    mdx = 0.0f;
+    best = cost0;
+    sdy = 0.0f;
+    sdx = 0.0f;
+  }
+  const int o = a.tiles_off * p + t;
+  out_mdy[o] = mdy;
+  out_mdx[o] = mdx;
+  out_sdy[o] = sdy;
+  out_sdx[o] = sdx;
+  out_best[o] = best;
+}
+
+// ---- MotionConfidence (motion.cpp:321-387) + final vectors. One CTA per pair.
+__global__ void __launch_bounds__(256) k_me_confidence(const MeField* __restrict__ mf,
+                                                       const MePair* __restrict__ pairs,
+                                                       int npairs, const float* __restrict__ blur,
+                                                       MeArgs a, const float* __restrict__ mdy,
+                                                       const float* __restrict__ mdx,
+                                                       const float* __restrict__ sdy,
+                                                       const float* __restrict__ sdx,
+                                                       const float* __restrict__ bestv,
+                                                       float* __restrict__ out_dy,
+                                                       float* __restrict__ out_dx,
+                                                       float* __restrict__ out_conf) {
+  extern __shared__ float me_sm[];
+  __shared__ unsigned hist[256];
+  __shared__ unsigned bc[2];
+  const int p = blockIdx.x;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur];
+  const int h = mc.h, w = mc.w, tile = a.tile;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const int nt = th * tw;
+  float* ratios = me_sm;         // nt
+  float* conf0 = me_sm + nt;     // nt
+  const float* A = blur + mc.b_off;
+  const int o = a.tiles_off * p;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    const int ty = t / tw, tx = t % tw;
+    // pixels of this tile: rows/cols mapped by min(y / tile, th - 1)
+    const int y0 = ty * tile, y1 = (ty == th - 1) ? h : (ty + 1) * tile;
+    const int x0 = tx * tile, x1 = (tx == tw - 1) ? w : (tx + 1) * tile;
+    float sum = 0.0f, sum2 = 0.0f, np = 0.0f;
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) {
+        const float v = A[(int64_t)y * mc.pitch + x];
+        sum += v;
+        sum2 += v * v;
+        np += 1.0f;
+      }
+    const float norm = 1.0f / fmaxf(1.0f, np);
+    const float tmean = sum * norm;
+    const float tvar = sum2 * norm - tmean * tmean;
+    const float best = bestv[o + t];
+    const float energy = (tvar + 1.0f) * fmaxf(1.0f, np);
+    conf0[t] = fminf(fmaxf(1.0f - best / energy, 0.0f), 1.0f);
+    ratios[t] = best / fmaxf(1.0f, np);
+  }
+  __syncthreads();
+  // Median (motion.cpp:80-91): nth_element at n/2, averaged with the (n/2-1)-th for even n
+  const int k = nt / 2;
+  float med = block_select_kth(ratios, nt, k, hist, bc);
+  if (nt % 2 == 0) {
+    const float lo = block_select_kth(ratios, nt, k - 1, hist, bc);
+    med = 0.5f * (med + lo);
+  }
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    const float excess = fmaxf(0.0f, ratios[t] - med);
+    float c = conf0[t];
+    c *= (med + 1.0f) / (med + 1.0f + excess);
+    c *= 6.0f / (6.0f + med);
+    out_conf[o + t] = c;
+    out_dy[o + t] = mdy[o + t] + sdy[o + t];
+    out_dx[o + t] = mdx[o + t] + sdx[o + t];
+  }
+}
+
+void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const MePair* d_pairs,
+                   int npairs, const MeArgs& a, const MeBuffers& b, cudaStream_t st) {
+  if (nf <= 0 || npairs <= 0) return;
+  const int r = 2;
+  // blur every field's luma (A = blur(y_cur), B = blur(y_ref) share per field)
+  k_blur_v<<<dim3((max_w + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.luma, b.tmp, r, 0);
+  k_blur_h<<<dim3((max_h + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.tmp, b.blur, r);
+  k_decimate<<<dim3(((max_h / 4) * (max_w / 4) + 255) / 256, nf), 256, 0, st>>>(d_fields, nf, b.blur, b.dec);
+  const int ct = a.tile / 4 > 4 ? a.tile / 4 : 4;
+  const int cth = ((max_h / 4) + ct - 1) / ct, ctw = ((max_w / 4) + ct - 1) / ct;
+  k_me_coarse<<<dim3((cth * ctw + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, b.dec, a,
+                                                               b.cdy, b.cdx);
+  const int th = (max_h + a.tile - 1) / a.tile, tw = (max_w + a.tile - 1) / a.tile;
+  k_me_refine<<<dim3((th * tw + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, b.blur, a,
+                                                             b.cdy, b.cdx, b.mdy, b.mdx, b.sdy,
+                                                             b.sdx, b.best);
+  const int smem = 2 * th * tw * (int)sizeof(float);
+  k_me_confidence<<<npairs, 256, smem, st>>>(d_fields, d_pairs, npairs, b.blur, a, b.mdy, b.mdx,
+                                             b.sdy, b.sdx, b.best, b.dy, b.dx, b.conf);
+}
+
+// ---------------------------------------------------------------------------
+// VectorsPerPixel (temporal.cpp:45-112): 3x3 median outlier snap on the tile
+// grid, then bilinear interpolation between tile centres.
+// ---------------------------------------------------------------------------
+__device__ float median9(float* v) {
+  // exact middle of 9 values (nth_element(v, v + 4, v + 9))
+  for (int i = 0; i < 5; ++i) {
+    int mi = i;
+    for (int j = i + 1; j < 9; ++j)
+      if (v[j] < v[mi]) mi = j;
+    const float t = v[i];
+    v[i] = v[mi];
+    v[mi] = t;
+  }
+  return v[4];
+}
+
+// Snapped tile vectors; one thread per (pair, tile).
+__global__ void k_vec_snap(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                           int npairs, MeArgs a, const float* __restrict__ dy_in,
+                           const float* __restrict__ dx_in, float* __restrict__ dy_out,
+                           float* __restrict__ dx_out) {
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MeField mc = mf[pairs[p].cur];
+  const int th = (mc.h + a.tile - 1) / a.tile, tw = (mc.w + a.tile - 1) / a.tile;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= th * tw) return;
+  const int o = a.tiles_off * p;
+  float vy = dy_in[o + t], vx = dx_in[o + t];
+  if (th >= 3 && tw >= 3) {
+    const int ty = t / tw, tx = t % tw;
+    float ay[9], ax[9];
+    int q = 0;
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int yy = clampi(ty + dy, 0, th - 1), xx = clampi(tx + dx, 0, tw - 1);
+        ay[q] = dy_in[o + yy * tw + xx];
+        ax[q] = dx_in[o + yy * tw + xx];
+        ++q;
+      }
+    const float my = median9(ay), mx = median9(ax);
+    const float dis = fabsf(vy - my) + fabsf(vx - mx);
+    if (dis > 3.0f) {
+      vy = my;
+      vx = mx;
+    }
+  }
+  dy_out[o + t] = vy;
+  dx_out[o + t] = vx;
+}
+
+__device__ __forceinline__ void bracket(int coord, int n_tiles, int tile, int* lo, float* frac) {
+  if (n_tiles > 1) {
+    const float rel = (float)coord / (float)tile - 0.5f;
+    *lo = clampi((int)floorf(rel), 0, n_tiles - 2);
+    const float centre_lo = ((float)*lo + 0.5f) * (float)tile;
+    *frac = fminf(fmaxf(((float)coord - centre_lo) / (float)tile, 0.0f), 1.0f);
+  } else {
+    *lo = 0;
+    *frac = 0.0f;
+  }
+}
+
+__device__ __forceinline__ float interp_tiles(const float* v, int tw, int iy, int iy1, int ix,
+                                              int ix1, float fy, float fx) {
+  const float v00 = v[iy * tw + ix], v10 = v[iy1 * tw + ix];
+  const float v01 = v[iy * tw + ix1], v11 = v[iy1 * tw + ix1];
+  return v00 * (1 - fy) * (1 - fx) + v10 * fy * (1 - fx) + v01 * (1 - fy) * fx + v11 * fy * fx;
+}
+
+// Per-pixel vectors for one pair, written as the warp source indices
+// (sy, sx) = (clamp(y - lround(vdy)), clamp(x - lround(vdx))) packed in an
+// int2, plus (optionally) the interpolated squared confidence (fast mode).
+__global__ void k_vec_pixels(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                             int npairs, MeArgs a, const float* __restrict__ sdy,
+                             const float* __restrict__ sdx, int2* __restrict__ src_idx,
+                             const int64_t* __restrict__ pix_off) {
+  const int p = blockIdx.z;
+  if (p >= npairs) return;
+  const MeField mc = mf[pairs[p].cur];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= mc.w || y >= mc.h) return;
+  const int th = (mc.h + a.tile - 1) / a.tile, tw = (mc.w + a.tile - 1) / a.tile;
+  int iy, ix;
+  float fy, fx;
+  bracket(y, th, a.tile, &iy, &fy);
+  bracket(x, tw, a.tile, &ix, &fx);
+  const int iy1 = min(iy + 1, th - 1), ix1 = min(ix + 1, tw - 1);
+  const int o = a.tiles_off * p;
+  const float vy = interp_tiles(sdy + o, tw, iy, iy1, ix, ix1, fy, fx);
+  const float vx = interp_tiles(sdx + o, tw, iy, iy1, ix, ix1, fy, fx);
+  const int sy = clampi(y - (int)lroundf(vy), 0, mc.h - 1);
+  const int sx = clampi(x - (int)lroundf(vx), 0, mc.w - 1);
+  src_idx[pix_off[p] + (int64_t)y * mc.pitch + x] = make_int2(sy, sx);
+}
+
+// Squared per-tile confidence -> per pixel.
+//   fast: VectorsPerPixel of conf^2 (snap + bilinear), temporal.cpp:245-254
+//   slow: nearest tile, squared, then BoxBlur radius 8, temporal.cpp:227-243
+__global__ void k_conf_sq(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                          int npairs, MeArgs a, const float* __restrict__ conf,
+                          float* __restrict__ c2) {
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MeField mc = mf[pairs[p].cur];
+  const int nt = ((mc.h + a.tile - 1) / a.tile) * ((mc.w + a.tile - 1) / a.tile);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const float c = conf[a.tiles_off * p + t];
+  c2[a.tiles_off * p + t] = c * c;
+}
+
+__global__ void k_conf_pixels_fast(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                                   int npairs, MeArgs a, const float* __restrict__ c2s,
+                                   float* __restrict__ out, const int64_t* __restrict__ pix_off) {
+  const int p = blockIdx.z;
+  if (p >= npairs) return;
+  const MeField mc = mf[pairs[p].cur];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= mc.w || y >= mc.h) return;
+  const int th = (mc.h + a.tile - 1) / a.tile, tw = (mc.w + a.tile - 1) / a.tile;
+  int iy, ix;
+  float fy, fx;
+  bracket(y, th, a.tile, &iy, &fy);
+  bracket(x, tw, a.tile, &ix, &fx);
+  out[pix_off[p] + (int64_t)y * mc.pitch + x] =
+      interp_tiles(c2s + a.tiles_off * p, tw, iy, min(iy + 1, th - 1), ix, min(ix + 1, tw - 1), fy, fx);
+}
+
+__global__ void k_conf_pixels_nearest(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                                      int npairs, MeArgs a, const float* __restrict__ conf,
+                                      float* __restrict__ out, const int64_t* __restrict__ pix_off) {
+  const int p = blockIdx.z;
+  if (p >= npairs) return;
+  const MeField mc = mf[pairs[p].cur];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= mc.w || y >= mc.h) return;
+  const int th = (mc.h + a.tile - 1) / a.tile, tw = (mc.w + a.tile - 1) / a.tile;
+  const int ty = min(y / a.tile, th - 1), tx = min(x / a.tile, tw - 1);
+  const float c = conf[a.tiles_off * p + ty * tw + tx];
+  out[pix_off[p] + (int64_t)y * mc.pitch + x] = c * c;
+}
+
+// BoxBlur radius r over per-pair planes (same prefix-sum arithmetic as the
+// luma blur); in place through a scratch plane.
+__global__ void k_pair_blur_v(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                              int npairs, const float* __restrict__ src, float* __restrict__ dst,
+                              const int64_t* __restrict__ pix_off, int r) {
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MeField m = mf[pairs[p].cur];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= m.w) return;
+  const float* s = src + pix_off[p];
+  float* d = dst + pix_off[p];
+  const double norm = (double)(1.0f / (float)(2 * r + 1));
+  double ring[32];
+  const int R = 2 * r + 2;
+  double c = 0.0;
+  ring[0] = 0.0;
+  int next = 1;
+  for (int y = 0; y < m.h; ++y) {
+    const int y0 = y - r < 0 ? 0 : y - r;
+    const int y1 = y + r + 1 > m.h ? m.h : y + r + 1;
+    while (next <= y1) {
+      c = c + (double)s[(int64_t)(next - 1) * m.pitch + x];
+      ring[next % R] = c;
+      ++next;
+    }
+    d[(int64_t)y * m.pitch + x] = (float)((ring[y1 % R] - ring[y0 % R]) * norm);
+  }
+}
+
+__global__ void k_pair_blur_h(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                              int npairs, const float* __restrict__ src, float* __restrict__ dst,
+                              const int64_t* __restrict__ pix_off, int r) {
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MeField m = mf[pairs[p].cur];
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= m.h) return;
+  const float* s = src + pix_off[p] + (int64_t)y * m.pitch;
+  float* d = dst + pix_off[p] + (int64_t)y * m.pitch;
+  const double norm = (double)(1.0f / (float)(2 * r + 1));
+  double ring[32];
+  const int R = 2 * r + 2;
+  double c = 0.0;
+  ring[0] = 0.0;
+  int next = 1;
+  for (int x = 0; x < m.w; ++x) {
+    const int x0 = x - r < 0 ? 0 : x - r;
+    const int x1 = x + r + 1 > m.w ? m.w : x + r + 1;
+    while (next <= x1) {
+      c = c + (double)s[next - 1];
+      ring[next % R] = c;
+      ++next;
+    }
+    d[x] = (float)((ring[x1 % R] - ring[x0 % R]) * norm);
+  }
+}
+
+void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                    int max_w, const MeArgs& a, const VecBuffers& v, bool fast_conf,
+                    cudaStream_t st) {
+  if (npairs <= 0) return;
+  const int th = (max_h + a.tile - 1) / a.tile, tw = (max_w + a.tile - 1) / a.tile;
+  const int nt = th * tw;
+  k_vec_snap<<<dim3((nt + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, a, v.dy, v.dx,
+                                                          v.snap_dy, v.snap_dx);
+  k_vec_pixels<<<dim3((max_w + 127) / 128, max_h, npairs), 128, 0, st>>>(
+      d_fields, d_pairs, npairs, a, v.snap_dy, v.snap_dx, v.src_idx, v.pix_off);
+  if (fast_conf) {
+    k_conf_sq<<<dim3((nt + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, a, v.conf, v.c2);
+    k_vec_snap<<<dim3((nt + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, a, v.c2, v.c2,
+                                                            v.c2_snap, v.c2_snap2);
+    k_conf_pixels_fast<<<dim3((max_w + 127) / 128, max_h, npairs), 128, 0, st>>>(
+        d_fields, d_pairs, npairs, a, v.c2_snap, v.conf_px, v.pix_off);
+  } else {
+    k_conf_pixels_nearest<<<dim3((max_w + 127) / 128, max_h, npairs), 128, 0, st>>>(
+        d_fields, d_pairs, npairs, a, v.conf, v.conf_tmp, v.pix_off);
+    k_pair_blur_v<<<dim3((max_w + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
+                                                                     v.conf_tmp, v.conf_px,
+                                                                     v.pix_off, 8);
+    k_pair_blur_h<<<dim3((max_h + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
+                                                                     v.conf_px, v.conf_tmp,
+                                                                     v.pix_off, 8);
+    cudaMemcpyAsync(v.conf_px, v.conf_tmp, v.conf_bytes, cudaMemcpyDeviceToDevice, st);
+  }
+}
+
+}  // namespace hvdg
