@@ -23,6 +23,7 @@
 #include "hvdg_host.h"
 #include "k_init.h"
 #include "k_motion.h"
+#include "k_temporal.h"
 #include "k_prep.h"
 #include "k_solver.h"
 
@@ -544,27 +545,37 @@ struct RunOpts {
   const float* chi0_in = nullptr;    // dense h x w x 2
 };
 
-// The 2-D pipeline over one batch: lock-in, crop, init, aniso, solver.
-hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
-                      hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt) {
+// A batch uploaded to the arena: layout, table offsets, launch count.
+struct Staged {
   Batch b;
+  size_t it_itab = 0, it_crf = 0, it_crfirst = 0, it_pitch = 0, it_pxoff = 0, it_rbo = 0;
+  size_t extra = 0;  // offset of the caller's extra region (after the batch layout)
+  int launches = 0;
+};
+
+// Plan the batch, reserve the arena (+ `extra_bytes` for the caller), upload
+// the tables and raw samples, reset the solver control state.
+hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
+                         const RunOpts& opt, size_t extra_bytes, Staged& S) {
+  Batch& b = S.b;
   hvdg_status st = plan_batch(ctx, in, n, cfg, ctx->band_rows, b);
   if (st != HVDG_OK) return st;
   const Layout& L = b.L;
-  st = ctx->arena.reserve(L.total);
+  S.extra = align_up(L.total, 256);
+  st = ctx->arena.reserve(S.extra + extra_bytes);
   if (st != HVDG_OK) {
     ctx->last_error = "device arena allocation failed";
     return st;
   }
   cudaStream_t s = ctx->stream;
   cudaError_t e;
-  // ---- tables to the device (one staging copy) ----
   std::vector<char> host(L.o_S - L.o_prep, 0);
   auto put = [&](size_t off, const void* src, size_t bytes) {
     if (bytes) std::memcpy(host.data() + (off - L.o_prep), src, bytes);
   };
   for (int i = 0; i < n; ++i) {
-    b.prep[i].samples = opt.device_io ? in[i].samples : (const void*)(at<char>(ctx, L.o_raw) + b.fp[i].raw_off);
+    b.prep[i].samples = opt.device_io ? in[i].samples
+                                      : (const void*)(at<char>(ctx, L.o_raw) + b.fp[i].raw_off);
   }
   put(L.o_prep, b.prep.data(), sizeof(hvdg::PrepDesc) * n);
   put(L.o_fields, b.fields.data(), sizeof(FieldDesc) * n);
@@ -588,27 +599,26 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
     put(L.o_twc, twc.data(), sizeof(float2) * twc.size());
   }
   size_t it = L.o_itab;
-  const size_t it_itab = it;
+  S.it_itab = it;
   put(it, b.itab.data(), sizeof(int) * b.itab.size());
   it += sizeof(int) * b.itab.size();
-  const size_t it_crf = it;
+  S.it_crf = it;
   put(it, b.crop_row_field.data(), sizeof(int) * b.crop_row_field.size());
   it += sizeof(int) * b.crop_row_field.size();
-  const size_t it_crfirst = it;
+  S.it_crfirst = it;
   put(it, b.crop_row_first.data(), sizeof(int) * b.crop_row_first.size());
   it += sizeof(int) * b.crop_row_first.size();
-  const size_t it_pitch = it;
+  S.it_pitch = it;
   put(it, b.pitches.data(), sizeof(int) * b.pitches.size());
   it += sizeof(int) * b.pitches.size();
   it = align_up(it, 8);
-  const size_t it_pxoff = it;
+  S.it_pxoff = it;
   put(it, b.px_offs.data(), sizeof(int64_t) * b.px_offs.size());
   it += sizeof(int64_t) * b.px_offs.size();
-  const size_t it_rbo = it;
+  S.it_rbo = it;
   put(it, b.rowbuf_offs.data(), sizeof(int64_t) * b.rowbuf_offs.size());
 
   cudaEventRecord(ctx->ev[0], s);
-  // raw samples
   if (!opt.device_io && opt.do_lockin) {
     for (int i = 0; i < n; ++i) {
       e = cudaMemcpyAsync(at<char>(ctx, L.o_raw) + b.fp[i].raw_off, in[i].samples,
@@ -622,9 +632,16 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
   cudaMemsetAsync(at<char>(ctx, L.o_arrive), 0, sizeof(int) * n, s);
   cudaMemsetAsync(at<char>(ctx, L.o_flags), 0, sizeof(int) * 4, s);
   cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
-  int launches = 0;
+  return HVDG_OK;
+}
 
-  // ---- lock-in + crop ----
+// Lock-in (or caller phases), crop (or caller S), caller chi0, holographic init.
+hvdg_status stage_prepare(hvdg_ctx* ctx, Staged& S, const RunOpts& opt) {
+  const Batch& b = S.b;
+  const Layout& L = b.L;
+  const int n = (int)b.fp.size();
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
   cudaEventRecord(ctx->ev[1], s);
   hvdg::LockinOut lo;
   lo.theta = at<float>(ctx, L.o_theta);
@@ -634,7 +651,7 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
   std::vector<float4> lph_host;
   if (opt.do_lockin) {
     hvdg::launch_burst_lockin(at<hvdg::PrepDesc>(ctx, L.o_prep), n, lo, s);
-    launches += 1;
+    S.launches += 1;
   } else {
     // caller-supplied active-line phases (one field): exp(i theta) in FP64
     const FieldPlan& p = b.fp[0];
@@ -647,6 +664,9 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
     e = cudaMemcpyAsync(at<float4>(ctx, L.o_lineph), lph_host.data(), sizeof(float4) * p.h,
                         cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D line phasors");
+    // the host copy must outlive the async copy
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D line phasors");
   }
   if (opt.s_in) {
     const FieldPlan& p = b.fp[0];
@@ -654,11 +674,11 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
                           sizeof(float) * p.w, sizeof(float) * p.w, p.h, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D S");
   } else {
-    hvdg::launch_crop(at<hvdg::PrepDesc>(ctx, L.o_prep), at<int>(ctx, it_crf),
-                      at<int>(ctx, it_crfirst), L.total_lines, at<float>(ctx, L.o_S),
-                      at<int64_t>(ctx, it_pxoff), at<int>(ctx, it_pitch),
+    hvdg::launch_crop(at<hvdg::PrepDesc>(ctx, L.o_prep), at<int>(ctx, S.it_crf),
+                      at<int>(ctx, S.it_crfirst), L.total_lines, at<float>(ctx, L.o_S),
+                      at<int64_t>(ctx, S.it_pxoff), at<int>(ctx, S.it_pitch),
                       at<int>(ctx, L.o_flags) + 1, s);
-    launches += 1;
+    S.launches += 1;
   }
   if (opt.chi0_in) {
     const FieldPlan& p = b.fp[0];
@@ -666,46 +686,45 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
                           sizeof(float2) * p.w, sizeof(float2) * p.w, p.h, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D chi0");
   }
-  // ---- holographic init ----
-  hvdg::InitArgs ia;
-  ia.fields = at<FieldDesc>(ctx, L.o_fields);
-  ia.geoms = at<GeomDesc>(ctx, L.o_geoms);
-  ia.S = at<float>(ctx, L.o_S);
-  ia.line_phasor = at<float4>(ctx, L.o_lineph);
-  ia.col_phasor = at<float2>(ctx, L.o_colph);
-  ia.khat = at<float2>(ctx, L.o_khat);
-  ia.tw_row = at<float2>(ctx, L.o_twr);
-  ia.tw_col = at<float2>(ctx, L.o_twc);
-  ia.rowbuf = at<float2>(ctx, L.o_rowbuf);
-  ia.rowbuf_off = at<int64_t>(ctx, it_rbo);
-  ia.chi1 = at<float2>(ctx, L.o_G0);
-  ia.chi2 = at<float2>(ctx, L.o_D0);
-  ia.chi0 = at<float2>(ctx, L.o_X0);
-  ia.Y = at<float>(ctx, L.o_Y);
-  const int* itb = at<int>(ctx, it_itab);
-  ia.prow_field = itb + b.it_prow_field;
-  ia.prow_first = itb + b.it_prow_first;
-  ia.cgrp_field = itb + b.it_cgrp_field;
-  ia.cgrp_first = itb + b.it_cgrp_first;
-  ia.btile_field = itb + b.it_btile_field;
-  ia.btile_first = itb + b.it_btile_first;
   if (opt.do_init) {
+    hvdg::InitArgs ia;
+    ia.fields = at<FieldDesc>(ctx, L.o_fields);
+    ia.geoms = at<GeomDesc>(ctx, L.o_geoms);
+    ia.S = at<float>(ctx, L.o_S);
+    ia.line_phasor = at<float4>(ctx, L.o_lineph);
+    ia.col_phasor = at<float2>(ctx, L.o_colph);
+    ia.khat = at<float2>(ctx, L.o_khat);
+    ia.tw_row = at<float2>(ctx, L.o_twr);
+    ia.tw_col = at<float2>(ctx, L.o_twc);
+    ia.rowbuf = at<float2>(ctx, L.o_rowbuf);
+    ia.rowbuf_off = at<int64_t>(ctx, S.it_rbo);
+    ia.chi1 = at<float2>(ctx, L.o_G0);
+    ia.chi2 = at<float2>(ctx, L.o_D0);
+    ia.chi0 = at<float2>(ctx, L.o_X0);
+    ia.Y = at<float>(ctx, L.o_Y);
+    const int* itb = at<int>(ctx, S.it_itab);
+    ia.prow_field = itb + b.it_prow_field;
+    ia.prow_first = itb + b.it_prow_first;
+    ia.cgrp_field = itb + b.it_cgrp_field;
+    ia.cgrp_first = itb + b.it_cgrp_first;
+    ia.btile_field = itb + b.it_btile_field;
+    ia.btile_first = itb + b.it_btile_first;
     hvdg::launch_init(ia, L.total_prows, L.total_cgroups, L.total_btiles, s);
-    launches += 3;
+    S.launches += 3;
   }
-  if (opt.do_solve) {
-    hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), n, at<float2>(ctx, L.o_X0), s);
-    launches += 1;
-  }
-  cudaEventRecord(ctx->ev[2], s);
-  // ---- solver ----
+  return HVDG_OK;
+}
+
+hvdg::SolverArgs solver_args(hvdg_ctx* ctx, const Staged& S) {
+  const Layout& L = S.b.L;
   hvdg::SolverArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.fields = at<FieldDesc>(ctx, L.o_fields);
   sa.ctl = at<FieldCtl>(ctx, L.o_ctl);
   sa.units = at<Unit>(ctx, L.o_units);
+  sa.unit_base = 0;
   sa.n_units = L.total_units;
-  sa.n_phases = b.max_phases;
+  sa.n_phases = S.b.max_phases;
   sa.queue = at<unsigned long long>(ctx, L.o_queue);
   sa.done_phase = at<int>(ctx, L.o_done);
   sa.arrive = at<int>(ctx, L.o_arrive);
@@ -724,19 +743,26 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
   sa.Y = at<float>(ctx, L.o_Y);
   sa.line_phasor = at<float4>(ctx, L.o_lineph);
   sa.col_phasor = at<float2>(ctx, L.o_colph);
+  return sa;
+}
+
+int solver_grid(hvdg_ctx* ctx, int n_units) {
   const int per_sm = ctx->ctas_per_sm > 0 ? ctx->ctas_per_sm
                                           : std::max(1, hvdg::solver_max_blocks_per_sm());
-  int grid = ctx->sm_count * per_sm;
+  const int grid = ctx->sm_count * per_sm;
   // never more warps than the first phase can use
-  grid = std::max(1, std::min(grid, (L.total_units + (hvdg::kSolverThreads / 32) - 1) /
+  return std::max(1, std::min(grid, (n_units + (hvdg::kSolverThreads / 32) - 1) /
                                         (hvdg::kSolverThreads / 32)));
-  if (opt.do_solve) {
-    e = hvdg::launch_solver(sa, grid, s);
-    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
-    launches += 1;
-  }
-  cudaEventRecord(ctx->ev[3], s);
-  // ---- outputs ----
+}
+
+// Copy the outputs, read the flags, synchronise, fill the diagnostics.
+hvdg_status stage_finish(hvdg_ctx* ctx, Staged& S, hvdg_field_out* out, const RunOpts& opt,
+                         hvdg_diag* diag) {
+  const Batch& b = S.b;
+  const Layout& L = b.L;
+  const int n = (int)b.fp.size();
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
   const cudaMemcpyKind kind = opt.device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   for (int i = 0; i < n; ++i) {
     const FieldPlan& p = b.fp[i];
@@ -764,8 +790,9 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
   e = cudaMemcpyAsync(flags, at<int>(ctx, L.o_flags), sizeof(flags), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy flags");
   std::vector<FieldCtl> ctl(n);
-  if (diag) cudaMemcpyAsync(ctl.data(), at<FieldCtl>(ctx, L.o_ctl), sizeof(FieldCtl) * n,
-                            cudaMemcpyDeviceToHost, s);
+  if (diag)
+    cudaMemcpyAsync(ctl.data(), at<FieldCtl>(ctx, L.o_ctl), sizeof(FieldCtl) * n,
+                    cudaMemcpyDeviceToHost, s);
   cudaEventRecord(ctx->ev[4], s);
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "stream sync");
@@ -782,7 +809,7 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
       diag->solver_pixel_iters += (int64_t)ctl[i].cg_iters * b.fp[i].h * b.fp[i].w;
       diag->solver_pixel_outers += (int64_t)b.fields[i].n_outer * b.fp[i].h * b.fp[i].w;
     }
-    diag->kernel_launches += launches;
+    diag->kernel_launches += S.launches;
   }
   if (flags[1]) {
     ctx->last_error = "non-finite input samples";
@@ -793,6 +820,31 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
     return HVDG_ERR_DEVICE_TIMEOUT;
   }
   return HVDG_OK;
+}
+
+// The 2-D pipeline over one batch: lock-in, crop, init, aniso, solver.
+hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
+                      hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt) {
+  Staged S;
+  hvdg_status st = stage_upload(ctx, in, n, cfg, opt, 0, S);
+  if (st != HVDG_OK) return st;
+  st = stage_prepare(ctx, S, opt);
+  if (st != HVDG_OK) return st;
+  const Layout& L = S.b.L;
+  cudaStream_t s = ctx->stream;
+  if (opt.do_solve) {
+    hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), n, at<float2>(ctx, L.o_X0), s);
+    S.launches += 1;
+  }
+  cudaEventRecord(ctx->ev[2], s);
+  if (opt.do_solve) {
+    const hvdg::SolverArgs sa = solver_args(ctx, S);
+    const cudaError_t e = hvdg::launch_solver(sa, solver_grid(ctx, L.total_units), s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
+    S.launches += 1;
+  }
+  cudaEventRecord(ctx->ev[3], s);
+  return stage_finish(ctx, S, out, opt, diag);
 }
 
 hvdg_status validate_fields(const hvdg_field_in* fields, int n, const hvdg_config* cfg,
@@ -811,6 +863,429 @@ hvdg_status validate_fields(const hvdg_field_in* fields, int n, const hvdg_confi
   return HVDG_OK;
 }
 
+float median_mean(std::vector<float> v) {
+  // MedianOf (sequence.cpp:29-39): mean of the two middles for even n
+  if (v.empty()) return 0.0f;
+  const size_t k = v.size() / 2;
+  std::nth_element(v.begin(), v.begin() + k, v.end());
+  float m = v[k];
+  if (v.size() % 2 == 0) {
+    std::nth_element(v.begin(), v.begin() + k - 1, v.begin() + k);
+    m = 0.5f * (m + v[k - 1]);
+  }
+  return m;
+}
+
+// Adaptive temporal strength (sequence.cpp:526-646): same-parity pair
+// ambiguity from a triangle-7 demodulation of S by each field's carrier,
+// per horizontal band, p95 of bands, median over pairs, noise-floor removal.
+float adaptive_strength(const std::vector<std::vector<float>>& Sh,
+                        const std::vector<std::vector<float4>>& Lh, const std::vector<float2>& P,
+                        int h, int w, int stride, float nr_eps, float* amb_out) {
+  static const float kW[7] = {1.f, 2.f, 3.f, 4.f, 3.f, 2.f, 1.f};
+  const int nf = (int)Sh.size();
+  auto car = [&](int f, int y, int x) {
+    const float4 L = Lh[f][y];
+    const float2 c = make_float2(L.x * P[x].x - L.y * P[x].y, L.x * P[x].y + L.y * P[x].x);
+    return L.z < 0.f ? make_float2(-c.x, c.y) : c;
+  };
+  std::vector<float> ambs;
+  for (int j = 0; j + stride < nf; ++j) {
+    const int k = j + stride;
+    std::vector<double> band_acc;
+    std::vector<long> band_n;
+    double acc = 0.0;
+    long n = 0;
+    int yi = 0;
+    for (int y = 2; y < h - 2; y += 3, ++yi) {
+      const int band = yi / 8;
+      if (band >= (int)band_acc.size()) {
+        band_acc.push_back(0.0);
+        band_n.push_back(0);
+      }
+      for (int x = 4; x + 7 < w; x += 4) {
+        float mj = 0.f, mk = 0.f;
+        for (int q = 0; q < 4; ++q) {
+          mj += Sh[j][(size_t)y * w + x + q];
+          mk += Sh[k][(size_t)y * w + x + q];
+        }
+        if (std::fabs(mj - mk) * 0.25f > nr_eps) continue;
+        auto demod = [&](int f) {
+          float dr = 0.f, di = 0.f;
+          for (int q = 0; q < 7; ++q) {
+            const float sv = kW[q] * Sh[f][(size_t)y * w + x + q];
+            const float2 c = car(f, y, x + q);
+            dr += sv * c.x;
+            di += -sv * c.y;
+          }
+          return make_float2(dr * (1.0f / 16.0f), di * (1.0f / 16.0f));
+        };
+        const float2 dj = demod(j), dk = demod(k);
+        const float er = dj.x - dk.x, ei = dj.y - dk.y;
+        const double e = 0.25 * (double)(er * er + ei * ei);
+        acc += e;
+        ++n;
+        band_acc[band] += e;
+        ++band_n[band];
+      }
+    }
+    if (n > 0) {
+      std::vector<float> brms;
+      for (size_t b = 0; b < band_acc.size(); ++b)
+        if (band_n[b] >= 8) brms.push_back((float)(band_acc[b] / band_n[b]));
+      if (!brms.empty()) {
+        const size_t k95 = std::min(brms.size() - 1, (size_t)(0.95 * brms.size()));
+        std::nth_element(brms.begin(), brms.begin() + k95, brms.end());
+        ambs.push_back(std::sqrt(brms[k95]));
+      } else {
+        ambs.push_back(std::sqrt((float)(acc / n)));
+      }
+    }
+  }
+  float amb = median_mean(ambs);
+  const float sigma_d = nr_eps > 0.0f ? nr_eps / 3.0f : 1.0f;
+  const float noise_floor = sigma_d * 0.29f;
+  amb = std::sqrt(std::max(0.0f, amb * amb - noise_floor * noise_floor));
+  if (amb_out) *amb_out = amb;
+  return std::min(std::max(0.5f * amb - 0.05f, 0.0f), 1.5f);
+}
+
+// DecodeFieldWindowWithInits (sequence.cpp:423-1116) for one window of one
+// geometry, temporal terms included: noise self-calibration, adaptive
+// strength, coloured Gauss-Seidel sweep (or the sequential sweep in slow
+// mode); per colour, motion estimation on the current luma state, warps,
+// confidence upsampling, the odd-offset envelope gate and the neighbour
+// planes, then the solver over that colour's fields.
+hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
+                             const hvdg_config* cfg_in, hvdg_field_out* out, hvdg_diag* diag,
+                             const RunOpts& opt) {
+  hvdg_config cfg = *cfg_in;
+  const hvdg_geometry& g = *in[0].geometry;
+  const bool pal = uses_vswitch(g);
+  std::vector<int> offs;
+  if (cfg.extended_temporal) {
+    offs = pal ? (cfg.bidirectional ? std::vector<int>{-4, -3, -2, -1, 1, 2, 3, 4}
+                                    : std::vector<int>{-4, -3, -2, -1})
+               : (cfg.bidirectional ? std::vector<int>{-3, -2, -1, 1, 2, 3}
+                                    : std::vector<int>{-3, -2, -1});
+  } else {
+    offs = cfg.bidirectional ? std::vector<int>{-2, -1, 1, 2} : std::vector<int>{-2, -1};
+  }
+  if (pal) {
+    if (cfg.coherence_gate == 0.6f) cfg.coherence_gate = 1.0f;
+    if (cfg.nr_radius == 2) cfg.nr_radius = 4;
+  }
+  // ---- layout: batch + 3-D regions ----
+  Batch plan;
+  hvdg_status st = plan_batch(ctx, in, nf, &cfg, ctx->band_rows, plan);
+  if (st != HVDG_OK) return st;
+  const int h = plan.fp[0].h, w = plan.fp[0].w, pitch = plan.fp[0].pitch;
+  const int64_t plane = (int64_t)h * pitch;
+  const int nofs = (int)offs.size();
+  const int tile = cfg.mc_tile, search = cfg.mc_search;
+  if (tile < 1 || search < 0 || tile > 1024 || search > 64) return HVDG_ERR_BAD_ARGUMENT;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile, nt = th * tw;
+  const int ct = std::max(4, tile / 4);
+  const int nct = std::max(1, ((h / 4 + ct - 1) / ct) * ((w / 4 + ct - 1) / ct));
+  const int dpitch = pitch / 4;
+  const int64_t dplane = (int64_t)(h / 4 + 1) * dpitch;
+  const int max_pairs = nf * nofs;
+  size_t xo = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = xo;
+    xo = align_up(xo + bytes, 256);
+    return r;
+  };
+  const size_t x_M = take(sizeof(float4) * plane * nf);
+  const size_t x_B = take(sizeof(float2) * plane * nf);
+  const size_t x_nbr = take(sizeof(float4) * plane * nf * nofs);
+  const size_t x_tmp = take(sizeof(float) * plane * nf);
+  const size_t x_blur = take(sizeof(float) * plane * nf);
+  const size_t x_dec = take(sizeof(float) * dplane * nf);
+  const size_t x_cdy = take(sizeof(float) * nct * max_pairs);
+  const size_t x_cdx = take(sizeof(float) * nct * max_pairs);
+  size_t x_t[13];
+  for (int i = 0; i < 13; ++i) x_t[i] = take(sizeof(float) * nt * max_pairs);
+  const size_t x_src = take(sizeof(int2) * plane * max_pairs);
+  const size_t x_cpx = take(sizeof(float) * plane * max_pairs);
+  const size_t x_ctmp = take(sizeof(float) * plane * max_pairs);
+  size_t x_env[5];
+  for (int i = 0; i < 5; ++i) x_env[i] = take(sizeof(float) * plane * nf);
+  const size_t env_samples = ((size_t)h * w + 6) / 7;
+  const size_t x_escr = take(sizeof(float) * env_samples * nf);
+  const size_t x_nscr = take(sizeof(float) * (size_t)h * std::max(1, w - 8) * nf);
+  const size_t x_small = take(sizeof(float) * 4 * nf + sizeof(int64_t) * (3 * nf + max_pairs) +
+                              sizeof(int) * nf + sizeof(hvdg::MeField) * nf +
+                              sizeof(hvdg::MePair) * max_pairs +
+                              sizeof(hvdg::NbrPair) * max_pairs + 1024);
+  Staged S;
+  st = stage_upload(ctx, in, nf, &cfg, opt, xo, S);
+  if (st != HVDG_OK) return st;
+  Batch& b = S.b;
+  const Layout& L = b.L;
+  auto X = [&](size_t off) { return S.extra + off; };
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  st = stage_prepare(ctx, S, opt);
+  if (st != HVDG_OK) return st;
+
+  // ---- small device tables ----
+  char* small = at<char>(ctx, X(x_small));
+  float* d_sigma = reinterpret_cast<float*>(small);
+  float* d_floor2 = d_sigma + nf;
+  int64_t* d_nscr_off = reinterpret_cast<int64_t*>(align_up((size_t)(d_floor2 + nf), 8));
+  int64_t* d_escr_off = d_nscr_off + nf;
+  int64_t* d_pix_off = d_escr_off + nf;
+  int* d_list = reinterpret_cast<int*>(d_pix_off + max_pairs);
+  hvdg::MeField* d_mf = reinterpret_cast<hvdg::MeField*>(align_up((size_t)(d_list + nf), 16));
+  hvdg::MePair* d_mp = reinterpret_cast<hvdg::MePair*>(d_mf + nf);
+  hvdg::NbrPair* d_np = reinterpret_cast<hvdg::NbrPair*>(d_mp + max_pairs);
+  std::vector<int64_t> nscr_off(nf), escr_off(nf), pix_off(max_pairs);
+  std::vector<hvdg::MeField> mf(nf);
+  for (int j = 0; j < nf; ++j) {
+    nscr_off[j] = (int64_t)j * h * std::max(1, w - 8);
+    escr_off[j] = (int64_t)j * env_samples;
+    mf[j].h = h;
+    mf[j].w = w;
+    mf[j].pitch = pitch;
+    mf[j].dpitch = dpitch;
+    mf[j].y_off = b.fp[j].px_off;
+    mf[j].t_off = b.fp[j].px_off;
+    mf[j].b_off = b.fp[j].px_off;
+    mf[j].d_off = (int64_t)j * dplane;
+  }
+  for (int p = 0; p < max_pairs; ++p) pix_off[p] = (int64_t)p * plane;
+  e = cudaMemcpyAsync(d_nscr_off, nscr_off.data(), sizeof(int64_t) * nf, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_pix_off, pix_off.data(), sizeof(int64_t) * max_pairs, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_mf, mf.data(), sizeof(hvdg::MeField) * nf, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D window tables");
+
+  // ---- noise self-calibration (sequence.cpp:437-449) ----
+  hvdg::launch_noise(at<FieldDesc>(ctx, L.o_fields), nf, at<float>(ctx, L.o_S),
+                     at<float>(ctx, X(x_nscr)), d_nscr_off, d_sigma, s);
+  std::vector<float> sig(nf);
+  e = cudaMemcpyAsync(sig.data(), d_sigma, sizeof(float) * nf, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "noise estimate");
+  const float sigma = median_mean(sig);
+  if (cfg.temporal_eps <= 0.0f) cfg.temporal_eps = std::min(std::max(7.0f * sigma, 4.0f), 20.0f);
+  if (cfg.nr_eps <= 0.0f) cfg.nr_eps = std::min(std::max(3.0f * sigma, 3.0f), 12.0f);
+  float amb = 0.0f;
+  const int amb_stride = pal ? 4 : 2;
+  if (cfg.temporal_strength == 0.0f && cfg.cg_iterations > 0 && nf > amb_stride) {
+    std::vector<std::vector<float>> Sh(nf, std::vector<float>((size_t)h * w));
+    std::vector<std::vector<float4>> Lh(nf, std::vector<float4>(h));
+    for (int j = 0; j < nf; ++j) {
+      e = cudaMemcpy2DAsync(Sh[j].data(), sizeof(float) * w, at<float>(ctx, L.o_S) + b.fp[j].px_off,
+                            sizeof(float) * pitch, sizeof(float) * w, h, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(Lh[j].data(), at<float4>(ctx, L.o_lineph) + b.fp[j].line_off,
+                            sizeof(float4) * h, cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "D2H window state");
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "D2H window state");
+    cfg.temporal_strength = adaptive_strength(Sh, Lh, b.gtabs[0]->col_phasor, h, w, amb_stride,
+                                              cfg.nr_eps, &amb);
+  }
+  if (cfg.temporal_strength < 0.0f) cfg.temporal_strength = 0.0f;
+  if (diag) {
+    diag->sigma_ire = sigma;
+    diag->ambiguity_ire = amb;
+    diag->resolved_strength = std::max(0.0f, cfg.temporal_strength);
+    diag->temporal_eps = cfg.temporal_eps;
+    diag->nr_eps = cfg.nr_eps;
+  }
+  const bool has_temporal = cfg.temporal_strength > 0.0f && cfg.cg_iterations > 0;
+  const int n_passes = has_temporal ? std::max(1, cfg.passes) : 1;
+  if (has_temporal) {
+    const bool anchor = n_passes > 1 && cfg.nr_anchor > 0.0f && nf > 1;
+    bool gate_any = false;
+    for (int pass = 0; pass < n_passes; ++pass)
+      if (cfg.coherence_gate > 0.0f && !(cfg.fast && pass == 0)) gate_any = true;
+    if (cfg.trajectory_fit || cfg.psi_init || anchor || gate_any) {
+      ctx->last_error =
+          "temporal window decode needs trajectory_fit=0, psi_init=0, no anchored pass "
+          "(passes=1 or nr_anchor=0) and no coherence gate in this build";
+      return HVDG_ERR_UNSUPPORTED;
+    }
+  }
+  // ---- colours (sequence.cpp:1052-1099) ----
+  std::vector<std::vector<int>> colors;
+  if ((cfg.fast || !has_temporal) && cfg.parallel_across_fields) {
+    int max_off = 0;
+    for (int o : offs) max_off = std::max(max_off, std::abs(o));
+    const int reach = std::max(max_off, cfg.nr_anchor > 0.0f ? cfg.nr_radius : 0);
+    const int stride = has_temporal ? reach + 1 : 1;
+    for (int c = 0; c < stride; ++c) {
+      std::vector<int> col;
+      for (int j = c; j < nf; j += stride) col.push_back(j);
+      if (!col.empty()) colors.push_back(col);
+    }
+  } else if (!has_temporal) {
+    std::vector<int> all;
+    for (int j = 0; j < nf; ++j) all.push_back(j);
+    colors.push_back(all);
+  } else {
+    for (int j = 0; j < nf; ++j) colors.push_back({j});
+  }
+  // units regrouped by colour (each field's units stay contiguous)
+  std::vector<Unit> cunits;
+  std::vector<int> cbegin, ccount, cphases;
+  for (const auto& col : colors) {
+    cbegin.push_back((int)cunits.size());
+    int ph = 0;
+    for (int j : col) {
+      FieldDesc& f = b.fields[j];
+      const int ub = (int)cunits.size();
+      for (int u = 0; u < f.unit_count; ++u) cunits.push_back(b.units[f.unit_begin + u]);
+      f.unit_begin = ub;
+      ph = std::max(ph, f.n_phases);
+    }
+    ccount.push_back((int)cunits.size() - cbegin.back());
+    cphases.push_back(ph);
+  }
+  // neighbour planes per field (slot per valid offset)
+  for (int j = 0; j < nf; ++j) {
+    FieldDesc& f = b.fields[j];
+    f.nu = has_temporal ? cfg.temporal_strength : 0.0f;
+    f.eps_t = cfg.temporal_eps;
+    f.nbr_off = (int64_t)j * nofs * plane;
+    f.plane_px = plane;
+    f.n_nbr = 0;
+    f.has_nbr = 0;
+  }
+  e = cudaMemcpyAsync(at<Unit>(ctx, L.o_units), cunits.data(), sizeof(Unit) * cunits.size(),
+                      cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D units");
+  hvdg::SolverArgs sa = solver_args(ctx, S);
+  sa.M = at<float4>(ctx, X(x_M));
+  sa.B = at<float2>(ctx, X(x_B));
+  sa.nbr = at<float4>(ctx, X(x_nbr));
+  hvdg::MeArgs ma;
+  ma.tile = tile;
+  ma.search = search;
+  ma.coarse_off = nct;
+  ma.tiles_off = nt;
+  hvdg::MeBuffers mb;
+  mb.luma = at<float>(ctx, L.o_Y);
+  mb.tmp = at<float>(ctx, X(x_tmp));
+  mb.blur = at<float>(ctx, X(x_blur));
+  mb.dec = at<float>(ctx, X(x_dec));
+  mb.cdy = at<float>(ctx, X(x_cdy));
+  mb.cdx = at<float>(ctx, X(x_cdx));
+  mb.mdy = at<float>(ctx, X(x_t[0]));
+  mb.mdx = at<float>(ctx, X(x_t[1]));
+  mb.sdy = at<float>(ctx, X(x_t[2]));
+  mb.sdx = at<float>(ctx, X(x_t[3]));
+  mb.best = at<float>(ctx, X(x_t[4]));
+  mb.dy = at<float>(ctx, X(x_t[5]));
+  mb.dx = at<float>(ctx, X(x_t[6]));
+  mb.conf = at<float>(ctx, X(x_t[7]));
+  hvdg::VecBuffers vb;
+  vb.dy = mb.dy;
+  vb.dx = mb.dx;
+  vb.conf = mb.conf;
+  vb.snap_dy = at<float>(ctx, X(x_t[8]));
+  vb.snap_dx = at<float>(ctx, X(x_t[9]));
+  vb.c2 = at<float>(ctx, X(x_t[10]));
+  vb.c2_snap = at<float>(ctx, X(x_t[11]));
+  vb.c2_snap2 = at<float>(ctx, X(x_t[12]));
+  vb.src_idx = at<int2>(ctx, X(x_src));
+  vb.pix_off = d_pix_off;
+  vb.conf_tmp = at<float>(ctx, X(x_ctmp));
+  vb.conf_px = at<float>(ctx, X(x_cpx));
+  hvdg::EnvBuffers eb;
+  eb.gmag = at<float>(ctx, X(x_env[0]));
+  eb.lapmag = at<float>(ctx, X(x_env[1]));
+  eb.vraw = at<float>(ctx, X(x_env[2]));
+  eb.traw = at<float>(ctx, X(x_env[3]));
+  eb.gate = at<float>(ctx, X(x_env[4]));
+  eb.scratch = at<float>(ctx, X(x_escr));
+  eb.scratch_off = d_escr_off;
+  eb.floor2 = d_floor2;
+  const float e2 = cfg.temporal_eps * cfg.temporal_eps;
+  const float floor_max = std::min(std::max(cfg.odd_gate_floor, 0.0f), 1.0f);
+  cudaEventRecord(ctx->ev[2], s);
+  for (int pass = 0; pass < n_passes; ++pass) {
+    for (size_t ci = 0; ci < colors.size(); ++ci) {
+      const std::vector<int>& col = colors[ci];
+      std::vector<hvdg::MePair> mp;
+      std::vector<hvdg::NbrPair> np;
+      std::vector<int> env_list;
+      std::vector<int64_t> env_off;
+      if (has_temporal) {
+        for (int j : col) {
+          int slot = 0;
+          bool any_odd = false;
+          for (int o : offs) {
+            const int k = j + o;
+            if (k < 0 || k >= nf) continue;
+            mp.push_back(hvdg::MePair{k, j});
+            np.push_back(hvdg::NbrPair{k, j, slot++, (o & 1) != 0 ? 1 : 0});
+            any_odd = any_odd || (o & 1) != 0;
+          }
+          b.fields[j].n_nbr = slot;
+          b.fields[j].has_nbr = slot > 0 ? 1 : 0;
+          if (!slot) b.fields[j].nu = 0.0f;
+          if (any_odd) {
+            env_list.push_back(j);
+            env_off.push_back(escr_off[j]);
+          }
+        }
+      }
+      e = cudaMemcpyAsync(at<FieldDesc>(ctx, L.o_fields), b.fields.data(), sizeof(FieldDesc) * nf,
+                          cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D fields");
+      const int npairs = (int)mp.size();
+      if (npairs > 0) {
+        e = cudaMemcpyAsync(d_mp, mp.data(), sizeof(hvdg::MePair) * npairs, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_np, np.data(), sizeof(hvdg::NbrPair) * npairs, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D pairs");
+        hvdg::launch_motion(d_mf, nf, h, w, d_mp, npairs, ma, mb, s);
+        vb.conf_bytes = sizeof(float) * plane * npairs;
+        hvdg::launch_vectors(d_mf, d_mp, npairs, h, w, ma, vb, cfg.fast != 0, s);
+        S.launches += 8;
+        if (!env_list.empty()) {
+          e = cudaMemcpyAsync(d_list, env_list.data(), sizeof(int) * env_list.size(),
+                              cudaMemcpyHostToDevice, s);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_escr_off, env_off.data(), sizeof(int64_t) * env_off.size(),
+                                cudaMemcpyHostToDevice, s);
+          if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D env list");
+          hvdg::launch_envelope(at<FieldDesc>(ctx, L.o_fields), d_list, (int)env_list.size(), h, w,
+                                at<float>(ctx, L.o_Y), at<float2>(ctx, L.o_X0), eb, e2, floor_max,
+                                s);
+          S.launches += 4;
+        }
+        hvdg::launch_nbr_assemble(at<FieldDesc>(ctx, L.o_fields), d_np, npairs, h, w,
+                                  at<float>(ctx, L.o_S), at<float4>(ctx, L.o_lineph),
+                                  at<float2>(ctx, L.o_colph), vb.src_idx, vb.conf_px, d_pix_off,
+                                  eb.gate, at<float4>(ctx, X(x_nbr)), s);
+        S.launches += 1;
+      }
+      // solver state reset for this colour, aniso at the current chi
+      cudaMemsetAsync(at<char>(ctx, L.o_ctl), 0, sizeof(FieldCtl) * nf, s);
+      cudaMemsetAsync(at<char>(ctx, L.o_arrive), 0, sizeof(int) * nf, s);
+      cudaMemsetAsync(at<char>(ctx, L.o_done), 0xff, sizeof(int) * nf, s);
+      cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
+      hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), nf, at<float2>(ctx, L.o_X0), s);
+      sa.unit_base = cbegin[ci];
+      sa.n_units = ccount[ci];
+      sa.n_phases = cphases[ci];
+      e = hvdg::launch_solver(sa, solver_grid(ctx, ccount[ci]), s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
+      S.launches += 2;
+      // the solved fields' luma / chi now replace their init state (Ys[j], chis[j])
+    }
+  }
+  cudaEventRecord(ctx->ev[3], s);
+  return stage_finish(ctx, S, out, opt, diag);
+}
+
 // DecodeFieldWindow (sequence.cpp:270-281, 423-1116) over one window of one
 // geometry. With the temporal terms off every field is independent (the
 // stride-1 sweep, sequence.cpp:1076-1084) and the window is one batch.
@@ -819,13 +1294,11 @@ hvdg_status decode_window_impl(hvdg_ctx* ctx, const hvdg_field_in* fields, int n
   const hvdg_geometry& g = *fields[0].geometry;
   const int amb_stride = uses_vswitch(g) ? 4 : 2;
   const bool scan = cfg->temporal_strength == 0.0f && cfg->cg_iterations > 0 && n > amb_stride;
-  if (scan || cfg->temporal_strength > 0.0f) {
-    ctx->last_error = "temporal (3-D) window decode is not available in this build";
-    return HVDG_ERR_UNSUPPORTED;
-  }
   cudaSetDevice(ctx->device);
   if (diag) std::memset(diag, 0, sizeof(*diag));
   RunOpts opt;
+  if (n > 1 && (scan || cfg->temporal_strength > 0.0f))
+    return decode_window_3d(ctx, fields, n, cfg, out, diag, opt);
   if (ctx->batched) return run_batch(ctx, fields, n, cfg, out, diag, opt);
   for (int i = 0; i < n; ++i) {
     const hvdg_status st = run_batch(ctx, fields + i, 1, cfg, out + i, diag, opt);

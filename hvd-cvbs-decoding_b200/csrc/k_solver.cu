@@ -807,7 +807,7 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(SolverArgs A) {
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= total) break;
     const int p = (int)(item / A.n_units);
-    const int ui = (int)(item % A.n_units);
+    const int ui = A.unit_base + (int)(item % A.n_units);
     const Unit u = A.units[ui];
     const FieldDesc f = A.fields[u.field];
     if (p >= f.n_phases) continue;

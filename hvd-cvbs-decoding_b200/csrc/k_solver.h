@@ -15,7 +15,8 @@ struct SolverArgs {
   const FieldDesc* fields;
   FieldCtl* ctl;
   const Unit* units;
-  int n_units;                  // units per phase (all fields)
+  int unit_base;                // this launch processes units[unit_base, unit_base + n_units)
+  int n_units;                  // units per phase (fields of this launch)
   int n_phases;                 // max phases over fields
   unsigned long long* queue;    // work counter (zeroed before launch)
   int* done_phase;              // per field, -1 before launch

@@ -878,3 +878,113 @@ def detect_field_parity(b1, b2, fp, g) -> int:
     if hi <= 1e-9 or (hi - lo) / hi < 0.02:
         return 0
     return 1 if ep < em else -1
+
+
+# --------------------------------------------------------------------------
+# Temporal (3-D) field window (engine/sequence.cpp:423-1116), the subset with
+# no anchor pass, no coherence gate, no trajectory fit, no PSI init.
+# --------------------------------------------------------------------------
+
+def _smooth_rows(src):
+    """smooth_rows (sequence.cpp:860-889): sqrt of the mean over [x-2, x+2]
+    clipped to the row."""
+    h, w = src.shape
+    c = np.zeros((h, w + 1))
+    c[:, 1:] = np.cumsum(src, axis=1)
+    x = np.arange(w)
+    lo = np.maximum(x - 2, 0)
+    hi = np.minimum(x + 2, w - 1)
+    n = hi - lo + 1
+    return np.sqrt((c[:, hi + 1] - c[:, lo]) / n)
+
+
+def envelope_gate(Y, chi, eps_t, odd_gate_floor):
+    """Odd-offset half-line envelope gate (sequence.cpp:797-932, 1000-1026):
+    returns max(floor_i, e2 / (e2 + b^2)) per pixel."""
+    h, w = Y.shape
+    ym = np.maximum(np.arange(h) - 1, 0)
+    yp = np.minimum(np.arange(h) + 1, h - 1)
+    dyu = Y - Y[ym]
+    dyd = Y[yp] - Y
+    dcu = np.abs(chi - chi[ym])
+    dcd = np.abs(chi[yp] - chi)
+    gmag = np.maximum(dyu ** 2 + dcu ** 2, dyd ** 2 + dcd ** 2)
+    ly = Y - 0.5 * (Y[ym] + Y[yp])
+    lc = np.abs(chi - 0.5 * (chi[ym] + chi[yp]))
+    lapmag = ly ** 2 + lc ** 2
+    vgrad = _smooth_rows(gmag)
+    med = mean_median(vgrad.ravel()[::7])
+    vgrad = np.sqrt(np.maximum(0.0, vgrad ** 2 - 2.25 * med * med))
+    traw = _smooth_rows(lapmag)
+    t = np.where(vgrad > 1e-6, np.clip(traw / np.where(vgrad > 1e-6, vgrad, 1.0), 0.0, 1.0), 0.0)
+    lapsm = 1.0 - t * t
+    e2 = eps_t * eps_t
+    floor_i = float(np.clip(odd_gate_floor, 0.0, 1.0)) * lapsm
+    return np.maximum(floor_i, e2 / (e2 + vgrad ** 2))
+
+
+def temporal_offsets(cfg, pal):
+    """sequence.cpp:451-468."""
+    if cfg.extended_temporal:
+        if pal:
+            return [-4, -3, -2, -1, 1, 2, 3, 4] if cfg.bidirectional else [-4, -3, -2, -1]
+        return [-3, -2, -1, 1, 2, 3] if cfg.bidirectional else [-3, -2, -1]
+    return [-2, -1, 1, 2] if cfg.bidirectional else [-2, -1]
+
+
+def decode_window_temporal(fields_ire, parities, g, cfg, strength):
+    """DecodeFieldWindowWithInits with a fixed temporal strength > 0, one
+    pass: per field (in the reference's sweep order) EstimateMotion on the
+    current luma state, integer warps of the neighbours' composite and
+    carrier, confidence upsample, odd-offset envelope gate, VariationalRefine
+    with neighbour terms; output-fidelity luma."""
+    import copy
+    pal = uses_vswitch(g)
+    obs = [prepare_field(f, g, cfg, p) for f, p in zip(fields_ire, parities)]
+    nf = len(obs)
+    sig = [estimate_noise_ire(o.s) for o in obs]
+    sigma = mean_median(sig)
+    eps_t = cfg.temporal_eps if cfg.temporal_eps > 0 else float(np.clip(7 * sigma, 4, 20))
+    c2 = copy.copy(cfg)
+    c2.temporal_strength = strength
+    c2.temporal_eps = eps_t
+    Ys, chis = [], []
+    for o in obs:
+        y0, chi0 = holographic_init(o.s, o.carrier, g)
+        Ys.append(y0)
+        chis.append(chi0)
+    offs = temporal_offsets(cfg, pal)
+    max_off = max(abs(o) for o in offs)
+    reach = max(max_off, cfg.nr_radius if cfg.nr_anchor > 0 else 0)
+    if cfg.fast and cfg.parallel_across_fields:
+        order = [list(range(c, nf, reach + 1)) for c in range(reach + 1)]
+    else:
+        order = [[j] for j in range(nf)]
+    h, w = obs[0].s.shape
+    for colour in order:
+        state = [(Y.copy(), c.copy()) for Y, c in zip(Ys, chis)]
+        for j in colour:
+            Yj, chij = state[j]
+            nbrs = []
+            gate = None
+            for o in offs:
+                k = j + o
+                if k < 0 or k >= nf:
+                    continue
+                dy, dx, conf = estimate_motion(state[k][0], Yj, cfg.mc_tile, cfg.mc_search)
+                vdy, vdx = vectors_per_pixel(dy, dx, cfg.mc_tile, h, w)
+                comp = warp_by_tiles(obs[k].s, vdy, vdx)
+                car = warp_by_tiles(obs[k].carrier, vdy, vdx)
+                cf = upsample_confidence(conf, cfg.mc_tile, h, w, fast=bool(cfg.fast))
+                if o & 1:
+                    if gate is None:
+                        gate = envelope_gate(Yj, chij, eps_t, cfg.odd_gate_floor)
+                    cf = cf * gate
+                nbrs.append(Neighbor(comp, car, cf))
+            y, chi = variational_refine(obs[j].s, obs[j].carrier, chij, c2, is_pal=pal,
+                                        neighbors=nbrs)
+            Ys[j], chis[j] = y, chi
+    out = []
+    for j in range(nf):
+        out.append((obs[j].s - np.real(chis[j] * obs[j].carrier), chis[j]))
+    return out
