@@ -543,6 +543,7 @@ struct RunOpts {
   const float* theta_in = nullptr;   // active-line theta
   const int8_t* vswitch_in = nullptr;
   const float* chi0_in = nullptr;    // dense h x w x 2
+  float* amp_out = nullptr;          // optional per-field BurstAmplitudeIre (host)
 };
 
 // A batch uploaded to the arena: layout, table offsets, launch count.
@@ -652,6 +653,13 @@ hvdg_status stage_prepare(hvdg_ctx* ctx, Staged& S, const RunOpts& opt) {
   if (opt.do_lockin) {
     hvdg::launch_burst_lockin(at<hvdg::PrepDesc>(ctx, L.o_prep), n, lo, s);
     S.launches += 1;
+    if (opt.amp_out) {
+      hvdg::launch_burst_amplitude(at<hvdg::PrepDesc>(ctx, L.o_prep), n, at<float>(ctx, L.o_amp), s);
+      e = cudaMemcpyAsync(opt.amp_out, at<float>(ctx, L.o_amp), sizeof(float) * n,
+                          cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy burst amplitudes");
+      S.launches += 1;
+    }
   } else {
     // caller-supplied active-line phases (one field): exp(i theta) in FP64
     const FieldPlan& p = b.fp[0];
@@ -1290,21 +1298,108 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
 // geometry. With the temporal terms off every field is independent (the
 // stride-1 sweep, sequence.cpp:1076-1084) and the window is one batch.
 hvdg_status decode_window_impl(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
-                               const hvdg_config* cfg, hvdg_field_out* out, hvdg_diag* diag) {
+                               const hvdg_config* cfg, hvdg_field_out* out, hvdg_diag* diag,
+                               const RunOpts& opt = RunOpts()) {
   const hvdg_geometry& g = *fields[0].geometry;
   const int amb_stride = uses_vswitch(g) ? 4 : 2;
   const bool scan = cfg->temporal_strength == 0.0f && cfg->cg_iterations > 0 && n > amb_stride;
   cudaSetDevice(ctx->device);
   if (diag) std::memset(diag, 0, sizeof(*diag));
-  RunOpts opt;
   if (n > 1 && (scan || cfg->temporal_strength > 0.0f))
     return decode_window_3d(ctx, fields, n, cfg, out, diag, opt);
-  if (ctx->batched) return run_batch(ctx, fields, n, cfg, out, diag, opt);
+  if (ctx->batched || opt.amp_out) return run_batch(ctx, fields, n, cfg, out, diag, opt);
   for (int i = 0; i < n; ++i) {
     const hvdg_status st = run_batch(ctx, fields + i, 1, cfg, out + i, diag, opt);
     if (st != HVDG_OK) return st;
   }
   return HVDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Frame bridge (hvd-core/src/frame_bridge.cpp): de-weave, field-order vote,
+// weave + 10-bit requantisation, on the host around the device window decode.
+// ---------------------------------------------------------------------------
+int64_t frame_line_offset(const hvdg_frame_params& fp, int line) {
+  // FrameLineOffset (frame_bridge.h:106-112)
+  int64_t off = (int64_t)line * fp.frame_width;
+  for (int i = 0; i < fp.extra_sample_line_count && i < HVDG_MAX_EXTRA_SAMPLE_LINES; ++i)
+    if (fp.extra_sample_lines[i] < line) ++off;
+  return off;
+}
+
+hvdg_geometry geometry_from_params(const hvdg_frame_params& fp) {
+  // FieldGeometryFromParams (frame_bridge.cpp:43-59)
+  hvdg_geometry g;
+  std::memset(&g, 0, sizeof(g));
+  g.field_width = fp.frame_width;
+  g.field_height = fp.field1_lines;
+  g.active_video_start = fp.active_video_start;
+  g.active_video_end = fp.active_video_end;
+  g.colour_burst_start = fp.colour_burst_start;
+  g.colour_burst_end = fp.colour_burst_end;
+  g.first_active_field_line = fp.first_active_frame_line / 2;
+  g.last_active_field_line = fp.last_active_frame_line != 0 ? fp.last_active_frame_line / 2 : 0;
+  g.sample_rate = fp.sample_rate;
+  g.subcarrier_hz = fp.subcarrier_hz;
+  g.standard = fp.standard;
+  return g;
+}
+
+// SplitFrameFields (frame_bridge.cpp:61-99): block 1 / block 2 in IRE.
+void split_frame_fields(const int16_t* frame, const hvdg_frame_params& fp, float* top,
+                        float* bottom) {
+  const int fw = fp.frame_width, fh = fp.frame_height, f1 = fp.field1_lines, f2 = fh - f1;
+  const float cpi = (fp.white_level - fp.blanking_level) / 100.0f;
+  for (int y = 0; y < f1; ++y) {
+    const int64_t ot = frame_line_offset(fp, y);
+    const int64_t ob = frame_line_offset(fp, f1 + y);
+    for (int x = 0; x < fw; ++x) {
+      const float st = (y < f1) ? (float)frame[ot + x] : fp.blanking_level;
+      const float sb = (y < f2) ? (float)frame[ob + x] : fp.blanking_level;
+      top[(size_t)y * fw + x] = (st - fp.blanking_level) / cpi;
+      bottom[(size_t)y * fw + x] = (sb - fp.blanking_level) / cpi;
+    }
+  }
+}
+
+// DetectFieldParity (frame_bridge.cpp:102-149).
+int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_params& fp,
+                        const hvdg_geometry& g) {
+  const int fw = fp.frame_width;
+  const int fal = g.first_active_field_line, lal = last_active_line(g);
+  const int a0 = fp.active_video_start, a1 = fp.active_video_end;
+  const int lines = lal - fal, width = a1 - a0;
+  if (lines < 8 || width < 32) return 0;
+  const int ystep = std::max(1, lines / 120);
+  double ep = 0.0, em = 0.0;
+  long n = 0;
+  for (int r = fal + 1; r + 1 < lal; r += ystep) {
+    for (int x = a0; x + 4 <= a1; x += 16) {
+      auto lp = [&](const float* p, int row) {
+        const float* q = p + (size_t)row * fw + x;
+        return 0.25f * (q[0] + q[1] + q[2] + q[3]);
+      };
+      const float b = lp(b2, r), ac = lp(b1, r), au = lp(b1, r - 1), ad = lp(b1, r + 1);
+      ep += std::fabs(b - 0.5f * (ac + ad));
+      em += std::fabs(b - 0.5f * (ac + au));
+      ++n;
+    }
+  }
+  if (n == 0) return 0;
+  ep /= (double)n;
+  em /= (double)n;
+  const double lo = std::min(ep, em), hi = std::max(ep, em);
+  if (hi <= 1e-9 || (hi - lo) / hi < 0.02) return 0;
+  return ep < em ? +1 : -1;
+}
+
+int16_t clamp_u10(float v) {
+  const long r = std::lround(v);
+  return (int16_t)std::min<long>(std::max<long>(r, 0), 1023);
+}
+int16_t clamp_s10(float v) {
+  const long r = std::lround(v);
+  return (int16_t)std::min<long>(std::max<long>(r, -1023), 1023);
 }
 
 // Lock-in / burst amplitude of one IRE field (kernel-level entry points).
@@ -1662,9 +1757,136 @@ hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* cons
                                               const hvdg_frame_params* fp, const hvdg_config* cfg,
                                               hvdg_yc_frame* out, hvdg_diag* diag) {
   if (!ctx || !fp || !cfg) return HVDG_ERR_BAD_ARGUMENT;
-  (void)frames; (void)n_frames; (void)core_begin; (void)core_end; (void)out; (void)diag;
-  ctx->last_error = "frame bridge is not available in this build";
-  return HVDG_ERR_UNSUPPORTED;
+  // the reference returns an empty vector for these windows (frame_bridge.cpp:728-731)
+  if (n_frames <= 0 || !frames || core_begin < 0 || core_end > n_frames || core_begin >= core_end)
+    return HVDG_ERR_BAD_ARGUMENT;
+  if (!out) return HVDG_ERR_BAD_ARGUMENT;
+  for (int t = 0; t < n_frames; ++t)
+    if (!frames[t]) return HVDG_ERR_BAD_ARGUMENT;
+  for (int t = 0; t < core_end - core_begin; ++t)
+    if (!out[t].luma || !out[t].chroma || !out[t].u_plane || !out[t].v_plane)
+      return HVDG_ERR_BAD_ARGUMENT;
+  const hvdg_frame_params& P = *fp;
+  if (P.frame_width < 1 || P.frame_height < 2 || P.field1_lines < 1 ||
+      P.field1_lines > P.frame_height || !(P.white_level != P.blanking_level))
+    return HVDG_ERR_BAD_GEOMETRY;
+  const hvdg_geometry g = geometry_from_params(P);
+  hvdg_status st = check_geometry(&g);
+  if (st != HVDG_OK) return st;
+  const int fw = P.frame_width, fh = P.frame_height, f1 = P.field1_lines;
+  const float scale = (P.white_level - P.blanking_level) / 100.0f;
+  // ---- de-weave + field-order vote ----
+  const int nfield = 2 * n_frames;
+  std::vector<std::vector<float>> ire(nfield, std::vector<float>((size_t)f1 * fw));
+  for (int t = 0; t < n_frames; ++t)
+    split_frame_fields(frames[t], P, ire[2 * t].data(), ire[2 * t + 1].data());
+  bool f1_bottom = cfg->field_order == 2;
+  if (cfg->field_order == 0) {
+    int vote = 0;
+    for (int t = 0; t < n_frames; ++t)
+      vote += detect_field_parity(ire[2 * t].data(), ire[2 * t + 1].data(), P, g);
+    f1_bottom = vote < 0;
+  }
+  const int p_first = f1_bottom ? 1 : 0;
+  // ---- window decode (burst amplitudes measured on the same upload) ----
+  const int h = last_active_line(g) - g.first_active_field_line;
+  const int w = g.active_video_end - g.active_video_start;
+  std::vector<hvdg_field_in> fi(nfield);
+  std::vector<hvdg_field_out> fo(nfield);
+  std::vector<std::vector<float>> Yd(nfield, std::vector<float>((size_t)h * w));
+  std::vector<std::vector<float>> Cd(nfield, std::vector<float>((size_t)h * w * 2));
+  std::vector<std::vector<float>> th(nfield, std::vector<float>(f1));
+  std::vector<std::vector<int8_t>> vs(nfield, std::vector<int8_t>(f1));
+  for (int j = 0; j < nfield; ++j) {
+    std::memset(&fi[j], 0, sizeof(fi[j]));
+    fi[j].samples = ire[j].data();
+    fi[j].sample_type = HVDG_SAMPLES_F32_IRE;
+    fi[j].parity = (j % 2 == 0) ? p_first : 1 - p_first;
+    fi[j].geometry = &g;
+    fi[j].irls_outer = 0;
+    fi[j].cg_iterations = -1;
+    fo[j].luma = Yd[j].data();
+    fo[j].chroma = Cd[j].data();
+    fo[j].theta = th[j].data();
+    fo[j].vswitch = vs[j].data();
+  }
+  std::vector<float> amps(nfield, 0.0f);
+  RunOpts opt;
+  opt.amp_out = amps.data();
+  hvdg_diag local;
+  hvdg_diag* dg = diag ? diag : &local;
+  st = decode_window_impl(ctx, fi.data(), nfield, cfg, fo.data(), dg, opt);
+  if (st != HVDG_OK) return st;
+  float acc_gain = 1.0f;
+  if (cfg->acc) {
+    std::vector<float> a = amps;
+    const size_t k = a.size() / 2;
+    std::nth_element(a.begin(), a.begin() + k, a.end());
+    acc_gain = std::min(std::max(nominal_burst(g) / std::max(a[k], 1.0f), 0.5f), 2.0f);
+  }
+  const float gain = cfg->chroma_gain * acc_gain;
+  dg->acc_gain = acc_gain;
+  // ---- weave core frames by true parity + 10-bit requantisation ----
+  const int fal = g.first_active_field_line, a0 = P.active_video_start;
+  const double w0 = phase_per_sample(g);
+  const bool vsw = uses_vswitch(g);
+  std::vector<float2> colp(w);
+  for (int x = 0; x < w; ++x) {
+    const int smp = g.active_video_start + x;
+    if (g.subcarrier_hz <= 0.0) {
+      static const float2 q[4] = {{1.f, 0.f}, {0.f, 1.f}, {-1.f, 0.f}, {0.f, -1.f}};
+      colp[x] = q[smp & 3];
+    } else {
+      colp[x] = make_float2((float)std::cos(w0 * smp), (float)std::sin(w0 * smp));
+    }
+  }
+  for (int t = core_begin; t < core_end; ++t) {
+    hvdg_yc_frame& yc = out[t - core_begin];
+    const size_t sz = (size_t)fw * fh;
+    std::fill(yc.chroma, yc.chroma + sz, (int16_t)0);
+    std::fill(yc.u_plane, yc.u_plane + sz, 0.0);
+    std::fill(yc.v_plane, yc.v_plane + sz, 0.0);
+    for (int line = 0; line < fh; ++line) {
+      const int64_t src = frame_line_offset(P, line);
+      std::copy(frames[t] + src, frames[t] + src + fw, yc.luma + (size_t)line * fw);
+    }
+    const int j0 = 2 * t, j1 = j0 + 1;
+    int p0 = fi[j0].parity, p1 = fi[j1].parity;
+    if (p0 == p1) {
+      p0 = 0;
+      p1 = 1;
+    }
+    for (int r = 0; r < 2 * h; ++r) {
+      const bool row_even = (r % 2) == 0;
+      const bool use_first = (r % 2) == p0;
+      const int j = use_first ? j0 : j1;
+      const int fl = r / 2;
+      const int flat_line = row_even ? (fal + fl) : (f1 + fal + fl);
+      if (flat_line < 0 || flat_line >= fh) continue;
+      const double thv = (double)th[j][fal + fl];
+      const float2 Lc = make_float2((float)std::cos(thv), (float)std::sin(thv));
+      const bool sw = vsw && vs[j][fal + fl] < 0;
+      for (int c = 0; c < w; ++c) {
+        const int flat_col = a0 + c;
+        if (flat_col < 0 || flat_col >= fw) continue;
+        const size_t idx = (size_t)flat_line * fw + flat_col;
+        const float y_ire = Yd[j][(size_t)fl * w + c];
+        float cr = Cd[j][2 * ((size_t)fl * w + c)], ci = Cd[j][2 * ((size_t)fl * w + c) + 1];
+        if (cfg->monochrome) {
+          cr = 0.0f;
+          ci = 0.0f;
+        }
+        float car_r = Lc.x * colp[c].x - Lc.y * colp[c].y;
+        const float car_i = Lc.x * colp[c].y + Lc.y * colp[c].x;
+        if (sw) car_r = -car_r;
+        yc.luma[idx] = clamp_u10(P.blanking_level + y_ire * scale);
+        yc.chroma[idx] = clamp_s10((cr * car_r - ci * car_i) * scale);
+        yc.v_plane[idx] = gain * (double)cr * scale;
+        yc.u_plane[idx] = gain * (double)(-ci) * scale;
+      }
+    }
+  }
+  return HVDG_OK;
 }
 
 hvdg_status hvdg_holographic_init(hvdg_ctx* ctx, const float* s, const float* theta_active,

@@ -232,3 +232,63 @@ def default_config(**kw) -> Config:
 
 def default_geometry(standard: int) -> Geometry:
     return _cabi.default_geometry(standard)
+
+
+def frame_params(standard: int, blanking=240.0, white=800.0, black=None) -> _cabi.FrameParams:
+    """FrameParams (frame_bridge.h:40-101) for the 4fsc frame layouts. PAL
+    frames carry 4 extra samples (709 379 per frame, EBU Tech. 3280-E): two on
+    frame line 312 and two on 624; FrameLineOffset counts one sample per
+    listed entry, so each of those lines is listed twice."""
+    fp = _cabi.FrameParams()
+    g = _cabi.default_geometry(standard)
+    fp.standard = standard
+    fp.frame_width = g.field_width
+    if standard == _cabi.STD_PAL:
+        fp.frame_height, fp.field1_lines = 625, 313
+        for i, ln in enumerate((312, 312, 624, 624)):
+            fp.extra_sample_lines[i] = ln
+        fp.extra_sample_line_count = 4
+    else:
+        fp.frame_height, fp.field1_lines = 525, 263
+    fp.active_video_start, fp.active_video_end = g.active_video_start, g.active_video_end
+    fp.colour_burst_start, fp.colour_burst_end = g.colour_burst_start, g.colour_burst_end
+    fp.first_active_frame_line = 2 * g.first_active_field_line
+    fp.last_active_frame_line = 0
+    fp.blanking_level = blanking
+    fp.white_level = white
+    fp.black_level = blanking if black is None else black
+    fp.chroma_dc = 0.0
+    fp.sample_rate = g.sample_rate
+    fp.subcarrier_hz = 0.0
+    return fp
+
+
+def frame_buffer_size(fp: _cabi.FrameParams) -> int:
+    return fp.frame_width * fp.frame_height + fp.extra_sample_line_count
+
+
+def _decode_frames(self, frames, core_begin, core_end, fp, cfg):
+    """hvd::DecodeFrameSequenceWindow: frames are flat int16 field-sequential
+    buffers; returns one dict(luma, chroma, u, v) per core frame."""
+    n = len(frames)
+    fr = [np.ascontiguousarray(f, dtype=np.int16) for f in frames]
+    ptrs = (C.c_void_p * max(n, 1))(*[f.ctypes.data for f in fr])
+    m = max(core_end - core_begin, 0)
+    sz = fp.frame_width * fp.frame_height
+    res = [dict(luma=np.zeros(sz, np.int16), chroma=np.zeros(sz, np.int16),
+                u=np.zeros(sz, np.float64), v=np.zeros(sz, np.float64)) for _ in range(m)]
+    outs = (_cabi.YcFrame * max(m, 1))()
+    for t, r in enumerate(res):
+        outs[t].luma = r["luma"].ctypes.data
+        outs[t].chroma = r["chroma"].ctypes.data
+        outs[t].u_plane = r["u"].ctypes.data
+        outs[t].v_plane = r["v"].ctypes.data
+    self.last_diag = Diag()
+    st = self.lib.hvdg_decode_frame_sequence_window(self._h, ptrs, n, core_begin, core_end,
+                                                    C.byref(fp), C.byref(cfg), outs,
+                                                    C.byref(self.last_diag))
+    self._check(st, "hvdg_decode_frame_sequence_window")
+    return res
+
+
+Context.decode_frame_sequence_window = _decode_frames

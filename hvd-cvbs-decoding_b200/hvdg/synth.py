@@ -261,3 +261,32 @@ def mixed_batch(seed: int, n_ntsc: int = 40, n_pal: int = 24,
         f.cg_iterations = outer * cg_per_outer
         out.append(f)
     return out
+
+
+def make_frames(seed: int, standard: int, n_frames: int, noise_sigma: float = 0.5,
+                moving: bool = False, blanking: float = 240.0, white: float = 800.0):
+    """Field-sequential 10-bit int16 frame buffers (the plugin's CVBS frame
+    layout, frame_bridge.h:12-23): field 1 lines, then field 2 lines, with the
+    PAL extra samples on frame lines 312 and 624. Returns (frames, fields)."""
+    fields = make_sequence(seed, standard, 2 * n_frames, noise_sigma, moving)
+    g = _cabi.default_geometry(standard)
+    fw = g.field_width
+    if standard == _cabi.STD_PAL:
+        fh, f1, extra = 625, 313, (312, 624)
+    else:
+        fh, f1, extra = 525, 263, ()
+    f2 = fh - f1
+    cpi = (white - blanking) / 100.0
+    frames = []
+    for t in range(n_frames):
+        top = to_ire(fields[2 * t].samples)
+        bot = to_ire(fields[2 * t + 1].samples)
+        lines = [top[y] for y in range(f1)] + [bot[y] for y in range(f2)]
+        buf = []
+        for i, ln in enumerate(lines):
+            codes = np.clip(np.rint(blanking + ln * cpi), -32768, 32767).astype(np.int16)
+            buf.append(codes)
+            if i in extra:
+                buf.append(codes[-2:])  # the two extra samples of this line
+        frames.append(np.concatenate(buf))
+    return frames, fields
