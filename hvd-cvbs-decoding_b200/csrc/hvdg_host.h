@@ -12,11 +12,12 @@ struct hvdg_ctx;
 
 namespace hvdg {
 
-// Grow-only device arena (one allocation per context; zeroed when grown).
+// Grow-only device arena (one allocation per context; zeroed when grown,
+// in order on the context stream `st`).
 struct DeviceArena {
   void* base = nullptr;
   size_t capacity = 0;
-  hvdg_status reserve(size_t bytes);
+  hvdg_status reserve(size_t bytes, cudaStream_t st);
   ~DeviceArena();
 };
 

@@ -334,14 +334,23 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
   }
 }
 
+constexpr int kAnisoSmem = 2 * 24576 * (int)sizeof(float);
+
+void configure_init_kernels() {
+  cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       3 * kRowFft * (int)sizeof(float2));
+  cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kColGroup * 2 * kColFft * (int)sizeof(float2));
+  cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, kAnisoSmem);
+}
+
 void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
                  cudaStream_t st) {
   static bool configured = false;
   const int row_smem = 3 * kRowFft * sizeof(float2);
   const int col_smem = kColGroup * 2 * kColFft * sizeof(float2);
   if (!configured) {
-    cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem);
-    cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem);
+    configure_init_kernels();
     configured = true;
   }
   if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
@@ -353,7 +362,7 @@ void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStr
   static bool configured = false;
   const int smem = 2 * kAnisoMax * sizeof(float);
   if (!configured) {
-    cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    configure_init_kernels();
     configured = true;
   }
   if (n_fields > 0) k_aniso<<<n_fields, 1024, smem, st>>>(d_fields, chi0);

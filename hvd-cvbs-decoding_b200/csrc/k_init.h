@@ -31,6 +31,7 @@ struct InitArgs {
   const int* btile_first;      // field -> first blend tile
 };
 
+void configure_init_kernels();
 void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
                  cudaStream_t st);
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st);

@@ -345,11 +345,15 @@ __global__ void k_crop(const PrepDesc* __restrict__ descs, const int* __restrict
 
 constexpr size_t kLockinSmem = 10 * kMaxLines * sizeof(double) + 2 * kMaxLines;
 
+void configure_prep_kernels() {
+  cudaFuncSetAttribute(k_burst_lockin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kLockinSmem);
+}
+
 void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_burst_lockin, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kLockinSmem);
+    configure_prep_kernels();
     configured = true;
   }
   if (n > 0) k_burst_lockin<<<n, 256, kLockinSmem, st>>>(d_descs, out);

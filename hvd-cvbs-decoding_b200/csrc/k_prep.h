@@ -35,6 +35,7 @@ struct LockinOut {
   float4* line_phasor;   // optional, active lines: (cos, sin, sign, 0)
 };
 
+void configure_prep_kernels();
 void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStream_t st);
 void launch_burst_amplitude(const PrepDesc* d_descs, int n, float* d_amp, cudaStream_t st);
 void launch_crop(const PrepDesc* d_descs, const int* d_row_field, const int* d_row_first,
