@@ -52,12 +52,15 @@ WORKLOADS = {
     "mixed64": (N_NTSC, N_PAL, (4, 12), 50),
     # profiling case: same kernels, working set (~260 MB) above L2, short solve
     "small16": (16, 0, (2, 2), 10),
+    # profiling case that fills every SM: 32 NTSC fields (~0.6 GB), 2 x 20 CG
+    "prof32": (32, 0, (2, 2), 20),
 }
 
 
 WORKLOAD_DESC = {
     "mixed64": "mixed-64: 40 NTSC 910x263 + 24 PAL 1135x313 uint16, irls U{4..12} x 50 CG",
     "small16": "small-16 (profiling): 16 NTSC 910x263 uint16, irls 2 x 10 CG",
+    "prof32": "prof-32 (profiling): 32 NTSC 910x263 uint16, irls 2 x 20 CG",
 }
 
 

@@ -943,7 +943,10 @@ std::string batch_signature(const hvdg_field_in* in, int n, const hvdg_config* c
 hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
                             hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt) {
   std::string sig = batch_signature(in, n, cfg);
-  sig += "|b" + std::to_string(opt.band_rows) + "c" + std::to_string(opt.ctas_per_sm);
+  // the effective tiling (a per-call override, else the context setting)
+  const int band = opt.band_rows >= 0 ? opt.band_rows : ctx->band_rows;
+  const int ctas = opt.ctas_per_sm >= 0 ? opt.ctas_per_sm : ctx->ctas_per_sm;
+  sig += "|b" + std::to_string(band) + "c" + std::to_string(ctas);
   char buf[64];
   for (int i = 0; i < n; ++i) {
     std::snprintf(buf, sizeof(buf), "|%p,%p,%p,%p,%d,%d", in[i].samples, (void*)out[i].luma,

@@ -125,8 +125,8 @@ __device__ __forceinline__ void r_form(const SolverArgs& A, const FieldDesc& f, 
   }
 }
 
-__device__ void phase_reweight(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
-                               const FieldCtl& c) {
+__device__ __noinline__ void phase_reweight(const SolverArgs& A, const FieldDesc& f, Unit u,
+                                            int lane, FieldCtl c) {
   const Lanes l = make_lanes(A, f, u.x0, lane);
   const int64_t base = f.px_off;
   const float2* X = A.X[c.xsel] + base;
@@ -215,19 +215,16 @@ __device__ void phase_reweight(const SolverArgs& A, const FieldDesc& f, const Un
 }
 
 // ---------------------------------------------------------------------------
-// Stencil phases: G (gradient at chi, with S) and I (one fused CG sweep).
+// G phase: the gradient at chi (with S) -> G[0], and its squared norm.
 // ---------------------------------------------------------------------------
 struct SRow {
   float2 ca, cb;
-  float2 ua, ub, uh;   // operand (chi for G, d_k for I), halo
-  float ya, yb, yh;    // S - Re[u c] (G) or -Re[u c] (I)
-  float2 gka, gkb;     // I: g_k
-  float2 doa, dob;     // I: d_{k-1} (pending chi step)
+  float2 ua, ub, uh;   // chi, halo
+  float ya, yb, yh;    // S - Re[chi c]
 };
 
-template <bool MODE_I>
 __device__ __forceinline__ void s_form(const SolverArgs& A, const FieldDesc& f, const Lanes& l,
-                                       const FieldCtl& c, bool first, int y, SRow& r) {
+                                       const FieldCtl& c, int y, SRow& r) {
   const int64_t base = f.px_off;
   const int64_t o = (int64_t)y * f.pitch + l.xa;
   const float4 L = __ldg(A.line_phasor + f.line_off + y);
@@ -235,84 +232,38 @@ __device__ __forceinline__ void s_form(const SolverArgs& A, const FieldDesc& f, 
   r.ca = carrier(Lc, l.Pa, L.z);
   r.cb = carrier(Lc, l.Pb, L.z);
   const float2 z = make_float2(0.f, 0.f);
-  if (!MODE_I) {
-    const float2* X = A.X[c.xsel] + base;
-    float Sa, Sb;
-    ld_pair(X + o, r.ua, r.ub);
-    ld_pairf(A.S + base + o, Sa, Sb);
-    if (!l.va) r.ua = z;
-    if (!l.vb) r.ub = z;
-    r.ya = l.va ? Sa - re_mul(r.ua, r.ca) : 0.f;
-    r.yb = l.vb ? Sb - re_mul(r.ub, r.cb) : 0.f;
-    r.uh = z;
-    r.yh = 0.f;
-    if (l.hv) {
-      const int64_t oh = (int64_t)y * f.pitch + l.hx;
-      r.uh = __ldcg(X + oh);
-      r.yh = __ldcg(A.S + base + oh) - re_mul(r.uh, carrier(Lc, l.Ph, L.z));
-    }
-  } else {
-    const float2* G = A.G[c.sel] + base;
-    const float2* Q = A.Q[c.sel] + base;
-    const float2* D = A.D[c.sel] + base;
-    float2 ga, gb;
-    ld_pair(G + o, ga, gb);
-    if (first) {
-      r.gka = ga;
-      r.gkb = gb;
-      r.ua = make_float2(-ga.x, -ga.y);
-      r.ub = make_float2(-gb.x, -gb.y);
-      r.doa = z;
-      r.dob = z;
-    } else {
-      float2 qa, qb, da, db;
-      ld_pair(Q + o, qa, qb);
-      ld_pair(D + o, da, db);
-      r.gka = cadd(ga, cscale(qa, c.alpha));
-      r.gkb = cadd(gb, cscale(qb, c.alpha));
-      r.ua = cadd(make_float2(-r.gka.x, -r.gka.y), cscale(da, c.beta));
-      r.ub = cadd(make_float2(-r.gkb.x, -r.gkb.y), cscale(db, c.beta));
-      r.doa = da;
-      r.dob = db;
-    }
-    if (!l.va) { r.ua = z; r.gka = z; }
-    if (!l.vb) { r.ub = z; r.gkb = z; }
-    r.ya = -re_mul(r.ua, r.ca);
-    r.yb = -re_mul(r.ub, r.cb);
-    r.uh = z;
-    r.yh = 0.f;
-    if (l.hv) {
-      const int64_t oh = (int64_t)y * f.pitch + l.hx;
-      const float2 gh = __ldcg(G + oh);
-      float2 dh;
-      if (first) {
-        dh = make_float2(-gh.x, -gh.y);
-      } else {
-        const float2 gkh = cadd(gh, cscale(__ldcg(Q + oh), c.alpha));
-        dh = cadd(make_float2(-gkh.x, -gkh.y), cscale(__ldcg(D + oh), c.beta));
-      }
-      r.uh = dh;
-      r.yh = -re_mul(dh, carrier(Lc, l.Ph, L.z));
-    }
+  const float2* X = A.X[c.xsel] + base;
+  float Sa, Sb;
+  ld_pair(X + o, r.ua, r.ub);
+  ld_pairf(A.S + base + o, Sa, Sb);
+  if (!l.va) r.ua = z;
+  if (!l.vb) r.ub = z;
+  r.ya = l.va ? Sa - re_mul(r.ua, r.ca) : 0.f;
+  r.yb = l.vb ? Sb - re_mul(r.ub, r.cb) : 0.f;
+  r.uh = z;
+  r.yh = 0.f;
+  if (l.hv) {
+    const int64_t oh = (int64_t)y * f.pitch + l.hx;
+    r.uh = __ldcg(X + oh);
+    r.yh = __ldcg(A.S + base + oh) - re_mul(r.uh, carrier(Lc, l.Ph, L.z));
   }
 }
 
-template <bool MODE_I>
-__device__ void phase_stencil(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
-                              const FieldCtl& c, bool first, double* part) {
+__device__ __noinline__ double phase_gradient(const SolverArgs& A, const FieldDesc& f, Unit u,
+                                              int lane, FieldCtl c) {
   const Lanes l = make_lanes(A, f, u.x0, lane);
   const int64_t base = f.px_off;
   const float4* W = A.W + base;
   const float mu_h = f.mu_h, mu_v = f.mu_v;
   const float2 z = make_float2(0.f, 0.f);
-  double pH = 0.0, pgd = 0.0, pgq = 0.0, pqq = 0.0, pgg = 0.0;
+  double pgg = 0.0;
   SRow cur, nxt;
   float aypa = 0.f, aypb = 0.f;
   float2 bypa = z, bypb = z;
-  s_form<MODE_I>(A, f, l, c, first, u.y0, cur);
+  s_form(A, f, l, c, u.y0, cur);
   if (u.y0 > 0) {
     SRow prv;
-    s_form<MODE_I>(A, f, l, c, first, u.y0 - 1, prv);
+    s_form(A, f, l, c, u.y0 - 1, prv);
     const int64_t op = (int64_t)(u.y0 - 1) * f.pitch + l.xa;
     const float4 wpa = __ldcg(W + op), wpb = __ldcg(W + op + 1);
     aypa = wpa.y * (cur.ya - prv.ya);
@@ -322,7 +273,7 @@ __device__ void phase_stencil(const SolverArgs& A, const FieldDesc& f, const Uni
   }
   for (int y = u.y0; y < u.y1; ++y) {
     const bool hn = y + 1 < f.h;
-    if (hn) s_form<MODE_I>(A, f, l, c, first, y + 1, nxt);
+    if (hn) s_form(A, f, l, c, y + 1, nxt);
     const int64_t o = (int64_t)y * f.pitch + l.xa;
     const float4 wa = __ldcg(W + o), wb = __ldcg(W + o + 1);
     float4 wh = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -371,82 +322,53 @@ __device__ void phase_stencil(const SolverArgs& A, const FieldDesc& f, const Uni
     ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
     if (f.has_nbr) {
       const float4 Ma = __ldcg(A.M + base + o), Mb = __ldcg(A.M + base + o + 1);
-      // M u with u as the real 2-vector (Re, Im)
+      // M u with u as the real 2-vector (Re, Im), plus the constant b
       oa.x += Ma.x * cur.ua.x + Ma.y * cur.ua.y;
       oa.y += Ma.y * cur.ua.x + Ma.z * cur.ua.y;
       ob.x += Mb.x * cur.ub.x + Mb.y * cur.ub.y;
       ob.y += Mb.y * cur.ub.x + Mb.z * cur.ub.y;
-      if (!MODE_I) {
-        float2 ba, bb;
-        ld_pair(A.B + base + o, ba, bb);
-        oa = cadd(oa, ba);
-        ob = cadd(ob, bb);
-      }
-      if (MODE_I) {
-        pH += 0.5 * (double)(Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
-                             Ma.z * cur.ua.y * cur.ua.y) * l.va;
-        pH += 0.5 * (double)(Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
-                             Mb.z * cur.ub.y * cur.ub.y) * l.vb;
-      }
+      float2 ba, bb;
+      ld_pair(A.B + base + o, ba, bb);
+      oa = cadd(oa, ba);
+      ob = cadd(ob, bb);
     }
     if (!l.va) oa = z;
     if (!l.vb) ob = z;
-    if (!MODE_I) {
-      st_pair(A.G[0] + base + o, oa, ob, l.va, l.vb);
-      pgg += (double)cnorm(oa) + (double)cnorm(ob);
-    } else {
-      if (l.va)
-        pH += (double)wa.x * dxya * dxya + (double)wa.y * dyya * dyya +
-              (double)mu_h * wa.z * cnorm(dxua) + (double)mu_v * wa.w * cnorm(dyua);
-      if (l.vb)
-        pH += (double)wb.x * dxyb * dxyb + (double)wb.y * dyyb * dyyb +
-              (double)mu_h * wb.z * cnorm(dxub) + (double)mu_v * wb.w * cnorm(dyub);
-      pgd += (double)cur.gka.x * cur.ua.x + (double)cur.gka.y * cur.ua.y +
-             (double)cur.gkb.x * cur.ub.x + (double)cur.gkb.y * cur.ub.y;
-      pgq += (double)cur.gka.x * oa.x + (double)cur.gka.y * oa.y + (double)cur.gkb.x * ob.x +
-             (double)cur.gkb.y * ob.y;
-      pqq += (double)cnorm(oa) + (double)cnorm(ob);
-      pgg += (double)cnorm(cur.gka) + (double)cnorm(cur.gkb);
-      const int s2 = c.sel ^ 1;
-      st_pair(A.G[s2] + base + o, cur.gka, cur.gkb, l.va, l.vb);
-      st_pair(A.D[s2] + base + o, cur.ua, cur.ub, l.va, l.vb);
-      st_pair(A.Q[s2] + base + o, oa, ob, l.va, l.vb);
-      if (!first) {
-        float2* X = A.X[c.xsel] + base;
-        float2 xa, xb;
-        ld_pair(X + o, xa, xb);
-        xa = cadd(xa, cscale(cur.doa, c.alpha));
-        xb = cadd(xb, cscale(cur.dob, c.alpha));
-        st_pair(X + o, xa, xb, l.va, l.vb);
-      }
-    }
+    st_pair(A.G[0] + base + o, oa, ob, l.va, l.vb);
+    pgg += (double)cnorm(oa) + (double)cnorm(ob);
     aypa = aya;
     aypb = ayb;
     bypa = bya;
     bypb = byb;
     cur = nxt;
   }
-  part[0] = MODE_I ? pH : pgg;
-  part[1] = pgd;
-  part[2] = pgq;
-  part[3] = pqq;
-  part[4] = pgg;
+  return pgg;
 }
 
 // ---------------------------------------------------------------------------
 // I phase with TMA-staged rows. Each warp owns a ring of kNS row slots in
 // shared memory; lane 0 fills them with 1-D bulk copies (cp.async.bulk,
 // mbarrier-tracked) of the g / q / d row segments (strip + 2-pixel halo
-// each side), the chi row segment and the weight row segment (strip + left
-// halo), so up to kNS - 1 rows are in flight per warp without holding
-// registers. Rows of one unit: [max(y0 - 1, 0), min(y1, h - 1)].
+// each side), the chi row segment, the weight row segment (strip + left
+// halo) and the row's line phasor, so up to kNS - 1 rows are in flight per
+// warp without holding registers. Rows of one unit: [max(y0 - 1, 0),
+// min(y1, h - 1)].
+//
+// Register economy: between rows only the operands of the vertical
+// differences (d_k and its luma part -Re[d_k c]) and the vertical fluxes of
+// the row above are carried; everything else of the current row (g_k,
+// d_{k-1}, carriers, halo) is re-read from its slot. The inner products
+// are accumulated per lane in FP32 over the unit's rows and reduced across
+// the warp and the field in FP64 (one conversion per lane per unit).
 // ---------------------------------------------------------------------------
 constexpr int kSlotG = (kStrip + 4) * 8;        // 544 B: columns x0-2 .. x0+65
 constexpr int kSlotX = kStrip * 8;              // 512 B: columns x0 .. x0+63
 constexpr int kSlotW = (kStrip + 1) * 16;       // 1040 B: columns x0-1 .. x0+63
 constexpr int kOffQ = kSlotG, kOffD = 2 * kSlotG, kOffX = 3 * kSlotG, kOffW = 3 * kSlotG + kSlotX;
-constexpr int kSlotBytes = kOffW + kSlotW;      // 3184 B
+constexpr int kOffL = kOffW + kSlotW;           // 16 B: the row's line phasor
+constexpr int kSlotBytes = kOffL + 16;          // 3200 B
 constexpr int kWarpRingBytes = kNS * kSlotBytes + kNS * 8;
+static_assert(kSlotBytes % 16 == 0 && kOffL % 16 == 0, "bulk copies need 16-byte slots");
 
 struct Ring {
   char* slots;
@@ -468,7 +390,7 @@ __device__ __forceinline__ void ring_issue(Ring& r, int slot, const SolverArgs& 
   const int woff = (ws - (x0 - 1)) * 16;
   const bool qd = !first;
   const bool xx = need_x && !first;
-  const uint32_t total = gb + wb + (qd ? 2 * gb : 0u) + (xx ? (uint32_t)kSlotX : 0u);
+  const uint32_t total = gb + wb + 16u + (qd ? 2 * gb : 0u) + (xx ? (uint32_t)kSlotX : 0u);
   mbar_expect_tx(bar, total);
   bulk_g2s(dst + goff, A.G[c.sel] + row + gs, gb, bar);
   if (qd) {
@@ -477,6 +399,7 @@ __device__ __forceinline__ void ring_issue(Ring& r, int slot, const SolverArgs& 
   }
   if (xx) bulk_g2s(dst + kOffX, A.X[c.xsel] + row + x0, kSlotX, bar);
   bulk_g2s(dst + kOffW + woff, A.W + row + ws, wb, bar);
+  bulk_g2s(dst + kOffL, A.line_phasor + f.line_off + y, 16u, bar);
 }
 
 __device__ __forceinline__ bool ring_wait(Ring& r, int slot) {
@@ -485,55 +408,43 @@ __device__ __forceinline__ bool ring_wait(Ring& r, int slot) {
   return ok;
 }
 
-// Form g_k, d_k, dY for one row from a ring slot (I phase).
-__device__ __forceinline__ void ring_form(const char* slot, const SolverArgs& A,
-                                          const FieldDesc& f, const Lanes& l, const FieldCtl& c,
-                                          bool first, int lane, int y, SRow& r) {
-  const float4 L = __ldg(A.line_phasor + f.line_off + y);
-  const float2 Lc = make_float2(L.x, L.y);
-  r.ca = carrier(Lc, l.Pa, L.z);
-  r.cb = carrier(Lc, l.Pb, L.z);
-  const float2 z = make_float2(0.f, 0.f);
+// g_k = g + alpha q and d_{k-1} of this lane's two pixels, from a slot.
+__device__ __forceinline__ void slot_gd(const char* slot, const FieldCtl& c, bool first, int lane,
+                                        float2& gka, float2& gkb, float2& doa, float2& dob) {
   const float4 g4 = *reinterpret_cast<const float4*>(slot + 16 + 16 * lane);
-  const float2 ga = make_float2(g4.x, g4.y), gb = make_float2(g4.z, g4.w);
+  gka = make_float2(g4.x, g4.y);
+  gkb = make_float2(g4.z, g4.w);
   if (first) {
-    r.gka = ga;
-    r.gkb = gb;
-    r.ua = make_float2(-ga.x, -ga.y);
-    r.ub = make_float2(-gb.x, -gb.y);
-    r.doa = z;
-    r.dob = z;
+    doa = make_float2(0.f, 0.f);
+    dob = doa;
   } else {
     const float4 q4 = *reinterpret_cast<const float4*>(slot + kOffQ + 16 + 16 * lane);
     const float4 d4 = *reinterpret_cast<const float4*>(slot + kOffD + 16 + 16 * lane);
-    r.gka = cadd(ga, cscale(make_float2(q4.x, q4.y), c.alpha));
-    r.gkb = cadd(gb, cscale(make_float2(q4.z, q4.w), c.alpha));
-    r.doa = make_float2(d4.x, d4.y);
-    r.dob = make_float2(d4.z, d4.w);
-    r.ua = cadd(make_float2(-r.gka.x, -r.gka.y), cscale(r.doa, c.beta));
-    r.ub = cadd(make_float2(-r.gkb.x, -r.gkb.y), cscale(r.dob, c.beta));
+    gka = cadd(gka, cscale(make_float2(q4.x, q4.y), c.alpha));
+    gkb = cadd(gkb, cscale(make_float2(q4.z, q4.w), c.alpha));
+    doa = make_float2(d4.x, d4.y);
+    dob = make_float2(d4.z, d4.w);
   }
-  if (!l.va) { r.ua = z; r.gka = z; }
-  if (!l.vb) { r.ub = z; r.gkb = z; }
-  r.ya = -re_mul(r.ua, r.ca);
-  r.yb = -re_mul(r.ub, r.cb);
-  r.uh = z;
-  r.yh = 0.f;
-  if (l.hv) {
-    const int hl = lane == 0 ? 1 : kStrip + 2;  // local column of x0-1 / x0+64
-    const float2 gh = *reinterpret_cast<const float2*>(slot + 8 * hl);
-    float2 dh;
-    if (first) {
-      dh = make_float2(-gh.x, -gh.y);
-    } else {
-      const float2 qh = *reinterpret_cast<const float2*>(slot + kOffQ + 8 * hl);
-      const float2 dd = *reinterpret_cast<const float2*>(slot + kOffD + 8 * hl);
-      const float2 gkh = cadd(gh, cscale(qh, c.alpha));
-      dh = cadd(make_float2(-gkh.x, -gkh.y), cscale(dd, c.beta));
-    }
-    r.uh = dh;
-    r.yh = -re_mul(dh, carrier(Lc, l.Ph, L.z));
-  }
+}
+
+// d_k = -g_k + beta d_{k-1} (zero outside the field) and its luma part.
+struct DRow {
+  float2 ua, ub;
+  float ya, yb;
+};
+
+__device__ __forceinline__ void slot_d(const char* slot, const Lanes& l, const FieldCtl& c,
+                                       bool first, int lane, DRow& r) {
+  float2 gka, gkb, doa, dob;
+  slot_gd(slot, c, first, lane, gka, gkb, doa, dob);
+  const float4 L = *reinterpret_cast<const float4*>(slot + kOffL);
+  const float2 Lc = make_float2(L.x, L.y);
+  r.ua = cadd(make_float2(-gka.x, -gka.y), cscale(doa, c.beta));
+  r.ub = cadd(make_float2(-gkb.x, -gkb.y), cscale(dob, c.beta));
+  if (!l.va) r.ua = make_float2(0.f, 0.f);
+  if (!l.vb) r.ub = make_float2(0.f, 0.f);
+  r.ya = -re_mul(r.ua, carrier(Lc, l.Pa, L.z));
+  r.yb = -re_mul(r.ub, carrier(Lc, l.Pb, L.z));
 }
 
 __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
@@ -544,7 +455,7 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
   const float2 z = make_float2(0.f, 0.f);
   const int ybeg = max(u.y0 - 1, 0), yend = min(u.y1, f.h - 1);
   const int nrows = yend - ybeg + 1;
-  double pH = 0.0, pgd = 0.0, pgq = 0.0, pqq = 0.0, pgg = 0.0;
+  float pH = 0.f, pgd = 0.f, pgq = 0.f, pqq = 0.f, pgg = 0.f;
   bool ok = true;
   __syncwarp();
   if (lane == 0) {
@@ -565,16 +476,16 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
       ring_issue(ring, inext % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
     }
   };
-  SRow cur, nxt;
+  DRow cur, nxt;
   float aypa = 0.f, aypb = 0.f;
   float2 bypa = z, bypb = z;
   int icur = 0;
   if (u.y0 > 0) {
-    SRow prv;
+    DRow prv;
     ok &= ring_wait(ring, 0);
-    ring_form(slot_ptr(0), A, f, l, c, first, lane, u.y0 - 1, prv);
+    slot_d(slot_ptr(0), l, c, first, lane, prv);
     ok &= ring_wait(ring, 1 % kNS);
-    ring_form(slot_ptr(1), A, f, l, c, first, lane, u.y0, cur);
+    slot_d(slot_ptr(1), l, c, first, lane, cur);
     const char* w0 = slot_ptr(0) + kOffW;
     const float4 wpa = *reinterpret_cast<const float4*>(w0 + 16 * (1 + 2 * lane));
     const float4 wpb = *reinterpret_cast<const float4*>(w0 + 16 * (2 + 2 * lane));
@@ -586,16 +497,43 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     icur = 1;
   } else {
     ok &= ring_wait(ring, 0);
-    ring_form(slot_ptr(0), A, f, l, c, first, lane, u.y0, cur);
+    slot_d(slot_ptr(0), l, c, first, lane, cur);
   }
   const int s2 = c.sel ^ 1;
+  float2* Gw = A.G[s2] + base;
+  float2* Dw = A.D[s2] + base;
+  float2* Qw = A.Q[s2] + base;
+  float2* Xw = A.X[c.xsel] + base;
   for (int y = u.y0; y < u.y1; ++y) {
     const bool hn = y + 1 < f.h;
     if (hn) {
       ok &= ring_wait(ring, (icur + 1) % kNS);
-      ring_form(slot_ptr(icur + 1), A, f, l, c, first, lane, y + 1, nxt);
+      slot_d(slot_ptr(icur + 1), l, c, first, lane, nxt);
     }
     const char* sl = slot_ptr(icur);
+    // the current row's g_k, d_{k-1}, carriers and halo, re-read from its slot
+    float2 gka, gkb, doa, dob;
+    slot_gd(sl, c, first, lane, gka, gkb, doa, dob);
+    if (!l.va) gka = z;
+    if (!l.vb) gkb = z;
+    const float4 L = *reinterpret_cast<const float4*>(sl + kOffL);
+    const float2 Lc = make_float2(L.x, L.y);
+    const float2 ca = carrier(Lc, l.Pa, L.z), cb = carrier(Lc, l.Pb, L.z);
+    float2 uh = z;
+    float yh = 0.f;
+    if (l.hv) {
+      const int hl = lane == 0 ? 1 : kStrip + 2;  // local column of x0-1 / x0+64
+      const float2 gh = *reinterpret_cast<const float2*>(sl + 8 * hl);
+      if (first) {
+        uh = make_float2(-gh.x, -gh.y);
+      } else {
+        const float2 qh = *reinterpret_cast<const float2*>(sl + kOffQ + 8 * hl);
+        const float2 dd = *reinterpret_cast<const float2*>(sl + kOffD + 8 * hl);
+        const float2 gkh = cadd(gh, cscale(qh, c.alpha));
+        uh = cadd(make_float2(-gkh.x, -gkh.y), cscale(dd, c.beta));
+      }
+      yh = -re_mul(uh, carrier(Lc, l.Ph, L.z));
+    }
     const float4 wa = *reinterpret_cast<const float4*>(sl + kOffW + 16 * (1 + 2 * lane));
     const float4 wb = *reinterpret_cast<const float4*>(sl + kOffW + 16 * (2 + 2 * lane));
     float4 wh = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -604,8 +542,8 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     float2 u_r = make_float2(__shfl_down_sync(0xffffffffu, cur.ua.x, 1),
                              __shfl_down_sync(0xffffffffu, cur.ua.y, 1));
     if (lane == 31) {
-      y_r = cur.yh;
-      u_r = cur.uh;
+      y_r = yh;
+      u_r = uh;
     }
     const bool ia = l.xa < f.w - 1, ib = l.xb < f.w - 1;
     const float dxya = ia ? cur.yb - cur.ya : 0.f;
@@ -619,8 +557,8 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
                              __shfl_up_sync(0xffffffffu, bxb.y, 1));
     if (lane == 0) {
       if (l.hv && l.hx < f.w - 1) {
-        axl = wh.x * (cur.ya - cur.yh);
-        bxl = cscale(csub(cur.ua, cur.uh), wh.z);
+        axl = wh.x * (cur.ya - yh);
+        bxl = cscale(csub(cur.ua, uh), wh.z);
       } else {
         axl = 0.f;
         bxl = z;
@@ -634,8 +572,8 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     const float2 bya = cscale(dyua, wa.w), byb = cscale(dyub, wb.w);
     const float ima = 2.f * ((axl - axa) + (aypa - aya));
     const float imb = 2.f * ((axa - axb) + (aypb - ayb));
-    float2 oa = make_float2(-ima * cur.ca.x, ima * cur.ca.y);
-    float2 ob = make_float2(-imb * cur.cb.x, imb * cur.cb.y);
+    float2 oa = make_float2(-ima * ca.x, ima * ca.y);
+    float2 ob = make_float2(-imb * cb.x, imb * cb.y);
     oa = cadd(oa, cscale(cadd(cscale(csub(bxl, bxa), mu_h), cscale(csub(bypa, bya), mu_v)), 2.f));
     ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
     const int64_t o = (int64_t)y * f.pitch + l.xa;
@@ -646,34 +584,32 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
       ob.x += Mb.x * cur.ub.x + Mb.y * cur.ub.y;
       ob.y += Mb.y * cur.ub.x + Mb.z * cur.ub.y;
       if (l.va)
-        pH += 0.5 * (double)(Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
-                             Ma.z * cur.ua.y * cur.ua.y);
+        pH += 0.5f * (Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
+                      Ma.z * cur.ua.y * cur.ua.y);
       if (l.vb)
-        pH += 0.5 * (double)(Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
-                             Mb.z * cur.ub.y * cur.ub.y);
+        pH += 0.5f * (Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
+                      Mb.z * cur.ub.y * cur.ub.y);
     }
     if (!l.va) oa = z;
     if (!l.vb) ob = z;
     if (l.va)
-      pH += (double)wa.x * dxya * dxya + (double)wa.y * dyya * dyya +
-            (double)mu_h * wa.z * cnorm(dxua) + (double)mu_v * wa.w * cnorm(dyua);
+      pH += wa.x * dxya * dxya + wa.y * dyya * dyya + mu_h * wa.z * cnorm(dxua) +
+            mu_v * wa.w * cnorm(dyua);
     if (l.vb)
-      pH += (double)wb.x * dxyb * dxyb + (double)wb.y * dyyb * dyyb +
-            (double)mu_h * wb.z * cnorm(dxub) + (double)mu_v * wb.w * cnorm(dyub);
-    pgd += (double)cur.gka.x * cur.ua.x + (double)cur.gka.y * cur.ua.y +
-           (double)cur.gkb.x * cur.ub.x + (double)cur.gkb.y * cur.ub.y;
-    pgq += (double)cur.gka.x * oa.x + (double)cur.gka.y * oa.y + (double)cur.gkb.x * ob.x +
-           (double)cur.gkb.y * ob.y;
-    pqq += (double)cnorm(oa) + (double)cnorm(ob);
-    pgg += (double)cnorm(cur.gka) + (double)cnorm(cur.gkb);
-    st_pair(A.G[s2] + base + o, cur.gka, cur.gkb, l.va, l.vb);
-    st_pair(A.D[s2] + base + o, cur.ua, cur.ub, l.va, l.vb);
-    st_pair(A.Q[s2] + base + o, oa, ob, l.va, l.vb);
+      pH += wb.x * dxyb * dxyb + wb.y * dyyb * dyyb + mu_h * wb.z * cnorm(dxub) +
+            mu_v * wb.w * cnorm(dyub);
+    pgd += (gka.x * cur.ua.x + gka.y * cur.ua.y) + (gkb.x * cur.ub.x + gkb.y * cur.ub.y);
+    pgq += (gka.x * oa.x + gka.y * oa.y) + (gkb.x * ob.x + gkb.y * ob.y);
+    pqq += cnorm(oa) + cnorm(ob);
+    pgg += cnorm(gka) + cnorm(gkb);
+    st_pair(Gw + o, gka, gkb, l.va, l.vb);
+    st_pair(Dw + o, cur.ua, cur.ub, l.va, l.vb);
+    st_pair(Qw + o, oa, ob, l.va, l.vb);
     if (!first) {
       const float4 x4 = *reinterpret_cast<const float4*>(sl + kOffX + 16 * lane);
-      const float2 xa = cadd(make_float2(x4.x, x4.y), cscale(cur.doa, c.alpha));
-      const float2 xb = cadd(make_float2(x4.z, x4.w), cscale(cur.dob, c.alpha));
-      st_pair(A.X[c.xsel] + base + o, xa, xb, l.va, l.vb);
+      const float2 xa = cadd(make_float2(x4.x, x4.y), cscale(doa, c.alpha));
+      const float2 xb = cadd(make_float2(x4.z, x4.w), cscale(dob, c.alpha));
+      st_pair(Xw + o, xa, xb, l.va, l.vb);
     }
     issue_after(icur);
     aypa = aya;
@@ -693,8 +629,8 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
 
 // F phase: apply the pending step, output-fidelity luma Y = S - Re[chi c]
 // (variational.cpp:552-555, sequence.cpp:1102-1114); final chi -> X[0].
-__device__ void phase_final(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
-                            const FieldCtl& c) {
+__device__ __noinline__ void phase_final(const SolverArgs& A, const FieldDesc& f, Unit u, int lane,
+                                         FieldCtl c) {
   const Lanes l = make_lanes(A, f, u.x0, lane);
   const int64_t base = f.px_off;
   const float2* X = A.X[c.xsel] + base;
@@ -729,7 +665,8 @@ __device__ void phase_final(const SolverArgs& A, const FieldDesc& f, const Unit&
 // Field-level completion: fixed-order reduction of the unit partials and the
 // CG scalar logic (variational.cpp:519-549).
 // ---------------------------------------------------------------------------
-__device__ void complete_phase(const SolverArgs& A, const FieldDesc& f, int fi, int kind, int k,
+__device__ __noinline__ void complete_phase(const SolverArgs& A, const FieldDesc& f, int fi,
+                                            int kind, int k,
                                int p, int lane) {
   FieldCtl* c = A.ctl + fi;
   double s[kNPart];
@@ -784,7 +721,7 @@ __device__ void complete_phase(const SolverArgs& A, const FieldDesc& f, int fi, 
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kSolverThreads, 2) k_solver(SolverArgs A) {
+__global__ void __launch_bounds__(kSolverThreads, 2) k_solver(const __grid_constant__ SolverArgs A) {
   const int lane = threadIdx.x & 31;
   extern __shared__ __align__(16) char solver_smem[];
   Ring ring;
@@ -843,17 +780,20 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(SolverArgs A) {
       k = r - 2;
     }
     double part[kNPart] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // the rarely taken phases are out of line (their registers do not
+    // constrain the CG sweep); they read the field from its global copy
+    const FieldDesc& fg = A.fields[u.field];
     if (kind == kPhaseR) {
-      phase_reweight(A, f, u, lane, c);
+      phase_reweight(A, fg, u, lane, c);
     } else if (kind == kPhaseG) {
-      phase_stencil<false>(A, f, u, lane, c, false, part);
+      part[0] = part[4] = phase_gradient(A, fg, u, lane, c);
     } else if (kind == kPhaseI) {
       if (!phase_iter(A, f, u, lane, c, k == 0, ring, part)) {
         if (lane == 0) atomicOr(A.err, 2);
         break;
       }
     } else {
-      phase_final(A, f, u, lane, c);
+      phase_final(A, fg, u, lane, c);
     }
     if (kind == kPhaseG || kind == kPhaseI) {
 #pragma unroll
@@ -869,7 +809,7 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(SolverArgs A) {
     if (last) {
       if (lane == 0) A.arrive[u.field] = 0;
       __threadfence();
-      complete_phase(A, f, u.field, kind, k, p, lane);
+      complete_phase(A, fg, u.field, kind, k, p, lane);
     }
   }
 }
