@@ -123,15 +123,25 @@ class Context:
             keep.append(arr[i].geometry)
         return arr, keep
 
-    def _alloc_out(self, fields, want_theta: bool):
+    def _alloc_out(self, fields, want_theta: bool, out=None):
         outs, res = (FieldOut * max(len(fields), 1))(), []
+        if out is not None and len(out) != len(fields):
+            raise ValueError(f"out: {len(out)} buffers for {len(fields)} fields")
         for i, f in enumerate(fields):
             g = f.geometry
-            d = Decoded(np.zeros((g.active_lines, g.active_width), np.float32),
-                        np.zeros((g.active_lines, g.active_width), np.complex64))
+            shape = (g.active_lines, g.active_width)
+            if out is not None:
+                d = out[i]
+                if (d.luma.shape != shape or d.luma.dtype != np.float32
+                        or not d.luma.flags.c_contiguous or d.chroma.shape != shape
+                        or d.chroma.dtype != np.complex64 or not d.chroma.flags.c_contiguous):
+                    raise ValueError(f"out[{i}]: need C-contiguous float32 luma and complex64 "
+                                     f"chroma of shape {shape}")
+            else:
+                d = Decoded(np.zeros(shape, np.float32), np.zeros(shape, np.complex64))
             outs[i].luma = d.luma.ctypes.data
             outs[i].chroma = d.chroma.ctypes.data
-            if want_theta:
+            if want_theta and (d.theta is None or d.vswitch is None):
                 d.theta = np.zeros(g.field_height, np.float32)
                 d.vswitch = np.zeros(g.field_height, np.int8)
                 outs[i].theta = d.theta.ctypes.data
@@ -139,10 +149,14 @@ class Context:
             res.append(d)
         return outs, res
 
-    def decode_fields(self, fields, cfg: Config, want_theta: bool = False) -> list[Decoded]:
-        """Independent 2-D fields (mixed geometry / budget) in one batch."""
+    def decode_fields(self, fields, cfg: Config, want_theta: bool = False,
+                      out: list[Decoded] | None = None) -> list[Decoded]:
+        """Independent 2-D fields (mixed geometry / budget) in one batch.
+        `out` optionally supplies the output buffers (one Decoded per field,
+        e.g. views of page-locked memory, which the device writes at full
+        copy bandwidth); they are filled in place and returned."""
         arr, keep = self._build_fields(fields)
-        outs, res = self._alloc_out(fields, want_theta)
+        outs, res = self._alloc_out(fields, want_theta, out)
         self.last_diag = Diag()
         st = self.lib.hvdg_decode_fields(self._h, arr, len(fields), C.byref(cfg), outs,
                                          C.byref(self.last_diag))
