@@ -299,6 +299,9 @@ PinnedArena::~PinnedArena() {
 
 namespace {
 
+// tile count limit of one integer-SAD confidence pass (its doubles live in shared memory)
+constexpr int kSadMaxTiles = 6144;
+
 // ---------------------------------------------------------------------------
 // Batch planning
 // ---------------------------------------------------------------------------
@@ -1241,9 +1244,19 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   const int h = plan.fp[0].h, w = plan.fp[0].w, pitch = plan.fp[0].pitch;
   const int64_t plane = (int64_t)h * pitch;
   const int nofs = (int)offs.size();
-  const int tile = cfg.mc_tile, search = cfg.mc_search;
+  // me_mode 1: integer-SAD blocks (me_block, +-me_range); else the reference's
+  // float-SSD pyramid on mc_tile tiles (+-mc_search)
+  const bool sad_me = cfg.me_mode == 1;
+  const int tile = sad_me ? cfg.me_block : cfg.mc_tile;
+  const int search = sad_me ? cfg.me_range : cfg.mc_search;
   if (tile < 1 || search < 0 || tile > 1024 || search > 64) return HVDG_ERR_BAD_ARGUMENT;
+  if (cfg.me_mode < 0 || cfg.me_mode > 1) return HVDG_ERR_BAD_ARGUMENT;
   const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile, nt = th * tw;
+  if (sad_me && (tile > hvdg::sad_max_block() || search > hvdg::sad_max_range() ||
+                 nt > kSadMaxTiles)) {
+    ctx->last_error = "integer-SAD motion: block, range or tile count above the supported maximum";
+    return HVDG_ERR_UNSUPPORTED;
+  }
   const int ct = std::max(4, tile / 4);
   const int nct = std::max(1, ((h / 4 + ct - 1) / ct) * ((w / 4 + ct - 1) / ct));
   const int dpitch = pitch / 4;
@@ -1265,6 +1278,9 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   const size_t x_cdx = take(sizeof(float) * nct * max_pairs);
   size_t x_t[13];
   for (int i = 0; i < 13; ++i) x_t[i] = take(sizeof(float) * nt * max_pairs);
+  size_t x_sd[4] = {0, 0, 0, 0};  // integer-SAD tile statistics (doubles)
+  if (sad_me)
+    for (int i = 0; i < 4; ++i) x_sd[i] = take(sizeof(double) * nt * max_pairs);
   const size_t x_src = take(sizeof(int2) * plane * max_pairs);
   const size_t x_cpx = take(sizeof(float) * plane * max_pairs);
   const size_t x_ctmp = take(sizeof(float) * plane * max_pairs);
@@ -1443,6 +1459,25 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   mb.dy = at<float>(ctx, X(x_t[5]));
   mb.dx = at<float>(ctx, X(x_t[6]));
   mb.conf = at<float>(ctx, X(x_t[7]));
+  hvdg::SadArgs sad_a;
+  sad_a.block = tile;
+  sad_a.range = search;
+  sad_a.tiles_off = nt;
+  hvdg::SadBuffers sad_b;
+  sad_b.luma = mb.luma;
+  sad_b.vsum = reinterpret_cast<int*>(mb.tmp);
+  sad_b.qblur = reinterpret_cast<int*>(mb.blur);
+  sad_b.mdy = mb.mdy;
+  sad_b.mdx = mb.mdx;
+  sad_b.sdy = mb.sdy;
+  sad_b.sdx = mb.sdx;
+  sad_b.dy = mb.dy;
+  sad_b.dx = mb.dx;
+  sad_b.conf = mb.conf;
+  sad_b.bestv = sad_me ? at<double>(ctx, X(x_sd[0])) : nullptr;
+  sad_b.s1 = sad_me ? at<double>(ctx, X(x_sd[1])) : nullptr;
+  sad_b.s2 = sad_me ? at<double>(ctx, X(x_sd[2])) : nullptr;
+  sad_b.npx = sad_me ? at<double>(ctx, X(x_sd[3])) : nullptr;
   hvdg::VecBuffers vb;
   vb.dy = mb.dy;
   vb.dx = mb.dx;
@@ -1504,7 +1539,10 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(d_np, np.data(), sizeof(hvdg::NbrPair) * npairs, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D pairs");
-        hvdg::launch_motion(d_mf, nf, h, w, d_mp, npairs, ma, mb, s);
+        if (sad_me)
+          hvdg::launch_motion_sad(d_mf, nf, h, w, d_mp, npairs, sad_a, sad_b, s);
+        else
+          hvdg::launch_motion(d_mf, nf, h, w, d_mp, npairs, ma, mb, s);
         vb.conf_bytes = sizeof(float) * plane * npairs;
         hvdg::launch_vectors(d_mf, d_mp, npairs, h, w, ma, vb, cfg.fast != 0, s);
         S.launches += 8;
@@ -1710,6 +1748,92 @@ hvdg_status lockin_one(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometr
   }
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "lock-in");
+  return HVDG_OK;
+}
+
+// Integer-SAD motion estimation of one pair (me_mode 1): block x block
+// tiles, exhaustive +-range; tile outputs like EstimateMotion's.
+hvdg_status estimate_motion_sad(hvdg_ctx* ctx, const float* y_ref, const float* y_cur, int h,
+                                int w, int block, int range, float* dy, float* dx,
+                                float* confidence) {
+  if (block > hvdg::sad_max_block() || range > hvdg::sad_max_range()) {
+    ctx->last_error = "integer-SAD motion: block or range above the supported maximum";
+    return HVDG_ERR_UNSUPPORTED;
+  }
+  const int th = (h + block - 1) / block, tw = (w + block - 1) / block, nt = th * tw;
+  if (nt > kSadMaxTiles) {
+    ctx->last_error = "integer-SAD motion: too many tiles for one confidence pass";
+    return HVDG_ERR_UNSUPPORTED;
+  }
+  cudaSetDevice(ctx->device);
+  const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
+  const size_t plane = (size_t)h * pitch;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes, 256);
+    return r;
+  };
+  const size_t o_f = take(sizeof(hvdg::MeField) * 2);
+  const size_t o_p = take(sizeof(hvdg::MePair));
+  const size_t o_l = take(sizeof(float) * 2 * plane);
+  const size_t o_v = take(sizeof(int) * 2 * plane);
+  const size_t o_q = take(sizeof(int) * 2 * plane);
+  size_t of[7], od[4];
+  for (int i = 0; i < 7; ++i) of[i] = take(sizeof(float) * nt);
+  for (int i = 0; i < 4; ++i) od[i] = take(sizeof(double) * nt);
+  hvdg_status st = ctx->arena.reserve(o, ctx->stream);
+  if (st != HVDG_OK) return st;
+  ctx->epoch += 1;
+  char* base = static_cast<char*>(ctx->arena.base);
+  hvdg::MeField mf[2];
+  for (int i = 0; i < 2; ++i) {
+    std::memset(&mf[i], 0, sizeof(mf[i]));
+    mf[i].h = h;
+    mf[i].w = w;
+    mf[i].pitch = pitch;
+    mf[i].y_off = mf[i].t_off = mf[i].b_off = (int64_t)i * plane;
+  }
+  const hvdg::MePair pr{0, 1};
+  cudaStream_t s = ctx->stream;
+  cudaGetLastError();
+  cudaError_t e = cudaMemcpyAsync(base + o_f, mf, sizeof(mf), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_p, &pr, sizeof(pr), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(base + o_l, sizeof(float) * pitch, y_ref, sizeof(float) * w,
+                          sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(base + o_l + sizeof(float) * plane, sizeof(float) * pitch, y_cur,
+                          sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D motion inputs");
+  hvdg::SadArgs a;
+  a.block = block;
+  a.range = range;
+  a.tiles_off = nt;
+  hvdg::SadBuffers b;
+  b.luma = reinterpret_cast<const float*>(base + o_l);
+  b.vsum = reinterpret_cast<int*>(base + o_v);
+  b.qblur = reinterpret_cast<int*>(base + o_q);
+  b.mdy = reinterpret_cast<float*>(base + of[0]);
+  b.mdx = reinterpret_cast<float*>(base + of[1]);
+  b.sdy = reinterpret_cast<float*>(base + of[2]);
+  b.sdx = reinterpret_cast<float*>(base + of[3]);
+  b.dy = reinterpret_cast<float*>(base + of[4]);
+  b.dx = reinterpret_cast<float*>(base + of[5]);
+  b.conf = reinterpret_cast<float*>(base + of[6]);
+  b.bestv = reinterpret_cast<double*>(base + od[0]);
+  b.s1 = reinterpret_cast<double*>(base + od[1]);
+  b.s2 = reinterpret_cast<double*>(base + od[2]);
+  b.npx = reinterpret_cast<double*>(base + od[3]);
+  hvdg::launch_motion_sad(reinterpret_cast<const hvdg::MeField*>(base + o_f), 2, h, w,
+                          reinterpret_cast<const hvdg::MePair*>(base + o_p), 1, a, b, s);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, b.dy, sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dx, b.dx, sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(confidence, b.conf, sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "integer-SAD motion estimation");
   return HVDG_OK;
 }
 
@@ -1933,10 +2057,8 @@ hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref, const float*
   if (!ctx || !y_ref || !y_cur || !dy || !dx || !confidence || h < 1 || w < 1 || tile < 1 ||
       search < 0 || me_mode < 0 || me_mode > 1)
     return HVDG_ERR_BAD_ARGUMENT;
-  if (me_mode == 1) {
-    ctx->last_error = "integer-SAD motion mode is not available in this build";
-    return HVDG_ERR_UNSUPPORTED;
-  }
+  if (me_mode == 1) return estimate_motion_sad(ctx, y_ref, y_cur, h, w, tile, search, dy, dx,
+                                               confidence);
   if (4 * tile > 4096 || search > 64) return HVDG_ERR_UNSUPPORTED;
   cudaSetDevice(ctx->device);
   const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;

@@ -338,6 +338,316 @@ void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const 
 }
 
 // ---------------------------------------------------------------------------
+// Integer-SAD motion mode (me_mode 1): exhaustive +-range search of
+// block x block tiles on uint16-quantised, integer-box-blurred luma. The
+// cost has no reference counterpart (the reference matches float SSD); the
+// control structure follows EstimateMotion (motion.cpp:397-488) -- visit
+// order RangeFromCentre (:286-298), strict-less update (:244), bias
+// 1 + 0.02 (|dy| + |dx|), zero-motion margin 0.85 (:455-473), parabolic
+// sub-pel (:437-452), MotionConfidence (:321-387) -- with every decision
+// exact in integers: SAD_a (50 + L1_a) < SAD_b (50 + L1_b), and
+// 20 best > 17 cost0 for the margin. A parallel argmin over the key
+// (biased cost, visit index) selects the same candidate as the reference's
+// sequential strict-less scan.
+// ---------------------------------------------------------------------------
+constexpr float kQuantZero = 16384.0f;   // 0 IRE
+constexpr float kQuantScale = 348.16f;   // codes per IRE
+constexpr int kSadMaxBlock = 32;
+constexpr int kSadMaxRange = 22;         // (2 range + 1)^2 visit indices fit in 11 bits
+constexpr int kSadGroup = 8;             // consecutive dx per thread
+constexpr int kSadThreads = 192;
+
+int sad_max_block() { return kSadMaxBlock; }
+int sad_max_range() { return kSadMaxRange; }
+
+__device__ __forceinline__ int quant_luma(float y) {
+  const float t = kQuantZero + kQuantScale * y;  // multiply, then add (no FMA in this unit)
+  return (int)fminf(fmaxf(rintf(t), 0.0f), 65535.0f);
+}
+
+// Vertical 5-row window sums of the quantised luma (zero outside the field).
+// One thread per (field, column).
+__global__ void k_sad_vsum(const MeField* __restrict__ mf, int nf, const float* __restrict__ luma,
+                           int* __restrict__ vsum) {
+  const int f = blockIdx.y;
+  const MeField m = mf[f];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= m.w) return;
+  const float* Y = luma + m.y_off;
+  int* V = vsum + m.t_off;
+  int ring[5] = {0, 0, 0, 0, 0};
+  int acc = 0;
+  // rows y - 2 .. y + 2; prime with rows 0 .. 1
+  for (int y = 0; y < 2 && y < m.h; ++y) {
+    ring[y] = quant_luma(Y[(int64_t)y * m.pitch + x]);
+    acc += ring[y];
+  }
+  for (int y = 0; y < m.h; ++y) {
+    const int yn = y + 2;
+    if (yn < m.h) {
+      const int q = quant_luma(Y[(int64_t)yn * m.pitch + x]);
+      acc += q;
+      ring[yn % 5] = q;
+    }
+    V[(int64_t)y * m.pitch + x] = acc;
+    const int yo = y - 2;
+    if (yo >= 0) {
+      acc -= ring[yo % 5];
+      ring[yo % 5] = 0;
+    }
+  }
+}
+
+// Horizontal 5-column sums of vsum, rounded division by 25. One thread per
+// (field, row).
+__global__ void k_sad_hsum(const MeField* __restrict__ mf, int nf, const int* __restrict__ vsum,
+                           int* __restrict__ qblur) {
+  const int f = blockIdx.y;
+  const MeField m = mf[f];
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= m.h) return;
+  const int* V = vsum + m.t_off + (int64_t)y * m.pitch;
+  int* Q = qblur + m.b_off + (int64_t)y * m.pitch;
+  int acc = 0;
+  for (int x = 0; x < 2 && x < m.w; ++x) acc += V[x];
+  for (int x = 0; x < m.w; ++x) {
+    if (x + 2 < m.w) acc += V[x + 2];
+    Q[x] = (acc + 12) / 25;
+    if (x - 2 >= 0) acc -= V[x - 2];
+  }
+}
+
+__device__ __forceinline__ int centre_out_index(int d) {
+  return d == 0 ? 0 : (d > 0 ? 2 * d : -2 * d - 1);
+}
+
+// SAD over the tile of source offset (dy, dx), one warp (lanes over pixels).
+__device__ __forceinline__ unsigned long long warp_tile_cost(const int* As, const int* Bs, int b,
+                                                             int ww, int S, int bh, int bw,
+                                                             int dy, int dx, bool squared,
+                                                             int lane) {
+  unsigned long long acc = 0;
+  for (int i = lane; i < bh * bw; i += 32) {
+    const int yy = i / bw, xx = i % bw;
+    const int d = As[yy * b + xx] - Bs[(yy - dy + S) * ww + (xx - dx + S)];
+    acc += squared ? (unsigned long long)((long long)d * d) : (unsigned long long)abs(d);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+// One CTA per (tile, pair).
+__global__ void __launch_bounds__(kSadThreads) k_sad_search(const MeField* __restrict__ mf,
+                                                            const MePair* __restrict__ pairs,
+                                                            const int* __restrict__ qblur,
+                                                            SadArgs a, SadBuffers out) {
+  const int p = blockIdx.y, t = blockIdx.x;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int h = mc.h, w = mc.w, b = a.block, s = a.range;
+  const int th = (h + b - 1) / b, tw = (w + b - 1) / b;
+  if (t >= th * tw) return;
+  const int ty = t / tw, tx = t % tw;
+  const int y0 = ty * b, x0 = tx * b;
+  const int bh = min(b, h - y0), bw = min(b, w - x0);
+  const int S = s + 1;          // window margin: the search range plus the sub-pel neighbours
+  const int ww = b + 2 * S;
+  extern __shared__ int sad_sm[];
+  int* As = sad_sm;             // b x b
+  int* Bs = sad_sm + b * b;     // ww x ww, B(clamp(y0 - S + wy), clamp(x0 - S + wx))
+  __shared__ unsigned long long red[kSadThreads / 32];
+  __shared__ unsigned long long sh_sad0, sh_best, sh_side[4], sh_ssd;
+  __shared__ long long sh_s1, sh_s2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int* QA = qblur + mc.b_off;
+  const int* QB = qblur + mr.b_off;
+  for (int i = tid; i < bh * bw; i += blockDim.x)
+    As[(i / bw) * b + i % bw] = QA[(int64_t)(y0 + i / bw) * mc.pitch + x0 + i % bw];
+  for (int i = tid; i < ww * ww; i += blockDim.x) {
+    const int wy = i / ww, wx = i % ww;
+    const int sy = clampi(y0 - S + wy, 0, h - 1), sx = clampi(x0 - S + wx, 0, w - 1);
+    Bs[i] = QB[(int64_t)sy * mr.pitch + sx];
+  }
+  __syncthreads();
+  // candidates: (dy, group of kSadGroup consecutive dx), key = cost << 11 | visit index
+  const int n = 2 * s + 1;
+  const int ngroups = (n + kSadGroup - 1) / kSadGroup;
+  unsigned long long bestkey = ~0ull;
+  for (int it = tid; it < n * ngroups; it += blockDim.x) {
+    const int dy = it / ngroups - s;
+    const int dxg = -s + (it % ngroups) * kSadGroup;
+    unsigned acc[kSadGroup];
+#pragma unroll
+    for (int g = 0; g < kSadGroup; ++g) acc[g] = 0u;
+    for (int yy = 0; yy < bh; ++yy) {
+      const int* ar = As + yy * b;
+      // window row for this dy; column of pixel xx under offset dxg + g:
+      // xx - dxg - g + S
+      const int* br = Bs + (yy - dy + S) * ww + (S - dxg);
+      for (int xx = 0; xx < bw; ++xx) {
+        const int av = ar[xx];
+#pragma unroll
+        for (int g = 0; g < kSadGroup; ++g) {
+          const int col = xx - g;  // relative to br; >= -(kSadGroup - 1)
+          acc[g] += (unsigned)abs(av - br[col]);
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kSadGroup; ++g) {
+      const int dx = dxg + g;
+      if (dx > s) break;
+      const unsigned long long cost =
+          (unsigned long long)acc[g] * (unsigned long long)(50 + abs(dy) + abs(dx));
+      const unsigned long long ci =
+          (unsigned long long)(centre_out_index(dy) * n + centre_out_index(dx));
+      const unsigned long long key = (cost << 11) | ci;
+      if (key < bestkey) bestkey = key;
+      if (dy == 0 && dx == 0) sh_sad0 = acc[g];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, bestkey, o);
+    if (v < bestkey) bestkey = v;
+  }
+  if (lane == 0) red[warp] = bestkey;
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long m = red[0];
+    for (int i = 1; i < (int)(blockDim.x / 32); ++i) m = red[i] < m ? red[i] : m;
+    sh_best = m;
+  }
+  __syncthreads();
+  const unsigned long long best = sh_best >> 11;
+  const int ci = (int)(sh_best & 2047ull);
+  const int mdy = centre_out(ci / n), mdx = centre_out(ci % n);
+  // the sub-pel neighbours' unbiased SADs, the zero-margin decision, then the
+  // SSD at the final vector and the tile statistics of A (one warp each)
+  const unsigned long long cost0 = 50ull * sh_sad0;
+  const bool zero = 20ull * best > 17ull * cost0;
+  const int fdy = zero ? 0 : mdy, fdx = zero ? 0 : mdx;
+  if (warp < 4) {
+    const int oy = warp == 0 ? -1 : (warp == 1 ? 1 : 0);
+    const int ox = warp == 2 ? -1 : (warp == 3 ? 1 : 0);
+    const unsigned long long v =
+        warp_tile_cost(As, Bs, b, ww, S, bh, bw, mdy + oy, mdx + ox, false, lane);
+    if (lane == 0) sh_side[warp] = v;
+  } else if (warp == 4) {
+    const unsigned long long v = warp_tile_cost(As, Bs, b, ww, S, bh, bw, fdy, fdx, true, lane);
+    if (lane == 0) sh_ssd = v;
+  } else if (warp == 5) {
+    long long s1 = 0, s2 = 0;
+    for (int i = lane; i < bh * bw; i += 32) {
+      const long long v = As[(i / bw) * b + i % bw];
+      s1 += v;
+      s2 += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+      sh_s1 = s1;
+      sh_s2 = s2;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // parabola through (-1, 50 SAD_m), (0, best), (+1, 50 SAD_p): exact
+    // integer numerator and denominator, one division
+    auto parabolic = [&](unsigned long long sm, unsigned long long sp) -> double {
+      const long long num = 50ll * (long long)sm - 50ll * (long long)sp;
+      const long long den = 50ll * (long long)sm - 2ll * (long long)best + 50ll * (long long)sp;
+      double sub = den > 0 ? 0.5 * (double)num / (double)den : 0.0;
+      return fmin(fmax(sub, -0.5), 0.5);
+    };
+    double sdy = parabolic(sh_side[0], sh_side[1]);
+    double sdx = parabolic(sh_side[2], sh_side[3]);
+    if (zero) {
+      sdy = 0.0;
+      sdx = 0.0;
+    }
+    const int o = a.tiles_off * p + t;
+    out.mdy[o] = (float)fdy;
+    out.mdx[o] = (float)fdx;
+    out.sdy[o] = (float)sdy;
+    out.sdx[o] = (float)sdx;
+    const double sc2 = (double)kQuantScale * (double)kQuantScale;
+    out.bestv[o] = (double)(sh_ssd * (unsigned long long)(50 + abs(fdy) + abs(fdx))) / (50.0 * sc2);
+    out.s1[o] = (double)sh_s1;
+    out.s2[o] = (double)sh_s2;
+    out.npx[o] = (double)(bh * bw);
+    out.dy[o] = (float)((double)fdy + sdy);
+    out.dx[o] = (float)((double)fdx + sdx);
+  }
+}
+
+// Exact k-th smallest of v[0..n) (stable rank count), by the whole CTA.
+__device__ double block_kth_double(const double* v, int n, int k, double* slot) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = v[i];
+    int less = 0, eq_before = 0;
+    for (int j = 0; j < n; ++j) {
+      const double y = v[j];
+      less += y < x;
+      eq_before += (y == x) & (j < i);
+    }
+    if (less + eq_before == k) *slot = x;
+  }
+  __syncthreads();
+  const double r = *slot;
+  __syncthreads();
+  return r;
+}
+
+// MotionConfidence on the IRE scale from the exact integer statistics. One
+// CTA per pair.
+__global__ void __launch_bounds__(256) k_sad_confidence(const MeField* __restrict__ mf,
+                                                        const MePair* __restrict__ pairs,
+                                                        SadArgs a, SadBuffers out) {
+  extern __shared__ double sadc_sm[];
+  __shared__ double slot;
+  const int p = blockIdx.x;
+  const MeField mc = mf[pairs[p].cur];
+  const int b = a.block;
+  const int th = (mc.h + b - 1) / b, tw = (mc.w + b - 1) / b, nt = th * tw;
+  double* ratios = sadc_sm;
+  const int o = a.tiles_off * p;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x)
+    ratios[t] = out.bestv[o + t] / fmax(1.0, out.npx[o + t]);
+  __syncthreads();
+  const int k = nt / 2;
+  double med = block_kth_double(ratios, nt, k, &slot);
+  if (nt % 2 == 0) med = 0.5 * (med + block_kth_double(ratios, nt, k - 1, &slot));
+  const double sc2 = (double)kQuantScale * (double)kQuantScale;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    const double npx = out.npx[o + t];
+    const double norm = 1.0 / fmax(1.0, npx);
+    const double tmean = out.s1[o + t] * norm;
+    const double tvar = (out.s2[o + t] * norm - tmean * tmean) / sc2;
+    const double energy = (tvar + 1.0) * fmax(1.0, npx);
+    double c = fmin(fmax(1.0 - out.bestv[o + t] / energy, 0.0), 1.0);
+    const double excess = fmax(0.0, ratios[t] - med);
+    c = c * ((med + 1.0) / (med + 1.0 + excess));
+    c = c * (6.0 / (6.0 + med));
+    out.conf[o + t] = (float)c;
+  }
+}
+
+void launch_motion_sad(const MeField* d_fields, int nf, int max_h, int max_w,
+                       const MePair* d_pairs, int npairs, const SadArgs& a, const SadBuffers& b,
+                       cudaStream_t st) {
+  if (nf <= 0 || npairs <= 0) return;
+  k_sad_vsum<<<dim3((max_w + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.luma, b.vsum);
+  k_sad_hsum<<<dim3((max_h + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.vsum, b.qblur);
+  const int th = (max_h + a.block - 1) / a.block, tw = (max_w + a.block - 1) / a.block;
+  const int ww = a.block + 2 * (a.range + 1);
+  const int smem = (a.block * a.block + ww * ww) * (int)sizeof(int);
+  k_sad_search<<<dim3(th * tw, npairs), kSadThreads, smem, st>>>(d_fields, d_pairs, b.qblur, a, b);
+  k_sad_confidence<<<npairs, 256, th * tw * (int)sizeof(double), st>>>(d_fields, d_pairs, a, b);
+}
+
+// ---------------------------------------------------------------------------
 // VectorsPerPixel (temporal.cpp:45-112): 3x3 median outlier snap on the tile
 // grid, then bilinear interpolation between tile centres.
 // ---------------------------------------------------------------------------

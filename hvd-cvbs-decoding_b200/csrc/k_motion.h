@@ -47,6 +47,26 @@ struct VecBuffers {
   size_t conf_bytes;
 };
 
+// Integer-SAD mode (me_mode 1): block x block tiles, exhaustive +-range.
+struct SadArgs {
+  int block, range;
+  int tiles_off;   // per-pair stride of the tile arrays
+};
+
+struct SadBuffers {
+  const float* luma;               // per field at MeField::y_off
+  int* vsum;                       // per field at MeField::t_off (vertical window sums)
+  int* qblur;                      // per field at MeField::b_off (quantised, blurred luma)
+  float *mdy, *mdx, *sdy, *sdx;    // per tile: integer vector, sub-pel offsets
+  double *bestv, *s1, *s2, *npx;   // per tile: biased SSD (IRE^2), sums of A, pixel count
+  float *dy, *dx, *conf;           // per tile outputs (as EstimateMotion's)
+};
+
+int sad_max_block();
+int sad_max_range();
+void launch_motion_sad(const MeField* d_fields, int nf, int max_h, int max_w,
+                       const MePair* d_pairs, int npairs, const SadArgs& a, const SadBuffers& b,
+                       cudaStream_t st);
 void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const MePair* d_pairs,
                    int npairs, const MeArgs& a, const MeBuffers& b, cudaStream_t st);
 void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,

@@ -740,6 +740,142 @@ def estimate_motion(y_ref, y_cur, tile=32, search=8):
     return mdy + sdy, mdx + sdx, conf
 
 
+# --------------------------------------------------------------------------
+# Integer-SAD motion mode (me_mode 1). No reference counterpart for the cost:
+# the reference's EstimateMotion uses float SSD. This mode keeps its control
+# structure (motion.cpp:397-488: centre-out visit order RangeFromCentre
+# :286-298, strict-less update :244, bias 1 + 0.02 (|dy| + |dx|), zero-motion
+# margin 0.85 :455-473, parabolic sub-pel :437-452, MotionConfidence
+# :321-387) with every decision exact in integers.
+# --------------------------------------------------------------------------
+QUANT_ZERO = np.float32(16384.0)    # 0 IRE
+QUANT_SCALE = np.float32(348.16)    # codes per IRE (100 IRE = 51200)
+
+
+def quantise_luma(y):
+    """uint16 codes of float32 IRE luma: rint(16384 + 348.16 y) in float32
+    (multiply, then add), clamped to [0, 65535]."""
+    t = QUANT_ZERO + QUANT_SCALE * np.asarray(y, np.float32)
+    return np.clip(np.rint(t), 0, 65535).astype(np.int64)
+
+
+def box_blur_int(q, r=2):
+    """Integer BoxBlur: zero-padded (2r+1)^2 window sum, rounded division by
+    (2r+1)^2 ((sum + k2 // 2) // k2)."""
+    q = np.asarray(q, np.int64)
+    h, w = q.shape
+    k = 2 * r + 1
+    p = np.pad(q, r)
+    v = np.zeros((h, w + 2 * r), np.int64)
+    for d in range(k):
+        v += p[d:d + h, :]
+    o = np.zeros((h, w), np.int64)
+    for d in range(k):
+        o += v[:, d:d + w]
+    k2 = k * k
+    return (o + k2 // 2) // k2
+
+
+def _centre_out_index(d):
+    return 0 if d == 0 else (2 * d if d > 0 else -2 * d - 1)
+
+
+def _tile_sums(e, tile, th, tw):
+    """Per-tile sums; the last tile row / column holds the remainder
+    (th = ceil(h / tile)), so zero padding to th x tw whole tiles is exact."""
+    h, w = e.shape
+    p = np.zeros((th * tile, tw * tile), e.dtype)
+    p[:h, :w] = e
+    return p.reshape(th, tile, tw, tile).sum(axis=(1, 3))
+
+
+def _shifted(B, dy, dx):
+    """B(clamp(y - dy), clamp(x - dx)) over the whole plane."""
+    h, w = B.shape
+    sy = np.clip(np.arange(h) - dy, 0, h - 1)
+    sx = np.clip(np.arange(w) - dx, 0, w - 1)
+    return B[sy][:, sx]
+
+
+def _shifted_tiles(B, dyt, dxt, tile):
+    """Per-pixel source with a per-tile integer vector."""
+    h, w = B.shape
+    th, tw = dyt.shape
+    ty = np.minimum(np.arange(h) // tile, th - 1)
+    tx = np.minimum(np.arange(w) // tile, tw - 1)
+    vy = dyt[ty][:, tx]
+    vx = dxt[ty][:, tx]
+    yy, xx = np.meshgrid(np.arange(h), np.arange(w), indexing="ij")
+    return B[np.clip(yy - vy, 0, h - 1), np.clip(xx - vx, 0, w - 1)]
+
+
+def estimate_motion_sad(y_ref, y_cur, block=16, search=16):
+    """Exhaustive +-search integer-SAD block matching of block x block tiles
+    on quantised, integer-blurred luma (me_mode 1). Returns per-tile
+    (dy, dx, confidence) as float32, like estimate_motion."""
+    A = box_blur_int(quantise_luma(y_cur))
+    B = box_blur_int(quantise_luma(y_ref))
+    h, w = A.shape
+    th, tw = -(-h // block), -(-w // block)
+    rc = range_from_centre(-search, search)
+    n = len(rc)
+    best = np.full((th, tw), np.iinfo(np.int64).max, np.int64)
+    bci = np.zeros((th, tw), np.int64)
+    sad0 = None
+    for i, dy in enumerate(rc):
+        for j, dx in enumerate(rc):
+            sad = _tile_sums(np.abs(A - _shifted(B, dy, dx)), block, th, tw)
+            if dy == 0 and dx == 0:
+                sad0 = sad.copy()
+            cost = sad * (50 + abs(dy) + abs(dx))
+            upd = cost < best                      # strict-less in visit order
+            best = np.where(upd, cost, best)
+            bci = np.where(upd, i * n + j, bci)
+    mdy = np.array([[rc[c // n] for c in row] for row in bci], np.int64)
+    mdx = np.array([[rc[c % n] for c in row] for row in bci], np.int64)
+    # parabolic sub-pel from the unbiased SADs either side (x50 scale, exact)
+    def sad_at(vy, vx):
+        return _tile_sums(np.abs(A - _shifted_tiles(B, vy, vx, block)), block, th, tw)
+
+    def parabolic(sm, sp):
+        num = 50 * sm - 50 * sp
+        den = 50 * sm - 2 * best + 50 * sp
+        sub = np.where(den > 0, 0.5 * num.astype(np.float64) / np.maximum(den, 1), 0.0)
+        return np.clip(sub, -0.5, 0.5)
+    sdy = parabolic(sad_at(mdy - 1, mdx), sad_at(mdy + 1, mdx))
+    sdx = parabolic(sad_at(mdy, mdx - 1), sad_at(mdy, mdx + 1))
+    cost0 = 50 * sad0
+    m = 20 * best > 17 * cost0                     # best > 0.85 cost0
+    mdy = np.where(m, 0, mdy)
+    mdx = np.where(m, 0, mdx)
+    sdy = np.where(m, 0.0, sdy)
+    sdx = np.where(m, 0.0, sdx)
+    # MotionConfidence on the IRE scale from exact integer sums: the biased
+    # SSD at the chosen vector and the tile statistics of A
+    ssd = _tile_sums((A - _shifted_tiles(B, mdy, mdx, block)) ** 2, block, th, tw)
+    l1 = np.abs(mdy) + np.abs(mdx)
+    npx = _tile_sums(np.ones_like(A), block, th, tw).astype(np.float64)
+    s1 = _tile_sums(A, block, th, tw).astype(np.float64)
+    s2 = _tile_sums(A * A, block, th, tw).astype(np.float64)
+    sc2 = float(QUANT_SCALE) * float(QUANT_SCALE)
+    bestv = (ssd * (50 + l1)).astype(np.float64) / (50.0 * sc2)
+    norm = 1.0 / np.maximum(1.0, npx)
+    tmean = s1 * norm
+    tvar = (s2 * norm - tmean * tmean) / sc2
+    energy = (tvar + 1.0) * np.maximum(1.0, npx)
+    conf = np.clip(1.0 - bestv / energy, 0.0, 1.0)
+    ratios = bestv / np.maximum(1.0, npx)
+    v = np.sort(ratios.ravel())
+    k = v.size // 2
+    med = v[k] if v.size % 2 else 0.5 * (v[k] + v[k - 1])
+    excess = np.maximum(0.0, ratios - med)
+    conf = conf * ((med + 1.0) / (med + 1.0 + excess))
+    conf = conf * (6.0 / (6.0 + med))
+    dy = (mdy.astype(np.float64) + sdy).astype(np.float32)
+    dx = (mdx.astype(np.float64) + sdx).astype(np.float32)
+    return dy, dx, conf.astype(np.float32)
+
+
 def _median3(v):
     """Median3 (temporal.cpp:20-41): 3x3 edge-padded median; < 3 tiles: copy."""
     th, tw = v.shape
@@ -971,11 +1107,16 @@ def decode_window_temporal(fields_ire, parities, g, cfg, strength):
                 k = j + o
                 if k < 0 or k >= nf:
                     continue
-                dy, dx, conf = estimate_motion(state[k][0], Yj, cfg.mc_tile, cfg.mc_search)
-                vdy, vdx = vectors_per_pixel(dy, dx, cfg.mc_tile, h, w)
+                if getattr(cfg, "me_mode", 0) == 1:
+                    tile = cfg.me_block
+                    dy, dx, conf = estimate_motion_sad(state[k][0], Yj, cfg.me_block, cfg.me_range)
+                else:
+                    tile = cfg.mc_tile
+                    dy, dx, conf = estimate_motion(state[k][0], Yj, cfg.mc_tile, cfg.mc_search)
+                vdy, vdx = vectors_per_pixel(dy, dx, tile, h, w)
                 comp = warp_by_tiles(obs[k].s, vdy, vdx)
                 car = warp_by_tiles(obs[k].carrier, vdy, vdx)
-                cf = upsample_confidence(conf, cfg.mc_tile, h, w, fast=bool(cfg.fast))
+                cf = upsample_confidence(conf, tile, h, w, fast=bool(cfg.fast))
                 if o & 1:
                     if gate is None:
                         gate = envelope_gate(Yj, chij, eps_t, cfg.odd_gate_floor)

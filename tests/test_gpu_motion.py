@@ -41,3 +41,28 @@ def test_motion_full_field_vs_reference(ctx, std, tile, search):
     # FP64 oracle: same vectors up to float rounding of the sub-pel fit
     agree = (np.abs(ody - dy) < 1e-3) & (np.abs(odx - dx) < 1e-3)
     assert agree.mean() > 0.95
+
+
+def _sad_pair(kind):
+    if kind == "ntsc" or kind == "pal":
+        std = _cabi.STD_NTSC if kind == "ntsc" else _cabi.STD_PAL
+        seq = synth.make_sequence(9 + std, std, 3, moving=True)
+        return seq[0].y_true.astype(np.float32), seq[2].y_true.astype(np.float32)
+    rng = np.random.default_rng(17)
+    a = (rng.normal(50, 25, size=(37, 53))).astype(np.float32)
+    b = np.roll(a, (2, -3), axis=(0, 1)) + rng.normal(0, 1, size=a.shape).astype(np.float32)
+    return a, b.astype(np.float32)
+
+
+@pytest.mark.parametrize("kind,block,rng_", [("ntsc", 16, 16), ("pal", 16, 16), ("odd", 16, 5),
+                                             ("odd", 8, 7), ("ntsc", 32, 22)])
+def test_sad_motion_bit_exact_vs_restatement(ctx, kind, block, rng_):
+    """Integer-SAD mode (me_mode 1) against its CPU restatement: identical
+    vectors, sub-pel offsets and confidences, including partial edge
+    blocks and ties."""
+    a, b = _sad_pair(kind)
+    dy, dx, cf = ctx.estimate_motion(a, b, block, rng_, me_mode=1)
+    ody, odx, ocf = O.estimate_motion_sad(a, b, block, rng_)
+    assert np.array_equal(dy, ody)
+    assert np.array_equal(dx, odx)
+    assert np.array_equal(cf, ocf)

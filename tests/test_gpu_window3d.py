@@ -41,3 +41,26 @@ def test_window_temporal_vs_reference(ctx, std, fast):
               f"  vs-ref Y {psnr(outs[j].luma, ys[j]):.1f} dB")
         assert abs(pg - pr) < 0.05
         assert abs(cg - cr) < 0.05
+
+
+def test_window_temporal_integer_sad_me_vs_oracle(ctx):
+    """The 3-D window with the integer-SAD motion mode (me_mode 1, 16 x 16
+    blocks, +-16) against the FP64 oracle running the same mode: PSNR against
+    ground truth within 0.05 dB per field."""
+    std, nf = _cabi.STD_NTSC, 4
+    seq = synth.make_sequence(31, std, nf, noise_sigma=1.0, moving=True)
+    g = _cabi.default_geometry(std)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6,
+                             temporal_strength=0.5, passes=1, nr_anchor=0.0, coherence_gate=0.0,
+                             trajectory_fit=0, me_mode=1, me_block=16, me_range=16)
+    outs = ctx.decode_field_window([api.Field(f.samples, g, parity=f.parity) for f in seq], cfg)
+    ref = O.decode_window_temporal([synth.to_ire(f.samples) for f in seq], [f.parity for f in seq],
+                                   g, cfg, 0.5)
+    for j in range(nf):
+        pg = psnr(outs[j].luma, seq[j].y_true)
+        po = psnr(ref[j][0], seq[j].y_true)
+        cg = psnr(outs[j].chroma, seq[j].chi_true)
+        co = psnr(ref[j][1], seq[j].chi_true)
+        print(f"sad-me field {j}: Y gpu {pg:.3f} oracle {po:.3f}  C gpu {cg:.3f} oracle {co:.3f}")
+        assert abs(pg - po) < 0.05
+        assert abs(cg - co) < 0.05

@@ -152,6 +152,44 @@ def test_motion_recovers_shift():
     assert np.abs(dx[inner][conf] + 2).max() <= 0.6
 
 
+def test_sad_motion_recovers_integer_shift():
+    """Integer-SAD mode (me_mode 1): an integer (3, -5) shift of a textured
+    plane is found exactly on interior blocks, with |sub-pel| <= 0.5."""
+    rng = np.random.default_rng(12)
+    h, w = 96, 128
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    tex = (40 * np.sin(yy * 0.31) * np.cos(xx * 0.27) + 15 * np.sin(xx * 0.23 + yy * 0.17)
+           + rng.uniform(-10, 10, size=(h, w)) + 50).astype(np.float32)
+    cur = tex[np.clip(np.arange(h) - 3, 0, h - 1)][:, np.clip(np.arange(w) + 5, 0, w - 1)]
+    dy, dx, cf = O.estimate_motion_sad(tex, cur, 16, 8)
+    inner = (slice(1, -1), slice(1, -1))
+    assert np.array_equal(np.round(dy[inner]), np.full_like(dy[inner], 3))
+    assert np.array_equal(np.round(dx[inner]), np.full_like(dx[inner], -5))
+    assert np.abs(dy - np.round(dy)).max() <= 0.5 and np.abs(dx - np.round(dx)).max() <= 0.5
+    assert cf[inner].min() > 0.0
+
+
+def test_sad_motion_ties_pick_zero_first():
+    """Strict-less update in centre-out order: on a flat plane every
+    candidate ties and the zero vector (visited first) is kept."""
+    a = np.full((40, 56), 37.25, np.float32)
+    dy, dx, _ = O.estimate_motion_sad(a, a, 16, 6)
+    assert not dy.any() and not dx.any()
+
+
+def test_sad_quantise_and_integer_blur():
+    """0 IRE -> 16384, 100 IRE -> 51200, clamped to uint16; the integer
+    blur is the zero-padded 5 x 5 box sum with rounded division."""
+    q = O.quantise_luma(np.array([[0.0, 100.0, -100.0, 200.0]], np.float32))
+    assert q.tolist() == [[16384, 51200, 0, 65535]]
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 65536, size=(19, 23))
+    b = O.box_blur_int(a, 2)
+    p = np.pad(a, 2)
+    naive = np.array([[p[y:y + 5, x:x + 5].sum() for x in range(23)] for y in range(19)])
+    assert np.array_equal(b, (naive + 12) // 25)
+
+
 def test_lossless_identity():
     """lossless_identity_test.cpp:40-101: init and refine keep
     |S - Y - Re[chi c]| < 1e-3."""
