@@ -21,6 +21,7 @@
 #include "hvdg.h"
 #include "hvdg_internal.h"
 #include "hvdg_host.h"
+#include "k_adjoint.h"
 #include "k_init.h"
 #include "k_motion.h"
 #include "k_temporal.h"
@@ -705,6 +706,36 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
   return HVDG_OK;
 }
 
+// Holographic-init kernel arguments for a staged batch (variants chi1 / chi2
+// land in G0 / D0, the blend in X0 and Y).
+hvdg::InitArgs init_args(hvdg_ctx* ctx, const Staged& S) {
+  const Batch& b = S.b;
+  const Layout& L = b.L;
+  hvdg::InitArgs ia;
+  ia.fields = at<FieldDesc>(ctx, L.o_fields);
+  ia.geoms = at<GeomDesc>(ctx, L.o_geoms);
+  ia.S = at<float>(ctx, L.o_S);
+  ia.line_phasor = at<float4>(ctx, L.o_lineph);
+  ia.col_phasor = at<float2>(ctx, L.o_colph);
+  ia.khat = at<float2>(ctx, L.o_khat);
+  ia.tw_row = at<float2>(ctx, L.o_twr);
+  ia.tw_col = at<float2>(ctx, L.o_twc);
+  ia.rowbuf = at<float2>(ctx, L.o_rowbuf);
+  ia.rowbuf_off = at<int64_t>(ctx, S.it_rbo);
+  ia.chi1 = at<float2>(ctx, L.o_G0);
+  ia.chi2 = at<float2>(ctx, L.o_D0);
+  ia.chi0 = at<float2>(ctx, L.o_X0);
+  ia.Y = at<float>(ctx, L.o_Y);
+  const int* itb = at<int>(ctx, S.it_itab);
+  ia.prow_field = itb + b.it_prow_field;
+  ia.prow_first = itb + b.it_prow_first;
+  ia.cgrp_field = itb + b.it_cgrp_field;
+  ia.cgrp_first = itb + b.it_cgrp_first;
+  ia.btile_field = itb + b.it_btile_field;
+  ia.btile_first = itb + b.it_btile_first;
+  return ia;
+}
+
 // Lock-in (or caller phases), crop (or caller S), caller chi0, holographic init.
 hvdg_status stage_prepare(hvdg_ctx* ctx, Staged& S, const RunOpts& opt) {
   const Batch& b = S.b;
@@ -764,28 +795,7 @@ hvdg_status stage_prepare(hvdg_ctx* ctx, Staged& S, const RunOpts& opt) {
     if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D chi0");
   }
   if (opt.do_init) {
-    hvdg::InitArgs ia;
-    ia.fields = at<FieldDesc>(ctx, L.o_fields);
-    ia.geoms = at<GeomDesc>(ctx, L.o_geoms);
-    ia.S = at<float>(ctx, L.o_S);
-    ia.line_phasor = at<float4>(ctx, L.o_lineph);
-    ia.col_phasor = at<float2>(ctx, L.o_colph);
-    ia.khat = at<float2>(ctx, L.o_khat);
-    ia.tw_row = at<float2>(ctx, L.o_twr);
-    ia.tw_col = at<float2>(ctx, L.o_twc);
-    ia.rowbuf = at<float2>(ctx, L.o_rowbuf);
-    ia.rowbuf_off = at<int64_t>(ctx, S.it_rbo);
-    ia.chi1 = at<float2>(ctx, L.o_G0);
-    ia.chi2 = at<float2>(ctx, L.o_D0);
-    ia.chi0 = at<float2>(ctx, L.o_X0);
-    ia.Y = at<float>(ctx, L.o_Y);
-    const int* itb = at<int>(ctx, S.it_itab);
-    ia.prow_field = itb + b.it_prow_field;
-    ia.prow_first = itb + b.it_prow_first;
-    ia.cgrp_field = itb + b.it_cgrp_field;
-    ia.cgrp_first = itb + b.it_cgrp_first;
-    ia.btile_field = itb + b.it_btile_field;
-    ia.btile_first = itb + b.it_btile_first;
+    const hvdg::InitArgs ia = init_args(ctx, S);
     hvdg::launch_init(ia, L.total_prows, L.total_cgroups, L.total_btiles, s);
     S.launches += 3;
   }
@@ -1837,6 +1847,269 @@ hvdg_status estimate_motion_sad(hvdg_ctx* ctx, const float* y_ref, const float* 
   return HVDG_OK;
 }
 
+// Decode adjoint of one 2-D field (no reference counterpart): forward with
+// the IRLS iterates checkpointed (one solver launch per outer, so chi_o and
+// the weights W(chi_o) can be kept), then the reverse sweep over the outers
+// (an adjoint CG solve per outer in the same persistent solver, weights
+// frozen, right-hand side injected as a constant gradient term), then the
+// HolographicInit adjoint and the crop / level transposes.
+hvdg_status decode_adjoint_field(hvdg_ctx* ctx, const hvdg_field_in& fi, const hvdg_config& cfg,
+                                 const float* y_bar, const float* chi_bar, float* samples_bar,
+                                 double* scalar_bar, int adj_iters, hvdg_field_out* out,
+                                 hvdg_diag* diag) {
+  const hvdg_geometry& g = *fi.geometry;
+  const int h = last_active_line(g) - g.first_active_field_line;
+  const int w = g.active_video_end - g.active_video_start;
+  const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
+  const int pad = std::min(hvdg::kInitPad, h - 1 > 0 ? h - 1 : 0);
+  const int hp = h + 2 * pad;
+  const int64_t plane = (int64_t)h * pitch;
+  const int64_t rplane = (int64_t)hp * pitch;
+  // the forward's budget, one outer per solver launch
+  const int n_outer = std::max(1, fi.irls_outer > 0 ? fi.irls_outer : cfg.irls_outer);
+  const int cg_cfg = fi.cg_iterations >= 0 ? fi.cg_iterations : cfg.cg_iterations;
+  const int cg_total = cfg.fast ? cg_cfg * 2 / 3 : cg_cfg;
+  const int n_inner = std::max(1, cg_total / n_outer);
+  hvdg_config c1 = cfg;
+  c1.irls_outer = 1;
+  c1.cg_iterations = n_inner;
+  c1.fast = 0;
+  c1.cg_tol = cfg.cg_tol > 0.0f ? cfg.cg_tol : (cfg.fast ? 0.10f : 0.02f);
+  hvdg_field_in f1 = fi;
+  f1.irls_outer = 1;
+  f1.cg_iterations = n_inner;
+  hvdg::AdjGeom ag;
+  ag.h = h;
+  ag.w = w;
+  ag.pitch = pitch;
+  ag.hp = hp;
+  ag.pad = pad;
+  const int nb = hvdg::adj_blocks(ag);
+  size_t xo = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = xo;
+    xo = align_up(xo + bytes, 256);
+    return r;
+  };
+  const size_t x_ck = take(sizeof(float2) * plane * (n_outer + 1));
+  const size_t x_wk = take(sizeof(float4) * plane * n_outer);
+  const size_t x_cv = take(sizeof(float2) * plane * 2);
+  const size_t x_zero = take(sizeof(float) * plane);
+  const size_t x_B = take(sizeof(float2) * plane);
+  const size_t x_yb = take(sizeof(float) * plane);
+  const size_t x_cb = take(sizeof(float2) * plane);
+  const size_t x_sb = take(sizeof(float) * plane);
+  const size_t x_pa = take(sizeof(float2) * plane * 4);
+  const size_t x_ai = take(sizeof(float2) * plane * 5);
+  const size_t x_ain = take(sizeof(float2) * rplane * 2);
+  const size_t x_aout = take(sizeof(float2) * rplane * 2);
+  const size_t x_part = take(sizeof(double) * 4 * nb);
+  const size_t x_acc = take(sizeof(double) * 4);
+  const size_t x_smp = take(sizeof(float) * (size_t)g.field_height * g.field_width);
+  RunOpts opt;
+  Staged S;
+  hvdg_status st = stage_upload(ctx, &f1, 1, &c1, opt, xo, S);
+  if (st != HVDG_OK) return st;
+  const Layout& L = S.b.L;
+  auto X = [&](size_t off) { return S.extra + off; };
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  st = stage_prepare(ctx, S, opt);
+  if (st != HVDG_OK) return st;
+  ag.line_phasor = at<float4>(ctx, L.o_lineph);
+  ag.col_phasor = at<float2>(ctx, L.o_colph);
+  float2* ck = at<float2>(ctx, X(x_ck));
+  float4* wk = at<float4>(ctx, X(x_wk));
+  float2* cv = at<float2>(ctx, X(x_cv));
+  // init variants and chi_0 (before the solver reuses G0 / D0)
+  e = cudaMemcpyAsync(cv, at<float2>(ctx, L.o_G0), sizeof(float2) * plane, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(cv + plane, at<float2>(ctx, L.o_D0), sizeof(float2) * plane,
+                        cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ck, at<float2>(ctx, L.o_X0), sizeof(float2) * plane, cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint checkpoints");
+  hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), 1, at<float2>(ctx, L.o_X0), s);
+  // ---- forward, one outer per launch ----
+  hvdg::SolverArgs sa = solver_args(ctx, S);
+  const int grid = solver_grid(ctx, L.total_units);
+  int cg_run = 0;
+  for (int o = 0; o < n_outer; ++o) {
+    stage_reset(ctx, S);
+    e = hvdg::launch_solver(sa, grid, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint forward solver");
+    e = cudaMemcpyAsync(ck + (o + 1) * plane, at<float2>(ctx, L.o_X0), sizeof(float2) * plane,
+                        cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(wk + o * plane, at<float4>(ctx, L.o_W), sizeof(float4) * plane,
+                          cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint checkpoints");
+    FieldCtl ctl;
+    int flags[4];
+    e = cudaMemcpyAsync(&ctl, at<FieldCtl>(ctx, L.o_ctl), sizeof(ctl), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(flags, at<int>(ctx, L.o_flags), sizeof(flags), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint forward");
+    if (flags[1]) {
+      ctx->last_error = "non-finite input samples";
+      return HVDG_ERR_NONFINITE_INPUT;
+    }
+    if (flags[0]) {
+      ctx->last_error = "device-side bounded wait expired in the solver";
+      return HVDG_ERR_DEVICE_TIMEOUT;
+    }
+    cg_run += ctl.cg_iters;
+  }
+  if (out && (out->luma || out->chroma)) {
+    if (out->luma)
+      e = cudaMemcpy2DAsync(out->luma, sizeof(float) * w, at<float>(ctx, L.o_Y), sizeof(float) * pitch,
+                            sizeof(float) * w, h, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && out->chroma)
+      e = cudaMemcpy2DAsync(out->chroma, sizeof(float2) * w, at<float2>(ctx, L.o_X0),
+                            sizeof(float2) * pitch, sizeof(float2) * w, h, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint forward outputs");
+  }
+  // ---- reverse sweep ----
+  FieldDesc fd;
+  e = cudaMemcpyAsync(&fd, at<FieldDesc>(ctx, L.o_fields), sizeof(fd), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint field descriptor");
+  hvdg::AdjScalars sc;
+  sc.eps = cfg.charbonnier_eps;
+  sc.eps_c = cfg.chroma_eps;
+  sc.k = cfg.structure_coupling;
+  sc.mu_h = fd.mu_h;
+  sc.mu_v = fd.mu_v;
+  sc.aniso = cfg.lambda_c != 0.0f ? fd.mu_h / cfg.lambda_c : 1.0f;
+  FieldDesc fa = fd;
+  fa.n_outer = 1;
+  fa.n_inner = adj_iters;
+  fa.n_phases = 2 + adj_iters + 1;
+  fa.cg_tol = 1e-6f;
+  fa.adj_flags = hvdg::kAdjFixedW | hvdg::kAdjExtB;
+  fa.has_nbr = 0;
+  float* zero = at<float>(ctx, X(x_zero));
+  float2* B = at<float2>(ctx, X(x_B));
+  float* yb = at<float>(ctx, X(x_yb));
+  float2* cb = at<float2>(ctx, X(x_cb));
+  float* sb = at<float>(ctx, X(x_sb));
+  float2* pa = at<float2>(ctx, X(x_pa));
+  double* part = at<double>(ctx, X(x_part));
+  double* acc = at<double>(ctx, X(x_acc));
+  e = cudaMemsetAsync(zero, 0, sizeof(float) * plane, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(yb, 0, sizeof(float) * plane, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cb, 0, sizeof(float2) * plane, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(double) * 4, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(yb, sizeof(float) * pitch, y_bar, sizeof(float) * w, sizeof(float) * w, h,
+                          cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(cb, sizeof(float2) * pitch, chi_bar, sizeof(float2) * w,
+                          sizeof(float2) * w, h, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(at<FieldDesc>(ctx, L.o_fields), &fa, sizeof(fa), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint cotangents");
+  hvdg::launch_adj_output(ag, yb, sb, cb, s);
+  hvdg::SolverArgs sadj = sa;
+  sadj.S = zero;
+  sadj.B = B;
+  sadj.n_phases = fa.n_phases;
+  std::vector<double> np(nb);
+  int adj_run = 0;
+  for (int o = n_outer - 1; o >= 0; --o) {
+    // scale the right-hand side to unit rms (the solver's absolute exit is
+    // relative to the field size)
+    hvdg::launch_adj_norm(ag, cb, part, s);
+    e = cudaMemcpyAsync(np.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint norm");
+    double ss = 0.0;
+    for (int i = 0; i < nb; ++i) ss += np[i];
+    if (!(ss > 0.0)) {
+      // zero cotangent: every contribution of this and earlier outers is zero
+      break;
+    }
+    const float sigma = (float)(1.0 / std::sqrt(ss / ((double)h * w)));
+    hvdg::launch_adj_rhs(ag, cb, sigma, B, s);
+    e = cudaMemcpyAsync(at<float4>(ctx, L.o_W), wk + o * plane, sizeof(float4) * plane,
+                        cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(at<float2>(ctx, L.o_X0), 0, sizeof(float2) * plane, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint solve setup");
+    stage_reset(ctx, S);
+    e = hvdg::launch_solver(sadj, grid, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint solver");
+    hvdg::AdjOuter ao;
+    ao.S = at<float>(ctx, L.o_S);
+    ao.lam = at<float2>(ctx, L.o_X0);
+    ao.inv_sigma = 1.0f / sigma;
+    ao.chi1 = ck + (o + 1) * plane;
+    ao.chi0 = ck + o * plane;
+    ao.W = wk + o * plane;
+    ao.P = pa;
+    ao.GB = pa + plane;
+    ao.A1 = pa + 2 * plane;
+    ao.A2 = pa + 3 * plane;
+    ao.partials = part;
+    hvdg::launch_adj_outer(ag, sc, ao, acc, sb, cb, s);
+    FieldCtl ctl;
+    int flags[4];
+    e = cudaMemcpyAsync(&ctl, at<FieldCtl>(ctx, L.o_ctl), sizeof(ctl), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(flags, at<int>(ctx, L.o_flags), sizeof(flags), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint outer");
+    if (flags[0]) {
+      ctx->last_error = "device-side bounded wait expired in the adjoint solver";
+      return HVDG_ERR_DEVICE_TIMEOUT;
+    }
+    adj_run += ctl.cg_iters;
+  }
+  // ---- HolographicInit adjoint (chibar now holds the cotangent of chi_0) ----
+  float2* ai = at<float2>(ctx, X(x_ai));
+  float2* ain = at<float2>(ctx, X(x_ain));
+  float2* aout = at<float2>(ctx, X(x_aout));
+  hvdg::AdjInit ia;
+  ia.S = at<float>(ctx, L.o_S);
+  ia.chi1 = cv;
+  ia.chi2 = cv + plane;
+  ia.chi0bar = cb;
+  ia.a = ai;
+  ia.tmp = ai + plane;
+  ia.ebar = ai + 2 * plane;
+  ia.cb1 = ai + 3 * plane;
+  ia.cb2 = ai + 4 * plane;
+  ia.adj_in = ain;
+  e = cudaMemsetAsync(ain, 0, sizeof(float2) * rplane * 2, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint init setup");
+  hvdg::launch_adj_init_pointwise(ag, ia, sb, s);
+  hvdg::InitArgs fa_init = init_args(ctx, S);
+  fa_init.adj_in = ain;
+  fa_init.adj_out = aout;
+  hvdg::launch_init_filter_adjoint(fa_init, L.total_prows, L.total_cgroups, s);
+  hvdg::launch_adj_fold(ag, aout, sb, s);
+  const float cpi = fi.sample_type == HVDG_SAMPLES_F32_IRE
+                        ? 1.0f
+                        : (fi.white_level - fi.blanking_level) / 100.0f;
+  float* smp = at<float>(ctx, X(x_smp));
+  hvdg::launch_adj_samples(ag, sb, 1.0f / cpi, g.field_height, g.field_width,
+                           g.first_active_field_line, g.active_video_start, smp, s);
+  double accv[4];
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(samples_bar, smp, sizeof(float) * (size_t)g.field_height * g.field_width,
+                        cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(accv, acc, sizeof(accv), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adjoint outputs");
+  for (int i = 0; i < 4; ++i) scalar_bar[i] += accv[i];
+  if (diag) {
+    diag->cg_iterations_run += cg_run + adj_run;
+    diag->kernel_launches += 8 + n_outer * 6 + 12;
+  }
+  return HVDG_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -2334,6 +2607,37 @@ hvdg_status hvdg_variational_refine(hvdg_ctx* ctx, const float* s, const float* 
   opt.vswitch_in = vswitch_active;
   opt.chi0_in = chi0;
   return run_batch(ctx, &fi, 1, cfg, &fo, nullptr, opt);
+}
+
+hvdg_status hvdg_decode_fields_adjoint(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                                       const hvdg_config* cfg, const float* const* y_bar,
+                                       const float* const* chi_bar, float* const* samples_bar,
+                                       double* scalar_bar, int adjoint_cg_iterations,
+                                       hvdg_field_out* out, hvdg_diag* diag) {
+  if (!ctx || !cfg || n < 0 || (n > 0 && (!fields || !y_bar || !chi_bar || !samples_bar)) ||
+      !scalar_bar)
+    return HVDG_ERR_BAD_ARGUMENT;
+  if (cfg->temporal_strength >= 0.0f) {
+    ctx->last_error = "the adjoint covers the 2-D decode (temporal_strength < 0)";
+    return HVDG_ERR_UNSUPPORTED;
+  }
+  if (cfg->diag_prior > 0.0f || cfg->symmetry_variant) return HVDG_ERR_UNSUPPORTED;
+  for (int i = 0; i < n; ++i) {
+    if (!fields[i].samples || !fields[i].geometry || !y_bar[i] || !chi_bar[i] || !samples_bar[i])
+      return HVDG_ERR_BAD_ARGUMENT;
+    const hvdg_status st = check_geometry(fields[i].geometry);
+    if (st != HVDG_OK) return st;
+  }
+  cudaSetDevice(ctx->device);
+  const int iters = adjoint_cg_iterations > 0 ? adjoint_cg_iterations : 300;
+  for (int i = 0; i < 4; ++i) scalar_bar[i] = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const hvdg_status st = decode_adjoint_field(ctx, fields[i], *cfg, y_bar[i], chi_bar[i],
+                                                samples_bar[i], scalar_bar, iters,
+                                                out ? &out[i] : nullptr, diag);
+    if (st != HVDG_OK) return st;
+  }
+  return HVDG_OK;
 }
 
 }  // extern "C"

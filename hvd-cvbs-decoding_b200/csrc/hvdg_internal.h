@@ -47,8 +47,15 @@ struct FieldDesc {
   int unit_begin;      // first solver unit of this field
   int unit_count;      // number of solver units
   int n_phases;        // n_outer * (2 + n_inner) + 1
-  int pad0;
+  int adj_flags;       // adjoint solves: kAdjFixedW | kAdjExtB (0 for decodes)
 };
+
+// FieldDesc::adj_flags. kAdjFixedW: the R phase keeps the weights already in
+// W (the forward's lagged weights) instead of recomputing them from chi;
+// kAdjExtB: the G phase adds the constant plane B (the adjoint right-hand
+// side) to the gradient.
+constexpr int kAdjFixedW = 1;
+constexpr int kAdjExtB = 2;
 
 // Per-geometry init tables.
 struct GeomDesc {

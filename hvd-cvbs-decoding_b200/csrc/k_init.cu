@@ -119,6 +119,26 @@ __global__ void __launch_bounds__(256) k_init_rows(InitArgs a) {
   const GeomDesc gd = a.geoms[f.geom];
   const int yp = r - a.prow_first[f_idx];
   const int sy = mirror_row(yp - gd.pad, f.h);
+  if (a.adj_in) {
+    // adjoint mode: each variant filters its own input row
+    for (int v = 0; v < 2; ++v) {
+      const float2* in = a.adj_in + a.rowbuf_off[f_idx] + ((int64_t)v * gd.hp + yp) * f.pitch;
+      for (int i = threadIdx.x; i < kRowFft; i += blockDim.x)
+        P[i] = i < f.w ? in[i] : make_float2(0.f, 0.f);
+      __syncthreads();
+      float2* sp = fft_stockham<kRowFft, false>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+      const float2* kh = a.khat + gd.khat_row_off + v * kRowFft;
+      float2* oth = sp == P ? Q : P;
+      for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) oth[i] = cmul(sp[i], __ldg(kh + i));
+      __syncthreads();
+      float2* res = fft_stockham<kRowFft, true>(oth, sp, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+      float2* out = a.rowbuf + a.rowbuf_off[f_idx] + ((int64_t)v * gd.hp + yp) * f.pitch;
+      for (int i = threadIdx.x; i < f.pitch; i += blockDim.x)
+        out[i] = i < f.w ? res[i] : make_float2(0.f, 0.f);
+      __syncthreads();
+    }
+    return;
+  }
   const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
   for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) {
     float2 v = make_float2(0.f, 0.f);
@@ -179,11 +199,20 @@ __global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
     if (res != A)
       for (int i = lane; i < kColFft; i += 32) A[i] = res[i];
     __syncthreads();
-    float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
-    for (int i = threadIdx.x; i < f.h * kColGroup; i += blockDim.x) {
-      const int y = i / kColGroup, c = i % kColGroup;
-      if (x0 + c < f.w)
-        dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * kColFft + y + gd.pad];
+    if (a.adj_out) {
+      // adjoint mode: every padded row (the transposed crop)
+      float2* dst = a.adj_out + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
+      for (int i = threadIdx.x; i < gd.hp * kColGroup; i += blockDim.x) {
+        const int y = i / kColGroup, c = i % kColGroup;
+        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * kColFft + y];
+      }
+    } else {
+      float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
+      for (int i = threadIdx.x; i < f.h * kColGroup; i += blockDim.x) {
+        const int y = i / kColGroup, c = i % kColGroup;
+        if (x0 + c < f.w)
+          dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * kColFft + y + gd.pad];
+      }
     }
     __syncthreads();
   }
@@ -356,6 +385,19 @@ void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int tota
   if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
   if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
   if (total_btiles > 0) k_init_blend<<<total_btiles, 256, 0, st>>>(a);
+}
+
+void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cgroups,
+                                cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    configure_init_kernels();
+    configured = true;
+  }
+  const int row_smem = 3 * kRowFft * sizeof(float2);
+  const int col_smem = kColGroup * 2 * kColFft * sizeof(float2);
+  if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
+  if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
 }
 
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {

@@ -29,11 +29,22 @@ struct InitArgs {
   const int* cgrp_first;       // field -> first column group
   const int* btile_field;      // blend tile -> field
   const int* btile_first;      // field -> first blend tile
+  // Adjoint mode (both non-null): the rows pass filters the two variant
+  // planes of adj_in (per field at rowbuf_off, 2 x hp x pitch, pad rows
+  // included) instead of the demodulated composite, and the columns pass
+  // writes all hp filtered rows of each variant to adj_out (same layout)
+  // instead of the cropped chi1 / chi2. The filters are real and even, so
+  // this applies the adjoint of the forward crop (the x2 included).
+  const float2* adj_in = nullptr;
+  float2* adj_out = nullptr;
 };
 
 void configure_init_kernels();
 void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
                  cudaStream_t st);
+// Adjoint of the two row / column filter passes (rows, then columns; no blend).
+void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cgroups,
+                                cudaStream_t st);
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st);
 int aniso_max_samples();
 int init_col_group();

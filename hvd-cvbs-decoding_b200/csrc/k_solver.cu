@@ -136,6 +136,22 @@ __device__ __noinline__ void phase_reweight(const SolverArgs& A, const FieldDesc
   float4* W = A.W + base;
   const bool pend = c.pending != 0;
   const float alpha = c.alpha;
+  if (f.adj_flags & kAdjFixedW) {
+    // weights given: only apply the pending step into the other chi buffer
+    for (int y = u.y0; y < u.y1; ++y) {
+      const int64_t o = (int64_t)y * f.pitch + l.xa;
+      float2 xa, xb;
+      ld_pair(X + o, xa, xb);
+      if (pend) {
+        float2 da, db;
+        ld_pair(D + o, da, db);
+        xa = cadd(xa, cscale(da, alpha));
+        xb = cadd(xb, cscale(db, alpha));
+      }
+      st_pair(Xo + o, xa, xb, l.va, l.vb);
+    }
+    return;
+  }
   const float eps = f.eps, epsc = f.eps_c, k = f.k_coupling;
   const float e2 = eps * eps, ec2 = epsc * epsc;
   RRow cur, nxt;
@@ -327,6 +343,11 @@ __device__ __noinline__ double phase_gradient(const SolverArgs& A, const FieldDe
       oa.y += Ma.y * cur.ua.x + Ma.z * cur.ua.y;
       ob.x += Mb.x * cur.ub.x + Mb.y * cur.ub.y;
       ob.y += Mb.y * cur.ub.x + Mb.z * cur.ub.y;
+      float2 ba, bb;
+      ld_pair(A.B + base + o, ba, bb);
+      oa = cadd(oa, ba);
+      ob = cadd(ob, bb);
+    } else if (f.adj_flags & kAdjExtB) {
       float2 ba, bb;
       ld_pair(A.B + base + o, ba, bb);
       oa = cadd(oa, ba);

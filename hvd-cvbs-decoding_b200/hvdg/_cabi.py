@@ -345,3 +345,6 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_estimate_motion.restype = C.c_int
     lib.hvdg_holographic_init_noalloc.argtypes = [vp, vp, vp, P(Geometry), vp, vp]
     lib.hvdg_holographic_init_noalloc.restype = C.c_int
+    lib.hvdg_decode_fields_adjoint.argtypes = [vp, P(FieldIn), C.c_int, P(Config), P(vp), P(vp),
+                                               P(vp), P(C.c_double), C.c_int, P(FieldOut), P(Diag)]
+    lib.hvdg_decode_fields_adjoint.restype = C.c_int

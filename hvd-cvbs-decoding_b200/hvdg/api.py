@@ -184,6 +184,39 @@ class Context:
         self._check(st, "hvdg_decode_fields_device")
         return d
 
+    def decode_fields_adjoint(self, fields, cfg: Config, y_bar, chi_bar,
+                              adjoint_cg_iterations: int = 0, want_forward: bool = False):
+        """Gradients of a scalar loss through the 2-D decode of `fields`
+        (hvdg_decode_fields_adjoint). y_bar[i] / chi_bar[i]: the loss
+        cotangents of field i's decoded luma (float) and chroma (complex).
+        Returns (samples_bar, scalars, forward): samples_bar[i] is d loss /
+        d sample (field_height x field_width), scalars maps lambda_c,
+        charbonnier_eps, chroma_eps, structure_coupling to their gradients,
+        forward is the recomputed decode (list of Decoded) or None."""
+        arr, keep = self._build_fields(fields)
+        n = len(fields)
+        yb = [np.ascontiguousarray(a, np.float32) for a in y_bar]
+        cb = [np.ascontiguousarray(a, np.complex64) for a in chi_bar]
+        sb = [np.zeros((f.geometry.field_height, f.geometry.field_width), np.float32)
+              for f in fields]
+        for i, f in enumerate(fields):
+            shape = (f.geometry.active_lines, f.geometry.active_width)
+            if yb[i].shape != shape or cb[i].shape != shape:
+                raise ValueError(f"field {i}: cotangents must have shape {shape}")
+        ybp = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in yb])
+        cbp = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in cb])
+        sbp = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in sb])
+        sc = (C.c_double * 4)()
+        outs, res = (self._alloc_out(fields, False) if want_forward else (None, None))
+        self.last_diag = Diag()
+        st = self.lib.hvdg_decode_fields_adjoint(self._h, arr, n, C.byref(cfg), ybp, cbp, sbp, sc,
+                                                 int(adjoint_cg_iterations), outs,
+                                                 C.byref(self.last_diag))
+        self._check(st, "hvdg_decode_fields_adjoint")
+        del keep
+        names = ("lambda_c", "charbonnier_eps", "chroma_eps", "structure_coupling")
+        return sb, dict(zip(names, list(sc))), res
+
     # ---- kernel level --------------------------------------------------------
     def burst_lockin(self, field_ire: np.ndarray, g: Geometry):
         f = np.ascontiguousarray(field_ire, dtype=np.float32)

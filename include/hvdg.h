@@ -303,6 +303,35 @@ hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref,
                                  float* confidence);
 
 /* ------------------------------------------------------------------------ */
+/* Adjoint                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference (it has no adjoint): gradients of a scalar
+ * loss on the decoded planes, for research and training.
+ * For each field of a 2-D decode (lock-in, HolographicInit, IRLS + CG
+ * VariationalRefine, output luma; cfg->temporal_strength < 0), given the
+ * loss cotangents y_bar[i] (active_lines x active_width floats) and
+ * chi_bar[i] (active_lines x active_width x 2 floats) of the decoded Y and
+ * chi, writes samples_bar[i] (field_height x field_width floats): d loss /
+ * d sample value -- per code for integer samples, per IRE for float samples
+ * -- and sets scalar_bar[0..3] to the gradients with respect to
+ * cfg->lambda_c, charbonnier_eps, chroma_eps and structure_coupling, summed
+ * over the fields.
+ * The forward is recomputed with every IRLS iterate checkpointed. Each
+ * outer's quadratic is differentiated as solved exactly (implicit function:
+ * one adjoint CG solve of adjoint_cg_iterations, <= 0 = 300, on the same SPD
+ * operator per outer), so the result is exact when the forward's CG budget
+ * converges every outer. Held at their forward values (no gradient through
+ * them): the lock-in carrier phase and the chroma-anisotropy split; samples
+ * outside the active window therefore get zero gradient.
+ * out (optional, may be NULL): the recomputed forward's luma / chroma. */
+hvdg_status hvdg_decode_fields_adjoint(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                                       const hvdg_config* cfg, const float* const* y_bar,
+                                       const float* const* chi_bar, float* const* samples_bar,
+                                       double* scalar_bar, int adjoint_cg_iterations,
+                                       hvdg_field_out* out, hvdg_diag* diag);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free entry point                                               */
 /* ------------------------------------------------------------------------ */
 
