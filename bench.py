@@ -70,6 +70,28 @@ def workload(seed: int, name: str = "mixed64"):
     return synth.mixed_batch(seed, nn, npal, outer_range=outer, cg_per_outer=cg)
 
 
+def rank_workload(rank: int, name: str = "mixed64"):
+    """Each rank decodes its own batch (fields are independent: weak
+    scaling, no data-path collective)."""
+    return workload(1000 + rank, name)
+
+
+def max_over_ranks(values, dist, device):
+    """Element-wise max of per-rank timings (the slowest rank sets the job
+    time)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def throughput(fields_per_rank: int, steps: int, world: int, ms_total: float) -> float:
+    """Whole-job fields/s: every rank's fields over the slowest rank's time."""
+    return fields_per_rank * steps * world / (ms_total / 1000.0)
+
+
 def solver_config():
     from hvdg import api
     return api.default_config(fast=0, cg_tol=1e-6, temporal_strength=-1.0)
@@ -194,6 +216,136 @@ def reference_arm(args, rank, world):
     return 0
 
 
+# The other configurations of the path (parity cases; measured, not the
+# headline): one NTSC field; 16-field NTSC / PAL motion windows (3-D, integer
+# SAD motion, 10 x 50); the adjoint on 8 NTSC fields (10 x 50).
+CONFIGS = {
+    "cfg0-ntsc1": "config 0: 1 NTSC 910x263 uint16 field, 5 IRLS x 30 CG, no motion",
+    "cfg1-ntsc16-3d": "config 1: 16 NTSC fields (8 frames), moving rectangles, 3-D window "
+                      "(strength 0.5, 1 pass, no anchor / gate / trajectory fit), integer-SAD "
+                      "motion 16x16 +-16, 10 IRLS x 50 CG",
+    "cfg2-pal16-3d": "config 2: 16 PAL 1135x313 fields, same motion, window and solver as config 1",
+    "cfg4-adjoint8": "config 4: forward + adjoint of 8 NTSC fields, 10 IRLS x 50 CG, "
+                     "gradients w.r.t. 4 scalars and the samples",
+}
+
+
+def config_cfg(name):
+    from hvdg import api
+    if name == "cfg0-ntsc1":
+        return api.default_config(irls_outer=5, cg_iterations=150, fast=0, cg_tol=1e-6,
+                                  temporal_strength=-1.0)
+    if name in ("cfg1-ntsc16-3d", "cfg2-pal16-3d"):
+        return api.default_config(irls_outer=10, cg_iterations=500, fast=0, cg_tol=1e-6,
+                                  temporal_strength=0.5, passes=1, nr_anchor=0.0,
+                                  coherence_gate=0.0, trajectory_fit=0, me_mode=1, me_block=16,
+                                  me_range=16)
+    return api.default_config(irls_outer=10, cg_iterations=500, fast=0, cg_tol=1e-6,
+                              temporal_strength=-1.0)
+
+
+def config_fields(name):
+    from hvdg import _cabi, synth
+    if name == "cfg0-ntsc1":
+        return [synth.make_field(0, _cabi.STD_NTSC, 0.5)]
+    if name == "cfg1-ntsc16-3d":
+        return synth.make_sequence(101, _cabi.STD_NTSC, 16, noise_sigma=0.5, moving=True)
+    if name == "cfg2-pal16-3d":
+        return synth.make_sequence(102, _cabi.STD_PAL, 16, noise_sigma=0.5, moving=True)
+    return [synth.make_field(200 + i, _cabi.STD_NTSC, 0.5) for i in range(8)]
+
+
+def config_arm(args, rank, world):
+    """One JSON line for a parity configuration: fields/s through the public
+    API (host buffers, wall clock of the synchronous call, copies included)
+    and the device time of the same calls from the library's events."""
+    if rank != 0:
+        return 0
+    from hvdg import _cabi, api, synth
+    name = args.workload
+    cfg = config_cfg(name)
+    fields = config_fields(name)
+    geoms = [_cabi.default_geometry(f.standard) for f in fields]
+    hf = [api.Field(f.samples, g, parity=f.parity) for f, g in zip(fields, geoms)]
+    n = len(hf)
+    if args.impl == "reference":
+        from oracle import ref
+        if not ref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+            return 0
+        if name == "cfg4-adjoint8":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no adjoint (no CPU counterpart to time)"}))
+            return 0
+        threads = os.cpu_count() or 1
+        ref.set_threads(threads)
+        ires = [synth.to_ire(f.samples) for f in fields]
+        times = []
+        for _ in range(max(1, args.steps)):
+            t = time.perf_counter()
+            if name == "cfg0-ntsc1":
+                ref.decode_fields(ires, [f.parity for f in fields], geoms, [cfg] * n,
+                                  across_fields=False)
+            else:
+                ref.decode_field_window(ires, [f.parity for f in fields], geoms[0], cfg)
+            times.append(time.perf_counter() - t)
+        v = n * len(times) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": f"fields/s ({CONFIGS[name]})",
+                          "value": v, "unit": "fields/s", "n_gpus": world, "steps": len(times),
+                          "warmup": 0, "higher_is_better": True, "dtype": "f32",
+                          "data": "synthetic (seeded hvdg.synth)",
+                          "config": {"workload": CONFIGS[name],
+                                     "note": "the reference's float-SSD motion search "
+                                             "(it has no integer-SAD mode)" if "3d" in name else ""},
+                          "cpu_baseline": {"value": v, "unit": "fields/s", "cores": threads,
+                                           "kind": "reference", "sample": f"{n} fields per step"},
+                          "e2e": {"value": v, "unit": "fields/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return 0
+    ctx = api.Context(0)
+    extra = {}
+
+    def step():
+        if name == "cfg0-ntsc1":
+            out = ctx.decode_fields(hf, cfg)
+        elif name == "cfg4-adjoint8":
+            out = ctx.decode_fields(hf, cfg)
+            yb, cb = [], []
+            for d, f in zip(out, fields):
+                npx = d.luma.size
+                yb.append((2 * (d.luma - f.y_true) / npx).astype(np.float32))
+                cb.append((2 * (d.chroma - f.chi_true) / npx).astype(np.complex64))
+            ctx.decode_fields_adjoint(hf, cfg, yb, cb, 300)
+        else:
+            out = ctx.decode_field_window(hf, cfg)
+        return out
+
+    for _ in range(args.warmup):
+        step()
+    wall, dev = 0.0, 0.0
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        out = step()
+        wall += time.perf_counter() - t
+        dev += ctx.last_diag.ms_total
+    psnr = []
+    for d, f in zip(out, fields):
+        dd = d.luma.astype(np.float64) - f.y_true
+        psnr.append(10 * np.log10(100.0 ** 2 / np.mean(dd * dd)))
+    line = {"metric": f"fields/s ({CONFIGS[name]})", "value": n * args.steps / wall,
+            "unit": "fields/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded hvdg.synth)",
+            "config": {"workload": CONFIGS[name], "timing": "wall clock of the synchronous "
+                       "host-buffer call (uploads, kernels, downloads)"},
+            "device_ms_per_step_last_call": dev / args.steps if name != "cfg4-adjoint8" else None,
+            "psnr_y_db_mean": float(np.mean(psnr))}
+    line.update(extra)
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,13 +354,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS) + sorted(CONFIGS))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in CONFIGS:
+        return config_arm(args, rank, world)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
 
@@ -223,7 +377,7 @@ def main():
 
     from hvdg import _cabi, api
     cfg = solver_config()
-    fields = workload(1000 + rank, args.workload)
+    fields = rank_workload(rank, args.workload)
     ctx = api.Context(local)
 
     # ---- device-resident inputs / outputs ----
@@ -276,9 +430,7 @@ def main():
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     if dist is not None:
-        t = torch.tensor([ms_total, ms_solver], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total, ms_solver = float(t[0]), float(t[1])
+        ms_total, ms_solver = max_over_ranks([ms_total, ms_solver], dist, "cuda")
         dist.barrier()
 
     # ---- e2e through the host-buffer API (pinned in/out) ----
@@ -309,9 +461,7 @@ def main():
     h2d = sum(f.samples.nbytes for f in fields)
     d2h = sum(o.luma.nbytes + o.chroma.nbytes for o in out)
     if dist is not None:
-        tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt[0])
+        e2e_t = max_over_ranks([e2e_t], dist, "cuda")[0]
 
     # ---- plain one-field-per-launch path ----
     plain = None
@@ -326,13 +476,11 @@ def main():
             pt += ctx.decode_fields_device(fin, fout, n, cfg).ms_total
         ctx.set_batching(True)
         if dist is not None:
-            tt = torch.tensor([pt], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            pt = float(tt[0])
+            pt = max_over_ranks([pt], dist, "cuda")[0]
         plain = {"value": n * psteps * world / (pt / 1000.0), "unit": "fields/s",
                  "ms_per_step": pt / psteps}
 
-    value = n * args.steps * world / (ms_total / 1000.0)
+    value = throughput(n, args.steps, world, ms_total)
     peak, peak_kind = measured_peaks()
     alg_bytes_per_launch = (ALG_BYTES_ITER * pix_iters + ALG_BYTES_OUTER * pix_outers) / args.steps
     solver_s = ms_solver / 1000.0 / args.steps
