@@ -349,6 +349,29 @@ struct Batch {
 
 int elem_size(int sample_type) { return sample_type == HVDG_SAMPLES_F32_IRE ? 4 : 2; }
 
+// Solver band height when none is set: the tallest band (fewest halo rows)
+// that still gives every resident warp a unit of the fields solved
+// together; small batches (one field, one colour of a 3-D window) get short
+// bands, so a phase is not bound by one warp walking 32 rows.
+int auto_band_rows_hw(hvdg_ctx* ctx, const std::vector<std::pair<int, int>>& hw) {
+  const int warps = ctx->sm_count * std::max(1, hvdg::solver_max_blocks_per_sm()) *
+                    (hvdg::kSolverThreads / 32);
+  static const int cand[] = {32, 24, 16, 12, 8, 6, 4};
+  for (int band : cand) {
+    int64_t units = 0;
+    for (const auto& p : hw)
+      units += (int64_t)((p.second + hvdg::kStrip - 1) / hvdg::kStrip) * ((p.first + band - 1) / band);
+    if (units >= warps) return band;
+  }
+  return 4;
+}
+
+int auto_band_rows(hvdg_ctx* ctx, const std::vector<FieldPlan>& fp) {
+  std::vector<std::pair<int, int>> hw;
+  for (const FieldPlan& p : fp) hw.emplace_back(p.h, p.w);
+  return auto_band_rows_hw(ctx, hw);
+}
+
 hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
                        int band_rows, Batch& b) {
   b = Batch();
@@ -409,7 +432,7 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     ncol += t.w;
   }
   // per-field descriptors, units
-  const int band = band_rows > 0 ? band_rows : 32;
+  const int band = band_rows > 0 ? band_rows : auto_band_rows(ctx, b.fp);
   for (int i = 0; i < n; ++i) {
     const FieldPlan& p = b.fp[i];
     const hvdg_geometry& g = *p.g;
@@ -1247,9 +1270,29 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
     if (cfg.coherence_gate == 0.6f) cfg.coherence_gate = 1.0f;
     if (cfg.nr_radius == 2) cfg.nr_radius = 4;
   }
+  // ---- solver band height: set by the fields solved together (one colour
+  // of the sweep: every field alone in the slow temporal sweep) ----
+  RunOpts o3 = opt;
+  if (o3.band_rows < 0 && ctx->band_rows <= 0) {
+    const bool temporal = cfg.temporal_strength > 0.0f && cfg.cg_iterations > 0;
+    int colour = nf;
+    if ((cfg.fast || !temporal) && cfg.parallel_across_fields) {
+      int max_off = 0;
+      for (int o : offs) max_off = std::max(max_off, std::abs(o));
+      const int reach = std::max(max_off, cfg.nr_anchor > 0.0f ? cfg.nr_radius : 0);
+      const int stride = temporal ? reach + 1 : 1;
+      colour = (nf + stride - 1) / stride;
+    } else if (temporal) {
+      colour = 1;
+    }
+    const int hh = last_active_line(g) - g.first_active_field_line;
+    const int ww = g.active_video_end - g.active_video_start;
+    o3.band_rows = auto_band_rows_hw(ctx, std::vector<std::pair<int, int>>(colour, {hh, ww}));
+  }
   // ---- layout: batch + 3-D regions ----
   Batch plan;
-  hvdg_status st = plan_batch(ctx, in, nf, &cfg, ctx->band_rows, plan);
+  hvdg_status st = plan_batch(ctx, in, nf, &cfg, o3.band_rows >= 0 ? o3.band_rows : ctx->band_rows,
+                              plan);
   if (st != HVDG_OK) return st;
   const int h = plan.fp[0].h, w = plan.fp[0].w, pitch = plan.fp[0].pitch;
   const int64_t plane = (int64_t)h * pitch;
@@ -1304,7 +1347,7 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
                               sizeof(hvdg::MePair) * max_pairs +
                               sizeof(hvdg::NbrPair) * max_pairs + 1024);
   Staged S;
-  st = stage_upload(ctx, in, nf, &cfg, opt, xo, S);
+  st = stage_upload(ctx, in, nf, &cfg, o3, xo, S);
   if (st != HVDG_OK) return st;
   Batch& b = S.b;
   const Layout& L = b.L;
