@@ -1337,6 +1337,15 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   const size_t x_src = take(sizeof(int2) * plane * max_pairs);
   const size_t x_cpx = take(sizeof(float) * plane * max_pairs);
   const size_t x_ctmp = take(sizeof(float) * plane * max_pairs);
+  // fast-mode motion cache (pass-0 motion reused by later passes,
+  // sequence.cpp:674-692): dy, dx, conf per window pair slot
+  const size_t x_mcache = take(sizeof(float) * 3 * (size_t)nt * max_pairs);
+  // coherence gate: 4 channel planes per pair of the largest colour + scratch
+  const bool gate_cfg = cfg.coherence_gate > 0.0f;
+  const int64_t coh_stride = gate_cfg ? plane * max_pairs : 0;
+  const size_t x_coh = take(sizeof(float) * 4 * (size_t)coh_stride);
+  const size_t x_ctab = take(sizeof(hvdg::TrajGroup) * 2 * nf + sizeof(hvdg::TrajPair) * max_pairs +
+                             sizeof(int) * 2 * max_pairs + 256);
   size_t x_env[5];
   for (int i = 0; i < 5; ++i) x_env[i] = take(sizeof(float) * plane * nf);
   const size_t env_samples = ((size_t)h * w + 6) / 7;
@@ -1433,12 +1442,14 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
     bool gate_any = false;
     for (int pass = 0; pass < n_passes; ++pass)
       if (cfg.coherence_gate > 0.0f && !(cfg.fast && pass == 0)) gate_any = true;
-    if (cfg.trajectory_fit || cfg.psi_init || anchor || gate_any) {
+    (void)gate_any;
+    if (cfg.psi_init || anchor) {
       ctx->last_error =
-          "temporal window decode needs trajectory_fit=0, psi_init=0, no anchored pass "
-          "(passes=1 or nr_anchor=0) and no coherence gate in this build";
+          "temporal window decode needs psi_init=0 and no anchored pass (passes=1 or "
+          "nr_anchor=0) in this build";
       return HVDG_ERR_UNSUPPORTED;
     }
+    if (nofs > hvdg::kTrajMaxPairs) return HVDG_ERR_UNSUPPORTED;
   }
   // ---- colours (sequence.cpp:1052-1099) ----
   std::vector<std::vector<int>> colors;
@@ -1563,15 +1574,29 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
       std::vector<hvdg::NbrPair> np;
       std::vector<int> env_list;
       std::vector<int64_t> env_off;
+      // pairs: the fully searched ones first, then (fast mode with the
+      // trajectory fit, float motion) the predicted + verified ones
+      // (sequence.cpp:699-763)
+      std::vector<hvdg::TrajPair> tp;
+      std::vector<hvdg::TrajGroup> groups, searched;
+      std::vector<int> grp, gid;
+      int n_full = 0;
       if (has_temporal) {
-        for (int j : col) {
+        struct P {
+          int k, j, slot, odd, g, o, oi;
+        };
+        std::vector<P> full, pred;
+        const bool predict = cfg.fast && cfg.trajectory_fit && !sad_me;
+        for (int gi = 0; gi < (int)col.size(); ++gi) {
+          const int j = col[gi];
           int slot = 0;
           bool any_odd = false;
-          for (int o : offs) {
+          for (int oi = 0; oi < nofs; ++oi) {
+            const int o = offs[oi];
             const int k = j + o;
             if (k < 0 || k >= nf) continue;
-            mp.push_back(hvdg::MePair{k, j});
-            np.push_back(hvdg::NbrPair{k, j, slot++, (o & 1) != 0 ? 1 : 0});
+            const bool is_full = !predict || o == -1 || o == 1 || o == 2;
+            (is_full ? full : pred).push_back(P{k, j, slot++, (o & 1) != 0 ? 1 : 0, gi, o, oi});
             any_odd = any_odd || (o & 1) != 0;
           }
           b.fields[j].n_nbr = slot;
@@ -1580,6 +1605,23 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
           if (any_odd) {
             env_list.push_back(j);
             env_off.push_back(escr_off[j]);
+          }
+        }
+        groups.assign(col.size(), hvdg::TrajGroup{});
+        searched.assign(col.size(), hvdg::TrajGroup{});
+        for (auto& G : groups) G.count = 0;
+        for (auto& G : searched) G.count = 0;
+        n_full = (int)full.size();
+        for (int pass_list = 0; pass_list < 2; ++pass_list) {
+          for (const P& q : pass_list == 0 ? full : pred) {
+            const int pi = (int)mp.size();
+            mp.push_back(hvdg::MePair{q.k, q.j});
+            np.push_back(hvdg::NbrPair{q.k, q.j, q.slot, q.odd});
+            tp.push_back(hvdg::TrajPair{q.o, (float)(in[q.k].parity - in[q.j].parity) / 2.0f});
+            gid.push_back(q.j * nofs + q.oi);
+            groups[q.g].pair[groups[q.g].count++] = pi;
+            if (pass_list == 0) searched[q.g].pair[searched[q.g].count++] = pi;
+            else grp.push_back(q.g);
           }
         }
       }
@@ -1592,13 +1634,74 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(d_np, np.data(), sizeof(hvdg::NbrPair) * npairs, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D pairs");
-        if (sad_me)
-          hvdg::launch_motion_sad(d_mf, nf, h, w, d_mp, npairs, sad_a, sad_b, s);
-        else
-          hvdg::launch_motion(d_mf, nf, h, w, d_mp, npairs, ma, mb, s);
+        // small tables of this colour
+        char* ct = at<char>(ctx, X(x_ctab));
+        hvdg::TrajGroup* d_groups = reinterpret_cast<hvdg::TrajGroup*>(ct);
+        hvdg::TrajGroup* d_searched = d_groups + nf;
+        hvdg::TrajPair* d_tp = reinterpret_cast<hvdg::TrajPair*>(d_searched + nf);
+        int* d_grp = reinterpret_cast<int*>(d_tp + max_pairs);
+        int* d_gid = d_grp + max_pairs;
+        e = cudaMemcpyAsync(d_groups, groups.data(), sizeof(hvdg::TrajGroup) * groups.size(),
+                            cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_searched, searched.data(), sizeof(hvdg::TrajGroup) * searched.size(),
+                              cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_tp, tp.data(), sizeof(hvdg::TrajPair) * tp.size(),
+                              cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && !grp.empty())
+          e = cudaMemcpyAsync(d_grp, grp.data(), sizeof(int) * grp.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_gid, gid.data(), sizeof(int) * gid.size(), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D trajectory tables");
+        float* mcache = at<float>(ctx, X(x_mcache));
+        const int64_t mc_stride = (int64_t)nt * max_pairs;
+        if (cfg.fast && pass > 0) {
+          // fast mode: every pair's motion comes from pass 0
+          hvdg::launch_motion_cache(d_gid, npairs, nt, nt, mb.dy, mb.dx, mb.conf, mcache, mc_stride,
+                                    false, s);
+        } else {
+          if (sad_me)
+            hvdg::launch_motion_sad(d_mf, nf, h, w, d_mp, n_full, sad_a, sad_b, s);
+          else
+            hvdg::launch_motion(d_mf, nf, h, w, d_mp, n_full, ma, mb, s);
+          const int npred = npairs - n_full;
+          if (npred > 0) {
+            const int64_t ofs = (int64_t)n_full * nt;
+            hvdg::launch_traj_verify(d_mf, d_mp, n_full, npred, d_grp, d_searched, d_tp, mb.blur, h,
+                                     w, ma, mb.dy, mb.dx, mb.mdy, mb.mdx, mb.sdy, mb.sdx, mb.best,
+                                     s);
+            hvdg::launch_me_confidence(d_mf, d_mp + n_full, npred, h, w, ma, mb.blur, mb.mdy + ofs,
+                                       mb.mdx + ofs, mb.sdy + ofs, mb.sdx + ofs, mb.best + ofs,
+                                       mb.dy + ofs, mb.dx + ofs, mb.conf + ofs, s);
+            S.launches += 2;
+          }
+          if (cfg.trajectory_fit && npairs >= 2) {
+            hvdg::launch_traj_snap(d_mf, d_mp, d_groups, (int)groups.size(), d_tp, h, w, tile, nt,
+                                   mb.dy, mb.dx, mb.conf, s);
+            S.launches += 1;
+          }
+          if (cfg.fast && n_passes > 1)
+            hvdg::launch_motion_cache(d_gid, npairs, nt, nt, mb.dy, mb.dx, mb.conf, mcache,
+                                      mc_stride, true, s);
+        }
         vb.conf_bytes = sizeof(float) * plane * npairs;
         hvdg::launch_vectors(d_mf, d_mp, npairs, h, w, ma, vb, cfg.fast != 0, s);
         S.launches += 8;
+        if (gate_cfg && !(cfg.fast && pass == 0)) {
+          // coherence gate against the current chi of both fields
+          hvdg::CohBuffers cb;
+          cb.chi = at<float2>(ctx, L.o_X0);
+          cb.snap_dy = vb.snap_dy;
+          cb.snap_dx = vb.snap_dx;
+          cb.terms = at<float>(ctx, X(x_coh));
+          cb.tmp = vb.conf_tmp;
+          cb.conf_px = vb.conf_px;
+          cb.pix_off = d_pix_off;
+          cb.chan_stride = coh_stride;
+          hvdg::launch_coherence_gate(d_mf, d_mp, npairs, h, w, ma, cb, cfg.coherence_gate, s);
+          S.launches += 10;
+        }
         if (!env_list.empty()) {
           e = cudaMemcpyAsync(d_list, env_list.data(), sizeof(int) * env_list.size(),
                               cudaMemcpyHostToDevice, s);

@@ -852,6 +852,226 @@ __global__ void k_pair_blur_h(const MeField* __restrict__ mf, const MePair* __re
   }
 }
 
+// ---------------------------------------------------------------------------
+// Trajectory consensus, fast-mode verification, motion cache, coherence gate
+// ---------------------------------------------------------------------------
+// numpy.median of up to kTrajMaxPairs values (Median, motion.cpp:80-91 and
+// MedianOf, sequence.cpp:29-39: the mean of the two middles for even n)
+__device__ float median_small(float* v, int n) {
+  for (int i = 1; i < n; ++i) {
+    const float x = v[i];
+    int j = i - 1;
+    while (j >= 0 && v[j] > x) {
+      v[j + 1] = v[j];
+      --j;
+    }
+    v[j + 1] = x;
+  }
+  const int k = n / 2;
+  float m = v[k];
+  if (n % 2 == 0) m = 0.5f * (m + v[k - 1]);
+  return m;
+}
+
+// TrajectorySnap (motion.cpp:565-601) with FitTrajectory (:532-563): one
+// thread per (field group, tile).
+__global__ void k_traj_snap(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                            const TrajGroup* __restrict__ groups, int ngroups,
+                            const TrajPair* __restrict__ tp, int tile, int tiles_off,
+                            float* __restrict__ dy, float* __restrict__ dx,
+                            const float* __restrict__ conf) {
+  const int g = blockIdx.y;
+  if (g >= ngroups) return;
+  const TrajGroup G = groups[g];
+  if (G.count < 2) return;
+  const MeField mc = mf[pairs[G.pair[0]].cur];
+  const int th = (mc.h + tile - 1) / tile, tw = (mc.w + tile - 1) / tile;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= th * tw) return;
+  float sy[kTrajMaxPairs], sx[kTrajMaxPairs];
+  int n = 0;
+  for (int i = 0; i < G.count; ++i) {
+    const int p = G.pair[i];
+    const TrajPair q = tp[p];
+    if (q.offset == 0) continue;
+    const int o = tiles_off * p + t;
+    if (conf[o] <= 0.15f) continue;
+    const float of = (float)q.offset;
+    sy[n] = (dy[o] - q.parity_shift) / of;
+    sx[n] = dx[o] / of;
+    ++n;
+  }
+  float vym = 0.0f, vxm = 0.0f;
+  if (n > 0) {
+    vym = median_small(sy, n);
+    vxm = median_small(sx, n);
+  }
+  // consensus: the snap applies where >= 3 offsets agree within 1.5 px
+  float agree = 0.0f;
+  for (int i = 0; i < G.count; ++i) {
+    const int p = G.pair[i];
+    const TrajPair q = tp[p];
+    const int o = tiles_off * p + t;
+    const float of = (float)q.offset;
+    const float py = of * vym + q.parity_shift;
+    const float px = of * vxm;
+    const float dev = fabsf(dy[o] - py) + fabsf(dx[o] - px);
+    if (dev <= 1.5f) agree += 1.0f;
+  }
+  if (agree < 3.0f) return;
+  for (int i = 0; i < G.count; ++i) {
+    const int p = G.pair[i];
+    const TrajPair q = tp[p];
+    const int o = tiles_off * p + t;
+    const float of = (float)q.offset;
+    const float py = of * vym + q.parity_shift;
+    const float px = of * vxm;
+    const float dev = fabsf(dy[o] - py) + fabsf(dx[o] - px);
+    if (dev <= 1.5f) {
+      dy[o] = py;
+      dx[o] = px;
+    }
+  }
+}
+
+// Fast-mode prediction (sequence.cpp:714-763) + VerifyMotion (motion.cpp:490-530).
+__global__ void k_traj_verify(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                              int base, int npred, const int* __restrict__ grp,
+                              const TrajGroup* __restrict__ searched,
+                              const TrajPair* __restrict__ tp, const float* __restrict__ blur,
+                              MeArgs a, const float* __restrict__ dy_in,
+                              const float* __restrict__ dx_in, float* __restrict__ out_mdy,
+                              float* __restrict__ out_mdx, float* __restrict__ out_sdy,
+                              float* __restrict__ out_sdx, float* __restrict__ out_best) {
+  const int i = blockIdx.y;
+  if (i >= npred) return;
+  const int p = base + i;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int h = mc.h, w = mc.w, tile = a.tile;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= th * tw) return;
+  const TrajGroup S = searched[grp[i]];
+  float sy[kTrajMaxPairs], sx[kTrajMaxPairs];
+  for (int k = 0; k < S.count; ++k) {
+    const int q = S.pair[k];
+    const TrajPair m = tp[q];
+    const float of = (float)m.offset;
+    sy[k] = (dy_in[a.tiles_off * q + t] - m.parity_shift) / of;
+    sx[k] = dx_in[a.tiles_off * q + t] / of;
+  }
+  const float vym0 = S.count > 0 ? median_small(sy, S.count) : 0.0f;
+  const float vxm0 = S.count > 0 ? median_small(sx, S.count) : 0.0f;
+  const TrajPair me = tp[p];
+  const float pdy = (float)me.offset * vym0 + me.parity_shift;
+  const float pdx = (float)me.offset * vxm0;
+  const int iy = (int)lroundf(pdy), ix = (int)lroundf(pdx);
+  const float* A = blur + mc.b_off;
+  const float* B = blur + mr.b_off;
+  const int y0 = (t / tw) * tile, y1 = min(y0 + tile, h);
+  const int x0 = (t % tw) * tile, x1 = min(x0 + tile, w);
+  const float inf = __int_as_float(0x7f800000);
+  // one relative candidate at the rounded prediction, one absolute at zero
+  const float pred = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, iy, ix, inf) * 1.0f;
+  const float zero = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, 0, 0, inf) * 1.0f;
+  const int o = a.tiles_off * p + t;
+  if (zero <= pred) {
+    out_mdy[o] = 0.0f;
+    out_mdx[o] = 0.0f;
+    out_best[o] = zero;
+  } else {
+    // the full float prediction is kept where it won
+    out_mdy[o] = pdy;
+    out_mdx[o] = pdx;
+    out_best[o] = pred;
+  }
+  out_sdy[o] = 0.0f;
+  out_sdx[o] = 0.0f;
+}
+
+__global__ void k_motion_cache(const int* __restrict__ gid, int npairs, int nt, int tiles_off,
+                               float* __restrict__ dy, float* __restrict__ dx,
+                               float* __restrict__ conf, float* __restrict__ cache,
+                               int64_t stride, int store) {
+  const int i = blockIdx.y;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npairs || t >= nt) return;
+  const int64_t c = (int64_t)gid[i] * nt + t;
+  const int o = tiles_off * i + t;
+  if (store) {
+    cache[c] = dy[o];
+    cache[stride + c] = dx[o];
+    cache[2 * stride + c] = conf[o];
+  } else {
+    dy[o] = cache[c];
+    dx[o] = cache[stride + c];
+    conf[o] = cache[2 * stride + c];
+  }
+}
+
+// Cross terms of chi_j and chi_k bilinearly warped by the snapped per-pixel
+// vectors (WarpBilinearTiles, temporal.cpp:140-168, row offset 0).
+__global__ void k_coh_terms(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                            int npairs, MeArgs a, CohBuffers b) {
+  const int p = blockIdx.z;
+  if (p >= npairs) return;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= mc.w || y >= mc.h) return;
+  const int th = (mc.h + a.tile - 1) / a.tile, tw = (mc.w + a.tile - 1) / a.tile;
+  int iy, ix;
+  float fyb, fxb;
+  bracket(y, th, a.tile, &iy, &fyb);
+  bracket(x, tw, a.tile, &ix, &fxb);
+  const int iy1 = min(iy + 1, th - 1), ix1 = min(ix + 1, tw - 1);
+  const int o = a.tiles_off * p;
+  const float vy = interp_tiles(b.snap_dy + o, tw, iy, iy1, ix, ix1, fyb, fxb);
+  const float vx = interp_tiles(b.snap_dx + o, tw, iy, iy1, ix, ix1, fyb, fxb);
+  float sy = (float)y - vy + 0.0f;
+  float sx = (float)x - vx;
+  sy = fminf(fmaxf(sy, 0.0f), (float)mr.h - 1.001f);
+  sx = fminf(fmaxf(sx, 0.0f), (float)mr.w - 1.001f);
+  const int y0 = (int)sy, x0 = (int)sx;
+  const float fy = sy - (float)y0, fx = sx - (float)x0;
+  const int y1 = min(y0 + 1, mr.h - 1), x1 = min(x0 + 1, mr.w - 1);
+  const float2* K = b.chi + mr.y_off;
+  const float2 k00 = K[(int64_t)y0 * mr.pitch + x0], k10 = K[(int64_t)y1 * mr.pitch + x0];
+  const float2 k01 = K[(int64_t)y0 * mr.pitch + x1], k11 = K[(int64_t)y1 * mr.pitch + x1];
+  const float wre = k00.x * (1 - fy) * (1 - fx) + k10.x * fy * (1 - fx) + k01.x * (1 - fy) * fx +
+                    k11.x * fy * fx;
+  const float wim = k00.y * (1 - fy) * (1 - fx) + k10.y * fy * (1 - fx) + k01.y * (1 - fy) * fx +
+                    k11.y * fy * fx;
+  const float2 z1 = b.chi[mc.y_off + (int64_t)y * mc.pitch + x];
+  // z1 * conj(cw)
+  const float cre = z1.x * wre - z1.y * (-wim);
+  const float cim = z1.x * (-wim) + z1.y * wre;
+  const int64_t q = b.pix_off[p] + (int64_t)y * mc.pitch + x;
+  b.terms[q] = cre;
+  b.terms[b.chan_stride + q] = cim;
+  b.terms[2 * b.chan_stride + q] = z1.x * z1.x + z1.y * z1.y;
+  b.terms[3 * b.chan_stride + q] = wre * wre + wim * wim;
+}
+
+__global__ void k_coh_apply(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                            int npairs, CohBuffers b, float gate) {
+  const int p = blockIdx.z;
+  if (p >= npairs) return;
+  const MeField mc = mf[pairs[p].cur];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= mc.w || y >= mc.h) return;
+  const int64_t q = b.pix_off[p] + (int64_t)y * mc.pitch + x;
+  const float re = b.terms[q], im = b.terms[b.chan_stride + q];
+  const float m1 = b.terms[2 * b.chan_stride + q], m2 = b.terms[3 * b.chan_stride + q];
+  const float num = sqrtf(re * re + im * im);
+  const float den = sqrtf(fmaxf(0.0f, m1 * m2)) + 1e-6f;
+  const float gamma = fminf(fmaxf(num / den, 0.0f), 1.0f);
+  b.conf_px[q] *= (1.0f - gate) + gate * gamma;
+}
+
 void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
                     int max_w, const MeArgs& a, const VecBuffers& v, bool fast_conf,
                     cudaStream_t st) {
@@ -879,6 +1099,64 @@ void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, 
                                                                      v.pix_off, 8);
     cudaMemcpyAsync(v.conf_px, v.conf_tmp, v.conf_bytes, cudaMemcpyDeviceToDevice, st);
   }
+}
+
+void launch_traj_snap(const MeField* d_fields, const MePair* d_pairs, const TrajGroup* d_groups,
+                      int ngroups, const TrajPair* d_tp, int max_h, int max_w, int tile,
+                      int tiles_off, float* dy, float* dx, const float* conf, cudaStream_t st) {
+  if (ngroups <= 0) return;
+  const int nt = ((max_h + tile - 1) / tile) * ((max_w + tile - 1) / tile);
+  k_traj_snap<<<dim3((nt + 63) / 64, ngroups), 64, 0, st>>>(d_fields, d_pairs, d_groups, ngroups,
+                                                           d_tp, tile, tiles_off, dy, dx, conf);
+}
+
+void launch_traj_verify(const MeField* d_fields, const MePair* d_pairs, int base, int npred,
+                        const int* d_grp, const TrajGroup* d_searched, const TrajPair* d_tp,
+                        const float* blur, int max_h, int max_w, const MeArgs& a,
+                        const float* dy_in, const float* dx_in, float* mdy, float* mdx,
+                        float* sdy, float* sdx, float* best, cudaStream_t st) {
+  if (npred <= 0) return;
+  const int nt = ((max_h + a.tile - 1) / a.tile) * ((max_w + a.tile - 1) / a.tile);
+  k_traj_verify<<<dim3((nt + 63) / 64, npred), 64, 0, st>>>(d_fields, d_pairs, base, npred, d_grp,
+                                                           d_searched, d_tp, blur, a, dy_in, dx_in,
+                                                           mdy, mdx, sdy, sdx, best);
+}
+
+void launch_me_confidence(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                          int max_w, const MeArgs& a, const float* blur, const float* mdy,
+                          const float* mdx, const float* sdy, const float* sdx, const float* best,
+                          float* dy, float* dx, float* conf, cudaStream_t st) {
+  if (npairs <= 0) return;
+  const int th = (max_h + a.tile - 1) / a.tile, tw = (max_w + a.tile - 1) / a.tile;
+  const int smem = 2 * th * tw * (int)sizeof(float);
+  k_me_confidence<<<npairs, 256, smem, st>>>(d_fields, d_pairs, npairs, blur, a, mdy, mdx, sdy, sdx,
+                                             best, dy, dx, conf);
+}
+
+void launch_motion_cache(const int* d_gid, int npairs, int nt, int tiles_off, float* dy, float* dx,
+                         float* conf, float* cache, int64_t cache_stride, bool store,
+                         cudaStream_t st) {
+  if (npairs <= 0) return;
+  k_motion_cache<<<dim3((nt + 127) / 128, npairs), 128, 0, st>>>(d_gid, npairs, nt, tiles_off, dy,
+                                                                dx, conf, cache, cache_stride,
+                                                                store ? 1 : 0);
+}
+
+void launch_coherence_gate(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                           int max_w, const MeArgs& a, const CohBuffers& b, float gate,
+                           cudaStream_t st) {
+  if (npairs <= 0) return;
+  const dim3 grid((max_w + 127) / 128, max_h, npairs);
+  k_coh_terms<<<grid, 128, 0, st>>>(d_fields, d_pairs, npairs, a, b);
+  // ComplexCoherence's four BoxBlur(r = 6) passes (temporal.cpp:186-189)
+  for (int c = 0; c < 4; ++c) {
+    float* ch = b.terms + c * b.chan_stride;
+    k_pair_blur_v<<<dim3((max_w + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs, ch,
+                                                                    b.tmp, b.pix_off, 6);
+    k_pair_blur_h<<<dim3((max_h + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
+                                                                    b.tmp, ch, b.pix_off, 6);
+  }
+  k_coh_apply<<<grid, 128, 0, st>>>(d_fields, d_pairs, npairs, b, gate);
 }
 
 }  // namespace hvdg

@@ -62,6 +62,61 @@ struct SadBuffers {
   float *dy, *dx, *conf;           // per tile outputs (as EstimateMotion's)
 };
 
+// Trajectory consensus (motion.cpp:532-601) over the pairs of each field
+// solved in one colour: pair index lists per field, offset and half-line
+// parity shift per pair. Vectors are snapped in place.
+constexpr int kTrajMaxPairs = 8;
+struct TrajGroup {
+  int count;
+  int pair[kTrajMaxPairs];     // indices into the colour's pair list
+};
+struct TrajPair {
+  int offset;                  // k - j
+  float parity_shift;          // (p_k - p_j) / 2
+};
+void launch_traj_snap(const MeField* d_fields, const MePair* d_pairs, const TrajGroup* d_groups,
+                      int ngroups, const TrajPair* d_tp, int max_h, int max_w, int tile,
+                      int tiles_off, float* dy, float* dx, const float* conf, cudaStream_t st);
+// Fast-mode predicted vectors audited by VerifyMotion (motion.cpp:490-530,
+// sequence.cpp:714-763): for pair p (index base + i of the colour's list) of
+// field group grp[i], the median velocity of the group's searched pairs
+// predicts the vector; the SSD at its rounding competes with zero. Writes
+// mdy / mdx (sdy = sdx = 0) and best at the pair's slot; confidences follow
+// with launch_me_confidence.
+void launch_traj_verify(const MeField* d_fields, const MePair* d_pairs, int base, int npred,
+                        const int* d_grp, const TrajGroup* d_searched, const TrajPair* d_tp,
+                        const float* blur, int max_h, int max_w, const MeArgs& a,
+                        const float* dy_in, const float* dx_in, float* mdy, float* mdx,
+                        float* sdy, float* sdx, float* best, cudaStream_t st);
+// MotionConfidence + final vectors for `npairs` pairs whose tile arrays start
+// at the given pointers (pair i at offset i * a.tiles_off).
+void launch_me_confidence(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                          int max_w, const MeArgs& a, const float* blur, const float* mdy,
+                          const float* mdx, const float* sdy, const float* sdx, const float* best,
+                          float* dy, float* dx, float* conf, cudaStream_t st);
+// Tile vectors / confidences of a colour's pairs to / from the window-wide
+// motion cache (slot gid[i] per pair; fast mode reuses pass-0 motion).
+void launch_motion_cache(const int* d_gid, int npairs, int nt, int tiles_off, float* dy, float* dx,
+                         float* conf, float* cache, int64_t cache_stride, bool store,
+                         cudaStream_t st);
+// Coherence gate (sequence.cpp:946-998, ComplexCoherence temporal.cpp:172-202):
+// conf_px *= (1 - a) + a gamma, gamma the |box-blurred cross term| over the
+// blurred energies of chi_j and chi_k bilinearly warped by the snapped
+// per-pixel vectors (radius 6).
+struct CohBuffers {
+  const float2* chi;           // per field at MeField::y_off (current chi)
+  const float* snap_dy;        // snapped tile vectors (pair i at i * tiles_off)
+  const float* snap_dx;
+  float* terms;                // 4 planes per pair: re, im, |chi_j|^2, |cw|^2
+  float* tmp;                  // one plane per pair
+  float* conf_px;              // per-pixel confidence per pair (pix_off)
+  const int64_t* pix_off;      // per-pair plane offset
+  int64_t chan_stride;         // floats between the 4 channel blocks of terms
+};
+void launch_coherence_gate(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                           int max_w, const MeArgs& a, const CohBuffers& b, float gate,
+                           cudaStream_t st);
+
 int sad_max_block();
 int sad_max_range();
 void launch_motion_sad(const MeField* d_fields, int nf, int max_h, int max_w,

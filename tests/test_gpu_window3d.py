@@ -43,6 +43,36 @@ def test_window_temporal_vs_reference(ctx, std, fast):
         assert abs(cg - cr) < 0.05
 
 
+@pytest.mark.parametrize("std,fast,passes", [(_cabi.STD_NTSC, 0, 1), (_cabi.STD_NTSC, 1, 2),
+                                             (_cabi.STD_PAL, 1, 2)])
+def test_window_trajectory_and_coherence_gate_vs_reference(ctx, std, fast, passes):
+    """The default motion pipeline of the 3-D window: trajectory consensus
+    snap (slow), predicted + verified vectors for the unsearched offsets and
+    the pass-0 motion cache (fast), and the coherence gate (slow from pass 0,
+    fast from pass 1), against the compiled reference on the same fields."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    nf = 8
+    seq = synth.make_sequence(61 + std, std, nf, noise_sigma=1.0, moving=True)
+    g = _cabi.default_geometry(std)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=fast, cg_tol=1e-6,
+                             temporal_strength=0.5, passes=passes, nr_anchor=0.0,
+                             coherence_gate=0.6, trajectory_fit=1)
+    outs = ctx.decode_field_window([api.Field(f.samples, g, parity=f.parity) for f in seq], cfg)
+    ires = [synth.to_ire(f.samples) for f in seq]
+    ys, cs, _ = ref.decode_field_window(ires, [f.parity for f in seq], g, cfg)
+    for j in range(nf):
+        pg = psnr(outs[j].luma, seq[j].y_true)
+        pr = psnr(ys[j], seq[j].y_true)
+        cg = psnr(outs[j].chroma, seq[j].chi_true)
+        cr = psnr(cs[j], seq[j].chi_true)
+        print(f"traj std={std} fast={fast} passes={passes} field {j}: Y gpu {pg:.3f} ref {pr:.3f}"
+              f"  C gpu {cg:.3f} ref {cr:.3f}")
+        assert abs(pg - pr) < 0.05
+        assert abs(cg - cr) < 0.05
+
+
 def test_window_temporal_integer_sad_me_vs_oracle(ctx):
     """The 3-D window with the integer-SAD motion mode (me_mode 1, 16 x 16
     blocks, +-16) against the FP64 oracle running the same mode: PSNR against
