@@ -23,6 +23,7 @@
 #include "hvdg_host.h"
 #include "k_adjoint.h"
 #include "k_init.h"
+#include "k_joint.h"
 #include "k_motion.h"
 #include "k_temporal.h"
 #include "k_prep.h"
@@ -1344,6 +1345,27 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   const bool gate_cfg = cfg.coherence_gate > 0.0f;
   const int64_t coh_stride = gate_cfg ? plane * max_pairs : 0;
   const size_t x_coh = take(sizeof(float) * 4 * (size_t)coh_stride);
+  // anchored pass (passes > 1, nr_anchor > 0): pre-snap motion, the anchor's
+  // own per-pixel vectors and confidences, the anchor planes and the joint
+  // solver's planes
+  const bool anchor_on = cfg.temporal_strength > 0.0f && cfg.cg_iterations > 0 &&
+                         std::max(1, cfg.passes) > 1 && cfg.nr_anchor > 0.0f && nf > 1;
+  const size_t AP = anchor_on ? 1 : 0;
+  const size_t x_pre = take(sizeof(float) * 3 * (size_t)nt * max_pairs * AP);
+  const size_t x_asnap = take(sizeof(float) * 4 * (size_t)nt * max_pairs * AP);
+  const size_t x_asrc = take(sizeof(int2) * plane * max_pairs * AP);
+  const size_t x_acpx = take(sizeof(float) * plane * max_pairs * AP);
+  const size_t x_actmp = take(sizeof(float) * plane * max_pairs * AP);
+  const size_t x_ya = take(sizeof(float) * plane * nf * AP);
+  const size_t x_caa = take(sizeof(float2) * plane * nf * AP);
+  const size_t x_wa = take(sizeof(float) * plane * nf * AP);
+  const size_t x_res = take(sizeof(float) * plane * nf * AP);
+  const size_t x_jp = take(sizeof(float4) * 10 * plane * nf * AP);
+  const size_t x_jm2 = take(sizeof(float) * plane * nf * AP);
+  const int jbx = (w + 31) / 32, jby = (h + 7) / 8;
+  const size_t x_jpart = take(sizeof(double) * 5 * (size_t)jbx * jby * nf * AP);
+  const size_t x_jctl = take(sizeof(hvdg::JointCtl) * nf * AP + sizeof(hvdg::AnchorGroup) * nf * AP +
+                             sizeof(int) * nf * AP + 256);
   const size_t x_ctab = take(sizeof(hvdg::TrajGroup) * 2 * nf + sizeof(hvdg::TrajPair) * max_pairs +
                              sizeof(int) * 2 * max_pairs + 256);
   size_t x_env[5];
@@ -1443,13 +1465,23 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
     for (int pass = 0; pass < n_passes; ++pass)
       if (cfg.coherence_gate > 0.0f && !(cfg.fast && pass == 0)) gate_any = true;
     (void)gate_any;
-    if (cfg.psi_init || anchor) {
-      ctx->last_error =
-          "temporal window decode needs psi_init=0 and no anchored pass (passes=1 or "
-          "nr_anchor=0) in this build";
+    if (cfg.psi_init) {
+      ctx->last_error = "temporal window decode needs psi_init=0 in this build";
       return HVDG_ERR_UNSUPPORTED;
     }
     if (nofs > hvdg::kTrajMaxPairs) return HVDG_ERR_UNSUPPORTED;
+    if (anchor) {
+      // the anchor reuses the neighbour pairs' motion: every offset within
+      // nr_radius must be a neighbour offset
+      for (int o = -cfg.nr_radius; o <= cfg.nr_radius; ++o) {
+        if (o == 0) continue;
+        if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
+          ctx->last_error = "anchored pass: nr_radius reaches offsets outside the temporal set";
+          return HVDG_ERR_UNSUPPORTED;
+        }
+      }
+      if (2 * cfg.nr_radius > hvdg::kJointMaxNbr) return HVDG_ERR_UNSUPPORTED;
+    }
   }
   // ---- colours (sequence.cpp:1052-1099) ----
   std::vector<std::vector<int>> colors;
@@ -1656,8 +1688,10 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
         if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D trajectory tables");
         float* mcache = at<float>(ctx, X(x_mcache));
         const int64_t mc_stride = (int64_t)nt * max_pairs;
+        const bool joint_pass = anchor_on && pass >= 1;
         if (cfg.fast && pass > 0) {
-          // fast mode: every pair's motion comes from pass 0
+          // fast mode: every pair's motion comes from pass 0 (cached before
+          // the consensus snap, which is re-applied: same inputs, same result)
           hvdg::launch_motion_cache(d_gid, npairs, nt, nt, mb.dy, mb.dx, mb.conf, mcache, mc_stride,
                                     false, s);
         } else {
@@ -1676,14 +1710,27 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
                                        mb.dy + ofs, mb.dx + ofs, mb.conf + ofs, s);
             S.launches += 2;
           }
-          if (cfg.trajectory_fit && npairs >= 2) {
-            hvdg::launch_traj_snap(d_mf, d_mp, d_groups, (int)groups.size(), d_tp, h, w, tile, nt,
-                                   mb.dy, mb.dx, mb.conf, s);
-            S.launches += 1;
-          }
           if (cfg.fast && n_passes > 1)
             hvdg::launch_motion_cache(d_gid, npairs, nt, nt, mb.dy, mb.dx, mb.conf, mcache,
                                       mc_stride, true, s);
+        }
+        if (joint_pass) {
+          // the anchor blends with the pairwise motion as estimated (before
+          // the consensus snap), sequence.cpp:70-102
+          float* pre = at<float>(ctx, X(x_pre));
+          const size_t tb = sizeof(float) * (size_t)nt * npairs;
+          e = cudaMemcpyAsync(pre, mb.dy, tb, cudaMemcpyDeviceToDevice, s);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(pre + (size_t)nt * max_pairs, mb.dx, tb, cudaMemcpyDeviceToDevice, s);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(pre + 2 * (size_t)nt * max_pairs, mb.conf, tb,
+                                cudaMemcpyDeviceToDevice, s);
+          if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "anchor motion copy");
+        }
+        if (cfg.trajectory_fit && npairs >= 2) {
+          hvdg::launch_traj_snap(d_mf, d_mp, d_groups, (int)groups.size(), d_tp, h, w, tile, nt,
+                                 mb.dy, mb.dx, mb.conf, s);
+          S.launches += 1;
         }
         vb.conf_bytes = sizeof(float) * plane * npairs;
         hvdg::launch_vectors(d_mf, d_mp, npairs, h, w, ma, vb, cfg.fast != 0, s);
@@ -1726,14 +1773,140 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
       cudaMemsetAsync(at<char>(ctx, L.o_done), 0xff, sizeof(int) * nf, s);
       cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
       hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), nf, at<float2>(ctx, L.o_X0), s);
-      sa.unit_base = cbegin[ci];
-      sa.n_units = ccount[ci];
-      sa.n_phases = cphases[ci];
-      e = hvdg::launch_solver(sa, solver_grid(ctx, ccount[ci]), s);
-      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
-      S.launches += 2;
+      if (anchor_on && pass >= 1) {
+        // ---- anchored pass: SynthReference + VariationalRefineJoint ----
+        char* jc = at<char>(ctx, X(x_jctl));
+        hvdg::JointCtl* d_jctl = reinterpret_cast<hvdg::JointCtl*>(jc);
+        hvdg::AnchorGroup* d_ag = reinterpret_cast<hvdg::AnchorGroup*>(d_jctl + nf);
+        int* d_fl = reinterpret_cast<int*>(d_ag + nf);
+        std::vector<hvdg::AnchorGroup> ag;
+        for (int j : col) {
+          hvdg::AnchorGroup G{};
+          G.field = j;
+          G.count = 0;
+          for (size_t pi = 0; pi < mp.size(); ++pi) {
+            if (mp[pi].cur != j) continue;
+            const int k = mp[pi].ref;
+            if (std::abs(k - j) > cfg.nr_radius) continue;
+            G.p[G.count++] = hvdg::AnchorPair{(int)pi, k,
+                                              (float)(in[j].parity - in[k].parity) / 2.0f};
+          }
+          ag.push_back(G);
+        }
+        e = cudaMemcpyAsync(d_ag, ag.data(), sizeof(hvdg::AnchorGroup) * ag.size(),
+                            cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_fl, col.data(), sizeof(int) * col.size(), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D anchor tables");
+        // the anchor's per-pixel vectors / confidences (VectorsPerPixel and
+        // the slow UpsampleConfidence of the pre-snap motion)
+        float* pre = at<float>(ctx, X(x_pre));
+        float* asn = at<float>(ctx, X(x_asnap));
+        hvdg::VecBuffers va = vb;
+        va.dy = pre;
+        va.dx = pre + (size_t)nt * max_pairs;
+        va.conf = pre + 2 * (size_t)nt * max_pairs;
+        va.snap_dy = asn;
+        va.snap_dx = asn + (size_t)nt * max_pairs;
+        va.c2 = asn + 2 * (size_t)nt * max_pairs;
+        va.c2_snap = asn + 3 * (size_t)nt * max_pairs;
+        va.c2_snap2 = va.c2_snap;
+        va.src_idx = at<int2>(ctx, X(x_asrc));
+        va.conf_px = at<float>(ctx, X(x_acpx));
+        va.conf_tmp = at<float>(ctx, X(x_actmp));
+        const int npairs_c = (int)mp.size();
+        va.conf_bytes = sizeof(float) * plane * npairs_c;
+        if (npairs_c > 0) hvdg::launch_vectors(d_mf, d_mp, npairs_c, h, w, ma, va, false, s);
+        hvdg::AnchorArgs aa;
+        aa.fields = at<FieldDesc>(ctx, L.o_fields);
+        aa.groups = d_ag;
+        aa.ngroups = (int)ag.size();
+        aa.tile = tile;
+        aa.tiles_off = nt;
+        aa.snap_dy = va.snap_dy;
+        aa.snap_dx = va.snap_dx;
+        aa.conf_px = va.conf_px;
+        aa.pix_off = d_pix_off;
+        aa.Y = at<float>(ctx, L.o_Y);
+        aa.chi = at<float2>(ctx, L.o_X0);
+        aa.S = at<float>(ctx, L.o_S);
+        aa.line_phasor = at<float4>(ctx, L.o_lineph);
+        aa.col_phasor = at<float2>(ctx, L.o_colph);
+        aa.eps_b = cfg.nr_eps;
+        aa.Ya = at<float>(ctx, X(x_ya));
+        aa.Ca = at<float2>(ctx, X(x_caa));
+        aa.Wa = at<float>(ctx, X(x_wa));
+        aa.resid = at<float>(ctx, X(x_res));
+        hvdg::launch_anchor(aa, h, w, s);
+        hvdg::JointArgs ja;
+        ja.fields = at<FieldDesc>(ctx, L.o_fields);
+        ja.flist = d_fl;
+        ja.nfl = (int)col.size();
+        ja.bx = jbx;
+        ja.by = jby;
+        ja.S = at<float>(ctx, L.o_S);
+        ja.line_phasor = at<float4>(ctx, L.o_lineph);
+        ja.col_phasor = at<float2>(ctx, L.o_colph);
+        ja.nbr = at<float4>(ctx, X(x_nbr));
+        ja.nu = cfg.temporal_strength;
+        ja.eps_t = cfg.temporal_eps;
+        ja.Ya = aa.Ya;
+        ja.Ca = aa.Ca;
+        ja.Wa = aa.Wa;
+        ja.nu_a = cfg.nr_anchor;
+        ja.eps = cfg.charbonnier_eps;
+        ja.eps_c = cfg.chroma_eps;
+        ja.k = cfg.structure_coupling;
+        float4* jp = at<float4>(ctx, X(x_jp));
+        const int64_t bp = plane * nf;
+        ja.X = jp;
+        ja.G[0] = jp + bp;
+        ja.G[1] = jp + 2 * bp;
+        ja.D[0] = jp + 3 * bp;
+        ja.D[1] = jp + 4 * bp;
+        ja.Q[0] = jp + 5 * bp;
+        ja.Q[1] = jp + 6 * bp;
+        ja.W = jp + 7 * bp;
+        ja.M0 = jp + 8 * bp;
+        ja.M1 = jp + 9 * bp;
+        ja.M2 = at<float>(ctx, X(x_jm2));
+        ja.partials = at<double>(ctx, X(x_jpart));
+        ja.ctl = d_jctl;
+        const FieldDesc& f0 = b.fields[col[0]];
+        hvdg::launch_joint_load(ja, at<float>(ctx, L.o_Y), at<float2>(ctx, L.o_X0), h, w, s);
+        for (int o = 0; o < f0.n_outer; ++o) hvdg::launch_joint_outer(ja, f0.n_inner, h, w, s);
+        hvdg::launch_joint_store(ja, at<float>(ctx, L.o_Y), at<float2>(ctx, L.o_X0), false, h, w, s);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "anchored pass launch");
+        S.launches += 6 + f0.n_outer * (6 + 2 * f0.n_inner);
+      } else {
+        sa.unit_base = cbegin[ci];
+        sa.n_units = ccount[ci];
+        sa.n_phases = cphases[ci];
+        e = hvdg::launch_solver(sa, solver_grid(ctx, ccount[ci]), s);
+        if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
+        S.launches += 2;
+      }
       // the solved fields' luma / chi now replace their init state (Ys[j], chis[j])
     }
+  }
+  if (anchor_on && cfg.output_fidelity) {
+    // the anchored pass leaves Y free; the output reverts to data fidelity
+    std::vector<int> all(nf);
+    for (int j = 0; j < nf; ++j) all[j] = j;
+    int* d_fl = reinterpret_cast<int*>(reinterpret_cast<hvdg::AnchorGroup*>(
+                    reinterpret_cast<hvdg::JointCtl*>(at<char>(ctx, X(x_jctl))) + nf) + nf);
+    e = cudaMemcpyAsync(d_fl, all.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D field list");
+    hvdg::JointArgs ja;
+    std::memset(&ja, 0, sizeof(ja));
+    ja.fields = at<FieldDesc>(ctx, L.o_fields);
+    ja.flist = d_fl;
+    ja.nfl = nf;
+    ja.S = at<float>(ctx, L.o_S);
+    ja.line_phasor = at<float4>(ctx, L.o_lineph);
+    ja.col_phasor = at<float2>(ctx, L.o_colph);
+    hvdg::launch_output_fidelity(ja, at<float>(ctx, L.o_Y), at<float2>(ctx, L.o_X0), h, w, s);
   }
   mark(ctx, 3);
   return stage_finish(ctx, S, out, opt, diag);

@@ -73,6 +73,42 @@ def test_window_trajectory_and_coherence_gate_vs_reference(ctx, std, fast, passe
         assert abs(cg - cr) < 0.05
 
 
+@pytest.mark.parametrize("std,fast", [(_cabi.STD_NTSC, 0), (_cabi.STD_NTSC, 1), (_cabi.STD_PAL, 1)])
+def test_window_anchored_pass_vs_reference(ctx, std, fast):
+    """The reference's default 3-D configuration: two passes, the second
+    anchored (SynthReference + VariationalRefineJoint with Y free), with the
+    trajectory snap and the coherence gate, against the compiled reference.
+    Tolerance: window-mean PSNR within 0.05 dB, each field within 0.15 dB.
+    The slow anchored pass re-runs motion estimation on the pass-0 outputs,
+    so FP32 rounding differences flip near-tie motion decisions: the
+    reference itself moves by up to 0.14 dB (chroma, one field) when its
+    input is perturbed by 2e-3 IRE of noise."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    nf = 8
+    seq = synth.make_sequence(71 + std, std, nf, noise_sigma=1.0, moving=True)
+    g = _cabi.default_geometry(std)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=fast, cg_tol=1e-6,
+                             temporal_strength=0.5)
+    assert cfg.passes == 2 and cfg.nr_anchor > 0 and cfg.trajectory_fit == 1
+    outs = ctx.decode_field_window([api.Field(f.samples, g, parity=f.parity) for f in seq], cfg)
+    ires = [synth.to_ire(f.samples) for f in seq]
+    ys, cs, _ = ref.decode_field_window(ires, [f.parity for f in seq], g, cfg)
+    dys, dcs = [], []
+    for j in range(nf):
+        pg = psnr(outs[j].luma, seq[j].y_true)
+        pr = psnr(ys[j], seq[j].y_true)
+        cg = psnr(outs[j].chroma, seq[j].chi_true)
+        cr = psnr(cs[j], seq[j].chi_true)
+        print(f"anchor std={std} fast={fast} field {j}: Y gpu {pg:.3f} ref {pr:.3f}"
+              f"  C gpu {cg:.3f} ref {cr:.3f}")
+        dys.append(pg - pr)
+        dcs.append(cg - cr)
+    assert abs(np.mean(dys)) < 0.05 and abs(np.mean(dcs)) < 0.05
+    assert np.max(np.abs(dys)) < 0.15 and np.max(np.abs(dcs)) < 0.15
+
+
 def test_window_temporal_integer_sad_me_vs_oracle(ctx):
     """The 3-D window with the integer-SAD motion mode (me_mode 1, 16 x 16
     blocks, +-16) against the FP64 oracle running the same mode: PSNR against
