@@ -1364,8 +1364,8 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   const size_t x_jm2 = take(sizeof(float) * plane * nf * AP);
   const int jbx = (w + 31) / 32, jby = (h + 7) / 8;
   const size_t x_jpart = take(sizeof(double) * 5 * (size_t)jbx * jby * nf * AP);
-  const size_t x_jctl = take(sizeof(hvdg::JointCtl) * nf * AP + sizeof(hvdg::AnchorGroup) * nf * AP +
-                             sizeof(int) * nf * AP + 256);
+  const size_t x_jctl = take(sizeof(hvdg::JointCtl) * nf + sizeof(hvdg::AnchorGroup) * nf +
+                             sizeof(int) * nf + 256);
   const size_t x_ctab = take(sizeof(hvdg::TrajGroup) * 2 * nf + sizeof(hvdg::TrajPair) * max_pairs +
                              sizeof(int) * 2 * max_pairs + 256);
   size_t x_env[5];
@@ -1465,10 +1465,6 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
     for (int pass = 0; pass < n_passes; ++pass)
       if (cfg.coherence_gate > 0.0f && !(cfg.fast && pass == 0)) gate_any = true;
     (void)gate_any;
-    if (cfg.psi_init) {
-      ctx->last_error = "temporal window decode needs psi_init=0 in this build";
-      return HVDG_ERR_UNSUPPORTED;
-    }
     if (nofs > hvdg::kTrajMaxPairs) return HVDG_ERR_UNSUPPORTED;
     if (anchor) {
       // the anchor reuses the neighbour pairs' motion: every offset within
@@ -1772,6 +1768,26 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
       cudaMemsetAsync(at<char>(ctx, L.o_arrive), 0, sizeof(int) * nf, s);
       cudaMemsetAsync(at<char>(ctx, L.o_done), 0xff, sizeof(int) * nf, s);
       cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
+      if (pass == 0 && cfg.psi_init && has_temporal) {
+        // PsiClosedForm init of the colour's fields that have neighbours
+        // (sequence.cpp:1033-1035), before the anisotropy is resolved
+        char* jc = at<char>(ctx, X(x_jctl));
+        int* d_fl = reinterpret_cast<int*>(reinterpret_cast<hvdg::AnchorGroup*>(
+                        reinterpret_cast<hvdg::JointCtl*>(jc) + nf) + nf);
+        e = cudaMemcpyAsync(d_fl, col.data(), sizeof(int) * col.size(), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D psi field list");
+        hvdg::JointArgs pj;
+        std::memset(&pj, 0, sizeof(pj));
+        pj.fields = at<FieldDesc>(ctx, L.o_fields);
+        pj.flist = d_fl;
+        pj.nfl = (int)col.size();
+        pj.S = at<float>(ctx, L.o_S);
+        pj.line_phasor = at<float4>(ctx, L.o_lineph);
+        pj.col_phasor = at<float2>(ctx, L.o_colph);
+        pj.nbr = at<float4>(ctx, X(x_nbr));
+        hvdg::launch_psi_init(pj, at<float2>(ctx, L.o_X0), h, w, s);
+        S.launches += 1;
+      }
       hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), nf, at<float2>(ctx, L.o_X0), s);
       if (anchor_on && pass >= 1) {
         // ---- anchored pass: SynthReference + VariationalRefineJoint ----

@@ -464,6 +464,56 @@ __global__ void k_anchor_weight(AnchorArgs a) {
   a.Wa[f.px_off + (int64_t)y * f.pitch + x] = eb2 / (r * r + eb2);
 }
 
+__global__ void k_psi_init(JointArgs a, float2* __restrict__ chi) {
+  const int fi = blockIdx.z;
+  const FieldDesc f = a.fields[a.flist[fi]];
+  if (f.n_nbr <= 0) return;
+  const int x = blockIdx.x * kBX + threadIdx.x, y = blockIdx.y * kBY + threadIdx.y;
+  if (x >= f.w || y >= f.h) return;
+  const int64_t lo = (int64_t)y * f.pitch + x;
+  const int64_t o = f.px_off + lo;
+  const float kEpsT = 6.0f;  // the refine's robust gate at the init point
+  double a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0;
+  double b1 = 0, b2 = 0, b3 = 0;
+  double wsum = 0.0;
+  auto add = [&](float Sk, float2 ck, float wk) {
+    const double rc = ck.x, ic = -ck.y;
+    a11 += wk;
+    a12 += wk * rc;
+    a13 += wk * ic;
+    a22 += wk * rc * rc;
+    a23 += wk * rc * ic;
+    a33 += wk * ic * ic;
+    b1 += wk * Sk;
+    b2 += wk * Sk * rc;
+    b3 += wk * Sk * ic;
+  };
+  const float2 c = car_at(a.line_phasor, a.col_phasor, f, y, x);
+  const float Sv = a.S[o];
+  const float2 cf = chi[o];
+  add(Sv, c, 1.0f);
+  for (int j = 0; j < f.n_nbr; ++j) {
+    const float4 nb = a.nbr[f.nbr_off + (int64_t)j * f.plane_px + lo];
+    // neighbour composite S + (S_w - S), carrier c - dc
+    const float2 cw = make_float2(c.x - nb.y, c.y - nb.z);
+    const float rt = nb.x + (cf.x * nb.y - cf.y * nb.z);
+    const float wk = nb.w * kEpsT * kEpsT / (rt * rt + kEpsT * kEpsT);
+    add(Sv + nb.x, cw, wk);
+    wsum += wk;
+  }
+  const double det = a11 * (a22 * a33 - a23 * a23) - a12 * (a12 * a33 - a23 * a13) +
+                     a13 * (a12 * a23 - a22 * a13);
+  const double a11c = fmax(a11, 1e-9);
+  const bool ok = det > 1e-3 * a11c * a11c * a11c * 0.01;
+  const double d = ok ? det : 1.0;
+  const double q1 = (a11 * (b2 * a33 - b3 * a23) - b1 * (a12 * a33 - a23 * a13) +
+                     a13 * (a12 * b3 - b2 * a13)) / d;
+  const double q2 = (a11 * (a22 * b3 - a23 * b2) - a12 * (a12 * b3 - b2 * a13) +
+                     b1 * (a12 * a23 - a22 * a13)) / d;
+  const float t = ok ? fminf(fmaxf((float)(wsum / 2.0), 0.0f), 1.0f) : 0.0f;
+  chi[o] = make_float2(t * (float)q1 + (1.0f - t) * cf.x, t * (float)q2 + (1.0f - t) * cf.y);
+}
+
 dim3 jgrid(int max_w, int max_h, int n) {
   return dim3((max_w + kBX - 1) / kBX, (max_h + kBY - 1) / kBY, n);
 }
@@ -508,6 +558,11 @@ void launch_anchor(const AnchorArgs& a, int max_h, int max_w, cudaStream_t st) {
   const dim3 gr = jgrid(max_w, max_h, a.ngroups), bl(kBX, kBY);
   k_anchor_blend<<<gr, bl, 0, st>>>(a);
   k_anchor_weight<<<gr, bl, 0, st>>>(a);
+}
+
+void launch_psi_init(const JointArgs& a, float2* chi, int max_h, int max_w, cudaStream_t st) {
+  if (a.nfl <= 0) return;
+  k_psi_init<<<jgrid(max_w, max_h, a.nfl), dim3(kBX, kBY), 0, st>>>(a, chi);
 }
 
 }  // namespace hvdg

@@ -94,4 +94,11 @@ struct AnchorArgs {
 };
 void launch_anchor(const AnchorArgs& a, int max_h, int max_w, cudaStream_t st);
 
+// PsiClosedForm (sequence.cpp:160-227): per pixel, the weighted normal
+// equations of the field's own observation and its motion-compensated
+// neighbours (an N-step phase-shifting set) solved in closed form, blended
+// with the current chi by the neighbours' total confidence. Overwrites chi
+// of the fields in a.flist that have neighbour planes.
+void launch_psi_init(const JointArgs& a, float2* chi, int max_h, int max_w, cudaStream_t st);
+
 }  // namespace hvdg

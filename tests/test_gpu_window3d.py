@@ -109,6 +109,49 @@ def test_window_anchored_pass_vs_reference(ctx, std, fast):
     assert np.max(np.abs(dys)) < 0.15 and np.max(np.abs(dcs)) < 0.15
 
 
+@pytest.mark.parametrize("fast", [0, 1])
+def test_window_psi_init_vs_reference(ctx, fast):
+    """psi_init: the closed-form phase-shifting init of every field that has
+    neighbours (PsiClosedForm) before its pass-0 solve, against the compiled
+    reference. The closed form switches on a near-singular determinant test,
+    so the reference's own output moves by up to ~3 dB per field when its
+    input is perturbed by 2e-3 IRE of noise; the test therefore bounds the
+    device-vs-reference PSNR differences by the reference's spread under three
+    such perturbations: window mean |dPSNR| <= 2 x the reference's mean
+    spread + 0.1 dB, and within 0.15 dB on fields where the reference is
+    stable (spread < 0.01 dB)."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    std, nf = _cabi.STD_NTSC, 8
+    seq = synth.make_sequence(81, std, nf, noise_sigma=1.0, moving=True)
+    g = _cabi.default_geometry(std)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=fast, cg_tol=1e-6,
+                             temporal_strength=0.5, passes=1, psi_init=1)
+    outs = ctx.decode_field_window([api.Field(f.samples, g, parity=f.parity) for f in seq], cfg)
+    ires = [synth.to_ire(f.samples) for f in seq]
+    par = [f.parity for f in seq]
+    ys, cs, _ = ref.decode_field_window(ires, par, g, cfg)
+    spread_y, spread_c = np.zeros(nf), np.zeros(nf)
+    for seed in (0, 1, 2):
+        rng = np.random.default_rng(seed)
+        pert = [(x + rng.normal(0, 2e-3, x.shape)).astype(np.float32) for x in ires]
+        yp, cp, _ = ref.decode_field_window(pert, par, g, cfg)
+        for j in range(nf):
+            spread_y[j] = max(spread_y[j], abs(psnr(yp[j], seq[j].y_true) - psnr(ys[j], seq[j].y_true)))
+            spread_c[j] = max(spread_c[j], abs(psnr(cp[j], seq[j].chi_true) - psnr(cs[j], seq[j].chi_true)))
+    dys = np.array([psnr(outs[j].luma, seq[j].y_true) - psnr(ys[j], seq[j].y_true) for j in range(nf)])
+    dcs = np.array([psnr(outs[j].chroma, seq[j].chi_true) - psnr(cs[j], seq[j].chi_true)
+                    for j in range(nf)])
+    for j in range(nf):
+        print(f"psi fast={fast} field {j}: dY {dys[j]:.4f} (ref spread {spread_y[j]:.4f})"
+              f"  dC {dcs[j]:.4f} (ref spread {spread_c[j]:.4f})")
+    assert np.mean(np.abs(dys)) <= 2 * np.mean(spread_y) + 0.1
+    assert np.mean(np.abs(dcs)) <= 2 * np.mean(spread_c) + 0.1
+    stable = (spread_y < 0.01) & (spread_c < 0.01)
+    assert np.all(np.abs(dys[stable]) < 0.15) and np.all(np.abs(dcs[stable]) < 0.15)
+
+
 def test_window_temporal_integer_sad_me_vs_oracle(ctx):
     """The 3-D window with the integer-SAD motion mode (me_mode 1, 16 x 16
     blocks, +-16) against the FP64 oracle running the same mode: PSNR against
