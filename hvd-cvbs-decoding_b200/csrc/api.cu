@@ -22,6 +22,7 @@
 #include "hvdg_internal.h"
 #include "hvdg_host.h"
 #include "k_adjoint.h"
+#include "k_frame.h"
 #include "k_init.h"
 #include "k_joint.h"
 #include "k_motion.h"
@@ -64,6 +65,18 @@ float nominal_burst(const hvdg_geometry& g) {
   return g.standard == HVDG_STD_PAL ? 21.43f : 20.0f;
 }
 
+// Device-path limits of one solve plane of w x h (documented in
+// include/hvdg.h): the row / column cyclic-convolution lengths of the init
+// and the auto-aniso sample buffer.
+hvdg_status check_plane(int w, int h, bool vsw, int col_max) {
+  const int pad = std::min(hvdg::kInitPad, h - 1);
+  if (2 * w - 1 > hvdg::kRowFft || 2 * (h + 2 * pad) - 1 > col_max) return HVDG_ERR_UNSUPPORTED;
+  const int group = vsw ? 4 : 2;
+  const int64_t n = (int64_t)((h / group) / 2) * ((w + 1) / 3);
+  if (n > hvdg::aniso_max_samples()) return HVDG_ERR_UNSUPPORTED;
+  return HVDG_OK;
+}
+
 hvdg_status check_geometry(const hvdg_geometry* g) {
   if (!g) return HVDG_ERR_BAD_ARGUMENT;
   if (g->standard < 0 || g->standard > 2) return HVDG_ERR_BAD_ARGUMENT;
@@ -83,8 +96,8 @@ hvdg_status check_geometry(const hvdg_geometry* g) {
   if (g->field_height > hvdg::kMaxLines) return HVDG_ERR_UNSUPPORTED;
   const int w = g->active_video_end - g->active_video_start;
   const int h = lal - g->first_active_field_line;
-  const int pad = std::min(hvdg::kInitPad, h - 1);
-  if (2 * w - 1 > hvdg::kRowFft || 2 * (h + 2 * pad) - 1 > hvdg::kColFft) return HVDG_ERR_UNSUPPORTED;
+  const hvdg_status st = check_plane(w, h, uses_vswitch(*g), hvdg::kColFft);
+  if (st != HVDG_OK) return st;
   if (g->colour_burst_end - g->colour_burst_start > 64 + 3) return HVDG_ERR_UNSUPPORTED;
   return HVDG_OK;
 }
@@ -131,8 +144,9 @@ std::vector<cd> kernel_spectrum(const std::vector<double>& mask, int M, double s
 
 struct GeomTables {
   int w, h, hp, pad;
+  int col_m;                     // column convolution length (kColFft or kColFftWide)
   std::vector<float2> khat_row;  // 2 * kRowFft
-  std::vector<float2> khat_col;  // 2 * kColFft
+  std::vector<float2> khat_col;  // 2 * col_m
   std::vector<float2> col_phasor;
 };
 
@@ -145,6 +159,7 @@ GeomTables make_geom_tables(const hvdg_geometry& g) {
   t.h = last_active_line(g) - g.first_active_field_line;
   t.pad = std::min(hvdg::kInitPad, t.h > 1 ? t.h - 1 : 0);
   t.hp = t.h + 2 * t.pad;
+  t.col_m = 2 * t.hp - 1 <= hvdg::kColFft ? hvdg::kColFft : hvdg::kColFftWide;
   for (int v = 0; v < 2; ++v) {
     std::vector<double> gx(t.w), gy(t.hp);
     const double cx = kVariants[v][0] * 1.0e6;
@@ -160,7 +175,7 @@ GeomTables make_geom_tables(const hvdg_geometry& g) {
     for (const cd& c : kernel_spectrum(gx, hvdg::kRowFft, 1.0))
       t.khat_row.push_back(make_float2((float)c.real(), (float)c.imag()));
     // x2 of the init (holographic_init.cpp:247-251) folded into the column pass
-    for (const cd& c : kernel_spectrum(gy, hvdg::kColFft, 2.0))
+    for (const cd& c : kernel_spectrum(gy, t.col_m, 2.0))
       t.khat_col.push_back(make_float2((float)c.real(), (float)c.imag()));
   }
   const double w0 = phase_per_sample(g);
@@ -307,14 +322,23 @@ constexpr int kSadMaxTiles = 6144;
 // ---------------------------------------------------------------------------
 // Batch planning
 // ---------------------------------------------------------------------------
+// One solve plane: a field's active picture, or a woven frame's.
 struct FieldPlan {
   const hvdg_geometry* g;
   int h, w, pitch, fh, fw;
   int64_t px_off;
-  int line_off, theta_off, geom_slot;
-  int64_t raw_off, raw_bytes;
+  int line_off, geom_slot;
   int hp;
   int64_t rowbuf_off;
+};
+
+// One source field of the lock-in / crop kernels (one per plane, or two per
+// woven plane): its raw samples in the arena and its full-field per-line
+// outputs.
+struct PrepPlan {
+  int fh, fw;
+  int theta_off;
+  int64_t raw_off, raw_bytes;
 };
 
 struct Layout {
@@ -332,6 +356,7 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Batch {
   std::vector<FieldPlan> fp;
+  std::vector<PrepPlan> pp;
   std::vector<hvdg::PrepDesc> prep;
   std::vector<FieldDesc> fields;
   std::vector<GeomDesc> geoms;
@@ -341,7 +366,7 @@ struct Batch {
   std::vector<int> itab;  // prow_field | prow_first | cgrp_field | cgrp_first | btile_field | btile_first
   int it_prow_field, it_prow_first, it_cgrp_field, it_cgrp_first, it_btile_field, it_btile_first;
   std::vector<int64_t> rowbuf_offs;
-  std::vector<int> crop_row_field, crop_row_first;
+  std::vector<int4> crop_rows;  // per S row: (plane, row, source field, source line)
   std::vector<int64_t> px_offs;
   std::vector<int> pitches;
   Layout L;
@@ -373,14 +398,37 @@ int auto_band_rows(hvdg_ctx* ctx, const std::vector<FieldPlan>& fp) {
   return auto_band_rows_hw(ctx, hw);
 }
 
+// Plan a batch. Normally every entry of `in` is one plane. With
+// `weave_geom` set, `in` holds 2 m source fields, two per woven frame
+// (WeaveAndBuildCarrier, engine.cpp:53-126): the field whose parity is 0
+// lands on the even rows of its frame's plane, the other on the odd rows,
+// and the planes take the geometry *weave_geom (the woven active picture:
+// no blanking, 2 x active lines). The source fields are F32 IRE planes
+// written on the device (the caller's split), so no raw upload is planned
+// for them beyond their f32 slots.
 hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
-                       int band_rows, Batch& b) {
+                       int band_rows, Batch& b, const hvdg_geometry* weave_geom = nullptr) {
   b = Batch();
   std::map<GeomKey, int> slot;
   int64_t px = 0, rawb = 0, rowb = 0;
   int lines = 0, theta = 0;
-  for (int i = 0; i < n; ++i) {
-    const hvdg_geometry& g = *in[i].geometry;
+  if (weave_geom && (n % 2) != 0) return HVDG_ERR_BAD_ARGUMENT;
+  const int m = weave_geom ? n / 2 : n;
+  for (int k = 0; k < n; ++k) {
+    const hvdg_geometry& g = *in[k].geometry;
+    PrepPlan q;
+    q.fh = g.field_height;
+    q.fw = g.field_width;
+    q.theta_off = theta;
+    theta += q.fh;
+    q.raw_bytes = (int64_t)q.fh * q.fw * elem_size(in[k].sample_type);
+    q.raw_off = rawb;
+    rawb += align_up(q.raw_bytes, 256);
+    b.pp.push_back(q);
+  }
+  for (int i = 0; i < m; ++i) {
+    const hvdg_geometry* gp = weave_geom ? weave_geom : in[i].geometry;
+    const hvdg_geometry& g = *gp;
     const GeomKey key = geom_key(g);
     auto it = ctx->geoms.find(key);
     if (it == ctx->geoms.end()) it = ctx->geoms.emplace(key, make_geom_tables(g)).first;
@@ -394,7 +442,7 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
       gs = sit->second;
     }
     FieldPlan p;
-    p.g = in[i].geometry;
+    p.g = gp;
     p.fh = g.field_height;
     p.fw = g.field_width;
     p.h = last_active_line(g) - g.first_active_field_line;
@@ -404,12 +452,7 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     px += (int64_t)p.h * p.pitch;
     p.line_off = lines;
     lines += p.h;
-    p.theta_off = theta;
-    theta += p.fh;
     p.geom_slot = gs;
-    p.raw_bytes = (int64_t)p.fh * p.fw * elem_size(in[i].sample_type);
-    p.raw_off = rawb;
-    rawb += align_up(p.raw_bytes, 256);
     p.hp = it->second.hp;
     p.rowbuf_off = rowb;
     rowb += 2LL * p.hp * p.pitch;
@@ -427,16 +470,18 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     gd.khat_row_off = nkhat;
     nkhat += 2 * hvdg::kRowFft;
     gd.khat_col_off = nkhat;
-    nkhat += 2 * hvdg::kColFft;
+    gd.col_m = t.col_m;
+    nkhat += 2 * t.col_m;
     b.geoms.push_back(gd);
     b.gcol_off.push_back(ncol);
     ncol += t.w;
   }
   // per-field descriptors, units
   const int band = band_rows > 0 ? band_rows : auto_band_rows(ctx, b.fp);
-  for (int i = 0; i < n; ++i) {
+  for (int i = 0; i < m; ++i) {
     const FieldPlan& p = b.fp[i];
     const hvdg_geometry& g = *p.g;
+    const hvdg_field_in& fi = in[weave_geom ? 2 * i : i];
     FieldDesc f;
     std::memset(&f, 0, sizeof(f));
     f.h = p.h;
@@ -450,8 +495,8 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     f.geom = p.geom_slot;
     f.is_pal = uses_vswitch(g) ? 1 : 0;
     // solver budget (variational.cpp:224-230)
-    const int outer_cfg = in[i].irls_outer > 0 ? in[i].irls_outer : cfg->irls_outer;
-    const int cg_cfg = in[i].cg_iterations >= 0 ? in[i].cg_iterations : cfg->cg_iterations;
+    const int outer_cfg = fi.irls_outer > 0 ? fi.irls_outer : cfg->irls_outer;
+    const int cg_cfg = fi.cg_iterations >= 0 ? fi.cg_iterations : cfg->cg_iterations;
     f.n_outer = std::max(1, outer_cfg);
     const int cg_total = cfg->fast ? cg_cfg * 2 / 3 : cg_cfg;
     f.n_inner = std::max(1, cg_total / f.n_outer);
@@ -472,14 +517,27 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     b.max_phases = std::max(b.max_phases, f.n_phases);
     b.fields.push_back(f);
 
+    b.px_offs.push_back(p.px_off);
+    b.pitches.push_back(p.pitch);
+    b.rowbuf_offs.push_back(p.rowbuf_off);
+  }
+  // source-field descriptors and the crop rows
+  for (int k = 0; k < n; ++k) {
+    const hvdg_geometry& g = *in[k].geometry;
+    const PrepPlan& q = b.pp[k];
+    const int plane = weave_geom ? k / 2 : k;
+    const FieldPlan& p = b.fp[plane];
+    // woven: this field's active line y lands on plane row 2 y + row0
+    const int row0 = weave_geom ? (in[k].parity == 0 ? 0 : 1) : 0;
+    const int step = weave_geom ? 2 : 1;
     hvdg::PrepDesc pd;
     std::memset(&pd, 0, sizeof(pd));
-    pd.sample_type = in[i].sample_type;
+    pd.sample_type = in[k].sample_type;
     pd.quadrant = g.subcarrier_hz <= 0.0 ? 1 : 0;
-    pd.blank = in[i].blanking_level;
-    pd.codes_per_ire = (in[i].white_level - in[i].blanking_level) / 100.0f;
-    pd.fh = p.fh;
-    pd.fw = p.fw;
+    pd.blank = in[k].blanking_level;
+    pd.codes_per_ire = (in[k].white_level - in[k].blanking_level) / 100.0f;
+    pd.fh = q.fh;
+    pd.fw = q.fw;
     pd.bx0 = g.colour_burst_start;
     pd.bx1 = g.colour_burst_end;
     pd.fal = g.first_active_field_line;
@@ -491,22 +549,20 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     pd.w0 = phase_per_sample(g);
     pd.adv = line_advance(g);
     pd.chroma_phase_off = -cfg->chroma_phase_deg * 3.14159265358979323846f / 180.0f;
-    pd.theta_off = p.theta_off;
-    pd.line_off = p.line_off;
+    pd.theta_off = q.theta_off;
+    pd.line_off = p.line_off + row0;
+    pd.line_step = step;
     b.prep.push_back(pd);
-    b.px_offs.push_back(p.px_off);
-    b.pitches.push_back(p.pitch);
-    b.rowbuf_offs.push_back(p.rowbuf_off);
-    for (int y = 0; y < p.h; ++y) {
-      b.crop_row_field.push_back(i);
-    }
-    b.crop_row_first.push_back(p.line_off);
+    const int lines_k = pd.lal - pd.fal;
+    for (int y = 0; y < lines_k; ++y)
+      b.crop_rows.push_back(make_int4(plane, row0 + step * y, k, pd.fal + y));
   }
   // init tables
   std::vector<int> prow_field, prow_first, cgrp_field, cgrp_first, btile_field, btile_first;
-  const int cg = hvdg::init_col_group(), bt = hvdg::init_blend_tile();
-  for (int i = 0; i < n; ++i) {
+  const int bt = hvdg::init_blend_tile();
+  for (int i = 0; i < m; ++i) {
     const FieldPlan& p = b.fp[i];
+    const int cg = hvdg::init_col_group(b.gtabs[p.geom_slot]->col_m);
     prow_first.push_back((int)prow_field.size());
     for (int y = 0; y < p.hp; ++y) prow_field.push_back(i);
     cgrp_first.push_back((int)cgrp_field.size());
@@ -546,13 +602,13 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
   };
   L.o_raw = take(rawb);
   L.o_prep = take(sizeof(hvdg::PrepDesc) * n);
-  L.o_fields = take(sizeof(FieldDesc) * n);
+  L.o_fields = take(sizeof(FieldDesc) * m);
   L.o_geoms = take(sizeof(GeomDesc) * b.geoms.size());
-  L.o_ctl = take(sizeof(FieldCtl) * n);
+  L.o_ctl = take(sizeof(FieldCtl) * m);
   L.o_units = take(sizeof(Unit) * b.units.size());
   L.o_partials = take(sizeof(double) * 5 * b.units.size());
-  L.o_done = take(sizeof(int) * n);
-  L.o_arrive = take(sizeof(int) * n);
+  L.o_done = take(sizeof(int) * m);
+  L.o_arrive = take(sizeof(int) * m);
   L.o_flags = take(sizeof(int) * 4);
   L.o_queue = take(sizeof(unsigned long long));
   L.o_lineph = take(sizeof(float4) * lines);
@@ -564,9 +620,8 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
   L.o_twr = take(sizeof(float2) * hvdg::kRowFft);
   L.o_twc = take(sizeof(float2) * hvdg::kColFft);
   L.o_amp = take(sizeof(float) * n);
-  // crop tables: crop_row_field | crop_row_first | px_offs(int64) | pitches
-  L.o_itab = take(sizeof(int) * (b.itab.size() + b.crop_row_field.size() + b.crop_row_first.size() +
-                                 b.pitches.size()) +
+  // index tables: itab | pitches | crop rows (int4) | px_offs (int64) | rowbuf offs (int64)
+  L.o_itab = take(sizeof(int) * (b.itab.size() + b.pitches.size()) + sizeof(int4) * b.crop_rows.size() +
                   sizeof(int64_t) * (b.px_offs.size() + b.rowbuf_offs.size()) + 64);
   L.o_S = take(sizeof(float) * px);
   L.o_Y = take(sizeof(float) * px);
@@ -602,12 +657,15 @@ struct RunOpts {
   bool tables_only = false;          // stage_upload without the per-call reset
   int band_rows = -1;                // solver band height override (-1: context setting)
   int ctas_per_sm = -1;              // solver CTAs per SM override (-1: context setting)
+  // woven frames: `in` holds two source fields per plane (plan_batch); their
+  // F32 IRE samples are written into the arena's raw slots on the device
+  const hvdg_geometry* weave_geom = nullptr;
 };
 
 // A batch uploaded to the arena: layout, table offsets, launch count.
 struct Staged {
   Batch b;
-  size_t it_itab = 0, it_crf = 0, it_crfirst = 0, it_pitch = 0, it_pxoff = 0, it_rbo = 0;
+  size_t it_itab = 0, it_crop = 0, it_pitch = 0, it_pxoff = 0, it_rbo = 0;
   size_t extra = 0;  // offset of the caller's extra region (after the batch layout)
   int launches = 0;
 };
@@ -656,9 +714,11 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
   // drop a stale non-sticky error left by an earlier, already reported call,
   // so the launch checks below see only this call's launches
   cudaGetLastError();
-  hvdg_status st = plan_batch(ctx, in, n, cfg, opt.band_rows >= 0 ? opt.band_rows : ctx->band_rows, b);
+  hvdg_status st = plan_batch(ctx, in, n, cfg, opt.band_rows >= 0 ? opt.band_rows : ctx->band_rows, b,
+                              opt.weave_geom);
   if (st != HVDG_OK) return st;
   const Layout& L = b.L;
+  const int m = (int)b.fp.size();
   S.extra = align_up(L.total, 256);
   st = ctx->arena.reserve(S.extra + extra_bytes, ctx->stream);
   if (st != HVDG_OK) {
@@ -671,17 +731,18 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
   auto put = [&](size_t off, const void* src, size_t bytes) {
     if (bytes) std::memcpy(host.data() + (off - L.o_prep), src, bytes);
   };
-  for (int i = 0; i < n; ++i) {
-    b.prep[i].samples = opt.device_io ? in[i].samples
-                                      : (const void*)(at<char>(ctx, L.o_raw) + b.fp[i].raw_off);
+  for (int k = 0; k < n; ++k) {
+    b.prep[k].samples = (opt.device_io && !opt.weave_geom)
+                            ? in[k].samples
+                            : (const void*)(at<char>(ctx, L.o_raw) + b.pp[k].raw_off);
   }
   put(L.o_prep, b.prep.data(), sizeof(hvdg::PrepDesc) * n);
-  put(L.o_fields, b.fields.data(), sizeof(FieldDesc) * n);
+  put(L.o_fields, b.fields.data(), sizeof(FieldDesc) * m);
   put(L.o_geoms, b.geoms.data(), sizeof(GeomDesc) * b.geoms.size());
   put(L.o_units, b.units.data(), sizeof(Unit) * b.units.size());
   {
-    std::vector<int> done(n, -1);
-    put(L.o_done, done.data(), sizeof(int) * n);
+    std::vector<int> done(m, -1);
+    put(L.o_done, done.data(), sizeof(int) * m);
   }
   {
     std::vector<float2> col, kh;
@@ -700,26 +761,23 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
   S.it_itab = it;
   put(it, b.itab.data(), sizeof(int) * b.itab.size());
   it += sizeof(int) * b.itab.size();
-  S.it_crf = it;
-  put(it, b.crop_row_field.data(), sizeof(int) * b.crop_row_field.size());
-  it += sizeof(int) * b.crop_row_field.size();
-  S.it_crfirst = it;
-  put(it, b.crop_row_first.data(), sizeof(int) * b.crop_row_first.size());
-  it += sizeof(int) * b.crop_row_first.size();
   S.it_pitch = it;
   put(it, b.pitches.data(), sizeof(int) * b.pitches.size());
   it += sizeof(int) * b.pitches.size();
-  it = align_up(it, 8);
+  it = align_up(it, 16);
+  S.it_crop = it;
+  put(it, b.crop_rows.data(), sizeof(int4) * b.crop_rows.size());
+  it += sizeof(int4) * b.crop_rows.size();
   S.it_pxoff = it;
   put(it, b.px_offs.data(), sizeof(int64_t) * b.px_offs.size());
   it += sizeof(int64_t) * b.px_offs.size();
   S.it_rbo = it;
   put(it, b.rowbuf_offs.data(), sizeof(int64_t) * b.rowbuf_offs.size());
 
-  if (!opt.device_io && opt.do_lockin) {
+  if (!opt.device_io && opt.do_lockin && !opt.weave_geom) {
     for (int i = 0; i < n; ++i) {
-      e = cudaMemcpyAsync(at<char>(ctx, L.o_raw) + b.fp[i].raw_off, in[i].samples,
-                          (size_t)b.fp[i].raw_bytes, cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync(at<char>(ctx, L.o_raw) + b.pp[i].raw_off, in[i].samples,
+                          (size_t)b.pp[i].raw_bytes, cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D samples");
     }
   }
@@ -764,7 +822,7 @@ hvdg::InitArgs init_args(hvdg_ctx* ctx, const Staged& S) {
 hvdg_status stage_prepare(hvdg_ctx* ctx, Staged& S, const RunOpts& opt) {
   const Batch& b = S.b;
   const Layout& L = b.L;
-  const int n = (int)b.fp.size();
+  const int n = (int)b.prep.size();  // source fields
   cudaStream_t s = ctx->stream;
   cudaError_t e;
   mark(ctx, 1);
@@ -806,10 +864,9 @@ hvdg_status stage_prepare(hvdg_ctx* ctx, Staged& S, const RunOpts& opt) {
                           sizeof(float) * p.w, sizeof(float) * p.w, p.h, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D S");
   } else {
-    hvdg::launch_crop(at<hvdg::PrepDesc>(ctx, L.o_prep), at<int>(ctx, S.it_crf),
-                      at<int>(ctx, S.it_crfirst), L.total_lines, at<float>(ctx, L.o_S),
-                      at<int64_t>(ctx, S.it_pxoff), at<int>(ctx, S.it_pitch),
-                      at<int>(ctx, L.o_flags) + 1, s);
+    hvdg::launch_crop(at<hvdg::PrepDesc>(ctx, L.o_prep), at<int4>(ctx, S.it_crop),
+                      (int)b.crop_rows.size(), at<float>(ctx, L.o_S), at<int64_t>(ctx, S.it_pxoff),
+                      at<int>(ctx, S.it_pitch), at<int>(ctx, L.o_flags) + 1, s);
     S.launches += 1;
   }
   if (opt.chi0_in) {
@@ -890,13 +947,16 @@ hvdg_status stage_finish(hvdg_ctx* ctx, Staged& S, hvdg_field_out* out, const Ru
                             sizeof(float2) * p.pitch, sizeof(float2) * p.w, p.h, kind, s);
       if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy chroma");
     }
-    if (out[i].theta) {
-      e = cudaMemcpyAsync(out[i].theta, at<float>(ctx, L.o_theta) + p.theta_off, sizeof(float) * p.fh,
-                          kind, s);
+    // per-field phases (planes that are fields: one source field each)
+    const bool own = b.pp.size() == b.fp.size();
+    if (out[i].theta && own) {
+      e = cudaMemcpyAsync(out[i].theta, at<float>(ctx, L.o_theta) + b.pp[i].theta_off,
+                          sizeof(float) * b.pp[i].fh, kind, s);
       if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy theta");
     }
-    if (out[i].vswitch) {
-      e = cudaMemcpyAsync(out[i].vswitch, at<signed char>(ctx, L.o_vsw) + p.theta_off, p.fh, kind, s);
+    if (out[i].vswitch && own) {
+      e = cudaMemcpyAsync(out[i].vswitch, at<signed char>(ctx, L.o_vsw) + b.pp[i].theta_off,
+                          b.pp[i].fh, kind, s);
       if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy vswitch");
     }
   }
@@ -943,7 +1003,7 @@ hvdg_status run_batch_once(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const 
   const Layout& L = S.b.L;
   cudaStream_t s = ctx->stream;
   if (opt.do_solve) {
-    hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), n, at<float2>(ctx, L.o_X0), s);
+    hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), (int)S.b.fp.size(), at<float2>(ctx, L.o_X0), s);
     S.launches += 1;
   }
   mark(ctx, 2);
@@ -1040,11 +1100,11 @@ hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const
                           sizeof(float2) * p.pitch, sizeof(float2) * p.w, p.h,
                           cudaMemcpyDeviceToDevice, s);
       if (out[i].theta)
-        cudaMemcpyAsync(out[i].theta, at<float>(ctx, L.o_theta) + p.theta_off,
-                        sizeof(float) * p.fh, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(out[i].theta, at<float>(ctx, L.o_theta) + S.b.pp[i].theta_off,
+                        sizeof(float) * S.b.pp[i].fh, cudaMemcpyDeviceToDevice, s);
       if (out[i].vswitch)
-        cudaMemcpyAsync(out[i].vswitch, at<signed char>(ctx, L.o_vsw) + p.theta_off, p.fh,
-                        cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(out[i].vswitch, at<signed char>(ctx, L.o_vsw) + S.b.pp[i].theta_off,
+                        S.b.pp[i].fh, cudaMemcpyDeviceToDevice, s);
     }
     cudaMemcpyAsync(ctx->flags_host, at<int>(ctx, L.o_flags), sizeof(int) * 4,
                     cudaMemcpyDeviceToHost, s);
@@ -1996,10 +2056,10 @@ void split_frame_fields(const int16_t* frame, const hvdg_frame_params& fp, float
   }
 }
 
-// DetectFieldParity (frame_bridge.cpp:102-149).
-int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_params& fp,
-                        const hvdg_geometry& g) {
-  const int fw = fp.frame_width;
+// DetectFieldParity (frame_bridge.cpp:102-149) over a sampler
+// ire(block, field_line, x) of the two de-woven fields in IRE.
+template <typename Ire>
+int detect_field_parity_t(Ire ire, const hvdg_frame_params& fp, const hvdg_geometry& g) {
   const int fal = g.first_active_field_line, lal = last_active_line(g);
   const int a0 = fp.active_video_start, a1 = fp.active_video_end;
   const int lines = lal - fal, width = a1 - a0;
@@ -2009,11 +2069,10 @@ int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_param
   long n = 0;
   for (int r = fal + 1; r + 1 < lal; r += ystep) {
     for (int x = a0; x + 4 <= a1; x += 16) {
-      auto lp = [&](const float* p, int row) {
-        const float* q = p + (size_t)row * fw + x;
-        return 0.25f * (q[0] + q[1] + q[2] + q[3]);
+      auto lp = [&](int k, int row) {
+        return 0.25f * (ire(k, row, x) + ire(k, row, x + 1) + ire(k, row, x + 2) + ire(k, row, x + 3));
       };
-      const float b = lp(b2, r), ac = lp(b1, r), au = lp(b1, r - 1), ad = lp(b1, r + 1);
+      const float b = lp(1, r), ac = lp(0, r), au = lp(0, r - 1), ad = lp(0, r + 1);
       ep += std::fabs(b - 0.5f * (ac + ad));
       em += std::fabs(b - 0.5f * (ac + au));
       ++n;
@@ -2025,6 +2084,29 @@ int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_param
   const double lo = std::min(ep, em), hi = std::max(ep, em);
   if (hi <= 1e-9 || (hi - lo) / hi < 0.02) return 0;
   return ep < em ? +1 : -1;
+}
+
+int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_params& fp,
+                        const hvdg_geometry& g) {
+  const int fw = fp.frame_width;
+  return detect_field_parity_t(
+      [&](int k, int row, int x) { return (k == 0 ? b1 : b2)[(size_t)row * fw + x]; }, fp, g);
+}
+
+// The same vote read straight from an int16 frame: each sample the vote
+// touches is converted exactly as SplitFrameFields converts it.
+int detect_field_parity_frame(const int16_t* frame, const hvdg_frame_params& fp,
+                              const hvdg_geometry& g) {
+  const int f1 = fp.field1_lines, fh = fp.frame_height;
+  const float cpi = (fp.white_level - fp.blanking_level) / 100.0f;
+  return detect_field_parity_t(
+      [&](int k, int row, int x) {
+        const int flat = k == 0 ? row : f1 + row;
+        const bool valid = k == 0 ? row < f1 : flat < fh;
+        const float s = valid ? (float)frame[frame_line_offset(fp, flat) + x] : fp.blanking_level;
+        return (s - fp.blanking_level) / cpi;
+      },
+      fp, g);
 }
 
 int16_t clamp_u10(float v) {
@@ -2071,6 +2153,7 @@ hvdg_status lockin_one(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometr
   pd.nominal_burst = nominal_burst(*g);
   pd.w0 = phase_per_sample(*g);
   pd.adv = line_advance(*g);
+  pd.line_step = 1;
   cudaStream_t s = ctx->stream;
   cudaError_t e = cudaMemcpyAsync(base + o_field, field_ire, fbytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D field");
@@ -2441,6 +2524,226 @@ hvdg_status decode_adjoint_field(hvdg_ctx* ctx, const hvdg_field_in& fi, const h
   if (diag) {
     diag->cg_iterations_run += cg_run + adj_run;
     diag->kernel_launches += 8 + n_outer * 6 + 12;
+  }
+  return HVDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Woven-frame decode: DecodeFrameBuffer (frame_bridge.cpp:168-255, engine
+// DecodeFrame engine.cpp:141-195) and DecodeYcFrameBuffer
+// (frame_bridge.cpp:263-377, engine DecodeChromaOnly engine.cpp:197-237), n
+// independent frames in one batch. On the device: de-weave of the int16
+// frames (k_frame_split), per-field lock-in + burst amplitude, the weave of
+// S and of the line phasors straight into the woven plane (crop rows and
+// line_step), holographic init on the woven plane (column length 2048),
+// then -- composite only -- aniso + IRLS / CG; re-weave and requantisation
+// (k_frame_out). On the host: the field-order vote and the copies.
+// `chroma` frames are the composite frames (yc = false) or the C channel
+// (yc = true, with `luma` the Y channel passed through).
+// ---------------------------------------------------------------------------
+hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
+                                const int16_t* const* luma, int n, const hvdg_frame_params* fp,
+                                const hvdg_config* cfg, hvdg_yc_frame* out, hvdg_diag* diag,
+                                bool yc) {
+  if (!ctx || !fp || !cfg || n < 0 || (n > 0 && (!chroma || !out || (yc && !luma))))
+    return HVDG_ERR_BAD_ARGUMENT;
+  for (int t = 0; t < n; ++t) {
+    if (!chroma[t] || (yc && !luma[t])) return HVDG_ERR_BAD_ARGUMENT;
+    if (!out[t].luma || !out[t].chroma || !out[t].u_plane || !out[t].v_plane)
+      return HVDG_ERR_BAD_ARGUMENT;
+  }
+  const hvdg_frame_params& P = *fp;
+  if (P.frame_width < 1 || P.frame_height < 2 || P.field1_lines < 1 ||
+      P.field1_lines > P.frame_height || !(P.white_level != P.blanking_level))
+    return HVDG_ERR_BAD_GEOMETRY;
+  const hvdg_geometry g = geometry_from_params(P);
+  hvdg_status st = check_geometry(&g);
+  if (st != HVDG_OK) return st;
+  const int lines = last_active_line(g) - g.first_active_field_line;
+  const int w = g.active_video_end - g.active_video_start;
+  st = check_plane(w, 2 * lines, uses_vswitch(g), hvdg::kColFftWide);
+  if (st != HVDG_OK) {
+    ctx->last_error = "woven frame beyond the device-path limits";
+    return st;
+  }
+  if (cfg->diag_prior > 0.0f || cfg->symmetry_variant) return HVDG_ERR_UNSUPPORTED;
+  if (diag) std::memset(diag, 0, sizeof(*diag));
+  if (n == 0) return HVDG_OK;
+  cudaSetDevice(ctx->device);
+  const int fw = P.frame_width, fh = P.frame_height, f1 = P.field1_lines;
+  // the woven plane: no blanking, 2 x active lines, the field's columns
+  hvdg_geometry gw = g;
+  gw.field_height = 2 * lines;
+  gw.first_active_field_line = 0;
+  gw.last_active_field_line = 2 * lines;
+  // field order per frame (ResolveField1IsBottom, frame_bridge.cpp:152-160;
+  // the Y/C path resolves auto to the format convention, :283-287). The
+  // field flagged first lands on the even woven rows (engine.cpp:55-57).
+  std::vector<hvdg_field_in> fi(2 * (size_t)n);
+  for (int t = 0; t < n; ++t) {
+    bool f1_bottom = cfg->field_order == 2;
+    if (!yc && cfg->field_order == 0) f1_bottom = detect_field_parity_frame(chroma[t], P, g) < 0;
+    for (int k = 0; k < 2; ++k) {
+      hvdg_field_in& f = fi[2 * t + k];
+      std::memset(&f, 0, sizeof(f));
+      f.samples = nullptr;
+      f.sample_type = HVDG_SAMPLES_F32_IRE;
+      f.parity = (k == 0) == !f1_bottom ? 0 : 1;
+      f.geometry = &g;
+      f.irls_outer = 0;
+      f.cg_iterations = -1;
+    }
+  }
+  RunOpts opt;
+  opt.weave_geom = &gw;
+  opt.do_solve = !yc && cfg->cg_iterations > 0 && !cfg->monochrome;
+  // extra region: line offsets | source frames | pass-through luma | outputs
+  const int64_t need = frame_line_offset(P, fh - 1) + fw;  // samples the reference reads
+  const int64_t stride = (int64_t)align_up((size_t)need, 128);
+  const size_t npx = (size_t)fw * fh;
+  const size_t o_lines = 0;
+  const size_t o_src = align_up(sizeof(int64_t) * fh, 256);
+  const size_t o_pass = align_up(o_src + sizeof(int16_t) * stride * n, 256);
+  const size_t o_ol = align_up(o_pass + (yc ? sizeof(int16_t) * stride * n : 0), 256);
+  const size_t o_oc = align_up(o_ol + sizeof(int16_t) * npx * n, 256);
+  const size_t o_ou = align_up(o_oc + sizeof(int16_t) * npx * n, 256);
+  const size_t o_ov = align_up(o_ou + sizeof(double) * npx * n, 256);
+  const size_t xbytes = align_up(o_ov + sizeof(double) * npx * n, 256);
+  Staged S;
+  st = stage_upload(ctx, fi.data(), 2 * n, cfg, opt, xbytes, S);
+  if (st != HVDG_OK) return st;
+  const Batch& b = S.b;
+  const Layout& L = b.L;
+  cudaStream_t s = ctx->stream;
+  char* X = at<char>(ctx, S.extra);
+  std::vector<int64_t> loff(fh);
+  for (int y = 0; y < fh; ++y) loff[y] = frame_line_offset(P, y);
+  cudaError_t e = cudaMemcpyAsync(X + o_lines, loff.data(), sizeof(int64_t) * fh,
+                                  cudaMemcpyHostToDevice, s);
+  for (int t = 0; t < n && e == cudaSuccess; ++t) {
+    e = cudaMemcpyAsync(X + o_src + sizeof(int16_t) * stride * t, chroma[t], sizeof(int16_t) * need,
+                        cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && yc)
+      e = cudaMemcpyAsync(X + o_pass + sizeof(int16_t) * stride * t, luma[t],
+                          sizeof(int16_t) * need, cudaMemcpyHostToDevice, s);
+  }
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D frames");
+  const float cpi = (P.white_level - P.blanking_level) / 100.0f;
+  hvdg::FrameSplitArgs sp;
+  sp.frames = reinterpret_cast<const int16_t*>(X + o_src);
+  sp.frame_stride = stride;
+  sp.line_off = reinterpret_cast<const int64_t*>(X + o_lines);
+  sp.fw = fw;
+  sp.fh = fh;
+  sp.f1 = f1;
+  sp.center = yc ? P.chroma_dc : P.blanking_level;
+  sp.codes_per_ire = cpi;
+  sp.fields = at<float>(ctx, L.o_raw);
+  sp.field_stride = (b.pp.size() > 1 ? b.pp[1].raw_off - b.pp[0].raw_off : 0) / (int64_t)sizeof(float);
+  hvdg::launch_frame_split(sp, n, s);
+  S.launches += 1;
+  st = stage_prepare(ctx, S, opt);
+  if (st != HVDG_OK) return st;
+  hvdg::launch_burst_amplitude(at<hvdg::PrepDesc>(ctx, L.o_prep), 2 * n, at<float>(ctx, L.o_amp), s);
+  S.launches += 1;
+  if (opt.do_solve) {
+    hvdg::launch_aniso(at<FieldDesc>(ctx, L.o_fields), n, at<float2>(ctx, L.o_X0), s);
+    S.launches += 1;
+  }
+  mark(ctx, 2);
+  if (opt.do_solve) {
+    const hvdg::SolverArgs sa = solver_args(ctx, S);
+    e = hvdg::launch_solver(sa, solver_grid(ctx, L.total_units, opt.ctas_per_sm), s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "solver launch");
+    S.launches += 1;
+  }
+  mark(ctx, 3);
+  const FieldPlan& p0 = b.fp[0];
+  hvdg::FrameOutArgs fo;
+  fo.Y = at<float>(ctx, L.o_Y);
+  fo.chi = at<float2>(ctx, L.o_X0);
+  fo.S = at<float>(ctx, L.o_S);
+  fo.plane_stride = n > 1 ? b.fp[1].px_off - p0.px_off : 0;
+  fo.pitch = p0.pitch;
+  fo.h = p0.h;
+  fo.w = p0.w;
+  fo.line_phasor = at<float4>(ctx, L.o_lineph);
+  fo.col_phasor = at<float2>(ctx, L.o_colph);
+  fo.amp = at<float>(ctx, L.o_amp);
+  fo.passthrough = reinterpret_cast<const int16_t*>(X + (yc ? o_pass : o_src));
+  fo.frame_stride = stride;
+  fo.line_off = reinterpret_cast<const int64_t*>(X + o_lines);
+  fo.fw = fw;
+  fo.fh = fh;
+  fo.f1 = f1;
+  fo.fal = g.first_active_field_line;
+  fo.a0 = P.active_video_start;
+  fo.blank = P.blanking_level;
+  fo.scale = cpi;
+  fo.chroma_gain = cfg->chroma_gain;
+  fo.nominal_burst = nominal_burst(g);
+  fo.acc = cfg->acc ? 1 : 0;
+  fo.yc = yc ? 1 : 0;
+  fo.mono = (!yc && cfg->monochrome) ? 1 : 0;
+  fo.luma = reinterpret_cast<int16_t*>(X + o_ol);
+  fo.chroma = reinterpret_cast<int16_t*>(X + o_oc);
+  fo.u = reinterpret_cast<double*>(X + o_ou);
+  fo.v = reinterpret_cast<double*>(X + o_ov);
+  hvdg::launch_frame_out(fo, n, s);
+  S.launches += 1;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "frame kernels");
+  for (int t = 0; t < n && e == cudaSuccess; ++t) {
+    e = cudaMemcpyAsync(out[t].luma, fo.luma + npx * t, sizeof(int16_t) * npx,
+                        cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out[t].chroma, fo.chroma + npx * t, sizeof(int16_t) * npx,
+                          cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out[t].u_plane, fo.u + npx * t, sizeof(double) * npx,
+                          cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out[t].v_plane, fo.v + npx * t, sizeof(double) * npx,
+                          cudaMemcpyDeviceToHost, s);
+  }
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "D2H frames");
+  int flags[4] = {0, 0, 0, 0};
+  float amp01[2] = {0.f, 0.f};
+  std::vector<FieldCtl> ctl(n);
+  e = cudaMemcpyAsync(flags, at<int>(ctx, L.o_flags), sizeof(flags), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(amp01, at<float>(ctx, L.o_amp), sizeof(amp01), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && diag)
+    e = cudaMemcpyAsync(ctl.data(), at<FieldCtl>(ctx, L.o_ctl), sizeof(FieldCtl) * n,
+                        cudaMemcpyDeviceToHost, s);
+  mark(ctx, 4);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "frame decode sync");
+  if (diag) {
+    diag->ms_total = elapsed(ctx, 0, 4);
+    diag->ms_solver = elapsed(ctx, 2, 3);
+    diag->ms_init = elapsed(ctx, 1, 2);
+    float acc = 1.0f;
+    if (cfg->acc) {
+      const float m = 0.5f * (amp01[0] + amp01[1]);
+      acc = std::min(std::max(nominal_burst(g) / std::max(m, 1.0f), 0.5f), 2.0f);
+    }
+    diag->acc_gain = acc;
+    for (int i = 0; i < n; ++i) {
+      if (opt.do_solve) diag->cg_iterations_run += ctl[i].cg_iters;
+      if (opt.do_solve) diag->solver_pixel_iters += (int64_t)ctl[i].cg_iters * b.fp[i].h * b.fp[i].w;
+      if (opt.do_solve)
+        diag->solver_pixel_outers += (int64_t)b.fields[i].n_outer * b.fp[i].h * b.fp[i].w;
+    }
+    diag->kernel_launches = S.launches;
+  }
+  if (flags[1]) {
+    ctx->last_error = "non-finite input samples";
+    return HVDG_ERR_NONFINITE_INPUT;
+  }
+  if (flags[0]) {
+    ctx->last_error = "device-side bounded wait expired in the solver";
+    return HVDG_ERR_DEVICE_TIMEOUT;
   }
   return HVDG_OK;
 }
@@ -2882,6 +3185,33 @@ hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* cons
     }
   }
   return HVDG_OK;
+}
+
+hvdg_status hvdg_decode_frame_buffer(hvdg_ctx* ctx, const int16_t* frame,
+                                     const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                     hvdg_yc_frame* out) {
+  if (!frame || !out) return HVDG_ERR_BAD_ARGUMENT;
+  return decode_woven_frames(ctx, &frame, nullptr, 1, fp, cfg, out, nullptr, false);
+}
+
+hvdg_status hvdg_decode_frame_buffers(hvdg_ctx* ctx, const int16_t* const* frames, int n_frames,
+                                      const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                      hvdg_yc_frame* out, hvdg_diag* diag) {
+  return decode_woven_frames(ctx, frames, nullptr, n_frames, fp, cfg, out, diag, false);
+}
+
+hvdg_status hvdg_decode_yc_frame_buffer(hvdg_ctx* ctx, const int16_t* luma, const int16_t* chroma,
+                                        const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                        hvdg_yc_frame* out) {
+  if (!luma || !chroma || !out) return HVDG_ERR_BAD_ARGUMENT;
+  return decode_woven_frames(ctx, &chroma, &luma, 1, fp, cfg, out, nullptr, true);
+}
+
+hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* luma,
+                                         const int16_t* const* chroma, int n_frames,
+                                         const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                         hvdg_yc_frame* out, hvdg_diag* diag) {
+  return decode_woven_frames(ctx, chroma, luma, n_frames, fp, cfg, out, diag, true);
 }
 
 hvdg_status hvdg_holographic_init(hvdg_ctx* ctx, const float* s, const float* theta_active,

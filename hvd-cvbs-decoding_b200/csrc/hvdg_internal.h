@@ -18,7 +18,8 @@ namespace hvdg {
 constexpr int kStrip = 64;        // solver strip width (columns per warp unit)
 constexpr int kMaxLines = 1024;   // max field lines handled by the lock-in kernel
 constexpr int kRowFft = 2048;     // init: row cyclic-convolution length
-constexpr int kColFft = 1024;     // init: column cyclic-convolution length
+constexpr int kColFft = 1024;     // init: column cyclic-convolution length (field planes)
+constexpr int kColFftWide = 2048; // init: column length of taller planes (woven frames)
 constexpr int kInitPad = 16;      // init: reflect-101 row pad (holographic_init.cpp:214-222)
 
 // Per-field descriptor (device copy is read-only during a launch except the
@@ -62,7 +63,8 @@ struct GeomDesc {
   int w, h, hp;        // active width, active lines, padded lines (h + 2 pad)
   int pad;             // row pad
   int khat_row_off;    // offset (float2) of the 2 row kernels' spectra (2 * kRowFft)
-  int khat_col_off;    // offset (float2) of the 2 column kernels' spectra (2 * kColFft)
+  int khat_col_off;    // offset (float2) of the 2 column kernels' spectra (2 * col_m)
+  int col_m;           // column convolution length: kColFft or kColFftWide
 };
 
 // Solver control block, one per field (written by the last arriver of each

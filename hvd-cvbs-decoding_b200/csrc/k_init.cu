@@ -166,55 +166,82 @@ __global__ void __launch_bounds__(256) k_init_rows(InitArgs a) {
 }
 
 // ---- columns ---------------------------------------------------------------
-// grid = (column groups of 8, over all fields); block = 256 (8 warps, one
-// column each); dynamic smem = 8 * 2 * kColFft float2.
+// grid = (column groups over all fields); block = 256; dynamic smem =
+// 2 * 8 * kColFft float2 = 2 * 4 * kColFftWide float2. The column length M of
+// a geometry is 1024 (field planes: 2 hp - 1 <= 1024; 8 columns per CTA, one
+// warp each) or 2048 (woven frames, hp up to 1024; 4 columns per CTA, two
+// warps each, paired by a named barrier).
 constexpr int kColGroup = 8;
-__global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
+constexpr int kColGroupWide = 4;
+constexpr int kColSmem = 2 * kColGroup * kColFft * (int)sizeof(float2);
+static_assert(2 * kColGroupWide * kColFftWide * (int)sizeof(float2) == kColSmem,
+              "both column variants use the same shared-memory footprint");
+
+struct PairSync {  // the 64 threads of one column (named barrier 1 + pair)
+  int id;
+  __device__ void operator()() const { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+};
+
+template <int M, int G, typename Sync>
+__device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDesc& f,
+                                               const GeomDesc& gd, int f_idx, int x0,
+                                               const float2* __restrict__ tw, int ct, int nct,
+                                               int col, Sync sync) {
   extern __shared__ float2 sm_cols[];
+  float2* A = sm_cols + col * 2 * M;
+  float2* B = A + M;
+  for (int v = 0; v < 2; ++v) {
+    const float2* src = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
+    // cooperative coalesced load: thread -> (row, column-in-group)
+    for (int i = threadIdx.x; i < M * G; i += blockDim.x) {
+      const int row = i / G, c = i % G;
+      float2 val = make_float2(0.f, 0.f);
+      if (row < gd.hp && x0 + c < f.w) val = src[(int64_t)row * f.pitch + x0 + c];
+      sm_cols[c * 2 * M + row] = val;
+    }
+    __syncthreads();
+    float2* spec = fft_stockham<M, false>(A, B, tw, ct, nct, sync);
+    const float2* kh = a.khat + gd.khat_col_off + v * M;
+    float2* other = spec == A ? B : A;
+    for (int i = ct; i < M; i += nct) other[i] = cmul(spec[i], __ldg(kh + i));
+    sync();
+    float2* res = fft_stockham<M, true>(other, spec, tw, ct, nct, sync);
+    // result must land where the cooperative store reads it: column c at A_c
+    if (res != A)
+      for (int i = ct; i < M; i += nct) A[i] = res[i];
+    __syncthreads();
+    if (a.adj_out) {
+      // adjoint mode: every padded row (the transposed crop)
+      float2* dst = a.adj_out + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
+      for (int i = threadIdx.x; i < gd.hp * G; i += blockDim.x) {
+        const int y = i / G, c = i % G;
+        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * M + y];
+      }
+    } else {
+      float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
+      for (int i = threadIdx.x; i < f.h * G; i += blockDim.x) {
+        const int y = i / G, c = i % G;
+        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * M + y + gd.pad];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gidx = blockIdx.x;
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
-  const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
-  float2* A = sm_cols + warp * 2 * kColFft;
-  float2* B = A + kColFft;
-  for (int v = 0; v < 2; ++v) {
-    const float2* src = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
-    // cooperative coalesced load: thread -> (row, column-in-group)
-    for (int i = threadIdx.x; i < kColFft * kColGroup; i += blockDim.x) {
-      const int row = i / kColGroup, c = i % kColGroup;
-      float2 val = make_float2(0.f, 0.f);
-      if (row < gd.hp && x0 + c < f.w) val = src[(int64_t)row * f.pitch + x0 + c];
-      sm_cols[c * 2 * kColFft + row] = val;
-    }
-    __syncthreads();
-    float2* spec = fft_stockham<kColFft, false>(A, B, a.tw_col, lane, 32, WarpSync());
-    const float2* kh = a.khat + gd.khat_col_off + v * kColFft;
-    float2* other = spec == A ? B : A;
-    for (int i = lane; i < kColFft; i += 32) other[i] = cmul(spec[i], __ldg(kh + i));
-    __syncwarp();
-    float2* res = fft_stockham<kColFft, true>(other, spec, a.tw_col, lane, 32, WarpSync());
-    // result must land where the cooperative store reads it: column c at A_c
-    if (res != A)
-      for (int i = lane; i < kColFft; i += 32) A[i] = res[i];
-    __syncthreads();
-    if (a.adj_out) {
-      // adjoint mode: every padded row (the transposed crop)
-      float2* dst = a.adj_out + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
-      for (int i = threadIdx.x; i < gd.hp * kColGroup; i += blockDim.x) {
-        const int y = i / kColGroup, c = i % kColGroup;
-        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * kColFft + y];
-      }
-    } else {
-      float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
-      for (int i = threadIdx.x; i < f.h * kColGroup; i += blockDim.x) {
-        const int y = i / kColGroup, c = i % kColGroup;
-        if (x0 + c < f.w)
-          dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * kColFft + y + gd.pad];
-      }
-    }
-    __syncthreads();
+  if (gd.col_m == kColFftWide) {
+    const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
+    const int pair = threadIdx.x >> 6;
+    init_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 63,
+                                               64, pair, PairSync{1 + pair});
+  } else {
+    const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
+    init_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, lane, 32, warp, WarpSync());
   }
 }
 
@@ -310,8 +337,9 @@ __global__ void __launch_bounds__(256) k_init_blend(InitArgs a) {
 // ---- auto chroma anisotropy (variational.cpp:130-196) ----------------------
 // One CTA (1024 threads) per field: p98 of |delta| of 2-line (NTSC) / 4-line
 // (PAL) group averages, sampled at odd group rows and every 3rd column,
-// exact k-th element by radix select.
-constexpr int kAnisoMax = 24576;
+// exact k-th element by radix select; the horizontal and the vertical
+// samples take turns in one shared buffer.
+constexpr int kAnisoMax = 49152;
 __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2* __restrict__ chi0) {
   extern __shared__ float sm_an[];
   __shared__ unsigned hist[256];
@@ -324,34 +352,27 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
     const int nt = Hh / 2;                // t = 1, 3, 5, ... < Hh
     const int nx = (f.w - 1 + 2) / 3;     // x = 1, 4, 7, ... < w
     int n = nt * nx;
-    if (n > kAnisoMax) n = kAnisoMax;     // geometry guard (host rejects larger)
-    float* gx = sm_an;
-    float* gy = sm_an + kAnisoMax;
+    if (n > kAnisoMax) n = kAnisoMax;     // geometry guard (the host rejects larger)
     const float2* c = chi0 + f.px_off;
     const float inv = 1.0f / (float)group;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int ti = i / nx, xi = i % nx;
-      const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
-      float2 p = make_float2(0.f, 0.f), pl = p, pu = p;
-      for (int k = 0; k < group; ++k) {
-        p = cadd(p, c[(int64_t)(group * tt + k) * f.pitch + x]);
-        pl = cadd(pl, c[(int64_t)(group * tt + k) * f.pitch + x - 1]);
-        pu = cadd(pu, c[(int64_t)(group * (tt - 1) + k) * f.pitch + x]);
+    float p98[2] = {0.f, 0.f};
+    for (int axis = 0; axis < 2; ++axis) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int ti = i / nx, xi = i % nx;
+        const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
+        float2 p = make_float2(0.f, 0.f), q = p;
+        for (int k = 0; k < group; ++k) {
+          p = cadd(p, c[(int64_t)(group * tt + k) * f.pitch + x]);
+          q = cadd(q, axis == 0 ? c[(int64_t)(group * tt + k) * f.pitch + x - 1]
+                                : c[(int64_t)(group * (tt - 1) + k) * f.pitch + x]);
+        }
+        sm_an[i] = sqrtf(cnorm(csub(cscale(p, inv), cscale(q, inv))));
       }
-      p = cscale(p, inv);
-      pl = cscale(pl, inv);
-      pu = cscale(pu, inv);
-      gx[i] = sqrtf(cnorm(csub(p, pl)));
-      gy[i] = sqrtf(cnorm(csub(p, pu)));
+      __syncthreads();
+      if (n > 0) p98[axis] = block_select_kth(sm_an, n, n - 1 - n / 50, hist, bc);
+      __syncthreads();
     }
-    __syncthreads();
-    float px = 0.f, py = 0.f;
-    if (n > 0) {
-      const int k = n - 1 - n / 50;
-      px = block_select_kth(gx, n, k, hist, bc);
-      py = block_select_kth(gy, n, k, hist, bc);
-    }
-    const float r = py / fmaxf(px, 1e-6f);
+    const float r = p98[1] / fmaxf(p98[0], 1e-6f);
     if (f.is_pal)
       aniso = fminf(fmaxf(0.7f + 0.9f * (r - 1.3f), 0.55f), 1.0f);
     else
@@ -363,13 +384,12 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
   }
 }
 
-constexpr int kAnisoSmem = 2 * 24576 * (int)sizeof(float);
+constexpr int kAnisoSmem = kAnisoMax * (int)sizeof(float);
 
 void configure_init_kernels() {
   cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        3 * kRowFft * (int)sizeof(float2));
-  cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kColGroup * 2 * kColFft * (int)sizeof(float2));
+  cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
   cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, kAnisoSmem);
 }
 
@@ -377,7 +397,7 @@ void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int tota
                  cudaStream_t st) {
   static bool configured = false;
   const int row_smem = 3 * kRowFft * sizeof(float2);
-  const int col_smem = kColGroup * 2 * kColFft * sizeof(float2);
+  const int col_smem = kColSmem;
   if (!configured) {
     configure_init_kernels();
     configured = true;
@@ -395,14 +415,14 @@ void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cg
     configured = true;
   }
   const int row_smem = 3 * kRowFft * sizeof(float2);
-  const int col_smem = kColGroup * 2 * kColFft * sizeof(float2);
+  const int col_smem = kColSmem;
   if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
   if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
 }
 
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {
   static bool configured = false;
-  const int smem = 2 * kAnisoMax * sizeof(float);
+  const int smem = kAnisoSmem;
   if (!configured) {
     configure_init_kernels();
     configured = true;
@@ -411,7 +431,7 @@ void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStr
 }
 
 int aniso_max_samples() { return kAnisoMax; }
-int init_col_group() { return kColGroup; }
+int init_col_group(int col_m) { return col_m == kColFftWide ? kColGroupWide : kColGroup; }
 int init_blend_tile() { return kBT; }
 
 }  // namespace hvdg

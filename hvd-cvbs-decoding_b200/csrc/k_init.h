@@ -16,7 +16,7 @@ struct InitArgs {
   const float2* col_phasor;    // per geometry column exp(i w0 (a0 + x))
   const float2* khat;          // kernel spectra (row / column, 2 variants each)
   const float2* tw_row;        // exp(-2 pi i k / kRowFft)
-  const float2* tw_col;        // exp(-2 pi i k / kColFft)
+  const float2* tw_col;        // exp(-2 pi i k / kColFft) (the wide columns use tw_row)
   float2* rowbuf;              // row-filtered variants: per field 2 x hp x pitch
   const int64_t* rowbuf_off;   // per field offset into rowbuf (float2)
   float2* chi1;                // variant outputs (pitched like the planes)
@@ -47,7 +47,8 @@ void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cg
                                 cudaStream_t st);
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st);
 int aniso_max_samples();
-int init_col_group();
+// columns per CTA of the column pass for a geometry with column length col_m
+int init_col_group(int col_m);
 int init_blend_tile();
 
 }  // namespace hvdg

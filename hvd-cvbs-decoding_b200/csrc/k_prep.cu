@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(256) k_burst_lockin(const PrepDesc* __restrict
     if (out.line_phasor && y >= p.fal && y < p.lal) {
       double s, c;
       sincos(th, &s, &c);
-      out.line_phasor[p.line_off + (y - p.fal)] =
+      out.line_phasor[p.line_off + (y - p.fal) * p.line_step] =
           make_float4((float)c, (float)s, sw[y] < 0 ? -1.0f : 1.0f, 0.0f);
     }
   }
@@ -321,18 +321,19 @@ __global__ void __launch_bounds__(256) k_burst_amplitude(const PrepDesc* __restr
 }
 
 // Active crop + level conversion into the pitched S plane; zero fill of the
-// pitch padding; non-finite detection. grid = (rows of all fields).
-__global__ void k_crop(const PrepDesc* __restrict__ descs, const int* __restrict__ row_field,
-                       const int* __restrict__ row_first, float* __restrict__ S,
-                       const int64_t* __restrict__ px_off, const int* __restrict__ pitch,
-                       int* __restrict__ nonfinite) {
-  const int r = blockIdx.x;
-  const int f = row_field[r];
-  const int y = r - row_first[f];
-  const PrepDesc p = descs[f];
+// pitch padding; non-finite detection. grid = (rows of all planes); row r
+// copies source line rows[r].w of source field rows[r].z into row rows[r].y
+// of plane rows[r].x (a field's own active picture, or one line of a woven
+// frame).
+__global__ void k_crop(const PrepDesc* __restrict__ descs, const int4* __restrict__ rows,
+                       float* __restrict__ S, const int64_t* __restrict__ px_off,
+                       const int* __restrict__ pitch, int* __restrict__ nonfinite) {
+  const int4 rw = rows[blockIdx.x];
+  const int f = rw.x;
+  const PrepDesc p = descs[rw.z];
   const int w = p.a1 - p.a0;
-  float* dst = S + px_off[f] + (int64_t)y * pitch[f];
-  const int64_t src = (int64_t)(p.fal + y) * p.fw + p.a0;
+  float* dst = S + px_off[f] + (int64_t)rw.y * pitch[f];
+  const int64_t src = (int64_t)rw.w * p.fw + p.a0;
   for (int x = threadIdx.x; x < pitch[f]; x += blockDim.x) {
     float v = 0.0f;
     if (x < w) {
@@ -361,12 +362,10 @@ void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStre
 void launch_burst_amplitude(const PrepDesc* d_descs, int n, float* d_amp, cudaStream_t st) {
   if (n > 0) k_burst_amplitude<<<n, 256, 0, st>>>(d_descs, d_amp);
 }
-void launch_crop(const PrepDesc* d_descs, const int* d_row_field, const int* d_row_first,
-                 int total_rows, float* d_S, const int64_t* d_px_off, const int* d_pitch,
-                 int* d_nonfinite, cudaStream_t st) {
+void launch_crop(const PrepDesc* d_descs, const int4* d_rows, int total_rows, float* d_S,
+                 const int64_t* d_px_off, const int* d_pitch, int* d_nonfinite, cudaStream_t st) {
   if (total_rows > 0)
-    k_crop<<<total_rows, 256, 0, st>>>(d_descs, d_row_field, d_row_first, d_S, d_px_off,
-                                       d_pitch, d_nonfinite);
+    k_crop<<<total_rows, 256, 0, st>>>(d_descs, d_rows, d_S, d_px_off, d_pitch, d_nonfinite);
 }
 
 }  // namespace hvdg

@@ -24,8 +24,8 @@ struct PrepDesc {
   double adv;              // line advance
   float chroma_phase_off;  // -chroma_phase_deg * pi / 180 (float, as the reference)
   int theta_off;           // offset of this field in the full-field per-line outputs
-  int line_off;            // offset of this field's ACTIVE lines in the line-phasor table
-  int pad0;
+  int line_off;            // line-phasor index of this field's first ACTIVE line
+  int line_step;           // index step per active line (1; 2 in a woven frame)
 };
 
 struct LockinOut {
@@ -38,8 +38,8 @@ struct LockinOut {
 void configure_prep_kernels();
 void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStream_t st);
 void launch_burst_amplitude(const PrepDesc* d_descs, int n, float* d_amp, cudaStream_t st);
-void launch_crop(const PrepDesc* d_descs, const int* d_row_field, const int* d_row_first,
-                 int total_rows, float* d_S, const int64_t* d_px_off, const int* d_pitch,
-                 int* d_nonfinite, cudaStream_t st);
+// rows: per S row (plane, plane row, source field, source line)
+void launch_crop(const PrepDesc* d_descs, const int4* d_rows, int total_rows, float* d_S,
+                 const int64_t* d_px_off, const int* d_pitch, int* d_nonfinite, cudaStream_t st);
 
 }  // namespace hvdg

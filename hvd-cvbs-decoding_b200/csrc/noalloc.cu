@@ -87,7 +87,7 @@ extern "C" hvdg_status hvdg_holographic_init_noalloc(const float* s, const float
   int hp = 0, pad = 0;
   hvdg::init_tables_for(*g, &khat, &colph, &twr, &twc, &hp, &pad);
   const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
-  const int cgroup = hvdg::init_col_group(), bt = hvdg::init_blend_tile();
+  const int cgroup = hvdg::init_col_group(hvdg::kColFft), bt = hvdg::init_blend_tile();
   const int ngroups = (w + cgroup - 1) / cgroup;
   const int ntiles = ((h + bt - 1) / bt) * ((w + bt - 1) / bt);
 
@@ -137,6 +137,7 @@ extern "C" hvdg_status hvdg_holographic_init_noalloc(const float* s, const float
   gd.pad = pad;
   gd.khat_row_off = 0;
   gd.khat_col_off = 2 * hvdg::kRowFft;
+  gd.col_m = hvdg::kColFft;
   std::vector<float4> lph(h);
   for (int y = 0; y < h; ++y) {
     const double th = (double)theta_active[y];

@@ -332,6 +332,16 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_decode_frame_sequence_window.argtypes = [
         vp, P(vp), C.c_int, C.c_int, C.c_int, P(FrameParams), P(Config), P(YcFrame), P(Diag)]
     lib.hvdg_decode_frame_sequence_window.restype = C.c_int
+    lib.hvdg_decode_frame_buffer.argtypes = [vp, vp, P(FrameParams), P(Config), P(YcFrame)]
+    lib.hvdg_decode_frame_buffer.restype = C.c_int
+    lib.hvdg_decode_frame_buffers.argtypes = [vp, P(vp), C.c_int, P(FrameParams), P(Config),
+                                              P(YcFrame), P(Diag)]
+    lib.hvdg_decode_frame_buffers.restype = C.c_int
+    lib.hvdg_decode_yc_frame_buffer.argtypes = [vp, vp, vp, P(FrameParams), P(Config), P(YcFrame)]
+    lib.hvdg_decode_yc_frame_buffer.restype = C.c_int
+    lib.hvdg_decode_yc_frame_buffers.argtypes = [vp, P(vp), P(vp), C.c_int, P(FrameParams),
+                                                 P(Config), P(YcFrame), P(Diag)]
+    lib.hvdg_decode_yc_frame_buffers.restype = C.c_int
     lib.hvdg_burst_lockin.argtypes = [vp, vp, P(Geometry), vp, vp]
     lib.hvdg_burst_lockin.restype = C.c_int
     lib.hvdg_burst_amplitude.argtypes = [vp, vp, P(Geometry), P(C.c_float)]

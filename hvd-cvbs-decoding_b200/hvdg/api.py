@@ -339,3 +339,74 @@ def _decode_frames(self, frames, core_begin, core_end, fp, cfg):
 
 
 Context.decode_frame_sequence_window = _decode_frames
+
+
+def _yc_frames(fp, m):
+    sz = fp.frame_width * fp.frame_height
+    res = [dict(luma=np.zeros(sz, np.int16), chroma=np.zeros(sz, np.int16),
+                u=np.zeros(sz, np.float64), v=np.zeros(sz, np.float64)) for _ in range(m)]
+    outs = (_cabi.YcFrame * max(m, 1))()
+    for t, r in enumerate(res):
+        outs[t].luma = r["luma"].ctypes.data
+        outs[t].chroma = r["chroma"].ctypes.data
+        outs[t].u_plane = r["u"].ctypes.data
+        outs[t].v_plane = r["v"].ctypes.data
+    return res, outs
+
+
+def _ptrs(arrs):
+    return (C.c_void_p * max(len(arrs), 1))(*[a.ctypes.data for a in arrs])
+
+
+def _decode_frame_buffer(self, frame, fp, cfg):
+    """hvd::DecodeFrameBuffer: one flat int16 field-sequential composite
+    frame -> dict(luma, chroma, u, v) (frame_width x frame_height each)."""
+    fr = np.ascontiguousarray(frame, dtype=np.int16)
+    res, outs = _yc_frames(fp, 1)
+    st = self.lib.hvdg_decode_frame_buffer(self._h, fr.ctypes.data, C.byref(fp), C.byref(cfg),
+                                           outs)
+    self._check(st, "hvdg_decode_frame_buffer")
+    return res[0]
+
+
+def _decode_frame_buffers(self, frames, fp, cfg):
+    """n independent frames of decode_frame_buffer in one batch."""
+    fr = [np.ascontiguousarray(f, dtype=np.int16) for f in frames]
+    res, outs = _yc_frames(fp, len(fr))
+    self.last_diag = Diag()
+    st = self.lib.hvdg_decode_frame_buffers(self._h, _ptrs(fr), len(fr), C.byref(fp),
+                                            C.byref(cfg), outs, C.byref(self.last_diag))
+    self._check(st, "hvdg_decode_frame_buffers")
+    return res
+
+
+def _decode_yc_frame_buffer(self, luma, chroma, fp, cfg):
+    """hvd::DecodeYcFrameBuffer: Y and C int16 frames -> dict(luma, chroma, u, v)."""
+    y = np.ascontiguousarray(luma, dtype=np.int16)
+    c = np.ascontiguousarray(chroma, dtype=np.int16)
+    res, outs = _yc_frames(fp, 1)
+    st = self.lib.hvdg_decode_yc_frame_buffer(self._h, y.ctypes.data, c.ctypes.data, C.byref(fp),
+                                              C.byref(cfg), outs)
+    self._check(st, "hvdg_decode_yc_frame_buffer")
+    return res[0]
+
+
+def _decode_yc_frame_buffers(self, lumas, chromas, fp, cfg):
+    """n independent frames of decode_yc_frame_buffer in one batch."""
+    ys = [np.ascontiguousarray(a, dtype=np.int16) for a in lumas]
+    cs = [np.ascontiguousarray(a, dtype=np.int16) for a in chromas]
+    if len(ys) != len(cs):
+        raise ValueError("one chroma frame per luma frame")
+    res, outs = _yc_frames(fp, len(ys))
+    self.last_diag = Diag()
+    st = self.lib.hvdg_decode_yc_frame_buffers(self._h, _ptrs(ys), _ptrs(cs), len(ys),
+                                               C.byref(fp), C.byref(cfg), outs,
+                                               C.byref(self.last_diag))
+    self._check(st, "hvdg_decode_yc_frame_buffers")
+    return res
+
+
+Context.decode_frame_buffer = _decode_frame_buffer
+Context.decode_frame_buffers = _decode_frame_buffers
+Context.decode_yc_frame_buffer = _decode_yc_frame_buffer
+Context.decode_yc_frame_buffers = _decode_yc_frame_buffers

@@ -159,8 +159,10 @@ def _field_phase(standard: int, field_index: int, base: float) -> float:
 def make_field(seed: int, standard: int = _cabi.STD_NTSC, noise_sigma: float = 0.5,
                field_index: int = 0, parity: int | None = None, scene: Scene | None = None,
                theta_base: float | None = None,
-               geometry: _cabi.Geometry | None = None) -> FieldSample:
-    """One composite field as uint16 codes, plus its ground truth."""
+               geometry: _cabi.Geometry | None = None, return_parts: bool = False):
+    """One composite field as uint16 codes, plus its ground truth. With
+    return_parts: (field, luma part, chroma part, noise) in IRE, the parts
+    being the noiseless luma (+ sync) and chroma (+ burst) of the field."""
     g = geometry or _cabi.default_geometry(standard)
     rng = np.random.default_rng(np.uint64(seed) * np.uint64(7919) + np.uint64(field_index))
     sc = scene or make_scene(seed, standard, geometry=g)
@@ -206,12 +208,14 @@ def make_field(seed: int, standard: int = _cabi.STD_NTSC, noise_sigma: float = 0
     if pal:
         car = np.where(vsw[:, None] < 0, -np.conj(car), car)
 
-    ire = np.zeros((fh, fw))
-    # active picture
-    ire[fal:lal, a0:a1] = luma + np.real(chi * car[fal:lal, a0:a1])
+    # luma part (active luma + sync) and chroma part (active chroma + burst)
+    y_part = np.zeros((fh, fw))
+    c_part = np.zeros((fh, fw))
+    y_part[fal:lal, a0:a1] = luma
+    c_part[fal:lal, a0:a1] = np.real(chi * car[fal:lal, a0:a1])
     # sync pulse (4.7 us)
     sync_len = min(int(round(4.7e-6 * fs)), max(0, g.colour_burst_start - 8))
-    ire[:, :sync_len] = -40.0
+    y_part[:, :sync_len] = -40.0
     # burst: 9 (NTSC) / 10 (PAL) cycles centred on the burst window
     b0, b1 = g.colour_burst_start, g.colour_burst_end
     ncyc = 10 if pal else 9
@@ -222,11 +226,16 @@ def make_field(seed: int, standard: int = _cabi.STD_NTSC, noise_sigma: float = 0
         chi_b = amp * (np.sin(np.pi / 4) + 1j * np.cos(np.pi / 4))
     else:
         chi_b = 1j * amp
-    ire[:, bs:bs + blen] = np.real(chi_b * car[:, bs:bs + blen])
-    ire += rng.normal(0.0, noise_sigma, size=ire.shape)
+    c_part[:, bs:bs + blen] = np.real(chi_b * car[:, bs:bs + blen])
+    ire = y_part + c_part
+    noise = rng.normal(0.0, noise_sigma, size=ire.shape)
+    ire += noise
     codes = np.clip(np.rint(BLANK_CODE + ire * CODES_PER_IRE), 0, 65535).astype(np.uint16)
-    return FieldSample(codes, parity, standard, luma.astype(np.float32),
+    fsmp = FieldSample(codes, parity, standard, luma.astype(np.float32),
                        chi.astype(np.complex64), theta, vsw, noise_sigma)
+    if return_parts:
+        return fsmp, y_part, c_part, noise
+    return fsmp
 
 
 def make_sequence(seed: int, standard: int, n_fields: int, noise_sigma: float = 0.5,
@@ -290,3 +299,43 @@ def make_frames(seed: int, standard: int, n_frames: int, noise_sigma: float = 0.
                 buf.append(codes[-2:])  # the two extra samples of this line
         frames.append(np.concatenate(buf))
     return frames, fields
+
+
+def make_yc_frames(seed: int, standard: int, n_frames: int, noise_sigma: float = 0.5,
+                   moving: bool = False, blanking: float = 240.0, white: float = 800.0,
+                   chroma_dc: float = 512.0):
+    """Y/C-native frame pairs in the same field-sequential int16 layout as
+    make_frames: the Y channel (luma + sync, levels as make_frames) and the C
+    channel (chroma + burst, centred on chroma_dc), each with its own noise.
+    Returns (luma_frames, chroma_frames, fields)."""
+    sc = make_scene(seed, standard, n_rects=4 if moving else 0)
+    base = float(np.random.default_rng(seed + 17).uniform(-np.pi, np.pi))
+    g = _cabi.default_geometry(standard)
+    if standard == _cabi.STD_PAL:
+        fh, f1, extra = 625, 313, (312, 624)
+    else:
+        fh, f1, extra = 525, 263, ()
+    f2 = fh - f1
+    cpi = (white - blanking) / 100.0
+    rng = np.random.default_rng(seed + 101)
+    ys, cs, fields = [], [], []
+    for t in range(n_frames):
+        parts = [make_field(seed, standard, noise_sigma, field_index=2 * t + k, parity=k,
+                            scene=sc, theta_base=base, return_parts=True) for k in range(2)]
+        fields += [p[0] for p in parts]
+        yl = [parts[0][1][y] for y in range(f1)] + [parts[1][1][y] for y in range(f2)]
+        cl = [parts[0][2][y] for y in range(f1)] + [parts[1][2][y] for y in range(f2)]
+        ybuf, cbuf = [], []
+        for i, (ly, lc) in enumerate(zip(yl, cl)):
+            yc_ = np.rint(blanking + (ly + rng.normal(0, noise_sigma, ly.shape)) * cpi)
+            cc_ = np.rint(chroma_dc + (lc + rng.normal(0, noise_sigma, lc.shape)) * cpi)
+            yc_ = np.clip(yc_, -32768, 32767).astype(np.int16)
+            cc_ = np.clip(cc_, -32768, 32767).astype(np.int16)
+            ybuf.append(yc_)
+            cbuf.append(cc_)
+            if i in extra:
+                ybuf.append(yc_[-2:])
+                cbuf.append(cc_[-2:])
+        ys.append(np.concatenate(ybuf))
+        cs.append(np.concatenate(cbuf))
+    return ys, cs, fields

@@ -8,6 +8,8 @@
  * project; each declaration below cites the one it stands in for):
  *
  *   hvd-core/src/frame_bridge.h:196-199   hvd::DecodeFrameSequenceWindow
+ *   hvd-core/src/frame_bridge.h:149-150   hvd::DecodeFrameBuffer (engine.h:89 DecodeFrame)
+ *   hvd-core/src/frame_bridge.h:223-226   hvd::DecodeYcFrameBuffer (engine.h:106 DecodeChromaOnly)
  *   hvd-core/src/engine/engine.h:112-114  HvdEngine::DecodeSequenceWindow
  *   hvd-core/src/engine/sequence.h:60-61  PrepareFieldObs
  *   hvd-core/src/engine/sequence.h:98-101 DecodeFieldWindow
@@ -259,6 +261,39 @@ hvdg_status hvdg_decode_frame_sequence_window(
     hvdg_ctx* ctx, const int16_t* const* frames, int n_frames, int core_begin,
     int core_end, const hvdg_frame_params* fp, const hvdg_config* cfg,
     hvdg_yc_frame* out, hvdg_diag* diag);
+
+/* hvd::DecodeFrameBuffer (frame_bridge.h:149-150, frame_bridge.cpp:161-255) via HvdEngine::DecodeFrame
+ * (engine.cpp:141-195): the 2-D frame-weave decode of one field-sequential
+ * int16 composite frame -- split, field-order vote (cfg->field_order),
+ * per-field lock-in, weave of the two fields' active pictures and carriers,
+ * holographic init + IRLS / CG on the woven frame, lossless chroma S - Y,
+ * ACC, re-weave and 10-bit requantisation into `out` (frame_width x
+ * frame_height each). The source frame holds FrameLineOffset(fp,
+ * frame_height - 1) + frame_width samples at least. */
+hvdg_status hvdg_decode_frame_buffer(hvdg_ctx* ctx, const int16_t* frame,
+                                     const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                     hvdg_yc_frame* out);
+/* n independent frames of hvdg_decode_frame_buffer in one batched launch
+ * sequence (no reference counterpart: the reference decodes frame by frame).
+ * diag (optional) reports the first frame's ACC gain. */
+hvdg_status hvdg_decode_frame_buffers(hvdg_ctx* ctx, const int16_t* const* frames, int n_frames,
+                                      const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                      hvdg_yc_frame* out, hvdg_diag* diag);
+/* hvd::DecodeYcFrameBuffer (frame_bridge.h:223-226, frame_bridge.cpp:263-377) via
+ * HvdEngine::DecodeChromaOnly (engine.cpp:197-237): Y/C-native input. The C
+ * channel is de-woven around fp->chroma_dc, woven with its per-field
+ * lock-in carriers and cropped by the holographic init alone (no IRLS / CG);
+ * luma passes through from the Y channel. chroma = Re[chi c] requantised,
+ * u / v from chi with ACC. Field order: cfg->field_order 2 puts field 1 on
+ * the odd rows, anything else on the even rows (no vote on this path). */
+hvdg_status hvdg_decode_yc_frame_buffer(hvdg_ctx* ctx, const int16_t* luma, const int16_t* chroma,
+                                        const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                        hvdg_yc_frame* out);
+/* n independent frames of hvdg_decode_yc_frame_buffer in one batch. */
+hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* luma,
+                                         const int16_t* const* chroma, int n_frames,
+                                         const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                         hvdg_yc_frame* out, hvdg_diag* diag);
 
 /* ------------------------------------------------------------------------ */
 /* Kernel level (host buffers)                                               */

@@ -66,6 +66,10 @@ def _declare(L):
                                                       P(_cabi.FrameParams), P(_cabi.Config),
                                                       P(vp), P(vp), P(vp), P(vp)]
     L.hvdref_split_frame_fields.argtypes = [vp, P(_cabi.FrameParams), vp, vp]
+    L.hvdref_decode_frame_buffer.argtypes = [vp, P(_cabi.FrameParams), P(_cabi.Config), vp, vp,
+                                             vp, vp]
+    L.hvdref_decode_yc_frame_buffer.argtypes = [vp, vp, P(_cabi.FrameParams), P(_cabi.Config),
+                                                vp, vp, vp, vp]
     L.hvdref_detect_field_parity.argtypes = [vp, vp, P(_cabi.FrameParams)]
     L.hvdref_fft2d.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp]
 
@@ -229,6 +233,31 @@ def decode_frame_sequence_window(frames, core_begin, core_end, fp, cfg):
                                                     C.byref(fp), C.byref(cfg),
                                                     arr(L), arr(Cc), arr(U), arr(Vv))
     return [dict(luma=L[t], chroma=Cc[t], u=U[t], v=Vv[t]) for t in range(got)]
+
+
+def _yc_out(fp):
+    sz = fp.frame_width * fp.frame_height
+    return (np.zeros(sz, np.int16), np.zeros(sz, np.int16), np.zeros(sz, np.float64),
+            np.zeros(sz, np.float64))
+
+
+def decode_frame_buffer(frame, fp, cfg):
+    """hvd::DecodeFrameBuffer on one int16 frame: dict(luma, chroma, u, v)."""
+    fr = np.ascontiguousarray(frame, dtype=np.int16)
+    L, Cc, U, Vv = _yc_out(fp)
+    lib().hvdref_decode_frame_buffer(_p(fr), C.byref(fp), C.byref(cfg), _p(L), _p(Cc), _p(U),
+                                     _p(Vv))
+    return dict(luma=L, chroma=Cc, u=U, v=Vv)
+
+
+def decode_yc_frame_buffer(luma, chroma, fp, cfg):
+    """hvd::DecodeYcFrameBuffer on one Y/C int16 frame pair."""
+    y = np.ascontiguousarray(luma, dtype=np.int16)
+    c = np.ascontiguousarray(chroma, dtype=np.int16)
+    L, Cc, U, Vv = _yc_out(fp)
+    lib().hvdref_decode_yc_frame_buffer(_p(y), _p(c), C.byref(fp), C.byref(cfg), _p(L), _p(Cc),
+                                        _p(U), _p(Vv))
+    return dict(luma=L, chroma=Cc, u=U, v=Vv)
 
 
 def split_frame_fields(frame, fp):

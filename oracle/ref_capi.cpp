@@ -360,6 +360,32 @@ int hvdref_decode_frame_sequence_window(const int16_t* const* frames, int nframe
   return static_cast<int>(out.size());
 }
 
+static void CopyYc(const hvd::YcFrameS16& o, int16_t* luma, int16_t* chroma, double* u,
+                   double* v) {
+  std::copy(o.luma.begin(), o.luma.end(), luma);
+  std::copy(o.chroma.begin(), o.chroma.end(), chroma);
+  std::copy(o.u_plane.begin(), o.u_plane.end(), u);
+  std::copy(o.v_plane.begin(), o.v_plane.end(), v);
+}
+
+// hvd::DecodeFrameBuffer (frame_bridge.cpp:161): the frame-weave decode of
+// one composite frame; fw*fh outputs.
+void hvdref_decode_frame_buffer(const int16_t* frame, const hvdg_frame_params* fp,
+                                const hvdg_config* cfg, int16_t* luma, int16_t* chroma,
+                                double* u, double* v) {
+  hvd::HvdEngine engine;
+  CopyYc(hvd::DecodeFrameBuffer(frame, ToFp(*fp), ToCfg(*cfg), engine), luma, chroma, u, v);
+}
+
+// hvd::DecodeYcFrameBuffer (frame_bridge.cpp:263): Y/C-native input.
+void hvdref_decode_yc_frame_buffer(const int16_t* luma_in, const int16_t* chroma_in,
+                                   const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                   int16_t* luma, int16_t* chroma, double* u, double* v) {
+  hvd::HvdEngine engine;
+  CopyYc(hvd::DecodeYcFrameBuffer(luma_in, chroma_in, ToFp(*fp), ToCfg(*cfg), engine), luma,
+         chroma, u, v);
+}
+
 // SplitFrameFields (frame_bridge.cpp:61): block-1 / block-2 fields in IRE.
 void hvdref_split_frame_fields(const int16_t* frame, const hvdg_frame_params* fp,
                                float* top, float* bottom) {

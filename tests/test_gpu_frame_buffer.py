@@ -1,0 +1,143 @@
+"""Woven-frame entry points against the reference on the same int16 frames:
+
+- hvdg_decode_frame_buffer ~ hvd::DecodeFrameBuffer (frame_bridge.cpp:161-255,
+  engine DecodeFrame engine.cpp:141-195): split, field-order vote, per-field
+  lock-in, weave, holographic init (column length 2048: woven NTSC pads to
+  516 rows, PAL to 614) + IRLS / CG on the woven frame, lossless chroma
+  S - Y, ACC, re-weave, 10-bit requantisation;
+- hvdg_decode_yc_frame_buffer ~ hvd::DecodeYcFrameBuffer
+  (frame_bridge.cpp:263-377, engine DecodeChromaOnly engine.cpp:197-237):
+  C channel de-woven around chroma_dc, init only, chroma = Re[chi c], luma
+  passed through.
+
+Codes are compared exactly up to rare +-1 rounding flips (the float chi of
+the two implementations differs in its last bits: FFT-convolution init,
+reduction order of the FP32 solver, FP64 carrier phases here), u / v within
+0.05 codes on NTSC. PAL's per-line phases grow to ~1500 rad, where the
+reference's float carrier phase (MakeCarrierPal, ntsc_geometry.cpp:438-456)
+carries ~1e-4 rad of rounding: ~0.02 codes of chroma per sample. The
+reference itself moves by 0.10 codes of u / v on the PAL frame of
+test_frame_buffer_vs_reference when only its carrier phase is evaluated in
+double instead of float, so PAL is held to 0.15 codes of u / v and 0.5 % of
++-1 code flips.
+Pass-through luma and everything outside the active picture must be
+identical."""
+import numpy as np
+import pytest
+
+from hvdg import _cabi, api, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref():
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    return ref
+
+
+def _compare(got, want, tag, pal=False):
+    flip_frac, uv_tol = (5e-3, 0.15) if pal else (2e-3, 0.05)
+    for key in ("luma", "chroma"):
+        d = np.abs(got[key].astype(np.int32) - want[key].astype(np.int32))
+        print(f"{tag} {key}: max {d.max()} frac>0 {(d > 0).mean():.2e}")
+        assert d.max() <= 1, (tag, key)
+        assert (d > 0).mean() < flip_frac, (tag, key)
+    for key in ("u", "v"):
+        du = np.abs(got[key] - want[key])
+        print(f"{tag} {key}: max {du.max():.3e}")
+        assert du.max() < uv_tol, (tag, key)
+        # zero exactly where the reference is zero (outside the active picture)
+        assert np.all(got[key][want[key] == 0.0] == 0.0), (tag, key)
+
+
+def _cfg(**kw):
+    base = dict(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6)
+    base.update(kw)
+    return api.default_config(**base)
+
+
+@pytest.mark.parametrize("std", [_cabi.STD_NTSC, _cabi.STD_PAL])
+@pytest.mark.parametrize("field_order", [0, 2])
+def test_frame_buffer_vs_reference(ctx, std, field_order):
+    ref = _ref()
+    frames, _ = synth.make_frames(61 + std, std, 1, noise_sigma=1.0)
+    fp = api.frame_params(std)
+    cfg = _cfg(field_order=field_order)
+    got = ctx.decode_frame_buffer(frames[0], fp, cfg)
+    want = ref.decode_frame_buffer(frames[0], fp, cfg)
+    _compare(got, want, f"composite std={std} order={field_order}", pal=std == _cabi.STD_PAL)
+
+
+@pytest.mark.parametrize("opts", [dict(monochrome=1), dict(acc=0, chroma_gain=1.3),
+                                  dict(cg_iterations=0), dict(chroma_phase_deg=20.0),
+                                  dict(field_order=1, chroma_aniso=0.7)])
+def test_frame_buffer_options_vs_reference(ctx, opts):
+    ref = _ref()
+    std = _cabi.STD_PAL if "chroma_phase_deg" in opts else _cabi.STD_NTSC
+    frames, _ = synth.make_frames(71, std, 1, noise_sigma=1.0)
+    fp = api.frame_params(std)
+    cfg = _cfg(**opts)
+    got = ctx.decode_frame_buffer(frames[0], fp, cfg)
+    want = ref.decode_frame_buffer(frames[0], fp, cfg)
+    _compare(got, want, f"composite {opts}", pal=std == _cabi.STD_PAL)
+
+
+@pytest.mark.parametrize("std", [_cabi.STD_NTSC, _cabi.STD_PAL])
+@pytest.mark.parametrize("field_order", [0, 2])
+def test_yc_frame_buffer_vs_reference(ctx, std, field_order):
+    ref = _ref()
+    ys, cs, _ = synth.make_yc_frames(81 + std, std, 1, noise_sigma=0.7)
+    fp = api.frame_params(std)
+    fp.chroma_dc = 512.0
+    cfg = _cfg(field_order=field_order)
+    got = ctx.decode_yc_frame_buffer(ys[0], cs[0], fp, cfg)
+    want = ref.decode_yc_frame_buffer(ys[0], cs[0], fp, cfg)
+    _compare(got, want, f"yc std={std} order={field_order}", pal=std == _cabi.STD_PAL)
+    # luma passes straight through, line by line through FrameLineOffset
+    assert np.array_equal(got["luma"], want["luma"])
+
+
+def test_batched_frames_equal_single_calls(ctx):
+    """With the solver band height pinned (the automatic one depends on the
+    batch size), a batch of frames decodes bit-for-bit like one-frame calls:
+    every reduction is per unit in a fixed order."""
+    frames, _ = synth.make_frames(91, _cabi.STD_NTSC, 3, noise_sigma=1.0, moving=True)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = _cfg()
+    ctx.set_tuning(16, 0)
+    try:
+        _batched_vs_single(ctx, frames, fp, cfg)
+    finally:
+        ctx.set_tuning(0, 0)
+
+
+def _batched_vs_single(ctx, frames, fp, cfg):
+    batch = ctx.decode_frame_buffers(frames, fp, cfg)
+    assert ctx.last_diag.kernel_launches > 0
+    for t, f in enumerate(frames):
+        one = ctx.decode_frame_buffer(f, fp, cfg)
+        for key in ("luma", "chroma", "u", "v"):
+            assert np.array_equal(batch[t][key], one[key]), (t, key)
+    ys, cs, _ = synth.make_yc_frames(92, _cabi.STD_PAL, 2, noise_sigma=0.7)
+    fpp = api.frame_params(_cabi.STD_PAL)
+    fpp.chroma_dc = 512.0
+    yb = ctx.decode_yc_frame_buffers(ys, cs, fpp, cfg)
+    for t in range(2):
+        one = ctx.decode_yc_frame_buffer(ys[t], cs[t], fpp, cfg)
+        for key in ("luma", "chroma", "u", "v"):
+            assert np.array_equal(yb[t][key], one[key]), (t, key)
+
+
+def test_frame_buffer_lossless_split(ctx):
+    """luma + chroma reconstructs the composite to one code inside the
+    active picture (the YcFrameS16 contract, frame_bridge.h:114-122)."""
+    frames, _ = synth.make_frames(95, _cabi.STD_NTSC, 1, noise_sigma=0.5)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    got = ctx.decode_frame_buffer(frames[0], fp, _cfg())
+    src = frames[0].astype(np.int32)
+    rec = got["luma"].astype(np.int32) + got["chroma"].astype(np.int32)
+    active = got["u"] != 0.0
+    assert np.abs(rec - src)[active].max() <= 1
+    assert np.array_equal(got["luma"][~active], frames[0][~active])
