@@ -227,7 +227,13 @@ CONFIGS = {
     "cfg2-pal16-3d": "config 2: 16 PAL 1135x313 fields, same motion, window and solver as config 1",
     "cfg4-adjoint8": "config 4: forward + adjoint of 8 NTSC fields, 10 IRLS x 50 CG, "
                      "gradients w.r.t. 4 scalars and the samples",
+    "frames8-ntsc": "8 NTSC 910x525 int16 composite frames through DecodeFrameBuffer "
+                    "(frame-weave 2-D decode, default HvdConfig), one frame per reference call, "
+                    "one batch here",
+    "yc8-pal": "8 PAL 1135x625 Y/C int16 frame pairs through DecodeYcFrameBuffer "
+               "(chroma-only init, default HvdConfig)",
 }
+FRAME_CONFIGS = ("frames8-ntsc", "yc8-pal")
 
 
 def config_cfg(name):
@@ -253,6 +259,116 @@ def config_fields(name):
     if name == "cfg2-pal16-3d":
         return synth.make_sequence(102, _cabi.STD_PAL, 16, noise_sigma=0.5, moving=True)
     return [synth.make_field(200 + i, _cabi.STD_NTSC, 0.5) for i in range(8)]
+
+
+def frame_arm(args, rank, world):
+    """Frames/s of the woven-frame entry points through the public API (host
+    int16 frames in, the four YcFrameS16 planes out; wall clock of the
+    synchronous call), or of the reference's own per-frame calls."""
+    if rank != 0:
+        return 0
+    from hvdg import _cabi, api, synth
+    name = args.workload
+    cfg = api.default_config()
+    n = 8
+    if name == "frames8-ntsc":
+        std = _cabi.STD_NTSC
+        frames, _ = synth.make_frames(300, std, n, noise_sigma=0.5, moving=True)
+        ys = cs = None
+    else:
+        std = _cabi.STD_PAL
+        ys, cs, _ = synth.make_yc_frames(301, std, n, noise_sigma=0.5, moving=True)
+    fp = api.frame_params(std)
+    if ys is not None:
+        fp.chroma_dc = 512.0
+    npx = fp.frame_width * fp.frame_height
+    in_bytes = (2 if ys is not None else 1) * 2 * api.frame_buffer_size(fp) * n
+    out_bytes = (2 + 2 + 8 + 8) * npx * n
+    if args.impl == "reference":
+        from oracle import ref
+        if not ref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+            return 0
+        threads = os.cpu_count() or 1
+        ref.set_threads(threads)
+        times = []
+        for _ in range(max(1, args.steps)):
+            t = time.perf_counter()
+            for k in range(n):
+                if ys is None:
+                    ref.decode_frame_buffer(frames[k], fp, cfg)
+                else:
+                    ref.decode_yc_frame_buffer(ys[k], cs[k], fp, cfg)
+            times.append(time.perf_counter() - t)
+        v = n * len(times) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": f"frames/s ({CONFIGS[name]})",
+                          "value": v, "unit": "frames/s", "n_gpus": world, "steps": len(times),
+                          "warmup": 0, "higher_is_better": True, "dtype": "f32",
+                          "data": "synthetic (seeded hvdg.synth)",
+                          "config": {"workload": CONFIGS[name]},
+                          "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads,
+                                           "kind": "reference",
+                                           "sample": f"{n} frames per step, one call each"},
+                          "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        return t
+
+    def pinned_zeros(k, dt):
+        return torch.zeros(k, dtype=dt, pin_memory=True)
+
+    ctx = api.Context(0)
+    keep = []
+    if ys is None:
+        frames = [pinned(f) for f in frames]
+        keep += frames
+        frames = [t.numpy() for t in frames]
+    else:
+        ys = [pinned(a) for a in ys]
+        cs = [pinned(a) for a in cs]
+        keep += ys + cs
+        ys, cs = [t.numpy() for t in ys], [t.numpy() for t in cs]
+    outs = []
+    for _ in range(n):
+        planes = dict(luma=pinned_zeros(npx, torch.int16), chroma=pinned_zeros(npx, torch.int16),
+                      u=pinned_zeros(npx, torch.float64), v=pinned_zeros(npx, torch.float64))
+        keep += list(planes.values())
+        outs.append({k: t.numpy() for k, t in planes.items()})
+
+    def step():
+        if ys is None:
+            return ctx.decode_frame_buffers(frames, fp, cfg, out=outs)
+        return ctx.decode_yc_frame_buffers(ys, cs, fp, cfg, out=outs)
+
+    for _ in range(args.warmup):
+        step()
+    wall, dev = 0.0, 0.0
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        step()
+        wall += time.perf_counter() - t
+        dev += ctx.last_diag.ms_total
+    launches = ctx.last_diag.kernel_launches
+    line = {"metric": f"frames/s ({CONFIGS[name]})", "value": n * args.steps / wall,
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded hvdg.synth)",
+            "config": {"workload": CONFIGS[name], "timing": "wall clock of the synchronous "
+                       "host-buffer call (uploads, kernels, downloads; pinned host frames and "
+                       "output planes)"},
+            "device_frames_per_s": n * args.steps / (dev / 1000.0) if dev > 0 else None,
+            "device_note": "device time of the kernels (split to re-weave), copies excluded",
+            "gpu_launches": launches * args.steps,
+            "e2e": {"value": n * args.steps / wall, "unit": "frames/s",
+                    "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes}}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
 
 
 def config_arm(args, rank, world):
@@ -361,6 +477,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in FRAME_CONFIGS:
+        return frame_arm(args, rank, world)
     if args.workload in CONFIGS:
         return config_arm(args, rank, world)
     if args.impl == "reference":

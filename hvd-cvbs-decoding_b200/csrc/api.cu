@@ -2628,6 +2628,7 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
                           sizeof(int16_t) * need, cudaMemcpyHostToDevice, s);
   }
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D frames");
+  mark(ctx, 0);  // device time of the kernels: from the split to the re-weave
   const float cpi = (P.white_level - P.blanking_level) / 100.0f;
   hvdg::FrameSplitArgs sp;
   sp.frames = reinterpret_cast<const int16_t*>(X + o_src);
@@ -2691,6 +2692,7 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   fo.v = reinterpret_cast<double*>(X + o_ov);
   hvdg::launch_frame_out(fo, n, s);
   S.launches += 1;
+  mark(ctx, 4);
   e = cudaGetLastError();
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "frame kernels");
   for (int t = 0; t < n && e == cudaSuccess; ++t) {
@@ -2716,7 +2718,6 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   if (e == cudaSuccess && diag)
     e = cudaMemcpyAsync(ctl.data(), at<FieldCtl>(ctx, L.o_ctl), sizeof(FieldCtl) * n,
                         cudaMemcpyDeviceToHost, s);
-  mark(ctx, 4);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "frame decode sync");
   if (diag) {

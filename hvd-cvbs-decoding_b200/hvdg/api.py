@@ -341,10 +341,23 @@ def _decode_frames(self, frames, core_begin, core_end, fp, cfg):
 Context.decode_frame_sequence_window = _decode_frames
 
 
-def _yc_frames(fp, m):
+def _yc_frames(fp, m, out=None):
     sz = fp.frame_width * fp.frame_height
-    res = [dict(luma=np.zeros(sz, np.int16), chroma=np.zeros(sz, np.int16),
-                u=np.zeros(sz, np.float64), v=np.zeros(sz, np.float64)) for _ in range(m)]
+    if out is not None:
+        # caller-owned (e.g. pinned) planes: dicts of contiguous arrays of sz
+        # elements (luma / chroma int16, u / v float64)
+        if len(out) != m:
+            raise ValueError("one output dict per frame")
+        for r in out:
+            for key, dt in (("luma", np.int16), ("chroma", np.int16), ("u", np.float64),
+                            ("v", np.float64)):
+                a = r[key]
+                if a.dtype != dt or a.size != sz or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"output plane {key}: {sz} contiguous {np.dtype(dt)}")
+        res = out
+    else:
+        res = [dict(luma=np.zeros(sz, np.int16), chroma=np.zeros(sz, np.int16),
+                    u=np.zeros(sz, np.float64), v=np.zeros(sz, np.float64)) for _ in range(m)]
     outs = (_cabi.YcFrame * max(m, 1))()
     for t, r in enumerate(res):
         outs[t].luma = r["luma"].ctypes.data
@@ -369,10 +382,11 @@ def _decode_frame_buffer(self, frame, fp, cfg):
     return res[0]
 
 
-def _decode_frame_buffers(self, frames, fp, cfg):
-    """n independent frames of decode_frame_buffer in one batch."""
+def _decode_frame_buffers(self, frames, fp, cfg, out=None):
+    """n independent frames of decode_frame_buffer in one batch; `out`
+    (optional) = caller-owned output dicts (see _yc_frames)."""
     fr = [np.ascontiguousarray(f, dtype=np.int16) for f in frames]
-    res, outs = _yc_frames(fp, len(fr))
+    res, outs = _yc_frames(fp, len(fr), out)
     self.last_diag = Diag()
     st = self.lib.hvdg_decode_frame_buffers(self._h, _ptrs(fr), len(fr), C.byref(fp),
                                             C.byref(cfg), outs, C.byref(self.last_diag))
@@ -391,13 +405,13 @@ def _decode_yc_frame_buffer(self, luma, chroma, fp, cfg):
     return res[0]
 
 
-def _decode_yc_frame_buffers(self, lumas, chromas, fp, cfg):
+def _decode_yc_frame_buffers(self, lumas, chromas, fp, cfg, out=None):
     """n independent frames of decode_yc_frame_buffer in one batch."""
     ys = [np.ascontiguousarray(a, dtype=np.int16) for a in lumas]
     cs = [np.ascontiguousarray(a, dtype=np.int16) for a in chromas]
     if len(ys) != len(cs):
         raise ValueError("one chroma frame per luma frame")
-    res, outs = _yc_frames(fp, len(ys))
+    res, outs = _yc_frames(fp, len(ys), out)
     self.last_diag = Diag()
     st = self.lib.hvdg_decode_yc_frame_buffers(self._h, _ptrs(ys), _ptrs(cs), len(ys),
                                                C.byref(fp), C.byref(cfg), outs,

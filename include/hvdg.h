@@ -275,7 +275,10 @@ hvdg_status hvdg_decode_frame_buffer(hvdg_ctx* ctx, const int16_t* frame,
                                      hvdg_yc_frame* out);
 /* n independent frames of hvdg_decode_frame_buffer in one batched launch
  * sequence (no reference counterpart: the reference decodes frame by frame).
- * diag (optional) reports the first frame's ACC gain. */
+ * diag (optional) reports the first frame's ACC gain; its ms_total is the
+ * device time of the kernels (frame split to re-weave), the host <-> device
+ * copies of the frames excluded. Pinned host frames and planes copy at the
+ * link's full rate. */
 hvdg_status hvdg_decode_frame_buffers(hvdg_ctx* ctx, const int16_t* const* frames, int n_frames,
                                       const hvdg_frame_params* fp, const hvdg_config* cfg,
                                       hvdg_yc_frame* out, hvdg_diag* diag);
