@@ -2109,6 +2109,221 @@ int detect_field_parity_frame(const int16_t* frame, const hvdg_frame_params& fp,
       fp, g);
 }
 
+// ---------------------------------------------------------------------------
+// Selective 3-D (DecodeWindowSelective, frame_bridge.cpp:490-718): a
+// full-window 2-D decode, the Y/C-ambiguous boxes of its first field
+// (AmbiguousBoxes, frame_bridge.cpp:402-580), the full 3-D window decode of
+// each box, feather-blended in. A box's FieldObs crop (CropObs,
+// frame_bridge.cpp:582-593) is the same field seen through a narrower active
+// window -- S and the carrier of the crop are the crop of the field's, and
+// the decode reads the geometry only for those and the sample rate -- so a
+// box decodes as the window under a cropped geometry.
+// ---------------------------------------------------------------------------
+struct SelBox {
+  int fy0 = 0, fy1 = 0, x0 = 0, x1 = 0;  // field coordinates inside the active picture
+  bool valid = false;                     // an invalid single box: run full 3-D
+};
+
+// AmbiguousBoxes: tile score sqrt(luma HF energy x chroma-magnitude HF
+// energy) over 16 x 16 tiles (HF = minus a count-normalised 8 x 8 box mean),
+// tiles >= 4 x the median score, kept where >= 2 of their 8 neighbours are
+// flagged and off the outer tile ring; row bands of >= 2 such tiles (at
+// most 4, closest bands merged), per band one box per column run (gap <= 2,
+// single tiles dropped) with a 16-row / 48-column halo. Empty: stay 2-D;
+// one invalid box: no band but a median above 3 IRE^2, or the boxes cover
+// more than max_area of the field.
+std::vector<SelBox> ambiguous_boxes(const float* Y, const float* chi_ri, int h, int w,
+                                    float max_area) {
+  const int T = 16, HX = 48, HY = 16, K = T / 2;
+  const int th = (h + T - 1) / T, tw = (w + T - 1) / T;
+  const size_t np = (size_t)h * w;
+  std::vector<float> ya(Y, Y + np), ca(np);
+  for (size_t i = 0; i < np; ++i)
+    ca[i] = std::abs(std::complex<float>(chi_ri[2 * i], chi_ri[2 * i + 1]));
+  // count-normalised separable box mean over offsets [-K/2, K - K/2)
+  auto box_mean = [&](const std::vector<float>& a) {
+    std::vector<float> v(np), o(np);
+    for (int x = 0; x < w; ++x)
+      for (int y = 0; y < h; ++y) {
+        float acc = 0.0f;
+        int n = 0;
+        for (int d = -K / 2; d < K - K / 2; ++d) {
+          if (y + d < 0 || y + d >= h) continue;
+          acc += a[(size_t)(y + d) * w + x];
+          ++n;
+        }
+        v[(size_t)y * w + x] = acc / std::max(n, 1);
+      }
+    for (int y = 0; y < h; ++y)
+      for (int x = 0; x < w; ++x) {
+        float acc = 0.0f;
+        int n = 0;
+        for (int d = -K / 2; d < K - K / 2; ++d) {
+          if (x + d < 0 || x + d >= w) continue;
+          acc += v[(size_t)y * w + x + d];
+          ++n;
+        }
+        o[(size_t)y * w + x] = acc / std::max(n, 1);
+      }
+    return o;
+  };
+  const std::vector<float> ly = box_mean(ya), lc = box_mean(ca);
+  std::vector<double> ey((size_t)th * tw, 0.0), ec((size_t)th * tw, 0.0);
+  std::vector<int> cnt((size_t)th * tw, 0);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const size_t i = (size_t)y * w + x, t = (size_t)(y / T) * tw + x / T;
+      const double dy = ya[i] - ly[i], dc = ca[i] - lc[i];
+      ey[t] += dy * dy;
+      ec[t] += dc * dc;
+      ++cnt[t];
+    }
+  std::vector<float> score((size_t)th * tw);
+  for (size_t t = 0; t < score.size(); ++t)
+    score[t] = (float)std::sqrt((ey[t] / std::max(cnt[t], 1)) * (ec[t] / std::max(cnt[t], 1)));
+  std::vector<float> srt = score;
+  std::nth_element(srt.begin(), srt.begin() + srt.size() / 2, srt.end());
+  const float med = srt[srt.size() / 2];
+  const float thr = 4.0f * med;
+  auto flag = [&](int ty, int tx) { return score[(size_t)ty * tw + tx] >= thr; };
+  std::vector<char> dense((size_t)th * tw, 0);
+  for (int ty = 1; ty + 1 < th; ++ty)
+    for (int tx = 1; tx + 1 < tw; ++tx) {
+      if (!flag(ty, tx)) continue;
+      int nb = 0;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+          if (dy || dx) nb += flag(ty + dy, tx + dx);
+      dense[(size_t)ty * tw + tx] = nb >= 2;
+    }
+  std::vector<std::pair<int, int>> bands;
+  for (int ty = 0; ty < th; ++ty) {
+    int row_n = 0;
+    for (int tx = 0; tx < tw; ++tx) row_n += dense[(size_t)ty * tw + tx];
+    if (row_n < 2) continue;
+    if (!bands.empty() && ty - bands.back().second <= 1)
+      bands.back().second = ty;
+    else
+      bands.emplace_back(ty, ty);
+  }
+  std::vector<SelBox> boxes;
+  if (bands.empty()) {
+    if (med > 3.0f) boxes.push_back(SelBox{});
+    return boxes;
+  }
+  while (bands.size() > 4) {  // merge the two closest neighbouring bands
+    size_t bi = 0;
+    int best = INT32_MAX;
+    for (size_t i = 0; i + 1 < bands.size(); ++i) {
+      const int gap = bands[i + 1].first - bands[i].second;
+      if (gap < best) {
+        best = gap;
+        bi = i;
+      }
+    }
+    bands[bi].second = bands[bi + 1].second;
+    bands.erase(bands.begin() + (long)bi + 1);
+  }
+  for (const auto& bd : bands) {
+    std::vector<char> col(tw, 0);
+    for (int ty = bd.first; ty <= bd.second; ++ty)
+      for (int tx = 0; tx < tw; ++tx) col[tx] |= dense[(size_t)ty * tw + tx];
+    int y0 = std::max(0, bd.first * T - HY);
+    y0 -= y0 % 2;  // keep the crop on the field's line parity
+    const int y1 = std::min(h, (bd.second + 1) * T + HY);
+    std::vector<std::pair<int, int>> runs;
+    for (int tx = 0; tx < tw; ++tx) {
+      if (!col[tx]) continue;
+      if (!runs.empty() && tx - runs.back().second <= 2)
+        runs.back().second = tx;
+      else
+        runs.emplace_back(tx, tx);
+    }
+    const size_t first = boxes.size();
+    for (const auto& r : runs) {
+      if (r.second - r.first < 1) continue;
+      const int x0 = std::max(0, r.first * T - HX), x1 = std::min(w, (r.second + 1) * T + HX);
+      if (boxes.size() > first && x0 <= boxes.back().x1) {
+        boxes.back().x1 = x1;
+      } else {
+        SelBox b;
+        b.fy0 = y0;
+        b.fy1 = y1;
+        b.x0 = x0;
+        b.x1 = x1;
+        b.valid = true;
+        boxes.push_back(b);
+      }
+    }
+  }
+  double area = 0.0;
+  for (const SelBox& b : boxes) area += (double)(b.fy1 - b.fy0) * (b.x1 - b.x0);
+  if (area > (double)max_area * h * w) {
+    boxes.clear();
+    boxes.push_back(SelBox{});
+  }
+  return boxes;
+}
+
+// The 3-D part of DecodeWindowSelective on top of the 2-D decode already in
+// Yd / Cd (h x w per field; Cd interleaved re, im).
+hvdg_status decode_selective_boxes(hvdg_ctx* ctx, const std::vector<hvdg_field_in>& fi,
+                                   const hvdg_geometry& g, const hvdg_config* cfg,
+                                   std::vector<std::vector<float>>& Yd,
+                                   std::vector<std::vector<float>>& Cd) {
+  const int nf = (int)fi.size();
+  const int h = last_active_line(g) - g.first_active_field_line;
+  const int w = g.active_video_end - g.active_video_start;
+  const std::vector<SelBox> boxes =
+      ambiguous_boxes(Yd[0].data(), Cd[0].data(), h, w, cfg->selective_max_area);
+  if (boxes.empty()) return HVDG_OK;
+  std::vector<hvdg_field_out> fo(nf);
+  if (!boxes[0].valid) {  // ambiguity everywhere: the full 3-D window
+    for (int j = 0; j < nf; ++j) fo[j] = hvdg_field_out{Yd[j].data(), Cd[j].data(), nullptr, nullptr};
+    return decode_window_impl(ctx, fi.data(), nf, cfg, fo.data(), nullptr);
+  }
+  for (const SelBox& b : boxes) {
+    hvdg_geometry gb = g;
+    gb.first_active_field_line = g.first_active_field_line + b.fy0;
+    gb.last_active_field_line = g.first_active_field_line + b.fy1;
+    gb.active_video_start = g.active_video_start + b.x0;
+    gb.active_video_end = g.active_video_start + b.x1;
+    const int bh = b.fy1 - b.fy0, bw = b.x1 - b.x0;
+    std::vector<hvdg_field_in> fb = fi;
+    std::vector<std::vector<float>> Y3(nf, std::vector<float>((size_t)bh * bw)),
+        C3(nf, std::vector<float>((size_t)bh * bw * 2));
+    for (int j = 0; j < nf; ++j) {
+      fb[j].geometry = &gb;
+      fo[j] = hvdg_field_out{Y3[j].data(), C3[j].data(), nullptr, nullptr};
+    }
+    const hvdg_status st = decode_window_impl(ctx, fb.data(), nf, cfg, fo.data(), nullptr);
+    if (st != HVDG_OK) return st;
+    // feather: linear ramps over min(16, bh / 3) rows and min(48, bw / 3) columns
+    const int hy = std::min(16, bh / 3), hx = std::min(48, bw / 3);
+    for (int j = 0; j < nf; ++j)
+      for (int y = 0; y < bh; ++y) {
+        float ry = 1.0f;
+        if (y < hy)
+          ry = (float)y / hy;
+        else if (y >= bh - hy)
+          ry = (float)(bh - 1 - y) / hy;
+        for (int x = 0; x < bw; ++x) {
+          float rx = 1.0f;
+          if (x < hx)
+            rx = (float)x / hx;
+          else if (x >= bw - hx)
+            rx = (float)(bw - 1 - x) / hx;
+          const float m = ry * rx;
+          const size_t o = (size_t)(b.fy0 + y) * w + b.x0 + x, q = (size_t)y * bw + x;
+          Yd[j][o] = Yd[j][o] * (1.0f - m) + Y3[j][q] * m;
+          Cd[j][2 * o] = Cd[j][2 * o] * (1.0f - m) + C3[j][2 * q] * m;
+          Cd[j][2 * o + 1] = Cd[j][2 * o + 1] * (1.0f - m) + C3[j][2 * q + 1] * m;
+        }
+      }
+  }
+  return HVDG_OK;
+}
+
 int16_t clamp_u10(float v) {
   const long r = std::lround(v);
   return (int16_t)std::min<long>(std::max<long>(r, 0), 1023);
@@ -2808,6 +3023,8 @@ void hvdg_config_default(hvdg_config* c) {
   c->odd_gate_floor = 0.35f;
   c->output_fidelity = 1;
   c->psi_init = 0;
+  c->selective_3d = 0;
+  c->selective_max_area = 0.45f;
   c->me_mode = 0;
   c->me_block = 16;
   c->me_range = 16;
@@ -3114,7 +3331,16 @@ hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* cons
   opt.amp_out = amps.data();
   hvdg_diag local;
   hvdg_diag* dg = diag ? diag : &local;
-  st = decode_window_impl(ctx, fi.data(), nfield, cfg, fo.data(), dg, opt);
+  if (cfg->selective_3d && cfg->cg_iterations > 0 && cfg->temporal_strength >= 0.0f) {
+    // frame_bridge.cpp:800-802: the 2-D base, then the ambiguous boxes in 3-D
+    hvdg_config c2d = *cfg;
+    c2d.temporal_strength = -1.0f;
+    st = decode_window_impl(ctx, fi.data(), nfield, &c2d, fo.data(), dg, opt);
+    if (st != HVDG_OK) return st;
+    st = decode_selective_boxes(ctx, fi, g, cfg, Yd, Cd);
+  } else {
+    st = decode_window_impl(ctx, fi.data(), nfield, cfg, fo.data(), dg, opt);
+  }
   if (st != HVDG_OK) return st;
   float acc_gain = 1.0f;
   if (cfg->acc) {
@@ -3213,6 +3439,26 @@ hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* lu
                                          const hvdg_frame_params* fp, const hvdg_config* cfg,
                                          hvdg_yc_frame* out, hvdg_diag* diag) {
   return decode_woven_frames(ctx, chroma, luma, n_frames, fp, cfg, out, diag, true);
+}
+
+hvdg_status hvdg_ambiguous_boxes(const float* luma, const float* chroma, int h, int w,
+                                 float max_area, int32_t* boxes, int max_boxes, int* n_boxes) {
+  if (!luma || !chroma || !n_boxes || h < 1 || w < 1 || max_boxes < 0 ||
+      (max_boxes > 0 && !boxes))
+    return HVDG_ERR_BAD_ARGUMENT;
+  const std::vector<SelBox> b = ambiguous_boxes(luma, chroma, h, w, max_area);
+  if (!b.empty() && !b[0].valid) {
+    *n_boxes = -1;
+    return HVDG_OK;
+  }
+  *n_boxes = (int)b.size();
+  for (int i = 0; i < (int)b.size() && i < max_boxes; ++i) {
+    boxes[4 * i + 0] = b[i].fy0;
+    boxes[4 * i + 1] = b[i].fy1;
+    boxes[4 * i + 2] = b[i].x0;
+    boxes[4 * i + 3] = b[i].x1;
+  }
+  return HVDG_OK;
 }
 
 hvdg_status hvdg_holographic_init(hvdg_ctx* ctx, const float* s, const float* theta_active,

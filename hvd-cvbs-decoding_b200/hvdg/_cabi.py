@@ -110,10 +110,12 @@ class Config(C.Structure):
         ("odd_gate_floor", C.c_float),
         ("output_fidelity", C.c_int32),
         ("psi_init", C.c_int32),
+        ("selective_3d", C.c_int32),
+        ("selective_max_area", C.c_float),
         ("me_mode", C.c_int32),
         ("me_block", C.c_int32),
         ("me_range", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -235,6 +237,8 @@ def default_config() -> Config:
     c.odd_gate_floor = 0.35
     c.output_fidelity = 1
     c.psi_init = 0
+    c.selective_3d = 0
+    c.selective_max_area = 0.45
     c.me_mode = 0
     c.me_block = 16
     c.me_range = 16
@@ -332,6 +336,9 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_decode_frame_sequence_window.argtypes = [
         vp, P(vp), C.c_int, C.c_int, C.c_int, P(FrameParams), P(Config), P(YcFrame), P(Diag)]
     lib.hvdg_decode_frame_sequence_window.restype = C.c_int
+    lib.hvdg_ambiguous_boxes.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float, vp, C.c_int,
+                                         P(C.c_int)]
+    lib.hvdg_ambiguous_boxes.restype = C.c_int
     lib.hvdg_decode_frame_buffer.argtypes = [vp, vp, P(FrameParams), P(Config), P(YcFrame)]
     lib.hvdg_decode_frame_buffer.restype = C.c_int
     lib.hvdg_decode_frame_buffers.argtypes = [vp, P(vp), C.c_int, P(FrameParams), P(Config),

@@ -277,6 +277,24 @@ def default_config(**kw) -> Config:
     return _cabi.config_copy(_cabi.default_config(), **kw)
 
 
+def ambiguous_boxes(luma: np.ndarray, chroma: np.ndarray, max_area: float = 0.45):
+    """AmbiguousBoxes (the selective 3-D detector) on one decoded field:
+    a list of (fy0, fy1, x0, x1), [] = stay 2-D, None = full 3-D."""
+    lib = _cabi.load_library()
+    y = np.ascontiguousarray(luma, dtype=np.float32)
+    c = np.ascontiguousarray(chroma, dtype=np.complex64)
+    h, w = y.shape
+    buf = np.zeros(4 * 64, np.int32)
+    n = C.c_int(0)
+    st = lib.hvdg_ambiguous_boxes(y.ctypes.data, c.ctypes.data, h, w, float(max_area),
+                                  buf.ctypes.data, 64, C.byref(n))
+    if st != 0:
+        raise HvdgError(st, "hvdg_ambiguous_boxes")
+    if n.value < 0:
+        return None
+    return [tuple(int(v) for v in buf[4 * i:4 * i + 4]) for i in range(min(n.value, 64))]
+
+
 def default_geometry(standard: int) -> Geometry:
     return _cabi.default_geometry(standard)
 

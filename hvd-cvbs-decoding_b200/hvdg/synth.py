@@ -63,6 +63,7 @@ class Scene:
     edges: list = field(default_factory=list)
     patches: list = field(default_factory=list)
     rects: list = field(default_factory=list)
+    grilles: list = field(default_factory=list)
 
 
 def _lowpass_rows(a: np.ndarray, sigma_px: float) -> np.ndarray:
@@ -80,7 +81,11 @@ def _lowpass_rows(a: np.ndarray, sigma_px: float) -> np.ndarray:
 
 
 def make_scene(seed: int, standard: int, n_rects: int = 0,
-               geometry: _cabi.Geometry | None = None) -> Scene:
+               geometry: _cabi.Geometry | None = None, grille=None) -> Scene:
+    """`grille` (optional): (r0, r1, c0, c1, period_px, amp_ire) with the
+    box in fractions of the frame -- a localized luma grating near the
+    subcarrier (a fan grille / blinds), the Y/C-ambiguous content selective
+    3-D targets."""
     g = geometry or _cabi.default_geometry(standard)
     rng = np.random.default_rng(seed)
     rows = 2 * g.active_lines
@@ -109,6 +114,9 @@ def make_scene(seed: int, standard: int, n_rects: int = 0,
             # per-frame motion: integer or half-pel, +/-12 px, +/-6 frame lines
             vx=rng.integers(-24, 25) / 2.0, vy=rng.integers(-12, 13) / 2.0,
             y=rng.uniform(10, 90), a=rng.uniform(-40, 40), b=rng.uniform(-40, 40)))
+    if grille is not None:
+        r0, r1, c0, c1, period, amp = grille
+        sc.grilles.append((r0 * rows, r1 * rows, c0 * w, c1 * w, period, amp))
     return sc
 
 
@@ -137,6 +145,9 @@ def render(sc: Scene, frame_rows: np.ndarray, t_frames: float):
         m = (y >= r0) & (y < r1) & (x >= c0) & (x < c1)
         ca = np.where(m, va, ca)
         cb = np.where(m, vb, cb)
+    for (r0, r1, c0, c1, period, amp) in sc.grilles:
+        m = (y >= r0) & (y < r1) & (x >= c0) & (x < c1)
+        luma = luma + np.where(m, amp * np.cos(2 * np.pi * x / period), 0.0)
     for r in sc.rects:
         rr0 = r["r0"] + r["vy"] * t_frames
         cc0 = r["c0"] + r["vx"] * t_frames
@@ -239,9 +250,11 @@ def make_field(seed: int, standard: int = _cabi.STD_NTSC, noise_sigma: float = 0
 
 
 def make_sequence(seed: int, standard: int, n_fields: int, noise_sigma: float = 0.5,
-                  moving: bool = True) -> list[FieldSample]:
-    """Consecutive fields (two per frame, parity alternating) of one scene."""
-    sc = make_scene(seed, standard, n_rects=4 if moving else 0)
+                  moving: bool = True, grille=None, scene: Scene | None = None
+                  ) -> list[FieldSample]:
+    """Consecutive fields (two per frame, parity alternating) of one scene
+    (`scene` overrides the seeded one)."""
+    sc = scene or make_scene(seed, standard, n_rects=4 if moving else 0, grille=grille)
     base = float(np.random.default_rng(seed + 17).uniform(-np.pi, np.pi))
     return [make_field(seed, standard, noise_sigma, field_index=j, parity=j % 2,
                        scene=sc, theta_base=base) for j in range(n_fields)]
@@ -273,11 +286,13 @@ def mixed_batch(seed: int, n_ntsc: int = 40, n_pal: int = 24,
 
 
 def make_frames(seed: int, standard: int, n_frames: int, noise_sigma: float = 0.5,
-                moving: bool = False, blanking: float = 240.0, white: float = 800.0):
+                moving: bool = False, blanking: float = 240.0, white: float = 800.0,
+                grille=None, scene: Scene | None = None):
     """Field-sequential 10-bit int16 frame buffers (the plugin's CVBS frame
     layout, frame_bridge.h:12-23): field 1 lines, then field 2 lines, with the
     PAL extra samples on frame lines 312 and 624. Returns (frames, fields)."""
-    fields = make_sequence(seed, standard, 2 * n_frames, noise_sigma, moving)
+    fields = make_sequence(seed, standard, 2 * n_frames, noise_sigma, moving, grille=grille,
+                           scene=scene)
     g = _cabi.default_geometry(standard)
     fw = g.field_width
     if standard == _cabi.STD_PAL:
@@ -339,3 +354,24 @@ def make_yc_frames(seed: int, standard: int, n_frames: int, noise_sigma: float =
         ys.append(np.concatenate(ybuf))
         cs.append(np.concatenate(cbuf))
     return ys, cs, fields
+
+
+def grille_scene(seed: int, standard: int, grille=(0.35, 0.6, 0.3, 0.55, 4.6, 18.0),
+                 n_rects: int = 0) -> Scene:
+    """A flat, colourless scene (one broad luma blob) with one localized luma
+    grating near the subcarrier: the case selective 3-D is for -- the
+    ambiguity detector should find the grating's box and nothing else."""
+    g = _cabi.default_geometry(standard)
+    rows, w = 2 * g.active_lines, g.active_width
+    sc = Scene(seed, standard, rows, w)
+    sc.blobs.append((rows / 2, w / 2, 0.6 * rows, 0.6 * w, 20.0))
+    r0, r1, c0, c1, period, amp = grille
+    sc.grilles.append((r0 * rows, r1 * rows, c0 * w, c1 * w, period, amp))
+    rng = np.random.default_rng(seed)
+    for _ in range(n_rects):
+        hh, ww = rng.uniform(0.12, 0.2) * rows, rng.uniform(0.06, 0.12) * w
+        sc.rects.append(dict(r0=rng.uniform(0.1, 0.9) * rows - hh / 2,
+                             c0=rng.uniform(0.1, 0.9) * w - ww / 2, h=hh, w=ww,
+                             vx=rng.integers(-8, 9) / 2.0, vy=rng.integers(-4, 5) / 2.0,
+                             y=rng.uniform(30, 70), a=0.0, b=0.0))
+    return sc

@@ -121,12 +121,15 @@ typedef struct hvdg_config {
   float odd_gate_floor;      /* 0.35 */
   int32_t output_fidelity;   /* 1    */
   int32_t psi_init;          /* 0    */
+  int32_t selective_3d;      /* 0; full-window 2-D + 3-D on the ambiguous boxes
+                                (hvd_config.h:405-416, frame_bridge.cpp:402-718) */
+  float selective_max_area;  /* 0.45 */
   /* ---- B200 build extensions (no HvdConfig counterpart) ---- */
   int32_t me_mode;           /* 0 = reference float-SSD pyramid (motion.cpp:397-488),
                                 1 = exhaustive integer SAD on uint16-quantised luma */
   int32_t me_block;          /* block size for me_mode 1 (16) */
   int32_t me_range;          /* +/- search range for me_mode 1 (16) */
-  int32_t reserved[5];
+  int32_t reserved[3];
 } hvdg_config;
 
 /* Mirror of hvd::FrameParams (frame_bridge.h:40-101). */
@@ -301,6 +304,15 @@ hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* lu
 /* ------------------------------------------------------------------------ */
 /* Kernel level (host buffers)                                               */
 /* ------------------------------------------------------------------------ */
+
+/* AmbiguousBoxes (frame_bridge.cpp:402-580, the selective 3-D detector) on
+ * one decoded field (luma h x w, chroma h x w x 2), host only. Writes up to
+ * max_boxes boxes as (fy0, fy1, x0, x1) in active-picture coordinates and
+ * sets *n_boxes to their count: 0 = stay 2-D, -1 = run the full 3-D window
+ * (ambiguity everywhere). */
+hvdg_status hvdg_ambiguous_boxes(const float* luma, const float* chroma, int h, int w,
+                                 float max_area, int32_t* boxes, int max_boxes, int* n_boxes);
+
 
 /* BurstLockinPhase (lockin.cpp:169-254) on NTSC, BurstLockinPhasePal
  * (lockin.cpp:325-417) on the PAL family. `field_ire` is field_height x

@@ -1016,6 +1016,97 @@ def detect_field_parity(b1, b2, fp, g) -> int:
     return 1 if ep < em else -1
 
 
+def ambiguous_boxes(Y, chi, max_area=0.45):
+    """AmbiguousBoxes (frame_bridge.cpp:402-580) in float32 / float64 as the
+    reference: [] = stay 2-D, None = full 3-D, else [(fy0, fy1, x0, x1)]."""
+    T, HX, HY, K = 16, 48, 16, 8
+    ya = np.asarray(Y, np.float32)
+    ca = np.abs(np.asarray(chi, np.complex64)).astype(np.float32)
+    h, w = ya.shape
+    th, tw = (h + T - 1) // T, (w + T - 1) // T
+
+    def box_mean(a):
+        def along(a, axis):
+            n = a.shape[axis]
+            acc = np.zeros_like(a)
+            cnt = np.zeros(n, np.int64)
+            for d in range(-K // 2, K - K // 2):
+                lo, hi = max(0, -d), min(n, n - d)
+                if hi <= lo:
+                    continue
+                if axis == 0:
+                    acc[lo:hi] = acc[lo:hi] + a[lo + d:hi + d]
+                else:
+                    acc[:, lo:hi] = acc[:, lo:hi] + a[:, lo + d:hi + d]
+                cnt[lo:hi] += 1
+            c = np.maximum(cnt, 1).astype(np.float32)
+            return acc / (c[:, None] if axis == 0 else c[None, :])
+        return along(along(a, 0), 1)
+
+    dy = (ya - box_mean(ya)).astype(np.float64)
+    dc = (ca - box_mean(ca)).astype(np.float64)
+    score = np.zeros((th, tw), np.float32)
+    for ty in range(th):
+        for tx in range(tw):
+            sl = (slice(ty * T, min(h, ty * T + T)), slice(tx * T, min(w, tx * T + T)))
+            n = dy[sl].size
+            ey = np.cumsum((dy[sl] * dy[sl]).ravel())[-1]   # sequential, raster order
+            ec = np.cumsum((dc[sl] * dc[sl]).ravel())[-1]
+            score[ty, tx] = np.float32(math.sqrt((ey / n) * (ec / n)))
+    flat = score.ravel().copy()
+    k = flat.size // 2
+    med = np.float32(np.partition(flat, k)[k])
+    flagged = score >= np.float32(4.0) * med
+    dense = np.zeros((th, tw), bool)
+    for ty in range(1, th - 1):
+        for tx in range(1, tw - 1):
+            if flagged[ty, tx]:
+                nb = int(flagged[ty - 1:ty + 2, tx - 1:tx + 2].sum()) - 1
+                dense[ty, tx] = nb >= 2
+    bands = []
+    for ty in range(th):
+        if dense[ty].sum() < 2:
+            continue
+        if bands and ty - bands[-1][1] <= 1:
+            bands[-1][1] = ty
+        else:
+            bands.append([ty, ty])
+    if not bands:
+        return None if med > np.float32(3.0) else []
+    while len(bands) > 4:
+        gaps = [bands[i + 1][0] - bands[i][1] for i in range(len(bands) - 1)]
+        bi = int(np.argmin(gaps))           # first of the smallest gaps
+        bands[bi][1] = bands[bi + 1][1]
+        del bands[bi + 1]
+    boxes = []
+    for tr0, tr1 in bands:
+        col = dense[tr0:tr1 + 1].any(axis=0)
+        y0 = max(0, tr0 * T - HY)
+        y0 -= y0 % 2
+        y1 = min(h, (tr1 + 1) * T + HY)
+        runs = []
+        for tx in range(tw):
+            if not col[tx]:
+                continue
+            if runs and tx - runs[-1][1] <= 2:
+                runs[-1][1] = tx
+            else:
+                runs.append([tx, tx])
+        first = len(boxes)
+        for c0, c1 in runs:
+            if c1 - c0 < 1:
+                continue
+            x0, x1 = max(0, c0 * T - HX), min(w, (c1 + 1) * T + HX)
+            if len(boxes) > first and x0 <= boxes[-1][3]:
+                boxes[-1][3] = x1
+            else:
+                boxes.append([y0, y1, x0, x1])
+    area = sum(float(b[1] - b[0]) * (b[3] - b[2]) for b in boxes)
+    if area > float(np.float32(max_area)) * h * w:
+        return None
+    return [tuple(b) for b in boxes]
+
+
 # --------------------------------------------------------------------------
 # Temporal (3-D) field window (engine/sequence.cpp:423-1116), the subset with
 # no anchor pass, no coherence gate, no trajectory fit, no PSI init.

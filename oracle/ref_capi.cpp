@@ -82,6 +82,8 @@ hvd::HvdConfig ToCfg(const hvdg_config& c) {
   o.odd_gate_floor = c.odd_gate_floor;
   o.output_fidelity = c.output_fidelity != 0;
   o.psi_init = c.psi_init != 0;
+  o.selective_3d = c.selective_3d != 0;
+  o.selective_max_area = c.selective_max_area;
   return o;
 }
 

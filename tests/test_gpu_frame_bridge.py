@@ -59,3 +59,42 @@ def test_frame_window_rejects_empty_window(ctx):
     with pytest.raises(api.HvdgError) as e:
         ctx.decode_frame_sequence_window(frames, 1, 1, fp, api.default_config())
     assert e.value.status == _cabi.ERR_BAD_ARGUMENT
+
+
+@pytest.mark.parametrize("std,n_rects", [(_cabi.STD_NTSC, 0), (_cabi.STD_PAL, 2)])
+def test_selective_3d_window_vs_reference(ctx, std, n_rects):
+    """Selective 3-D (DecodeWindowSelective, frame_bridge.cpp:596-718): the
+    2-D window plus the 3-D window decoded on each ambiguous box (a cropped
+    geometry on the device), feather-blended. Against the compiled reference
+    with the temporal tolerances above; outside the boxes the output is the
+    device's plain 2-D window exactly."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    sc = synth.grille_scene(7, std, n_rects=n_rects)
+    frames, _ = synth.make_frames(7, std, 3, noise_sigma=0.7, moving=n_rects > 0, scene=sc)
+    fp = api.frame_params(std)
+    base = dict(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6)
+    cfg = api.default_config(temporal_strength=0.5, passes=1, nr_anchor=0.0, coherence_gate=0.0,
+                             trajectory_fit=0, selective_3d=1, **base)
+    got = ctx.decode_frame_sequence_window(frames, 1, 2, fp, cfg)
+    want = ref.decode_frame_sequence_window(frames, 1, 2, fp, cfg)
+    two = ctx.decode_frame_sequence_window(frames, 1, 2, fp,
+                                           api.default_config(temporal_strength=-1.0, **base))
+    for key in ("luma", "chroma"):
+        d = np.abs(got[0][key].astype(np.int32) - want[0][key].astype(np.int32))
+        print(f"selective std={std} {key}: max {d.max()} frac>0 {(d > 0).mean():.2e}")
+        assert (d > 1).mean() < 1e-3, key
+        assert (d > 0).mean() < 2e-2, key
+    for key in ("u", "v"):
+        du = np.abs(got[0][key] - want[0][key])
+        assert np.quantile(du, 0.99) < 0.05 and np.quantile(du, 0.999) < 0.5, key
+    g = _cabi.default_geometry(std)
+    moved = (got[0]["luma"] != two[0]["luma"]).reshape(fp.frame_height, fp.frame_width)
+    assert moved.any()
+    rows = np.nonzero(moved.any(axis=1))[0]
+    cols = np.nonzero(moved.any(axis=0))[0]
+    a0, a1 = g.active_video_start, g.active_video_end
+    # the boxes are strictly inside the active picture, not the whole of it
+    assert cols.min() > a0 and cols.max() < a1 - 1
+    assert len(rows) < 0.8 * 2 * g.active_lines
