@@ -148,6 +148,11 @@ struct GeomTables {
   std::vector<float2> khat_row;  // 2 * kRowFft
   std::vector<float2> khat_col;  // 2 * col_m
   std::vector<float2> col_phasor;
+  // symmetry variant (built on first use): row chirp (w) | row chirp-filter
+  // spectrum (kRowFft) | column chirp (hp) | column filter spectrum (col_m) |
+  // gx (w) | gy (hp), the last two in .x
+  bool sym_ready = false;
+  std::vector<float2> sym;
 };
 
 // The two crop variants of HolographicInit (holographic_init.cpp:236).
@@ -190,6 +195,72 @@ GeomTables make_geom_tables(const hvdg_geometry& g) {
     }
   }
   return t;
+}
+
+// In-place radix-2 DFT of a power-of-two length, exp(-2 pi i jk / n), double.
+void host_fft(std::vector<cd>& a) {
+  const int n = (int)a.size();
+  for (int i = 1, j = 0; i < n; ++i) {
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    for (int i = 0; i < n; i += len)
+      for (int k = 0; k < len / 2; ++k) {
+        const double ang = -2.0 * kPi * k / len;
+        const cd u = a[i + k], v = a[i + k + len / 2] * cd(std::cos(ang), std::sin(ang));
+        a[i + k] = u + v;
+        a[i + k + len / 2] = u - v;
+      }
+  }
+}
+
+// Bluestein tables of an exact-length DFT of length N through a cyclic
+// convolution of length M: chirp c[n] = exp(-i pi n^2 / N) and the spectrum
+// of the filter conj(c) wrapped to length M, divided by M.
+void bluestein_tables(int N, int M, std::vector<float2>* out) {
+  std::vector<cd> c(N);
+  for (int k = 0; k < N; ++k) {
+    const int64_t kk = (int64_t)k * k % (2LL * N);  // exact reduction of the phase
+    c[k] = cd(std::cos(kPi * (double)kk / N), -std::sin(kPi * (double)kk / N));
+  }
+  for (int k = 0; k < N; ++k) out->push_back(make_float2((float)c[k].real(), (float)c[k].imag()));
+  std::vector<cd> h(M, cd(0, 0));
+  for (int k = 0; k < N; ++k) {
+    h[k] = std::conj(c[k]);
+    if (k) h[M - k] = std::conj(c[k]);
+  }
+  host_fft(h);
+  for (int m = 0; m < M; ++m)
+    out->push_back(make_float2((float)(h[m].real() / M), (float)(h[m].imag() / M)));
+}
+
+// The symmetry variant's tables (holographic_init.cpp:265-306). Its crop
+// {1.3 MHz, 60 c/ph} multiplies the spectrum directly, so gx / gy are
+// evaluated as GaussianLpf does (holographic_init.cpp:16-56): float
+// frequencies, float cutoffs, float exp.
+void make_sym_tables(GeomTables& t, const hvdg_geometry& g) {
+  t.sym.clear();
+  bluestein_tables(t.w, hvdg::kRowFft, &t.sym);
+  bluestein_tables(t.hp, t.col_m, &t.sym);
+  auto freq = [](int i, int n, double d) {
+    const double inv = 1.0 / ((double)n * d);
+    const int half = (n % 2 == 0) ? n / 2 : (n + 1) / 2;
+    return (float)((i < half ? i : i - n) * inv);
+  };
+  const float cx = 1.3f * 1.0e6f;
+  const float cy = 60.0f / (2.0f * (float)t.h);
+  for (int x = 0; x < t.w; ++x) {
+    const float r = freq(x, t.w, 1.0 / g.sample_rate) / cx;
+    t.sym.push_back(make_float2(std::exp(-0.5f * r * r), 0.f));
+  }
+  for (int y = 0; y < t.hp; ++y) {
+    const float r = freq(y, t.hp, 1.0) / cy;
+    t.sym.push_back(make_float2(std::exp(-0.5f * r * r), 0.f));
+  }
+  t.sym_ready = true;
 }
 
 using GeomKey = std::tuple<int, int, int, int, int, int, double, double>;
@@ -432,6 +503,7 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     const GeomKey key = geom_key(g);
     auto it = ctx->geoms.find(key);
     if (it == ctx->geoms.end()) it = ctx->geoms.emplace(key, make_geom_tables(g)).first;
+    if (cfg->symmetry_variant && !it->second.sym_ready) make_sym_tables(it->second, g);
     int gs;
     auto sit = slot.find(key);
     if (sit == slot.end()) {
@@ -472,6 +544,17 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     gd.khat_col_off = nkhat;
     gd.col_m = t.col_m;
     nkhat += 2 * t.col_m;
+    gd.sym_row_chirp = gd.sym_row_hhat = gd.sym_col_chirp = gd.sym_col_hhat = -1;
+    gd.sym_gx = gd.sym_gy = -1;
+    if (cfg->symmetry_variant) {
+      gd.sym_row_chirp = nkhat;
+      gd.sym_row_hhat = gd.sym_row_chirp + t.w;
+      gd.sym_col_chirp = gd.sym_row_hhat + hvdg::kRowFft;
+      gd.sym_col_hhat = gd.sym_col_chirp + t.hp;
+      gd.sym_gx = gd.sym_col_hhat + t.col_m;
+      gd.sym_gy = gd.sym_gx + t.w;
+      nkhat += (int)t.sym.size();
+    }
     b.geoms.push_back(gd);
     b.gcol_off.push_back(ncol);
     ncol += t.w;
@@ -750,6 +833,8 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
       col.insert(col.end(), b.gtabs[g]->col_phasor.begin(), b.gtabs[g]->col_phasor.end());
       kh.insert(kh.end(), b.gtabs[g]->khat_row.begin(), b.gtabs[g]->khat_row.end());
       kh.insert(kh.end(), b.gtabs[g]->khat_col.begin(), b.gtabs[g]->khat_col.end());
+      if (b.geoms[g].sym_row_chirp >= 0)
+        kh.insert(kh.end(), b.gtabs[g]->sym.begin(), b.gtabs[g]->sym.end());
     }
     put(L.o_colph, col.data(), sizeof(float2) * col.size());
     put(L.o_khat, kh.data(), sizeof(float2) * kh.size());
@@ -808,6 +893,8 @@ hvdg::InitArgs init_args(hvdg_ctx* ctx, const Staged& S) {
   ia.chi2 = at<float2>(ctx, L.o_D0);
   ia.chi0 = at<float2>(ctx, L.o_X0);
   ia.Y = at<float>(ctx, L.o_Y);
+  // the symmetry variant's output: Q0 (the solver's planes are free during the init)
+  ia.chi3 = (!b.geoms.empty() && b.geoms[0].sym_row_chirp >= 0) ? at<float2>(ctx, L.o_Q0) : nullptr;
   const int* itb = at<int>(ctx, S.it_itab);
   ia.prow_field = itb + b.it_prow_field;
   ia.prow_first = itb + b.it_prow_first;
@@ -1206,7 +1293,7 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
 hvdg_status validate_fields(const hvdg_field_in* fields, int n, const hvdg_config* cfg,
                             hvdg_field_out* out) {
   if (n < 0 || (n > 0 && (!fields || !out)) || !cfg) return HVDG_ERR_BAD_ARGUMENT;
-  if (cfg->diag_prior > 0.0f || cfg->symmetry_variant) return HVDG_ERR_UNSUPPORTED;
+  if (cfg->diag_prior > 0.0f) return HVDG_ERR_UNSUPPORTED;
   for (int i = 0; i < n; ++i) {
     if (!fields[i].samples || !fields[i].geometry) return HVDG_ERR_BAD_ARGUMENT;
     if (fields[i].sample_type < 0 || fields[i].sample_type > 2) return HVDG_ERR_BAD_ARGUMENT;
@@ -2781,7 +2868,7 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
     ctx->last_error = "woven frame beyond the device-path limits";
     return st;
   }
-  if (cfg->diag_prior > 0.0f || cfg->symmetry_variant) return HVDG_ERR_UNSUPPORTED;
+  if (cfg->diag_prior > 0.0f) return HVDG_ERR_UNSUPPORTED;
   if (diag) std::memset(diag, 0, sizeof(*diag));
   if (n == 0) return HVDG_OK;
   cudaSetDevice(ctx->device);

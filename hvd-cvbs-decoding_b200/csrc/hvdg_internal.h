@@ -65,6 +65,11 @@ struct GeomDesc {
   int khat_row_off;    // offset (float2) of the 2 row kernels' spectra (2 * kRowFft)
   int khat_col_off;    // offset (float2) of the 2 column kernels' spectra (2 * col_m)
   int col_m;           // column convolution length: kColFft or kColFftWide
+  // symmetry-variant tables (offsets into the same float2 table; -1 when
+  // the batch runs without the variant): Bluestein chirps exp(-i pi n^2 / N)
+  // and chirp-filter spectra (1/M folded in) of the exact-length row (w)
+  // and column (hp) DFTs, and the {1.3 MHz, 60 c/ph} crop (gx, gy in .x)
+  int sym_row_chirp, sym_row_hhat, sym_col_chirp, sym_col_hhat, sym_gx, sym_gy;
 };
 
 // Solver control block, one per field (written by the last arriver of each

@@ -245,6 +245,166 @@ __global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
   }
 }
 
+// ---- symmetry variant (holographic_init.cpp:265-306) ------------------------
+// The certification min(|D[k]|, |D[-k]|) / (|D[k]| + eps) is not separable,
+// so this variant needs the exact hp x w 2-D DFT of the padded demodulated
+// field. Each exact-length 1-D DFT runs as Bluestein's chirp-z transform
+// (Bluestein 1970): with c[n] = exp(-i pi n^2 / N),
+//   X[k] = c[k] sum_n (x[n] c[n]) conj(c[k - n]),
+// a cyclic convolution of length M >= 2 N - 1 (rows 2048, columns col_m):
+// FFT, multiply by hhat = FFT_M(conj(c), wrapped) / M, inverse FFT. The
+// inverse 2-D DFT is conj(DFT(conj(X))) / (hp w): conjugate on the column
+// pass's load and on the row pass's store. rowbuf (free once the column pass
+// of the two crop variants is done) holds plane 0 = the spectrum and
+// plane 1 = the certified spectrum, per field.
+
+// mode 0: forward DFT of padded row yp of the demodulated field -> plane 0.
+// mode 1: last pass of the inverse, rows [pad, pad + h) of plane 1 -> chi3,
+//         x 2 / (hp w) (Fft2d::Inverse's 1 / (hp w), then the init's x2).
+// grid = total padded rows; block 256; dynamic smem 2 x kRowFft float2.
+__global__ void __launch_bounds__(256) k_sym_rows(InitArgs a, int mode) {
+  extern __shared__ float2 sm_sym[];
+  float2* P = sm_sym;
+  float2* Q = P + kRowFft;
+  const int r = blockIdx.x;
+  const int f_idx = a.prow_field[r];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  const int yp = r - a.prow_first[f_idx];
+  if (mode == 1 && (yp < gd.pad || yp >= gd.pad + f.h)) return;  // uniform per CTA
+  const float2* chirp = a.khat + gd.sym_row_chirp;
+  const float2* hh = a.khat + gd.sym_row_hhat;
+  float2* plane0 = a.rowbuf + a.rowbuf_off[f_idx];
+  float2* plane1 = plane0 + (int64_t)gd.hp * f.pitch;
+  if (mode == 0) {
+    const int sy = mirror_row(yp - gd.pad, f.h);
+    const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
+    for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) {
+      float2 v = make_float2(0.f, 0.f);
+      if (i < f.w) {
+        const float s = S[i];
+        const float2 c = carrier_at(a, f, sy, i);
+        v = cmul(make_float2(s * c.x, -s * c.y), __ldg(chirp + i));
+      }
+      P[i] = v;
+    }
+  } else {
+    const float2* src = plane1 + (int64_t)yp * f.pitch;
+    for (int i = threadIdx.x; i < kRowFft; i += blockDim.x)
+      P[i] = i < f.w ? cmul(src[i], __ldg(chirp + i)) : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* spec = fft_stockham<kRowFft, false>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+  float2* oth = spec == P ? Q : P;
+  for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) oth[i] = cmul(spec[i], __ldg(hh + i));
+  __syncthreads();
+  float2* res = fft_stockham<kRowFft, true>(oth, spec, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+  if (mode == 0) {
+    float2* dst = plane0 + (int64_t)yp * f.pitch;
+    for (int i = threadIdx.x; i < f.pitch; i += blockDim.x)
+      dst[i] = i < f.w ? cmul(res[i], __ldg(chirp + i)) : make_float2(0.f, 0.f);
+  } else {
+    const float scale = 2.0f / ((float)gd.hp * (float)f.w);
+    float2* dst = a.chi3 + f.px_off + (int64_t)(yp - gd.pad) * f.pitch;
+    for (int i = threadIdx.x; i < f.pitch; i += blockDim.x) {
+      float2 v = make_float2(0.f, 0.f);
+      if (i < f.w) {
+        const float2 X = cmul(res[i], __ldg(chirp + i));
+        v = make_float2(X.x * scale, -X.y * scale);
+      }
+      dst[i] = v;
+    }
+  }
+}
+
+// Column DFTs in place. mode 0: forward on plane 0; mode 1: the conjugated
+// input of the inverse, on plane 1 (the row pass conjugates the output).
+template <int M, int G, typename Sync>
+__device__ __forceinline__ void sym_cols_body(const InitArgs& a, const FieldDesc& f,
+                                              const GeomDesc& gd, int f_idx, int x0,
+                                              const float2* __restrict__ tw, int ct, int nct,
+                                              int col, Sync sync, int mode) {
+  extern __shared__ float2 sm_cols[];
+  float2* A = sm_cols + col * 2 * M;
+  float2* B = A + M;
+  const float2* chirp = a.khat + gd.sym_col_chirp;
+  const float2* hh = a.khat + gd.sym_col_hhat;
+  float2* plane = a.rowbuf + a.rowbuf_off[f_idx] + (mode ? (int64_t)gd.hp * f.pitch : 0);
+  for (int i = threadIdx.x; i < M * G; i += blockDim.x) {
+    const int row = i / G, c = i % G;
+    float2 v = make_float2(0.f, 0.f);
+    if (row < gd.hp && x0 + c < f.w) {
+      v = plane[(int64_t)row * f.pitch + x0 + c];
+      if (mode) v.y = -v.y;
+      v = cmul(v, __ldg(chirp + row));
+    }
+    sm_cols[c * 2 * M + row] = v;
+  }
+  __syncthreads();
+  float2* spec = fft_stockham<M, false>(A, B, tw, ct, nct, sync);
+  float2* other = spec == A ? B : A;
+  for (int i = ct; i < M; i += nct) other[i] = cmul(spec[i], __ldg(hh + i));
+  sync();
+  float2* res = fft_stockham<M, true>(other, spec, tw, ct, nct, sync);
+  if (res != A)
+    for (int i = ct; i < M; i += nct) A[i] = res[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < gd.hp * G; i += blockDim.x) {
+    const int row = i / G, c = i % G;
+    if (x0 + c < f.w)
+      plane[(int64_t)row * f.pitch + x0 + c] = cmul(sm_cols[c * 2 * M + row], __ldg(chirp + row));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sym_cols(InitArgs a, int mode) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gidx = blockIdx.x;
+  const int f_idx = a.cgrp_field[gidx];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  if (gd.col_m == kColFftWide) {
+    const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
+    const int pair = threadIdx.x >> 6;
+    sym_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 63, 64,
+                                              pair, PairSync{1 + pair}, mode);
+  } else {
+    const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
+    sym_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, lane, 32, warp, WarpSync(),
+                                      mode);
+  }
+}
+
+// Certified spectrum (holographic_init.cpp:276-290): plane 1 = plane 0 x
+// min(m, m_r) / (m + 1e-6) x gy[y] gx[x], m_r the magnitude at the point
+// reflection ((hp - y) mod hp, (w - x) mod w). grid = total padded rows.
+__global__ void __launch_bounds__(256) k_sym_certify(InitArgs a) {
+  const int r = blockIdx.x;
+  const int f_idx = a.prow_field[r];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  const int y = r - a.prow_first[f_idx];
+  const int ry = (gd.hp - y) % gd.hp;
+  const float2* plane0 = a.rowbuf + a.rowbuf_off[f_idx];
+  float2* dst = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)(gd.hp + y) * f.pitch;
+  const float2* row = plane0 + (int64_t)y * f.pitch;
+  const float2* rrow = plane0 + (int64_t)ry * f.pitch;
+  const float gy = __ldg(a.khat + gd.sym_gy + y).x;
+  for (int x = threadIdx.x; x < f.pitch; x += blockDim.x) {
+    float2 v = make_float2(0.f, 0.f);
+    if (x < f.w) {
+      const int rx = (f.w - x) % f.w;
+      const float2 X = row[x];
+      const float m = hypotf(X.x, X.y);
+      const float2 R = rrow[rx];
+      const float mr = hypotf(R.x, R.y);
+      const float sym = fminf(m, mr) / (m + 1e-6f);
+      const float k = gy * __ldg(a.khat + gd.sym_gx + x).x;
+      v = make_float2(X.x * sym * k, X.y * sym * k);
+    }
+    dst[x] = v;
+  }
+}
+
 // ---- blend -----------------------------------------------------------------
 // Edge-energy blend (holographic_init.cpp:240-316). 32 x 32 output tile per
 // CTA; y_v on the tile + 4 halo (forward difference + box radius 3); the box
@@ -263,8 +423,9 @@ __global__ void __launch_bounds__(256) k_init_blend(InitArgs a) {
   __shared__ float wsum[kBT][kBT];
   __shared__ float2 num[kBT][kBT];
   const float* S = a.S + f.px_off;
-  for (int v = 0; v < 2; ++v) {
-    const float2* chi = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
+  const int nv = a.chi3 ? 3 : 2;
+  for (int v = 0; v < nv; ++v) {
+    const float2* chi = (v == 0 ? a.chi1 : (v == 1 ? a.chi2 : a.chi3)) + f.px_off;
     // residual luma on [ty0-3, ty0+kBT+5) x [tx0-3, ...)
     for (int i = threadIdx.x; i < kBH * kBH; i += blockDim.x) {
       const int ly = i / kBH, lx = i % kBH;
@@ -390,6 +551,7 @@ void configure_init_kernels() {
   cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        3 * kRowFft * (int)sizeof(float2));
   cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
+  cudaFuncSetAttribute(k_sym_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
   cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, kAnisoSmem);
 }
 
@@ -404,6 +566,14 @@ void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int tota
   }
   if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
   if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
+  if (a.chi3 && total_prows > 0 && total_cgroups > 0) {
+    const int sym_smem = 2 * kRowFft * sizeof(float2);
+    k_sym_rows<<<total_prows, 256, sym_smem, st>>>(a, 0);
+    k_sym_cols<<<total_cgroups, 256, col_smem, st>>>(a, 0);
+    k_sym_certify<<<total_prows, 256, 0, st>>>(a);
+    k_sym_cols<<<total_cgroups, 256, col_smem, st>>>(a, 1);
+    k_sym_rows<<<total_prows, 256, sym_smem, st>>>(a, 1);
+  }
   if (total_btiles > 0) k_init_blend<<<total_btiles, 256, 0, st>>>(a);
 }
 

@@ -37,6 +37,12 @@ struct InitArgs {
   // this applies the adjoint of the forward crop (the x2 included).
   const float2* adj_in = nullptr;
   float2* adj_out = nullptr;
+  // Symmetry variant (holographic_init.cpp:265-306), when chi3 is set: the
+  // exact hp x w 2-D DFT of the padded demodulated field (Bluestein rows /
+  // columns through rowbuf, which is free once the column pass is done),
+  // the certified spectrum, its inverse cropped into chi3, blended as the
+  // third variant.
+  float2* chi3 = nullptr;
 };
 
 void configure_init_kernels();

@@ -100,7 +100,8 @@ typedef struct hvdg_config {
   float cg_tol;              /* 0 = auto (0.02 slow / 0.10 fast) */
   int32_t fast;              /* 1    */
   int32_t parallel_across_fields; /* 1 (CPU-baseline knob; the device path always batches) */
-  int32_t symmetry_variant;  /* 0; 1 is HVDG_ERR_UNSUPPORTED on the device path */
+  int32_t symmetry_variant;  /* 0; 1 adds the spectral-symmetry third init variant
+                                (holographic_init.cpp:265-306); refused by the adjoint */
   int32_t acc;               /* 1    */
   float chroma_gain;         /* 1.0  */
   int32_t monochrome;        /* 0    */

@@ -390,8 +390,23 @@ def edge_energy(y):
 INIT_VARIANTS = ((0.8, 120.0), (1.8, 30.0))  # holographic_init.cpp:236
 
 
-def holographic_init(s, carrier, g):
-    """HolographicInit (holographic_init.cpp:200-317), symmetry variant off."""
+def symmetry_certify(spec, gy, gx):
+    """The third variant's spectrum (holographic_init.cpp:265-290): each bin
+    weighted by min(|D[k]|, |D[-k]|) / (|D[k]| + 1e-6) -- bin k pairs with
+    its point reflection ((hp - y) mod hp, (w - x) mod w) -- and the
+    {1.3 MHz, 60 c/ph} Gaussian crop."""
+    hp, w = spec.shape
+    mag = np.abs(spec)
+    ry = (hp - np.arange(hp)) % hp
+    rx = (w - np.arange(w)) % w
+    mr = mag[ry][:, rx]
+    sym = np.minimum(mag, mr) / (mag + 1e-6)
+    return spec * sym * gy[:, None] * gx[None, :]
+
+
+def holographic_init(s, carrier, g, symmetry_variant=False):
+    """HolographicInit (holographic_init.cpp:200-317), with the optional
+    spectral-symmetry third variant (:265-306)."""
     s = np.asarray(s, np.float64)
     h, w = s.shape
     demod = s * np.conj(carrier)
@@ -401,9 +416,15 @@ def holographic_init(s, carrier, g):
     spec = np.fft.fft2(demod[rows])
     num = np.zeros((h, w), np.complex128)
     wsum = np.zeros((h, w))
+    crops = []
     for (mhz, cph) in INIT_VARIANTS:
         gy, gx = gaussian_lpf(hp, w, g, mhz, cph, h)
-        chi_v = np.fft.ifft2(spec * gy[:, None] * gx[None, :])[pad:pad + h] * 2.0
+        crops.append(spec * gy[:, None] * gx[None, :])
+    if symmetry_variant:
+        gy, gx = gaussian_lpf(hp, w, g, 1.3, 60.0, h)
+        crops.append(symmetry_certify(spec, gy, gx))
+    for crop in crops:
+        chi_v = np.fft.ifft2(crop)[pad:pad + h] * 2.0
         y_v = s - np.real(chi_v * carrier)
         wt = 1.0 / (edge_energy(y_v) + 0.5)
         num += chi_v * wt
@@ -584,7 +605,8 @@ def decode_fields_2d(fields_ire, parities, g, cfg):
     out = []
     for f, p in zip(fields_ire, parities):
         obs = prepare_field(f, g, cfg, p)
-        _, chi0 = holographic_init(obs.s, obs.carrier, g)
+        _, chi0 = holographic_init(obs.s, obs.carrier, g,
+                                   bool(getattr(cfg, "symmetry_variant", 0)))
         y, chi = variational_refine(obs.s, obs.carrier, chi0, cfg, is_pal=uses_vswitch(g))
         if cfg.output_fidelity:
             y = obs.s - np.real(chi * obs.carrier)
@@ -1177,7 +1199,7 @@ def decode_window_temporal(fields_ire, parities, g, cfg, strength):
     c2.temporal_eps = eps_t
     Ys, chis = [], []
     for o in obs:
-        y0, chi0 = holographic_init(o.s, o.carrier, g)
+        y0, chi0 = holographic_init(o.s, o.carrier, g, bool(getattr(cfg, "symmetry_variant", 0)))
         Ys.append(y0)
         chis.append(chi0)
     offs = temporal_offsets(cfg, pal)

@@ -49,3 +49,34 @@ def test_decode_field_matches_oracle(ctx, std):
     # lossless split: Y + Re[chi c] == S
     s = obs.s
     assert np.abs(out.luma + np.real(out.chroma * obs.carrier) - s).max() < 2e-3
+
+
+@pytest.mark.parametrize("std", [_cabi.STD_NTSC, _cabi.STD_PAL])
+def test_symmetry_variant_vs_oracle(ctx, std):
+    """HolographicInit's spectral-symmetry third variant
+    (holographic_init.cpp:265-306: exact hp x w 2-D DFT by Bluestein rows /
+    columns on the device, certified spectrum, inverse, blended third) --
+    the init alone and the whole 2-D decode against the FP64 oracle."""
+    g = _cabi.default_geometry(std)
+    f = synth.make_field(21 + std, std, noise_sigma=0.5)
+    cfg = _cfg(symmetry_variant=1)
+    ire = synth.to_ire(f.samples)
+    obs = O.prepare_field(ire, g, cfg, 0)
+    fal, lal = g.first_active_field_line, g.last_active_line
+    th = obs.theta[fal:lal].astype(np.float32)
+    sw = obs.vswitch[fal:lal].astype(np.int8)
+    y0, chi0 = ctx.holographic_init(obs.s.astype(np.float32), th, sw, g, cfg)
+    yo, co = O.holographic_init(obs.s, O.make_carrier(th, sw, g), g, symmetry_variant=True)
+    _, cplain = O.holographic_init(obs.s, O.make_carrier(th, sw, g), g)
+    dc, dy = np.abs(chi0 - co).max(), np.abs(y0 - yo).max()
+    print(f"std={std} init: max dchi {dc:.3g} max dY {dy:.3g} "
+          f"(variant moves chi by {np.abs(co - cplain).max():.3g})")
+    assert np.abs(co - cplain).max() > 0.5
+    assert dc < 5e-3 and dy < 5e-3
+    out = ctx.decode_fields([api.Field(f.samples, g, parity=0)], cfg)[0]
+    (yd, cd, _), = O.decode_fields_2d([ire], [0], g, cfg)
+    print(f"std={std} decode: max dY {np.abs(out.luma - yd).max():.3g} "
+          f"max dC {np.abs(out.chroma - cd).max():.3g}")
+    assert abs(psnr(out.luma, f.y_true) - psnr(yd, f.y_true)) < 0.05
+    assert abs(psnr(out.chroma, f.chi_true) - psnr(cd, f.chi_true)) < 0.05
+    assert np.abs(out.luma - yd).max() < 0.05 and np.abs(out.chroma - cd).max() < 0.05

@@ -72,7 +72,8 @@ def test_frame_buffer_vs_reference(ctx, std, field_order):
 
 @pytest.mark.parametrize("opts", [dict(monochrome=1), dict(acc=0, chroma_gain=1.3),
                                   dict(cg_iterations=0), dict(chroma_phase_deg=20.0),
-                                  dict(field_order=1, chroma_aniso=0.7)])
+                                  dict(field_order=1, chroma_aniso=0.7),
+                                  dict(symmetry_variant=1)])
 def test_frame_buffer_options_vs_reference(ctx, opts):
     ref = _ref()
     std = _cabi.STD_PAL if "chroma_phase_deg" in opts else _cabi.STD_NTSC

@@ -313,3 +313,24 @@ def test_single_reduction_cg_recurrence():
     gg = np.vdot(g0, g0).real
     pred = gg + 2 * a * np.real(np.vdot(g0, q)) + a * a * np.vdot(q, q).real
     assert abs(pred - np.vdot(g1, g1).real) < 1e-9 * gg
+
+
+@pytest.mark.parametrize("tag", ["ntsc", "pal"])
+def test_oracle_symmetry_variant_matches_reference(tag):
+    """HolographicInit's optional spectral-symmetry third variant
+    (holographic_init.cpp:265-306): the oracle's restatement against the
+    compiled reference on the golden field's prepared S and carrier."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    from hvdg import api
+    d = np.load(GOLD / f"field_{tag}_small.npz")
+    g = geom_from(d["geometry"], d["sample_rate"])
+    s, c = d["s"].astype(np.float64), d["carrier"].astype(np.complex128)
+    y0, chi0 = O.holographic_init(s, c, g, symmetry_variant=True)
+    _, chi_plain = O.holographic_init(s, c, g)
+    assert np.abs(chi0 - chi_plain).max() > 0.5     # the variant changes the init
+    ry0, rchi0 = ref.holographic_init(d["s"], d["carrier"], g,
+                                      api.default_config(symmetry_variant=1))
+    assert np.abs(chi0 - rchi0).max() < 1e-4
+    assert np.abs(y0 - ry0).max() < 1e-4
