@@ -311,6 +311,8 @@ struct hvdg_ctx {
   // autotuner: batch signature -> (band rows, CTAs per SM)
   int autotune = 1;
   std::map<std::string, std::pair<int, int>> tune;
+  // diagnostic maps of the sequence frame bridge (empty: off)
+  std::string debug_dir;
 };
 
 namespace hvdg {
@@ -2411,6 +2413,57 @@ hvdg_status decode_selective_boxes(hvdg_ctx* ctx, const std::vector<hvdg_field_i
   return HVDG_OK;
 }
 
+// The sequence bridge's diagnostic maps (frame_bridge.cpp:807-865): one
+// decision-log line per call appended to <dir>/diag.txt, and per core frame
+// <dir>/rainbow_<id>.pgm, the woven map of residual chroma in the decoded
+// luma: the triangle-7 demodulation of Y by the field's own carrier, summed
+// with the same-parity field two ahead (or behind) -- static luma cancels
+// between same-parity fields (the carrier has flipped), a correlated
+// separation error survives; 0..8 IRE -> 0..255.
+void write_debug_maps(const std::string& dir, int64_t base_frame_id, int core_begin, int core_end,
+                      bool f1_bottom, const hvdg_diag& d, float acc_gain,
+                      const std::vector<std::vector<float>>& Y,
+                      const std::vector<std::vector<float2>>& car, const std::vector<int>& parity,
+                      int lines, int aw) {
+  if (FILE* log = std::fopen((dir + "/diag.txt").c_str(), "a")) {
+    std::fprintf(log, "frames %lld..%lld: f1_bottom=%d sigma=%g amb=%g strength=%g eps_t=%g nr_eps=%g acc=%g\n",
+                 (long long)(base_frame_id + core_begin), (long long)(base_frame_id + core_end - 1),
+                 f1_bottom ? 1 : 0, d.sigma_ire, d.ambiguity_ire, d.resolved_strength,
+                 d.temporal_eps, d.nr_eps, acc_gain);
+    std::fclose(log);
+  }
+  static const float kW[7] = {1, 2, 3, 4, 3, 2, 1};
+  const int nfields = (int)Y.size();
+  for (int t = core_begin; t < core_end; ++t) {
+    std::vector<uint8_t> img((size_t)2 * lines * aw, 0);
+    for (int half = 0; half < 2; ++half) {
+      const int j = 2 * t + half;
+      const int j2 = (j + 2 < nfields) ? j + 2 : j - 2;
+      const int p = parity[j];
+      for (int r = 0; r < lines; ++r)
+        for (int x = 0; x + 7 <= aw; ++x) {
+          std::complex<float> dj(0.f, 0.f), dk(0.f, 0.f);
+          for (int k = 0; k < 7; ++k) {
+            const size_t o = (size_t)r * aw + x + k;
+            dj += kW[k] * Y[j][o] * std::conj(std::complex<float>(car[j][o].x, car[j][o].y));
+            if (j2 >= 0)
+              dk += kW[k] * Y[j2][o] * std::conj(std::complex<float>(car[j2][o].x, car[j2][o].y));
+          }
+          const float e = (j2 >= 0) ? std::abs(dj + dk) / 32.0f : std::abs(dj) / 16.0f;
+          const int v = std::min(std::max((int)(e * 32.0f), 0), 255);
+          img[(size_t)(2 * r + p) * aw + x + 3] = (uint8_t)v;
+        }
+    }
+    char name[64];
+    std::snprintf(name, sizeof(name), "/rainbow_%06lld.pgm", (long long)(base_frame_id + t));
+    if (FILE* f = std::fopen((dir + name).c_str(), "wb")) {
+      std::fprintf(f, "P5\n%d %d\n255\n", aw, 2 * lines);
+      std::fwrite(img.data(), 1, img.size(), f);
+      std::fclose(f);
+    }
+  }
+}
+
 int16_t clamp_u10(float v) {
   const long r = std::lround(v);
   return (int16_t)std::min<long>(std::max<long>(r, 0), 1023);
@@ -3355,10 +3408,26 @@ hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref, const float*
   return HVDG_OK;
 }
 
+hvdg_status hvdg_set_debug_dir(hvdg_ctx* ctx, const char* dir) {
+  if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  ctx->debug_dir = dir ? dir : "";
+  return HVDG_OK;
+}
+
 hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* const* frames,
                                               int n_frames, int core_begin, int core_end,
                                               const hvdg_frame_params* fp, const hvdg_config* cfg,
                                               hvdg_yc_frame* out, hvdg_diag* diag) {
+  return hvdg_decode_frame_sequence_window_at(ctx, frames, n_frames, core_begin, core_end, 0, fp,
+                                              cfg, out, diag);
+}
+
+hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* const* frames,
+                                                 int n_frames, int core_begin, int core_end,
+                                                 int64_t base_frame_id,
+                                                 const hvdg_frame_params* fp,
+                                                 const hvdg_config* cfg, hvdg_yc_frame* out,
+                                                 hvdg_diag* diag) {
   if (!ctx || !fp || !cfg) return HVDG_ERR_BAD_ARGUMENT;
   // the reference returns an empty vector for these windows (frame_bridge.cpp:728-731)
   if (n_frames <= 0 || !frames || core_begin < 0 || core_end > n_frames || core_begin >= core_end)
@@ -3451,6 +3520,29 @@ hvdg_status hvdg_decode_frame_sequence_window(hvdg_ctx* ctx, const int16_t* cons
     } else {
       colp[x] = make_float2((float)std::cos(w0 * smp), (float)std::sin(w0 * smp));
     }
+  }
+  if (!ctx->debug_dir.empty()) {
+    // diagnostic maps (frame_bridge.cpp:807-865): the per-call decision log
+    // and, per core frame, the woven residual-chroma-in-luma map
+    std::vector<std::vector<float2>> car(nfield);
+    for (int j = 0; j < nfield; ++j) {
+      car[j].resize((size_t)h * w);
+      for (int y = 0; y < h; ++y) {
+        const double thv = (double)th[j][fal + y];
+        const float2 Lc = make_float2((float)std::cos(thv), (float)std::sin(thv));
+        const bool sw = vsw && vs[j][fal + y] < 0;
+        for (int x = 0; x < w; ++x) {
+          float cr = Lc.x * colp[x].x - Lc.y * colp[x].y;
+          const float ci = Lc.x * colp[x].y + Lc.y * colp[x].x;
+          if (sw) cr = -cr;
+          car[j][(size_t)y * w + x] = make_float2(cr, ci);
+        }
+      }
+    }
+    std::vector<int> parity(nfield);
+    for (int j = 0; j < nfield; ++j) parity[j] = fi[j].parity;
+    write_debug_maps(ctx->debug_dir, base_frame_id, core_begin, core_end, f1_bottom, *dg, acc_gain,
+                     Yd, car, parity, h, w);
   }
   for (int t = core_begin; t < core_end; ++t) {
     hvdg_yc_frame& yc = out[t - core_begin];
@@ -3545,6 +3637,160 @@ hvdg_status hvdg_ambiguous_boxes(const float* luma, const float* chroma, int h, 
     boxes[4 * i + 2] = b[i].x0;
     boxes[4 * i + 3] = b[i].x1;
   }
+  return HVDG_OK;
+}
+
+hvdg_status hvdg_drizzle_frame(hvdg_ctx* ctx, const float* const* luma, const float* const* chroma,
+                               const int32_t* parities, int n, int j0, int h, int w,
+                               const hvdg_config* cfg, int scale, float* out_luma,
+                               float* out_chroma) {
+  if (!ctx || !luma || !chroma || !parities || !cfg || !out_luma || !out_chroma || n < 2 ||
+      j0 < 0 || j0 + 1 >= n || h < 1 || w < 1 || scale < 1 || cfg->mc_tile < 1 ||
+      cfg->mc_search < 0 || cfg->nr_radius < 0)
+    return HVDG_ERR_BAD_ARGUMENT;
+  for (int i = 0; i < n; ++i)
+    if (!luma[i] || !chroma[i]) return HVDG_ERR_BAD_ARGUMENT;
+  const int tile = cfg->mc_tile, search = cfg->mc_search;
+  if (4 * tile > 4096 || search > 64) return HVDG_ERR_UNSUPPORTED;
+  cudaSetDevice(ctx->device);
+  // pairs (sequence.cpp:300-310): for each target jt in {j0, j0 + 1}, the
+  // sources k within 2 nr_radius fields, the sibling skipped, the target
+  // itself with zero motion and confidence 1
+  std::vector<hvdg::MePair> mp;
+  std::vector<hvdg::DrizzlePair> dp;
+  for (int jt = j0; jt <= j0 + 1; ++jt)
+    for (int k = std::max(0, j0 - 2 * cfg->nr_radius);
+         k < std::min(n, j0 + 2 + 2 * cfg->nr_radius); ++k) {
+      if ((k == j0 || k == j0 + 1) && k != jt) continue;
+      hvdg::DrizzlePair d{k, jt, -1, 0};
+      if (k != jt) {
+        d.me = (int)mp.size();
+        mp.push_back(hvdg::MePair{k, jt});
+      }
+      dp.push_back(d);
+    }
+  const int P = (int)mp.size();
+  const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
+  const int dpitch = pitch / 4;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const int ct = std::max(4, tile / 4);
+  const int cth = (h / 4 + ct - 1) / ct, ctw = (w / 4 + ct - 1) / ct;
+  const size_t plane = (size_t)h * pitch;
+  const int HF = 2 * h * scale;
+  const size_t fine = (size_t)HF * w;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes, 256);
+    return r;
+  };
+  const size_t o_f = take(sizeof(hvdg::MeField) * n);
+  const size_t o_p = take(sizeof(hvdg::MePair) * std::max(P, 1));
+  const size_t o_dp = take(sizeof(hvdg::DrizzlePair) * dp.size());
+  const size_t o_par = take(sizeof(int) * n);
+  const size_t o_l = take(sizeof(float) * n * plane);
+  const size_t o_c = take(sizeof(float2) * n * plane);
+  const size_t o_t = take(sizeof(float) * n * plane);
+  const size_t o_b = take(sizeof(float) * n * plane);
+  const size_t o_d = take(sizeof(float) * n * (size_t)(h / 4 + 1) * dpitch);
+  const size_t nct = (size_t)std::max(1, cth * ctw), nt = (size_t)th * tw;
+  const size_t o_cdy = take(sizeof(float) * nct * std::max(P, 1));
+  const size_t o_cdx = take(sizeof(float) * nct * std::max(P, 1));
+  size_t ot[10];
+  for (int i = 0; i < 10; ++i) ot[i] = take(sizeof(float) * nt * std::max(P, 1));
+  const size_t o_acc = take(sizeof(float) * 4 * fine);
+  const size_t o_oy = take(sizeof(float) * fine);
+  const size_t o_oc = take(sizeof(float2) * fine);
+  hvdg_status st = ctx->arena.reserve(o, ctx->stream);
+  if (st != HVDG_OK) return st;
+  ctx->epoch += 1;
+  cudaGetLastError();
+  char* base = static_cast<char*>(ctx->arena.base);
+  std::vector<hvdg::MeField> mf(n);
+  for (int i = 0; i < n; ++i) {
+    mf[i].h = h;
+    mf[i].w = w;
+    mf[i].pitch = pitch;
+    mf[i].dpitch = dpitch;
+    mf[i].y_off = mf[i].t_off = mf[i].b_off = (int64_t)i * plane;
+    mf[i].d_off = (int64_t)i * (h / 4 + 1) * dpitch;
+  }
+  std::vector<int> par(parities, parities + n);
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(base + o_f, mf.data(), sizeof(hvdg::MeField) * n,
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && P > 0)
+    e = cudaMemcpyAsync(base + o_p, mp.data(), sizeof(hvdg::MePair) * P, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + o_dp, dp.data(), sizeof(hvdg::DrizzlePair) * dp.size(),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + o_par, par.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    e = cudaMemcpy2DAsync(base + o_l + sizeof(float) * plane * i, sizeof(float) * pitch, luma[i],
+                          sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(base + o_c + sizeof(float2) * plane * i, sizeof(float2) * pitch,
+                            chroma[i], sizeof(float2) * w, sizeof(float2) * w, h,
+                            cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + o_acc, 0, sizeof(float) * 4 * fine, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D drizzle inputs");
+  hvdg::MeArgs a;
+  a.tile = tile;
+  a.search = search;
+  a.coarse_off = (int)nct;
+  a.tiles_off = (int)nt;
+  hvdg::MeBuffers mb;
+  mb.luma = reinterpret_cast<const float*>(base + o_l);
+  mb.tmp = reinterpret_cast<float*>(base + o_t);
+  mb.blur = reinterpret_cast<float*>(base + o_b);
+  mb.dec = reinterpret_cast<float*>(base + o_d);
+  mb.cdy = reinterpret_cast<float*>(base + o_cdy);
+  mb.cdx = reinterpret_cast<float*>(base + o_cdx);
+  mb.mdy = reinterpret_cast<float*>(base + ot[0]);
+  mb.mdx = reinterpret_cast<float*>(base + ot[1]);
+  mb.sdy = reinterpret_cast<float*>(base + ot[2]);
+  mb.sdx = reinterpret_cast<float*>(base + ot[3]);
+  mb.best = reinterpret_cast<float*>(base + ot[4]);
+  mb.dy = reinterpret_cast<float*>(base + ot[5]);
+  mb.dx = reinterpret_cast<float*>(base + ot[6]);
+  mb.conf = reinterpret_cast<float*>(base + ot[7]);
+  const hvdg::MeField* d_f = reinterpret_cast<const hvdg::MeField*>(base + o_f);
+  const hvdg::MePair* d_p = reinterpret_cast<const hvdg::MePair*>(base + o_p);
+  float* snap_dy = reinterpret_cast<float*>(base + ot[8]);
+  float* snap_dx = reinterpret_cast<float*>(base + ot[9]);
+  if (P > 0) {
+    hvdg::launch_motion(d_f, n, h, w, d_p, P, a, mb, s);
+    hvdg::launch_vec_snap(d_f, d_p, P, h, w, a, mb.dy, mb.dx, snap_dy, snap_dx, s);
+  }
+  hvdg::DrizzleArgs da;
+  da.Y = mb.luma;
+  da.C = reinterpret_cast<const float2*>(base + o_c);
+  da.parity = reinterpret_cast<const int*>(base + o_par);
+  da.h = h;
+  da.w = w;
+  da.pitch = pitch;
+  da.tile = tile;
+  da.sdy = snap_dy;
+  da.sdx = snap_dx;
+  da.conf = mb.conf;
+  da.tiles_off = (int)nt;
+  da.eps_b = cfg->nr_eps > 0.0f ? cfg->nr_eps : 3.0f;
+  da.scale = scale;
+  da.j0 = j0;
+  da.acc = reinterpret_cast<float*>(base + o_acc);
+  da.out_y = reinterpret_cast<float*>(base + o_oy);
+  da.out_c = reinterpret_cast<float2*>(base + o_oc);
+  hvdg::launch_drizzle(reinterpret_cast<const hvdg::DrizzlePair*>(base + o_dp), (int)dp.size(), da,
+                       s);
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out_luma, da.out_y, sizeof(float) * fine, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out_chroma, da.out_c, sizeof(float2) * fine, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "drizzle");
   return HVDG_OK;
 }
 

@@ -1159,4 +1159,124 @@ void launch_coherence_gate(const MeField* d_fields, const MePair* d_pairs, int n
   k_coh_apply<<<grid, 128, 0, st>>>(d_fields, d_pairs, npairs, b, gate);
 }
 
+// ---------------------------------------------------------------------------
+// DrizzleFrame (sequence.cpp:283-421). Compiled with the rest of this file
+// without multiply-add contraction, so every deposit position, weight and
+// blend is the reference's float arithmetic; only the order of the float
+// accumulations differs (atomics), i.e. the sums agree to rounding.
+// ---------------------------------------------------------------------------
+
+// One thread per (pair, source sample): robust agreement weight with the
+// target's own decode at the rounded warp, linear split between the two
+// fine rows around (2 (y + vy) + p_k) scale.
+__global__ void k_drizzle_deposit(const DrizzlePair* __restrict__ pairs, int npairs, DrizzleArgs a) {
+  const int pi = blockIdx.z;
+  if (pi >= npairs) return;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= a.w || y >= a.h) return;
+  const DrizzlePair pr = pairs[pi];
+  const int L = a.h, W = a.w, HF = 2 * L * a.scale;
+  float vy = 0.0f, vx = 0.0f, cpx = 1.0f;
+  if (pr.me >= 0) {
+    const int th = (L + a.tile - 1) / a.tile, tw = (W + a.tile - 1) / a.tile;
+    int iy, ix;
+    float fy, fx;
+    bracket(y, th, a.tile, &iy, &fy);
+    bracket(x, tw, a.tile, &ix, &fx);
+    const int iy1 = min(iy + 1, th - 1), ix1 = min(ix + 1, tw - 1);
+    const int o = a.tiles_off * pr.me;
+    vy = interp_tiles(a.sdy + o, tw, iy, iy1, ix, ix1, fy, fx);
+    vx = interp_tiles(a.sdx + o, tw, iy, iy1, ix, ix1, fy, fx);
+    cpx = a.conf[o + min(y / a.tile, th - 1) * tw + min(x / a.tile, tw - 1)];
+  }
+  const int64_t plane = (int64_t)L * a.pitch;
+  const float* Yk = a.Y + plane * pr.src;
+  const float* Yt = a.Y + plane * pr.tgt;
+  const float2* Ck = a.C + plane * pr.src;
+  const float2* Ct = a.C + plane * pr.tgt;
+  const int syi = clampi((int)lroundf((float)y - vy), 0, L - 1);
+  const int sxi = clampi((int)lroundf((float)x - vx), 0, W - 1);
+  const float sk = Yk[(int64_t)y * a.pitch + x];
+  const float2 ck = Ck[(int64_t)y * a.pitch + x];
+  const float dY = sk - Yt[(int64_t)syi * a.pitch + sxi];
+  const float2 ct = Ct[(int64_t)syi * a.pitch + sxi];
+  const float dr = ck.x - ct.x, di = ck.y - ct.y;
+  const float d2 = dY * dY + (dr * dr + di * di);
+  const float wgt = cpx * a.eps_b * a.eps_b / (d2 + a.eps_b * a.eps_b);
+  const float yf = (2.0f * ((float)y + vy) + (float)a.parity[pr.src]) * (float)a.scale;
+  const int xs = clampi((int)lroundf((float)x + vx), 0, W - 1);
+  const int y0 = (int)floorf(yf);
+  const float fyr = yf - (float)y0;
+  const int64_t fp = (int64_t)HF * W;
+  for (int off = 0; off < 2; ++off) {
+    const int yt = clampi(y0 + off, 0, HF - 1);
+    const float ww = wgt * (off == 0 ? (1.0f - fyr) : fyr);
+    const int64_t q = (int64_t)yt * W + xs;
+    atomicAdd(a.acc + q, ww * sk);
+    atomicAdd(a.acc + fp + q, ww * ck.x);
+    atomicAdd(a.acc + 2 * fp + q, ww * ck.y);
+    atomicAdd(a.acc + 3 * fp + q, ww);
+  }
+}
+
+// Coverage blend with the linearly interpolated plain weave of fields j0,
+// j0 + 1 (sequence.cpp:385-419). One thread per fine sample.
+__global__ void k_drizzle_resolve(DrizzleArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  const int L = a.h, W = a.w, HF = 2 * L * a.scale;
+  if (x >= W || r >= HF) return;
+  const int64_t plane = (int64_t)L * a.pitch;
+  const int p0 = a.parity[a.j0], p1 = a.parity[a.j0 + 1];
+  auto woven = [&](int row, float2* c) {
+    // row 2 t + p1 from field j0 + 1 (written last), else 2 t + p0 from j0, else 0
+    const int t = row >> 1, par = row & 1;
+    const int64_t o = (int64_t)t * a.pitch + x;
+    if (par == p1) {
+      *c = a.C[plane * (a.j0 + 1) + o];
+      return a.Y[plane * (a.j0 + 1) + o];
+    }
+    if (par == p0) {
+      *c = a.C[plane * a.j0 + o];
+      return a.Y[plane * a.j0 + o];
+    }
+    *c = make_float2(0.f, 0.f);
+    return 0.0f;
+  };
+  const float fine = (float)r / (float)a.scale;
+  const int f0 = clampi((int)floorf(fine), 0, 2 * L - 2);
+  const float ff = fine - (float)f0;
+  float2 c0, c1;
+  const float y0v = woven(f0, &c0), y1v = woven(f0 + 1, &c1);
+  const float baseY = y0v * (1.0f - ff) + y1v * ff;
+  const float bcr = c0.x * (1.0f - ff) + c1.x * ff;
+  const float bci = c0.y * (1.0f - ff) + c1.y * ff;
+  const int64_t fp = (int64_t)HF * W, q = (int64_t)r * W + x;
+  const float aw = a.acc[3 * fp + q];
+  const float mix = aw / (aw + 0.35f);
+  const float den = fmaxf(aw, 1e-9f);
+  const float dzY = aw > 0.0f ? a.acc[q] / den : 0.0f;
+  const float dcr = aw > 0.0f ? a.acc[fp + q] / den : 0.0f;
+  const float dci = aw > 0.0f ? a.acc[2 * fp + q] / den : 0.0f;
+  a.out_y[q] = mix * dzY + (1.0f - mix) * baseY;
+  a.out_c[q] = make_float2(mix * dcr + (1.0f - mix) * bcr, mix * dci + (1.0f - mix) * bci);
+}
+
+void launch_drizzle(const DrizzlePair* d_pairs, int npairs, const DrizzleArgs& a, cudaStream_t st) {
+  const int HF = 2 * a.h * a.scale;
+  if (npairs > 0)
+    k_drizzle_deposit<<<dim3((a.w + 127) / 128, a.h, npairs), 128, 0, st>>>(d_pairs, npairs, a);
+  k_drizzle_resolve<<<dim3((a.w + 127) / 128, HF), 128, 0, st>>>(a);
+}
+
+void launch_vec_snap(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                     int max_w, const MeArgs& a, const float* dy, const float* dx, float* sdy,
+                     float* sdx, cudaStream_t st) {
+  if (npairs <= 0) return;
+  const int nt = ((max_h + a.tile - 1) / a.tile) * ((max_w + a.tile - 1) / a.tile);
+  k_vec_snap<<<dim3((nt + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, a, dy, dx,
+                                                          sdy, sdx);
+}
+
 }  // namespace hvdg

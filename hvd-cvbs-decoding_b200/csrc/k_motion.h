@@ -128,4 +128,34 @@ void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, 
                     int max_w, const MeArgs& a, const VecBuffers& v, bool fast_conf,
                     cudaStream_t st);
 
+// DrizzleFrame (sequence.cpp:283-421): deposits of every (source k, target
+// jt) pair's samples onto the fine grid of frame j0, then the coverage
+// blend with the plain woven decode.
+struct DrizzlePair {
+  int src, tgt;        // field indices (luma / chroma planes, parities)
+  int me;              // motion pair index (tiles at me * tiles_off), -1 = self (zero motion, conf 1)
+  int pad0;
+};
+struct DrizzleArgs {
+  const float* Y;      // n luma planes, pitched (pitch, plane = h * pitch)
+  const float2* C;     // n chroma planes, same layout
+  const int* parity;   // n
+  int h, w, pitch;
+  int tile;
+  const float* sdy;    // snapped tile vectors per motion pair
+  const float* sdx;
+  const float* conf;   // tile confidences per motion pair
+  int tiles_off;
+  float eps_b;
+  int scale, j0;
+  float* acc;          // 4 planes (Y, Re C, Im C, weight) of (2 h scale) x w
+  float* out_y;        // (2 h scale) x w
+  float2* out_c;
+};
+void launch_drizzle(const DrizzlePair* d_pairs, int npairs, const DrizzleArgs& a, cudaStream_t st);
+// the snap of launch_vectors alone (sdy / sdx from dy / dx)
+void launch_vec_snap(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,
+                     int max_w, const MeArgs& a, const float* dy, const float* dx, float* sdy,
+                     float* sdx, cudaStream_t st);
+
 }  // namespace hvdg

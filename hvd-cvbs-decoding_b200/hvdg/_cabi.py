@@ -336,6 +336,15 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_decode_frame_sequence_window.argtypes = [
         vp, P(vp), C.c_int, C.c_int, C.c_int, P(FrameParams), P(Config), P(YcFrame), P(Diag)]
     lib.hvdg_decode_frame_sequence_window.restype = C.c_int
+    lib.hvdg_decode_frame_sequence_window_at.argtypes = [
+        vp, P(vp), C.c_int, C.c_int, C.c_int, C.c_int64, P(FrameParams), P(Config), P(YcFrame),
+        P(Diag)]
+    lib.hvdg_decode_frame_sequence_window_at.restype = C.c_int
+    lib.hvdg_set_debug_dir.argtypes = [vp, C.c_char_p]
+    lib.hvdg_set_debug_dir.restype = C.c_int
+    lib.hvdg_drizzle_frame.argtypes = [vp, P(vp), P(vp), vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       P(Config), C.c_int, vp, vp]
+    lib.hvdg_drizzle_frame.restype = C.c_int
     lib.hvdg_ambiguous_boxes.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float, vp, C.c_int,
                                          P(C.c_int)]
     lib.hvdg_ambiguous_boxes.restype = C.c_int

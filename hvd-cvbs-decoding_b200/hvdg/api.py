@@ -332,7 +332,7 @@ def frame_buffer_size(fp: _cabi.FrameParams) -> int:
     return fp.frame_width * fp.frame_height + fp.extra_sample_line_count
 
 
-def _decode_frames(self, frames, core_begin, core_end, fp, cfg):
+def _decode_frames(self, frames, core_begin, core_end, fp, cfg, base_frame_id=0):
     """hvd::DecodeFrameSequenceWindow: frames are flat int16 field-sequential
     buffers; returns one dict(luma, chroma, u, v) per core frame."""
     n = len(frames)
@@ -349,14 +349,24 @@ def _decode_frames(self, frames, core_begin, core_end, fp, cfg):
         outs[t].u_plane = r["u"].ctypes.data
         outs[t].v_plane = r["v"].ctypes.data
     self.last_diag = Diag()
-    st = self.lib.hvdg_decode_frame_sequence_window(self._h, ptrs, n, core_begin, core_end,
-                                                    C.byref(fp), C.byref(cfg), outs,
-                                                    C.byref(self.last_diag))
+    st = self.lib.hvdg_decode_frame_sequence_window_at(self._h, ptrs, n, core_begin, core_end,
+                                                       int(base_frame_id), C.byref(fp),
+                                                       C.byref(cfg), outs, C.byref(self.last_diag))
     self._check(st, "hvdg_decode_frame_sequence_window")
     return res
 
 
 Context.decode_frame_sequence_window = _decode_frames
+
+
+def _set_debug_dir(self, path):
+    """HvdConfig::debug_dir: diagnostic maps of the sequence frame bridge
+    (None = off)."""
+    self._check(self.lib.hvdg_set_debug_dir(self._h, None if path is None else str(path).encode()),
+                "hvdg_set_debug_dir")
+
+
+Context.set_debug_dir = _set_debug_dir
 
 
 def _yc_frames(fp, m, out=None):
@@ -438,6 +448,23 @@ def _decode_yc_frame_buffers(self, lumas, chromas, fp, cfg, out=None):
     return res
 
 
+def _drizzle_frame(self, j0, lumas, chromas, parities, cfg, scale=2):
+    """DrizzleFrame: the frame of fields j0, j0 + 1 on a (2 h scale)-row
+    grid from the motion-compensated deposits of the fields around it."""
+    ys = [np.ascontiguousarray(y, dtype=np.float32) for y in lumas]
+    cs = [np.ascontiguousarray(c, dtype=np.complex64) for c in chromas]
+    n = len(ys)
+    h, w = ys[0].shape
+    par = np.ascontiguousarray(parities, dtype=np.int32)
+    oy = np.zeros((2 * h * scale, w), np.float32)
+    oc = np.zeros((2 * h * scale, w), np.complex64)
+    st = self.lib.hvdg_drizzle_frame(self._h, _ptrs(ys), _ptrs(cs), par.ctypes.data, n, j0, h, w,
+                                     C.byref(cfg), scale, oy.ctypes.data, oc.ctypes.data)
+    self._check(st, "hvdg_drizzle_frame")
+    return oy, oc
+
+
+Context.drizzle_frame = _drizzle_frame
 Context.decode_frame_buffer = _decode_frame_buffer
 Context.decode_frame_buffers = _decode_frame_buffers
 Context.decode_yc_frame_buffer = _decode_yc_frame_buffer

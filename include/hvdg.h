@@ -265,6 +265,17 @@ hvdg_status hvdg_decode_frame_sequence_window(
     hvdg_ctx* ctx, const int16_t* const* frames, int n_frames, int core_begin,
     int core_end, const hvdg_frame_params* fp, const hvdg_config* cfg,
     hvdg_yc_frame* out, hvdg_diag* diag);
+/* The same with the reference's base_frame_id (frame_bridge.h:196-199),
+ * which only numbers the diagnostic maps. */
+hvdg_status hvdg_decode_frame_sequence_window_at(
+    hvdg_ctx* ctx, const int16_t* const* frames, int n_frames, int core_begin,
+    int core_end, int64_t base_frame_id, const hvdg_frame_params* fp,
+    const hvdg_config* cfg, hvdg_yc_frame* out, hvdg_diag* diag);
+/* HvdConfig::debug_dir (hvd_config.h:314): when non-empty (NULL or "" = off),
+ * the sequence frame bridge appends its decision log to <dir>/diag.txt and
+ * writes one rainbow_<frame id>.pgm map per core frame
+ * (frame_bridge.cpp:807-865). Host-side file output; the decode is unchanged. */
+hvdg_status hvdg_set_debug_dir(hvdg_ctx* ctx, const char* dir);
 
 /* hvd::DecodeFrameBuffer (frame_bridge.h:149-150, frame_bridge.cpp:161-255) via HvdEngine::DecodeFrame
  * (engine.cpp:141-195): the 2-D frame-weave decode of one field-sequential
@@ -305,6 +316,19 @@ hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* lu
 /* ------------------------------------------------------------------------ */
 /* Kernel level (host buffers)                                               */
 /* ------------------------------------------------------------------------ */
+
+/* DrizzleFrame (sequence.h:123-130, sequence.cpp:283-421): the decoded
+ * fields luma[i] (h x w, IRE) / chroma[i] (h x w x 2) with their parities,
+ * motion-compensated and deposited onto the fine grid of the frame of fields
+ * j0, j0 + 1 ((2 h scale) x w), blended by coverage with the plain weave.
+ * Motion: the reference's float EstimateMotion (cfg->mc_tile,
+ * cfg->mc_search); robust scale cfg->nr_eps (0: 3 IRE); sources within
+ * 2 cfg->nr_radius fields. The deposits are float atomics: sums agree with
+ * the reference to rounding, not bit for bit. */
+hvdg_status hvdg_drizzle_frame(hvdg_ctx* ctx, const float* const* luma, const float* const* chroma,
+                               const int32_t* parities, int n, int j0, int h, int w,
+                               const hvdg_config* cfg, int scale, float* out_luma,
+                               float* out_chroma);
 
 /* AmbiguousBoxes (frame_bridge.cpp:402-580, the selective 3-D detector) on
  * one decoded field (luma h x w, chroma h x w x 2), host only. Writes up to

@@ -1038,6 +1038,68 @@ def detect_field_parity(b1, b2, fp, g) -> int:
     return 1 if ep < em else -1
 
 
+def drizzle_frame(j0, Ys, chis, parities, cfg, scale=2):
+    """DrizzleFrame (sequence.cpp:283-421) in FP64: each target field of the
+    frame (j0, j0 + 1) collects the motion-compensated samples of the fields
+    within 2 nr_radius (itself with zero motion and confidence 1), weighted
+    by confidence x eps_b^2 / (d^2 + eps_b^2) against its own decode at the
+    rounded warp and split linearly between the two fine rows around
+    (2 (y + vy) + p_k) scale; coverage-blended with the interpolated weave."""
+    L, W = np.asarray(Ys[j0]).shape
+    HF = 2 * L * scale
+    n = len(Ys)
+    tile, search, r = cfg.mc_tile, cfg.mc_search, cfg.nr_radius
+    eps_b = cfg.nr_eps if cfg.nr_eps > 0 else 3.0
+    acc = np.zeros((4, HF, W))
+    yy, xx = np.mgrid[0:L, 0:W].astype(np.float64)
+    Ys = [np.asarray(y, np.float64) for y in Ys]
+    chis = [np.asarray(c, np.complex128) for c in chis]
+    for jt in (j0, j0 + 1):
+        for k in range(max(0, j0 - 2 * r), min(n, j0 + 2 + 2 * r)):
+            if k in (j0, j0 + 1) and k != jt:
+                continue
+            if k == jt:
+                vy = np.zeros((L, W))
+                vx = np.zeros((L, W))
+                cpx = np.ones((L, W))
+            else:
+                mdy, mdx, conf = estimate_motion(Ys[k], Ys[jt], tile, search)
+                vy, vx = vectors_per_pixel(mdy, mdx, tile, L, W)
+                th, tw = conf.shape
+                cpx = conf[np.minimum(yy.astype(int) // tile, th - 1),
+                           np.minimum(xx.astype(int) // tile, tw - 1)]
+            syi = np.clip(_lround(yy - vy), 0, L - 1).astype(int)
+            sxi = np.clip(_lround(xx - vx), 0, W - 1).astype(int)
+            dY = Ys[k] - Ys[jt][syi, sxi]
+            d2 = dY * dY + np.abs(chis[k] - chis[jt][syi, sxi]) ** 2
+            wgt = cpx * eps_b * eps_b / (d2 + eps_b * eps_b)
+            yf = (2.0 * (yy + vy) + parities[k]) * scale
+            xs = np.clip(_lround(xx + vx), 0, W - 1).astype(int)
+            y0 = np.floor(yf).astype(int)
+            fy = yf - y0
+            for off in (0, 1):
+                yt = np.clip(y0 + off, 0, HF - 1)
+                ww = wgt * ((1.0 - fy) if off == 0 else fy)
+                for i, v in enumerate((ww * Ys[k], ww * chis[k].real, ww * chis[k].imag, ww)):
+                    np.add.at(acc[i], (yt.ravel(), xs.ravel()), v.ravel())
+    p0, p1 = parities[j0], parities[j0 + 1]
+    wy = np.zeros((2 * L, W))
+    wc = np.zeros((2 * L, W), np.complex128)
+    wy[p0::2], wc[p0::2] = Ys[j0], chis[j0]
+    wy[p1::2], wc[p1::2] = Ys[j0 + 1], chis[j0 + 1]
+    fine = np.arange(HF) / scale
+    f0 = np.clip(np.floor(fine).astype(int), 0, 2 * L - 2)
+    ff = (fine - f0)[:, None]
+    base_y = wy[f0] * (1 - ff) + wy[f0 + 1] * ff
+    base_c = wc[f0] * (1 - ff) + wc[f0 + 1] * ff
+    aw = acc[3]
+    mix = aw / (aw + 0.35)
+    den = np.maximum(aw, 1e-9)
+    dz_y = np.where(aw > 0, acc[0] / den, 0.0)
+    dz_c = np.where(aw > 0, (acc[1] + 1j * acc[2]) / den, 0.0)
+    return mix * dz_y + (1 - mix) * base_y, mix * dz_c + (1 - mix) * base_c
+
+
 def ambiguous_boxes(Y, chi, max_area=0.45):
     """AmbiguousBoxes (frame_bridge.cpp:402-580) in float32 / float64 as the
     reference: [] = stay 2-D, None = full 3-D, else [(fy0, fy1, x0, x1)]."""

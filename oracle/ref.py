@@ -66,6 +66,11 @@ def _declare(L):
                                                       P(_cabi.FrameParams), P(_cabi.Config),
                                                       P(vp), P(vp), P(vp), P(vp)]
     L.hvdref_split_frame_fields.argtypes = [vp, P(_cabi.FrameParams), vp, vp]
+    L.hvdref_decode_frame_sequence_window_debug.argtypes = [
+        P(vp), C.c_int, C.c_int, C.c_int, P(_cabi.FrameParams), P(_cabi.Config), C.c_char_p,
+        C.c_int64, P(vp), P(vp), P(vp), P(vp)]
+    L.hvdref_drizzle_frame.argtypes = [P(vp), P(vp), vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       P(_cabi.Config), C.c_int, vp, vp]
     L.hvdref_decode_frame_buffer.argtypes = [vp, P(_cabi.FrameParams), P(_cabi.Config), vp, vp,
                                              vp, vp]
     L.hvdref_decode_yc_frame_buffer.argtypes = [vp, vp, P(_cabi.FrameParams), P(_cabi.Config),
@@ -235,6 +240,21 @@ def decode_frame_sequence_window(frames, core_begin, core_end, fp, cfg):
     return [dict(luma=L[t], chroma=Cc[t], u=U[t], v=Vv[t]) for t in range(got)]
 
 
+def drizzle_frame(j0, Ys, chis, parities, cfg, scale=2):
+    """hvd::DrizzleFrame: (luma, chroma) of (2 h scale) x w."""
+    ys = [_f32(y) for y in Ys]
+    cs = [_c64(c) for c in chis]
+    n = len(ys)
+    h, w = ys[0].shape
+    par = np.ascontiguousarray(parities, dtype=np.int32)
+    oy = np.zeros((2 * h * scale, w), np.float32)
+    oc = np.zeros((2 * h * scale, w), np.complex64)
+    V = C.c_void_p * n
+    lib().hvdref_drizzle_frame(V(*[_p(y).value for y in ys]), V(*[_p(c).value for c in cs]),
+                               _p(par), n, j0, h, w, C.byref(cfg), scale, _p(oy), _p(oc))
+    return oy, oc
+
+
 def _yc_out(fp):
     sz = fp.frame_width * fp.frame_height
     return (np.zeros(sz, np.int16), np.zeros(sz, np.int16), np.zeros(sz, np.float64),
@@ -258,6 +278,22 @@ def decode_yc_frame_buffer(luma, chroma, fp, cfg):
     lib().hvdref_decode_yc_frame_buffer(_p(y), _p(c), C.byref(fp), C.byref(cfg), _p(L), _p(Cc),
                                         _p(U), _p(Vv))
     return dict(luma=L, chroma=Cc, u=U, v=Vv)
+
+
+def decode_frame_sequence_window_debug(frames, core_begin, core_end, fp, cfg, debug_dir,
+                                       base_frame_id=0):
+    """DecodeFrameSequenceWindow with HvdConfig::debug_dir set: the
+    diagnostic maps land in debug_dir."""
+    fr = [np.ascontiguousarray(f, dtype=np.int16) for f in frames]
+    m = max(core_end - core_begin, 0)
+    outs = [_yc_out(fp) for _ in range(m)]
+    Vp = C.c_void_p
+    arr = lambda lst: (Vp * max(len(lst), 1))(*[_p(a).value for a in lst])
+    got = lib().hvdref_decode_frame_sequence_window_debug(
+        arr(fr), len(fr), core_begin, core_end, C.byref(fp), C.byref(cfg),
+        str(debug_dir).encode(), int(base_frame_id), arr([o[0] for o in outs]),
+        arr([o[1] for o in outs]), arr([o[2] for o in outs]), arr([o[3] for o in outs]))
+    return [dict(luma=o[0], chroma=o[1], u=o[2], v=o[3]) for o in outs[:got]]
 
 
 def split_frame_fields(frame, fp):

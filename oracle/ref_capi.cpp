@@ -388,6 +388,41 @@ void hvdref_decode_yc_frame_buffer(const int16_t* luma_in, const int16_t* chroma
          chroma, u, v);
 }
 
+// DrizzleFrame (sequence.cpp:283): fields luma (h x w) / chroma (h x w x 2);
+// outputs (2 h scale) x w.
+void hvdref_drizzle_frame(const float* const* luma, const float* const* chroma,
+                          const int* parities, int n, int j0, int h, int w,
+                          const hvdg_config* cfg, int scale, float* out_luma, float* out_chroma) {
+  std::vector<hvd::Plane> Ys;
+  std::vector<hvd::ComplexPlane> Cs;
+  for (int i = 0; i < n; ++i) {
+    Ys.push_back(PlaneFrom(luma[i], h, w));
+    Cs.push_back(CPlaneFrom(chroma[i], h, w));
+  }
+  const std::vector<int> par(parities, parities + n);
+  const hvd::DrizzleResult r = hvd::DrizzleFrame(j0, Ys, Cs, par, ToCfg(*cfg), scale);
+  PlaneTo(r.luma, out_luma);
+  CPlaneTo(r.chroma, out_chroma);
+}
+
+// The same with HvdConfig::debug_dir and base_frame_id set (the diagnostic
+// maps, frame_bridge.cpp:807-865).
+int hvdref_decode_frame_sequence_window_debug(const int16_t* const* frames, int nframes,
+                                              int core_begin, int core_end,
+                                              const hvdg_frame_params* fp, const hvdg_config* cfg,
+                                              const char* debug_dir, int64_t base_frame_id,
+                                              int16_t* const* luma, int16_t* const* chroma,
+                                              double* const* u, double* const* v) {
+  const std::vector<const int16_t*> fr(frames, frames + nframes);
+  hvd::HvdEngine engine;
+  hvd::HvdConfig c = ToCfg(*cfg);
+  c.debug_dir = debug_dir ? debug_dir : "";
+  const std::vector<hvd::YcFrameS16> out = hvd::DecodeFrameSequenceWindow(
+      fr, core_begin, core_end, ToFp(*fp), c, engine, base_frame_id);
+  for (size_t t = 0; t < out.size(); ++t) CopyYc(out[t], luma[t], chroma[t], u[t], v[t]);
+  return static_cast<int>(out.size());
+}
+
 // SplitFrameFields (frame_bridge.cpp:61): block-1 / block-2 fields in IRE.
 void hvdref_split_frame_fields(const int16_t* frame, const hvdg_frame_params* fp,
                                float* top, float* bottom) {

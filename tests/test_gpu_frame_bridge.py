@@ -98,3 +98,42 @@ def test_selective_3d_window_vs_reference(ctx, std, n_rects):
     # the boxes are strictly inside the active picture, not the whole of it
     assert cols.min() > a0 and cols.max() < a1 - 1
     assert len(rows) < 0.8 * 2 * g.active_lines
+
+
+def _read_pgm(path):
+    data = path.read_bytes()
+    parts = data.split(b"\n", 3)
+    assert parts[0] == b"P5" and parts[2] == b"255"
+    w, h = (int(v) for v in parts[1].split())
+    return np.frombuffer(parts[3], np.uint8).reshape(h, w)
+
+
+def test_debug_maps_vs_reference(ctx, tmp_path):
+    """HvdConfig::debug_dir (frame_bridge.cpp:807-865): the decision log line
+    and the woven rainbow maps of the core frames. Map values are truncations
+    of float magnitudes, so a value at an integer boundary can differ by one."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    frames, _ = synth.make_frames(43, _cabi.STD_NTSC, 3, noise_sigma=1.0)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6,
+                             temporal_strength=-1.0)
+    mine, theirs = tmp_path / "gpu", tmp_path / "ref"
+    mine.mkdir()
+    theirs.mkdir()
+    ctx.set_debug_dir(mine)
+    try:
+        ctx.decode_frame_sequence_window(frames, 1, 3, fp, cfg, base_frame_id=100)
+    finally:
+        ctx.set_debug_dir(None)
+    ref.decode_frame_sequence_window_debug(frames, 1, 3, fp, cfg, theirs, base_frame_id=100)
+    for t in (101, 102):
+        a = _read_pgm(mine / f"rainbow_{t:06d}.pgm").astype(int)
+        b = _read_pgm(theirs / f"rainbow_{t:06d}.pgm").astype(int)
+        d = np.abs(a - b)
+        print(f"rainbow {t}: max {d.max()} frac>0 {(d > 0).mean():.2e} mean value {b.mean():.2f}")
+        assert a.shape == b.shape and d.max() <= 1 and (d > 0).mean() < 1e-2
+    mine_log = (mine / "diag.txt").read_text().split()
+    ref_log = (theirs / "diag.txt").read_text().split()
+    assert mine_log[:3] == ref_log[:3] == ["frames", "101..102:", "f1_bottom=0"]

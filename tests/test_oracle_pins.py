@@ -334,3 +334,27 @@ def test_oracle_symmetry_variant_matches_reference(tag):
                                       api.default_config(symmetry_variant=1))
     assert np.abs(chi0 - rchi0).max() < 1e-4
     assert np.abs(y0 - ry0).max() < 1e-4
+
+
+def test_oracle_drizzle_matches_reference():
+    """DrizzleFrame (sequence.cpp:283-421): the FP64 restatement against the
+    compiled reference on the reference's own 2-D decodes of a moving NTSC
+    window. Deposit positions are rounding decisions on motion vectors that
+    agree to ~1e-4 px, so a few samples land one row / column apart; the
+    rest agrees to float rounding."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    from hvdg import api, synth
+    g = _cabi.default_geometry(_cabi.STD_NTSC)
+    fs = synth.make_sequence(5, _cabi.STD_NTSC, 8, noise_sigma=0.5, moving=True)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6,
+                             temporal_strength=-1.0)
+    par = [f.parity for f in fs]
+    ys, cs, _ = ref.decode_field_window([synth.to_ire(f.samples) for f in fs], par, g, cfg)
+    ry, rc = ref.drizzle_frame(4, ys, cs, par, cfg, 2)
+    oy, oc = O.drizzle_frame(4, ys, cs, par, cfg, 2)
+    assert ry.shape == (2 * 2 * g.active_lines, g.active_width)
+    d, dc = np.abs(oy - ry), np.abs(oc - rc)
+    assert d.mean() < 1e-4 and dc.mean() < 1e-4
+    assert (d > 1e-3).mean() < 1e-3 and (dc > 1e-3).mean() < 1e-3
