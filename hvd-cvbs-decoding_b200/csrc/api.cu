@@ -313,6 +313,14 @@ struct hvdg_ctx {
   std::map<std::string, std::pair<int, int>> tune;
   // diagnostic maps of the sequence frame bridge (empty: off)
   std::string debug_dir;
+  // asynchronous device-resident decodes: ordering against the caller's
+  // stream, completion, and the result of a call that awaits hvdg_wait
+  cudaEvent_t ev_in = nullptr, ev_done = nullptr;
+  bool pending = false;           // a replay is in flight, hvdg_wait reads its flags
+  bool settled = false;           // pending_status / pending_diag hold a finished call
+  hvdg_status pending_status = HVDG_OK;
+  hvdg_diag pending_diag{};
+  bool pending_want_diag = false;
 };
 
 namespace hvdg {
@@ -742,6 +750,7 @@ struct RunOpts {
   bool tables_only = false;          // stage_upload without the per-call reset
   int band_rows = -1;                // solver band height override (-1: context setting)
   int ctas_per_sm = -1;              // solver CTAs per SM override (-1: context setting)
+  bool async = false;                // graph replay left in flight (hvdg_wait completes it)
   // woven frames: `in` holds two source fields per plane (plan_batch); their
   // F32 IRE samples are written into the arena's raw slots on the device
   const hvdg_geometry* weave_geom = nullptr;
@@ -1126,6 +1135,8 @@ std::string batch_signature(const hvdg_field_in* in, int n, const hvdg_config* c
 // Captured-graph replay of the batched device-resident decode. The tables
 // are uploaded outside the graph; the graph holds the per-call resets, the
 // kernels, the output copies and the flag read-back (into pinned memory).
+hvdg_status graph_result(hvdg_ctx* ctx, hvdg_diag* diag);
+
 hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
                             hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt) {
   std::string sig = batch_signature(in, n, cfg);
@@ -1223,8 +1234,20 @@ hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const
     }
   }
   e = cudaGraphLaunch(ctx->gexec, s);
+  if (opt.async) {
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_done, s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "graph launch");
+    ctx->pending = true;
+    return HVDG_OK;
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "graph launch");
+  return graph_result(ctx, diag);
+}
+
+// Diagnostics and status of the last replay of the cached graph (after it
+// completed): timing marks, CG counts, the device flags.
+hvdg_status graph_result(hvdg_ctx* ctx, hvdg_diag* diag) {
   if (diag) {
     diag->ms_total += elapsed(ctx, 0, 4);
     diag->ms_solver += elapsed(ctx, 2, 3);
@@ -3111,6 +3134,9 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
 // ===========================================================================
 extern "C" {
 
+static void settle(hvdg_ctx* ctx);
+
+
 int hvdg_abi_version(void) { return HVDG_ABI_VERSION; }
 
 const char* hvdg_status_string(hvdg_status s) {
@@ -3223,6 +3249,8 @@ hvdg_status hvdg_create(int device, hvdg_ctx** out) {
     return HVDG_ERR_CUDA;
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  cudaEventCreateWithFlags(&ctx->ev_in, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->ev_done, cudaEventDisableTiming);
   if (cudaMallocHost(&ctx->flags_host, sizeof(int) * 4) != cudaSuccess) {
     cudaGetLastError();
     ctx->flags_host = nullptr;
@@ -3242,6 +3270,8 @@ void hvdg_destroy(hvdg_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+  if (ctx->ev_in) cudaEventDestroy(ctx->ev_in);
+  if (ctx->ev_done) cudaEventDestroy(ctx->ev_done);
   if (ctx->flags_host) cudaFreeHost(ctx->flags_host);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
   cudaStreamDestroy(ctx->stream);
@@ -3253,22 +3283,38 @@ const char* hvdg_last_error(const hvdg_ctx* ctx) {
 }
 
 hvdg_status hvdg_set_batching(hvdg_ctx* ctx, int batched) {
+  settle(ctx);
   if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
   ctx->batched = batched ? 1 : 0;
   return HVDG_OK;
 }
 
 hvdg_status hvdg_set_tuning(hvdg_ctx* ctx, int band_rows, int ctas_per_sm) {
+  settle(ctx);
   if (!ctx || band_rows < 0 || ctas_per_sm < 0) return HVDG_ERR_BAD_ARGUMENT;
   ctx->band_rows = band_rows;
   ctx->ctas_per_sm = ctas_per_sm;
   return HVDG_OK;
 }
 
+// Complete an asynchronous call still in flight on the context (every entry
+// point that uses the context stream or the arena does this first); its
+// status and diagnostics wait for hvdg_wait.
+static void settle(hvdg_ctx* ctx) {
+  if (!ctx || !ctx->pending) return;
+  ctx->pending = false;
+  std::memset(&ctx->pending_diag, 0, sizeof(ctx->pending_diag));
+  const cudaError_t e = cudaEventSynchronize(ctx->ev_done);
+  ctx->pending_status = e != cudaSuccess ? hvdg::cuda_fail(ctx, e, "asynchronous decode")
+                                         : graph_result(ctx, &ctx->pending_diag);
+  ctx->settled = true;
+}
+
 static hvdg_status decode_fields_impl(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
                                       const hvdg_config* cfg, hvdg_field_out* out,
-                                      hvdg_diag* diag, bool device_io) {
+                                      hvdg_diag* diag, bool device_io, bool async = false) {
   if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  settle(ctx);
   hvdg_status st = validate_fields(fields, n, cfg, out);
   if (st != HVDG_OK) return st;
   if (n == 0) return HVDG_OK;
@@ -3276,6 +3322,7 @@ static hvdg_status decode_fields_impl(hvdg_ctx* ctx, const hvdg_field_in* fields
   if (diag) std::memset(diag, 0, sizeof(*diag));
   RunOpts opt;
   opt.device_io = device_io;
+  opt.async = async;
   if (ctx->batched) return run_batch(ctx, fields, n, cfg, out, diag, opt);
   for (int i = 0; i < n; ++i) {
     st = run_batch(ctx, fields + i, 1, cfg, out + i, diag, opt);
@@ -3295,9 +3342,53 @@ hvdg_status hvdg_decode_fields_device(hvdg_ctx* ctx, const hvdg_field_in* fields
   return decode_fields_impl(ctx, fields, n, cfg, out, diag, true);
 }
 
+hvdg_status hvdg_decode_fields_device_async(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
+                                            const hvdg_config* cfg, hvdg_field_out* out,
+                                            void* stream) {
+  if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  settle(ctx);
+  ctx->settled = false;
+  cudaSetDevice(ctx->device);
+  cudaStream_t us = static_cast<cudaStream_t>(stream);
+  if (us) {
+    // the decode reads what the caller's stream wrote before this call
+    cudaError_t e = cudaEventRecord(ctx->ev_in, us);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_in, 0);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "order after the caller's stream");
+  }
+  hvdg_diag d;
+  const hvdg_status st = decode_fields_impl(ctx, fields, n, cfg, out, &d, true, true);
+  if (st != HVDG_OK) return st;
+  if (!ctx->pending) {
+    // completed synchronously (first call of a batch shape, or no graphs)
+    ctx->pending_status = st;
+    ctx->pending_diag = d;
+    ctx->settled = true;
+    return HVDG_OK;
+  }
+  if (us) {
+    const cudaError_t e = cudaStreamWaitEvent(us, ctx->ev_done, 0);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "order the caller's stream after");
+  }
+  return HVDG_OK;
+}
+
+hvdg_status hvdg_wait(hvdg_ctx* ctx, hvdg_diag* diag) {
+  if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  settle(ctx);
+  if (!ctx->settled) {
+    if (diag) std::memset(diag, 0, sizeof(*diag));
+    return HVDG_OK;
+  }
+  ctx->settled = false;
+  if (diag) *diag = ctx->pending_diag;
+  return ctx->pending_status;
+}
+
 hvdg_status hvdg_decode_field_window(hvdg_ctx* ctx, const hvdg_field_in* fields, int n,
                                      const hvdg_config* cfg, hvdg_field_out* out,
                                      hvdg_diag* diag) {
+  settle(ctx);
   if (!ctx || !cfg) return HVDG_ERR_BAD_ARGUMENT;
   hvdg_status st = validate_fields(fields, n, cfg, out);
   if (st != HVDG_OK) return st;
@@ -3309,6 +3400,7 @@ hvdg_status hvdg_decode_field_window(hvdg_ctx* ctx, const hvdg_field_in* fields,
 
 hvdg_status hvdg_burst_lockin(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometry* g,
                               float* theta, int8_t* vswitch) {
+  settle(ctx);
   if (!ctx || !field_ire || !g || !theta) return HVDG_ERR_BAD_ARGUMENT;
   if (uses_vswitch(*g) && !vswitch) return HVDG_ERR_BAD_ARGUMENT;
   return lockin_one(ctx, field_ire, g, theta, vswitch, nullptr);
@@ -3316,6 +3408,7 @@ hvdg_status hvdg_burst_lockin(hvdg_ctx* ctx, const float* field_ire, const hvdg_
 
 hvdg_status hvdg_burst_amplitude(hvdg_ctx* ctx, const float* field_ire, const hvdg_geometry* g,
                                  float* amplitude_ire) {
+  settle(ctx);
   if (!ctx || !field_ire || !g || !amplitude_ire) return HVDG_ERR_BAD_ARGUMENT;
   return lockin_one(ctx, field_ire, g, nullptr, nullptr, amplitude_ire);
 }
@@ -3323,6 +3416,7 @@ hvdg_status hvdg_burst_amplitude(hvdg_ctx* ctx, const float* field_ire, const hv
 hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref, const float* y_cur, int h,
                                  int w, int tile, int search, int me_mode, float* dy, float* dx,
                                  float* confidence) {
+  settle(ctx);
   if (!ctx || !y_ref || !y_cur || !dy || !dx || !confidence || h < 1 || w < 1 || tile < 1 ||
       search < 0 || me_mode < 0 || me_mode > 1)
     return HVDG_ERR_BAD_ARGUMENT;
@@ -3428,6 +3522,7 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
                                                  const hvdg_frame_params* fp,
                                                  const hvdg_config* cfg, hvdg_yc_frame* out,
                                                  hvdg_diag* diag) {
+  settle(ctx);
   if (!ctx || !fp || !cfg) return HVDG_ERR_BAD_ARGUMENT;
   // the reference returns an empty vector for these windows (frame_bridge.cpp:728-731)
   if (n_frames <= 0 || !frames || core_begin < 0 || core_end > n_frames || core_begin >= core_end)
@@ -3596,6 +3691,7 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
 hvdg_status hvdg_decode_frame_buffer(hvdg_ctx* ctx, const int16_t* frame,
                                      const hvdg_frame_params* fp, const hvdg_config* cfg,
                                      hvdg_yc_frame* out) {
+  settle(ctx);
   if (!frame || !out) return HVDG_ERR_BAD_ARGUMENT;
   return decode_woven_frames(ctx, &frame, nullptr, 1, fp, cfg, out, nullptr, false);
 }
@@ -3603,12 +3699,14 @@ hvdg_status hvdg_decode_frame_buffer(hvdg_ctx* ctx, const int16_t* frame,
 hvdg_status hvdg_decode_frame_buffers(hvdg_ctx* ctx, const int16_t* const* frames, int n_frames,
                                       const hvdg_frame_params* fp, const hvdg_config* cfg,
                                       hvdg_yc_frame* out, hvdg_diag* diag) {
+  settle(ctx);
   return decode_woven_frames(ctx, frames, nullptr, n_frames, fp, cfg, out, diag, false);
 }
 
 hvdg_status hvdg_decode_yc_frame_buffer(hvdg_ctx* ctx, const int16_t* luma, const int16_t* chroma,
                                         const hvdg_frame_params* fp, const hvdg_config* cfg,
                                         hvdg_yc_frame* out) {
+  settle(ctx);
   if (!luma || !chroma || !out) return HVDG_ERR_BAD_ARGUMENT;
   return decode_woven_frames(ctx, &chroma, &luma, 1, fp, cfg, out, nullptr, true);
 }
@@ -3617,6 +3715,7 @@ hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* lu
                                          const int16_t* const* chroma, int n_frames,
                                          const hvdg_frame_params* fp, const hvdg_config* cfg,
                                          hvdg_yc_frame* out, hvdg_diag* diag) {
+  settle(ctx);
   return decode_woven_frames(ctx, chroma, luma, n_frames, fp, cfg, out, diag, true);
 }
 
@@ -3644,6 +3743,7 @@ hvdg_status hvdg_drizzle_frame(hvdg_ctx* ctx, const float* const* luma, const fl
                                const int32_t* parities, int n, int j0, int h, int w,
                                const hvdg_config* cfg, int scale, float* out_luma,
                                float* out_chroma) {
+  settle(ctx);
   if (!ctx || !luma || !chroma || !parities || !cfg || !out_luma || !out_chroma || n < 2 ||
       j0 < 0 || j0 + 1 >= n || h < 1 || w < 1 || scale < 1 || cfg->mc_tile < 1 ||
       cfg->mc_search < 0 || cfg->nr_radius < 0)
@@ -3797,6 +3897,7 @@ hvdg_status hvdg_drizzle_frame(hvdg_ctx* ctx, const float* const* luma, const fl
 hvdg_status hvdg_holographic_init(hvdg_ctx* ctx, const float* s, const float* theta_active,
                                   const int8_t* vswitch_active, const hvdg_geometry* g,
                                   const hvdg_config* cfg, float* luma0, float* chi0) {
+  settle(ctx);
   if (!ctx || !s || !theta_active || !g || !cfg || !luma0 || !chi0) return HVDG_ERR_BAD_ARGUMENT;
   hvdg_status st = check_geometry(g);
   if (st != HVDG_OK) return st;
@@ -3826,6 +3927,7 @@ hvdg_status hvdg_variational_refine(hvdg_ctx* ctx, const float* s, const float* 
                                     const int8_t* vswitch_active, const float* chi0,
                                     const hvdg_geometry* g, const hvdg_config* cfg, float* luma,
                                     float* chi) {
+  settle(ctx);
   if (!ctx || !s || !theta_active || !chi0 || !g || !cfg || !luma || !chi)
     return HVDG_ERR_BAD_ARGUMENT;
   hvdg_status st = check_geometry(g);
@@ -3859,6 +3961,7 @@ hvdg_status hvdg_decode_fields_adjoint(hvdg_ctx* ctx, const hvdg_field_in* field
                                        const float* const* chi_bar, float* const* samples_bar,
                                        double* scalar_bar, int adjoint_cg_iterations,
                                        hvdg_field_out* out, hvdg_diag* diag) {
+  settle(ctx);
   if (!ctx || !cfg || n < 0 || (n > 0 && (!fields || !y_bar || !chi_bar || !samples_bar)) ||
       !scalar_bar)
     return HVDG_ERR_BAD_ARGUMENT;

@@ -333,6 +333,11 @@ def _declare(lib: C.CDLL) -> None:
         f = getattr(lib, name)
         f.argtypes = [vp, P(FieldIn), C.c_int, P(Config), P(FieldOut), P(Diag)]
         f.restype = C.c_int
+    lib.hvdg_decode_fields_device_async.argtypes = [vp, P(FieldIn), C.c_int, P(Config),
+                                                    P(FieldOut), vp]
+    lib.hvdg_decode_fields_device_async.restype = C.c_int
+    lib.hvdg_wait.argtypes = [vp, P(Diag)]
+    lib.hvdg_wait.restype = C.c_int
     lib.hvdg_decode_frame_sequence_window.argtypes = [
         vp, P(vp), C.c_int, C.c_int, C.c_int, P(FrameParams), P(Config), P(YcFrame), P(Diag)]
     lib.hvdg_decode_frame_sequence_window.restype = C.c_int

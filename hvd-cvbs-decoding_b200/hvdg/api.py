@@ -184,6 +184,19 @@ class Context:
         self._check(st, "hvdg_decode_fields_device")
         return d
 
+    def decode_fields_device_async(self, fields_in, outs, n, cfg: Config, stream: int = 0):
+        """Asynchronous device-resident decode ordered against `stream` (a raw
+        cudaStream_t, e.g. torch.cuda.Stream().cuda_stream); complete it with
+        wait()."""
+        st = self.lib.hvdg_decode_fields_device_async(self._h, fields_in, int(n), C.byref(cfg),
+                                                      outs, C.c_void_p(stream or None))
+        self._check(st, "hvdg_decode_fields_device_async")
+
+    def wait(self) -> Diag:
+        d = Diag()
+        self._check(self.lib.hvdg_wait(self._h, C.byref(d)), "hvdg_wait")
+        return d
+
     def decode_fields_adjoint(self, fields, cfg: Config, y_bar, chi_bar,
                               adjoint_cg_iterations: int = 0, want_forward: bool = False):
         """Gradients of a scalar loss through the 2-D decode of `fields`

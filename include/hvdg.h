@@ -257,6 +257,21 @@ hvdg_status hvdg_decode_fields_device(hvdg_ctx* ctx, const hvdg_field_in* fields
                                       int n_fields, const hvdg_config* cfg,
                                       hvdg_field_out* out, hvdg_diag* diag);
 
+/* Asynchronous form of hvdg_decode_fields_device: enqueues the decode (the
+ * replay of the cached CUDA graph) and returns. `stream` (a cudaStream_t,
+ * may be NULL) orders it: the decode starts after the work the caller's
+ * stream enqueued before the call, and the caller's stream waits for the
+ * decode's completion. The first call of a batch shape (tuning + capture)
+ * completes before returning. hvdg_wait returns the call's status (device
+ * timeouts, non-finite input) and diagnostics; any other call on the context
+ * completes a call still in flight first, and hvdg_wait then reports it. */
+hvdg_status hvdg_decode_fields_device_async(hvdg_ctx* ctx, const hvdg_field_in* fields,
+                                            int n_fields, const hvdg_config* cfg,
+                                            hvdg_field_out* out, void* stream);
+/* Wait for the last asynchronous decode; its status and diag (optional).
+ * HVDG_OK with zeroed diag when none is outstanding. */
+hvdg_status hvdg_wait(hvdg_ctx* ctx, hvdg_diag* diag);
+
 /* hvd::DecodeFrameSequenceWindow (frame_bridge.cpp:722-947): split each
  * int16 frame into fields, ACC, field-order vote, window decode, weave and
  * 10-bit requantise. `out` has core_end - core_begin entries. Returns
