@@ -214,7 +214,15 @@ def make_field(seed: int, standard: int = _cabi.STD_NTSC, noise_sigma: float = 0
     chi = v - 1j * u
 
     xs = np.arange(fw)
-    phi = theta[:, None] + 0.5 * np.pi * xs[None, :]
+    w0 = 0.5 * np.pi
+    if g.subcarrier_hz > 0.0:
+        # a declared subcarrier: w0 = 2 pi fsc / fs, per-line advance from the
+        # fractional cycles per line (FieldGeometry::phase_per_sample /
+        # line_advance, ntsc_geometry.h:124-177)
+        w0 = 2.0 * np.pi * g.subcarrier_hz / g.sample_rate
+        cyc = g.subcarrier_hz * fw / g.sample_rate
+        theta = th0 + 2.0 * np.pi * (cyc - np.floor(cyc)) * line_idx
+    phi = theta[:, None] + w0 * xs[None, :]
     car = np.exp(1j * phi)
     if pal:
         car = np.where(vsw[:, None] < 0, -np.conj(car), car)

@@ -80,3 +80,43 @@ def test_symmetry_variant_vs_oracle(ctx, std):
     assert abs(psnr(out.luma, f.y_true) - psnr(yd, f.y_true)) < 0.05
     assert abs(psnr(out.chroma, f.chi_true) - psnr(cd, f.chi_true)) < 0.05
     assert np.abs(out.luma - yd).max() < 0.05 and np.abs(out.chroma - cd).max() < 0.05
+
+
+def _geometry_case(case):
+    if case == "pal_m":
+        # PAL-M: 525-line raster, PAL V-switch, 90 deg per line (ntsc_geometry.h:40-47, 165-166)
+        return _cabi.default_geometry(_cabi.STD_PAL_M), _cabi.STD_PAL_M
+    # a declared, non-standard subcarrier: w0 = 2 pi fsc / fs != pi / 2 and
+    # the per-line advance from the fractional cycles per line
+    g = _cabi.default_geometry(_cabi.STD_NTSC)
+    g.subcarrier_hz = _cabi.FSC_NTSC * (1.0 + 3e-4)
+    return g, _cabi.STD_NTSC
+
+
+@pytest.mark.parametrize("case", ["pal_m", "custom_fsc"])
+def test_other_standards_vs_oracle_and_reference(ctx, case):
+    """PAL-M and a declared subcarrier frequency (the lock-in's PAL-family
+    parity search at 90 deg / line; exact column phasors exp(i w0 x) instead
+    of the 4fsc quadrants) against the FP64 oracle and the compiled
+    reference."""
+    g, std = _geometry_case(case)
+    f = synth.make_field(31, std, noise_sigma=0.5, geometry=g)
+    cfg = _cfg()
+    out = ctx.decode_fields([api.Field(f.samples, g, parity=0)], cfg, want_theta=True)[0]
+    ire = synth.to_ire(f.samples)
+    (yo, chio, obs), = O.decode_fields_2d([ire], [0], g, cfg)
+    dth = np.abs(np.angle(np.exp(1j * (out.theta.astype(np.float64) - obs.theta))))
+    assert dth.max() < 1e-4
+    if std == _cabi.STD_PAL_M:
+        assert (out.vswitch == obs.vswitch).all()
+    dY, dC = np.abs(out.luma - yo).max(), np.abs(out.chroma - chio).max()
+    print(f"{case}: maxdY={dY:.3g} maxdC={dC:.3g} PSNR Y gpu={psnr(out.luma, f.y_true):.2f} "
+          f"oracle={psnr(yo, f.y_true):.2f}")
+    assert abs(psnr(out.luma, f.y_true) - psnr(yo, f.y_true)) < 0.05
+    assert abs(psnr(out.chroma, f.chi_true) - psnr(chio, f.chi_true)) < 0.05
+    assert dY < 0.05 and dC < 0.05
+    assert psnr(out.luma, f.y_true) > 35.0     # the decode actually separates
+    from oracle import ref
+    if ref.available():
+        (yr,), (cr,) = ref.decode_fields([ire], [0], [g], [cfg], across_fields=False)
+        assert np.abs(out.luma - yr).max() < 0.05 and np.abs(out.chroma - cr).max() < 0.05

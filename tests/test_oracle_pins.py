@@ -358,3 +358,26 @@ def test_oracle_drizzle_matches_reference():
     d, dc = np.abs(oy - ry), np.abs(oc - rc)
     assert d.mean() < 1e-4 and dc.mean() < 1e-4
     assert (d > 1e-3).mean() < 1e-3 and (dc > 1e-3).mean() < 1e-3
+
+
+@pytest.mark.parametrize("case", ["pal_m", "custom_fsc"])
+def test_oracle_other_standards_match_reference(case):
+    """PAL-M (90 deg / line, V-switch) and a declared subcarrier frequency
+    (exact column phasors, fractional line advance): the oracle's 2-D decode
+    against the compiled reference on the same field."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    from hvdg import api, synth
+    if case == "pal_m":
+        g, std = _cabi.default_geometry(_cabi.STD_PAL_M), _cabi.STD_PAL_M
+    else:
+        g, std = _cabi.default_geometry(_cabi.STD_NTSC), _cabi.STD_NTSC
+        g.subcarrier_hz = _cabi.FSC_NTSC * (1.0 + 3e-4)
+    f = synth.make_field(31, std, noise_sigma=0.5, geometry=g)
+    cfg = api.default_config(irls_outer=3, cg_iterations=60, fast=0, cg_tol=1e-6,
+                             temporal_strength=-1.0)
+    ire = synth.to_ire(f.samples)
+    (yo, co, _), = O.decode_fields_2d([ire], [0], g, cfg)
+    (yr,), (cr,) = ref.decode_fields([ire], [0], [g], [cfg], across_fields=False)
+    assert np.abs(yo - yr).max() < 2e-2 and np.abs(co - cr).max() < 2e-2
