@@ -74,3 +74,18 @@ def test_no_device_is_reported_not_faulted():
     lib = _cabi.load_library()
     h = C.c_void_p()
     assert lib.hvdg_create(0, C.byref(h)) == _cabi.ERR_NO_DEVICE
+
+
+def test_shim_library_exports_the_reference_entry_points():
+    """The drop-in shim, built against the reference's headers, exports the
+    reference's C++ frame-bridge functions (mangled hvd:: names) on top of
+    the product library; no GPU needed to load it."""
+    import subprocess
+    from oracle import shim
+    if not shim.available():
+        pytest.skip("shim not built (needs the reference's headers)")
+    shim.lib()
+    syms = subprocess.run(["nm", "-D", "--defined-only", str(shim.LIB_PATH)],
+                          capture_output=True, text=True).stdout
+    for name in ("DecodeFrameSequenceWindow", "DecodeFrameBuffer", "DecodeYcFrameBuffer"):
+        assert f"3hvd{len(name)}{name}" in syms, name
