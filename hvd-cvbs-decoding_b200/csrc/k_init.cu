@@ -166,13 +166,13 @@ __global__ void __launch_bounds__(256) k_init_rows(InitArgs a) {
 }
 
 // ---- columns ---------------------------------------------------------------
-// grid = (column groups over all fields); block = 256; dynamic smem =
-// 2 * 8 * kColFft float2 = 2 * 4 * kColFftWide float2. The column length M of
-// a geometry is 1024 (field planes: 2 hp - 1 <= 1024; 8 columns per CTA, one
-// warp each) or 2048 (woven frames, hp up to 1024; 4 columns per CTA, two
-// warps each, paired by a named barrier).
-constexpr int kColGroup = 8;
-constexpr int kColGroupWide = 4;
+// grid = (column groups over all fields); block = 256; dynamic smem 64 KiB
+// (3 CTAs per SM). The column length M of a geometry is 1024 (field planes:
+// 2 hp - 1 <= 1024; 4 columns per CTA, two warps per column) or 2048 (woven
+// frames, hp up to 1024; 2 columns per CTA, four warps per column); the
+// warps of a column synchronise on their own named barrier.
+constexpr int kColGroup = 4;
+constexpr int kColGroupWide = 2;
 constexpr int kColSmem = 2 * kColGroup * kColFft * (int)sizeof(float2);
 static_assert(2 * kColGroupWide * kColFftWide * (int)sizeof(float2) == kColSmem,
               "both column variants use the same shared-memory footprint");
@@ -180,6 +180,10 @@ static_assert(2 * kColGroupWide * kColFftWide * (int)sizeof(float2) == kColSmem,
 struct PairSync {  // the 64 threads of one column (named barrier 1 + pair)
   int id;
   __device__ void operator()() const { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+};
+struct QuadSync {  // the 128 threads of one wide column (named barrier 1 + half)
+  int id;
+  __device__ void operator()() const { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 };
 
 template <int M, int G, typename Sync>
@@ -234,15 +238,19 @@ __global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
+  const int pair = threadIdx.x >> 6;
   if (gd.col_m == kColFftWide) {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
-    const int pair = threadIdx.x >> 6;
-    init_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 63,
-                                               64, pair, PairSync{1 + pair});
+    const int half = threadIdx.x >> 7;
+    init_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 127,
+                                               128, half, QuadSync{1 + half});
   } else {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
-    init_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, lane, 32, warp, WarpSync());
+    init_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, threadIdx.x & 63, 64, pair,
+                                       PairSync{1 + pair});
   }
+  (void)warp;
+  (void)lane;
 }
 
 // ---- symmetry variant (holographic_init.cpp:265-306) ------------------------
@@ -362,16 +370,19 @@ __global__ void __launch_bounds__(256) k_sym_cols(InitArgs a, int mode) {
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
+  const int pair = threadIdx.x >> 6;
   if (gd.col_m == kColFftWide) {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
-    const int pair = threadIdx.x >> 6;
-    sym_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 63, 64,
-                                              pair, PairSync{1 + pair}, mode);
+    const int half = threadIdx.x >> 7;
+    sym_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 127,
+                                              128, half, QuadSync{1 + half}, mode);
   } else {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
-    sym_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, lane, 32, warp, WarpSync(),
-                                      mode);
+    sym_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, threadIdx.x & 63, 64, pair,
+                                      PairSync{1 + pair}, mode);
   }
+  (void)warp;
+  (void)lane;
 }
 
 // Certified spectrum (holographic_init.cpp:276-290): plane 1 = plane 0 x
