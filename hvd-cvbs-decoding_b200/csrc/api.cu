@@ -450,6 +450,9 @@ struct Batch {
   std::vector<int4> crop_rows;  // per S row: (plane, row, source field, source line)
   std::vector<int64_t> px_offs;
   std::vector<int> pitches;
+  // per field: the solver writes luma / chroma straight to the caller's
+  // buffers (FieldDesc out_y / out_c), so no copy follows
+  std::vector<char> direct_y, direct_c;
   Layout L;
   int max_phases = 0;
 };
@@ -751,6 +754,9 @@ struct RunOpts {
   int band_rows = -1;                // solver band height override (-1: context setting)
   int ctas_per_sm = -1;              // solver CTAs per SM override (-1: context setting)
   bool async = false;                // graph replay left in flight (hvdg_wait completes it)
+  // the call's outputs: where the solver can reach them (device buffers, or
+  // page-locked host buffers), its final phase writes them directly
+  const hvdg_field_out* out_direct = nullptr;
   // woven frames: `in` holds two source fields per plane (plan_batch); their
   // F32 IRE samples are written into the arena's raw slots on the device
   const hvdg_geometry* weave_geom = nullptr;
@@ -829,6 +835,28 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
     b.prep[k].samples = (opt.device_io && !opt.weave_geom)
                             ? in[k].samples
                             : (const void*)(at<char>(ctx, L.o_raw) + b.pp[k].raw_off);
+  }
+  b.direct_y.assign(m, 0);
+  b.direct_c.assign(m, 0);
+  if (opt.out_direct && opt.do_solve && !opt.weave_geom) {
+    // a buffer the kernel can address: device memory (device_io) or
+    // page-locked host memory mapped into the device's address space
+    auto reach = [&](void* p) -> void* {
+      if (!p) return nullptr;
+      if (opt.device_io) return p;
+      cudaPointerAttributes pa;
+      if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+      return pa.type == cudaMemoryTypeHost ? pa.devicePointer : nullptr;
+    };
+    for (int i = 0; i < m; ++i) {
+      b.fields[i].out_y = static_cast<float*>(reach(opt.out_direct[i].luma));
+      b.fields[i].out_c = static_cast<float2*>(reach(opt.out_direct[i].chroma));
+      b.direct_y[i] = b.fields[i].out_y != nullptr;
+      b.direct_c[i] = b.fields[i].out_c != nullptr;
+    }
   }
   put(L.o_prep, b.prep.data(), sizeof(hvdg::PrepDesc) * n);
   put(L.o_fields, b.fields.data(), sizeof(FieldDesc) * m);
@@ -1035,12 +1063,12 @@ hvdg_status stage_finish(hvdg_ctx* ctx, Staged& S, hvdg_field_out* out, const Ru
   const cudaMemcpyKind kind = opt.device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   for (int i = 0; i < n; ++i) {
     const FieldPlan& p = b.fp[i];
-    if (out[i].luma) {
+    if (out[i].luma && !b.direct_y[i]) {
       e = cudaMemcpy2DAsync(out[i].luma, sizeof(float) * p.w, at<float>(ctx, L.o_Y) + p.px_off,
                             sizeof(float) * p.pitch, sizeof(float) * p.w, p.h, kind, s);
       if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy luma");
     }
-    if (out[i].chroma) {
+    if (out[i].chroma && !b.direct_c[i]) {
       e = cudaMemcpy2DAsync(out[i].chroma, sizeof(float2) * p.w, at<float2>(ctx, L.o_X0) + p.px_off,
                             sizeof(float2) * p.pitch, sizeof(float2) * p.w, p.h, kind, s);
       if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "copy chroma");
@@ -1092,8 +1120,10 @@ hvdg_status stage_finish(hvdg_ctx* ctx, Staged& S, hvdg_field_out* out, const Ru
 
 // The 2-D pipeline over one batch: lock-in, crop, init, aniso, solver.
 hvdg_status run_batch_once(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_config* cfg,
-                           hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt) {
+                           hvdg_field_out* out, hvdg_diag* diag, const RunOpts& opt_in) {
   Staged S;
+  RunOpts opt = opt_in;
+  if (!opt.weave_geom) opt.out_direct = out;
   hvdg_status st = stage_upload(ctx, in, n, cfg, opt, 0, S);
   if (st != HVDG_OK) return st;
   st = stage_prepare(ctx, S, opt);
@@ -1160,6 +1190,7 @@ hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const
     }
     RunOpts o2 = opt;
     o2.tables_only = true;
+    o2.out_direct = out;
     Staged S;
     hvdg_status st = stage_upload(ctx, in, n, cfg, o2, 0, S);
     if (st != HVDG_OK) return st;
@@ -1191,11 +1222,11 @@ hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const
     }
     for (int i = 0; i < n && st == HVDG_OK; ++i) {
       const FieldPlan& p = S.b.fp[i];
-      if (out[i].luma)
+      if (out[i].luma && !S.b.direct_y[i])
         cudaMemcpy2DAsync(out[i].luma, sizeof(float) * p.w, at<float>(ctx, L.o_Y) + p.px_off,
                           sizeof(float) * p.pitch, sizeof(float) * p.w, p.h,
                           cudaMemcpyDeviceToDevice, s);
-      if (out[i].chroma)
+      if (out[i].chroma && !S.b.direct_c[i])
         cudaMemcpy2DAsync(out[i].chroma, sizeof(float2) * p.w, at<float2>(ctx, L.o_X0) + p.px_off,
                           sizeof(float2) * p.pitch, sizeof(float2) * p.w, p.h,
                           cudaMemcpyDeviceToDevice, s);

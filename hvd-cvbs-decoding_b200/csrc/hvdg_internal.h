@@ -49,6 +49,12 @@ struct FieldDesc {
   int unit_count;      // number of solver units
   int n_phases;        // n_outer * (2 + n_inner) + 1
   int adj_flags;       // adjoint solves: kAdjFixedW | kAdjExtB (0 for decodes)
+  // optional dense (row stride w) destinations the solver's final phase
+  // writes the field's luma / chroma to, besides the planes: the caller's
+  // device buffers, or its page-locked host buffers (mapped), so the copy
+  // out overlaps the other fields' solves
+  float* out_y;
+  float2* out_c;
 };
 
 // FieldDesc::adj_flags. kAdjFixedW: the R phase keeps the weights already in

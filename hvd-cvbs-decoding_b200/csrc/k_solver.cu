@@ -679,6 +679,23 @@ __device__ __noinline__ void phase_final(const SolverArgs& A, const FieldDesc& f
     } else if (l.va) {
       __stcg(A.Y + base + o, ya);
     }
+    const int64_t od = (int64_t)y * f.w + l.xa;  // dense destination index
+    if (f.out_c) {
+      if (l.va && l.vb && (od & 1) == 0) {
+        __stcs(reinterpret_cast<float4*>(f.out_c + od), make_float4(xa.x, xa.y, xb.x, xb.y));
+      } else {
+        if (l.va) __stcs(f.out_c + od, xa);
+        if (l.vb) __stcs(f.out_c + od + 1, xb);
+      }
+    }
+    if (f.out_y) {
+      if (l.va && l.vb && (od & 1) == 0) {
+        __stcs(reinterpret_cast<float2*>(f.out_y + od), make_float2(ya, yb));
+      } else {
+        if (l.va) __stcs(f.out_y + od, ya);
+        if (l.vb) __stcs(f.out_y + od + 1, yb);
+      }
+    }
   }
 }
 

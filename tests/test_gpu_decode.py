@@ -120,3 +120,30 @@ def test_other_standards_vs_oracle_and_reference(ctx, case):
     if ref.available():
         (yr,), (cr,) = ref.decode_fields([ire], [0], [g], [cfg], across_fields=False)
         assert np.abs(out.luma - yr).max() < 0.05 and np.abs(out.chroma - cr).max() < 0.05
+
+
+def test_pinned_outputs_written_by_the_solver(ctx):
+    """Page-locked output buffers are written by the solver's final phase
+    itself (mapped host memory), overlapping the other fields' solves; the
+    results equal those copied into pageable buffers, bit for bit, for a
+    mixed NTSC / PAL batch with an odd-width geometry (unaligned dense rows)."""
+    torch = pytest.importorskip("torch")
+    fs = synth.mixed_batch(5, 3, 2, outer_range=(2, 3), cg_per_outer=10)
+    geoms = [_cabi.default_geometry(f.standard) for f in fs]
+    g_odd = _cabi.geometry_copy(geoms[0], active_video_end=geoms[0].active_video_end - 1)
+    geoms[0] = g_odd
+    cfg = _cfg()
+    fields = [api.Field(f.samples, g, parity=f.parity, irls_outer=f.irls_outer,
+                        cg_iterations=f.cg_iterations) for f, g in zip(fs, geoms)]
+    ref_out = ctx.decode_fields(fields, cfg)
+    pinned, keep = [], []
+    for g in geoms:
+        ty = torch.zeros((g.active_lines, g.active_width), dtype=torch.float32, pin_memory=True)
+        tc = torch.zeros((g.active_lines, g.active_width, 2), dtype=torch.float32,
+                         pin_memory=True)
+        keep += [ty, tc]
+        pinned.append(api.Decoded(ty.numpy(), tc.numpy().view(np.complex64)[..., 0]))
+    got = ctx.decode_fields(fields, cfg, out=pinned)
+    for a, b in zip(got, ref_out):
+        assert np.array_equal(a.luma, b.luma)
+        assert np.array_equal(a.chroma, b.chroma)
