@@ -18,6 +18,8 @@
 //   k_init_blend: edge-energy blend -> chi0, Y0
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "hvdg_common.cuh"
 #include "k_init.h"
 
@@ -166,34 +168,206 @@ __global__ void __launch_bounds__(256) k_init_rows(InitArgs a) {
 }
 
 // ---- columns ---------------------------------------------------------------
-// grid = (column groups over all fields); block = 256; dynamic smem 64 KiB
-// (3 CTAs per SM). The column length M of a geometry is 1024 (field planes:
-// 2 hp - 1 <= 1024; 4 columns per CTA, two warps per column) or 2048 (woven
-// frames, hp up to 1024; 2 columns per CTA, four warps per column); the
-// warps of a column synchronise on their own named barrier.
+// grid = (column groups over all fields); block = 128; dynamic smem 32 KiB;
+// up to 170 registers, 3 CTAs per SM. The column length M of a geometry is
+// 1024 (field planes: 2 hp - 1 <= 1024; 4 columns per CTA, one warp each) or
+// 2048 (woven frames, hp up to 1024; 2 columns per CTA, two warps each). Each column's cyclic convolution runs
+// in registers (col_conv_reg): a column of 1024 is a 32 x 32 four-step FFT --
+// 32-point FFTs along each lane's 32 values, twiddles, a transpose through
+// the column's shared-memory slot, 32-point FFTs again -- and the inverse
+// mirrors it back to natural order; a column of 2048 adds one radix-2 step
+// (decimation in time forward, in frequency inverse) between the two warps.
+constexpr int kColThreads = 128;
 constexpr int kColGroup = 4;
 constexpr int kColGroupWide = 2;
-constexpr int kColSmem = 2 * kColGroup * kColFft * (int)sizeof(float2);
-static_assert(2 * kColGroupWide * kColFftWide * (int)sizeof(float2) == kColSmem,
+constexpr int kColSmem = kColGroup * kColFft * (int)sizeof(float2);
+static_assert(kColGroupWide * kColFftWide * (int)sizeof(float2) == kColSmem,
               "both column variants use the same shared-memory footprint");
 
-struct PairSync {  // the 64 threads of one column (named barrier 1 + pair)
+struct PairSync {  // the 64 threads of one wide column (named barrier 1 + pair)
   int id;
   __device__ void operator()() const { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 };
-struct QuadSync {  // the 128 threads of one wide column (named barrier 1 + half)
-  int id;
-  __device__ void operator()() const { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+__host__ __device__ constexpr int brev5(int i) {
+  return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
+}
+
+// exp(-2 pi i k / 32), k < 16, and exp(-2 pi i m / 64), m < 32: twiddles
+// read as constant-bank operands (no registers); filled from the host
+// (configure_init_kernels).
+__constant__ float2 c_tw32[16];
+__constant__ float2 c_tw64[32];
+
+// Keeps the compiler from hoisting the loads that follow above this point:
+// the register FFT holds 32 complex values per lane, and loads of all the
+// twiddles or spectrum values ahead of their use would not fit beside them.
+__device__ __forceinline__ void load_fence() { asm volatile("" ::: "memory"); }
+
+// v[j] *= exp(-+2 pi i lane j / 1024), j = 1..31 (INV: conjugate), each
+// twiddle the product of two table values, lane (8 a) and lane b.
+template <bool INV>
+__device__ __forceinline__ void twiddle1024(float2 (&v)[32], const float2* __restrict__ tw,
+                                            int lane) {
+  float2 wb[8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) wb[b] = __ldg(tw + ((lane * b) & 1023));
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    load_fence();
+    const float2 wa = __ldg(tw + ((8 * a * lane) & 1023));
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int j = 8 * a + b;
+      if (j == 0) continue;
+      float2 w = a == 0 ? wb[b] : (b == 0 ? wa : cmul(wa, wb[b]));
+      if (INV) w.y = -w.y;
+      v[j] = cmul(v[j], w);
+    }
+  }
+}
+
+// 32-point DFT of one lane's registers (radix-2 decimation in time, natural
+// order in and out; INV: conjugate twiddles, unnormalised).
+template <bool INV>
+__device__ __forceinline__ void fft32_reg(float2 (&v)[32], const float2* __restrict__ tw1024) {
+  (void)tw1024;
+  float2 a[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) a[i] = v[brev5(i)];
+#pragma unroll
+  for (int len = 2; len <= 32; len <<= 1) {
+    const int half = len >> 1;
+#pragma unroll
+    for (int k = 0; k < half; ++k) {
+      float2 w = make_float2(1.f, 0.f);
+      if (k) {
+        w = c_tw32[k * (32 / len)];
+        if (INV) w.y = -w.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 32; i += len) {
+        const float2 t = k ? cmul(a[i + k + half], w) : a[i + k + half];
+        const float2 u = a[i + k];
+        a[i + k] = cadd(u, t);
+        a[i + k + half] = csub(u, t);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = a[i];
+}
+
+// 1024-point DFT by one warp. In: lane l holds x[l + 32 k] in v[k]. Out:
+// lane j holds X[j + 32 m] in v[m]. scr: 1024 float2 of this warp's shared
+// memory (the transpose, XOR-swizzled so no access has bank conflicts).
+__device__ __forceinline__ void fft1024_fwd(float2 (&v)[32], float2* scr,
+                                            const float2* __restrict__ tw, int lane) {
+  fft32_reg<false>(v, tw);
+  twiddle1024<false>(v, tw, lane);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) scr[j * 32 + (lane ^ j)] = v[j];
+  __syncwarp();
+#pragma unroll
+  for (int l = 0; l < 32; ++l) v[l] = scr[lane * 32 + (l ^ lane)];
+  __syncwarp();
+  fft32_reg<false>(v, tw);
+}
+
+// The inverse (unnormalised): in, lane j holds Y[j + 32 m] in v[m]; out,
+// lane l holds y[l + 32 k] in v[k].
+__device__ __forceinline__ void fft1024_inv(float2 (&v)[32], float2* scr,
+                                            const float2* __restrict__ tw, int lane) {
+  fft32_reg<true>(v, tw);
+  twiddle1024<true>(v, tw, lane);
+  __syncwarp();
+#pragma unroll
+  for (int l = 0; l < 32; ++l) scr[l * 32 + (lane ^ l)] = v[l];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = scr[lane * 32 + (j ^ lane)];
+  __syncwarp();
+  fft32_reg<true>(v, tw);
+}
+
+struct NoSync {
+  __device__ void operator()() const { __syncwarp(); }
 };
+
+// In-place cyclic convolution of one column in shared memory:
+// buf[0, M) <- IFFT_M(FFT_M(buf) * kh), kh the kernel spectrum (1/M folded
+// in). M = 1024: one warp (sub 0). M = 2048: two warps (sub 0 / 1, paired
+// by `sync`), each taking one parity of the samples.
+template <int M, typename Sync>
+__device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restrict__ kh,
+                                             const float2* __restrict__ tw1024,
+                                             const float2* __restrict__ tw2048, int sub, int lane,
+                                             Sync sync) {
+  constexpr int S = M / 1024;
+  float2 v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = buf[(lane + 32 * k) * S + sub];
+  sync();
+  float2* scr = buf + sub * 1024;
+  fft1024_fwd(v, scr, tw1024, lane);  // E (sub 0) / O (sub 1) of the parities
+  if (S == 2) {
+    // X[q] = E[q] + W^q O[q], X[q + 1024] = E[q] - W^q O[q], W = exp(-2 pi i / 2048)
+    if (sub == 1) {
+      // W^(lane + 32 m) = W^lane exp(-2 pi i m / 64)
+      const float2 wl = __ldg(tw2048 + lane);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = cmul(v[m], cmul(wl, c_tw64[m]));
+    }
+    sync();
+#pragma unroll
+    for (int m = 0; m < 32; ++m) scr[lane + 32 * m] = v[m];
+    sync();
+    const float2* other = buf + (1 - sub) * 1024;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      const float2 o = other[lane + 32 * m];
+      v[m] = sub == 0 ? cadd(v[m], o) : csub(o, v[m]);
+    }
+    sync();
+  }
+#pragma unroll
+  for (int m = 0; m < 32; ++m) {
+    if ((m & 7) == 0) load_fence();
+    v[m] = cmul(v[m], __ldg(kh + sub * 1024 + lane + 32 * m));
+  }
+  if (S == 2) {
+    // even outputs from Y[q] + Y[q + 1024], odd from (Y[q] - Y[q + 1024]) W^-q
+#pragma unroll
+    for (int m = 0; m < 32; ++m) scr[lane + 32 * m] = v[m];
+    sync();
+    const float2* other = buf + (1 - sub) * 1024;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      const float2 o = other[lane + 32 * m];
+      if (sub == 0) {
+        v[m] = cadd(v[m], o);
+      } else {
+        float2 w = cmul(__ldg(tw2048 + lane), c_tw64[m]);
+        w.y = -w.y;
+        v[m] = cmul(csub(o, v[m]), w);
+      }
+    }
+    sync();
+  }
+  fft1024_inv(v, scr, tw1024, lane);
+  sync();
+#pragma unroll
+  for (int k = 0; k < 32; ++k) buf[(lane + 32 * k) * S + sub] = v[k];
+  sync();
+}
 
 template <int M, int G, typename Sync>
 __device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDesc& f,
-                                               const GeomDesc& gd, int f_idx, int x0,
-                                               const float2* __restrict__ tw, int ct, int nct,
-                                               int col, Sync sync) {
+                                               const GeomDesc& gd, int f_idx, int x0, int col,
+                                               int sub, int lane, Sync sync) {
   extern __shared__ float2 sm_cols[];
-  float2* A = sm_cols + col * 2 * M;
-  float2* B = A + M;
+  float2* buf = sm_cols + col * M;
   for (int v = 0; v < 2; ++v) {
     const float2* src = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
     // cooperative coalesced load: thread -> (row, column-in-group)
@@ -201,56 +375,44 @@ __device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDes
       const int row = i / G, c = i % G;
       float2 val = make_float2(0.f, 0.f);
       if (row < gd.hp && x0 + c < f.w) val = src[(int64_t)row * f.pitch + x0 + c];
-      sm_cols[c * 2 * M + row] = val;
+      sm_cols[c * M + row] = val;
     }
     __syncthreads();
-    float2* spec = fft_stockham<M, false>(A, B, tw, ct, nct, sync);
-    const float2* kh = a.khat + gd.khat_col_off + v * M;
-    float2* other = spec == A ? B : A;
-    for (int i = ct; i < M; i += nct) other[i] = cmul(spec[i], __ldg(kh + i));
-    sync();
-    float2* res = fft_stockham<M, true>(other, spec, tw, ct, nct, sync);
-    // result must land where the cooperative store reads it: column c at A_c
-    if (res != A)
-      for (int i = ct; i < M; i += nct) A[i] = res[i];
+    col_conv_reg<M>(buf, a.khat + gd.khat_col_off + v * M, a.tw_col, a.tw_row, sub, lane, sync);
     __syncthreads();
     if (a.adj_out) {
       // adjoint mode: every padded row (the transposed crop)
       float2* dst = a.adj_out + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
       for (int i = threadIdx.x; i < gd.hp * G; i += blockDim.x) {
         const int y = i / G, c = i % G;
-        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * M + y];
+        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * M + y];
       }
     } else {
       float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
       for (int i = threadIdx.x; i < f.h * G; i += blockDim.x) {
         const int y = i / G, c = i % G;
-        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * 2 * M + y + gd.pad];
+        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * M + y + gd.pad];
       }
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(256) k_init_cols(InitArgs a) {
+__global__ void __launch_bounds__(kColThreads, 3) k_init_cols(InitArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gidx = blockIdx.x;
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
-  const int pair = threadIdx.x >> 6;
   if (gd.col_m == kColFftWide) {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
-    const int half = threadIdx.x >> 7;
-    init_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 127,
-                                               128, half, QuadSync{1 + half});
+    const int pair = warp >> 1;
+    init_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, pair, warp & 1, lane,
+                                               PairSync{1 + pair});
   } else {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
-    init_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, threadIdx.x & 63, 64, pair,
-                                       PairSync{1 + pair});
+    init_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, warp, 0, lane, NoSync());
   }
-  (void)warp;
-  (void)lane;
 }
 
 // ---- symmetry variant (holographic_init.cpp:265-306) ------------------------
@@ -327,16 +489,14 @@ __global__ void __launch_bounds__(256) k_sym_rows(InitArgs a, int mode) {
 
 // Column DFTs in place. mode 0: forward on plane 0; mode 1: the conjugated
 // input of the inverse, on plane 1 (the row pass conjugates the output).
+// The chirps multiply on the way into and out of shared memory; the chirp
+// filter's cyclic convolution is col_conv_reg.
 template <int M, int G, typename Sync>
 __device__ __forceinline__ void sym_cols_body(const InitArgs& a, const FieldDesc& f,
-                                              const GeomDesc& gd, int f_idx, int x0,
-                                              const float2* __restrict__ tw, int ct, int nct,
-                                              int col, Sync sync, int mode) {
+                                              const GeomDesc& gd, int f_idx, int x0, int col,
+                                              int sub, int lane, Sync sync, int mode) {
   extern __shared__ float2 sm_cols[];
-  float2* A = sm_cols + col * 2 * M;
-  float2* B = A + M;
   const float2* chirp = a.khat + gd.sym_col_chirp;
-  const float2* hh = a.khat + gd.sym_col_hhat;
   float2* plane = a.rowbuf + a.rowbuf_off[f_idx] + (mode ? (int64_t)gd.hp * f.pitch : 0);
   for (int i = threadIdx.x; i < M * G; i += blockDim.x) {
     const int row = i / G, c = i % G;
@@ -346,43 +506,34 @@ __device__ __forceinline__ void sym_cols_body(const InitArgs& a, const FieldDesc
       if (mode) v.y = -v.y;
       v = cmul(v, __ldg(chirp + row));
     }
-    sm_cols[c * 2 * M + row] = v;
+    sm_cols[c * M + row] = v;
   }
   __syncthreads();
-  float2* spec = fft_stockham<M, false>(A, B, tw, ct, nct, sync);
-  float2* other = spec == A ? B : A;
-  for (int i = ct; i < M; i += nct) other[i] = cmul(spec[i], __ldg(hh + i));
-  sync();
-  float2* res = fft_stockham<M, true>(other, spec, tw, ct, nct, sync);
-  if (res != A)
-    for (int i = ct; i < M; i += nct) A[i] = res[i];
+  col_conv_reg<M>(sm_cols + col * M, a.khat + gd.sym_col_hhat, a.tw_col, a.tw_row, sub, lane,
+                  sync);
   __syncthreads();
   for (int i = threadIdx.x; i < gd.hp * G; i += blockDim.x) {
     const int row = i / G, c = i % G;
     if (x0 + c < f.w)
-      plane[(int64_t)row * f.pitch + x0 + c] = cmul(sm_cols[c * 2 * M + row], __ldg(chirp + row));
+      plane[(int64_t)row * f.pitch + x0 + c] = cmul(sm_cols[c * M + row], __ldg(chirp + row));
   }
 }
 
-__global__ void __launch_bounds__(256) k_sym_cols(InitArgs a, int mode) {
+__global__ void __launch_bounds__(kColThreads, 3) k_sym_cols(InitArgs a, int mode) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gidx = blockIdx.x;
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
-  const int pair = threadIdx.x >> 6;
   if (gd.col_m == kColFftWide) {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
-    const int half = threadIdx.x >> 7;
-    sym_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, a.tw_row, threadIdx.x & 127,
-                                              128, half, QuadSync{1 + half}, mode);
+    const int pair = warp >> 1;
+    sym_cols_body<kColFftWide, kColGroupWide>(a, f, gd, f_idx, x0, pair, warp & 1, lane,
+                                              PairSync{1 + pair}, mode);
   } else {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
-    sym_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, a.tw_col, threadIdx.x & 63, 64, pair,
-                                      PairSync{1 + pair}, mode);
+    sym_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, warp, 0, lane, NoSync(), mode);
   }
-  (void)warp;
-  (void)lane;
 }
 
 // Certified spectrum (holographic_init.cpp:276-290): plane 1 = plane 0 x
@@ -559,6 +710,18 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
 constexpr int kAnisoSmem = kAnisoMax * (int)sizeof(float);
 
 void configure_init_kernels() {
+  float2 tw32[16];
+  for (int k = 0; k < 16; ++k) {
+    const double a = -2.0 * 3.14159265358979323846 * k / 32.0;
+    tw32[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  cudaMemcpyToSymbol(c_tw32, tw32, sizeof(tw32));
+  float2 tw64[32];
+  for (int m = 0; m < 32; ++m) {
+    const double a = -2.0 * 3.14159265358979323846 * m / 64.0;
+    tw64[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  cudaMemcpyToSymbol(c_tw64, tw64, sizeof(tw64));
   cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        3 * kRowFft * (int)sizeof(float2));
   cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
@@ -576,13 +739,13 @@ void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int tota
     configured = true;
   }
   if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
-  if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
+  if (total_cgroups > 0) k_init_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a);
   if (a.chi3 && total_prows > 0 && total_cgroups > 0) {
     const int sym_smem = 2 * kRowFft * sizeof(float2);
     k_sym_rows<<<total_prows, 256, sym_smem, st>>>(a, 0);
-    k_sym_cols<<<total_cgroups, 256, col_smem, st>>>(a, 0);
+    k_sym_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a, 0);
     k_sym_certify<<<total_prows, 256, 0, st>>>(a);
-    k_sym_cols<<<total_cgroups, 256, col_smem, st>>>(a, 1);
+    k_sym_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a, 1);
     k_sym_rows<<<total_prows, 256, sym_smem, st>>>(a, 1);
   }
   if (total_btiles > 0) k_init_blend<<<total_btiles, 256, 0, st>>>(a);
@@ -598,7 +761,7 @@ void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cg
   const int row_smem = 3 * kRowFft * sizeof(float2);
   const int col_smem = kColSmem;
   if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
-  if (total_cgroups > 0) k_init_cols<<<total_cgroups, 256, col_smem, st>>>(a);
+  if (total_cgroups > 0) k_init_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a);
 }
 
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {

@@ -142,3 +142,32 @@ def test_frame_buffer_lossless_split(ctx):
     active = got["u"] != 0.0
     assert np.abs(rec - src)[active].max() <= 1
     assert np.array_equal(got["luma"][~active], frames[0][~active])
+
+
+def test_frame_buffer_error_statuses(ctx):
+    """Statuses at the boundary, as the reference's empty-result convention
+    maps onto them: bad frame parameters -> BAD_GEOMETRY, a woven plane
+    beyond the device-path limits -> UNSUPPORTED, n = 0 -> OK, nothing
+    decoded; the context stays usable."""
+    frames, _ = synth.make_frames(97, _cabi.STD_NTSC, 1, noise_sigma=0.5)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = _cfg()
+    bad = api.frame_params(_cabi.STD_NTSC)
+    bad.white_level = bad.blanking_level          # zero codes per IRE
+    with pytest.raises(api.HvdgError) as e:
+        ctx.decode_frame_buffer(frames[0], bad, cfg)
+    assert e.value.status == _cabi.ERR_BAD_GEOMETRY
+    tall = api.frame_params(_cabi.STD_NTSC)
+    tall.active_video_start, tall.active_video_end = 0, 910   # 2 w - 1 > 2048 is fine; w = 910
+    tall.first_active_frame_line = 0                           # 263 lines -> 526-row woven plane
+    out = ctx.decode_frame_buffer(frames[0], tall, cfg)        # still within the limits
+    assert out["luma"].shape == frames[0].shape
+    pal_frames, _ = synth.make_frames(98, _cabi.STD_PAL, 1, noise_sigma=0.5)
+    wide = api.frame_params(_cabi.STD_PAL)
+    wide.active_video_start, wide.active_video_end = 10, 1110  # 2 w - 1 > 2048
+    with pytest.raises(api.HvdgError) as e:
+        ctx.decode_frame_buffer(pal_frames[0], wide, cfg)
+    assert e.value.status == _cabi.ERR_UNSUPPORTED
+    assert ctx.decode_frame_buffers([], fp, cfg) == []
+    ok = ctx.decode_frame_buffer(frames[0], fp, cfg)
+    assert np.abs(ok["u"]).max() > 0
