@@ -753,7 +753,9 @@ __device__ __noinline__ void complete_phase(const SolverArgs& A, const FieldDesc
       c->pending = 0;
     }
     (void)k;
-    __threadfence();
+    // the release store orders this lane's control writes before the flag;
+    // the other units' plane writes are already ordered before it by their
+    // fence + arrival and this warp's fence after the last arrival
     st_release(A.done_phase + fi, publish);
   }
   __syncwarp();
