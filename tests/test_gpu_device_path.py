@@ -135,3 +135,34 @@ def test_async_device_decode_on_caller_stream():
                 c = cs[i].cpu().numpy().view(np.complex64)[..., 0]
                 assert np.abs(c - host[i].chroma).max() <= 1e-5, (rep, i)
         assert ctx.wait().cg_iterations_run == 0     # nothing outstanding
+
+
+def test_contexts_on_concurrent_host_threads():
+    """One context per host thread (the reference's one HvdEngine per
+    thread, frame_bridge.h:137-140): two threads decoding different batches
+    at the same time, each on its own context and stream, get exactly the
+    results of decoding one after the other."""
+    import threading
+    cfg = api.default_config(fast=0, cg_tol=1e-6, temporal_strength=-1.0)
+    batches = []
+    for seed in (81, 82):
+        fs = synth.mixed_batch(seed, 3, 2, outer_range=(2, 3), cg_per_outer=10)
+        batches.append([api.Field(f.samples, _cabi.default_geometry(f.standard), parity=f.parity,
+                                  irls_outer=f.irls_outer, cg_iterations=f.cg_iterations)
+                        for f in fs])
+    with api.Context(0) as c0, api.Context(0) as c1:
+        seq = [c0.decode_fields(b, cfg) for b in batches]
+        got = [None, None]
+
+        def run(i, ctx):
+            for _ in range(3):
+                got[i] = ctx.decode_fields(batches[i], cfg)
+
+        th = [threading.Thread(target=run, args=(i, c)) for i, c in enumerate((c0, c1))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    for i in range(2):
+        for a, b in zip(got[i], seq[i]):
+            assert np.array_equal(a.luma, b.luma) and np.array_equal(a.chroma, b.chroma), i
