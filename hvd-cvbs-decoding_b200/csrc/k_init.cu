@@ -10,11 +10,12 @@
 // "FFT -> mask -> inverse FFT" equals a circular convolution along rows with
 // k_x = IDFT_w(gx) followed by one along columns with k_y = IDFT_hp(gy). Each
 // circular convolution of length n runs as a cyclic convolution of
-// power-of-two length M >= 2n - 1 (rows: 2048, columns: 1024) with the
-// kernel's FFT precomputed on the host: forward radix-4/2 Stockham FFT in
-// shared memory, mask multiply fused in shared memory, inverse FFT, write.
-//   k_init_rows : one CTA per padded row -> both row-filtered variants
-//   k_init_cols : one CTA per 8-column group -> chi_1, chi_2 (x2 folded in)
+// power-of-two length M >= 2n - 1 (rows: 2048; columns: 1024, or 2048 for
+// woven frames) with the kernel's FFT precomputed on the host: a four-step
+// FFT held in registers (32 values per lane, one warp per 1024 points),
+// mask multiply in registers, inverse FFT, write.
+//   k_init_rows : one warp pair per padded row -> both row-filtered variants
+//   k_init_cols : one warp (pair) per column -> chi_1, chi_2 (x2 folded in)
 //   k_init_blend: edge-energy blend -> chi0, Y0
 #include <cuda_runtime.h>
 
@@ -22,6 +23,7 @@
 
 #include "hvdg_common.cuh"
 #include "k_init.h"
+#include "per_device.h"
 
 namespace hvdg {
 
@@ -106,65 +108,6 @@ __device__ __forceinline__ float2 carrier_at(const InitArgs& a, const FieldDesc&
   const float4 L = __ldg(a.line_phasor + f.line_off + y);
   const float2 P = __ldg(a.col_phasor + f.col_off + x);
   return carrier(make_float2(L.x, L.y), P, L.z);
-}
-
-// ---- rows ------------------------------------------------------------------
-// grid = total padded rows; block = 256; dynamic smem = 3 * kRowFft float2.
-__global__ void __launch_bounds__(256) k_init_rows(InitArgs a) {
-  extern __shared__ float2 sm_rows[];
-  float2* X = sm_rows;
-  float2* P = X + kRowFft;
-  float2* Q = P + kRowFft;
-  const int r = blockIdx.x;
-  const int f_idx = a.prow_field[r];
-  const FieldDesc f = a.fields[f_idx];
-  const GeomDesc gd = a.geoms[f.geom];
-  const int yp = r - a.prow_first[f_idx];
-  const int sy = mirror_row(yp - gd.pad, f.h);
-  if (a.adj_in) {
-    // adjoint mode: each variant filters its own input row
-    for (int v = 0; v < 2; ++v) {
-      const float2* in = a.adj_in + a.rowbuf_off[f_idx] + ((int64_t)v * gd.hp + yp) * f.pitch;
-      for (int i = threadIdx.x; i < kRowFft; i += blockDim.x)
-        P[i] = i < f.w ? in[i] : make_float2(0.f, 0.f);
-      __syncthreads();
-      float2* sp = fft_stockham<kRowFft, false>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
-      const float2* kh = a.khat + gd.khat_row_off + v * kRowFft;
-      float2* oth = sp == P ? Q : P;
-      for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) oth[i] = cmul(sp[i], __ldg(kh + i));
-      __syncthreads();
-      float2* res = fft_stockham<kRowFft, true>(oth, sp, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
-      float2* out = a.rowbuf + a.rowbuf_off[f_idx] + ((int64_t)v * gd.hp + yp) * f.pitch;
-      for (int i = threadIdx.x; i < f.pitch; i += blockDim.x)
-        out[i] = i < f.w ? res[i] : make_float2(0.f, 0.f);
-      __syncthreads();
-    }
-    return;
-  }
-  const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
-  for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) {
-    float2 v = make_float2(0.f, 0.f);
-    if (i < f.w) {
-      const float s = S[i];
-      const float2 c = carrier_at(a, f, sy, i);
-      v = make_float2(s * c.x, -s * c.y);  // S * conj(c)
-    }
-    P[i] = v;
-  }
-  __syncthreads();
-  float2* spec = fft_stockham<kRowFft, false>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
-  for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) X[i] = spec[i];
-  __syncthreads();
-  for (int v = 0; v < 2; ++v) {
-    const float2* kh = a.khat + gd.khat_row_off + v * kRowFft;
-    for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) P[i] = cmul(X[i], __ldg(kh + i));
-    __syncthreads();
-    float2* res = fft_stockham<kRowFft, true>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
-    float2* out = a.rowbuf + a.rowbuf_off[f_idx] + ((int64_t)v * gd.hp + yp) * f.pitch;
-    for (int i = threadIdx.x; i < f.pitch; i += blockDim.x)
-      out[i] = i < f.w ? res[i] : make_float2(0.f, 0.f);
-    __syncthreads();
-  }
 }
 
 // ---- columns ---------------------------------------------------------------
@@ -295,20 +238,17 @@ struct NoSync {
   __device__ void operator()() const { __syncwarp(); }
 };
 
-// In-place cyclic convolution of one column in shared memory:
-// buf[0, M) <- IFFT_M(FFT_M(buf) * kh), kh the kernel spectrum (1/M folded
-// in). M = 1024: one warp (sub 0). M = 2048: two warps (sub 0 / 1, paired
-// by `sync`), each taking one parity of the samples.
+// Forward DFT of length M (1024 or 2048) held in registers. In: v[k] =
+// x[(lane + 32 k) S + sub], S = M / 1024. Out: v[m] = X[sub 1024 + lane +
+// 32 m]. buf: the M float2 of shared memory of this column (or row), which
+// no thread of it reads any more. M = 1024: one warp (sub 0). M = 2048: two
+// warps (sub 0 / 1, paired by `sync`), each taking one parity of the samples.
 template <int M, typename Sync>
-__device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restrict__ kh,
-                                             const float2* __restrict__ tw1024,
-                                             const float2* __restrict__ tw2048, int sub, int lane,
-                                             Sync sync) {
+__device__ __forceinline__ void fft_reg_fwd(float2 (&v)[32], float2* buf,
+                                            const float2* __restrict__ tw1024,
+                                            const float2* __restrict__ tw2048, int sub, int lane,
+                                            Sync sync) {
   constexpr int S = M / 1024;
-  float2 v[32];
-#pragma unroll
-  for (int k = 0; k < 32; ++k) v[k] = buf[(lane + 32 * k) * S + sub];
-  sync();
   float2* scr = buf + sub * 1024;
   fft1024_fwd(v, scr, tw1024, lane);  // E (sub 0) / O (sub 1) of the parities
   if (S == 2) {
@@ -331,11 +271,17 @@ __device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restri
     }
     sync();
   }
-#pragma unroll
-  for (int m = 0; m < 32; ++m) {
-    if ((m & 7) == 0) load_fence();
-    v[m] = cmul(v[m], __ldg(kh + sub * 1024 + lane + 32 * m));
-  }
+}
+
+// The inverse (unnormalised), from fft_reg_fwd's output layout back to its
+// input layout; same buf and pairing.
+template <int M, typename Sync>
+__device__ __forceinline__ void fft_reg_inv(float2 (&v)[32], float2* buf,
+                                            const float2* __restrict__ tw1024,
+                                            const float2* __restrict__ tw2048, int sub, int lane,
+                                            Sync sync) {
+  constexpr int S = M / 1024;
+  float2* scr = buf + sub * 1024;
   if (S == 2) {
     // even outputs from Y[q] + Y[q + 1024], odd from (Y[q] - Y[q + 1024]) W^-q
 #pragma unroll
@@ -356,6 +302,28 @@ __device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restri
     sync();
   }
   fft1024_inv(v, scr, tw1024, lane);
+}
+
+// In-place cyclic convolution of one column in shared memory:
+// buf[0, M) <- IFFT_M(FFT_M(buf) * kh), kh the kernel spectrum (1/M folded
+// in).
+template <int M, typename Sync>
+__device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restrict__ kh,
+                                             const float2* __restrict__ tw1024,
+                                             const float2* __restrict__ tw2048, int sub, int lane,
+                                             Sync sync) {
+  constexpr int S = M / 1024;
+  float2 v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = buf[(lane + 32 * k) * S + sub];
+  sync();
+  fft_reg_fwd<M>(v, buf, tw1024, tw2048, sub, lane, sync);
+#pragma unroll
+  for (int m = 0; m < 32; ++m) {
+    if ((m & 7) == 0) load_fence();
+    v[m] = cmul(v[m], __ldg(kh + sub * 1024 + lane + 32 * m));
+  }
+  fft_reg_inv<M>(v, buf, tw1024, tw2048, sub, lane, sync);
   sync();
 #pragma unroll
   for (int k = 0; k < 32; ++k) buf[(lane + 32 * k) * S + sub] = v[k];
@@ -412,6 +380,98 @@ __global__ void __launch_bounds__(kColThreads, 3) k_init_cols(InitArgs a) {
   } else {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroup;
     init_cols_body<kColFft, kColGroup>(a, f, gd, f_idx, x0, warp, 0, lane, NoSync());
+  }
+}
+
+// ---- rows ------------------------------------------------------------------
+// grid = ceil(total padded rows / 2); block = 128 (two rows, a warp pair
+// each); dynamic smem 64 KiB (per row: the 2048-float2 slot of the register
+// FFT and the row's spectrum); up to 170 registers, 3 CTAs per SM. A row's
+// 2048-point DFT runs in registers like a wide column (fft_reg_fwd /
+// fft_reg_inv): warp `sub` of the pair loads the samples of parity `sub`,
+// already demodulated, straight from S. The spectrum is parked in shared
+// memory, each thread re-reading only the values it wrote, and filtered by
+// both variants' kernel spectra in turn; each result goes out through the
+// slot as one coalesced row of the pitch.
+constexpr int kRowThreads = 128;
+constexpr int kRowsPerCta = kRowThreads / 64;
+constexpr int kRowSmem = kRowsPerCta * 2 * kRowFft * (int)sizeof(float2);
+
+__global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int total_prows) {
+  extern __shared__ float2 sm_rows[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pair = warp >> 1, sub = warp & 1, tp = threadIdx.x & 63;
+  const int r = blockIdx.x * kRowsPerCta + pair;
+  if (r >= total_prows) return;  // only pair barriers below
+  const PairSync sync{1 + pair};
+  float2* buf = sm_rows + pair * 2 * kRowFft;
+  float2* spec = buf + kRowFft;
+  const int f_idx = a.prow_field[r];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  const int yp = r - a.prow_first[f_idx];
+  float2 v[32];
+  // v[k] (natural order, x = 2 (lane + 32 k) + sub) -> out[0, pitch), zero
+  // beyond the active width; leaves buf free.
+  auto store_row = [&](float2* out) {
+    sync();
+#pragma unroll
+    for (int k = 0; k < 32; ++k) buf[2 * (lane + 32 * k) + sub] = v[k];
+    sync();
+    for (int i = tp; i < f.pitch; i += 64) out[i] = i < f.w ? buf[i] : make_float2(0.f, 0.f);
+    sync();
+  };
+  if (a.adj_in) {
+    // adjoint mode: each variant filters its own input row
+    for (int var = 0; var < 2; ++var) {
+      const int64_t row = a.rowbuf_off[f_idx] + ((int64_t)var * gd.hp + yp) * f.pitch;
+      const float2* in = a.adj_in + row;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const int x = 2 * (lane + 32 * k) + sub;
+        v[k] = x < f.w ? in[x] : make_float2(0.f, 0.f);
+      }
+      fft_reg_fwd<kRowFft>(v, buf, a.tw_col, a.tw_row, sub, lane, sync);
+      const float2* kh = a.khat + gd.khat_row_off + var * kRowFft + sub * 1024 + lane;
+#pragma unroll
+      for (int m = 0; m < 32; ++m) {
+        if ((m & 7) == 0) load_fence();
+        v[m] = cmul(v[m], __ldg(kh + 32 * m));
+      }
+      fft_reg_inv<kRowFft>(v, buf, a.tw_col, a.tw_row, sub, lane, sync);
+      store_row(a.rowbuf + row);
+    }
+    return;
+  }
+  const int sy = mirror_row(yp - gd.pad, f.h);
+  const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
+  const float2* P = a.col_phasor + f.col_off;
+  const float4 L = __ldg(a.line_phasor + f.line_off + sy);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    if ((k & 7) == 0) load_fence();
+    const int x = 2 * (lane + 32 * k) + sub;
+    float2 val = make_float2(0.f, 0.f);
+    if (x < f.w) {
+      const float s = S[x];
+      const float2 c = carrier(make_float2(L.x, L.y), __ldg(P + x), L.z);
+      val = make_float2(s * c.x, -s * c.y);  // S * conj(c)
+    }
+    v[k] = val;
+  }
+  fft_reg_fwd<kRowFft>(v, buf, a.tw_col, a.tw_row, sub, lane, sync);
+  float2* my_spec = spec + sub * 1024 + lane;
+#pragma unroll
+  for (int m = 0; m < 32; ++m) my_spec[32 * m] = v[m];
+  for (int var = 0; var < 2; ++var) {
+    const float2* kh = a.khat + gd.khat_row_off + var * kRowFft + sub * 1024 + lane;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      if ((m & 7) == 0) load_fence();
+      v[m] = cmul(my_spec[32 * m], __ldg(kh + 32 * m));
+    }
+    fft_reg_inv<kRowFft>(v, buf, a.tw_col, a.tw_row, sub, lane, sync);
+    store_row(a.rowbuf + a.rowbuf_off[f_idx] + ((int64_t)var * gd.hp + yp) * f.pitch);
   }
 }
 
@@ -709,7 +769,7 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
 
 constexpr int kAnisoSmem = kAnisoMax * (int)sizeof(float);
 
-void configure_init_kernels() {
+static void configure_init_kernels_now() {
   float2 tw32[16];
   for (int k = 0; k < 16; ++k) {
     const double a = -2.0 * 3.14159265358979323846 * k / 32.0;
@@ -722,23 +782,25 @@ void configure_init_kernels() {
     tw64[m] = make_float2((float)std::cos(a), (float)std::sin(a));
   }
   cudaMemcpyToSymbol(c_tw64, tw64, sizeof(tw64));
-  cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       3 * kRowFft * (int)sizeof(float2));
+  cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmem);
   cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
   cudaFuncSetAttribute(k_sym_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
   cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, kAnisoSmem);
 }
 
+// Kernel attributes and the twiddle constants, once per device.
+void configure_init_kernels() {
+  static PerDeviceOnce once;
+  once(configure_init_kernels_now);
+}
+
 void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
                  cudaStream_t st) {
-  static bool configured = false;
-  const int row_smem = 3 * kRowFft * sizeof(float2);
   const int col_smem = kColSmem;
-  if (!configured) {
-    configure_init_kernels();
-    configured = true;
-  }
-  if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
+  configure_init_kernels();
+  if (total_prows > 0)
+    k_init_rows<<<(total_prows + kRowsPerCta - 1) / kRowsPerCta, kRowThreads, kRowSmem, st>>>(
+        a, total_prows);
   if (total_cgroups > 0) k_init_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a);
   if (a.chi3 && total_prows > 0 && total_cgroups > 0) {
     const int sym_smem = 2 * kRowFft * sizeof(float2);
@@ -753,24 +815,17 @@ void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int tota
 
 void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cgroups,
                                 cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    configure_init_kernels();
-    configured = true;
-  }
-  const int row_smem = 3 * kRowFft * sizeof(float2);
+  configure_init_kernels();
   const int col_smem = kColSmem;
-  if (total_prows > 0) k_init_rows<<<total_prows, 256, row_smem, st>>>(a);
+  if (total_prows > 0)
+    k_init_rows<<<(total_prows + kRowsPerCta - 1) / kRowsPerCta, kRowThreads, kRowSmem, st>>>(
+        a, total_prows);
   if (total_cgroups > 0) k_init_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a);
 }
 
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {
-  static bool configured = false;
   const int smem = kAnisoSmem;
-  if (!configured) {
-    configure_init_kernels();
-    configured = true;
-  }
+  configure_init_kernels();
   if (n_fields > 0) k_aniso<<<n_fields, 1024, smem, st>>>(d_fields, chi0);
 }
 

@@ -15,6 +15,7 @@
 
 #include "hvdg_common.cuh"
 #include "k_prep.h"
+#include "per_device.h"
 
 namespace hvdg {
 
@@ -346,17 +347,19 @@ __global__ void k_crop(const PrepDesc* __restrict__ descs, const int4* __restric
 
 constexpr size_t kLockinSmem = 10 * kMaxLines * sizeof(double) + 2 * kMaxLines;
 
-void configure_prep_kernels() {
+static void configure_prep_kernels_now() {
   cudaFuncSetAttribute(k_burst_lockin, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kLockinSmem);
 }
 
+// The lock-in kernel's shared-memory opt-in, once per device.
+void configure_prep_kernels() {
+  static PerDeviceOnce once;
+  once(configure_prep_kernels_now);
+}
+
 void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    configure_prep_kernels();
-    configured = true;
-  }
+  configure_prep_kernels();
   if (n > 0) k_burst_lockin<<<n, 256, kLockinSmem, st>>>(d_descs, out);
 }
 void launch_burst_amplitude(const PrepDesc* d_descs, int n, float* d_amp, cudaStream_t st) {

@@ -36,6 +36,7 @@
 
 #include "hvdg_common.cuh"
 #include "k_solver.h"
+#include "per_device.h"
 
 namespace hvdg {
 
@@ -856,12 +857,12 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(const __grid_const
 
 constexpr int kSolverSmem = (kSolverThreads / 32) * kWarpRingBytes;
 
+static PerDeviceOnce solver_once;
+
 static void configure_solver() {
-  static bool done = false;
-  if (!done) {
+  solver_once([] {
     cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolverSmem);
-    done = true;
-  }
+  });
 }
 
 int solver_max_blocks_per_sm() {
