@@ -596,6 +596,12 @@ hvdg_status hvdg_decode_yc_frame_buffers(hvdg_ctx* ctx, const int16_t* const* lu
   return decode_woven_frames(ctx, chroma, luma, n_frames, fp, cfg, out, diag, true);
 }
 
+hvdg_status hvdg_detect_field_parity(hvdg_ctx* ctx, const int16_t* const* frames, int n_frames,
+                                     const hvdg_frame_params* fp, int32_t* votes) {
+  settle(ctx);
+  return detect_field_parity_frames(ctx, frames, n_frames, fp, votes);
+}
+
 hvdg_status hvdg_ambiguous_boxes(const float* luma, const float* chroma, int h, int w,
                                  float max_area, int32_t* boxes, int max_boxes, int* n_boxes) {
   if (!luma || !chroma || !n_boxes || h < 1 || w < 1 || max_boxes < 0 ||

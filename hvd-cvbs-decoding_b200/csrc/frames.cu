@@ -89,22 +89,6 @@ int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_param
       [&](int k, int row, int x) { return (k == 0 ? b1 : b2)[(size_t)row * fw + x]; }, fp, g);
 }
 
-// The same vote read straight from an int16 frame: each sample the vote
-// touches is converted exactly as SplitFrameFields converts it.
-int detect_field_parity_frame(const int16_t* frame, const hvdg_frame_params& fp,
-                              const hvdg_geometry& g) {
-  const int f1 = fp.field1_lines, fh = fp.frame_height;
-  const float cpi = (fp.white_level - fp.blanking_level) / 100.0f;
-  return detect_field_parity_t(
-      [&](int k, int row, int x) {
-        const int flat = k == 0 ? row : f1 + row;
-        const bool valid = k == 0 ? row < f1 : flat < fh;
-        const float s = valid ? (float)frame[frame_line_offset(fp, flat) + x] : fp.blanking_level;
-        return (s - fp.blanking_level) / cpi;
-      },
-      fp, g);
-}
-
 // AmbiguousBoxes: tile score sqrt(luma HF energy x chroma-magnitude HF
 // energy) over 16 x 16 tiles (HF = minus a count-normalised 8 x 8 box mean),
 // tiles >= 4 x the median score, kept where >= 2 of their 8 neighbours are
@@ -365,6 +349,82 @@ int16_t clamp_s10(float v) {
   return (int16_t)std::min<long>(std::max<long>(r, -1023), 1023);
 }
 
+// The field-order vote's sample grid and levels (DetectFieldParity,
+// frame_bridge.cpp:102-149; the host restatement detect_field_parity_t):
+// field lines fal + 1, fal + 1 + ystep, ... below lal - 1, columns a0,
+// a0 + 16, ... with 4 samples each. rows * cols == 0: no vote (0).
+hvdg::FrameVoteArgs vote_grid(const hvdg_frame_params& P, const hvdg_geometry& g) {
+  hvdg::FrameVoteArgs v;
+  std::memset(&v, 0, sizeof(v));
+  const int fal = g.first_active_field_line, lal = last_active_line(g);
+  v.fh = P.frame_height;
+  v.f1 = P.field1_lines;
+  v.blank = P.blanking_level;
+  v.codes_per_ire = (P.white_level - P.blanking_level) / 100.0f;
+  v.r0 = fal + 1;
+  v.ystep = std::max(1, (lal - fal) / 120);
+  v.a0 = P.active_video_start;
+  if (lal - fal >= 8 && P.active_video_end - P.active_video_start >= 32) {
+    for (int r = fal + 1; r + 1 < lal; r += v.ystep) ++v.rows;
+    for (int x = P.active_video_start; x + 4 <= P.active_video_end; x += 16) ++v.cols;
+  }
+  return v;
+}
+
+// DetectFieldParity of n int16 frames on the device (k_frame_vote, the
+// decode's own vote): +1 block 1 on top, -1 block 2 on top, 0 undecided.
+hvdg_status detect_field_parity_frames(hvdg_ctx* ctx, const int16_t* const* frames, int n,
+                                       const hvdg_frame_params* fp, int32_t* votes) {
+  if (!ctx || !fp || n < 0 || (n > 0 && (!frames || !votes))) return HVDG_ERR_BAD_ARGUMENT;
+  for (int t = 0; t < n; ++t)
+    if (!frames[t]) return HVDG_ERR_BAD_ARGUMENT;
+  const hvdg_frame_params& P = *fp;
+  if (P.frame_width < 1 || P.frame_height < 2 || P.field1_lines < 1 ||
+      P.field1_lines > P.frame_height || !(P.white_level != P.blanking_level))
+    return HVDG_ERR_BAD_GEOMETRY;
+  const hvdg_geometry g = geometry_from_params(P);
+  hvdg_status st = check_geometry(&g);
+  if (st != HVDG_OK) return st;
+  if (n == 0) return HVDG_OK;
+  hvdg::FrameVoteArgs va = vote_grid(P, g);
+  if (va.rows * va.cols == 0) {
+    for (int t = 0; t < n; ++t) votes[t] = 0;
+    return HVDG_OK;
+  }
+  cudaSetDevice(ctx->device);
+  const int fh = P.frame_height;
+  const int64_t need = frame_line_offset(P, fh - 1) + P.frame_width;
+  const int64_t stride = (int64_t)align_up((size_t)need, 128);
+  const size_t o_lines = 0;
+  const size_t o_src = align_up(sizeof(int64_t) * fh, 256);
+  const size_t o_vote = align_up(o_src + sizeof(int16_t) * stride * n, 256);
+  const size_t total = align_up(o_vote + sizeof(int) * n, 256);
+  st = ctx->arena.reserve(total, ctx->stream);
+  if (st != HVDG_OK) return st;
+  ctx->epoch += 1;
+  char* X = at<char>(ctx, 0);
+  cudaStream_t s = ctx->stream;
+  std::vector<int64_t> loff(fh);
+  for (int y = 0; y < fh; ++y) loff[y] = frame_line_offset(P, y);
+  cudaError_t e = cudaMemcpyAsync(X + o_lines, loff.data(), sizeof(int64_t) * fh,
+                                  cudaMemcpyHostToDevice, s);
+  for (int t = 0; t < n && e == cudaSuccess; ++t)
+    e = cudaMemcpyAsync(X + o_src + sizeof(int16_t) * stride * t, frames[t],
+                        sizeof(int16_t) * need, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D frames");
+  va.frames = reinterpret_cast<const int16_t*>(X + o_src);
+  va.frame_stride = stride;
+  va.line_off = reinterpret_cast<const int64_t*>(X + o_lines);
+  va.vote = reinterpret_cast<int*>(X + o_vote);
+  hvdg::launch_frame_vote(va, n, s);
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(votes, X + o_vote, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "field-order vote");
+  return HVDG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Woven-frame decode: DecodeFrameBuffer (frame_bridge.cpp:168-255, engine
 // DecodeFrame engine.cpp:141-195) and DecodeYcFrameBuffer
@@ -415,22 +475,25 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   gw.last_active_field_line = 2 * lines;
   // field order per frame (ResolveField1IsBottom, frame_bridge.cpp:152-160;
   // the Y/C path resolves auto to the format convention, :283-287). The
-  // field flagged first lands on the even woven rows (engine.cpp:55-57).
+  // field flagged first lands on the even woven rows (engine.cpp:55-57):
+  // source slot 0 of a frame has parity 0 and the split fills it with the
+  // block the order (or the device vote, k_frame_vote) puts on top.
   std::vector<hvdg_field_in> fi(2 * (size_t)n);
   for (int t = 0; t < n; ++t) {
-    bool f1_bottom = cfg->field_order == 2;
-    if (!yc && cfg->field_order == 0) f1_bottom = detect_field_parity_frame(chroma[t], P, g) < 0;
     for (int k = 0; k < 2; ++k) {
       hvdg_field_in& f = fi[2 * t + k];
       std::memset(&f, 0, sizeof(f));
       f.samples = nullptr;
       f.sample_type = HVDG_SAMPLES_F32_IRE;
-      f.parity = (k == 0) == !f1_bottom ? 0 : 1;
+      f.parity = k;
       f.geometry = &g;
       f.irls_outer = 0;
       f.cg_iterations = -1;
     }
   }
+  const hvdg::FrameVoteArgs vg = vote_grid(P, g);  // rows * cols == 0: undecided = top
+  const bool device_vote = !yc && cfg->field_order == 0 && vg.rows * vg.cols > 0;
+  const int split_order = device_vote ? 2 : (cfg->field_order == 2 ? 1 : 0);
   RunOpts opt;
   opt.weave_geom = &gw;
   opt.do_solve = !yc && cfg->cg_iterations > 0 && !cfg->monochrome;
@@ -445,7 +508,8 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   const size_t o_oc = align_up(o_ol + sizeof(int16_t) * npx * n, 256);
   const size_t o_ou = align_up(o_oc + sizeof(int16_t) * npx * n, 256);
   const size_t o_ov = align_up(o_ou + sizeof(double) * npx * n, 256);
-  const size_t xbytes = align_up(o_ov + sizeof(double) * npx * n, 256);
+  const size_t o_vote = align_up(o_ov + sizeof(double) * npx * n, 256);
+  const size_t xbytes = align_up(o_vote + sizeof(int) * n, 256);
   Staged S;
   st = stage_upload(ctx, fi.data(), 2 * n, cfg, opt, xbytes, S);
   if (st != HVDG_OK) return st;
@@ -478,6 +542,17 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   sp.codes_per_ire = cpi;
   sp.fields = at<float>(ctx, L.o_raw);
   sp.field_stride = (b.pp.size() > 1 ? b.pp[1].raw_off - b.pp[0].raw_off : 0) / (int64_t)sizeof(float);
+  sp.order = split_order;
+  sp.vote = reinterpret_cast<const int*>(X + o_vote);
+  if (device_vote) {
+    hvdg::FrameVoteArgs va = vg;
+    va.frames = sp.frames;
+    va.frame_stride = stride;
+    va.line_off = sp.line_off;
+    va.vote = reinterpret_cast<int*>(X + o_vote);
+    hvdg::launch_frame_vote(va, n, s);
+    S.launches += 1;
+  }
   hvdg::launch_frame_split(sp, n, s);
   S.launches += 1;
   st = stage_prepare(ctx, S, opt);

@@ -19,10 +19,14 @@ namespace hvdg {
 // ntsc_geometry.h:225-228; the C channel's (c - chroma_dc) / scale,
 // frame_bridge.cpp:293-301). Lines are read through FrameLineOffset, so
 // PAL's non-orthogonal lines stay registered.
+// Slot 0 of a frame takes the block the field order puts on the even woven
+// rows, so the weave itself needs no per-frame decision.
 __global__ void __launch_bounds__(256) k_frame_split(FrameSplitArgs a) {
-  const int row = blockIdx.x;  // (2 t + k) * f1 + y
+  const int row = blockIdx.x;  // (2 t + slot) * f1 + y
   const int q = row / a.f1, y = row - q * a.f1;
-  const int t = q >> 1, k = q & 1;
+  const int t = q >> 1;
+  const int swap = a.order == 2 ? (a.vote[t] < 0) : a.order;
+  const int k = (q & 1) ^ swap;
   const int flat = k == 0 ? y : a.f1 + y;
   const bool valid = k == 0 ? (y < a.f1) : (flat < a.fh);
   const int16_t* src = a.frames + (int64_t)t * a.frame_stride + (valid ? a.line_off[flat] : 0);
@@ -31,6 +35,114 @@ __global__ void __launch_bounds__(256) k_frame_split(FrameSplitArgs a) {
     const float s = valid ? (float)src[x] : a.center;
     dst[x] = __fdiv_rn(__fsub_rn(s, a.center), a.codes_per_ire);
   }
+}
+
+// DetectFieldParity on the split fields, read straight from the int16 frame
+// with the split's conversion: over field lines r (r0 step ystep) and
+// columns x (a0 step 16), b / ac / au / ad = the 4-sample means at x of
+// block 2 line r and block 1 lines r, r - 1, r + 1; ep = mean |b - (ac +
+// ad) / 2|, em = mean |b - (ac + au) / 2|; undecided when the larger is
+// <= 1e-9 or they differ by < 2 % of it, else +1 when ep < em.
+//
+// The terms are float, computed with the same rounded operations as the
+// host's restatement. The host adds them in FP64 in loop order; here they
+// are first added in parallel. Both sums of n non-negative terms are within
+// (n - 1) u / (1 - (n - 1) u) of the exact one (u = 2^-53, recursive and
+// pairwise summation alike), so when the parallel means sit further than
+// that from every threshold of the decision the host's sums decide the same
+// way. Otherwise one thread re-adds the terms in the host's order
+// (kVoteChunk at a time through shared memory) and decides on those sums:
+// the decision is the host's in every case.
+constexpr int kVoteChunk = 2048;
+constexpr int kVoteThreads = 256;
+
+__global__ void __launch_bounds__(kVoteThreads) k_frame_vote(FrameVoteArgs a) {
+  __shared__ float tp[kVoteChunk], tm[kVoteChunk];
+  __shared__ double wsum[2][kVoteThreads / 32];
+  __shared__ int exact;
+  const int t = blockIdx.x;
+  const int16_t* frame = a.frames + (int64_t)t * a.frame_stride;
+  const int nt = a.rows * a.cols;
+  auto lp = [&](int k, int row, int x) {
+    const int flat = k == 0 ? row : a.f1 + row;
+    const bool valid = k == 0 ? row < a.f1 : flat < a.fh;
+    const int16_t* src = frame + (valid ? a.line_off[flat] + x : 0);
+    float acc = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float s = valid ? (float)src[j] : a.blank;
+      const float v = __fdiv_rn(__fsub_rn(s, a.blank), a.codes_per_ire);
+      acc = j == 0 ? v : __fadd_rn(acc, v);
+    }
+    return __fmul_rn(0.25f, acc);
+  };
+  auto terms = [&](int i, float& p, float& m) {
+    const int r = a.r0 + (i / a.cols) * a.ystep;
+    const int x = a.a0 + (i % a.cols) * 16;
+    const float b = lp(1, r, x), ac = lp(0, r, x), au = lp(0, r - 1, x), ad = lp(0, r + 1, x);
+    p = fabsf(__fsub_rn(b, __fmul_rn(0.5f, __fadd_rn(ac, ad))));
+    m = fabsf(__fsub_rn(b, __fmul_rn(0.5f, __fadd_rn(ac, au))));
+  };
+  // means that decide: +1 / -1 / 0
+  auto decide = [](double ep, double em) {
+    const double lo = fmin(ep, em), hi = fmax(ep, em);
+    if (hi <= 1e-9 || __ddiv_rn(__dsub_rn(hi, lo), hi) < 0.02) return 0;
+    return ep < em ? 1 : -1;
+  };
+  double sp = 0.0, sm = 0.0;
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+    float p, m;
+    terms(i, p, m);
+    sp += (double)p;
+    sm += (double)m;
+  }
+  sp = warp_sum(sp);
+  sm = warp_sum(sm);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    wsum[0][warp] = sp;
+    wsum[1][warp] = sm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    exact = 0;
+    if (nt > 0) {
+      double ep = 0.0, em = 0.0;
+      for (int w = 0; w < kVoteThreads / 32; ++w) {
+        ep += wsum[0][w];
+        em += wsum[1][w];
+      }
+      ep /= (double)nt;
+      em /= (double)nt;
+      // relative distance of either sum (after the mean's division) from
+      // the exact value, doubled for the two summation orders, with room
+      const double tol = 8.0 * ((double)nt + 2.0) * 1.1102230246251565e-16;
+      const double lo = fmin(ep, em), hi = fmax(ep, em);
+      const bool near_floor = fabs(hi - 1e-9) <= tol * hi;
+      const bool near_ratio = hi > 0.0 && fabs((hi - lo) / hi - 0.02) <= 4.0 * tol;
+      if (near_floor || near_ratio) exact = 1;
+      else a.vote[t] = decide(ep, em);
+    } else {
+      a.vote[t] = 0;
+    }
+  }
+  __syncthreads();
+  if (!exact) return;
+  double ep = 0.0, em = 0.0;
+  for (int base = 0; base < nt; base += kVoteChunk) {
+    const int m = min(kVoteChunk, nt - base);
+    for (int j = threadIdx.x; j < m; j += blockDim.x) terms(base + j, tp[j], tm[j]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int j = 0; j < m; ++j) {
+        ep = __dadd_rn(ep, (double)tp[j]);
+        em = __dadd_rn(em, (double)tm[j]);
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    a.vote[t] = decide(__ddiv_rn(ep, (double)nt), __ddiv_rn(em, (double)nt));
 }
 
 __device__ __forceinline__ int16_t clamp_u10(float v) {  // ClampU10, frame_bridge.cpp:25-28
@@ -95,6 +207,10 @@ __global__ void __launch_bounds__(256) k_frame_out(FrameOutArgs a) {
 void launch_frame_split(const FrameSplitArgs& a, int n_frames, cudaStream_t st) {
   const int rows = 2 * n_frames * a.f1;
   if (rows > 0) k_frame_split<<<rows, 256, 0, st>>>(a);
+}
+
+void launch_frame_vote(const FrameVoteArgs& a, int n_frames, cudaStream_t st) {
+  if (n_frames > 0) k_frame_vote<<<n_frames, kVoteThreads, 0, st>>>(a);
 }
 
 void launch_frame_out(const FrameOutArgs& a, int n_frames, cudaStream_t st) {

@@ -18,11 +18,31 @@ struct FrameSplitArgs {
   int fw, fh, f1;            // samples per line, flat lines, lines of field 1
   float center;              // blanking level (composite) or chroma_dc (C channel)
   float codes_per_ire;       // (white - blanking) / 100
-  float* fields;             // 2 n planes of f1 x fw: block 1 of frame t at 2 t, block 2 at 2 t + 1
+  float* fields;             // 2 n planes of f1 x fw: slot 0 of frame t at 2 t, slot 1 at 2 t + 1
   int64_t field_stride;      // floats between consecutive planes
+  // which flat block fills slot 0 (the field woven onto the even rows):
+  // order 0 -> block 1, 1 -> block 2, 2 -> block 2 where vote[t] < 0
+  int order;
+  const int* vote;
 };
 // grid: 2 n x f1 rows
 void launch_frame_split(const FrameSplitArgs& a, int n_frames, cudaStream_t st);
+
+// The field-order vote of every frame (DetectFieldParity behind
+// ResolveField1IsBottom, frame_bridge.cpp:152-160): +1 block 1 on top, -1
+// block 2 on top, 0 undecided.
+struct FrameVoteArgs {
+  const int16_t* frames;     // as FrameSplitArgs
+  int64_t frame_stride;
+  const int64_t* line_off;
+  int fh, f1;
+  float blank, codes_per_ire;
+  int r0, ystep, rows;       // field lines r0, r0 + ystep, ... (rows of them)
+  int a0, cols;              // columns a0, a0 + 16, ... (cols of them)
+  int* vote;                 // n
+};
+// grid: n frames
+void launch_frame_vote(const FrameVoteArgs& a, int n_frames, cudaStream_t st);
 
 struct FrameOutArgs {
   // woven planes (one geometry): Y, chi, S at plane_stride apart

@@ -290,8 +290,9 @@ void split_frame_fields(const int16_t* frame, const hvdg_frame_params& fp, float
                         float* bottom);
 int detect_field_parity(const float* b1, const float* b2, const hvdg_frame_params& fp,
                         const hvdg_geometry& g);
-int detect_field_parity_frame(const int16_t* frame, const hvdg_frame_params& fp,
-                              const hvdg_geometry& g);
+hvdg::FrameVoteArgs vote_grid(const hvdg_frame_params& P, const hvdg_geometry& g);
+hvdg_status detect_field_parity_frames(hvdg_ctx* ctx, const int16_t* const* frames, int n,
+                                       const hvdg_frame_params* fp, int32_t* votes);
 std::vector<SelBox> ambiguous_boxes(const float* Y, const float* chi_ri, int h, int w,
                                     float max_area);
 hvdg_status decode_selective_boxes(hvdg_ctx* ctx, const std::vector<hvdg_field_in>& fi,

@@ -353,6 +353,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_ambiguous_boxes.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float, vp, C.c_int,
                                          P(C.c_int)]
     lib.hvdg_ambiguous_boxes.restype = C.c_int
+    lib.hvdg_detect_field_parity.argtypes = [vp, P(vp), C.c_int, P(FrameParams), vp]
+    lib.hvdg_detect_field_parity.restype = C.c_int
     lib.hvdg_decode_frame_buffer.argtypes = [vp, vp, P(FrameParams), P(Config), P(YcFrame)]
     lib.hvdg_decode_frame_buffer.restype = C.c_int
     lib.hvdg_decode_frame_buffers.argtypes = [vp, P(vp), C.c_int, P(FrameParams), P(Config),

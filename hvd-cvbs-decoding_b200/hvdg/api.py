@@ -435,6 +435,17 @@ def _decode_frame_buffers(self, frames, fp, cfg, out=None):
     return res
 
 
+def _detect_field_parity(self, frames, fp):
+    """DetectFieldParity of each int16 frame (split as SplitFrameFields
+    splits it): +1 field 1 on top, -1 field 1 at the bottom, 0 no vote."""
+    fr = [np.ascontiguousarray(f, dtype=np.int16) for f in frames]
+    votes = np.zeros(max(len(fr), 1), np.int32)
+    st = self.lib.hvdg_detect_field_parity(self._h, _ptrs(fr), len(fr), C.byref(fp),
+                                           votes.ctypes.data)
+    self._check(st, "hvdg_detect_field_parity")
+    return votes[:len(fr)]
+
+
 def _decode_yc_frame_buffer(self, luma, chroma, fp, cfg):
     """hvd::DecodeYcFrameBuffer: Y and C int16 frames -> dict(luma, chroma, u, v)."""
     y = np.ascontiguousarray(luma, dtype=np.int16)
@@ -479,6 +490,7 @@ def _drizzle_frame(self, j0, lumas, chromas, parities, cfg, scale=2):
 
 Context.drizzle_frame = _drizzle_frame
 Context.decode_frame_buffer = _decode_frame_buffer
+Context.detect_field_parity = _detect_field_parity
 Context.decode_frame_buffers = _decode_frame_buffers
 Context.decode_yc_frame_buffer = _decode_yc_frame_buffer
 Context.decode_yc_frame_buffers = _decode_yc_frame_buffers

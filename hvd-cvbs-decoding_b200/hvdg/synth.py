@@ -295,10 +295,12 @@ def mixed_batch(seed: int, n_ntsc: int = 40, n_pal: int = 24,
 
 def make_frames(seed: int, standard: int, n_frames: int, noise_sigma: float = 0.5,
                 moving: bool = False, blanking: float = 240.0, white: float = 800.0,
-                grille=None, scene: Scene | None = None):
+                grille=None, scene: Scene | None = None, field1_bottom=False):
     """Field-sequential 10-bit int16 frame buffers (the plugin's CVBS frame
     layout, frame_bridge.h:12-23): field 1 lines, then field 2 lines, with the
-    PAL extra samples on frame lines 312 and 624. Returns (frames, fields)."""
+    PAL extra samples on frame lines 312 and 624. field1_bottom (a bool, or
+    one per frame): field 1 is the bottom (odd-parity) field of the pair.
+    Returns (frames, fields)."""
     fields = make_sequence(seed, standard, 2 * n_frames, noise_sigma, moving, grille=grille,
                            scene=scene)
     g = _cabi.default_geometry(standard)
@@ -313,6 +315,9 @@ def make_frames(seed: int, standard: int, n_frames: int, noise_sigma: float = 0.
     for t in range(n_frames):
         top = to_ire(fields[2 * t].samples)
         bot = to_ire(fields[2 * t + 1].samples)
+        fb = field1_bottom[t] if isinstance(field1_bottom, (list, tuple)) else field1_bottom
+        if fb:
+            top, bot = bot, top
         lines = [top[y] for y in range(f1)] + [bot[y] for y in range(f2)]
         buf = []
         for i, ln in enumerate(lines):

@@ -345,6 +345,15 @@ hvdg_status hvdg_drizzle_frame(hvdg_ctx* ctx, const float* const* luma, const fl
                                const hvdg_config* cfg, int scale, float* out_luma,
                                float* out_chroma);
 
+/* DetectFieldParity (frame_bridge.h:170-171, frame_bridge.cpp:102-149) of
+ * n field-sequential int16 frames, each split as SplitFrameFields splits it
+ * (frame_bridge.cpp:61-99): votes[t] = +1 (field 1 is the top field), -1
+ * (field 1 is the bottom field), 0 (no confident vote). The vote the
+ * automatic field order (cfg->field_order 0) of hvdg_decode_frame_buffer(s)
+ * takes, equal to the reference's for every input. */
+hvdg_status hvdg_detect_field_parity(hvdg_ctx* ctx, const int16_t* const* frames, int n_frames,
+                                     const hvdg_frame_params* fp, int32_t* votes);
+
 /* AmbiguousBoxes (frame_bridge.cpp:402-580, the selective 3-D detector) on
  * one decoded field (luma h x w, chroma h x w x 2), host only. Writes up to
  * max_boxes boxes as (fy0, fy1, x0, x1) in active-picture coordinates and

@@ -14,11 +14,12 @@ import pytest
 from hvdg import _cabi, api, synth
 
 
-def _woven(ref, std, seed):
-    frames, _ = synth.make_frames(seed, std, 1, noise_sigma=1.0)
+def _woven(ref, std, frame, field1_bottom=False):
     fp = api.frame_params(std)
     g = _cabi.default_geometry(std)
-    top, bot = ref.split_frame_fields(frames[0], fp)
+    top, bot = ref.split_frame_fields(frame, fp)
+    if field1_bottom:
+        top, bot = bot, top     # the field on the even woven rows first
     fal, lal = g.first_active_field_line, g.last_active_line
     a0, a1 = g.active_video_start, g.active_video_end
     th_t, vs_t = ref.burst_lockin(top, g)
@@ -44,20 +45,27 @@ def _carrier(th, vs, a0, a1, double):
     return c.astype(np.complex64)
 
 
-def test_reference_pal_weave_carrier_sensitivity():
-    from oracle import ref
-    if not ref.available():
-        pytest.skip("reference engine not built")
-    std = _cabi.STD_PAL
-    g, s, th, vs = _woven(ref, std, 62)
+def pal_carrier_sensitivity(ref, frame, cfg, field1_bottom=False):
+    """Max |u / v| (codes) the reference's woven-frame init + solve moves by
+    when the carrier phase of one PAL frame is evaluated in double instead
+    of float."""
+    g, s, th, vs = _woven(ref, _cabi.STD_PAL, frame, field1_bottom)
     assert th.max() > 1000.0  # the phases the float carrier rounds
-    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6)
     chis = []
     for double in (False, True):
         c = _carrier(th, vs, g.active_video_start, g.active_video_end, double)
         _, chi0 = ref.holographic_init(s, c, g, cfg)
         _, chi = ref.variational_refine(s, c, chi0, cfg, is_pal=True)
         chis.append(chi)
-    codes = np.abs(chis[0] - chis[1]).max() * 5.6
+    return np.abs(chis[0] - chis[1]).max() * 5.6
+
+
+def test_reference_pal_weave_carrier_sensitivity():
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    frames, _ = synth.make_frames(62, _cabi.STD_PAL, 1, noise_sigma=1.0)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6)
+    codes = pal_carrier_sensitivity(ref, frames[0], cfg)
     print(f"reference u/v move under a double carrier phase: {codes:.3f} codes")
     assert 0.03 < codes < 0.15

@@ -37,8 +37,9 @@ def _ref():
     return ref
 
 
-def _compare(got, want, tag, pal=False):
-    flip_frac, uv_tol = (5e-3, 0.15) if pal else (2e-3, 0.05)
+def _compare(got, want, tag, pal=False, uv_tol=None):
+    flip_frac, uv_default = (5e-3, 0.15) if pal else (2e-3, 0.05)
+    uv_tol = uv_default if uv_tol is None else uv_tol
     for key in ("luma", "chroma"):
         d = np.abs(got[key].astype(np.int32) - want[key].astype(np.int32))
         print(f"{tag} {key}: max {d.max()} frac>0 {(d > 0).mean():.2e}")
@@ -98,6 +99,90 @@ def test_yc_frame_buffer_vs_reference(ctx, std, field_order):
     _compare(got, want, f"yc std={std} order={field_order}", pal=std == _cabi.STD_PAL)
     # luma passes straight through, line by line through FrameLineOffset
     assert np.array_equal(got["luma"], want["luma"])
+
+
+@pytest.mark.parametrize("std", [_cabi.STD_NTSC, _cabi.STD_PAL])
+def test_field1_bottom_vote_vs_reference(ctx, std):
+    """Frames whose field 1 is the bottom field: the automatic order (the
+    device vote) must weave them as the reference's DetectFieldParity does.
+    The reference's auto decode equals its forced-bottom decode (its vote
+    said bottom), the device's auto decode equals the device's forced-bottom
+    decode bit for bit, and the two implementations agree as usual -- on PAL
+    u / v within twice the reference's own movement on this frame when its
+    carrier phase is evaluated in double (0.09 codes here)."""
+    ref = _ref()
+    frames, _ = synth.make_frames(63 + std, std, 1, noise_sigma=1.0, field1_bottom=True)
+    fp = api.frame_params(std)
+    uv_tol = None
+    if std == _cabi.STD_PAL:
+        from test_frame_buffer_pins import pal_carrier_sensitivity
+        uv_tol = 2.0 * pal_carrier_sensitivity(ref, frames[0], _cfg(), field1_bottom=True)
+    want = ref.decode_frame_buffer(frames[0], fp, _cfg(field_order=0))
+    want_b = ref.decode_frame_buffer(frames[0], fp, _cfg(field_order=2))
+    for key in ("luma", "chroma", "u", "v"):
+        assert np.array_equal(want[key], want_b[key]), key
+    got = ctx.decode_frame_buffer(frames[0], fp, _cfg(field_order=0))
+    got_b = ctx.decode_frame_buffer(frames[0], fp, _cfg(field_order=2))
+    for key in ("luma", "chroma", "u", "v"):
+        assert np.array_equal(got[key], got_b[key]), key
+    _compare(got, want, f"bottom-first std={std}", pal=std == _cabi.STD_PAL, uv_tol=uv_tol)
+
+
+def _ramp_frame(fp, slope, offset):
+    """Block 1 lines at 100 + slope y codes (levels 100 / 900: 8 codes per
+    IRE, so every term of the vote is exact), block 2 at the same ramp plus
+    `offset` codes. Offsets 99 put the vote's two means exactly 2 % apart
+    (the threshold: decided), 101 just inside it (undecided)."""
+    f1, fh, fw = fp.field1_lines, fp.frame_height, fp.frame_width
+    y = np.concatenate([np.arange(f1), np.arange(fh - f1)])
+    base = (100 + (slope * y if slope > 0 else 800 + slope * y)).astype(np.int32)
+    base[f1:] += offset
+    return np.repeat(base[:, None], fw, axis=1).astype(np.int16).ravel()
+
+
+def test_detect_field_parity_vs_reference(ctx):
+    """The device vote equals the reference's DetectFieldParity on every
+    frame: synthetic top- and bottom-first frames, a flat frame (0), and
+    ramps whose means sit exactly on the 2 % threshold (the case the
+    parallel sum hands to the in-order FP64 re-sum) or just inside it."""
+    ref = _ref()
+    for std in (_cabi.STD_NTSC, _cabi.STD_PAL):
+        fp = api.frame_params(std)
+        frames = []
+        for fb in (False, True):
+            fr, _ = synth.make_frames(81 + std, std, 2, noise_sigma=1.0, moving=True,
+                                      field1_bottom=fb)
+            frames += fr
+        size = api.frame_buffer_size(fp)
+        frames.append(np.full(size, int(fp.blanking_level), np.int16))
+        votes = ctx.detect_field_parity(frames, fp)
+        want = [ref.detect_field_parity(*ref.split_frame_fields(f, fp), fp) for f in frames]
+        assert list(votes) == want, (std, list(votes), want)
+        assert want[:4] == [1, 1, -1, -1] and want[4] == 0
+    fp = api.frame_params(_cabi.STD_NTSC)
+    fp.blanking_level, fp.white_level = 100.0, 900.0
+    ramps = [_ramp_frame(fp, 2, 99), _ramp_frame(fp, -2, 99), _ramp_frame(fp, 2, 101)]
+    votes = ctx.detect_field_parity(ramps, fp)
+    want = [ref.detect_field_parity(*ref.split_frame_fields(f, fp), fp) for f in ramps]
+    assert list(votes) == want == [1, -1, 0]
+
+
+def test_mixed_field_orders_in_one_batch(ctx):
+    """A batch whose frames vote differently: each frame is woven by its own
+    vote, bit for bit as its single-frame call (band height pinned)."""
+    order = [False, True, True, False]
+    frames, _ = synth.make_frames(93, _cabi.STD_NTSC, 4, noise_sigma=1.0, moving=True,
+                                  field1_bottom=order)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    ctx.set_tuning(16, 0)
+    try:
+        batch = ctx.decode_frame_buffers(frames, fp, _cfg(field_order=0))
+        for t, f in enumerate(frames):
+            forced = ctx.decode_frame_buffer(f, fp, _cfg(field_order=2 if order[t] else 1))
+            for key in ("luma", "chroma", "u", "v"):
+                assert np.array_equal(batch[t][key], forced[key]), (t, key)
+    finally:
+        ctx.set_tuning(0, 0)
 
 
 def test_batched_frames_equal_single_calls(ctx):
