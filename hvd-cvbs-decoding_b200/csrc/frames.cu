@@ -368,6 +368,7 @@ hvdg::FrameVoteArgs vote_grid(const hvdg_frame_params& P, const hvdg_geometry& g
     for (int r = fal + 1; r + 1 < lal; r += v.ystep) ++v.rows;
     for (int x = P.active_video_start; x + 4 <= P.active_video_end; x += 16) ++v.cols;
   }
+  v.blocks = hvdg::frame_vote_blocks(v.rows * v.cols);
   return v;
 }
 
@@ -398,7 +399,9 @@ hvdg_status detect_field_parity_frames(hvdg_ctx* ctx, const int16_t* const* fram
   const size_t o_lines = 0;
   const size_t o_src = align_up(sizeof(int64_t) * fh, 256);
   const size_t o_vote = align_up(o_src + sizeof(int16_t) * stride * n, 256);
-  const size_t total = align_up(o_vote + sizeof(int) * n, 256);
+  const size_t o_arrive = align_up(o_vote + sizeof(int) * n, 256);
+  const size_t o_part = align_up(o_arrive + sizeof(int) * n, 256);
+  const size_t total = align_up(o_part + sizeof(double) * 2 * va.blocks * n, 256);
   st = ctx->arena.reserve(total, ctx->stream);
   if (st != HVDG_OK) return st;
   ctx->epoch += 1;
@@ -416,6 +419,8 @@ hvdg_status detect_field_parity_frames(hvdg_ctx* ctx, const int16_t* const* fram
   va.frame_stride = stride;
   va.line_off = reinterpret_cast<const int64_t*>(X + o_lines);
   va.vote = reinterpret_cast<int*>(X + o_vote);
+  va.arrive = reinterpret_cast<int*>(X + o_arrive);
+  va.partial = reinterpret_cast<double*>(X + o_part);
   hvdg::launch_frame_vote(va, n, s);
   e = cudaGetLastError();
   if (e == cudaSuccess)
@@ -509,7 +514,9 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   const size_t o_ou = align_up(o_oc + sizeof(int16_t) * npx * n, 256);
   const size_t o_ov = align_up(o_ou + sizeof(double) * npx * n, 256);
   const size_t o_vote = align_up(o_ov + sizeof(double) * npx * n, 256);
-  const size_t xbytes = align_up(o_vote + sizeof(int) * n, 256);
+  const size_t o_arrive = align_up(o_vote + sizeof(int) * n, 256);
+  const size_t o_part = align_up(o_arrive + sizeof(int) * n, 256);
+  const size_t xbytes = align_up(o_part + (device_vote ? sizeof(double) * 2 * vg.blocks * n : 0), 256);
   Staged S;
   st = stage_upload(ctx, fi.data(), 2 * n, cfg, opt, xbytes, S);
   if (st != HVDG_OK) return st;
@@ -550,6 +557,8 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
     va.frame_stride = stride;
     va.line_off = sp.line_off;
     va.vote = reinterpret_cast<int*>(X + o_vote);
+    va.arrive = reinterpret_cast<int*>(X + o_arrive);
+    va.partial = reinterpret_cast<double*>(X + o_part);
     hvdg::launch_frame_vote(va, n, s);
     S.launches += 1;
   }

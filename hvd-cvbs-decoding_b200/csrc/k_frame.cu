@@ -8,6 +8,8 @@
 // land on the same side of every rounding boundary as the reference's.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "hvdg_common.cuh"
 #include "k_frame.h"
 
@@ -45,22 +47,24 @@ __global__ void __launch_bounds__(256) k_frame_split(FrameSplitArgs a) {
 // <= 1e-9 or they differ by < 2 % of it, else +1 when ep < em.
 //
 // The terms are float, computed with the same rounded operations as the
-// host's restatement. The host adds them in FP64 in loop order; here they
-// are first added in parallel. Both sums of n non-negative terms are within
-// (n - 1) u / (1 - (n - 1) u) of the exact one (u = 2^-53, recursive and
-// pairwise summation alike), so when the parallel means sit further than
-// that from every threshold of the decision the host's sums decide the same
-// way. Otherwise one thread re-adds the terms in the host's order
-// (kVoteChunk at a time through shared memory) and decides on those sums:
-// the decision is the host's in every case.
+// host's restatement. The host adds them in FP64 in loop order; here the
+// `blocks` CTAs of a frame add contiguous slices of them in parallel, and
+// the frame's last CTA to finish adds the slices' sums in slice order. Both
+// sums of n non-negative terms are within (n - 1) u / (1 - (n - 1) u) of
+// the exact one (u = 2^-53, any summation order), so when the parallel
+// means sit further than that from every threshold of the decision the
+// host's sums decide the same way. Otherwise that CTA re-adds the terms in
+// the host's order (kVoteChunk at a time through shared memory, one thread
+// adding) and decides on those sums: the decision is the host's in every
+// case.
 constexpr int kVoteChunk = 2048;
 constexpr int kVoteThreads = 256;
 
 __global__ void __launch_bounds__(kVoteThreads) k_frame_vote(FrameVoteArgs a) {
   __shared__ float tp[kVoteChunk], tm[kVoteChunk];
   __shared__ double wsum[2][kVoteThreads / 32];
-  __shared__ int exact;
-  const int t = blockIdx.x;
+  __shared__ int role;  // 0: done, 1: decided by the slice sums, 2: re-add in order
+  const int t = blockIdx.x / a.blocks, blk = blockIdx.x - t * a.blocks;
   const int16_t* frame = a.frames + (int64_t)t * a.frame_stride;
   const int nt = a.rows * a.cols;
   auto lp = [&](int k, int row, int x) {
@@ -89,8 +93,11 @@ __global__ void __launch_bounds__(kVoteThreads) k_frame_vote(FrameVoteArgs a) {
     if (hi <= 1e-9 || __ddiv_rn(__dsub_rn(hi, lo), hi) < 0.02) return 0;
     return ep < em ? 1 : -1;
   };
+  // this CTA's slice
+  const int per = (nt + a.blocks - 1) / a.blocks;
+  const int i0 = blk * per, i1 = min(nt, i0 + per);
   double sp = 0.0, sm = 0.0;
-  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     float p, m;
     terms(i, p, m);
     sp += (double)p;
@@ -105,29 +112,40 @@ __global__ void __launch_bounds__(kVoteThreads) k_frame_vote(FrameVoteArgs a) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    exact = 0;
-    if (nt > 0) {
+    double bp = 0.0, bm = 0.0;
+    for (int w = 0; w < kVoteThreads / 32; ++w) {
+      bp += wsum[0][w];
+      bm += wsum[1][w];
+    }
+    a.partial[2 * blockIdx.x] = bp;
+    a.partial[2 * blockIdx.x + 1] = bm;
+    __threadfence();
+    role = atomicAdd(a.arrive + t, 1) == a.blocks - 1 ? 1 : 0;
+    if (role) {
+      __threadfence();
       double ep = 0.0, em = 0.0;
-      for (int w = 0; w < kVoteThreads / 32; ++w) {
-        ep += wsum[0][w];
-        em += wsum[1][w];
+      for (int k = 0; k < a.blocks; ++k) {
+        ep += __ldcg(a.partial + 2 * (t * a.blocks + k));
+        em += __ldcg(a.partial + 2 * (t * a.blocks + k) + 1);
       }
-      ep /= (double)nt;
-      em /= (double)nt;
-      // relative distance of either sum (after the mean's division) from
-      // the exact value, doubled for the two summation orders, with room
-      const double tol = 8.0 * ((double)nt + 2.0) * 1.1102230246251565e-16;
-      const double lo = fmin(ep, em), hi = fmax(ep, em);
-      const bool near_floor = fabs(hi - 1e-9) <= tol * hi;
-      const bool near_ratio = hi > 0.0 && fabs((hi - lo) / hi - 0.02) <= 4.0 * tol;
-      if (near_floor || near_ratio) exact = 1;
-      else a.vote[t] = decide(ep, em);
-    } else {
-      a.vote[t] = 0;
+      if (nt > 0) {
+        ep /= (double)nt;
+        em /= (double)nt;
+        // relative distance of either sum (after the mean's division) from
+        // the exact value, doubled for the two summation orders, with room
+        const double tol = 8.0 * ((double)nt + 2.0) * 1.1102230246251565e-16;
+        const double lo = fmin(ep, em), hi = fmax(ep, em);
+        const bool near_floor = fabs(hi - 1e-9) <= tol * hi;
+        const bool near_ratio = hi > 0.0 && fabs((hi - lo) / hi - 0.02) <= 4.0 * tol;
+        if (near_floor || near_ratio) role = 2;
+        else a.vote[t] = decide(ep, em);
+      } else {
+        a.vote[t] = 0;
+      }
     }
   }
   __syncthreads();
-  if (!exact) return;
+  if (role != 2) return;
   double ep = 0.0, em = 0.0;
   for (int base = 0; base < nt; base += kVoteChunk) {
     const int m = min(kVoteChunk, nt - base);
@@ -209,8 +227,14 @@ void launch_frame_split(const FrameSplitArgs& a, int n_frames, cudaStream_t st) 
   if (rows > 0) k_frame_split<<<rows, 256, 0, st>>>(a);
 }
 
+int frame_vote_blocks(int terms) {
+  return std::max(1, std::min(64, (terms + kVoteThreads - 1) / kVoteThreads));
+}
+
 void launch_frame_vote(const FrameVoteArgs& a, int n_frames, cudaStream_t st) {
-  if (n_frames > 0) k_frame_vote<<<n_frames, kVoteThreads, 0, st>>>(a);
+  if (n_frames <= 0) return;
+  cudaMemsetAsync(a.arrive, 0, sizeof(int) * n_frames, st);
+  k_frame_vote<<<n_frames * a.blocks, kVoteThreads, 0, st>>>(a);
 }
 
 void launch_frame_out(const FrameOutArgs& a, int n_frames, cudaStream_t st) {

@@ -39,9 +39,13 @@ struct FrameVoteArgs {
   float blank, codes_per_ire;
   int r0, ystep, rows;       // field lines r0, r0 + ystep, ... (rows of them)
   int a0, cols;              // columns a0, a0 + 16, ... (cols of them)
+  int blocks;                // CTAs per frame (frame_vote_blocks)
+  double* partial;           // scratch: 2 doubles per CTA
+  int* arrive;               // scratch: n counters (zeroed by the launch)
   int* vote;                 // n
 };
-// grid: n frames
+int frame_vote_blocks(int terms);
+// grid: n frames x blocks
 void launch_frame_vote(const FrameVoteArgs& a, int n_frames, cudaStream_t st);
 
 struct FrameOutArgs {
