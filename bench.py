@@ -105,11 +105,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM traffic of the solver on this workload, from the
-    committed ncu summary (profiles/solver_traffic.json), or None."""
+def profile_traffic(name):
+    """Per-launch DRAM traffic of the solver on the mixed-64 workload, from
+    the committed ncu summary (profiles/solver_traffic.json); None for the
+    other workloads (not captured) or without the summary."""
     p = REPO / "profiles" / "solver_traffic.json"
-    if p.exists():
+    if name == "mixed64" and p.exists():
         try:
             return json.loads(p.read_text()).get("bytes_per_launch")
         except Exception:
@@ -604,7 +605,8 @@ def main():
     solver_s = ms_solver / 1000.0 / args.steps
     achieved = alg_bytes_per_launch / solver_s / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": profile_traffic(), "peak_kind": peak_kind,
+            "frac": achieved / peak, "traffic": profile_traffic(args.workload),
+            "peak_kind": peak_kind,
             "kernel": "k_solver (persistent IRLS + CG)",
             "alg_bytes_per_launch": alg_bytes_per_launch, "ms_per_launch": 1000 * solver_s}
 
