@@ -111,21 +111,28 @@ __device__ __forceinline__ float2 carrier_at(const InitArgs& a, const FieldDesc&
 }
 
 // ---- columns ---------------------------------------------------------------
-// grid = (column groups over all fields); block = 128; dynamic smem 32 KiB;
+// grid = (column groups over all fields); block = 128; dynamic smem ~32 KiB;
 // up to 170 registers, 3 CTAs per SM. The column length M of a geometry is
 // 1024 (field planes: 2 hp - 1 <= 1024; 4 columns per CTA, one warp each) or
-// 2048 (woven frames, hp up to 1024; 2 columns per CTA, two warps each). Each column's cyclic convolution runs
-// in registers (col_conv_reg): a column of 1024 is a 32 x 32 four-step FFT --
-// 32-point FFTs along each lane's 32 values, twiddles, a transpose through
+// 2048 (woven frames, hp up to 1024; 2 columns per CTA, two warps each).
+// Each column's cyclic convolution runs in registers (col_conv_reg): a
+// column of 1024 is a 32 x 32 four-step FFT -- 32-point FFTs along each
+// lane's 32 values, twiddles, a transpose through
 // the column's shared-memory slot, 32-point FFTs again -- and the inverse
 // mirrors it back to natural order; a column of 2048 adds one radix-2 step
 // (decimation in time forward, in frequency inverse) between the two warps.
 constexpr int kColThreads = 128;
 constexpr int kColGroup = 4;
 constexpr int kColGroupWide = 2;
-constexpr int kColSmem = kColGroup * kColFft * (int)sizeof(float2);
-static_assert(kColGroupWide * kColFftWide * (int)sizeof(float2) == kColSmem,
-              "both column variants use the same shared-memory footprint");
+// Columns sit kColPad float2 apart beyond their length, so the 4 columns
+// of a row in the coalesced fill and write-back alternate between the two
+// halves of the shared-memory banks (2-way instead of 4-way conflicts).
+constexpr int kColPad = 8;
+constexpr int kColSmem =
+    (kColGroup * (kColFft + kColPad) > kColGroupWide * (kColFftWide + kColPad)
+         ? kColGroup * (kColFft + kColPad)
+         : kColGroupWide * (kColFftWide + kColPad)) *
+    (int)sizeof(float2);
 
 struct PairSync {  // the 64 threads of one wide column (named barrier 1 + pair)
   int id;
@@ -335,7 +342,7 @@ __device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDes
                                                const GeomDesc& gd, int f_idx, int x0, int col,
                                                int sub, int lane, Sync sync) {
   extern __shared__ float2 sm_cols[];
-  float2* buf = sm_cols + col * M;
+  float2* buf = sm_cols + col * (M + kColPad);
   for (int v = 0; v < 2; ++v) {
     const float2* src = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
     // cooperative coalesced load: thread -> (row, column-in-group)
@@ -343,7 +350,7 @@ __device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDes
       const int row = i / G, c = i % G;
       float2 val = make_float2(0.f, 0.f);
       if (row < gd.hp && x0 + c < f.w) val = src[(int64_t)row * f.pitch + x0 + c];
-      sm_cols[c * M + row] = val;
+      sm_cols[c * (M + kColPad) + row] = val;
     }
     __syncthreads();
     col_conv_reg<M>(buf, a.khat + gd.khat_col_off + v * M, a.tw_col, a.tw_row, sub, lane, sync);
@@ -353,13 +360,14 @@ __device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDes
       float2* dst = a.adj_out + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
       for (int i = threadIdx.x; i < gd.hp * G; i += blockDim.x) {
         const int y = i / G, c = i % G;
-        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * M + y];
+        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * (M + kColPad) + y];
       }
     } else {
       float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off;
       for (int i = threadIdx.x; i < f.h * G; i += blockDim.x) {
         const int y = i / G, c = i % G;
-        if (x0 + c < f.w) dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * M + y + gd.pad];
+        if (x0 + c < f.w)
+          dst[(int64_t)y * f.pitch + x0 + c] = sm_cols[c * (M + kColPad) + y + gd.pad];
       }
     }
     __syncthreads();
@@ -566,16 +574,17 @@ __device__ __forceinline__ void sym_cols_body(const InitArgs& a, const FieldDesc
       if (mode) v.y = -v.y;
       v = cmul(v, __ldg(chirp + row));
     }
-    sm_cols[c * M + row] = v;
+    sm_cols[c * (M + kColPad) + row] = v;
   }
   __syncthreads();
-  col_conv_reg<M>(sm_cols + col * M, a.khat + gd.sym_col_hhat, a.tw_col, a.tw_row, sub, lane,
-                  sync);
+  col_conv_reg<M>(sm_cols + col * (M + kColPad), a.khat + gd.sym_col_hhat, a.tw_col, a.tw_row,
+                  sub, lane, sync);
   __syncthreads();
   for (int i = threadIdx.x; i < gd.hp * G; i += blockDim.x) {
     const int row = i / G, c = i % G;
     if (x0 + c < f.w)
-      plane[(int64_t)row * f.pitch + x0 + c] = cmul(sm_cols[c * M + row], __ldg(chirp + row));
+      plane[(int64_t)row * f.pitch + x0 + c] =
+          cmul(sm_cols[c * (M + kColPad) + row], __ldg(chirp + row));
   }
 }
 
