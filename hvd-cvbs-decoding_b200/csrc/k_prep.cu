@@ -8,8 +8,8 @@
 //
 // One CTA per field for the lock-in: the per-line quadrature demodulation is
 // a warp-shuffle reduction over the burst window accumulated in FP64; the
-// per-field trajectory smoothing (two Thomas solves over <= 1024 lines) is a
-// short serial section.
+// per-field trajectory smoothing (two tridiagonal solves over <= 1024 lines)
+// runs as a parallel cyclic reduction over the CTA.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -66,30 +66,68 @@ __device__ void block_rank_select(const double* v, int n, int k, double* out) {
   __syncthreads();
 }
 
-// Thomas algorithm for (diag(a) + lam L) x = a d (TridiagSmooth,
-// lockin.cpp:133-167). Serial; called by one thread.
-__device__ void tridiag_smooth(const double* d, const double* a, int n, double lam,
-                               double* x, double* c, double* dd) {
-  if (n == 0) return;
-  if (n == 1) {
-    x[0] = a[0] > 0.0 ? d[0] : 0.0;
+// (diag(a) + lam L) x = a d, L the path-graph Laplacian (the end lines have
+// one neighbour): TridiagSmooth (lockin.cpp:65-99), which sweeps it
+// serially (Thomas). Here by parallel cyclic reduction: every step
+// eliminates the neighbours at distance s from each equation at once, so
+// after ceil(log2 n) steps each equation holds its own unknown alone. The
+// system is symmetric and diagonally dominant (a >= 0, lam > 0), where the
+// reduction is stable; the answer differs from the serial sweep by FP64
+// rounding only. All threads of the CTA call it. Scratch: two buffers each
+// of the lower, diagonal, upper and right-hand-side coefficients.
+struct TriScratch {
+  double* lo[2];
+  double* di[2];
+  double* up[2];
+  double* rh[2];
+};
+
+__device__ void tridiag_smooth(const double* d, const double* a, int n, double lam, double* x,
+                               TriScratch t) {
+  if (n <= 1) {
+    if (n == 1 && threadIdx.x == 0) x[0] = a[0] > 0.0 ? d[0] : 0.0;
+    __syncthreads();
     return;
   }
-  const double off = -lam;
-  auto diag = [&](int i) {
-    double v = a[i] + 2.0 * lam;
-    if (i == 0 || i == n - 1) v -= lam;
-    return v;
-  };
-  c[0] = off / diag(0);
-  dd[0] = a[0] * d[0] / diag(0);
-  for (int i = 1; i < n; ++i) {
-    const double m = diag(i) - off * c[i - 1];
-    if (i < n - 1) c[i] = off / m;
-    dd[i] = (a[i] * d[i] - off * dd[i - 1]) / m;
+  double *lo = t.lo[0], *di = t.di[0], *up = t.up[0], *rh = t.rh[0];
+  double *lo2 = t.lo[1], *di2 = t.di[1], *up2 = t.up[1], *rh2 = t.rh[1];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    lo[i] = i > 0 ? -lam : 0.0;
+    up[i] = i < n - 1 ? -lam : 0.0;
+    di[i] = a[i] + 2.0 * lam - ((i == 0 || i == n - 1) ? lam : 0.0);
+    rh[i] = a[i] * d[i];
   }
-  x[n - 1] = dd[n - 1];
-  for (int i = n - 2; i >= 0; --i) x[i] = dd[i] - c[i] * x[i + 1];
+  __syncthreads();
+  for (int s = 1; s < n; s <<= 1) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int im = i - s, ip = i + s;
+      double b = di[i], r = rh[i], l = 0.0, u = 0.0;
+      if (im >= 0) {
+        const double k1 = lo[i] / di[im];
+        b -= up[im] * k1;
+        r -= rh[im] * k1;
+        l = -lo[im] * k1;
+      }
+      if (ip < n) {
+        const double k2 = up[i] / di[ip];
+        b -= lo[ip] * k2;
+        r -= rh[ip] * k2;
+        u = -up[ip] * k2;
+      }
+      lo2[i] = l;
+      di2[i] = b;
+      up2[i] = u;
+      rh2[i] = r;
+    }
+    __syncthreads();
+    double* tmp;
+    tmp = lo; lo = lo2; lo2 = tmp;
+    tmp = di; di = di2; di2 = tmp;
+    tmp = up; up = up2; up2 = tmp;
+    tmp = rh; rh = rh2; rh2 = tmp;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = rh[i] / di[i];
+  __syncthreads();
 }
 
 // One CTA per field. blockDim = 256.
@@ -108,10 +146,15 @@ __global__ void __launch_bounds__(256) k_burst_lockin(const PrepDesc* __restrict
   double* tc = model + kMaxLines;
   double* tdd = tc + kMaxLines;
   double* gbuf = tdd + kMaxLines;
-  signed char* good = reinterpret_cast<signed char*>(gbuf + kMaxLines);
+  double* e0 = gbuf + kMaxLines;
+  double* e1 = e0 + kMaxLines;
+  signed char* good = reinterpret_cast<signed char*>(e1 + kMaxLines);
   signed char* sw = good + kMaxLines;
   __shared__ double s_amax, s_med, s_score[2];
+  __shared__ double s_wmax[32];
   __shared__ int s_fg, s_ngood;
+  // the smoother's scratch: arrays free once the weights a[] are formed
+  const TriScratch tri{{zr, zi}, {amp, tc}, {tdd, gbuf}, {e0, e1}};
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int x0 = p.bx0, x1 = p.bx1, n = max(0, x1 - x0);
@@ -137,23 +180,37 @@ __global__ void __launch_bounds__(256) k_burst_lockin(const PrepDesc* __restrict
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  // good lines: amplitude above 20 % of the field's maximum
+  {
     double m = 0.0;
-    for (int y = 0; y < h; ++y) m = fmax(m, amp[y]);
-    s_amax = m;
-    const double thr = m > 0.0 ? m * 0.2 : 1.0;
-    int fg = -1, ng = 0;
-    for (int y = 0; y < h; ++y) {
+    for (int y = threadIdx.x; y < h; y += blockDim.x) m = fmax(m, amp[y]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) s_wmax[warp] = m;
+    if (threadIdx.x == 0) {
+      s_fg = h;
+      s_ngood = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = 0.0;
+      for (int w = 0; w < nwarps; ++w) mm = fmax(mm, s_wmax[w]);
+      s_amax = mm;
+    }
+    __syncthreads();
+    const double thr = s_amax > 0.0 ? s_amax * 0.2 : 1.0;
+    for (int y = threadIdx.x; y < h; y += blockDim.x) {
       good[y] = amp[y] > thr;
       if (good[y]) {
-        if (fg < 0) fg = y;
-        gbuf[ng++] = amp[y];
+        atomicMin(&s_fg, y);
+        // the median below is a rank selection: the order of gbuf is free
+        gbuf[atomicAdd(&s_ngood, 1)] = amp[y];
       }
     }
-    s_fg = fg;
-    s_ngood = ng;
+    __syncthreads();
+    if (threadIdx.x == 0 && s_fg == h) s_fg = -1;
+    __syncthreads();
   }
-  __syncthreads();
   const int fg = s_fg;
   const double adv = p.adv;
   const double hpi = 0.5 * CUDART_PI;
@@ -229,15 +286,15 @@ __global__ void __launch_bounds__(256) k_burst_lockin(const PrepDesc* __restrict
     for (int y = threadIdx.x; y < h; y += blockDim.x)
       a[y] = good[y] ? fmin(fmax(amp[y] / med, 0.0), 2.0) : 0.0;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      tridiag_smooth(d, a, h, 25.0, x, tc, tdd);
-      for (int y = 0; y < h; ++y) {
-        const double r = fabs(d[y] - x[y]);
-        a[y] = a[y] * 0.15 / fmax(r, 0.15);
-      }
-      tridiag_smooth(d, a, h, 25.0, x, tc, tdd);
-      for (int y = 0; y < h; ++y) x[y] = model[y] + x[y];
+    tridiag_smooth(d, a, h, 25.0, x, tri);
+    // one Huber reweighting, then the final smooth
+    for (int y = threadIdx.x; y < h; y += blockDim.x) {
+      const double r = fabs(d[y] - x[y]);
+      a[y] = a[y] * 0.15 / fmax(r, 0.15);
     }
+    __syncthreads();
+    tridiag_smooth(d, a, h, 25.0, x, tri);
+    for (int y = threadIdx.x; y < h; y += blockDim.x) x[y] = model[y] + x[y];
     __syncthreads();
   }
   // x[] now holds theta. Chroma-phase trim (ApplyChromaPhase).
@@ -345,7 +402,7 @@ __global__ void k_crop(const PrepDesc* __restrict__ descs, const int4* __restric
   }
 }
 
-constexpr size_t kLockinSmem = 10 * kMaxLines * sizeof(double) + 2 * kMaxLines;
+constexpr size_t kLockinSmem = 12 * kMaxLines * sizeof(double) + 2 * kMaxLines;
 
 static void configure_prep_kernels_now() {
   cudaFuncSetAttribute(k_burst_lockin, cudaFuncAttributeMaxDynamicSharedMemorySize,
