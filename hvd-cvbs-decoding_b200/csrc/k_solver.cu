@@ -705,14 +705,31 @@ __device__ __noinline__ void phase_final(const SolverArgs& A, const FieldDesc& f
 // CG scalar logic (variational.cpp:519-549).
 // ---------------------------------------------------------------------------
 __device__ __noinline__ void complete_phase(const SolverArgs& A, const FieldDesc& f, int fi,
-                                            int kind, int k,
-                               int p, int lane) {
+                                            int kind, int k, int p, int lane) {
   FieldCtl* c = A.ctl + fi;
   double s[kNPart];
 #pragma unroll
   for (int i = 0; i < kNPart; ++i) s[i] = 0.0;
   if (kind == kPhaseG || kind == kPhaseI) {
-    for (int uu = f.unit_begin + lane; uu < f.unit_begin + f.unit_count; uu += 32) {
+    // lane l adds units l, l + 32, l + 64, ... in that order; four units'
+    // partials are loaded ahead of their additions, so the chain waits on
+    // one L2 round trip per four units instead of per unit (same order,
+    // same sums)
+    const int ue = f.unit_begin + f.unit_count;
+    int uu = f.unit_begin + lane;
+    for (; uu + 96 < ue; uu += 128) {
+      double v[4][kNPart];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i < kNPart; ++i)
+          v[j][i] = __ldcg(A.partials + (int64_t)(uu + 32 * j) * kNPart + i);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i < kNPart; ++i) s[i] += v[j][i];
+    }
+    for (; uu < ue; uu += 32) {
 #pragma unroll
       for (int i = 0; i < kNPart; ++i) s[i] += __ldcg(A.partials + (int64_t)uu * kNPart + i);
     }
