@@ -233,8 +233,12 @@ CONFIGS = {
                     "one batch here",
     "yc8-pal": "8 PAL 1135x625 Y/C int16 frame pairs through DecodeYcFrameBuffer "
                "(chroma-only init, default HvdConfig)",
+    "window6-ntsc": "DecodeFrameSequenceWindow (the plugin's call): 6 NTSC 910x525 int16 "
+                    "composite frames of moving content, core frames 1-4, default HvdConfig "
+                    "(adaptive 3-D strength; 2 passes, the second anchored, when it resolves "
+                    "above 0; 4 IRLS x 2 CG, fast), host buffers",
 }
-FRAME_CONFIGS = ("frames8-ntsc", "yc8-pal")
+FRAME_CONFIGS = ("frames8-ntsc", "yc8-pal", "window6-ntsc")
 
 
 def config_cfg(name):
@@ -262,6 +266,73 @@ def config_fields(name):
     return [synth.make_field(200 + i, _cabi.STD_NTSC, 0.5) for i in range(8)]
 
 
+def window_arm(args):
+    """Core frames/s of the sequence window (DecodeFrameSequenceWindow, the
+    call the decode-orc stage makes) through the public API, wall clock of
+    the synchronous call with host buffers; or the reference's own call on
+    the host cores."""
+    from hvdg import _cabi, api, synth
+    name = args.workload
+    frames, _ = synth.make_frames(302, _cabi.STD_NTSC, 6, noise_sigma=0.5, moving=True)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = api.default_config()
+    core = (1, 5)
+    ncore = core[1] - core[0]
+    npx = fp.frame_width * fp.frame_height
+    in_bytes = 2 * api.frame_buffer_size(fp) * len(frames)
+    out_bytes = (2 + 2 + 8 + 8) * npx * ncore
+    if args.impl == "reference":
+        from oracle import ref
+        if not ref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+            return 0
+        threads = os.cpu_count() or 1
+        ref.set_threads(threads)
+        times = []
+        for _ in range(max(1, min(args.steps, 3))):
+            t = time.perf_counter()
+            ref.decode_frame_sequence_window(frames, core[0], core[1], fp, cfg)
+            times.append(time.perf_counter() - t)
+        v = ncore * len(times) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": f"core frames/s ({CONFIGS[name]})",
+                          "value": v, "unit": "frames/s", "n_gpus": 1, "steps": len(times),
+                          "warmup": 0, "higher_is_better": True, "dtype": "f32",
+                          "data": "synthetic (seeded hvdg.synth)",
+                          "config": {"workload": CONFIGS[name]},
+                          "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads,
+                                           "kind": "reference",
+                                           "sample": "one 6-frame window per step"},
+                          "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return 0
+    ctx = api.Context(0)
+    for _ in range(args.warmup):
+        ctx.decode_frame_sequence_window(frames, core[0], core[1], fp, cfg)
+    wall, dev, launches = 0.0, 0.0, 0
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        ctx.decode_frame_sequence_window(frames, core[0], core[1], fp, cfg)
+        wall += time.perf_counter() - t
+        dev += ctx.last_diag.ms_total
+        launches += ctx.last_diag.kernel_launches
+    d = ctx.last_diag
+    line = {"metric": f"core frames/s ({CONFIGS[name]})", "value": ncore * args.steps / wall,
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * wall / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded hvdg.synth)",
+            "config": {"workload": CONFIGS[name], "timing": "wall clock of the synchronous "
+                       "host-buffer call (uploads, kernels, host steps, downloads)"},
+            "device_ms_per_step": dev / args.steps if dev > 0 else None,
+            "resolved_strength": d.resolved_strength, "ambiguity_ire": d.ambiguity_ire,
+            "gpu_launches": launches,
+            "e2e": {"value": ncore * args.steps / wall, "unit": "frames/s",
+                    "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes}}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def frame_arm(args, rank, world):
     """Frames/s of the woven-frame entry points through the public API (host
     int16 frames in, the four YcFrameS16 planes out; wall clock of the
@@ -270,6 +341,8 @@ def frame_arm(args, rank, world):
         return 0
     from hvdg import _cabi, api, synth
     name = args.workload
+    if name == "window6-ntsc":
+        return window_arm(args)
     cfg = api.default_config()
     n = 8
     if name == "frames8-ntsc":

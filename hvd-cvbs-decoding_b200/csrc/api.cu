@@ -422,13 +422,16 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
   // ---- de-weave + field-order vote ----
   const int nfield = 2 * n_frames;
   std::vector<std::vector<float>> ire(nfield, std::vector<float>((size_t)f1 * fw));
-  for (int t = 0; t < n_frames; ++t)
+  std::vector<int> votes(n_frames, 0);
+  const bool auto_order = cfg->field_order == 0;
+  parallel_for(n_frames, [&](int t) {
     split_frame_fields(frames[t], P, ire[2 * t].data(), ire[2 * t + 1].data());
+    if (auto_order) votes[t] = detect_field_parity(ire[2 * t].data(), ire[2 * t + 1].data(), P, g);
+  });
   bool f1_bottom = cfg->field_order == 2;
-  if (cfg->field_order == 0) {
+  if (auto_order) {
     int vote = 0;
-    for (int t = 0; t < n_frames; ++t)
-      vote += detect_field_parity(ire[2 * t].data(), ire[2 * t + 1].data(), P, g);
+    for (int t = 0; t < n_frames; ++t) vote += votes[t];
     f1_bottom = vote < 0;
   }
   const int p_first = f1_bottom ? 1 : 0;
@@ -516,8 +519,9 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
     write_debug_maps(ctx->debug_dir, base_frame_id, core_begin, core_end, f1_bottom, *dg, acc_gain,
                      Yd, car, parity, h, w);
   }
-  for (int t = core_begin; t < core_end; ++t) {
-    hvdg_yc_frame& yc = out[t - core_begin];
+  parallel_for(core_end - core_begin, [&](int ti) {
+    const int t = core_begin + ti;
+    hvdg_yc_frame& yc = out[ti];
     const size_t sz = (size_t)fw * fh;
     std::fill(yc.chroma, yc.chroma + sz, (int16_t)0);
     std::fill(yc.u_plane, yc.u_plane + sz, 0.0);
@@ -561,7 +565,7 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
         yc.u_plane[idx] = gain * (double)(-ci) * scale;
       }
     }
-  }
+  });
   return HVDG_OK;
 }
 

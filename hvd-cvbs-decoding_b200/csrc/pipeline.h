@@ -8,12 +8,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -42,6 +44,29 @@ using cd = std::complex<double>;
 // ---------------------------------------------------------------------------
 // Geometry helpers (mirror FieldGeometry, ntsc_geometry.h:142-267)
 // ---------------------------------------------------------------------------
+// fn(i) for every i in [0, n), spread over up to 16 host threads (the
+// calling one included) for the per-frame / per-pair host loops of the
+// frame bridge; returns when all are done. Each i must write only its own
+// outputs, so the results do not depend on the thread count.
+template <typename F>
+void parallel_for(int n, F&& fn) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::min(n, std::min(hw, 16));
+  if (nt <= 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  auto work = [&]() {
+    for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) fn(i);
+  };
+  std::vector<std::thread> pool;
+  pool.reserve(nt - 1);
+  for (int k = 1; k < nt; ++k) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+}
+
 inline bool uses_vswitch(const hvdg_geometry& g) {
   return g.standard == HVDG_STD_PAL || g.standard == HVDG_STD_PAL_M;
 }

@@ -32,8 +32,11 @@ float adaptive_strength(const std::vector<std::vector<float>>& Sh,
     const float2 c = make_float2(L.x * P[x].x - L.y * P[x].y, L.x * P[x].y + L.y * P[x].x);
     return L.z < 0.f ? make_float2(-c.x, c.y) : c;
   };
-  std::vector<float> ambs;
-  for (int j = 0; j + stride < nf; ++j) {
+  // one value per pair, the pairs on parallel host threads
+  const int npairs = std::max(0, nf - stride);
+  std::vector<float> pair_amb(npairs, 0.0f);
+  std::vector<char> pair_ok(npairs, 0);
+  parallel_for(npairs, [&](int j) {
     const int k = j + stride;
     std::vector<double> band_acc;
     std::vector<long> band_n;
@@ -79,12 +82,16 @@ float adaptive_strength(const std::vector<std::vector<float>>& Sh,
       if (!brms.empty()) {
         const size_t k95 = std::min(brms.size() - 1, (size_t)(0.95 * brms.size()));
         std::nth_element(brms.begin(), brms.begin() + k95, brms.end());
-        ambs.push_back(std::sqrt(brms[k95]));
+        pair_amb[j] = std::sqrt(brms[k95]);
       } else {
-        ambs.push_back(std::sqrt((float)(acc / n)));
+        pair_amb[j] = std::sqrt((float)(acc / n));
       }
+      pair_ok[j] = 1;
     }
-  }
+  });
+  std::vector<float> ambs;
+  for (int j = 0; j < npairs; ++j)
+    if (pair_ok[j]) ambs.push_back(pair_amb[j]);
   float amb = median_mean(ambs);
   const float sigma_d = nr_eps > 0.0f ? nr_eps / 3.0f : 1.0f;
   const float noise_floor = sigma_d * 0.29f;
