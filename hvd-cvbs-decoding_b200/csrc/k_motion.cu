@@ -10,10 +10,12 @@
 //
 // Bit-exact to the reference's float arithmetic: this file is compiled with
 // FMA contraction off (--fmad=false), every float / double operation is
-// issued in the reference's order, and each (pair, tile) is one thread that
-// visits the candidates in the reference's centre-out order with the same
-// partial-distortion bail-out and strict-less update, so the selected
-// vectors, sub-pel fits and confidences equal the reference's bit for bit.
+// issued in the reference's order, and each (pair, tile) visits the
+// candidates in the reference's centre-out order with the same
+// partial-distortion bail-out and strict-less update (one thread per tile,
+// or for the refinement a warp per tile that replays the visit from
+// per-row running sums), so the selected vectors, sub-pel fits and
+// confidences equal the reference's bit for bit.
 #include <cuda_runtime.h>
 
 #include "hvdg_common.cuh"
@@ -251,6 +253,137 @@ __global__ void k_me_refine(const MeField* __restrict__ mf, const MePair* __rest
   out_best[o] = best;
 }
 
+// The same refinement with a warp per (pair, tile), for tiles of up to
+// kRefineWarpTile rows. Lane l computes the SSD of refine candidates l and
+// l + 32 (visit order) row by row in the reference's order, without the
+// bail-out, keeping the running sum after every row in shared memory. Lane
+// 0 then replays the reference's visit from those sums -- kill = best *
+// (1 / bias), the first row whose running sum reaches it ends the
+// candidate with that sum, strict-less update -- so every cost, decision
+// and vector is the per-thread kernel's; lanes 0-4 then take the four
+// CostAt sums and the zero-motion cost (full sums) at once.
+constexpr int kRefineCands = 49;  // RangeFromCentre(-3, 3)^2
+constexpr int kRefineWarpTile = 64;
+
+__global__ void k_me_refine_warp(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                                 int npairs, const float* __restrict__ blur, MeArgs a,
+                                 const float* __restrict__ cdy, const float* __restrict__ cdx,
+                                 float* __restrict__ out_mdy, float* __restrict__ out_mdx,
+                                 float* __restrict__ out_sdy, float* __restrict__ out_sdx,
+                                 float* __restrict__ out_best) {
+  extern __shared__ float me_part[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpc = blockDim.x >> 5;
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int h = mc.h, w = mc.w, tile = a.tile;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const int t = blockIdx.x * wpc + warp;
+  if (t >= th * tw) return;  // the whole warp; only warp-level sync below
+  float* part = me_part + (size_t)warp * kRefineCands * tile;
+  const int ty = t / tw, tx = t % tw;
+  const int hd = h / 4, wd = w / 4;
+  const int ct = tile / 4 > 4 ? tile / 4 : 4;
+  const int hh = (hd + ct - 1) / ct, ww = (wd + ct - 1) / ct;
+  const int gy = min((ty * hh) / th, hh - 1), gx = min((tx * ww) / tw, ww - 1);
+  const float base_dy = cdy[a.coarse_off * p + gy * ww + gx] * 4.0f;
+  const float base_dx = cdx[a.coarse_off * p + gy * ww + gx] * 4.0f;
+  const float* A = blur + mc.b_off;
+  const float* B = blur + mr.b_off;
+  const int y0 = ty * tile, y1 = min((ty + 1) * tile, h);
+  const int x0 = tx * tile, x1 = min((tx + 1) * tile, w);
+  const int rows = y1 - y0;
+  const float inf = __int_as_float(0x7f800000);
+  const int rby = (int)lroundf(base_dy), rbx = (int)lroundf(base_dx);
+  for (int c = lane; c < kRefineCands; c += 32) {
+    const int sy = rby + centre_out(c / 7), sx = rbx + centre_out(c % 7);
+    float acc = 0.0f;
+    for (int y = y0; y < y1; ++y) {
+      const float* arow = A + (int64_t)y * mc.pitch;
+      const float* brow = B + (int64_t)clampi(y - sy, 0, h - 1) * mc.pitch;
+      for (int x = x0; x < x1; ++x) {
+        const float diff = arow[x] - brow[clampi(x - sx, 0, w - 1)];
+        acc += diff * diff;
+      }
+      part[c * tile + (y - y0)] = acc;
+    }
+  }
+  __syncwarp();
+  float best = inf, mdy = 0.0f, mdx = 0.0f;
+  if (lane == 0) {
+    for (int c = 0; c < kRefineCands; ++c) {
+      const int dy = centre_out(c / 7), dx = centre_out(c % 7);
+      const float bias = 1.0f + 0.02f * (float)(abs(dy) + abs(dx));
+      const float inv_bias = 1.0f / bias;
+      const float kill = best * inv_bias;
+      const float* pc = part + c * tile;
+      float se = pc[rows - 1];
+      for (int r = 0; r < rows; ++r) {
+        if (pc[r] >= kill) {
+          se = pc[r];
+          break;
+        }
+      }
+      const float cost = se * bias;
+      if (cost < best) {
+        best = cost;
+        mdy = base_dy + (float)dy;
+        mdx = base_dx + (float)dx;
+      }
+    }
+  }
+  best = __shfl_sync(0xffffffffu, best, 0);
+  mdy = __shfl_sync(0xffffffffu, mdy, 0);
+  mdx = __shfl_sync(0xffffffffu, mdx, 0);
+  // CostAt at (+-1, 0), (0, +-1) and the zero-motion cost: full sums
+  const int iy = (int)lroundf(mdy), ix = (int)lroundf(mdx);
+  float v = 0.0f;
+  if (lane < 5) {
+    int sy = iy, sx = ix;
+    if (lane == 0) sy = (int)lroundf(mdy + -1.0f);
+    if (lane == 1) sy = (int)lroundf(mdy + 1.0f);
+    if (lane == 2) sx = (int)lroundf(mdx + -1.0f);
+    if (lane == 3) sx = (int)lroundf(mdx + 1.0f);
+    if (lane == 4) sy = sx = 0;
+    v = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, sy, sx, inf) * 1.0f;
+  }
+  const float cym = __shfl_sync(0xffffffffu, v, 0);
+  const float cyp = __shfl_sync(0xffffffffu, v, 1);
+  const float cxm = __shfl_sync(0xffffffffu, v, 2);
+  const float cxp = __shfl_sync(0xffffffffu, v, 3);
+  const float cost0 = __shfl_sync(0xffffffffu, v, 4);
+  if (lane != 0) return;
+  auto parabolic = [](float cm, float c0, float cp) {
+    const float den = cm - 2.0f * c0 + cp;
+    float sub = 0.0f;
+    if (den > 1e-9f) sub = 0.5f * (cm - cp) / fmaxf(den, 1e-9f);
+    return fminf(fmaxf(sub, -0.5f), 0.5f);
+  };
+  float sdy = parabolic(cym, best, cyp);
+  float sdx = parabolic(cxm, best, cxp);
+  const float best0 = cost0 * 1.0f;
+  if (best0 < best) {
+    mdy = 0.0f;
+    mdx = 0.0f;
+    best = best0;
+  }
+  if (best > 0.85f * cost0) {
+    mdy = 0.0f;
+    mdx = 0.0f;
+    best = cost0;
+    sdy = 0.0f;
+    sdx = 0.0f;
+  }
+  const int o = a.tiles_off * p + t;
+  out_mdy[o] = mdy;
+  out_mdx[o] = mdx;
+  out_sdy[o] = sdy;
+  out_sdx[o] = sdx;
+  out_best[o] = best;
+}
+
 // ---- MotionConfidence (motion.cpp:321-387) + final vectors. One CTA per pair.
 __global__ void __launch_bounds__(256) k_me_confidence(const MeField* __restrict__ mf,
                                                        const MePair* __restrict__ pairs,
@@ -329,9 +462,15 @@ void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const 
   k_me_coarse<<<dim3((cth * ctw + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, b.dec, a,
                                                                b.cdy, b.cdx);
   const int th = (max_h + a.tile - 1) / a.tile, tw = (max_w + a.tile - 1) / a.tile;
-  k_me_refine<<<dim3((th * tw + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, b.blur, a,
-                                                             b.cdy, b.cdx, b.mdy, b.mdx, b.sdy,
-                                                             b.sdx, b.best);
+  if (a.tile <= kRefineWarpTile) {
+    const int wpc = a.tile <= 32 ? 4 : 2;
+    const int rsmem = wpc * kRefineCands * a.tile * (int)sizeof(float);
+    k_me_refine_warp<<<dim3((th * tw + wpc - 1) / wpc, npairs), 32 * wpc, rsmem, st>>>(
+        d_fields, d_pairs, npairs, b.blur, a, b.cdy, b.cdx, b.mdy, b.mdx, b.sdy, b.sdx, b.best);
+  } else {
+    k_me_refine<<<dim3((th * tw + 63) / 64, npairs), 64, 0, st>>>(
+        d_fields, d_pairs, npairs, b.blur, a, b.cdy, b.cdx, b.mdy, b.mdx, b.sdy, b.sdx, b.best);
+  }
   const int smem = 2 * th * tw * (int)sizeof(float);
   k_me_confidence<<<npairs, 256, smem, st>>>(d_fields, d_pairs, npairs, b.blur, a, b.mdy, b.mdx,
                                              b.sdy, b.sdx, b.best, b.dy, b.dx, b.conf);

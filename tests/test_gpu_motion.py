@@ -20,9 +20,12 @@ def test_motion_bit_exact_vs_reference_golden(ctx):
     assert np.array_equal(cf, d["conf"])
 
 
-@pytest.mark.parametrize("std,tile,search", [(_cabi.STD_NTSC, 32, 16), (_cabi.STD_PAL, 16, 8)])
+@pytest.mark.parametrize("std,tile,search", [(_cabi.STD_NTSC, 32, 16), (_cabi.STD_PAL, 16, 8),
+                                             (_cabi.STD_NTSC, 80, 8)])
 def test_motion_full_field_vs_reference(ctx, std, tile, search):
-    """Two consecutive same-parity fields' init luma, full field size."""
+    """Two consecutive same-parity fields' init luma, full field size. Tiles
+    up to 64 rows refine with a warp per tile (the visit replayed from
+    per-row sums), larger ones with a thread per tile: both bit-exact."""
     from oracle import ref
     if not ref.available():
         pytest.skip("reference engine not built")
