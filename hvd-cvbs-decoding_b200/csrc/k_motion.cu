@@ -25,6 +25,47 @@ namespace hvdg {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// One line of BoxBlur (motion.cpp:21-55): prefix sums c_k = c_(k-1) +
+// s_(k-1) in double, in order, and out_i = (c_min(i+r+1, n) - c_max(i-r, 0))
+// * norm, from a ring of the last 2 r + 2 prefix sums; samples `ss` apart
+// in the source, outputs `ds` apart. Output i is written as soon as the
+// prefix its window ends at exists (the ones cut by the line's end last).
+// The samples are fetched kBoxChunk at a time ahead of their additions, so
+// the in-order sum waits on one memory round trip per chunk, not per
+// sample; the values are those of the sample-by-sample loop.
+constexpr int kBoxChunk = 16;
+
+__device__ __forceinline__ void box_line(const float* __restrict__ s, int64_t ss,
+                                         float* __restrict__ d, int64_t ds, int n, int r,
+                                         double norm) {
+  double ring[32];
+  const int R = 2 * r + 2;
+  double c = 0.0;
+  ring[0] = 0.0;
+  for (int k0 = 1; k0 <= n; k0 += kBoxChunk) {
+    float v[kBoxChunk];
+#pragma unroll
+    for (int j = 0; j < kBoxChunk; ++j) v[j] = k0 + j <= n ? s[(int64_t)(k0 - 1 + j) * ss] : 0.0f;
+#pragma unroll
+    for (int j = 0; j < kBoxChunk; ++j) {
+      const int k = k0 + j;
+      if (k <= n) {
+        c = c + (double)v[j];
+        ring[k % R] = c;
+        const int i = k - r - 1;
+        if (i >= 0) {
+          const int i0 = i - r > 0 ? i - r : 0;
+          d[(int64_t)i * ds] = (float)((c - ring[i0 % R]) * norm);
+        }
+      }
+    }
+  }
+  for (int i = n - r > 0 ? n - r : 0; i < n; ++i) {
+    const int i0 = i - r > 0 ? i - r : 0;
+    d[(int64_t)i * ds] = (float)((ring[n % R] - ring[i0 % R]) * norm);
+  }
+}
+
 // ---- BoxBlur (motion.cpp:21-55): double prefix sums, constant 1/(2r+1) ----
 // Vertical pass: one thread per (field, column).
 __global__ void k_blur_v(const MeField* __restrict__ mf, int nf, const float* __restrict__ src,
@@ -38,22 +79,7 @@ __global__ void k_blur_v(const MeField* __restrict__ mf, int nf, const float* __
   const float* s = src + sb;
   float* d = dst + m.t_off;
   const double norm = (double)(1.0f / (float)(2 * r + 1));
-  // ring of prefix sums c[y] for y in [y - r, y + r + 1]
-  double ring[32];
-  const int R = 2 * r + 2;
-  double c = 0.0;
-  ring[0] = 0.0;
-  int next = 1;  // index of the next prefix value to produce (c[next])
-  for (int y = 0; y < m.h; ++y) {
-    const int y0 = y - r < 0 ? 0 : y - r;
-    const int y1 = y + r + 1 > m.h ? m.h : y + r + 1;
-    while (next <= y1) {
-      c = c + (double)s[(int64_t)(next - 1) * m.pitch + x];
-      ring[next % R] = c;
-      ++next;
-    }
-    d[(int64_t)y * m.pitch + x] = (float)((ring[y1 % R] - ring[y0 % R]) * norm);
-  }
+  box_line(s + x, m.pitch, d + x, m.pitch, m.h, r, norm);
 }
 
 // Horizontal pass: one thread per (field, row).
@@ -67,21 +93,7 @@ __global__ void k_blur_h(const MeField* __restrict__ mf, int nf, const float* __
   const float* s = src + m.t_off + (int64_t)y * m.pitch;
   float* d = dst + m.b_off + (int64_t)y * m.pitch;
   const double norm = (double)(1.0f / (float)(2 * r + 1));
-  double ring[32];
-  const int R = 2 * r + 2;
-  double c = 0.0;
-  ring[0] = 0.0;
-  int next = 1;
-  for (int x = 0; x < m.w; ++x) {
-    const int x0 = x - r < 0 ? 0 : x - r;
-    const int x1 = x + r + 1 > m.w ? m.w : x + r + 1;
-    while (next <= x1) {
-      c = c + (double)s[next - 1];
-      ring[next % R] = c;
-      ++next;
-    }
-    d[x] = (float)((ring[x1 % R] - ring[x0 % R]) * norm);
-  }
+  box_line(s, 1, d, 1, m.w, r, norm);
 }
 
 // ---- Decimate (motion.cpp:59-78): 4 x 4 block mean ---------------------------
@@ -946,21 +958,7 @@ __global__ void k_pair_blur_v(const MeField* __restrict__ mf, const MePair* __re
   const float* s = src + pix_off[p];
   float* d = dst + pix_off[p];
   const double norm = (double)(1.0f / (float)(2 * r + 1));
-  double ring[32];
-  const int R = 2 * r + 2;
-  double c = 0.0;
-  ring[0] = 0.0;
-  int next = 1;
-  for (int y = 0; y < m.h; ++y) {
-    const int y0 = y - r < 0 ? 0 : y - r;
-    const int y1 = y + r + 1 > m.h ? m.h : y + r + 1;
-    while (next <= y1) {
-      c = c + (double)s[(int64_t)(next - 1) * m.pitch + x];
-      ring[next % R] = c;
-      ++next;
-    }
-    d[(int64_t)y * m.pitch + x] = (float)((ring[y1 % R] - ring[y0 % R]) * norm);
-  }
+  box_line(s + x, m.pitch, d + x, m.pitch, m.h, r, norm);
 }
 
 __global__ void k_pair_blur_h(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
@@ -974,21 +972,7 @@ __global__ void k_pair_blur_h(const MeField* __restrict__ mf, const MePair* __re
   const float* s = src + pix_off[p] + (int64_t)y * m.pitch;
   float* d = dst + pix_off[p] + (int64_t)y * m.pitch;
   const double norm = (double)(1.0f / (float)(2 * r + 1));
-  double ring[32];
-  const int R = 2 * r + 2;
-  double c = 0.0;
-  ring[0] = 0.0;
-  int next = 1;
-  for (int x = 0; x < m.w; ++x) {
-    const int x0 = x - r < 0 ? 0 : x - r;
-    const int x1 = x + r + 1 > m.w ? m.w : x + r + 1;
-    while (next <= x1) {
-      c = c + (double)s[next - 1];
-      ring[next % R] = c;
-      ++next;
-    }
-    d[x] = (float)((ring[x1 % R] - ring[x0 % R]) * norm);
-  }
+  box_line(s, 1, d, 1, m.w, r, norm);
 }
 
 // ---------------------------------------------------------------------------

@@ -80,6 +80,8 @@ __global__ void k_env_maps(const FieldDesc* __restrict__ fields, const int* __re
 
 // (2) smooth_rows (sequence.cpp:860-889): sliding sum over [x-2, x+2] clipped
 // to the row, sqrt(mean). One thread per (field, row), both maps.
+constexpr int kEnvChunk = 16;
+
 __global__ void k_env_smooth(const FieldDesc* __restrict__ fields, const int* __restrict__ list,
                              const float* __restrict__ gmag, const float* __restrict__ lapmag,
                              float* __restrict__ vraw, float* __restrict__ traw) {
@@ -92,14 +94,29 @@ __global__ void k_env_smooth(const FieldDesc* __restrict__ fields, const int* __
     float* out = (m == 0 ? vraw : traw) + f.px_off + (int64_t)y * f.pitch;
     float acc = 0.0f;
     for (int x = 0; x < (ww < 3 ? ww : 3); ++x) acc += src[x];
-    for (int x = 0; x < ww; ++x) {
-      const int lo = x - 2, hi = x + 2;
-      if (x > 0) {
-        if (hi < ww) acc += src[hi];
-        if (lo - 1 >= 0) acc -= src[lo - 1];
+    // the entering / leaving samples of kEnvChunk steps are fetched ahead of
+    // the in-order running sum (same additions, same order)
+    for (int x0 = 0; x0 < ww; x0 += kEnvChunk) {
+      float add[kEnvChunk], sub[kEnvChunk];
+#pragma unroll
+      for (int j = 0; j < kEnvChunk; ++j) {
+        const int x = x0 + j;
+        add[j] = x > 0 && x < ww && x + 2 < ww ? src[x + 2] : 0.0f;
+        sub[j] = x > 0 && x < ww && x - 3 >= 0 ? src[x - 3] : 0.0f;
       }
-      const int n_taps = (hi < ww - 1 ? hi : ww - 1) - (lo > 0 ? lo : 0) + 1;
-      out[x] = sqrtf(acc / (float)n_taps);
+#pragma unroll
+      for (int j = 0; j < kEnvChunk; ++j) {
+        const int x = x0 + j;
+        if (x < ww) {
+          const int lo = x - 2, hi = x + 2;
+          if (x > 0) {
+            if (hi < ww) acc += add[j];
+            if (lo - 1 >= 0) acc -= sub[j];
+          }
+          const int n_taps = (hi < ww - 1 ? hi : ww - 1) - (lo > 0 ? lo : 0) + 1;
+          out[x] = sqrtf(acc / (float)n_taps);
+        }
+      }
     }
   }
 }
