@@ -421,12 +421,33 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
   const float scale = (P.white_level - P.blanking_level) / 100.0f;
   // ---- de-weave + field-order vote ----
   const int nfield = 2 * n_frames;
-  std::vector<std::vector<float>> ire(nfield, std::vector<float>((size_t)f1 * fw));
+  // host planes in the context's page-locked staging area (the window's
+  // uploads and downloads then run at the link's rate); pageable when it
+  // cannot grow
+  const int h = last_active_line(g) - g.first_active_field_line;
+  const int w = g.active_video_end - g.active_video_start;
+  // each plane 256-byte aligned
+  const size_t n_ire = align_up((size_t)f1 * fw, 64), n_y = align_up((size_t)h * w, 64);
+  const size_t staging = (size_t)nfield * (n_ire + 3 * n_y);
+  std::vector<float> pageable;
+  float* stage = nullptr;
+  if (ctx->pinned.reserve(sizeof(float) * staging) == HVDG_OK) {
+    stage = static_cast<float*>(ctx->pinned.base);
+  } else {
+    pageable.resize(staging);
+    stage = pageable.data();
+  }
+  std::vector<float*> ire(nfield), Yd(nfield), Cd(nfield);
+  for (int j = 0; j < nfield; ++j) {
+    ire[j] = stage + (size_t)j * n_ire;
+    Yd[j] = stage + (size_t)nfield * n_ire + (size_t)j * n_y;
+    Cd[j] = stage + (size_t)nfield * (n_ire + n_y) + (size_t)j * 2 * n_y;
+  }
   std::vector<int> votes(n_frames, 0);
   const bool auto_order = cfg->field_order == 0;
   parallel_for(n_frames, [&](int t) {
-    split_frame_fields(frames[t], P, ire[2 * t].data(), ire[2 * t + 1].data());
-    if (auto_order) votes[t] = detect_field_parity(ire[2 * t].data(), ire[2 * t + 1].data(), P, g);
+    split_frame_fields(frames[t], P, ire[2 * t], ire[2 * t + 1]);
+    if (auto_order) votes[t] = detect_field_parity(ire[2 * t], ire[2 * t + 1], P, g);
   });
   bool f1_bottom = cfg->field_order == 2;
   if (auto_order) {
@@ -436,24 +457,20 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
   }
   const int p_first = f1_bottom ? 1 : 0;
   // ---- window decode (burst amplitudes measured on the same upload) ----
-  const int h = last_active_line(g) - g.first_active_field_line;
-  const int w = g.active_video_end - g.active_video_start;
   std::vector<hvdg_field_in> fi(nfield);
   std::vector<hvdg_field_out> fo(nfield);
-  std::vector<std::vector<float>> Yd(nfield, std::vector<float>((size_t)h * w));
-  std::vector<std::vector<float>> Cd(nfield, std::vector<float>((size_t)h * w * 2));
   std::vector<std::vector<float>> th(nfield, std::vector<float>(f1));
   std::vector<std::vector<int8_t>> vs(nfield, std::vector<int8_t>(f1));
   for (int j = 0; j < nfield; ++j) {
     std::memset(&fi[j], 0, sizeof(fi[j]));
-    fi[j].samples = ire[j].data();
+    fi[j].samples = ire[j];
     fi[j].sample_type = HVDG_SAMPLES_F32_IRE;
     fi[j].parity = (j % 2 == 0) ? p_first : 1 - p_first;
     fi[j].geometry = &g;
     fi[j].irls_outer = 0;
     fi[j].cg_iterations = -1;
-    fo[j].luma = Yd[j].data();
-    fo[j].chroma = Cd[j].data();
+    fo[j].luma = Yd[j];
+    fo[j].chroma = Cd[j];
     fo[j].theta = th[j].data();
     fo[j].vswitch = vs[j].data();
   }

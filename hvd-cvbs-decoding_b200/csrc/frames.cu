@@ -234,17 +234,17 @@ std::vector<SelBox> ambiguous_boxes(const float* Y, const float* chi_ri, int h, 
 // Yd / Cd (h x w per field; Cd interleaved re, im).
 hvdg_status decode_selective_boxes(hvdg_ctx* ctx, const std::vector<hvdg_field_in>& fi,
                                    const hvdg_geometry& g, const hvdg_config* cfg,
-                                   std::vector<std::vector<float>>& Yd,
-                                   std::vector<std::vector<float>>& Cd) {
+                                   const std::vector<float*>& Yd,
+                                   const std::vector<float*>& Cd) {
   const int nf = (int)fi.size();
   const int h = last_active_line(g) - g.first_active_field_line;
   const int w = g.active_video_end - g.active_video_start;
   const std::vector<SelBox> boxes =
-      ambiguous_boxes(Yd[0].data(), Cd[0].data(), h, w, cfg->selective_max_area);
+      ambiguous_boxes(Yd[0], Cd[0], h, w, cfg->selective_max_area);
   if (boxes.empty()) return HVDG_OK;
   std::vector<hvdg_field_out> fo(nf);
   if (!boxes[0].valid) {  // ambiguity everywhere: the full 3-D window
-    for (int j = 0; j < nf; ++j) fo[j] = hvdg_field_out{Yd[j].data(), Cd[j].data(), nullptr, nullptr};
+    for (int j = 0; j < nf; ++j) fo[j] = hvdg_field_out{Yd[j], Cd[j], nullptr, nullptr};
     return decode_window_impl(ctx, fi.data(), nf, cfg, fo.data(), nullptr);
   }
   for (const SelBox& b : boxes) {
@@ -298,7 +298,7 @@ hvdg_status decode_selective_boxes(hvdg_ctx* ctx, const std::vector<hvdg_field_i
 // separation error survives; 0..8 IRE -> 0..255.
 void write_debug_maps(const std::string& dir, int64_t base_frame_id, int core_begin, int core_end,
                       bool f1_bottom, const hvdg_diag& d, float acc_gain,
-                      const std::vector<std::vector<float>>& Y,
+                      const std::vector<float*>& Y,
                       const std::vector<std::vector<float2>>& car, const std::vector<int>& parity,
                       int lines, int aw) {
   if (FILE* log = std::fopen((dir + "/diag.txt").c_str(), "a")) {

@@ -680,17 +680,31 @@ __device__ __noinline__ void phase_final(const SolverArgs& A, const FieldDesc& f
     } else if (l.va) {
       __stcg(A.Y + base + o, ya);
     }
-    const int64_t od = (int64_t)y * f.w + l.xa;  // dense destination index
+    // dense destination index; the caller's buffers carry no alignment
+    // promise beyond a float's, so the wide stores are taken only where the
+    // address allows them
+    const int64_t od = (int64_t)y * f.w + l.xa;
     if (f.out_c) {
-      if (l.va && l.vb && (od & 1) == 0) {
-        __stcs(reinterpret_cast<float4*>(f.out_c + od), make_float4(xa.x, xa.y, xb.x, xb.y));
+      float* oc = reinterpret_cast<float*>(f.out_c) + 2 * od;
+      const uintptr_t ac = reinterpret_cast<uintptr_t>(oc);
+      if (l.va && l.vb && (ac & 15) == 0) {
+        __stcs(reinterpret_cast<float4*>(oc), make_float4(xa.x, xa.y, xb.x, xb.y));
+      } else if ((ac & 7) == 0) {
+        if (l.va) __stcs(reinterpret_cast<float2*>(oc), xa);
+        if (l.vb) __stcs(reinterpret_cast<float2*>(oc) + 1, xb);
       } else {
-        if (l.va) __stcs(f.out_c + od, xa);
-        if (l.vb) __stcs(f.out_c + od + 1, xb);
+        if (l.va) {
+          __stcs(oc, xa.x);
+          __stcs(oc + 1, xa.y);
+        }
+        if (l.vb) {
+          __stcs(oc + 2, xb.x);
+          __stcs(oc + 3, xb.y);
+        }
       }
     }
     if (f.out_y) {
-      if (l.va && l.vb && (od & 1) == 0) {
+      if (l.va && l.vb && ((reinterpret_cast<uintptr_t>(f.out_y + od) & 7) == 0)) {
         __stcs(reinterpret_cast<float2*>(f.out_y + od), make_float2(ya, yb));
       } else {
         if (l.va) __stcs(f.out_y + od, ya);

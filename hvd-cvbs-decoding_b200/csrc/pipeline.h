@@ -322,11 +322,11 @@ std::vector<SelBox> ambiguous_boxes(const float* Y, const float* chi_ri, int h, 
                                     float max_area);
 hvdg_status decode_selective_boxes(hvdg_ctx* ctx, const std::vector<hvdg_field_in>& fi,
                                    const hvdg_geometry& g, const hvdg_config* cfg,
-                                   std::vector<std::vector<float>>& Yd,
-                                   std::vector<std::vector<float>>& Cd);
+                                   const std::vector<float*>& Yd,
+                                   const std::vector<float*>& Cd);
 void write_debug_maps(const std::string& dir, int64_t base_frame_id, int core_begin, int core_end,
                       bool f1_bottom, const hvdg_diag& d, float acc_gain,
-                      const std::vector<std::vector<float>>& Y,
+                      const std::vector<float*>& Y,
                       const std::vector<std::vector<float2>>& car, const std::vector<int>& parity,
                       int lines, int aw);
 int16_t clamp_u10(float v);

@@ -4,7 +4,10 @@ band divides), a tiny plane (8 x 16), the largest planes the device path
 takes (active width 1024: row convolution 2047 <= 2048; 480 active lines:
 padded 512, column convolution 1023 <= 1024) and one past each limit
 (HVDG_ERR_UNSUPPORTED), non-finite samples (HVDG_ERR_NONFINITE_INPUT, the
-context stays usable) and the empty batch."""
+context stays usable), the empty batch, and caller output planes that
+start off any vector boundary."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -73,3 +76,43 @@ def test_nonfinite_input_and_empty_batch(ctx):
     assert e.value.status == _cabi.ERR_NONFINITE_INPUT
     assert ctx.decode_fields([], _cfg()) == []
     _vs_oracle(ctx, g, _cabi.STD_NTSC, 76)     # the context still decodes
+
+
+def test_unaligned_caller_output_buffers(ctx):
+    """Output planes at any float offset: page-locked host planes (written by
+    the solver through their mapped addresses) and device planes, starting
+    4 bytes past a 16-byte boundary, decode exactly like aligned ones."""
+    import torch
+    g = _cabi.default_geometry(_cabi.STD_NTSC)
+    f = synth.make_field(77, _cabi.STD_NTSC, 0.5)
+    cfg = _cfg()
+    want = ctx.decode_fields([api.Field(f.samples, g, parity=0)], cfg)[0]
+    h, w = g.active_lines, g.active_width
+    ybuf = torch.zeros(h * w + 4, dtype=torch.float32, pin_memory=True)
+    cbuf = torch.zeros(2 * h * w + 4, dtype=torch.float32, pin_memory=True)
+    y = ybuf.numpy()[1:1 + h * w].reshape(h, w)
+    c = cbuf.numpy()[1:1 + 2 * h * w].view(np.complex64).reshape(h, w)
+    assert y.ctypes.data % 16 == 4 and c.ctypes.data % 16 == 4
+    got = ctx.decode_fields([api.Field(f.samples, g, parity=0)], cfg, out=[api.Decoded(y, c)])[0]
+    assert np.array_equal(got.luma, want.luma) and np.array_equal(got.chroma, want.chroma)
+    # device-resident buffers at the same offsets
+    d_in = torch.from_numpy(f.samples.view(np.int16)).cuda()
+    d_y = torch.zeros(h * w + 4, dtype=torch.float32, device="cuda")
+    d_c = torch.zeros(2 * h * w + 4, dtype=torch.float32, device="cuda")
+    fin = (_cabi.FieldIn * 1)()
+    fout = (_cabi.FieldOut * 1)()
+    fin[0].samples = d_in.data_ptr()
+    fin[0].sample_type = _cabi.SAMPLES_U16
+    fin[0].parity = 0
+    fin[0].blanking_level = 16384.0
+    fin[0].white_level = 51200.0
+    fin[0].geometry = C.pointer(g)
+    fin[0].irls_outer = 0
+    fin[0].cg_iterations = -1
+    fout[0].luma = d_y.data_ptr() + 4
+    fout[0].chroma = d_c.data_ptr() + 4
+    ctx.decode_fields_device(fin, fout, 1, cfg)
+    torch.cuda.synchronize()
+    gy = d_y.cpu().numpy()[1:1 + h * w].reshape(h, w)
+    gc = d_c.cpu().numpy()[1:1 + 2 * h * w].view(np.complex64).reshape(h, w)
+    assert np.array_equal(gy, want.luma) and np.array_equal(gc, want.chroma)
