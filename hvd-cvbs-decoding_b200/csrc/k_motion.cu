@@ -178,6 +178,81 @@ __global__ void k_me_coarse(const MeField* __restrict__ mf, const MePair* __rest
   cdx[a.coarse_off * p + t] = bdx;
 }
 
+// The coarse pass with a warp per (pair, coarse tile) when the candidates
+// and tile rows fit (n^2 <= kCoarseWarpCands, ct <= kCoarseWarpRows): lanes
+// sum the candidates' SSD row by row in the reference's order, one lane
+// replays the visit from the per-row running sums (the zero vector, whose
+// cost needs the full sum, is never cut), as in k_me_refine_warp.
+constexpr int kCoarseWarpCands = 128;
+constexpr int kCoarseWarpRows = 16;
+
+__global__ void k_me_coarse_warp(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
+                                 int npairs, const float* __restrict__ dec, MeArgs a,
+                                 float* __restrict__ cdy, float* __restrict__ cdx) {
+  extern __shared__ float mc_part[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpc = blockDim.x >> 5;
+  const int p = blockIdx.y;
+  if (p >= npairs) return;
+  const MePair pr = pairs[p];
+  const MeField mc = mf[pr.cur], mr = mf[pr.ref];
+  const int hd = mc.h / 4, wd = mc.w / 4;
+  const int ct = a.tile / 4 > 4 ? a.tile / 4 : 4;
+  const int th = (hd + ct - 1) / ct, tw = (wd + ct - 1) / ct;
+  const int t = blockIdx.x * wpc + warp;
+  if (t >= th * tw) return;  // the whole warp; only warp-level sync below
+  const int ty = t / tw, tx = t % tw;
+  const int cs = (a.search + 3) / 4 > 1 ? (a.search + 3) / 4 : 1;
+  const int n = 2 * cs + 1;
+  const int ncand = n * n;
+  float* part = mc_part + (size_t)warp * kCoarseWarpCands * kCoarseWarpRows;
+  const float* A = dec + mc.d_off;
+  const float* B = dec + mr.d_off;
+  const int y0 = ty * ct, y1 = min((ty + 1) * ct, hd);
+  const int x0 = tx * ct, x1 = min((tx + 1) * ct, wd);
+  const int rows = y1 - y0;
+  for (int c = lane; c < ncand; c += 32) {
+    const int sy = centre_out(c / n), sx = centre_out(c % n);
+    float acc = 0.0f;
+    for (int y = y0; y < y1; ++y) {
+      const float* arow = A + (int64_t)y * mc.dpitch;
+      const float* brow = B + (int64_t)clampi(y - sy, 0, hd - 1) * mc.dpitch;
+      for (int x = x0; x < x1; ++x) {
+        const float diff = arow[x] - brow[clampi(x - sx, 0, wd - 1)];
+        acc += diff * diff;
+      }
+      part[c * kCoarseWarpRows + (y - y0)] = acc;
+    }
+  }
+  __syncwarp();
+  if (lane != 0) return;
+  float best = __int_as_float(0x7f800000);
+  float bdy = 0.0f, bdx = 0.0f;
+  for (int c = 0; c < ncand; ++c) {
+    const int dy = centre_out(c / n), dx = centre_out(c % n);
+    const float bias = 1.0f + 0.02f * (float)(abs(dy) + abs(dx));
+    const float inv_bias = 1.0f / bias;
+    const bool exact = dy == 0 && dx == 0;
+    const float kill = exact ? __int_as_float(0x7f800000) : best * inv_bias;
+    const float* pc = part + c * kCoarseWarpRows;
+    float se = pc[rows - 1];
+    for (int r = 0; r < rows; ++r) {
+      if (pc[r] >= kill) {
+        se = pc[r];
+        break;
+      }
+    }
+    const float cost = se * bias;
+    if (cost < best) {
+      best = cost;
+      bdy = (float)dy;
+      bdx = (float)dx;
+    }
+  }
+  cdy[a.coarse_off * p + t] = bdy;
+  cdx[a.coarse_off * p + t] = bdx;
+}
+
 // ---- full-res refinement, sub-pel fit, zero / margin rule (motion.cpp:415-473)
 __global__ void k_me_refine(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
                             int npairs, const float* __restrict__ blur, MeArgs a,
@@ -471,8 +546,16 @@ void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const 
   k_decimate<<<dim3(((max_h / 4) * (max_w / 4) + 255) / 256, nf), 256, 0, st>>>(d_fields, nf, b.blur, b.dec);
   const int ct = a.tile / 4 > 4 ? a.tile / 4 : 4;
   const int cth = ((max_h / 4) + ct - 1) / ct, ctw = ((max_w / 4) + ct - 1) / ct;
-  k_me_coarse<<<dim3((cth * ctw + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs, b.dec, a,
-                                                               b.cdy, b.cdx);
+  const int cn = 2 * ((a.search + 3) / 4 > 1 ? (a.search + 3) / 4 : 1) + 1;
+  if (cn * cn <= kCoarseWarpCands && ct <= kCoarseWarpRows) {
+    const int wpc = 4;
+    const int csmem = wpc * kCoarseWarpCands * kCoarseWarpRows * (int)sizeof(float);
+    k_me_coarse_warp<<<dim3((cth * ctw + wpc - 1) / wpc, npairs), 32 * wpc, csmem, st>>>(
+        d_fields, d_pairs, npairs, b.dec, a, b.cdy, b.cdx);
+  } else {
+    k_me_coarse<<<dim3((cth * ctw + 63) / 64, npairs), 64, 0, st>>>(d_fields, d_pairs, npairs,
+                                                                 b.dec, a, b.cdy, b.cdx);
+  }
   const int th = (max_h + a.tile - 1) / a.tile, tw = (max_w + a.tile - 1) / a.tile;
   if (a.tile <= kRefineWarpTile) {
     const int wpc = a.tile <= 32 ? 4 : 2;
