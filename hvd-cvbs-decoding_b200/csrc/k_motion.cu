@@ -66,6 +66,55 @@ __device__ __forceinline__ void box_line(const float* __restrict__ s, int64_t ss
   }
 }
 
+// box_line along rows for one warp: lane l runs row l of a 32-row band
+// (`rows` of them exist). The band's samples arrive 32 columns at a time
+// through shared memory, each load instruction reading one row's 32
+// consecutive columns, so the rows' in-order prefix sums wait on one
+// coalesced round trip per 32 columns.
+__device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float* __restrict__ d,
+                                              int64_t pitch, int rows, int n, int r,
+                                              double norm) {
+  __shared__ float tile[32][33];
+  const int lane = threadIdx.x & 31;
+  const bool live = lane < rows;
+  float* drow = d + (int64_t)lane * pitch;
+  double ring[32];
+  const int R = 2 * r + 2;
+  double c = 0.0;
+  ring[0] = 0.0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    {
+      // all 32 loads issued before the first store
+      float v[32];
+      const bool col = c0 + lane < n;
+#pragma unroll
+      for (int q = 0; q < 32; ++q) v[q] = col && q < rows ? s[(int64_t)q * pitch + c0 + lane] : 0.0f;
+#pragma unroll
+      for (int q = 0; q < 32; ++q) tile[q][lane] = v[q];
+    }
+    __syncwarp();
+    if (live) {
+      for (int j = 0; j < 32; ++j) {
+        const int k = c0 + j + 1;
+        if (k > n) break;
+        c = c + (double)tile[lane][j];
+        ring[k % R] = c;
+        const int i = k - r - 1;
+        if (i >= 0) {
+          const int i0 = i - r > 0 ? i - r : 0;
+          drow[i] = (float)((c - ring[i0 % R]) * norm);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (!live) return;
+  for (int i = n - r > 0 ? n - r : 0; i < n; ++i) {
+    const int i0 = i - r > 0 ? i - r : 0;
+    drow[i] = (float)((ring[n % R] - ring[i0 % R]) * norm);
+  }
+}
+
 // ---- BoxBlur (motion.cpp:21-55): double prefix sums, constant 1/(2r+1) ----
 // Vertical pass: one thread per (field, column).
 __global__ void k_blur_v(const MeField* __restrict__ mf, int nf, const float* __restrict__ src,
@@ -82,18 +131,17 @@ __global__ void k_blur_v(const MeField* __restrict__ mf, int nf, const float* __
   box_line(s + x, m.pitch, d + x, m.pitch, m.h, r, norm);
 }
 
-// Horizontal pass: one thread per (field, row).
+// Horizontal pass: one warp per (field, 32-row band).
 __global__ void k_blur_h(const MeField* __restrict__ mf, int nf, const float* __restrict__ src,
                          float* __restrict__ dst, int r) {
   const int f = blockIdx.y;
   if (f >= nf) return;
   const MeField m = mf[f];
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
-  if (y >= m.h) return;
-  const float* s = src + m.t_off + (int64_t)y * m.pitch;
-  float* d = dst + m.b_off + (int64_t)y * m.pitch;
+  const int y0 = blockIdx.x * 32;
+  if (y0 >= m.h) return;
   const double norm = (double)(1.0f / (float)(2 * r + 1));
-  box_line(s, 1, d, 1, m.w, r, norm);
+  box_rows_warp(src + m.t_off + (int64_t)y0 * m.pitch, dst + m.b_off + (int64_t)y0 * m.pitch,
+                m.pitch, min(32, m.h - y0), m.w, r, norm);
 }
 
 // ---- Decimate (motion.cpp:59-78): 4 x 4 block mean ---------------------------
@@ -542,7 +590,7 @@ void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const 
   const int r = 2;
   // blur every field's luma (A = blur(y_cur), B = blur(y_ref) share per field)
   k_blur_v<<<dim3((max_w + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.luma, b.tmp, r, 0);
-  k_blur_h<<<dim3((max_h + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.tmp, b.blur, r);
+  k_blur_h<<<dim3((max_h + 31) / 32, nf), 32, 0, st>>>(d_fields, nf, b.tmp, b.blur, r);
   k_decimate<<<dim3(((max_h / 4) * (max_w / 4) + 255) / 256, nf), 256, 0, st>>>(d_fields, nf, b.blur, b.dec);
   const int ct = a.tile / 4 > 4 ? a.tile / 4 : 4;
   const int cth = ((max_h / 4) + ct - 1) / ct, ctw = ((max_w / 4) + ct - 1) / ct;
@@ -1044,18 +1092,18 @@ __global__ void k_pair_blur_v(const MeField* __restrict__ mf, const MePair* __re
   box_line(s + x, m.pitch, d + x, m.pitch, m.h, r, norm);
 }
 
+// one warp per (pair, 32-row band)
 __global__ void k_pair_blur_h(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
                               int npairs, const float* __restrict__ src, float* __restrict__ dst,
                               const int64_t* __restrict__ pix_off, int r) {
   const int p = blockIdx.y;
   if (p >= npairs) return;
   const MeField m = mf[pairs[p].cur];
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
-  if (y >= m.h) return;
-  const float* s = src + pix_off[p] + (int64_t)y * m.pitch;
-  float* d = dst + pix_off[p] + (int64_t)y * m.pitch;
+  const int y0 = blockIdx.x * 32;
+  if (y0 >= m.h) return;
   const double norm = (double)(1.0f / (float)(2 * r + 1));
-  box_line(s, 1, d, 1, m.w, r, norm);
+  box_rows_warp(src + pix_off[p] + (int64_t)y0 * m.pitch, dst + pix_off[p] + (int64_t)y0 * m.pitch,
+                m.pitch, min(32, m.h - y0), m.w, r, norm);
 }
 
 // ---------------------------------------------------------------------------
@@ -1300,9 +1348,9 @@ void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, 
     k_pair_blur_v<<<dim3((max_w + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
                                                                      v.conf_tmp, v.conf_px,
                                                                      v.pix_off, 8);
-    k_pair_blur_h<<<dim3((max_h + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
-                                                                     v.conf_px, v.conf_tmp,
-                                                                     v.pix_off, 8);
+    k_pair_blur_h<<<dim3((max_h + 31) / 32, npairs), 32, 0, st>>>(d_fields, d_pairs, npairs,
+                                                                  v.conf_px, v.conf_tmp,
+                                                                  v.pix_off, 8);
     cudaMemcpyAsync(v.conf_px, v.conf_tmp, v.conf_bytes, cudaMemcpyDeviceToDevice, st);
   }
 }
@@ -1359,8 +1407,8 @@ void launch_coherence_gate(const MeField* d_fields, const MePair* d_pairs, int n
     float* ch = b.terms + c * b.chan_stride;
     k_pair_blur_v<<<dim3((max_w + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs, ch,
                                                                     b.tmp, b.pix_off, 6);
-    k_pair_blur_h<<<dim3((max_h + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
-                                                                    b.tmp, ch, b.pix_off, 6);
+    k_pair_blur_h<<<dim3((max_h + 31) / 32, npairs), 32, 0, st>>>(d_fields, d_pairs, npairs,
+                                                                 b.tmp, ch, b.pix_off, 6);
   }
   k_coh_apply<<<grid, 128, 0, st>>>(d_fields, d_pairs, npairs, b, gate);
 }
