@@ -75,13 +75,18 @@ __device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float
                                               int64_t pitch, int rows, int n, int r,
                                               double norm) {
   __shared__ float tile[32][33];
+  // each lane's ring of the last R = 2 r + 2 prefix sums (R <= 32); the
+  // prefix a window starts at, k - 2 r - 1, sits in the slot after prefix
+  // k's, so the slots advance by one per step without a division
+  __shared__ double sring[32][33];
   const int lane = threadIdx.x & 31;
   const bool live = lane < rows;
   float* drow = d + (int64_t)lane * pitch;
-  double ring[32];
+  double* ring = sring[lane];
   const int R = 2 * r + 2;
   double c = 0.0;
   ring[0] = 0.0;
+  int kr = 0;  // slot of prefix k
   for (int c0 = 0; c0 < n; c0 += 32) {
     {
       // all 32 loads issued before the first store
@@ -98,20 +103,26 @@ __device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float
         const int k = c0 + j + 1;
         if (k > n) break;
         c = c + (double)tile[lane][j];
-        ring[k % R] = c;
+        kr = kr + 1 == R ? 0 : kr + 1;
+        ring[kr] = c;
         const int i = k - r - 1;
         if (i >= 0) {
-          const int i0 = i - r > 0 ? i - r : 0;
-          drow[i] = (float)((c - ring[i0 % R]) * norm);
+          // window start max(i - r, 0): prefix k - R + 1 (the next slot) or 0
+          const double c0v = i - r > 0 ? ring[kr + 1 == R ? 0 : kr + 1] : ring[0];
+          drow[i] = (float)((c - c0v) * norm);
         }
       }
     }
     __syncwarp();
   }
   if (!live) return;
+  // outputs whose window is cut by the end: prefix n is in slot kr
   for (int i = n - r > 0 ? n - r : 0; i < n; ++i) {
     const int i0 = i - r > 0 ? i - r : 0;
-    drow[i] = (float)((ring[n % R] - ring[i0 % R]) * norm);
+    // slot of prefix i0: kr - (n - i0), wrapped
+    int si = kr - (n - i0) % R;
+    if (si < 0) si += R;
+    drow[i] = (float)((c - ring[i0 > 0 ? si : 0]) * norm);
   }
 }
 
