@@ -169,7 +169,10 @@ typedef struct hvdg_field_in {
   int32_t cg_iterations;      /* <  0: cfg->cg_iterations */
 } hvdg_field_in;
 
-/* One decoded field out (DecodedField, sequence.h:64-69). Caller-owned. */
+/* One decoded field out (DecodedField, sequence.h:64-69). Caller-owned;
+ * planes need only a float's alignment. Page-locked host planes (and device
+ * planes on the _device entry points) are written by the solver directly as
+ * each field finishes; pageable ones are copied after the launch. */
 typedef struct hvdg_field_out {
   float* luma;     /* active_lines x active_width, IRE */
   float* chroma;   /* active_lines x active_width x 2 (re, im), chi = V - iU, IRE */
