@@ -35,6 +35,10 @@ void init_tables_for(const hvdg_geometry& g, std::vector<float2>* khat_row_col,
                      std::vector<float2>* col_phasor, std::vector<float2>* tw_row,
                      std::vector<float2>* tw_col, int* hp, int* pad);
 
+// The geometry checks every field entry point applies (arguments, ranges,
+// device-path limits), as a status.
+hvdg_status check_field_geometry(const hvdg_geometry* g);
+
 // Records a CUDA failure in the context and maps it to a status.
 hvdg_status cuda_fail(hvdg_ctx* ctx, cudaError_t e, const char* what);
 

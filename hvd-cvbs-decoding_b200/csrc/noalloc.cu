@@ -10,10 +10,16 @@
 //
 // The array is HVDG_NOALLOC_SCRATCH_BYTES (32 MiB). It is part of the
 // module, so every GPU that loads this library holds it until the process
-// exits, whether or not the entry point is ever called. Host code cannot use
-// the symbol itself as a device address; the first call on each device looks
-// the address up with cudaGetSymbolAddress (with that device current) and
-// caches it, so that first call should come before any stream capture. The
+// exits, whether or not the entry point is ever called. The geometries the
+// init accepts at all (row convolution 2048 points: at most 1024 active
+// samples; column convolution 1024 points: at most 480 active lines) need at
+// most ~24 MiB of it (kWorstLayout below), so the array's size never limits
+// a field the context path takes. Host code cannot use the symbol itself as
+// a device address; the first call on each device looks the address up with
+// cudaGetSymbolAddress (with that device current) and caches it for the
+// life of the process, so that first call should come before any stream
+// capture, and a cudaDeviceReset of that device between calls is not
+// supported (the module may load again at another address). The
 // array keeps the last call's contents; every region a call reads is written
 // by that call first (the padded composite plane is cleared explicitly).
 // All calls share the one array, so calls whose work overlaps on the GPU
@@ -61,7 +67,18 @@ hvdg_status scratch_address(void** out) {
   return HVDG_OK;
 }
 
-size_t up(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t up(size_t x) { return (x + 255) / 256 * 256; }
+
+// The layout below at the largest plane the init accepts (w <= 1024 active
+// samples, h + 2 pad <= 512 padded lines), tables included: the scratch
+// array holds every accepted field.
+constexpr size_t kMaxW = hvdg::kRowFft / 2, kMaxHp = (hvdg::kColFft + 1) / 2;
+constexpr size_t kWorstLayout =
+    up(sizeof(hvdg::FieldDesc)) + up(sizeof(hvdg::GeomDesc)) + up(16 * kMaxHp) +
+    up(8 * kMaxW) + up(8 * (2 * hvdg::kRowFft + hvdg::kColFft)) + up(8 * hvdg::kRowFft) +
+    up(8 * hvdg::kColFft) + up(4 * (kMaxHp + 1 + kMaxW + 1 + kMaxHp * kMaxW + 1)) + up(8) +
+    2 * up(4 * kMaxHp * kMaxW) + 3 * up(8 * kMaxHp * kMaxW) + up(8 * 2 * kMaxHp * kMaxW);
+static_assert(kWorstLayout <= kScratchBytes, "scratch array smaller than the largest field");
 
 }  // namespace
 
@@ -72,14 +89,15 @@ extern "C" hvdg_status hvdg_holographic_init_noalloc(const float* s, const float
   using hvdg::FieldDesc;
   using hvdg::GeomDesc;
   if (!s || !theta_active || !g || !luma0 || !chi0) return HVDG_ERR_BAD_ARGUMENT;
+  // the same checks (and statuses) as hvdg_holographic_init, then the
+  // init's own convolution lengths
+  const hvdg_status gst = hvdg::check_field_geometry(g);
+  if (gst != HVDG_OK) return gst;
   const bool vsw = g->standard == HVDG_STD_PAL || g->standard == HVDG_STD_PAL_M;
   if (vsw && !vswitch_active) return HVDG_ERR_BAD_ARGUMENT;
   const int lal = g->last_active_field_line != 0 ? g->last_active_field_line : g->field_height;
   const int h = lal - g->first_active_field_line;
   const int w = g->active_video_end - g->active_video_start;
-  if (g->active_video_start < 0 || g->active_video_end > g->field_width || w < 2 ||
-      g->first_active_field_line < 0 || lal > g->field_height || h < 2 || !(g->sample_rate > 0.0))
-    return HVDG_ERR_BAD_GEOMETRY;
   const int pad0 = h - 1 < hvdg::kInitPad ? h - 1 : hvdg::kInitPad;
   if (2 * w - 1 > hvdg::kRowFft || 2 * (h + 2 * pad0) - 1 > hvdg::kColFft) return HVDG_ERR_UNSUPPORTED;
 
@@ -114,7 +132,7 @@ extern "C" hvdg_status hvdg_holographic_init_noalloc(const float* s, const float
   const size_t o_c1 = take(sizeof(float2) * h * pitch);
   const size_t o_c2 = take(sizeof(float2) * h * pitch);
   const size_t o_row = take(sizeof(float2) * 2 * (size_t)hp * pitch);
-  if (o > kScratchBytes) return HVDG_ERR_UNSUPPORTED;  // beyond the fixed scratch
+  if (o > kWorstLayout) return HVDG_ERR_UNSUPPORTED;  // cannot happen after the checks above
 
   void* vbase = nullptr;
   hvdg_status st = scratch_address(&vbase);

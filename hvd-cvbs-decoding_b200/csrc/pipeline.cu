@@ -1081,6 +1081,8 @@ namespace hvdg {
 using namespace hvdg_pipe;
 
 
+hvdg_status check_field_geometry(const hvdg_geometry* g) { return check_geometry(g); }
+
 // Init tables of one geometry (the same tables run_batch uploads), for
 // translation units that launch the init kernels on their own memory.
 void init_tables_for(const hvdg_geometry& g, std::vector<float2>* khat_row_col,

@@ -438,8 +438,9 @@ hvdg_status hvdg_decode_fields_adjoint(hvdg_ctx* ctx, const hvdg_field_in* field
 /* ------------------------------------------------------------------------ */
 
 /* No counterpart in the reference: this is an addition of this library.
- * HolographicInit (same kernels and results as hvdg_holographic_init) for
- * callers that cannot allocate device memory -- e.g. a plugin inside a host
+ * HolographicInit (the same kernels and results as hvdg_holographic_init with
+ * cfg->symmetry_variant = 0; the spectral-symmetry third variant is not run)
+ * for callers that cannot allocate device memory -- e.g. a plugin inside a host
  * application that owns the CUDA allocator, or a real-time path that must
  * not risk a cudaMalloc stall. It takes no context and calls no cudaMalloc,
  * cudaFree or allocating library routine: its scratch is one file-scope
@@ -447,12 +448,15 @@ hvdg_status hvdg_decode_fields_adjoint(hvdg_ctx* ctx, const hvdg_field_in* field
  * library holds until the process exits. Inputs and outputs are host
  * buffers, as for hvdg_holographic_init; work runs on the legacy default
  * stream of the current device and the call returns when it is done.
- * Limits: a field whose scratch layout exceeds the array (roughly more than
- * 1024 active samples or about 480 active lines) is rejected with
- * HVDG_ERR_UNSUPPORTED. The first call on each device looks up the array's
- * device address; make that first call before any stream capture. All calls
- * share the one array and it keeps the last call's contents, so calls that
- * overlap on the GPU (from several host threads) race: serialise them. */
+ * Limits: geometry is checked as for hvdg_holographic_init (same statuses);
+ * fields past the init's convolution lengths (more than 1024 active samples,
+ * or more than 480 active lines) are rejected with HVDG_ERR_UNSUPPORTED, and
+ * every field within them fits the array. The first call on each device
+ * looks up the array's device address and keeps it for the life of the
+ * process: make that first call before any stream capture, and do not
+ * cudaDeviceReset that device between calls. All calls share the one array
+ * and it keeps the last call's contents, so calls that overlap on the GPU
+ * (from several host threads) race: serialise them. */
 #define HVDG_NOALLOC_SCRATCH_BYTES (32u << 20)
 hvdg_status hvdg_holographic_init_noalloc(const float* s, const float* theta_active,
                                           const int8_t* vswitch_active,

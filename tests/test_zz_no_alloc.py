@@ -7,7 +7,10 @@ it through the C ABI twice in a row -- an NTSC field, then a PAL field, which
 reuses the same scratch with a different layout -- and checks each result
 against the context-based hvdg_holographic_init on the same inputs. It sits
 in its own file named to be collected last; it passes alone in a fresh
-process and after the other tests."""
+process and after the other tests. Its no-alloc calls come before it opens
+any context, so run alone it also covers the cold path: the first call in a
+process does the per-device set-up (the array's address, the init kernels'
+attributes and twiddle constants) itself."""
 import ctypes as C
 
 import numpy as np
@@ -32,15 +35,19 @@ def _prepared(std, seed):
 
 def test_noalloc_init_matches_context_init_twice():
     lib = _cabi.load_library()
+    cases = [(_cabi.STD_NTSC, 31), (_cabi.STD_PAL, 32)]
+    got = []
+    for std, seed in cases:     # no context exists yet in this test
+        g, cfg, s, th, sw = _prepared(std, seed)
+        y = np.zeros_like(s)
+        c = np.zeros(s.shape, np.complex64)
+        st = lib.hvdg_holographic_init_noalloc(s.ctypes.data, th.ctypes.data, sw.ctypes.data,
+                                               C.byref(g), y.ctypes.data, c.ctypes.data)
+        assert st == _cabi.OK, _cabi.STATUS_NAMES.get(st, st)
+        got.append((g, cfg, s, th, sw, y, c))
     with api.Context(0) as ctx:
-        for std, seed in ((_cabi.STD_NTSC, 31), (_cabi.STD_PAL, 32)):
-            g, cfg, s, th, sw = _prepared(std, seed)
+        for g, cfg, s, th, sw, y, c in got:
             y_ref, c_ref = ctx.holographic_init(s, th, sw, g, cfg)
-            y = np.zeros_like(s)
-            c = np.zeros(s.shape, np.complex64)
-            st = lib.hvdg_holographic_init_noalloc(s.ctypes.data, th.ctypes.data, sw.ctypes.data,
-                                                   C.byref(g), y.ctypes.data, c.ctypes.data)
-            assert st == _cabi.OK, _cabi.STATUS_NAMES.get(st, st)
             assert np.abs(y - y_ref).max() <= 1e-5
             assert np.abs(c - c_ref).max() <= 1e-5
 
