@@ -18,9 +18,15 @@ temporal terms off. Synthetic data (hvdg.synth), seeded per rank.
               its event-timed duration, against the measured HBM copy peak.
   cpu_baseline : the reference engine (oracle/_ref, compiled from the
               reference sources) on a bounded sample of the same workload on
-              the host cores.
+              the host cores (one quarter of the fields, counted by solver
+              work relative to the workload's mean).
+  parity    : outside the timed regions, the e2e call's planes against the
+              reference engine's on the cpu_baseline sample and against the
+              FP64 oracle on two of its fields: max |dY|, |dC| (IRE) and the
+              PSNR deltas against ground truth (the metric's 0.05 dB clause).
 
---impl reference times the reference engine alone (rank 0), same metric.
+--impl reference times the reference engine alone (rank 0), same metric,
+one workload quarter per step, rotating through all four.
 Multi-GPU (torchrun): each rank decodes its own 64-field batch (fields are
 independent; no collective on the data path); time = max over ranks.
 """
@@ -168,9 +174,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def run_reference(fields, threads: int) -> float:
+def run_reference(fields, threads: int, outputs: bool = False):
     """Decode `fields` with the reference engine (OpenMP across fields, as
-    parallel_across_fields does); returns seconds."""
+    parallel_across_fields does); returns seconds (and the decoded planes)."""
     from hvdg import _cabi, synth
     from oracle import ref
     ref.set_threads(threads)
@@ -180,8 +186,81 @@ def run_reference(fields, threads: int) -> float:
             for f in fields]
     ires = [synth.to_ire(f.samples) for f in fields]
     t = time.perf_counter()
-    ref.decode_fields(ires, [f.parity for f in fields], geoms, cfgs, across_fields=True)
-    return time.perf_counter() - t
+    res = ref.decode_fields(ires, [f.parity for f in fields], geoms, cfgs, across_fields=True)
+    dt = time.perf_counter() - t
+    return (dt, res) if outputs else dt
+
+
+def field_work(f) -> float:
+    """A field's solver work: active pixels x CG iteration budget."""
+    from hvdg import _cabi
+    g = _cabi.default_geometry(f.standard)
+    return float(g.active_lines * g.active_width * f.cg_iterations)
+
+
+def quarter_samples(fields, n_quarters: int = 4):
+    """The workload cut into consecutive quarters; a CPU step decodes one
+    quarter, successive steps rotate through them, so steps in multiples of
+    four decode the whole workload."""
+    q = (len(fields) + n_quarters - 1) // n_quarters
+    return [fields[i:i + q] for i in range(0, len(fields), q)]
+
+
+def field_equivalents(sample, fields) -> float:
+    """`sample`'s solver work in units of the workload's mean work per
+    field: the fields/s of a sample count the workload's fields it is
+    worth, so a heavier or lighter sample does not bias the rate."""
+    mean = sum(field_work(f) for f in fields) / len(fields)
+    return sum(field_work(f) for f in sample) / mean
+
+
+def _psnr(a, b, peak=100.0) -> float:
+    d = np.asarray(a, np.complex128) - np.asarray(b, np.complex128)
+    return float(10 * np.log10(peak ** 2 / np.mean(np.abs(d) ** 2)))
+
+
+def parity_leg(fields, out, sample, ref_y, ref_c, n_oracle: int = 2):
+    """Quality of the timed workload's outputs (the e2e call's planes),
+    outside every timed region: against the reference engine on the CPU
+    sample's fields, and against the FP64 oracle on the `n_oracle` lightest
+    fields of that sample (one NTSC, one PAL), in a spawn pool. PSNR deltas
+    are |PSNR(ours, truth) - PSNR(theirs, truth)| for luma and chroma."""
+    from oracle import jobs
+
+    def compare(ours, y, c, f):
+        return (float(np.abs(ours.luma - y).max()), float(np.abs(ours.chroma - c).max()),
+                abs(_psnr(ours.luma, f.y_true) - _psnr(y, f.y_true)),
+                abs(_psnr(ours.chroma, f.chi_true) - _psnr(c, f.chi_true)))
+
+    res = {}
+    rows = [compare(out[i], ref_y[i], ref_c[i], fields[i]) for i in range(len(sample))]
+    res["vs_reference"] = {"fields": len(rows), "max_dY_ire": max(r[0] for r in rows),
+                           "max_dC_ire": max(r[1] for r in rows),
+                           "max_psnr_delta_y_db": max(r[2] for r in rows),
+                           "max_psnr_delta_c_db": max(r[3] for r in rows)}
+    picks = []
+    for std in (0, 1):
+        cand = [i for i in range(len(sample)) if fields[i].standard == std]
+        if cand:
+            picks.append(min(cand, key=lambda i: field_work(fields[i])))
+    picks = picks[:n_oracle]
+    job_list = [(fields[i].samples, fields[i].standard, fields[i].parity,
+                 dict(fast=0, cg_tol=1e-6, temporal_strength=-1.0,
+                      irls_outer=fields[i].irls_outer, cg_iterations=fields[i].cg_iterations))
+                for i in picks]
+    orc = jobs.decode_fields_2d_parallel(job_list)
+    rows = [compare(out[i], y, c, fields[i]) for i, (y, c, _) in zip(picks, orc)]
+    res["vs_fp64_oracle"] = {"fields": [int(i) for i in picks],
+                             "max_dY_ire": max(r[0] for r in rows),
+                             "max_dC_ire": max(r[1] for r in rows),
+                             "max_psnr_delta_y_db": max(r[2] for r in rows),
+                             "max_psnr_delta_c_db": max(r[3] for r in rows)}
+    worst = max(res["vs_fp64_oracle"]["max_psnr_delta_y_db"],
+                res["vs_fp64_oracle"]["max_psnr_delta_c_db"],
+                res["vs_reference"]["max_psnr_delta_y_db"],
+                res["vs_reference"]["max_psnr_delta_c_db"])
+    res["within_0p05_db"] = bool(worst <= 0.05)
+    return res
 
 
 def reference_arm(args, rank, world):
@@ -194,15 +273,19 @@ def reference_arm(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference engine library oracle/_ref/libhvdref.so was not built"}))
         return 0
-    sample = fields[:max(8, min(threads, len(fields)))]
-    for _ in range(args.warmup):
-        run_reference(sample[:max(2, threads // 4)], threads)
-    times = [run_reference(sample, threads) for _ in range(args.steps)]
-    total = float(sum(times))
-    v = len(sample) * args.steps / total
-    desc = (f"{len(sample)} of the 64 workload fields per step "
-            f"({sum(f.standard == 0 for f in sample)} NTSC, {sum(f.standard == 1 for f in sample)} PAL), "
-            f"OpenMP across fields, {threads} threads")
+    quarters = quarter_samples(fields)
+    for i in range(args.warmup):
+        run_reference(quarters[i % len(quarters)][:max(2, threads // 4)], threads)
+    total, equiv = 0.0, 0.0
+    for i in range(args.steps):
+        sample = quarters[i % len(quarters)]
+        total += run_reference(sample, threads)
+        equiv += field_equivalents(sample, fields)
+    v = equiv / total
+    desc = (f"per step one quarter ({len(quarters[0])} fields) of the {len(fields)}-field workload, "
+            f"rotating (steps in multiples of {len(quarters)} cover every field equally); "
+            f"fields counted by solver work (active px x CG budget) relative to the workload's "
+            f"mean; OpenMP across fields, {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "fields/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
@@ -679,6 +762,8 @@ def main():
     achieved = alg_bytes_per_launch / solver_s / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": profile_traffic(args.workload),
+            "traffic_source": "committed ncu capture of this workload's solver launch "
+                              "(profiles/solver_traffic.json), not measured in this run",
             "peak_kind": peak_kind,
             "kernel": "k_solver (persistent IRLS + CG)",
             "alg_bytes_per_launch": alg_bytes_per_launch, "ms_per_launch": 1000 * solver_s}
@@ -704,13 +789,16 @@ def main():
         from oracle import ref
         if ref.available():
             threads = os.cpu_count() or 1
-            sample = fields[:max(8, min(threads, n))]
+            sample = quarter_samples(fields)[0]
             run_reference(sample[:2], threads)
-            ts = run_reference(sample, threads)
+            ts, (ry, rc) = run_reference(sample, threads, outputs=True)
             line["cpu_baseline"] = {
-                "value": len(sample) / ts, "unit": "fields/s", "cores": threads, "kind": "reference",
-                "sample": f"{len(sample)} of the 64 workload fields, reference engine "
-                          f"(oracle/_ref) OpenMP across fields"}
+                "value": field_equivalents(sample, fields) / ts, "unit": "fields/s",
+                "cores": threads, "kind": "reference",
+                "sample": f"the first {len(sample)} of the {n} workload fields, reference engine "
+                          f"(oracle/_ref) OpenMP across fields, counted by solver work relative "
+                          f"to the workload's mean"}
+            line["parity"] = parity_leg(fields, out, sample, ry, rc)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()

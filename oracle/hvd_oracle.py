@@ -537,6 +537,7 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
         return float(hh)
 
     iters = 0
+    outer_log = []     # per outer: (CG iterations, nearest |gg - threshold| / threshold)
     for _outer in range(irls_outer):
         yc = s - np.real(chi * c)
         gxY, gyY = Dx(yc), Dy(yc)
@@ -558,6 +559,8 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
         d = -g
         gg = float(np.sum(np.abs(g) ** 2))
         gg0 = gg
+        thr = max(tol * tol * gg0, 1e-10 * N)
+        near, n_it = np.inf, 0
         for _it in range(n_inner):
             hh = curv(d)
             if hh <= 1e-12:
@@ -571,12 +574,17 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
             d = -gn + beta * d
             g, gg = gn, ggn
             iters += 1
+            n_it += 1
+            if n_it < n_inner:
+                near = min(near, abs(gg - thr) / thr)
             if gg < tol * tol * gg0:
                 break
             if gg < 1e-10 * N:
                 break
+        outer_log.append((n_it, near))
     if stats is not None:
         stats["cg_iterations"] = iters
+        stats["outer_log"] = outer_log
         stats["aniso"] = aniso
     luma = s - np.real(chi * c)
     if return_weights:
@@ -598,16 +606,21 @@ def estimate_noise_ire(s) -> float:
     return q / 0.3186 / math.sqrt(6.0)
 
 
-def decode_fields_2d(fields_ire, parities, g, cfg):
+def decode_fields_2d(fields_ire, parities, g, cfg, stats=None):
     """PrepareFieldObs + DecodeFieldWindow with temporal terms off
     (sequence.cpp:229-281, 423-449, 660-669, 1076-1114): per field
-    HolographicInit + VariationalRefine, output-fidelity luma."""
+    HolographicInit + VariationalRefine, output-fidelity luma. `stats`, if
+    a list, receives each field's solver statistics (variational_refine)."""
     out = []
     for f, p in zip(fields_ire, parities):
         obs = prepare_field(f, g, cfg, p)
         _, chi0 = holographic_init(obs.s, obs.carrier, g,
                                    bool(getattr(cfg, "symmetry_variant", 0)))
-        y, chi = variational_refine(obs.s, obs.carrier, chi0, cfg, is_pal=uses_vswitch(g))
+        st = {} if stats is not None else None
+        y, chi = variational_refine(obs.s, obs.carrier, chi0, cfg, is_pal=uses_vswitch(g),
+                                    stats=st)
+        if stats is not None:
+            stats.append(st)
         if cfg.output_fidelity:
             y = obs.s - np.real(chi * obs.carrier)
         out.append((y, chi, obs))

@@ -27,3 +27,19 @@ def test_reference_arm_json_line(workload):
     assert line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_reference_sample_rotation_covers_the_workload():
+    """The reference arm's per-step samples: four rotating quarters of the
+    64-field workload whose work-weighted field counts add up to exactly
+    the workload's 64 fields, so any multiple of four steps times the same
+    configuration as the GPU arm."""
+    sys.path.insert(0, str(REPO))
+    import bench
+    fields = bench.workload(1000)
+    qs = bench.quarter_samples(fields)
+    assert len(qs) == 4 and sum(len(q) for q in qs) == len(fields) == 64
+    assert [f for q in qs for f in q] == fields
+    eq = [bench.field_equivalents(q, fields) for q in qs]
+    assert abs(sum(eq) - 64.0) < 1e-9
+    assert all(e > 0 for e in eq)
