@@ -379,9 +379,10 @@ __device__ __noinline__ double phase_gradient(const SolverArgs& A, const FieldDe
 // Register economy: between rows only the operands of the vertical
 // differences (d_k and its luma part -Re[d_k c]) and the vertical fluxes of
 // the row above are carried; everything else of the current row (g_k,
-// d_{k-1}, carriers, halo) is re-read from its slot. The inner products
-// are accumulated per lane in FP32 over the unit's rows and reduced across
-// the warp and the field in FP64 (one conversion per lane per unit).
+// d_{k-1}, carriers, halo) is re-read from its slot. Each row's inner-
+// product terms (at most eight per lane) are summed in FP32 and added to
+// per-lane FP64 accumulators, which are reduced across the warp and the
+// field in FP64 (variational.cpp:72-95 accumulates in double).
 // ---------------------------------------------------------------------------
 constexpr int kSlotG = (kStrip + 4) * 8;        // 544 B: columns x0-2 .. x0+65
 constexpr int kSlotX = kStrip * 8;              // 512 B: columns x0 .. x0+63
@@ -477,7 +478,7 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
   const float2 z = make_float2(0.f, 0.f);
   const int ybeg = max(u.y0 - 1, 0), yend = min(u.y1, f.h - 1);
   const int nrows = yend - ybeg + 1;
-  float pH = 0.f, pgd = 0.f, pgq = 0.f, pqq = 0.f, pgg = 0.f;
+  double pH = 0.0, pgd = 0.0, pgq = 0.0, pqq = 0.0, pgg = 0.0;
   bool ok = true;
   __syncwarp();
   if (lane == 0) {
@@ -599,6 +600,7 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     oa = cadd(oa, cscale(cadd(cscale(csub(bxl, bxa), mu_h), cscale(csub(bypa, bya), mu_v)), 2.f));
     ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
     const int64_t o = (int64_t)y * f.pitch + l.xa;
+    float rH = 0.f;
     if (f.has_nbr) {
       const float4 Ma = __ldcg(A.M + base + o), Mb = __ldcg(A.M + base + o + 1);
       oa.x += Ma.x * cur.ua.x + Ma.y * cur.ua.y;
@@ -606,24 +608,25 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
       ob.x += Mb.x * cur.ub.x + Mb.y * cur.ub.y;
       ob.y += Mb.y * cur.ub.x + Mb.z * cur.ub.y;
       if (l.va)
-        pH += 0.5f * (Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
+        rH += 0.5f * (Ma.x * cur.ua.x * cur.ua.x + 2.f * Ma.y * cur.ua.x * cur.ua.y +
                       Ma.z * cur.ua.y * cur.ua.y);
       if (l.vb)
-        pH += 0.5f * (Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
+        rH += 0.5f * (Mb.x * cur.ub.x * cur.ub.x + 2.f * Mb.y * cur.ub.x * cur.ub.y +
                       Mb.z * cur.ub.y * cur.ub.y);
     }
     if (!l.va) oa = z;
     if (!l.vb) ob = z;
     if (l.va)
-      pH += wa.x * dxya * dxya + wa.y * dyya * dyya + mu_h * wa.z * cnorm(dxua) +
+      rH += wa.x * dxya * dxya + wa.y * dyya * dyya + mu_h * wa.z * cnorm(dxua) +
             mu_v * wa.w * cnorm(dyua);
     if (l.vb)
-      pH += wb.x * dxyb * dxyb + wb.y * dyyb * dyyb + mu_h * wb.z * cnorm(dxub) +
+      rH += wb.x * dxyb * dxyb + wb.y * dyyb * dyyb + mu_h * wb.z * cnorm(dxub) +
             mu_v * wb.w * cnorm(dyub);
-    pgd += (gka.x * cur.ua.x + gka.y * cur.ua.y) + (gkb.x * cur.ub.x + gkb.y * cur.ub.y);
-    pgq += (gka.x * oa.x + gka.y * oa.y) + (gkb.x * ob.x + gkb.y * ob.y);
-    pqq += cnorm(oa) + cnorm(ob);
-    pgg += cnorm(gka) + cnorm(gkb);
+    pH += (double)rH;
+    pgd += (double)((gka.x * cur.ua.x + gka.y * cur.ua.y) + (gkb.x * cur.ub.x + gkb.y * cur.ub.y));
+    pgq += (double)((gka.x * oa.x + gka.y * oa.y) + (gkb.x * ob.x + gkb.y * ob.y));
+    pqq += (double)(cnorm(oa) + cnorm(ob));
+    pgg += (double)(cnorm(gka) + cnorm(gkb));
     st_pair(Gw + o, gka, gkb, l.va, l.vb);
     st_pair(Dw + o, cur.ua, cur.ub, l.va, l.vb);
     st_pair(Qw + o, oa, ob, l.va, l.vb);
@@ -767,19 +770,33 @@ __device__ __noinline__ void complete_phase(const SolverArgs& A, const FieldDesc
       c->gg = ggk;
       const int o = p / B;
       const int last_i = o * B + 1 + f.n_inner;
-      if (H <= 1e-12) {
+      const double tol = (double)f.cg_tol;
+      const double thr_rel = tol * tol * c->gg0, thr_abs = 1e-10 * (double)f.h * (double)f.w;
+      if (k >= 1 && (ggk < thr_rel || ggk < thr_abs)) {
+        // this sweep formed g_k = g_{k-1} + alpha q_{k-1} and applied
+        // chi_k = chi_{k-1} + alpha d_{k-1} in place; ||g_k||^2, measured
+        // here, is what the reference tests after its iteration k - 1
+        // (variational.cpp:547-548): exit with chi_k final
+        c->pending = 0;
+        publish = last_i;
+      } else if (H <= 1e-12) {
         c->pending = 0;
         publish = last_i;
       } else {
         const float alpha = (float)(-0.5 * gd / H);
-        const double gn = ggk + 2.0 * (double)alpha * gq + (double)alpha * (double)alpha * qq;
+        const double a = (double)alpha;
+        const double gn = ggk + 2.0 * a * gq + a * a * qq;
         c->alpha = alpha;
         c->beta = (float)(gn / fmax(ggk, 1e-30));
         c->gg_next = gn;
         c->pending = 1;
         c->cg_iters += 1;
-        const double tol = (double)f.cg_tol;
-        if (gn < tol * tol * c->gg0 || gn < 1e-10 * (double)f.h * (double)f.w) publish = last_i;
+        // ||g_{k+1}||^2 predicted by the recurrence: the exit is taken now
+        // only where the prediction lies below a threshold by more than its
+        // rounding bound (FP32 terms, FP64 sums); nearer the threshold the
+        // next sweep measures ||g_{k+1}||^2 and decides on that
+        const double bound = 1e-5 * (ggk + 2.0 * fabs(a * gq) + a * a * qq);
+        if (gn + bound < thr_rel || gn + bound < thr_abs) publish = last_i;
       }
     } else {
       c->pending = 0;
