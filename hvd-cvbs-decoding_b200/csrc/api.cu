@@ -174,6 +174,13 @@ hvdg_status hvdg_set_tuning(hvdg_ctx* ctx, int band_rows, int ctas_per_sm) {
   return HVDG_OK;
 }
 
+hvdg_status hvdg_set_device_wait_limit(hvdg_ctx* ctx, int64_t polls) {
+  settle(ctx);
+  if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
+  ctx->phase_wait_limit = polls > 0 ? (long long)polls : hvdg::kSpinLimit;
+  return HVDG_OK;
+}
+
 // Complete an asynchronous call still in flight on the context (every entry
 // point that uses the context stream or the arena does this first); its
 // status and diagnostics wait for hvdg_wait.

@@ -109,11 +109,11 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-constexpr long long kSpinLimit = 4000000;  // x ~0.5 us sleeps ~= 2 s
-__device__ __forceinline__ bool wait_at_least(const int* flag, int target) {
+__device__ __forceinline__ bool wait_at_least(const int* flag, int target,
+                                              long long limit = kSpinLimit) {
   long long n = 0;
   while (ld_acquire(flag) < target) {
-    if (++n > kSpinLimit) return false;
+    if (++n > limit) return false;
     __nanosleep(256);
   }
   return true;

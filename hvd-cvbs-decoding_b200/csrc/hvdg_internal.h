@@ -20,6 +20,7 @@ constexpr int kMaxLines = 1024;   // max field lines handled by the lock-in kern
 constexpr int kRowFft = 2048;     // init: row cyclic-convolution length
 constexpr int kColFft = 1024;     // init: column cyclic-convolution length (field planes)
 constexpr int kColFftWide = 2048; // init: column length of taller planes (woven frames)
+constexpr long long kSpinLimit = 4000000;  // bounded device waits: polls x ~0.5 us ~= 2 s
 constexpr int kInitPad = 16;      // init: reflect-101 row pad (holographic_init.cpp:214-222)
 
 // Per-field descriptor (device copy is read-only during a launch except the

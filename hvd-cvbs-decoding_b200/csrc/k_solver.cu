@@ -839,7 +839,7 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(const __grid_const
     if (p >= f.n_phases) continue;
     int ok = 1, dp = 0;
     if (lane == 0) {
-      ok = wait_at_least(A.done_phase + u.field, p - 1);
+      ok = wait_at_least(A.done_phase + u.field, p - 1, A.phase_wait_limit);
       dp = ld_acquire(A.done_phase + u.field);
     }
     ok = __shfl_sync(0xffffffffu, ok, 0);

@@ -23,6 +23,7 @@ struct SolverArgs {
   int* arrive;                  // per field, 0 before launch
   double* partials;             // per unit x 5
   int* err;                     // set on a bounded-wait timeout
+  long long phase_wait_limit;   // polls of a field's phase flag before giving up (err)
   const float* S;
   float2* X[2];                 // chi (double-buffered; final chi in X[0])
   float2* G[2];

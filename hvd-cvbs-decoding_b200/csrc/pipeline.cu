@@ -743,6 +743,7 @@ hvdg::SolverArgs solver_args(hvdg_ctx* ctx, const Staged& S) {
   sa.arrive = at<int>(ctx, L.o_arrive);
   sa.partials = at<double>(ctx, L.o_partials);
   sa.err = at<int>(ctx, L.o_flags);
+  sa.phase_wait_limit = ctx->phase_wait_limit;
   sa.S = at<float>(ctx, L.o_S);
   sa.X[0] = at<float2>(ctx, L.o_X0);
   sa.X[1] = at<float2>(ctx, L.o_X1);
@@ -885,7 +886,8 @@ hvdg_status run_batch_graph(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const
   // the effective tiling (a per-call override, else the context setting)
   const int band = opt.band_rows >= 0 ? opt.band_rows : ctx->band_rows;
   const int ctas = opt.ctas_per_sm >= 0 ? opt.ctas_per_sm : ctx->ctas_per_sm;
-  sig += "|b" + std::to_string(band) + "c" + std::to_string(ctas);
+  sig += "|b" + std::to_string(band) + "c" + std::to_string(ctas) + "w" +
+         std::to_string(ctx->phase_wait_limit);
   char buf[64];
   for (int i = 0; i < n; ++i) {
     std::snprintf(buf, sizeof(buf), "|%p,%p,%p,%p,%d,%d", in[i].samples, (void*)out[i].luma,

@@ -119,6 +119,7 @@ struct hvdg_ctx {
   int batched = 1;
   int band_rows = 0;
   int ctas_per_sm = 0;
+  long long phase_wait_limit = hvdg::kSpinLimit;  // solver phase-flag polls (~0.5 us each)
   hvdg::DeviceArena arena;
   hvdg::PinnedArena pinned;
   std::map<hvdg_pipe::GeomKey, hvdg_pipe::GeomTables> geoms;

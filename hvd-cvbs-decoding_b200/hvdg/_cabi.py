@@ -329,6 +329,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_set_batching.restype = C.c_int
     lib.hvdg_set_tuning.argtypes = [vp, C.c_int, C.c_int]
     lib.hvdg_set_tuning.restype = C.c_int
+    lib.hvdg_set_device_wait_limit.argtypes = [vp, C.c_int64]
+    lib.hvdg_set_device_wait_limit.restype = C.c_int
     for name in ("hvdg_decode_field_window", "hvdg_decode_fields", "hvdg_decode_fields_device"):
         f = getattr(lib, name)
         f.argtypes = [vp, P(FieldIn), C.c_int, P(Config), P(FieldOut), P(Diag)]

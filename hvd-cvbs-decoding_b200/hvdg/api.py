@@ -96,6 +96,12 @@ class Context:
     def set_tuning(self, band_rows: int = 0, ctas_per_sm: int = 0):
         self._check(self.lib.hvdg_set_tuning(self._h, int(band_rows), int(ctas_per_sm)), "set_tuning")
 
+    def set_device_wait_limit(self, polls: int = 0):
+        """Polls of a field's phase flag before the solver gives up with
+        HVDG_ERR_DEVICE_TIMEOUT (<= 0: the default, ~2 s)."""
+        self._check(self.lib.hvdg_set_device_wait_limit(self._h, int(polls)),
+                    "set_device_wait_limit")
+
     # ---- engine level ----------------------------------------------------
     def _build_fields(self, fields):
         n = len(fields)

@@ -232,6 +232,12 @@ const char* hvdg_last_error(const hvdg_ctx* ctx);
 hvdg_status hvdg_set_batching(hvdg_ctx* ctx, int batched);
 /* Solver tiling: band height (rows per work unit; 0 = autotuned). */
 hvdg_status hvdg_set_tuning(hvdg_ctx* ctx, int band_rows, int ctas_per_sm);
+/* Bound of the solver's device-side waits on a field's phase flag, in polls
+ * (~0.5 us each; <= 0 restores the default 4,000,000, ~2 s). A wait that
+ * runs out ends the launch and the call returns HVDG_ERR_DEVICE_TIMEOUT; the
+ * context stays usable. No reference counterpart (the reference's CPU loops
+ * have no waits to bound). */
+hvdg_status hvdg_set_device_wait_limit(hvdg_ctx* ctx, int64_t polls);
 
 /* ------------------------------------------------------------------------ */
 /* Engine level                                                              */
