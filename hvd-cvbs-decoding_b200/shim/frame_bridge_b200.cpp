@@ -9,14 +9,12 @@
 // state), same failure convention: an empty vector / a default YcFrameS16
 // where the reference returns one. Built inside the hvd-core tree in place
 // of those four functions of frame_bridge.cpp (its other helpers stay), the
-// decode-orc plugin links unchanged. Each HvdEngine gets one library
-// context (device arena, stream, graph cache), created on first use and
-// kept for the process's life; one engine per thread, as frame_bridge.h
-// asks of the reference. HVDG_DEVICE selects the CUDA device (default 0).
+// decode-orc plugin links unchanged. Each host thread gets one library
+// context (device arena, stream, graph cache), created on its first decode
+// and destroyed when the thread exits. HVDG_DEVICE selects the CUDA device
+// (default 0).
 #include <cstdint>
 #include <cstdlib>
-#include <map>
-#include <mutex>
 #include <vector>
 
 #include "frame_bridge.h"
@@ -25,17 +23,30 @@
 namespace hvd {
 namespace {
 
-hvdg_ctx* ContextFor(const HvdEngine* engine) {
-  static std::mutex mu;
-  static std::map<const HvdEngine*, hvdg_ctx*> contexts;
-  std::lock_guard<std::mutex> lock(mu);
-  auto it = contexts.find(engine);
-  if (it != contexts.end()) return it->second;
-  const char* dev = std::getenv("HVDG_DEVICE");
+// The library context of the calling thread. An HvdEngine must not be used
+// by two threads at once (frame_bridge.h:137-140), so the engines one thread
+// uses run one after another and can share that thread's context. Keying
+// contexts on the engine instead would keep one alive per engine for the
+// life of the process: the stage builds a fresh engine per export worker and
+// per preview trigger (hvd_chroma_decoder_stage.cpp:991, 1115, 1166), and
+// each context holds a device arena and page-locked staging. The context
+// is destroyed when its thread exits.
+struct ThreadContext {
   hvdg_ctx* ctx = nullptr;
-  if (hvdg_create(dev ? std::atoi(dev) : 0, &ctx) != HVDG_OK) return nullptr;
-  contexts.emplace(engine, ctx);
-  return ctx;
+  ~ThreadContext() {
+    if (ctx) hvdg_destroy(ctx);
+  }
+};
+
+hvdg_ctx* ContextFor(const HvdEngine* /*engine*/) {
+  thread_local ThreadContext tc;
+  if (!tc.ctx) {
+    const char* dev = std::getenv("HVDG_DEVICE");
+    hvdg_ctx* ctx = nullptr;
+    if (hvdg_create(dev ? std::atoi(dev) : 0, &ctx) != HVDG_OK) return nullptr;
+    tc.ctx = ctx;
+  }
+  return tc.ctx;
 }
 
 int32_t ToHvdg(VideoStandard s) {

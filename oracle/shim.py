@@ -36,6 +36,9 @@ def lib() -> C.CDLL:
         L.hvdshim_decode_yc_frame_buffer.argtypes = [vp, vp, P(_cabi.FrameParams),
                                                      P(_cabi.Config), vp, vp, vp, vp]
         L.hvdshim_decode_yc_frame_buffer.restype = C.c_int
+        L.hvdshim_decode_frame_buffer_workers.argtypes = [vp, P(_cabi.FrameParams),
+                                                          P(_cabi.Config), C.c_int]
+        L.hvdshim_decode_frame_buffer_workers.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -78,3 +81,12 @@ def decode_yc_frame_buffer(luma, chroma, fp, cfg):
                                               _ptr(o["luma"]), _ptr(o["chroma"]), _ptr(o["u"]),
                                               _ptr(o["v"]))
     return o if ok else None
+
+
+def decode_frame_buffer_workers(frame, fp, cfg, n_threads):
+    """hvd::DecodeFrameBuffer on `n_threads` short-lived worker threads, one
+    fresh HvdEngine each (the stage's export pattern); returns the number of
+    non-empty results."""
+    fr = np.ascontiguousarray(frame, dtype=np.int16)
+    return lib().hvdshim_decode_frame_buffer_workers(_ptr(fr), C.byref(fp), C.byref(cfg),
+                                                     int(n_threads))

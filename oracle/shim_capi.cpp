@@ -5,6 +5,7 @@
 // compare it with the reference engine (ref_capi.cpp) and with the library's
 // direct C ABI.
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include "ref_convert.h"
@@ -54,6 +55,25 @@ int hvdshim_decode_yc_frame_buffer(const int16_t* luma_in, const int16_t* chroma
   if (o.luma.empty()) return 0;
   CopyOut(o, luma, chroma, u, v);
   return 1;
+}
+
+// The stage's export pattern: `n_threads` worker threads one after another,
+// each with its own fresh HvdEngine, decoding `frame` through
+// hvd::DecodeFrameBuffer(..., engine) and exiting; returns how many decodes
+// came back non-empty. Used to check that worker threads leave no device
+// memory behind.
+int hvdshim_decode_frame_buffer_workers(const int16_t* frame, const hvdg_frame_params* fp,
+                                        const hvdg_config* cfg, int n_threads) {
+  int ok = 0;
+  for (int t = 0; t < n_threads; ++t) {
+    std::thread worker([&] {
+      hvd::HvdEngine engine;
+      const hvd::YcFrameS16 o = hvd::DecodeFrameBuffer(frame, ToFp(*fp), ToCfg(*cfg), engine);
+      if (!o.luma.empty()) ++ok;
+    });
+    worker.join();
+  }
+  return ok;
 }
 
 }  // extern "C"

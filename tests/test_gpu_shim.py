@@ -68,3 +68,25 @@ def test_shim_empty_window(ctx):
     frames, _ = synth.make_frames(3, _cabi.STD_NTSC, 1)
     fp = api.frame_params(_cabi.STD_NTSC)
     assert shim.decode_frame_sequence_window(frames, 1, 1, fp, api.default_config()) == []
+
+
+def test_shim_worker_threads_leave_no_device_memory(ctx):
+    """Each export worker of the stage builds its own HvdEngine on its own
+    thread (hvd_chroma_decoder_stage.cpp:991, 1115, 1166). The shim keeps
+    one library context per thread and destroys it when the thread exits,
+    so a stream of short-lived workers leaves the device's free memory where
+    it was (before: one context with its arena per engine, never freed)."""
+    torch = pytest.importorskip("torch")
+    shim = _shim()
+    frames, _ = synth.make_frames(57, _cabi.STD_NTSC, 1, noise_sigma=1.0)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6)
+    assert shim.decode_frame_buffer_workers(frames[0], fp, cfg, 2) == 2   # warm-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert shim.decode_frame_buffer_workers(frames[0], fp, cfg, 24) == 24
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    print(f"device free memory: {free0 / 2**20:.0f} MiB before, {free1 / 2**20:.0f} MiB after "
+          f"24 worker threads")
+    assert free1 >= free0 - (64 << 20)
