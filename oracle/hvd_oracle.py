@@ -336,6 +336,36 @@ def DyT(a):
     return d
 
 
+def D1(a):
+    """+45 deg (gradients.h:195-211): d[:-1, :-1] = a[1:, 1:] - a[:-1, :-1]."""
+    d = np.zeros_like(a)
+    d[:-1, :-1] = a[1:, 1:] - a[:-1, :-1]
+    return d
+
+
+def D1T(a):
+    """Adjoint of D1 (gradients.h:213-236)."""
+    d = np.zeros_like(a)
+    d[:-1, :-1] -= a[:-1, :-1]
+    d[1:, 1:] += a[:-1, :-1]
+    return d
+
+
+def D2(a):
+    """-45 deg (gradients.h:238-254): d[:-1, 1:] = a[1:, :-1] - a[:-1, 1:]."""
+    d = np.zeros_like(a)
+    d[:-1, 1:] = a[1:, :-1] - a[:-1, 1:]
+    return d
+
+
+def D2T(a):
+    """Adjoint of D2 (gradients.h:256-279)."""
+    d = np.zeros_like(a)
+    d[:-1, 1:] -= a[:-1, 1:]
+    d[1:, :-1] += a[:-1, 1:]
+    return d
+
+
 # --------------------------------------------------------------------------
 # Holographic init (engine/holographic_init.cpp)
 # --------------------------------------------------------------------------
@@ -490,17 +520,22 @@ def solver_budget(cfg):
 
 def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=None,
                        return_weights=False):
-    """VariationalRefine (variational.cpp:198-556), FP64 throughout.
-    diag_prior > 0 is not restated (off by default, unsupported on the
-    device path)."""
-    if cfg.diag_prior > 0.0:
-        raise NotImplementedError("diag_prior")
+    """VariationalRefine (variational.cpp:198-556), FP64 throughout,
+    including the oriented +-45 deg chroma prior of diag_prior > 0
+    (variational.cpp:207-222, 316-328, 371-383, 434-451)."""
     s = np.asarray(s, np.float64)
     c = np.asarray(carrier, np.complex128)
     eps, eps_c = float(cfg.charbonnier_eps), float(cfg.chroma_eps)
     aniso = resolve_chroma_aniso(np.asarray(chi0, np.complex128), cfg, is_pal)
     mu_h = cfg.lambda_c * aniso
     mu_v = float(cfg.lambda_c)
+    # oriented prior weight, distance-normalised by 1/2, and the total prior
+    # mass kept: mu_h, mu_v, mu_d scaled by tot0 / (tot0 + 2 mu_d)
+    mu_d = float(cfg.lambda_c) * float(cfg.diag_prior) * 0.5
+    if mu_d > 0.0:
+        tot0 = float(cfg.lambda_c) * (1.0 + aniso)
+        scale = tot0 / (tot0 + 2.0 * mu_d)
+        mu_h, mu_v, mu_d = mu_h * scale, mu_v * scale, mu_d * scale
     k = float(cfg.structure_coupling)
     nbrs = list(neighbors)
     nu = float(cfg.temporal_strength) if nbrs else 0.0
@@ -521,6 +556,8 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
         yc = s - np.real(ch * c)
         img = 2.0 * (DxT(W["wx"] * Dx(yc)) + DyT(W["wy"] * Dy(yc)))
         cpr = 2.0 * (mu_h * DxT(W["wcx"] * Dx(ch)) + mu_v * DyT(W["wcy"] * Dy(ch)))
+        if mu_d > 0.0:
+            cpr = cpr + 2.0 * mu_d * (D1T(W["wd1"] * D1(ch)) + D2T(W["wd2"] * D2(ch)))
         out = -img * np.conj(c) + cpr
         for j in range(len(nbrs)):
             out = out + 2.0 * nu * wts[j] * trm(ch, j) * np.conj(dcs[j])
@@ -531,6 +568,9 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
         hh = (np.sum(W["wx"] * Dx(dy) ** 2) + np.sum(W["wy"] * Dy(dy) ** 2)
               + mu_h * np.sum(W["wcx"] * np.abs(Dx(dd)) ** 2)
               + mu_v * np.sum(W["wcy"] * np.abs(Dy(dd)) ** 2))
+        if mu_d > 0.0:
+            hh += mu_d * (np.sum(W["wd1"] * np.abs(D1(dd)) ** 2)
+                          + np.sum(W["wd2"] * np.abs(D2(dd)) ** 2))
         for j in range(len(nbrs)):
             re = np.real(dd * dcs[j])
             hh += nu * np.sum(wts[j] * re * re)
@@ -546,6 +586,9 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
         W["wy"] = eps / np.sqrt(gyY ** 2 + e2)
         W["wcx"] = eps_c / np.sqrt(mx ** 2 + k * gxY ** 2 + ec2)
         W["wcy"] = eps_c / np.sqrt(my ** 2 + k * gyY ** 2 + ec2)
+        if mu_d > 0.0:
+            W["wd1"] = 1.0 / np.sqrt(1.0 + (np.abs(D1(chi)) / eps_c) ** 2)
+            W["wd2"] = 1.0 / np.sqrt(1.0 + (np.abs(D2(chi)) / eps_c) ** 2)
         if nu > 0.0:
             for j in range(len(nbrs)):
                 rt = trm(chi, j)
@@ -553,7 +596,7 @@ def variational_refine(s, carrier, chi0, cfg, is_pal=False, neighbors=(), stats=
             ps = np.ones_like(s)
             for j in range(len(nbrs)):
                 ps += nu * wts[j] * np.abs(dcs[j]) ** 2
-            for key in ("wx", "wy", "wcx", "wcy"):
+            for key in ("wx", "wy", "wcx", "wcy") + (("wd1", "wd2") if mu_d > 0.0 else ()):
                 W[key] = W[key] * ps
         g = grad(chi)
         d = -g
