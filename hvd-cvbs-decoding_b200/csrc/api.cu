@@ -843,7 +843,6 @@ hvdg_status hvdg_variational_refine(hvdg_ctx* ctx, const float* s, const float* 
     return HVDG_ERR_BAD_ARGUMENT;
   hvdg_status st = check_geometry(g);
   if (st != HVDG_OK) return st;
-  if (cfg->diag_prior > 0.0f) return HVDG_ERR_UNSUPPORTED;
   if (uses_vswitch(*g) && !vswitch_active) return HVDG_ERR_BAD_ARGUMENT;
   cudaSetDevice(ctx->device);
   hvdg_field_in fi;

@@ -468,7 +468,6 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
     ctx->last_error = "woven frame beyond the device-path limits";
     return st;
   }
-  if (cfg->diag_prior > 0.0f) return HVDG_ERR_UNSUPPORTED;
   if (diag) std::memset(diag, 0, sizeof(*diag));
   if (n == 0) return HVDG_OK;
   cudaSetDevice(ctx->device);

@@ -39,7 +39,9 @@ struct FieldDesc {
   float cg_tol;        // relative gradient-norm exit
   float eps, eps_c, k_coupling;  // Charbonnier scales, structure coupling
   float lambda_c, aniso_cfg;     // lambda_c, fixed aniso (> 0) or 0 = auto
+  float diag_prior;    // oriented +-45 deg chroma prior weight (0 = off)
   float mu_h, mu_v;    // written by the aniso kernel
+  float mu_d;          // oriented prior weight, written by the aniso kernel (0 = off)
   float nu;            // temporal strength (0 = 2-D)
   float eps_t;         // temporal robust scale
   int has_nbr;         // 3-D neighbour terms present (M / b planes valid)

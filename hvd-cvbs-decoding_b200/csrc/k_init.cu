@@ -771,8 +771,14 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
       aniso = fminf(fmaxf(0.5f + 1.1f * (r - 1.3f), 0.5f), 1.0f);
   }
   if (threadIdx.x == 0) {
-    f.mu_h = f.lambda_c * aniso;
-    f.mu_v = f.lambda_c;
+    // the oriented prior's weight, and the renormalisation that keeps the
+    // total chroma prior mass (variational.cpp:207-219)
+    const float mu_d = f.lambda_c * f.diag_prior * 0.5f;
+    const float tot0 = f.lambda_c * (1.0f + aniso);
+    const float scale = mu_d > 0.0f ? tot0 / (tot0 + 2.0f * mu_d) : 1.0f;
+    f.mu_h = (f.lambda_c * aniso) * scale;
+    f.mu_v = f.lambda_c * scale;
+    f.mu_d = mu_d > 0.0f ? mu_d * scale : 0.0f;
   }
 }
 

@@ -77,6 +77,32 @@ __device__ __forceinline__ LapOut lap(float4 c, float4 l, float4 r, float4 u, fl
   return o;
 }
 
+// The oriented chroma prior's part of L v at one pixel (gradients.h:195-279):
+// D1T(w1 D1 v) + D2T(w2 D2 v) on the chroma components, with
+// D1 v(y, x) = v(y+1, x+1) - v(y, x), D2 v(y, x) = v(y+1, x-1) - v(y, x)
+// (zero on the last row, last / first column), the adjoints gathered as
+// D1T p (y, x) = -p(y, x) + p(y-1, x-1), D2T p (y, x) = -p(y, x) + p(y-1, x+1);
+// w = (mu_d wd1, mu_d wd2) at the pixel (wc), its upper-left (wul) and
+// upper-right (wur) neighbours; adds the pixel's forward energy too.
+struct DiagNb {
+  float4 dr, dl, ul, ur;   // v at (y+1, x+1), (y+1, x-1), (y-1, x-1), (y-1, x+1)
+  float4 wc, wul, wur;
+  bool e1, e2, e1u, e2u;   // D1 / D2 exist at the pixel, at (y-1, x-1) / (y-1, x+1)
+};
+__device__ __forceinline__ void diag_lap(const DiagNb& n, float4 c, LapOut& o) {
+  const float z = 0.f;
+  const float p1y = n.e1 ? n.wc.x * (n.dr.y - c.y) : z, p1z = n.e1 ? n.wc.x * (n.dr.z - c.z) : z;
+  const float p2y = n.e2 ? n.wc.y * (n.dl.y - c.y) : z, p2z = n.e2 ? n.wc.y * (n.dl.z - c.z) : z;
+  const float q1y = n.e1u ? n.wul.x * (c.y - n.ul.y) : z, q1z = n.e1u ? n.wul.x * (c.z - n.ul.z) : z;
+  const float q2y = n.e2u ? n.wur.y * (c.y - n.ur.y) : z, q2z = n.e2u ? n.wur.y * (c.z - n.ur.z) : z;
+  o.lv.y += (q1y - p1y) + (q2y - p2y);
+  o.lv.z += (q1z - p1z) + (q2z - p2z);
+  const float d1y = n.e1 ? n.dr.y - c.y : z, d1z = n.e1 ? n.dr.z - c.z : z;
+  const float d2y = n.e2 ? n.dl.y - c.y : z, d2z = n.e2 ? n.dl.z - c.z : z;
+  o.energy += (n.e1 ? n.wc.x : z) * (d1y * d1y + d1z * d1z) +
+              (n.e2 ? n.wc.y : z) * (d2y * d2y + d2z * d2z);
+}
+
 template <int N>
 __device__ void block_sum(double (&v)[N], double* sh) {
   const int t = threadIdx.y * blockDim.x + threadIdx.x;
@@ -176,6 +202,16 @@ __global__ void k_joint_setup(JointArgs a) {
     b2 += wa * ca.y;
   }
   a.W[o] = make_float4(wx * ps, wy * ps, f.mu_h * (wcx * ps), f.mu_v * (wcy * ps));
+  if (a.diag) {
+    // oriented diffusivities of chi (variational.cpp:787-797, prior-scaled :838-841)
+    const bool e1 = hy && hx, e2 = hy && x >= 1;
+    const float4 c11 = e1 ? a.X[o + f.pitch + 1] : c0, c1m = e2 ? a.X[o + f.pitch - 1] : c0;
+    const float d1r = c11.y - c0.y, d1i = c11.z - c0.z, d2r = c1m.y - c0.y, d2i = c1m.z - c0.z;
+    const float c1 = sqrtf(d1r * d1r + d1i * d1i) / a.eps_c;
+    const float c2 = sqrtf(d2r * d2r + d2i * d2i) / a.eps_c;
+    const float wd1 = 1.0f / sqrtf(1.0f + c1 * c1), wd2 = 1.0f / sqrtf(1.0f + c2 * c2);
+    a.W2[o] = make_float4(f.mu_d * (wd1 * ps), f.mu_d * (wd2 * ps), 0.f, 0.f);
+  }
   a.M0[o] = make_float4(m00, m01, m02, m11);
   a.M1[o] = make_float4(m12, m22, b0, b1);
   a.M2[o] = b2;
@@ -196,7 +232,22 @@ __global__ void k_joint_grad(JointArgs a) {
     const float4 u = hu ? a.X[o - f.pitch] : c, d = hd ? a.X[o + f.pitch] : c;
     const float4 wc = a.W[o];
     const float4 wl = hl ? a.W[o - 1] : wc, wu = hu ? a.W[o - f.pitch] : wc;
-    const LapOut L = lap(c, l, r, u, d, wc, wl, wu, hl, hr, hu, hd);
+    LapOut L = lap(c, l, r, u, d, wc, wl, wu, hl, hr, hu, hd);
+    if (a.diag) {
+      DiagNb n;
+      n.e1 = hd && hr;
+      n.e2 = hd && hl;
+      n.e1u = hu && hl;
+      n.e2u = hu && hr;
+      n.dr = n.e1 ? a.X[o + f.pitch + 1] : c;
+      n.dl = n.e2 ? a.X[o + f.pitch - 1] : c;
+      n.ul = n.e1u ? a.X[o - f.pitch - 1] : c;
+      n.ur = n.e2u ? a.X[o - f.pitch + 1] : c;
+      n.wc = a.W2[o];
+      n.wul = n.e1u ? a.W2[o - f.pitch - 1] : n.wc;
+      n.wur = n.e2u ? a.W2[o - f.pitch + 1] : n.wc;
+      diag_lap(n, c, L);
+    }
     const float4 m0 = a.M0[o], m1 = a.M1[o];
     const float4 b = f4(m1.z, m1.w, a.M2[o]);
     const float4 g = sc4(add4(sub4(mv(m0, m1, c), b), L.lv), 2.f);
@@ -258,7 +309,22 @@ __global__ void k_joint_sweep(JointArgs a, int first) {
     const float4 du = hu ? dk(o - f.pitch) : dc, dd = hd ? dk(o + f.pitch) : dc;
     const float4 wc = a.W[o];
     const float4 wl = hl ? a.W[o - 1] : wc, wu = hu ? a.W[o - f.pitch] : wc;
-    const LapOut L = lap(dc, dl, dr, du, dd, wc, wl, wu, hl, hr, hu, hd);
+    LapOut L = lap(dc, dl, dr, du, dd, wc, wl, wu, hl, hr, hu, hd);
+    if (a.diag) {
+      DiagNb n;
+      n.e1 = hd && hr;
+      n.e2 = hd && hl;
+      n.e1u = hu && hl;
+      n.e2u = hu && hr;
+      n.dr = n.e1 ? dk(o + f.pitch + 1) : dc;
+      n.dl = n.e2 ? dk(o + f.pitch - 1) : dc;
+      n.ul = n.e1u ? dk(o - f.pitch - 1) : dc;
+      n.ur = n.e2u ? dk(o - f.pitch + 1) : dc;
+      n.wc = a.W2[o];
+      n.wul = n.e1u ? a.W2[o - f.pitch - 1] : n.wc;
+      n.wur = n.e2u ? a.W2[o - f.pitch + 1] : n.wc;
+      diag_lap(n, dc, L);
+    }
     const float4 m0 = a.M0[o], m1 = a.M1[o];
     const float4 md = mv(m0, m1, dc);
     const float4 qk = sc4(add4(md, L.lv), 2.f);

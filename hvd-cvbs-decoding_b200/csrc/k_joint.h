@@ -39,6 +39,9 @@ struct JointArgs {
   float4* D[2];
   float4* Q[2];
   float4* W;                   // (wx, wy, mu_h wcx, mu_v wcy), prior-scaled
+  float4* W2;                  // (mu_d wd1, mu_d wd2, -, -), prior-scaled: the oriented
+                               // chroma prior, when diag is set
+  int diag;                    // the fields carry the oriented prior (mu_d > 0)
   float4* M0;                  // (m00, m01, m02, m11)
   float4* M1;                  // (m12, m22, b0, b1)
   float* M2;                   // b2

@@ -34,6 +34,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "hvdg_common.cuh"
 #include "k_solver.h"
 #include "per_device.h"
@@ -82,6 +84,73 @@ __device__ __forceinline__ Lanes make_lanes(const SolverArgs& A, const FieldDesc
   l.Pb = l.vb ? __ldg(P + l.xb) : make_float2(0.f, 0.f);
   l.Ph = l.hv ? __ldg(P + l.hx) : make_float2(0.f, 0.f);
   return l;
+}
+
+// ---------------------------------------------------------------------------
+// Oriented (+-45 deg) chroma prior, diag_prior > 0 (variational.cpp:316-328,
+// 371-383; gradients.h:195-279): the fluxes p1 = wd1 D1 u and p2 = wd2 D2 u
+// of one row y (u = chi in the gradient, u = d in the CG sweep), with
+//   D1 u(y, x) = u(y+1, x+1) - u(y, x)   (0 on the last row / column),
+//   D2 u(y, x) = u(y+1, x-1) - u(y, x)   (0 on the last row / first column);
+// the adjoints gather D1T p1 (y, x) = -p1(y, x) + p1(y-1, x-1) and
+// D2T p2 (y, x) = -p2(y, x) + p2(y-1, x+1), so each row's fluxes are kept
+// for the next row, plus one halo flux per strip edge: lane 0 carries
+// p1(y, x0-1), lane 31 p2(y, x0+64). `hd` is the row's weighted energy
+// wd1 |D1 u|^2 + wd2 |D2 u|^2 over this lane's pixels (the curvature term).
+// ---------------------------------------------------------------------------
+struct DiagFlux {
+  float2 p1a, p1b, p2a, p2b, ph;
+};
+
+__device__ __forceinline__ void diag_flux(const Lanes& l, const FieldDesc& f, int lane, bool hn,
+                                          float2 ua, float2 ub, float2 uh, float2 na, float2 nb,
+                                          float2 nh, float2 wda, float2 wdb, float2 wdh,
+                                          DiagFlux& o, float& hd) {
+  // row y+1 at x+1 for pixel b and at x-1 for pixel a (neighbour lanes, or
+  // the row's halo at the strip edges: lane 31 holds x0+64, lane 0 x0-1)
+  float2 n_r = make_float2(__shfl_down_sync(0xffffffffu, na.x, 1),
+                           __shfl_down_sync(0xffffffffu, na.y, 1));
+  float2 n_l = make_float2(__shfl_up_sync(0xffffffffu, nb.x, 1),
+                           __shfl_up_sync(0xffffffffu, nb.y, 1));
+  if (lane == 31) n_r = nh;
+  if (lane == 0) n_l = nh;
+  const float2 z = make_float2(0.f, 0.f);
+  // weights are read only where the difference exists (the planes' padding
+  // columns hold no weights)
+  const bool e1a = hn && l.xa < f.w - 1, e1b = hn && l.xb < f.w - 1;
+  const bool e2a = hn && l.va && l.xa >= 1, e2b = hn && l.vb;
+  const float2 d1a = e1a ? csub(nb, ua) : z;
+  const float2 d1b = e1b ? csub(n_r, ub) : z;
+  const float2 d2a = e2a ? csub(n_l, ua) : z;
+  const float2 d2b = e2b ? csub(na, ub) : z;
+  const float w1a = e1a ? wda.x : 0.f, w1b = e1b ? wdb.x : 0.f;
+  const float w2a = e2a ? wda.y : 0.f, w2b = e2b ? wdb.y : 0.f;
+  o.p1a = cscale(d1a, w1a);
+  o.p1b = cscale(d1b, w1b);
+  o.p2a = cscale(d2a, w2a);
+  o.p2b = cscale(d2b, w2b);
+  hd = (w1a * cnorm(d1a) + w2a * cnorm(d2a)) + (w1b * cnorm(d1b) + w2b * cnorm(d2b));
+  o.ph = z;
+  if (hn && l.hv) {
+    if (lane == 0)
+      o.ph = cscale(csub(na, uh), wdh.x);  // p1(y, x0-1): u(y+1, x0) - u(y, x0-1)
+    else
+      o.ph = cscale(csub(nb, uh), wdh.y);  // p2(y, x0+64): u(y+1, x0+63) - u(y, x0+64)
+  }
+}
+
+// D1T p1 + D2T p2 at this lane's two pixels of row y, from the row's fluxes
+// `c` and the previous row's `p` (zero above the first row).
+__device__ __forceinline__ void diag_adjoint(int lane, const DiagFlux& c, const DiagFlux& p,
+                                             float2& ta, float2& tb) {
+  float2 q1l = make_float2(__shfl_up_sync(0xffffffffu, p.p1b.x, 1),
+                           __shfl_up_sync(0xffffffffu, p.p1b.y, 1));
+  float2 q2r = make_float2(__shfl_down_sync(0xffffffffu, p.p2a.x, 1),
+                           __shfl_down_sync(0xffffffffu, p.p2a.y, 1));
+  if (lane == 0) q1l = p.ph;   // p1(y-1, x0-1)
+  if (lane == 31) q2r = p.ph;  // p2(y-1, x0+64)
+  ta = cadd(csub(q1l, c.p1a), csub(p.p2b, c.p2a));
+  tb = cadd(csub(p.p1a, c.p1b), csub(q2r, c.p2b));
 }
 
 // ---------------------------------------------------------------------------
@@ -187,6 +256,29 @@ __device__ __noinline__ void phase_reweight(const SolverArgs& A, const FieldDesc
     wb.z = epsc / sqrtf(mxb * mxb + k * gxb * gxb + ec2);
     wb.w = epsc / sqrtf(myb * myb + k * gyb * gyb + ec2);
     const int64_t o = (int64_t)y * f.pitch + l.xa;
+    // oriented diffusivities 1 / sqrt(1 + (|D chi| / eps_c)^2) of the +45 deg
+    // difference D1 chi(y, x) = chi(y+1, x+1) - chi(y, x) and the -45 deg
+    // one D2 chi(y, x) = chi(y+1, x-1) - chi(y, x), zero on the last row and
+    // on the last / first column (variational.cpp:434-451, gradients.h:195-254)
+    float2 wda = make_float2(0.f, 0.f), wdb = wda;
+    const bool diag = f.mu_d > 0.f;
+    if (diag) {
+      float2 n_r = make_float2(__shfl_down_sync(0xffffffffu, nxt.xa_.x, 1),
+                               __shfl_down_sync(0xffffffffu, nxt.xa_.y, 1));
+      float2 n_l = make_float2(__shfl_up_sync(0xffffffffu, nxt.xb_.x, 1),
+                               __shfl_up_sync(0xffffffffu, nxt.xb_.y, 1));
+      if (lane == 31) n_r = nxt.xh;  // chi(y+1, x0+64)
+      if (lane == 0) n_l = nxt.xh;   // chi(y+1, x0-1)
+      const float2 z = make_float2(0.f, 0.f);
+      const float2 d1a = (hn && l.xa < f.w - 1) ? csub(nxt.xb_, cur.xa_) : z;
+      const float2 d1b = (hn && l.xb < f.w - 1) ? csub(n_r, cur.xb_) : z;
+      const float2 d2a = (hn && l.va && l.xa >= 1) ? csub(n_l, cur.xa_) : z;
+      const float2 d2b = (hn && l.vb) ? csub(nxt.xa_, cur.xb_) : z;
+      const float c1a = sqrtf(cnorm(d1a)) / epsc, c1b = sqrtf(cnorm(d1b)) / epsc;
+      const float c2a = sqrtf(cnorm(d2a)) / epsc, c2b = sqrtf(cnorm(d2b)) / epsc;
+      wda = make_float2(1.0f / sqrtf(1.0f + c1a * c1a), 1.0f / sqrtf(1.0f + c2a * c2a));
+      wdb = make_float2(1.0f / sqrtf(1.0f + c1b * c1b), 1.0f / sqrtf(1.0f + c2b * c2b));
+    }
     if (f.has_nbr) {
       // neighbour robust weights (variational.cpp:452-462), prior
       // renormalisation (:493-516) and the pointwise data term written as
@@ -220,12 +312,15 @@ __device__ __noinline__ void phase_reweight(const SolverArgs& A, const FieldDesc
       }
       wa.x *= psa; wa.y *= psa; wa.z *= psa; wa.w *= psa;
       wb.x *= psb; wb.y *= psb; wb.z *= psb; wb.w *= psb;
+      wda = cscale(wda, psa);
+      wdb = cscale(wdb, psb);
       if (l.va) __stcg(A.M + base + o, Ma);
       if (l.vb) __stcg(A.M + base + o + 1, Mb);
       st_pair(A.B + base + o, ba, bb, l.va, l.vb);
     }
     if (l.va) __stcg(W + o, wa);
     if (l.vb) __stcg(W + o + 1, wb);
+    if (diag) st_pair(A.W2 + base + o, wda, wdb, l.va, l.vb);
     st_pair(Xo + o, cur.xa_, cur.xb_, l.va, l.vb);
     cur = nxt;
   }
@@ -277,6 +372,16 @@ __device__ __noinline__ double phase_gradient(const SolverArgs& A, const FieldDe
   SRow cur, nxt;
   float aypa = 0.f, aypb = 0.f;
   float2 bypa = z, bypb = z;
+  const bool diag = f.mu_d > 0.f;
+  const float2* W2 = A.W2 + base;
+  // this lane's oriented weights at (y, own pixels) and at its halo column
+  auto wd_row = [&](int y, float2& wda, float2& wdb, float2& wdh) {
+    const int64_t o = (int64_t)y * f.pitch + l.xa;
+    ld_pair(W2 + o, wda, wdb);
+    wdh = l.hv ? __ldcg(W2 + (int64_t)y * f.pitch + l.hx) : z;
+  };
+  DiagFlux dprev = {z, z, z, z, z};
+  float hd_unused = 0.f;
   s_form(A, f, l, c, u.y0, cur);
   if (u.y0 > 0) {
     SRow prv;
@@ -287,6 +392,12 @@ __device__ __noinline__ double phase_gradient(const SolverArgs& A, const FieldDe
     aypb = wpb.y * (cur.yb - prv.yb);
     bypa = cscale(csub(cur.ua, prv.ua), wpa.w);
     bypb = cscale(csub(cur.ub, prv.ub), wpb.w);
+    if (diag) {
+      float2 wda, wdb, wdh;
+      wd_row(u.y0 - 1, wda, wdb, wdh);
+      diag_flux(l, f, lane, true, prv.ua, prv.ub, prv.uh, cur.ua, cur.ub, cur.uh, wda, wdb, wdh,
+                dprev, hd_unused);
+    }
   }
   for (int y = u.y0; y < u.y1; ++y) {
     const bool hn = y + 1 < f.h;
@@ -337,6 +448,18 @@ __device__ __noinline__ double phase_gradient(const SolverArgs& A, const FieldDe
     float2 ob = make_float2(-imb * cur.cb.x, imb * cur.cb.y);
     oa = cadd(oa, cscale(cadd(cscale(csub(bxl, bxa), mu_h), cscale(csub(bypa, bya), mu_v)), 2.f));
     ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
+    if (diag) {  // + 2 mu_d (D1T(wd1 D1 chi) + D2T(wd2 D2 chi))
+      float2 wda, wdb, wdh;
+      wd_row(y, wda, wdb, wdh);
+      DiagFlux dcur;
+      diag_flux(l, f, lane, hn, cur.ua, cur.ub, cur.uh, nxt.ua, nxt.ub, nxt.uh, wda, wdb, wdh,
+                dcur, hd_unused);
+      float2 ta, tb;
+      diag_adjoint(lane, dcur, dprev, ta, tb);
+      oa = cadd(oa, cscale(ta, 2.f * f.mu_d));
+      ob = cadd(ob, cscale(tb, 2.f * f.mu_d));
+      dprev = dcur;
+    }
     if (f.has_nbr) {
       const float4 Ma = __ldcg(A.M + base + o), Mb = __ldcg(A.M + base + o + 1);
       // M u with u as the real 2-vector (Re, Im), plus the constant b
@@ -390,8 +513,16 @@ constexpr int kSlotW = (kStrip + 1) * 16;       // 1040 B: columns x0-1 .. x0+63
 constexpr int kOffQ = kSlotG, kOffD = 2 * kSlotG, kOffX = 3 * kSlotG, kOffW = 3 * kSlotG + kSlotX;
 constexpr int kOffL = kOffW + kSlotW;           // 16 B: the row's line phasor
 constexpr int kSlotBytes = kOffL + 16;          // 3200 B
-constexpr int kWarpRingBytes = kNS * kSlotBytes + kNS * 8;
-static_assert(kSlotBytes % 16 == 0 && kOffL % 16 == 0, "bulk copies need 16-byte slots");
+// the oriented-prior variant adds the (wd1, wd2) row segment, columns
+// x0-2 .. x0+65 like g (float2: 16-byte aligned at x0-2)
+constexpr int kOffW2 = kSlotBytes;
+template <bool kDiag>
+struct RingLayout {
+  static constexpr int slot = kDiag ? kSlotBytes + kSlotG : kSlotBytes;  // 3200 / 3744 B
+  static constexpr int warp = kNS * slot + kNS * 8;
+};
+static_assert(kSlotBytes % 16 == 0 && kOffL % 16 == 0 && RingLayout<true>::slot % 16 == 0,
+              "bulk copies need 16-byte slots");
 
 struct Ring {
   char* slots;
@@ -399,10 +530,11 @@ struct Ring {
   uint32_t bits;  // per-slot phase parity
 };
 
+template <bool kDiag>
 __device__ __forceinline__ void ring_issue(Ring& r, int slot, const SolverArgs& A,
                                            const FieldDesc& f, const FieldCtl& c, int x0, int y,
                                            bool first, bool need_x) {
-  char* dst = r.slots + slot * kSlotBytes;
+  char* dst = r.slots + slot * RingLayout<kDiag>::slot;
   uint64_t* bar = r.bar + slot;
   const int64_t row = f.px_off + (int64_t)y * f.pitch;
   const int gs = max(x0 - 2, 0), ge = min(x0 + kStrip + 2, f.pitch);
@@ -413,8 +545,10 @@ __device__ __forceinline__ void ring_issue(Ring& r, int slot, const SolverArgs& 
   const int woff = (ws - (x0 - 1)) * 16;
   const bool qd = !first;
   const bool xx = need_x && !first;
-  const uint32_t total = gb + wb + 16u + (qd ? 2 * gb : 0u) + (xx ? (uint32_t)kSlotX : 0u);
+  const uint32_t total = gb + wb + 16u + (qd ? 2 * gb : 0u) + (xx ? (uint32_t)kSlotX : 0u) +
+                         (kDiag ? gb : 0u);
   mbar_expect_tx(bar, total);
+  if (kDiag) bulk_g2s(dst + kOffW2 + goff, A.W2 + row + gs, gb, bar);
   bulk_g2s(dst + goff, A.G[c.sel] + row + gs, gb, bar);
   if (qd) {
     bulk_g2s(dst + kOffQ + goff, A.Q[c.sel] + row + gs, gb, bar);
@@ -470,6 +604,36 @@ __device__ __forceinline__ void slot_d(const char* slot, const Lanes& l, const F
   r.yb = -re_mul(r.ub, carrier(Lc, l.Pb, L.z));
 }
 
+// d_k at this lane's halo column (lane 0: x0-1, lane 31: x0+64; zero for the
+// other lanes and outside the field), from a slot.
+__device__ __forceinline__ float2 slot_halo(const char* sl, const Lanes& l, const FieldCtl& c,
+                                            bool first, int lane) {
+  float2 uh = make_float2(0.f, 0.f);
+  if (l.hv) {
+    const int hl = lane == 0 ? 1 : kStrip + 2;  // local column of x0-1 / x0+64
+    const float2 gh = *reinterpret_cast<const float2*>(sl + 8 * hl);
+    if (first) {
+      uh = make_float2(-gh.x, -gh.y);
+    } else {
+      const float2 qh = *reinterpret_cast<const float2*>(sl + kOffQ + 8 * hl);
+      const float2 dd = *reinterpret_cast<const float2*>(sl + kOffD + 8 * hl);
+      const float2 gkh = cadd(gh, cscale(qh, c.alpha));
+      uh = cadd(make_float2(-gkh.x, -gkh.y), cscale(dd, c.beta));
+    }
+  }
+  return uh;
+}
+
+// this lane's (wd1, wd2) at its two pixels and at its halo column, from a slot
+__device__ __forceinline__ void slot_wd(const char* sl, int lane, float2& wda, float2& wdb,
+                                        float2& wdh) {
+  const float4 w = *reinterpret_cast<const float4*>(sl + kOffW2 + 16 + 16 * lane);
+  wda = make_float2(w.x, w.y);
+  wdb = make_float2(w.z, w.w);
+  wdh = *reinterpret_cast<const float2*>(sl + kOffW2 + 8 * (lane == 0 ? 1 : kStrip + 2));
+}
+
+template <bool kDiag>
 __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& u, int lane,
                            const FieldCtl& c, bool first, Ring& ring, double* part) {
   const Lanes l = make_lanes(A, f, u.x0, lane);
@@ -486,23 +650,26 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     fence_proxy_async_smem();
     for (int i = 0; i < min(kNS, nrows); ++i) {
       const int y = ybeg + i;
-      ring_issue(ring, i % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
+      ring_issue<kDiag>(ring, i % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
     }
   }
-  auto slot_ptr = [&](int i) { return ring.slots + (i % kNS) * kSlotBytes; };
+  auto slot_ptr = [&](int i) { return ring.slots + (i % kNS) * RingLayout<kDiag>::slot; };
   auto issue_after = [&](int i_free) {
     __syncwarp();
     const int inext = i_free + kNS;
     if (lane == 0 && inext < nrows) {
       fence_proxy_async_smem();
       const int y = ybeg + inext;
-      ring_issue(ring, inext % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
+      ring_issue<kDiag>(ring, inext % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
     }
   };
   DRow cur, nxt;
   float aypa = 0.f, aypb = 0.f;
   float2 bypa = z, bypb = z;
   int icur = 0;
+  // oriented prior: the previous row's fluxes and the next row's halo d
+  DiagFlux dprev = {z, z, z, z, z};
+  float2 nuh = z;
   if (u.y0 > 0) {
     DRow prv;
     ok &= ring_wait(ring, 0);
@@ -516,6 +683,14 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     aypb = wpb.y * (cur.yb - prv.yb);
     bypa = cscale(csub(cur.ua, prv.ua), wpa.w);
     bypb = cscale(csub(cur.ub, prv.ub), wpb.w);
+    if (kDiag && f.mu_d > 0.f) {
+      float2 wda, wdb, wdh;
+      slot_wd(slot_ptr(0), lane, wda, wdb, wdh);
+      float hd_unused;
+      diag_flux(l, f, lane, true, prv.ua, prv.ub, slot_halo(slot_ptr(0), l, c, first, lane),
+                cur.ua, cur.ub, slot_halo(slot_ptr(1), l, c, first, lane), wda, wdb, wdh, dprev,
+                hd_unused);
+    }
     issue_after(0);
     icur = 1;
   } else {
@@ -532,6 +707,7 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     if (hn) {
       ok &= ring_wait(ring, (icur + 1) % kNS);
       slot_d(slot_ptr(icur + 1), l, c, first, lane, nxt);
+      if constexpr (kDiag) nuh = slot_halo(slot_ptr(icur + 1), l, c, first, lane);
     }
     const char* sl = slot_ptr(icur);
     // the current row's g_k, d_{k-1}, carriers and halo, re-read from its slot
@@ -601,6 +777,19 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
     ob = cadd(ob, cscale(cadd(cscale(csub(bxa, bxb), mu_h), cscale(csub(bypb, byb), mu_v)), 2.f));
     const int64_t o = (int64_t)y * f.pitch + l.xa;
     float rH = 0.f;
+    if (kDiag && f.mu_d > 0.f) {  // + 2 mu_d (D1T(wd1 D1 d) + D2T(wd2 D2 d)), mu_d sum wd |D d|^2
+      float2 wda, wdb, wdh;
+      slot_wd(sl, lane, wda, wdb, wdh);
+      DiagFlux dcur;
+      float hd;
+      diag_flux(l, f, lane, hn, cur.ua, cur.ub, uh, nxt.ua, nxt.ub, nuh, wda, wdb, wdh, dcur, hd);
+      float2 ta, tb;
+      diag_adjoint(lane, dcur, dprev, ta, tb);
+      oa = cadd(oa, cscale(ta, 2.f * f.mu_d));
+      ob = cadd(ob, cscale(tb, 2.f * f.mu_d));
+      rH += f.mu_d * hd;
+      dprev = dcur;
+    }
     if (f.has_nbr) {
       const float4 Ma = __ldcg(A.M + base + o), Mb = __ldcg(A.M + base + o + 1);
       oa.x += Ma.x * cur.ua.x + Ma.y * cur.ua.y;
@@ -810,14 +999,19 @@ __device__ __noinline__ void complete_phase(const SolverArgs& A, const FieldDesc
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kSolverThreads, 2) k_solver(const __grid_constant__ SolverArgs A) {
+// kDiag: the instantiation for launches with the oriented chroma prior (a
+// larger ring slot and more carried state: one CTA per SM); the plain one
+// keeps two.
+template <bool kDiag>
+__global__ void __launch_bounds__(kSolverThreads, kDiag ? 1 : 2)
+    k_solver(const __grid_constant__ SolverArgs A) {
   const int lane = threadIdx.x & 31;
   extern __shared__ __align__(16) char solver_smem[];
   Ring ring;
   {
-    char* wbase = solver_smem + (threadIdx.x >> 5) * kWarpRingBytes;
+    char* wbase = solver_smem + (threadIdx.x >> 5) * RingLayout<kDiag>::warp;
     ring.slots = wbase;
-    ring.bar = reinterpret_cast<uint64_t*>(wbase + kNS * kSlotBytes);
+    ring.bar = reinterpret_cast<uint64_t*>(wbase + kNS * RingLayout<kDiag>::slot);
     ring.bits = 0;
     if (lane == 0) {
       for (int i = 0; i < kNS; ++i) mbar_init(ring.bar + i, 1);
@@ -877,7 +1071,7 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(const __grid_const
     } else if (kind == kPhaseG) {
       part[0] = part[4] = phase_gradient(A, fg, u, lane, c);
     } else if (kind == kPhaseI) {
-      if (!phase_iter(A, f, u, lane, c, k == 0, ring, part)) {
+      if (!phase_iter<kDiag>(A, f, u, lane, c, k == 0, ring, part)) {
         if (lane == 0) atomicOr(A.err, 2);
         break;
       }
@@ -903,20 +1097,31 @@ __global__ void __launch_bounds__(kSolverThreads, 2) k_solver(const __grid_const
   }
 }
 
-constexpr int kSolverSmem = (kSolverThreads / 32) * kWarpRingBytes;
+template <bool kDiag>
+constexpr int solver_smem() {
+  return (kSolverThreads / 32) * RingLayout<kDiag>::warp;
+}
 
 static PerDeviceOnce solver_once;
 
 static void configure_solver() {
   solver_once([] {
-    cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolverSmem);
+    cudaFuncSetAttribute(k_solver<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         solver_smem<false>());
+    cudaFuncSetAttribute(k_solver<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         solver_smem<true>());
   });
 }
 
-int solver_max_blocks_per_sm() {
+int solver_max_blocks_per_sm(bool diag) {
   configure_solver();
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solver, kSolverThreads, kSolverSmem);
+  if (diag)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solver<true>, kSolverThreads,
+                                                  solver_smem<true>());
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solver<false>, kSolverThreads,
+                                                  solver_smem<false>());
   return n;
 }
 
@@ -924,8 +1129,18 @@ cudaError_t launch_solver(const SolverArgs& args, int grid, cudaStream_t st) {
   configure_solver();
   SolverArgs a = args;
   void* params[] = {&a};
-  return cudaLaunchCooperativeKernel((const void*)k_solver, dim3(grid), dim3(kSolverThreads),
-                                     params, kSolverSmem, st);
+  if (a.W2) {
+    // the oriented-prior instantiation holds fewer CTAs per SM; the
+    // persistent grid never exceeds what is co-resident
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    grid = std::max(1, std::min(grid, sms * std::max(1, solver_max_blocks_per_sm(true))));
+    return cudaLaunchCooperativeKernel((const void*)k_solver<true>, dim3(grid),
+                                       dim3(kSolverThreads), params, solver_smem<true>(), st);
+  }
+  return cudaLaunchCooperativeKernel((const void*)k_solver<false>, dim3(grid),
+                                     dim3(kSolverThreads), params, solver_smem<false>(), st);
 }
 
 }  // namespace hvdg

@@ -30,6 +30,8 @@ struct SolverArgs {
   float2* D[2];
   float2* Q[2];
   float4* W;                    // (wx, wy, wcx, wcy)
+  float2* W2;                   // (wd1, wd2) oriented-prior weights; null when no field
+                                // of the launch has diag_prior > 0
   float* Y;                     // output-fidelity luma
   float4* M;                    // neighbour 2x2 data term (m11, m12, m22, -)
   float2* B;                    // neighbour constant term
@@ -38,7 +40,7 @@ struct SolverArgs {
   const float2* col_phasor;
 };
 
-int solver_max_blocks_per_sm();
+int solver_max_blocks_per_sm(bool diag = false);
 cudaError_t launch_solver(const SolverArgs& args, int grid, cudaStream_t st);
 
 }  // namespace hvdg

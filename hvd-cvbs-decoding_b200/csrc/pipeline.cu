@@ -354,8 +354,10 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     f.k_coupling = cfg->structure_coupling;
     f.lambda_c = cfg->lambda_c;
     f.aniso_cfg = cfg->chroma_aniso;
+    f.diag_prior = cfg->diag_prior > 0.0f ? cfg->diag_prior : 0.0f;
     f.mu_h = cfg->lambda_c;
     f.mu_v = cfg->lambda_c;
+    f.mu_d = 0.0f;
     f.plane_px = (int64_t)p.h * p.pitch;
     f.unit_begin = (int)b.units.size();
     for (int x0 = 0; x0 < p.w; x0 += hvdg::kStrip)
@@ -482,6 +484,9 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
   L.o_Q0 = take(sizeof(float2) * px);
   L.o_Q1 = take(sizeof(float2) * px);
   L.o_W = take(sizeof(float4) * px);
+  L.has_diag = false;
+  for (const FieldDesc& f : b.fields) L.has_diag |= f.diag_prior > 0.0f;
+  L.o_W2 = L.has_diag ? take(sizeof(float2) * px) : 0;
   L.o_rowbuf = take(sizeof(float2) * rowb);
   L.total = o;
   return HVDG_OK;
@@ -754,6 +759,7 @@ hvdg::SolverArgs solver_args(hvdg_ctx* ctx, const Staged& S) {
   sa.Q[0] = at<float2>(ctx, L.o_Q0);
   sa.Q[1] = at<float2>(ctx, L.o_Q1);
   sa.W = at<float4>(ctx, L.o_W);
+  sa.W2 = L.has_diag ? at<float2>(ctx, L.o_W2) : nullptr;
   sa.Y = at<float>(ctx, L.o_Y);
   sa.line_phasor = at<float4>(ctx, L.o_lineph);
   sa.col_phasor = at<float2>(ctx, L.o_colph);
@@ -1063,7 +1069,6 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
 hvdg_status validate_fields(const hvdg_field_in* fields, int n, const hvdg_config* cfg,
                             hvdg_field_out* out) {
   if (n < 0 || (n > 0 && (!fields || !out)) || !cfg) return HVDG_ERR_BAD_ARGUMENT;
-  if (cfg->diag_prior > 0.0f) return HVDG_ERR_UNSUPPORTED;
   for (int i = 0; i < n; ++i) {
     if (!fields[i].samples || !fields[i].geometry) return HVDG_ERR_BAD_ARGUMENT;
     if (fields[i].sample_type < 0 || fields[i].sample_type > 2) return HVDG_ERR_BAD_ARGUMENT;

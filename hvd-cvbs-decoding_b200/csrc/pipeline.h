@@ -183,6 +183,8 @@ struct Layout {
   size_t o_raw, o_prep, o_fields, o_geoms, o_ctl, o_units, o_partials, o_done, o_arrive,
       o_flags, o_queue, o_lineph, o_theta, o_theta64, o_vsw, o_colph, o_khat, o_twr, o_twc,
       o_S, o_Y, o_X0, o_X1, o_G0, o_G1, o_D0, o_D1, o_Q0, o_Q1, o_W, o_rowbuf, o_itab, o_amp;
+  size_t o_W2 = 0;   // (wd1, wd2) plane, only when a field has the oriented prior
+  bool has_diag = false;
   size_t total;
   int64_t total_px, total_rowbuf;
   int total_lines, total_theta, total_units, total_prows, total_cgroups, total_btiles;

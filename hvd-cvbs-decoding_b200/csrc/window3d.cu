@@ -214,7 +214,7 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   const size_t x_caa = take(sizeof(float2) * plane * nf * AP);
   const size_t x_wa = take(sizeof(float) * plane * nf * AP);
   const size_t x_res = take(sizeof(float) * plane * nf * AP);
-  const size_t x_jp = take(sizeof(float4) * 10 * plane * nf * AP);
+  const size_t x_jp = take(sizeof(float4) * (cfg.diag_prior > 0.0f ? 11 : 10) * plane * nf * AP);
   const size_t x_jm2 = take(sizeof(float) * plane * nf * AP);
   const int jbx = (w + 31) / 32, jby = (h + 7) / 8;
   const size_t x_jpart = take(sizeof(double) * 5 * (size_t)jbx * jby * nf * AP);
@@ -740,6 +740,8 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
         ja.M0 = jp + 8 * bp;
         ja.M1 = jp + 9 * bp;
         ja.M2 = at<float>(ctx, X(x_jm2));
+        ja.diag = cfg.diag_prior > 0.0f ? 1 : 0;
+        ja.W2 = ja.diag ? jp + 10 * bp : nullptr;
         ja.partials = at<double>(ctx, X(x_jpart));
         ja.ctl = d_jctl;
         const FieldDesc& f0 = b.fields[col[0]];

@@ -94,7 +94,7 @@ typedef struct hvdg_config {
   float charbonnier_eps;     /* 0.5  */
   float chroma_eps;          /* 1.0  */
   float structure_coupling;  /* 0.25 */
-  float diag_prior;          /* 0.0; > 0 is HVDG_ERR_UNSUPPORTED on the device path */
+  float diag_prior;          /* 0.0; > 0 adds the oriented +-45 deg chroma prior (the adjoint refuses it) */
   int32_t cg_iterations;     /* 2    */
   int32_t irls_outer;        /* 4    */
   float cg_tol;              /* 0 = auto (0.02 slow / 0.10 fast) */
