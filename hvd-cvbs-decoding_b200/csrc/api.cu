@@ -386,6 +386,90 @@ hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref, const float*
   return HVDG_OK;
 }
 
+hvdg_status hvdg_verify_motion(hvdg_ctx* ctx, const float* y_ref, const float* y_cur, int h,
+                               int w, int tile, const float* pdy, const float* pdx, float* dy,
+                               float* dx, float* confidence) {
+  settle(ctx);
+  if (!ctx || !y_ref || !y_cur || !pdy || !pdx || !dy || !dx || !confidence || h < 1 || w < 1 ||
+      tile < 1)
+    return HVDG_ERR_BAD_ARGUMENT;
+  if (tile > 4096) return HVDG_ERR_UNSUPPORTED;
+  cudaSetDevice(ctx->device);
+  const int pitch = (w + hvdg::kStrip - 1) / hvdg::kStrip * hvdg::kStrip;
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const size_t plane = (size_t)h * pitch, nt = (size_t)th * tw;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o = align_up(o + bytes, 256);
+    return r;
+  };
+  const size_t o_f = take(sizeof(hvdg::MeField) * 2);
+  const size_t o_p = take(sizeof(hvdg::MePair));
+  const size_t o_l = take(sizeof(float) * 2 * plane);
+  const size_t o_t = take(sizeof(float) * 2 * plane);
+  const size_t o_b = take(sizeof(float) * 2 * plane);
+  size_t ot[10];
+  for (int i = 0; i < 10; ++i) ot[i] = take(sizeof(float) * nt);
+  hvdg_status st = ctx->arena.reserve(o, ctx->stream);
+  if (st != HVDG_OK) return st;
+  ctx->epoch += 1;
+  char* base = static_cast<char*>(ctx->arena.base);
+  hvdg::MeField mf[2];
+  std::memset(mf, 0, sizeof(mf));
+  for (int i = 0; i < 2; ++i) {
+    mf[i].h = h;
+    mf[i].w = w;
+    mf[i].pitch = pitch;
+    mf[i].dpitch = pitch / 4;
+    mf[i].y_off = mf[i].t_off = mf[i].b_off = (int64_t)i * plane;
+  }
+  hvdg::MePair pr;  // plane 0 holds y_cur, plane 1 y_ref
+  pr.ref = 1;
+  pr.cur = 0;
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(base + o_f, mf, sizeof(mf), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_p, &pr, sizeof(pr), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(base + o_l, sizeof(float) * pitch, y_cur, sizeof(float) * w,
+                          sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(base + o_l + sizeof(float) * plane, sizeof(float) * pitch, y_ref,
+                          sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + ot[8], pdy, sizeof(float) * nt, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + ot[9], pdx, sizeof(float) * nt, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "H2D verify inputs");
+  hvdg::MeArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.tile = tile;
+  a.search = 0;
+  a.coarse_off = 1;
+  a.tiles_off = (int)nt;
+  hvdg::MeBuffers mb;
+  std::memset(&mb, 0, sizeof(mb));
+  mb.luma = reinterpret_cast<const float*>(base + o_l);
+  mb.tmp = reinterpret_cast<float*>(base + o_t);
+  mb.blur = reinterpret_cast<float*>(base + o_b);
+  auto P = [&](int i) { return reinterpret_cast<float*>(base + ot[i]); };
+  const hvdg::MeField* d_f = reinterpret_cast<const hvdg::MeField*>(base + o_f);
+  const hvdg::MePair* d_p = reinterpret_cast<const hvdg::MePair*>(base + o_p);
+  hvdg::launch_motion_blur(d_f, 2, h, w, mb, s);
+  hvdg::launch_traj_verify(d_f, d_p, 0, 1, nullptr, nullptr, nullptr, mb.blur, h, w, a, nullptr,
+                           nullptr, P(0), P(1), P(2), P(3), P(4), s, P(8), P(9));
+  hvdg::launch_me_confidence(d_f, d_p, 1, h, w, a, mb.blur, P(0), P(1), P(2), P(3), P(4), P(5),
+                             P(6), P(7), s);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, P(5), sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dx, P(6), sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(confidence, P(7), sizeof(float) * nt, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "motion verification");
+  return HVDG_OK;
+}
+
 hvdg_status hvdg_set_debug_dir(hvdg_ctx* ctx, const char* dir) {
   if (!ctx) return HVDG_ERR_BAD_ARGUMENT;
   ctx->debug_dir = dir ? dir : "";

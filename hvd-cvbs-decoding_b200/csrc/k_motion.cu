@@ -595,6 +595,13 @@ __global__ void __launch_bounds__(256) k_me_confidence(const MeField* __restrict
   }
 }
 
+void launch_motion_blur(const MeField* d_fields, int nf, int max_h, int max_w, const MeBuffers& b,
+                        cudaStream_t st) {
+  if (nf <= 0) return;
+  k_blur_v<<<dim3((max_w + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.luma, b.tmp, 2, 0);
+  k_blur_h<<<dim3((max_h + 31) / 32, nf), 32, 0, st>>>(d_fields, nf, b.tmp, b.blur, 2);
+}
+
 void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const MePair* d_pairs,
                    int npairs, const MeArgs& a, const MeBuffers& b, cudaStream_t st) {
   if (nf <= 0 || npairs <= 0) return;
@@ -1239,46 +1246,87 @@ __global__ void k_traj_snap(const MeField* __restrict__ mf, const MePair* __rest
 }
 
 // Fast-mode prediction (sequence.cpp:714-763) + VerifyMotion (motion.cpp:490-530).
+// Sum of squared differences over one tile with no bail-out (a lone
+// candidate: BmPass's kill stays infinite), rows in order and each row in
+// order -- the reference's float additions -- with each row's samples
+// loaded ahead of its additions.
+__device__ __forceinline__ float tile_ssd_full(const float* A, const float* B, int pitch, int h,
+                                               int w, int ty0, int ty1, int tx0, int tx1, int sy,
+                                               int sx) {
+  float acc = 0.0f;
+  for (int y = ty0; y < ty1; ++y) {
+    const float* arow = A + (int64_t)y * pitch;
+    const float* brow = B + (int64_t)clampi(y - sy, 0, h - 1) * pitch;
+    int x = tx0;
+    for (; x + 8 <= tx1; x += 8) {
+      float d[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) d[k] = arow[x + k] - brow[clampi(x + k - sx, 0, w - 1)];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc += d[k] * d[k];
+    }
+    for (; x < tx1; ++x) {
+      const float diff = arow[x] - brow[clampi(x - sx, 0, w - 1)];
+      acc += diff * diff;
+    }
+  }
+  return acc;
+}
+
+// VerifyMotion (motion.cpp:490-530) of pair base + i: one SSD at the rounded
+// prediction, one at zero, the prediction kept where it is strictly better.
+// The prediction is the trajectory median over the searched pairs of its
+// group (sequence.cpp:714-763), or, with pred_dy / pred_dx given, the
+// caller's per-tile vectors. Two adjacent threads per tile: the even one
+// evaluates the prediction, the odd one zero.
 __global__ void k_traj_verify(const MeField* __restrict__ mf, const MePair* __restrict__ pairs,
                               int base, int npred, const int* __restrict__ grp,
                               const TrajGroup* __restrict__ searched,
                               const TrajPair* __restrict__ tp, const float* __restrict__ blur,
                               MeArgs a, const float* __restrict__ dy_in,
-                              const float* __restrict__ dx_in, float* __restrict__ out_mdy,
+                              const float* __restrict__ dx_in, const float* __restrict__ pred_dy,
+                              const float* __restrict__ pred_dx, float* __restrict__ out_mdy,
                               float* __restrict__ out_mdx, float* __restrict__ out_sdy,
                               float* __restrict__ out_sdx, float* __restrict__ out_best) {
   const int i = blockIdx.y;
-  if (i >= npred) return;
+  if (i >= npred) return;  // uniform per block
   const int p = base + i;
   const MePair pr = pairs[p];
   const MeField mc = mf[pr.cur], mr = mf[pr.ref];
   const int h = mc.h, w = mc.w, tile = a.tile;
   const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= th * tw) return;
-  const TrajGroup S = searched[grp[i]];
-  float sy[kTrajMaxPairs], sx[kTrajMaxPairs];
-  for (int k = 0; k < S.count; ++k) {
-    const int q = S.pair[k];
-    const TrajPair m = tp[q];
-    const float of = (float)m.offset;
-    sy[k] = (dy_in[a.tiles_off * q + t] - m.parity_shift) / of;
-    sx[k] = dx_in[a.tiles_off * q + t] / of;
+  const int tt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = tt >> 1, cand = tt & 1;
+  const bool valid = t < th * tw;
+  float pdy = 0.0f, pdx = 0.0f, ssd = 0.0f;
+  if (valid) {
+    if (pred_dy) {
+      pdy = pred_dy[a.tiles_off * i + t];
+      pdx = pred_dx[a.tiles_off * i + t];
+    } else {
+      const TrajGroup S = searched[grp[i]];
+      float sy[kTrajMaxPairs], sx[kTrajMaxPairs];
+      for (int k = 0; k < S.count; ++k) {
+        const int q = S.pair[k];
+        const TrajPair m = tp[q];
+        const float of = (float)m.offset;
+        sy[k] = (dy_in[a.tiles_off * q + t] - m.parity_shift) / of;
+        sx[k] = dx_in[a.tiles_off * q + t] / of;
+      }
+      const float vym0 = S.count > 0 ? median_small(sy, S.count) : 0.0f;
+      const float vxm0 = S.count > 0 ? median_small(sx, S.count) : 0.0f;
+      const TrajPair me = tp[p];
+      pdy = (float)me.offset * vym0 + me.parity_shift;
+      pdx = (float)me.offset * vxm0;
+    }
+    const int iy = cand == 0 ? (int)lroundf(pdy) : 0, ix = cand == 0 ? (int)lroundf(pdx) : 0;
+    const int y0 = (t / tw) * tile, y1 = min(y0 + tile, h);
+    const int x0 = (t % tw) * tile, x1 = min(x0 + tile, w);
+    ssd = tile_ssd_full(blur + mc.b_off, blur + mr.b_off, mc.pitch, h, w, y0, y1, x0, x1, iy, ix);
   }
-  const float vym0 = S.count > 0 ? median_small(sy, S.count) : 0.0f;
-  const float vxm0 = S.count > 0 ? median_small(sx, S.count) : 0.0f;
-  const TrajPair me = tp[p];
-  const float pdy = (float)me.offset * vym0 + me.parity_shift;
-  const float pdx = (float)me.offset * vxm0;
-  const int iy = (int)lroundf(pdy), ix = (int)lroundf(pdx);
-  const float* A = blur + mc.b_off;
-  const float* B = blur + mr.b_off;
-  const int y0 = (t / tw) * tile, y1 = min(y0 + tile, h);
-  const int x0 = (t % tw) * tile, x1 = min(x0 + tile, w);
-  const float inf = __int_as_float(0x7f800000);
-  // one relative candidate at the rounded prediction, one absolute at zero
-  const float pred = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, iy, ix, inf) * 1.0f;
-  const float zero = tile_ssd(A, B, mc.pitch, h, w, y0, y1, x0, x1, 0, 0, inf) * 1.0f;
+  const float zero = __shfl_down_sync(0xffffffffu, ssd, 1);
+  if (!valid || cand != 0) return;
+  const float pred = ssd;
   const int o = a.tiles_off * p + t;
   if (zero <= pred) {
     out_mdy[o] = 0.0f;
@@ -1418,12 +1466,13 @@ void launch_traj_verify(const MeField* d_fields, const MePair* d_pairs, int base
                         const int* d_grp, const TrajGroup* d_searched, const TrajPair* d_tp,
                         const float* blur, int max_h, int max_w, const MeArgs& a,
                         const float* dy_in, const float* dx_in, float* mdy, float* mdx,
-                        float* sdy, float* sdx, float* best, cudaStream_t st) {
+                        float* sdy, float* sdx, float* best, cudaStream_t st,
+                        const float* pred_dy, const float* pred_dx) {
   if (npred <= 0) return;
   const int nt = ((max_h + a.tile - 1) / a.tile) * ((max_w + a.tile - 1) / a.tile);
-  k_traj_verify<<<dim3((nt + 63) / 64, npred), 64, 0, st>>>(d_fields, d_pairs, base, npred, d_grp,
-                                                           d_searched, d_tp, blur, a, dy_in, dx_in,
-                                                           mdy, mdx, sdy, sdx, best);
+  k_traj_verify<<<dim3((2 * nt + 63) / 64, npred), 64, 0, st>>>(
+      d_fields, d_pairs, base, npred, d_grp, d_searched, d_tp, blur, a, dy_in, dx_in, pred_dy,
+      pred_dx, mdy, mdx, sdy, sdx, best);
 }
 
 void launch_me_confidence(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,

@@ -87,7 +87,12 @@ void launch_traj_verify(const MeField* d_fields, const MePair* d_pairs, int base
                         const int* d_grp, const TrajGroup* d_searched, const TrajPair* d_tp,
                         const float* blur, int max_h, int max_w, const MeArgs& a,
                         const float* dy_in, const float* dx_in, float* mdy, float* mdx,
-                        float* sdy, float* sdx, float* best, cudaStream_t st);
+                        float* sdy, float* sdx, float* best, cudaStream_t st,
+                        const float* pred_dy = nullptr, const float* pred_dx = nullptr);
+// BoxBlur(r = 2) of every field's luma into b.blur (motion.cpp:399-400), as
+// launch_motion does first.
+void launch_motion_blur(const MeField* d_fields, int nf, int max_h, int max_w, const MeBuffers& b,
+                        cudaStream_t st);
 // MotionConfidence + final vectors for `npairs` pairs whose tile arrays start
 // at the given pointers (pair i at offset i * a.tiles_off).
 void launch_me_confidence(const MeField* d_fields, const MePair* d_pairs, int npairs, int max_h,

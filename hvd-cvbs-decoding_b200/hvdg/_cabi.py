@@ -378,6 +378,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.hvdg_estimate_motion.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_int, vp, vp, vp]
     lib.hvdg_estimate_motion.restype = C.c_int
+    lib.hvdg_verify_motion.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp]
+    lib.hvdg_verify_motion.restype = C.c_int
     lib.hvdg_holographic_init_noalloc.argtypes = [vp, vp, vp, P(Geometry), vp, vp]
     lib.hvdg_holographic_init_noalloc.restype = C.c_int
     lib.hvdg_decode_fields_adjoint.argtypes = [vp, P(FieldIn), C.c_int, P(Config), P(vp), P(vp),

@@ -291,6 +291,23 @@ class Context:
                     "hvdg_estimate_motion")
         return dy, dx, cf
 
+    def verify_motion(self, y_ref, y_cur, pdy, pdx, tile: int = 32):
+        """VerifyMotion (motion.cpp:490-530): per-tile predictions audited
+        against zero; returns (dy, dx, confidence) per tile."""
+        a = np.ascontiguousarray(y_ref, dtype=np.float32)
+        b = np.ascontiguousarray(y_cur, dtype=np.float32)
+        h, w = a.shape
+        pdy = np.ascontiguousarray(pdy, dtype=np.float32)
+        pdx = np.ascontiguousarray(pdx, dtype=np.float32)
+        if pdy.shape != (-(-h // tile), -(-w // tile)) or pdx.shape != pdy.shape:
+            raise ValueError("predictions must have one value per tile")
+        dy, dx, cf = (np.zeros(pdy.shape, np.float32) for _ in range(3))
+        self._check(self.lib.hvdg_verify_motion(self._h, a.ctypes.data, b.ctypes.data, h, w, tile,
+                                                pdy.ctypes.data, pdx.ctypes.data, dy.ctypes.data,
+                                                dx.ctypes.data, cf.ctypes.data),
+                    "hvdg_verify_motion")
+        return dy, dx, cf
+
 
 def default_config(**kw) -> Config:
     return _cabi.config_copy(_cabi.default_config(), **kw)

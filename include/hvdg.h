@@ -410,6 +410,17 @@ hvdg_status hvdg_estimate_motion(hvdg_ctx* ctx, const float* y_ref,
                                  int search, int me_mode, float* dy, float* dx,
                                  float* confidence);
 
+/* VerifyMotion (motion.cpp:490-530, declared motion.h:74-75): the predicted
+ * per-tile vectors pdy / pdx (ceil(h/tile) x ceil(w/tile), e.g. from a
+ * trajectory fit) audited on the r = 2 box-blurred planes -- one SSD at the
+ * rounded prediction, one at zero, the full prediction kept where it is
+ * strictly better -- and MotionConfidence of the result; outputs per tile
+ * like hvdg_estimate_motion. The fast 3-D window runs the same kernel on its
+ * trajectory predictions. */
+hvdg_status hvdg_verify_motion(hvdg_ctx* ctx, const float* y_ref, const float* y_cur, int h,
+                               int w, int tile, const float* pdy, const float* pdx, float* dy,
+                               float* dx, float* confidence);
+
 /* ------------------------------------------------------------------------ */
 /* Adjoint                                                                   */
 /* ------------------------------------------------------------------------ */

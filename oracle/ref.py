@@ -52,6 +52,7 @@ def _declare(L):
     L.hvdref_variational_refine.argtypes = [vp, vp, vp, C.c_int, C.c_int, P(_cabi.Config),
                                             C.c_int, C.c_int, P(vp), P(vp), P(vp), vp, vp]
     L.hvdref_estimate_motion.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]
+    L.hvdref_verify_motion.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp]
     L.hvdref_box_blur.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     L.hvdref_vectors_per_pixel.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                            vp, vp]
@@ -161,6 +162,17 @@ def estimate_motion(y_ref, y_cur, tile=32, search=16):
     dx = np.zeros_like(dy)
     cf = np.zeros_like(dy)
     lib().hvdref_estimate_motion(_p(a), _p(b), h, w, tile, search, _p(dy), _p(dx), _p(cf))
+    return dy, dx, cf
+
+
+def verify_motion(y_ref, y_cur, pdy, pdx, tile=32):
+    """VerifyMotion (motion.cpp:490-530) of the compiled reference."""
+    a, b = _f32(y_ref), _f32(y_cur)
+    h, w = a.shape
+    pdy, pdx = _f32(pdy), _f32(pdx)
+    dy, dx, cf = (np.zeros(pdy.shape, np.float32) for _ in range(3))
+    lib().hvdref_verify_motion(_p(a), _p(b), h, w, int(tile), _p(pdy), _p(pdx), _p(dy), _p(dx),
+                               _p(cf))
     return dy, dx, cf
 
 

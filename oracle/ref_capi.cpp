@@ -144,6 +144,19 @@ int hvdref_estimate_motion(const float* y_ref, const float* y_cur, int h, int w,
   return 0;
 }
 
+// VerifyMotion (motion.cpp:490-530): predictions pdy / pdx per tile.
+int hvdref_verify_motion(const float* y_ref, const float* y_cur, int h, int w, int tile,
+                         const float* pdy, const float* pdx, float* dy, float* dx, float* conf) {
+  const int th = (h + tile - 1) / tile, tw = (w + tile - 1) / tile;
+  const hvd::MotionField m =
+      hvd::VerifyMotion(PlaneFrom(y_ref, h, w), PlaneFrom(y_cur, h, w), PlaneFrom(pdy, th, tw),
+                        PlaneFrom(pdx, th, tw), tile);
+  PlaneTo(m.dy, dy);
+  PlaneTo(m.dx, dx);
+  PlaneTo(m.confidence, conf);
+  return 0;
+}
+
 // BoxBlur (motion.cpp:391), in place.
 void hvdref_box_blur(float* a, int h, int w, int r) {
   const hvd::Plane o = hvd::BoxBlur(PlaneFrom(a, h, w), r);

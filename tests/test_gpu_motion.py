@@ -69,3 +69,36 @@ def test_sad_motion_bit_exact_vs_restatement(ctx, kind, block, rng_):
     assert np.array_equal(dy, ody)
     assert np.array_equal(dx, odx)
     assert np.array_equal(cf, ocf)
+
+
+@pytest.mark.parametrize("kind,tile", [("ntsc", 32), ("pal", 32), ("odd", 16)])
+def test_verify_motion_bit_exact_vs_reference(ctx, kind, tile):
+    """VerifyMotion (motion.cpp:490-530) -- the fast 3-D window's audit of
+    its trajectory predictions -- through hvdg_verify_motion against the
+    compiled reference: identical vectors and confidences, with predictions
+    that win (near the true shift), lose to zero and tie with it."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    if kind == "odd":
+        a, b = _sad_pair("odd")
+    else:
+        std = _cabi.STD_NTSC if kind == "ntsc" else _cabi.STD_PAL
+        seq = synth.make_sequence(19 + std, std, 3, moving=True)
+        a, b = seq[0].y_true.astype(np.float32), seq[2].y_true.astype(np.float32)
+    h, w = a.shape
+    th, tw = -(-h // tile), -(-w // tile)
+    rng = np.random.default_rng(tile + h)
+    mdy, mdx, _ = ctx.estimate_motion(a, b, tile, 8)
+    # predictions: the searched vectors, perturbed by up to +-1.5 px, some
+    # exactly zero (ties with the zero candidate)
+    pdy = (mdy + rng.uniform(-1.5, 1.5, (th, tw))).astype(np.float32)
+    pdx = (mdx + rng.uniform(-1.5, 1.5, (th, tw))).astype(np.float32)
+    pdy[rng.random((th, tw)) < 0.15] = 0.0
+    pdx[rng.random((th, tw)) < 0.15] = 0.0
+    dy, dx, cf = ctx.verify_motion(a, b, pdy, pdx, tile)
+    rdy, rdx, rcf = ref.verify_motion(a, b, pdy, pdx, tile)
+    kept = (dy == pdy) & (dx == pdx)
+    print(f"{kind} tile {tile}: {kept.mean():.2f} of the predictions kept")
+    assert 0.0 < kept.mean() < 1.0
+    assert np.array_equal(dy, rdy) and np.array_equal(dx, rdx) and np.array_equal(cf, rcf)
