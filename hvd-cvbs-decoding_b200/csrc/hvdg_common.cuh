@@ -75,7 +75,13 @@ __device__ inline float block_select_kth(const float* v, int n, int k, unsigned*
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const uint32_t key = float_key(v[i]);
-      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+      // lanes counting into the same bin add once through their lowest lane
+      // (the keys of one selection crowd a few bins: without this the
+      // shared-memory atomics of a warp serialise)
+      const unsigned bin = (key & mask) == prefix ? (key >> shift) & 255u : 256u;
+      const unsigned peers = __match_any_sync(__activemask(), bin);
+      if (bin < 256u && (int)(__ffs(peers) - 1) == (int)(threadIdx.x & 31))
+        atomicAdd(&hist[bin], (unsigned)__popc(peers));
     }
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -42,6 +42,8 @@ struct FieldDesc {
   float diag_prior;    // oriented +-45 deg chroma prior weight (0 = off)
   float mu_h, mu_v;    // written by the aniso kernel
   float mu_d;          // oriented prior weight, written by the aniso kernel (0 = off)
+  float aniso_p98[2];  // the aniso kernel's horizontal / vertical p98 (scratch)
+  int aniso_arrive;    // the aniso kernel's per-field arrivals (two per run)
   float nu;            // temporal strength (0 = 2-D)
   float eps_t;         // temporal robust scale
   int has_nbr;         // 3-D neighbour terms present (M / b planes valid)

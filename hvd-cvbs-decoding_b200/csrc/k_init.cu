@@ -727,18 +727,20 @@ __global__ void __launch_bounds__(256) k_init_blend(InitArgs a) {
 }
 
 // ---- auto chroma anisotropy (variational.cpp:130-196) ----------------------
-// One CTA (1024 threads) per field: p98 of |delta| of 2-line (NTSC) / 4-line
-// (PAL) group averages, sampled at odd group rows and every 3rd column,
-// exact k-th element by radix select; the horizontal and the vertical
-// samples take turns in one shared buffer.
+// Two CTAs (1024 threads) per field, one per axis: p98 of |delta| of 2-line
+// (NTSC) / 4-line (PAL) group averages, sampled at odd group rows and every
+// 3rd column, horizontal (axis 0) or vertical (axis 1) neighbour, exact k-th
+// element by radix select. The field's second CTA to finish maps the ratio
+// of the two to the split and writes mu_h, mu_v, mu_d.
 constexpr int kAnisoMax = 49152;
 __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2* __restrict__ chi0) {
   extern __shared__ float sm_an[];
   __shared__ unsigned hist[256];
   __shared__ unsigned bc[2];
+  __shared__ int last;
   FieldDesc& f = fields[blockIdx.x];
-  float aniso = f.aniso_cfg;
-  if (!(aniso > 0.0f)) {
+  const int axis = blockIdx.y;
+  if (!(f.aniso_cfg > 0.0f)) {
     const int group = f.is_pal ? 4 : 2;
     const int Hh = f.h / group;
     const int nt = Hh / 2;                // t = 1, 3, 5, ... < Hh
@@ -747,39 +749,47 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
     if (n > kAnisoMax) n = kAnisoMax;     // geometry guard (the host rejects larger)
     const float2* c = chi0 + f.px_off;
     const float inv = 1.0f / (float)group;
-    float p98[2] = {0.f, 0.f};
-    for (int axis = 0; axis < 2; ++axis) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int ti = i / nx, xi = i % nx;
-        const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
-        float2 p = make_float2(0.f, 0.f), q = p;
-        for (int k = 0; k < group; ++k) {
-          p = cadd(p, c[(int64_t)(group * tt + k) * f.pitch + x]);
-          q = cadd(q, axis == 0 ? c[(int64_t)(group * tt + k) * f.pitch + x - 1]
-                                : c[(int64_t)(group * (tt - 1) + k) * f.pitch + x]);
-        }
-        sm_an[i] = sqrtf(cnorm(csub(cscale(p, inv), cscale(q, inv))));
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int ti = i / nx, xi = i % nx;
+      const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
+      float2 p = make_float2(0.f, 0.f), q = p;
+      for (int k = 0; k < group; ++k) {
+        p = cadd(p, c[(int64_t)(group * tt + k) * f.pitch + x]);
+        q = cadd(q, axis == 0 ? c[(int64_t)(group * tt + k) * f.pitch + x - 1]
+                              : c[(int64_t)(group * (tt - 1) + k) * f.pitch + x]);
       }
-      __syncthreads();
-      if (n > 0) p98[axis] = block_select_kth(sm_an, n, n - 1 - n / 50, hist, bc);
-      __syncthreads();
+      sm_an[i] = sqrtf(cnorm(csub(cscale(p, inv), cscale(q, inv))));
     }
-    const float r = p98[1] / fmaxf(p98[0], 1e-6f);
+    __syncthreads();
+    const float p98 = n > 0 ? block_select_kth(sm_an, n, n - 1 - n / 50, hist, bc) : 0.f;
+    if (threadIdx.x == 0) f.aniso_p98[axis] = p98;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    // two arrivals per run (the counter is not reset between graph replays)
+    last = (atomicAdd(&f.aniso_arrive, 1) & 1) == 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  float aniso = f.aniso_cfg;
+  if (!(aniso > 0.0f)) {
+    const float p0 = __ldcg(&f.aniso_p98[0]), p1 = __ldcg(&f.aniso_p98[1]);
+    const float r = p1 / fmaxf(p0, 1e-6f);
     if (f.is_pal)
       aniso = fminf(fmaxf(0.7f + 0.9f * (r - 1.3f), 0.55f), 1.0f);
     else
       aniso = fminf(fmaxf(0.5f + 1.1f * (r - 1.3f), 0.5f), 1.0f);
   }
-  if (threadIdx.x == 0) {
-    // the oriented prior's weight, and the renormalisation that keeps the
-    // total chroma prior mass (variational.cpp:207-219)
-    const float mu_d = f.lambda_c * f.diag_prior * 0.5f;
-    const float tot0 = f.lambda_c * (1.0f + aniso);
-    const float scale = mu_d > 0.0f ? tot0 / (tot0 + 2.0f * mu_d) : 1.0f;
-    f.mu_h = (f.lambda_c * aniso) * scale;
-    f.mu_v = f.lambda_c * scale;
-    f.mu_d = mu_d > 0.0f ? mu_d * scale : 0.0f;
-  }
+  // the oriented prior's weight, and the renormalisation that keeps the
+  // total chroma prior mass (variational.cpp:207-219)
+  const float mu_d = f.lambda_c * f.diag_prior * 0.5f;
+  const float tot0 = f.lambda_c * (1.0f + aniso);
+  const float scale = mu_d > 0.0f ? tot0 / (tot0 + 2.0f * mu_d) : 1.0f;
+  f.mu_h = (f.lambda_c * aniso) * scale;
+  f.mu_v = f.lambda_c * scale;
+  f.mu_d = mu_d > 0.0f ? mu_d * scale : 0.0f;
 }
 
 constexpr int kAnisoSmem = kAnisoMax * (int)sizeof(float);
@@ -841,7 +851,7 @@ void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cg
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {
   const int smem = kAnisoSmem;
   configure_init_kernels();
-  if (n_fields > 0) k_aniso<<<n_fields, 1024, smem, st>>>(d_fields, chi0);
+  if (n_fields > 0) k_aniso<<<dim3(n_fields, 2), 1024, smem, st>>>(d_fields, chi0);
 }
 
 int aniso_max_samples() { return kAnisoMax; }
