@@ -68,3 +68,90 @@ def test_two_rank_sharding_and_reduction():
     sys.path.insert(0, str(REPO))
     import bench
     assert bench.throughput(16, 5, 2, 1000.0) == 160.0
+
+
+def _chunk_worker(rank, world, port, q):
+    """Rank `rank` decodes its share of a 9-frame NTSC sequence's export
+    chunks (3-frame cores, 1 frame of context each side) through the
+    compiled reference engine's DecodeFrameSequenceWindow -- the decode
+    runs on the host here; the sharding, the halo windows and the gather
+    are the multi-GPU path's own -- and rank 0 gathers the frames."""
+    sys.path.insert(0, str(REPO))
+    sys.path.insert(0, str(REPO / "hvd-cvbs-decoding_b200"))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from hvdg import _cabi, api, sequence, synth
+    from oracle import ref
+    ref.set_threads(2)
+    frames, _ = synth.make_frames(91, _cabi.STD_NTSC, 9, noise_sigma=0.5, moving=True)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = api.default_config(irls_outer=2, cg_iterations=8, fast=1, cg_tol=1e-6,
+                             temporal_strength=0.5, passes=1, nr_anchor=0.0)
+    chunks = sequence.plan_chunks(0, len(frames) - 1, 3, 1, sequence.is_coupled(cfg))
+    mine = sequence.shard(chunks, world, rank)
+
+    def decode(win, cb, ce):
+        return ref.decode_frame_sequence_window(win, cb, ce, fp, cfg)
+
+    local = sequence.decode_chunks(decode, frames, mine)
+    got = sequence.gather_frames(local, len(chunks), dist)
+    q.put((rank, [c.index for c in mine], None if got is None else
+           [fr["luma"].tobytes() + fr["chroma"].tobytes() for fr in got]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_chunked_window_sharding():
+    """Chunks with their replicated halo frames decode the same on two
+    ranks as on one: every core frame comes back exactly once, in order,
+    equal to the single-process chunked decode."""
+    sys.path.insert(0, str(REPO))
+    from oracle import ref
+    if not ref.available():
+        import pytest
+        pytest.skip("reference engine not built")
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_chunk_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=600) for _ in range(world)], key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert res[0][1] == [0, 2] and res[1][1] == [1]
+    assert res[1][2] is None
+    gathered = res[0][2]
+    assert len(gathered) == 9
+    from hvdg import _cabi, api, sequence, synth
+    frames, _ = synth.make_frames(91, _cabi.STD_NTSC, 9, noise_sigma=0.5, moving=True)
+    fp = api.frame_params(_cabi.STD_NTSC)
+    cfg = api.default_config(irls_outer=2, cg_iterations=8, fast=1, cg_tol=1e-6,
+                             temporal_strength=0.5, passes=1, nr_anchor=0.0)
+    ref.set_threads(2)
+    chunks = sequence.plan_chunks(0, 8, 3, 1, True)
+    single = sequence.gather_frames(sequence.decode_chunks(
+        lambda w, cb, ce: ref.decode_frame_sequence_window(w, cb, ce, fp, cfg), frames, chunks),
+        len(chunks))
+    assert gathered == [fr["luma"].tobytes() + fr["chroma"].tobytes() for fr in single]
+
+
+def test_chunk_plan_matches_the_stage():
+    """The stage's chunk windows (hvd_chroma_decoder_stage.cpp:711-716,
+    997-1060): cores tile the range, windows add the overlap clipped to the
+    range, no overlap when the fields are decoupled; shards are disjoint
+    and cover every chunk."""
+    sys.path.insert(0, str(REPO / "hvd-cvbs-decoding_b200"))
+    from hvdg import sequence
+    cs = sequence.plan_chunks(10, 23, 6, 1, True)
+    assert [(c.first, c.last, c.w0, c.w1) for c in cs] == [(10, 15, 10, 16), (16, 21, 15, 22),
+                                                           (22, 23, 21, 23)]
+    assert [(c.core_begin, c.core_end) for c in cs] == [(0, 6), (1, 7), (1, 3)]
+    cs0 = sequence.plan_chunks(10, 23, 6, 1, False)
+    assert all(c.w0 == c.first and c.w1 == c.last for c in cs0)
+    for world in (1, 2, 3, 8):
+        got = sorted(c.index for r in range(world) for c in sequence.shard(cs, world, r))
+        assert got == [c.index for c in cs]
