@@ -20,6 +20,7 @@
 
 #include "hvdg_common.cuh"
 #include "k_motion.h"
+#include "per_device.h"
 
 namespace hvdg {
 
@@ -654,6 +655,11 @@ constexpr float kQuantZero = 16384.0f;   // 0 IRE
 constexpr float kQuantScale = 348.16f;   // codes per IRE
 constexpr int kSadMaxBlock = 32;
 constexpr int kSadMaxRange = 22;         // (2 range + 1)^2 visit indices fit in 11 bits
+// block, window and the window's integral image at the largest block and range
+constexpr int kSadMaxWin = kSadMaxBlock + 2 * (kSadMaxRange + 1);
+constexpr int kSadMaxSmem =
+    (kSadMaxBlock * kSadMaxBlock + kSadMaxWin * kSadMaxWin + (kSadMaxWin + 1) * (kSadMaxWin + 1)) *
+    (int)sizeof(int);
 constexpr int kSadThreads = 192;
 
 int sad_max_block() { return kSadMaxBlock; }
@@ -720,44 +726,37 @@ __device__ __forceinline__ int centre_out_index(int d) {
   return d == 0 ? 0 : (d > 0 ? 2 * d : -2 * d - 1);
 }
 
-// Block and window live in shared memory as packed halfword pairs: the
-// block's row yy as Ap[yy * hb + k] = A(yy, 2k) | A(yy, 2k + 1) << 16 (zero
-// past the tile's width), the window as Bp[i] = B[i] | B[i + 1] << 16 (every
-// starting column, so a pair at any offset is one word). Quantised samples
-// are 16-bit codes, so one __vsadu2 adds two exact absolute differences.
-__device__ __forceinline__ int sad_a(const unsigned* Ap, int hb, int yy, int xx) {
-  return (int)((Ap[yy * hb + (xx >> 1)] >> ((xx & 1) * 16)) & 0xFFFFu);
-}
-__device__ __forceinline__ int sad_b(const unsigned* Bp, int i) { return (int)(Bp[i] & 0xFFFFu); }
-
 // SAD (or SSD) over the tile of source offset (dy, dx), one warp (lanes over pixels).
-__device__ __forceinline__ unsigned long long warp_tile_cost(const unsigned* Ap, const unsigned* Bp,
-                                                             int hb, int ww, int S, int bh, int bw,
+__device__ __forceinline__ unsigned long long warp_tile_cost(const int* As, const int* Bs, int b,
+                                                             int ww, int S, int bh, int bw,
                                                              int dy, int dx, bool squared,
                                                              int lane) {
   unsigned long long acc = 0;
   for (int i = lane; i < bh * bw; i += 32) {
     const int yy = i / bw, xx = i % bw;
-    const int d = sad_a(Ap, hb, yy, xx) - sad_b(Bp, (yy - dy + S) * ww + (xx - dx + S));
+    const int d = As[yy * b + xx] - Bs[(yy - dy + S) * ww + (xx - dx + S)];
     acc += squared ? (unsigned long long)((long long)d * d) : (unsigned long long)abs(d);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   return acc;
 }
 
-// The exhaustive scan: each thread owns one dy and G consecutive dx; every
-// packed pair of the block is compared with the G window pairs under it
-// (a word per candidate), so each window word loaded serves several
-// candidates and each __vsadu2 two pixels. Returns the thread's best key
+// The exhaustive scan. For integers |a - b| = 2 max(a, b) - a - b, so a
+// candidate's SAD is 2 sum max(A, B) - sum A - sum B over its window, the
+// last from the window's integral image: one max and one add per candidate
+// pixel, all in exact integers. Each thread owns one dy and G consecutive
+// dx; blocks of BW = 16 columns keep a register window of the G + 15 row
+// values they read (one new load per pixel). Returns the thread's best key
 // (biased cost << 11 | centre-out visit index); the thread holding (0, 0)
 // stores its SAD in *sad0.
-template <int G>
-__device__ __forceinline__ unsigned long long sad_scan(const unsigned* Ap, const unsigned* Bp,
-                                                       int hb, int ww, int S, int bh, int bw, int s,
+template <int G, int BW>
+__device__ __forceinline__ unsigned long long sad_scan(const int* As, const int* Bs,
+                                                       const int* I, int b, int ww, int S, int bh,
+                                                       int bw, int s, unsigned sum_a,
                                                        unsigned long long* sad0) {
   const int n = 2 * s + 1;
   const int ngroups = (n + G - 1) / G;
-  const int npair = bw >> 1;
+  const int wi = ww + 1;
   unsigned long long bestkey = ~0ull;
   for (int it = threadIdx.x; it < n * ngroups; it += blockDim.x) {
     const int dy = it / ngroups - s;
@@ -766,32 +765,43 @@ __device__ __forceinline__ unsigned long long sad_scan(const unsigned* Ap, const
 #pragma unroll
     for (int g = 0; g < G; ++g) acc[g] = 0u;
     for (int yy = 0; yy < bh; ++yy) {
-      const unsigned* ar = Ap + yy * hb;
-      // window pair of pixel xx under offset dxg + g starts at br[xx - g]
-      const unsigned* br = Bp + (yy - dy + S) * ww + (S - dxg);
-#pragma unroll 4
-      for (int k = 0; k < npair; ++k) {
-        const unsigned a2 = ar[k];
+      const int* ar = As + yy * b;
+      // window value under pixel xx at offset dxg + g: br[xx - g]
+      const int* br = Bs + (yy - dy + S) * ww + (S - dxg);
+      if (BW == 16) {
+        int win[16 + G - 1];  // win[j] = br[j - (G - 1)]
 #pragma unroll
-        for (int g = 0; g < G; ++g) acc[g] = __vsadu2(a2, br[2 * k - g]) + acc[g];
-      }
-      if (bw & 1) {  // the odd last pixel: its pair's high half is zero in A, masked in B
-        const unsigned a1 = ar[npair];
+        for (int j = 0; j < 16 + G - 1; ++j) win[j] = br[j - (G - 1)];
 #pragma unroll
-        for (int g = 0; g < G; ++g) acc[g] = __vsadu2(a1, br[bw - 1 - g] & 0xFFFFu) + acc[g];
+        for (int xx = 0; xx < 16; ++xx) {
+          const int av = ar[xx];
+#pragma unroll
+          for (int g = 0; g < G; ++g) acc[g] += (unsigned)max(av, win[xx - g + G - 1]);
+        }
+      } else {
+        for (int xx = 0; xx < bw; ++xx) {
+          const int av = ar[xx];
+#pragma unroll
+          for (int g = 0; g < G; ++g) acc[g] += (unsigned)max(av, br[xx - g]);
+        }
       }
     }
+    const int r0 = S - dy;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       const int dx = dxg + g;
       if (dx > s) break;
+      const int c0 = S - dx;
+      const unsigned sum_b = (unsigned)(I[(r0 + bh) * wi + c0 + bw] - I[r0 * wi + c0 + bw] -
+                                        I[(r0 + bh) * wi + c0] + I[r0 * wi + c0]);
+      const unsigned sad = 2u * acc[g] - sum_a - sum_b;
       const unsigned long long cost =
-          (unsigned long long)acc[g] * (unsigned long long)(50 + abs(dy) + abs(dx));
+          (unsigned long long)sad * (unsigned long long)(50 + abs(dy) + abs(dx));
       const unsigned long long ci =
           (unsigned long long)(centre_out_index(dy) * n + centre_out_index(dx));
       const unsigned long long key = (cost << 11) | ci;
       if (key < bestkey) bestkey = key;
-      if (dy == 0 && dx == 0) *sad0 = acc[g];
+      if (dy == 0 && dx == 0) *sad0 = sad;
     }
   }
   return bestkey;
@@ -813,38 +823,63 @@ __global__ void __launch_bounds__(kSadThreads) k_sad_search(const MeField* __res
   const int bh = min(b, h - y0), bw = min(b, w - x0);
   const int S = s + 1;          // window margin: the search range plus the sub-pel neighbours
   const int ww = b + 2 * S;
-  const int hb = (b + 1) / 2;
-  extern __shared__ unsigned sad_sm[];
-  unsigned* Ap = sad_sm;            // b rows x hb pairs
-  unsigned* Bp = sad_sm + b * hb;   // ww x ww, B(clamp(y0 - S + wy), clamp(x0 - S + wx)) pairs
+  const int wi = ww + 1;
+  extern __shared__ int sad_sm[];
+  int* As = sad_sm;             // b x b
+  int* Bs = sad_sm + b * b;     // ww x ww, B(clamp(y0 - S + wy), clamp(x0 - S + wx))
+  int* I = Bs + ww * ww;        // (ww + 1)^2 integral image of Bs
   __shared__ unsigned long long red[kSadThreads / 32];
   __shared__ unsigned long long sh_sad0, sh_best, sh_side[4], sh_ssd;
   __shared__ long long sh_s1, sh_s2;
+  __shared__ unsigned sh_suma;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int* QA = qblur + mc.b_off;
   const int* QB = qblur + mr.b_off;
-  for (int i = tid; i < bh * hb; i += blockDim.x) {
-    const int yy = i / hb, x = 2 * (i % hb);
-    const int64_t row = (int64_t)(y0 + yy) * mc.pitch + x0;
-    const unsigned lo = x < bw ? (unsigned)QA[row + x] : 0u;
-    const unsigned hi = x + 1 < bw ? (unsigned)QA[row + x + 1] : 0u;
-    Ap[i] = lo | (hi << 16);
-  }
-  const int nw = ww * ww;
-  auto win = [&](int i) -> unsigned {
+  for (int i = tid; i < bh * bw; i += blockDim.x)
+    As[(i / bw) * b + i % bw] = QA[(int64_t)(y0 + i / bw) * mc.pitch + x0 + i % bw];
+  for (int i = tid; i < ww * ww; i += blockDim.x) {
     const int wy = i / ww, wx = i % ww;
     const int sy = clampi(y0 - S + wy, 0, h - 1), sx = clampi(x0 - S + wx, 0, w - 1);
-    return (unsigned)QB[(int64_t)sy * mr.pitch + sx];
-  };
-  for (int i = tid; i < nw; i += blockDim.x)
-    Bp[i] = win(i) | ((i + 1 < nw ? win(i + 1) : 0u) << 16);
+    Bs[i] = QB[(int64_t)sy * mr.pitch + sx];
+  }
+  __syncthreads();
+  // integral image: row prefix sums, then column prefix sums (exact ints:
+  // the whole window sums below 2^31)
+  for (int r = tid; r <= ww; r += blockDim.x) {
+    int* Ir = I + r * wi;
+    Ir[0] = 0;
+    int acc = 0;
+    if (r == 0) {
+      for (int c = 1; c <= ww; ++c) Ir[c] = 0;
+    } else {
+      const int* br = Bs + (r - 1) * ww;
+      for (int c = 1; c <= ww; ++c) {
+        acc += br[c - 1];
+        Ir[c] = acc;
+      }
+    }
+  }
+  if (warp == 0) {
+    unsigned sa = 0;
+    for (int i = lane; i < bh * bw; i += 32) sa += (unsigned)As[(i / bw) * b + i % bw];
+    for (int o = 16; o > 0; o >>= 1) sa += __shfl_xor_sync(0xffffffffu, sa, o);
+    if (lane == 0) sh_suma = sa;
+  }
+  __syncthreads();
+  for (int c = tid; c <= ww; c += blockDim.x)
+    for (int r = 1; r <= ww; ++r) I[r * wi + c] += I[(r - 1) * wi + c];
   __syncthreads();
   const int n = 2 * s + 1;
+  const unsigned sum_a = sh_suma;
   // G consecutive dx per thread: 11 when it divides the row of candidates
   // (no wasted candidates at +-16), else 8
-  unsigned long long bestkey = n % 11 == 0
-                                   ? sad_scan<11>(Ap, Bp, hb, ww, S, bh, bw, s, &sh_sad0)
-                                   : sad_scan<8>(Ap, Bp, hb, ww, S, bh, bw, s, &sh_sad0);
+  unsigned long long bestkey;
+  if (n % 11 == 0)
+    bestkey = bw == 16 ? sad_scan<11, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0)
+                       : sad_scan<11, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0);
+  else
+    bestkey = bw == 16 ? sad_scan<8, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0)
+                       : sad_scan<8, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0);
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long v = __shfl_xor_sync(0xffffffffu, bestkey, o);
     if (v < bestkey) bestkey = v;
@@ -869,15 +904,15 @@ __global__ void __launch_bounds__(kSadThreads) k_sad_search(const MeField* __res
     const int oy = warp == 0 ? -1 : (warp == 1 ? 1 : 0);
     const int ox = warp == 2 ? -1 : (warp == 3 ? 1 : 0);
     const unsigned long long v =
-        warp_tile_cost(Ap, Bp, hb, ww, S, bh, bw, mdy + oy, mdx + ox, false, lane);
+        warp_tile_cost(As, Bs, b, ww, S, bh, bw, mdy + oy, mdx + ox, false, lane);
     if (lane == 0) sh_side[warp] = v;
   } else if (warp == 4) {
-    const unsigned long long v = warp_tile_cost(Ap, Bp, hb, ww, S, bh, bw, fdy, fdx, true, lane);
+    const unsigned long long v = warp_tile_cost(As, Bs, b, ww, S, bh, bw, fdy, fdx, true, lane);
     if (lane == 0) sh_ssd = v;
   } else if (warp == 5) {
     long long s1 = 0, s2 = 0;
     for (int i = lane; i < bh * bw; i += 32) {
-      const long long v = sad_a(Ap, hb, i / bw, i % bw);
+      const long long v = As[(i / bw) * b + i % bw];
       s1 += v;
       s2 += v * v;
     }
@@ -981,7 +1016,11 @@ void launch_motion_sad(const MeField* d_fields, int nf, int max_h, int max_w,
   k_sad_hsum<<<dim3((max_h + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.vsum, b.qblur);
   const int th = (max_h + a.block - 1) / a.block, tw = (max_w + a.block - 1) / a.block;
   const int ww = a.block + 2 * (a.range + 1);
-  const int smem = (a.block * ((a.block + 1) / 2) + ww * ww) * (int)sizeof(unsigned);
+  const int smem = (a.block * a.block + ww * ww + (ww + 1) * (ww + 1)) * (int)sizeof(int);
+  static PerDeviceOnce sad_once;
+  sad_once([] {
+    cudaFuncSetAttribute(k_sad_search, cudaFuncAttributeMaxDynamicSharedMemorySize, kSadMaxSmem);
+  });
   k_sad_search<<<dim3(th * tw, npairs), kSadThreads, smem, st>>>(d_fields, d_pairs, b.qblur, a, b);
   k_sad_confidence<<<npairs, 256, th * tw * (int)sizeof(double), st>>>(d_fields, d_pairs, a, b);
 }
