@@ -660,7 +660,7 @@ constexpr int kSadMaxWin = kSadMaxBlock + 2 * (kSadMaxRange + 1);
 constexpr int kSadMaxSmem =
     (kSadMaxBlock * kSadMaxBlock + kSadMaxWin * kSadMaxWin + (kSadMaxWin + 1) * (kSadMaxWin + 1)) *
     (int)sizeof(int);
-constexpr int kSadThreads = 192;
+constexpr int kSadThreads = 224;
 
 int sad_max_block() { return kSadMaxBlock; }
 int sad_max_range() { return kSadMaxRange; }
@@ -744,48 +744,62 @@ __device__ __forceinline__ unsigned long long warp_tile_cost(const int* As, cons
 // The exhaustive scan. For integers |a - b| = 2 max(a, b) - a - b, so a
 // candidate's SAD is 2 sum max(A, B) - sum A - sum B over its window, the
 // last from the window's integral image: one max and one add per candidate
-// pixel, all in exact integers. Each thread owns one dy and G consecutive
-// dx; blocks of BW = 16 columns keep a register window of the G + 15 row
-// values they read (one new load per pixel). Returns the thread's best key
-// (biased cost << 11 | centre-out visit index); the thread holding (0, 0)
-// stores its SAD in *sad0.
+// pixel, all in exact integers. Each item is one dy and G consecutive dx;
+// its rows are split between two adjacent lanes (their sums meet by one
+// shuffle), which halves the dependent chain of a candidate's additions.
+// Blocks of BW = 16 columns keep a register window of the G + 15 row values
+// they read (one new load per pixel). Returns the thread's best key (biased
+// cost << 11 | centre-out visit index); the lane holding (0, 0) stores its
+// SAD in *sad0.
 template <int G, int BW>
 __device__ __forceinline__ unsigned long long sad_scan(const int* As, const int* Bs,
                                                        const int* I, int b, int ww, int S, int bh,
                                                        int bw, int s, unsigned sum_a,
-                                                       unsigned long long* sad0) {
+                                                       unsigned long long* sad0, unsigned one) {
   const int n = 2 * s + 1;
   const int ngroups = (n + G - 1) / G;
+  const int items = n * ngroups;
   const int wi = ww + 1;
+  const int hsplit = (bh + 1) / 2;
   unsigned long long bestkey = ~0ull;
-  for (int it = threadIdx.x; it < n * ngroups; it += blockDim.x) {
-    const int dy = it / ngroups - s;
-    const int dxg = -s + (it % ngroups) * G;
+  for (int base = 0; base < 2 * items; base += blockDim.x) {
+    const int it = base + threadIdx.x;
+    const bool valid = it < 2 * items;
+    const int item = it >> 1, half = it & 1;
+    const int dy = item / ngroups - s;
+    const int dxg = -s + (item % ngroups) * G;
     unsigned acc[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) acc[g] = 0u;
-    for (int yy = 0; yy < bh; ++yy) {
-      const int* ar = As + yy * b;
-      // window value under pixel xx at offset dxg + g: br[xx - g]
-      const int* br = Bs + (yy - dy + S) * ww + (S - dxg);
-      if (BW == 16) {
-        int win[16 + G - 1];  // win[j] = br[j - (G - 1)]
+    if (valid) {
+      const int yb = half ? hsplit : 0, ye = half ? bh : hsplit;
+      for (int yy = yb; yy < ye; ++yy) {
+        const int* ar = As + yy * b;
+        // window value under pixel xx at offset dxg + g: br[xx - g]
+        const int* br = Bs + (yy - dy + S) * ww + (S - dxg);
+        if (BW == 16) {
+          int win[16 + G - 1];  // win[j] = br[j - (G - 1)]
 #pragma unroll
-        for (int j = 0; j < 16 + G - 1; ++j) win[j] = br[j - (G - 1)];
+          for (int j = 0; j < 16 + G - 1; ++j) win[j] = br[j - (G - 1)];
 #pragma unroll
-        for (int xx = 0; xx < 16; ++xx) {
-          const int av = ar[xx];
+          for (int xx = 0; xx < 16; ++xx) {
+            const int av = ar[xx];
 #pragma unroll
-          for (int g = 0; g < G; ++g) acc[g] += (unsigned)max(av, win[xx - g + G - 1]);
-        }
-      } else {
-        for (int xx = 0; xx < bw; ++xx) {
-          const int av = ar[xx];
+            for (int g = 0; g < G; ++g)
+              acc[g] = (unsigned)max(av, win[xx - g + G - 1]) * one + acc[g];
+          }
+        } else {
+          for (int xx = 0; xx < bw; ++xx) {
+            const int av = ar[xx];
 #pragma unroll
-          for (int g = 0; g < G; ++g) acc[g] += (unsigned)max(av, br[xx - g]);
+            for (int g = 0; g < G; ++g) acc[g] = (unsigned)max(av, br[xx - g]) * one + acc[g];
+          }
         }
       }
     }
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] += __shfl_xor_sync(0xffffffffu, acc[g], 1);
+    if (!valid || half) continue;
     const int r0 = S - dy;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
@@ -808,7 +822,7 @@ __device__ __forceinline__ unsigned long long sad_scan(const int* As, const int*
 }
 
 // One CTA per (tile, pair).
-__global__ void __launch_bounds__(kSadThreads) k_sad_search(const MeField* __restrict__ mf,
+__global__ void __launch_bounds__(kSadThreads, 6) k_sad_search(const MeField* __restrict__ mf,
                                                             const MePair* __restrict__ pairs,
                                                             const int* __restrict__ qblur,
                                                             SadArgs a, SadBuffers out) {
@@ -871,15 +885,19 @@ __global__ void __launch_bounds__(kSadThreads) k_sad_search(const MeField* __res
   __syncthreads();
   const int n = 2 * s + 1;
   const unsigned sum_a = sh_suma;
+  // 1, in a form the compiler cannot fold: the accumulations are issued as
+  // multiply-adds, which run on the FMA pipe beside the max on the integer
+  // pipe (a plain add would share the integer pipe with the max)
+  const unsigned one = ((unsigned)a.block >> 30) | 1u;
   // G consecutive dx per thread: 11 when it divides the row of candidates
   // (no wasted candidates at +-16), else 8
   unsigned long long bestkey;
   if (n % 11 == 0)
-    bestkey = bw == 16 ? sad_scan<11, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0)
-                       : sad_scan<11, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0);
+    bestkey = bw == 16 ? sad_scan<11, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one)
+                       : sad_scan<11, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one);
   else
-    bestkey = bw == 16 ? sad_scan<8, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0)
-                       : sad_scan<8, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0);
+    bestkey = bw == 16 ? sad_scan<8, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one)
+                       : sad_scan<8, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one);
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long v = __shfl_xor_sync(0xffffffffu, bestkey, o);
     if (v < bestkey) bestkey = v;
