@@ -762,7 +762,7 @@ def main():
     achieved = alg_bytes_per_launch / solver_s / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": profile_traffic(args.workload),
-            "traffic_source": "committed ncu capture of this workload's solver launch "
+            "traffic_source": "committed one-pass ncu capture of this solver build on this workload "
                               "(profiles/solver_traffic.json), not measured in this run",
             "peak_kind": peak_kind,
             "kernel": "k_solver (persistent IRLS + CG)",

@@ -38,3 +38,29 @@ def decode_fields_2d_parallel(jobs):
     """decode_field_2d over `jobs` in a spawn pool; results in job order."""
     with pool(len(jobs)) as ex:
         return list(ex.map(decode_field_2d, jobs))
+
+
+def adjoint_field(job):
+    """One field through the FP64 adjoint oracle (hvd_adjoint: the decode's
+    forward with its IRLS checkpoints, the implicit-function adjoint of the
+    refine, then the init's adjoint). `job` = (uint16 samples, standard,
+    parity, config kwargs, luma cotangent, chroma cotangent). Returns
+    (d loss / d S on the active picture, {scalar name: gradient})."""
+    samples, standard, parity, cfg_kw, yb, cb = job
+    from hvdg import _cabi, api, synth
+    from oracle import hvd_adjoint as A
+    from oracle import hvd_oracle as O
+    g = _cabi.default_geometry(standard)
+    cfg = api.default_config(**cfg_kw)
+    obs = O.prepare_field(synth.to_ire(samples), g, cfg, parity)
+    _, _, chi0 = A.init_parts(obs.s, obs.carrier, g)
+    aniso = O.resolve_chroma_aniso(chi0, cfg, O.uses_vswitch(g))
+    chis = A.refine_forward_budget(obs.s, obs.carrier, chi0, cfg, aniso)
+    s_bar, chi0_bar, gl = A.refine_adjoint(obs.s, obs.carrier, chis, cfg, aniso, yb, cb, 1e-8, 3000)
+    return s_bar + A.init_adjoint(obs.s, obs.carrier, g, chi0_bar), gl
+
+
+def adjoint_fields_parallel(jobs):
+    """adjoint_field over `jobs` in a spawn pool; results in job order."""
+    with pool(len(jobs)) as ex:
+        return list(ex.map(adjoint_field, jobs))

@@ -107,3 +107,35 @@ def test_torch_autograd_binding(ctx):
     assert np.allclose(samples.grad.numpy(), np.stack(sbar), rtol=1e-5, atol=1e-12)
     assert abs(lc.grad.item() - sc["lambda_c"]) <= 1e-6 * abs(sc["lambda_c"]) + 1e-12
     assert abs(k.grad.item() - sc["structure_coupling"]) <= 1e-6 * abs(sc["structure_coupling"]) + 1e-12
+
+
+def test_adjoint_config4_batch_vs_fp64_oracle(ctx):
+    """Config 4 as configured: 8 NTSC fields in one batched adjoint call at
+    10 IRLS x 50 CG. Each field's sample gradient against the FP64 adjoint
+    oracle (1e-3 relative), and the batch's scalar gradients against the sum
+    of the oracle's per-field ones (1e-3 relative). The oracle runs field-
+    parallel in a spawn pool."""
+    from oracle import jobs
+    g = _cabi.default_geometry(_cabi.STD_NTSC)
+    fs = [synth.make_field(200 + i, _cabi.STD_NTSC, 0.5) for i in range(8)]
+    cfg = _cfg()
+    flds = [api.Field(f.samples, g, parity=i % 2) for i, f in enumerate(fs)]
+    decs = ctx.decode_fields(flds, cfg)
+    cots = [_loss_and_cot(d, f)[1:] for d, f in zip(decs, fs)]
+    sbar, sc, _ = ctx.decode_fields_adjoint(flds, cfg, [c[0] for c in cots], [c[1] for c in cots],
+                                            300)
+    kw = dict(irls_outer=10, cg_iterations=500, fast=0, cg_tol=1e-6, temporal_strength=-1.0)
+    orc = jobs.adjoint_fields_parallel([(f.samples, _cabi.STD_NTSC, i % 2, kw, c[0], c[1])
+                                        for i, (f, c) in enumerate(zip(fs, cots))])
+    fal, lal = g.first_active_field_line, g.last_active_line
+    a0, a1 = g.active_video_start, g.active_video_end
+    for i, (s_bar, _) in enumerate(orc):
+        got = sbar[i][fal:lal, a0:a1].astype(np.float64)
+        rel = np.linalg.norm(got - s_bar / CPI) / np.linalg.norm(s_bar / CPI)
+        print(f"field {i}: sample gradient rel L2 {rel:.2e}")
+        assert rel < 1e-3
+    for k_gpu, k_orc in (("lambda_c", "lambda_c"), ("charbonnier_eps", "eps"),
+                         ("chroma_eps", "eps_c"), ("structure_coupling", "k")):
+        want = sum(gl[k_orc] for _, gl in orc)
+        print(k_gpu, sc[k_gpu], want)
+        assert abs(sc[k_gpu] - want) <= 1e-3 * abs(want) + 1e-9
