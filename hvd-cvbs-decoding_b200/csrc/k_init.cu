@@ -312,8 +312,12 @@ __device__ __forceinline__ void fft_reg_inv(float2 (&v)[32], float2* buf,
 }
 
 // In-place cyclic convolution of one column in shared memory:
-// buf[0, M) <- IFFT_M(FFT_M(buf) * kh), kh the kernel spectrum (1/M folded
-// in).
+// buf[0, M / 2) <- IFFT_M(FFT_M(buf) * kh)[0, M / 2), kh the kernel
+// spectrum (1/M folded in). The column's samples fill at most its first
+// M / 2 entries (M >= 2 hp - 1), so the upper half is zero by construction:
+// it is neither read nor written, and the zeros, known at compile time,
+// prune the first radix-2 stage of the forward transform (and the unused
+// half of the inverse's last stage).
 template <int M, typename Sync>
 __device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restrict__ kh,
                                              const float2* __restrict__ tw1024,
@@ -322,7 +326,9 @@ __device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restri
   constexpr int S = M / 1024;
   float2 v[32];
 #pragma unroll
-  for (int k = 0; k < 32; ++k) v[k] = buf[(lane + 32 * k) * S + sub];
+  for (int k = 0; k < 16; ++k) v[k] = buf[(lane + 32 * k) * S + sub];
+#pragma unroll
+  for (int k = 16; k < 32; ++k) v[k] = make_float2(0.f, 0.f);
   sync();
   fft_reg_fwd<M>(v, buf, tw1024, tw2048, sub, lane, sync);
 #pragma unroll
@@ -333,7 +339,7 @@ __device__ __forceinline__ void col_conv_reg(float2* buf, const float2* __restri
   fft_reg_inv<M>(v, buf, tw1024, tw2048, sub, lane, sync);
   sync();
 #pragma unroll
-  for (int k = 0; k < 32; ++k) buf[(lane + 32 * k) * S + sub] = v[k];
+  for (int k = 0; k < 16; ++k) buf[(lane + 32 * k) * S + sub] = v[k];
   sync();
 }
 
@@ -345,12 +351,23 @@ __device__ __forceinline__ void init_cols_body(const InitArgs& a, const FieldDes
   float2* buf = sm_cols + col * (M + kColPad);
   for (int v = 0; v < 2; ++v) {
     const float2* src = a.rowbuf + a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch;
-    // cooperative coalesced load: thread -> (row, column-in-group)
-    for (int i = threadIdx.x; i < M * G; i += blockDim.x) {
+    // cooperative coalesced load of rows [0, hp), zeros to M / 2 (the input
+    // half of col_conv_reg): thread -> (row, column-in-group), all of a
+    // thread's loads issued before its shared-memory stores
+    constexpr int kPer = (M / 2) * G / kColThreads;
+    static_assert((M / 2) * G % kColThreads == 0, "fill split");
+    float2 val[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = threadIdx.x + j * kColThreads;
       const int row = i / G, c = i % G;
-      float2 val = make_float2(0.f, 0.f);
-      if (row < gd.hp && x0 + c < f.w) val = src[(int64_t)row * f.pitch + x0 + c];
-      sm_cols[c * (M + kColPad) + row] = val;
+      val[j] = make_float2(0.f, 0.f);
+      if (row < gd.hp && x0 + c < f.w) val[j] = src[(int64_t)row * f.pitch + x0 + c];
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = threadIdx.x + j * kColThreads;
+      sm_cols[(i % G) * (M + kColPad) + i / G] = val[j];
     }
     __syncthreads();
     col_conv_reg<M>(buf, a.khat + gd.khat_col_off + v * M, a.tw_col, a.tw_row, sub, lane, sync);
@@ -400,7 +417,9 @@ __global__ void __launch_bounds__(kColThreads, 3) k_init_cols(InitArgs a) {
 // already demodulated, straight from S. The spectrum is parked in shared
 // memory, each thread re-reading only the values it wrote, and filtered by
 // both variants' kernel spectra in turn; each result goes out through the
-// slot as one coalesced row of the pitch.
+// slot as one coalesced row of the pitch. A row's samples fill at most the
+// first half of the 2048 points (2 w - 1 <= 2048), so the upper half is a
+// compile-time zero on the way in and is not stored on the way out.
 constexpr int kRowThreads = 128;
 constexpr int kRowsPerCta = kRowThreads / 64;
 constexpr int kRowSmem = kRowsPerCta * 2 * kRowFft * (int)sizeof(float2);
@@ -424,7 +443,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
   auto store_row = [&](float2* out) {
     sync();
 #pragma unroll
-    for (int k = 0; k < 32; ++k) buf[2 * (lane + 32 * k) + sub] = v[k];
+    for (int k = 0; k < 16; ++k) buf[2 * (lane + 32 * k) + sub] = v[k];
     sync();
     for (int i = tp; i < f.pitch; i += 64) out[i] = i < f.w ? buf[i] : make_float2(0.f, 0.f);
     sync();
@@ -435,10 +454,12 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
       const int64_t row = a.rowbuf_off[f_idx] + ((int64_t)var * gd.hp + yp) * f.pitch;
       const float2* in = a.adj_in + row;
 #pragma unroll
-      for (int k = 0; k < 32; ++k) {
+      for (int k = 0; k < 16; ++k) {
         const int x = 2 * (lane + 32 * k) + sub;
         v[k] = x < f.w ? in[x] : make_float2(0.f, 0.f);
       }
+#pragma unroll
+      for (int k = 16; k < 32; ++k) v[k] = make_float2(0.f, 0.f);
       fft_reg_fwd<kRowFft>(v, buf, a.tw_col, a.tw_row, sub, lane, sync);
       const float2* kh = a.khat + gd.khat_row_off + var * kRowFft + sub * 1024 + lane;
 #pragma unroll
@@ -456,7 +477,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
   const float2* P = a.col_phasor + f.col_off;
   const float4 L = __ldg(a.line_phasor + f.line_off + sy);
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
+  for (int k = 0; k < 16; ++k) {
     if ((k & 7) == 0) load_fence();
     const int x = 2 * (lane + 32 * k) + sub;
     float2 val = make_float2(0.f, 0.f);
@@ -467,6 +488,8 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
     }
     v[k] = val;
   }
+#pragma unroll
+  for (int k = 16; k < 32; ++k) v[k] = make_float2(0.f, 0.f);
   fft_reg_fwd<kRowFft>(v, buf, a.tw_col, a.tw_row, sub, lane, sync);
   float2* my_spec = spec + sub * 1024 + lane;
 #pragma unroll
@@ -566,7 +589,7 @@ __device__ __forceinline__ void sym_cols_body(const InitArgs& a, const FieldDesc
   extern __shared__ float2 sm_cols[];
   const float2* chirp = a.khat + gd.sym_col_chirp;
   float2* plane = a.rowbuf + a.rowbuf_off[f_idx] + (mode ? (int64_t)gd.hp * f.pitch : 0);
-  for (int i = threadIdx.x; i < M * G; i += blockDim.x) {
+  for (int i = threadIdx.x; i < (M / 2) * G; i += blockDim.x) {
     const int row = i / G, c = i % G;
     float2 v = make_float2(0.f, 0.f);
     if (row < gd.hp && x0 + c < f.w) {
@@ -749,16 +772,40 @@ __global__ void __launch_bounds__(1024) k_aniso(FieldDesc* fields, const float2*
     if (n > kAnisoMax) n = kAnisoMax;     // geometry guard (the host rejects larger)
     const float2* c = chi0 + f.px_off;
     const float inv = 1.0f / (float)group;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int ti = i / nx, xi = i % nx;
-      const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
-      float2 p = make_float2(0.f, 0.f), q = p;
-      for (int k = 0; k < group; ++k) {
-        p = cadd(p, c[(int64_t)(group * tt + k) * f.pitch + x]);
-        q = cadd(q, axis == 0 ? c[(int64_t)(group * tt + k) * f.pitch + x - 1]
-                              : c[(int64_t)(group * (tt - 1) + k) * f.pitch + x]);
+    // kAnisoBatch samples per thread and pass, all their loads issued before
+    // the first sum (one L2 round trip per batch, not per sample)
+    constexpr int kAnisoBatch = 4;
+    for (int i0 = threadIdx.x; i0 < n; i0 += kAnisoBatch * blockDim.x) {
+      float2 pv[kAnisoBatch][4], qv[kAnisoBatch][4];
+#pragma unroll
+      for (int b = 0; b < kAnisoBatch; ++b) {
+        const int i = i0 + b * blockDim.x;
+        const int ti = i / nx, xi = i % nx;
+        const int tt = 1 + 2 * ti, x = 1 + 3 * xi;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          pv[b][k] = qv[b][k] = make_float2(0.f, 0.f);
+          if (i < n && k < group) {
+            pv[b][k] = c[(int64_t)(group * tt + k) * f.pitch + x];
+            qv[b][k] = axis == 0 ? c[(int64_t)(group * tt + k) * f.pitch + x - 1]
+                                 : c[(int64_t)(group * (tt - 1) + k) * f.pitch + x];
+          }
+        }
       }
-      sm_an[i] = sqrtf(cnorm(csub(cscale(p, inv), cscale(q, inv))));
+#pragma unroll
+      for (int b = 0; b < kAnisoBatch; ++b) {
+        const int i = i0 + b * blockDim.x;
+        float2 p = make_float2(0.f, 0.f), q = p;
+        // the same order of additions as one sample at a time: k = 0, 1, ...
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (k < group) {
+            p = cadd(p, pv[b][k]);
+            q = cadd(q, qv[b][k]);
+          }
+        }
+        if (i < n) sm_an[i] = sqrtf(cnorm(csub(cscale(p, inv), cscale(q, inv))));
+      }
     }
     __syncthreads();
     const float p98 = n > 0 ? block_select_kth(sm_an, n, n - 1 - n / 50, hist, bc) : 0.f;

@@ -317,14 +317,17 @@ __global__ void __launch_bounds__(256) k_burst_lockin(const PrepDesc* __restrict
   (void)theta;
 }
 
-// BurstAmplitudeIre (lockin.cpp:256-323). One CTA per field.
-__global__ void __launch_bounds__(256) k_burst_amplitude(const PrepDesc* __restrict__ descs,
-                                                         float* __restrict__ amp_out) {
+// BurstAmplitudeIre (lockin.cpp:256-323). One CTA of kAmpThreads per
+// field: a warp per line for the per-line envelope medians (a few fields per
+// call, so the lines are spread over 32 warps), then the block selects.
+constexpr int kAmpThreads = 1024;
+__global__ void __launch_bounds__(kAmpThreads) k_burst_amplitude(const PrepDesc* __restrict__ descs,
+                                                                 float* __restrict__ amp_out) {
   const PrepDesc p = descs[blockIdx.x];
   const int h = p.fh;
   const int x0 = p.bx0, x1 = p.bx1;
   __shared__ double per_line[kMaxLines];
-  __shared__ double env[8][64];
+  __shared__ double env[kAmpThreads / 32][64];
   __shared__ double s_m;
   __shared__ double good[kMaxLines];
   __shared__ int s_ng;
@@ -361,14 +364,13 @@ __global__ void __launch_bounds__(256) k_burst_amplitude(const PrepDesc* __restr
     __syncwarp();
   }
   __syncthreads();
+  if (threadIdx.x == 0) s_ng = 0;
   block_rank_select(per_line, h, h / 2, &s_m);
-  if (threadIdx.x == 0) {
-    const double thr = 0.25 * s_m;
-    int ng = 0;
-    for (int y = 0; y < h; ++y)
-      if (per_line[y] > thr) good[ng++] = per_line[y];
-    s_ng = ng;
-  }
+  // the lines above a quarter of the median, compacted in any order (the
+  // rank select below does not depend on it)
+  const double thr = 0.25 * s_m;
+  for (int y = threadIdx.x; y < h; y += blockDim.x)
+    if (per_line[y] > thr) good[atomicAdd(&s_ng, 1)] = per_line[y];
   __syncthreads();
   if (s_ng == 0) {
     if (threadIdx.x == 0) amp_out[blockIdx.x] = p.nominal_burst;
@@ -420,7 +422,7 @@ void launch_burst_lockin(const PrepDesc* d_descs, int n, LockinOut out, cudaStre
   if (n > 0) k_burst_lockin<<<n, 256, kLockinSmem, st>>>(d_descs, out);
 }
 void launch_burst_amplitude(const PrepDesc* d_descs, int n, float* d_amp, cudaStream_t st) {
-  if (n > 0) k_burst_amplitude<<<n, 256, 0, st>>>(d_descs, d_amp);
+  if (n > 0) k_burst_amplitude<<<n, kAmpThreads, 0, st>>>(d_descs, d_amp);
 }
 void launch_crop(const PrepDesc* d_descs, const int4* d_rows, int total_rows, float* d_S,
                  const int64_t* d_px_off, const int* d_pitch, int* d_nonfinite, cudaStream_t st) {
