@@ -22,10 +22,12 @@
 //  * Work is split into units (64-column strip x band of rows, one warp).
 //    Units of all fields and all phases form one ordered queue; a warp takes
 //    the next item, waits (bounded) until its field completed the previous
-//    phase, and the last unit to finish a phase reduces the field's partials
-//    in a fixed order and publishes the field's scalars. Fields therefore
-//    progress independently with no grid-wide barrier, and the reduction is
-//    deterministic.
+//    phase. Units arrive in groups of 32 consecutive units: the last unit
+//    of a group sums the group's partials, and the last group of the field
+//    sums the group sums and publishes the field's scalars, both in a fixed
+//    order. Fields therefore progress independently with no grid-wide
+//    barrier, the reduction is deterministic, and the end of a phase waits
+//    on two short reductions instead of one over every unit.
 //  * Planes read with a halo are double-buffered (chi, g, d, q) so a unit
 //    never reads a neighbour's freshly written rows.
 //  * Each lane owns two adjacent pixels (128-bit loads of complex pairs);
@@ -917,27 +919,26 @@ __device__ __noinline__ void complete_phase(const SolverArgs& A, const FieldDesc
 #pragma unroll
   for (int i = 0; i < kNPart; ++i) s[i] = 0.0;
   if (kind == kPhaseG || kind == kPhaseI) {
-    // lane l adds units l, l + 32, l + 64, ... in that order; four units'
-    // partials are loaded ahead of their additions, so the chain waits on
-    // one L2 round trip per four units instead of per unit (same order,
-    // same sums)
-    const int ue = f.unit_begin + f.unit_count;
-    int uu = f.unit_begin + lane;
-    for (; uu + 96 < ue; uu += 128) {
-      double v[4][kNPart];
+    // the field's group sums: lane l adds groups l, l + 32, ... in that
+    // order (a field has at most a few dozen groups: all loads of a lane
+    // are in flight together), then a fixed butterfly across the lanes
+    const int ng = (f.unit_count + kGroupUnits - 1) >> kGroupShift;
+    double v[4][kNPart];
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < kNPart; ++i)
-          v[j][i] = __ldcg(A.partials + (int64_t)(uu + 32 * j) * kNPart + i);
+      for (int i = 0; i < kNPart; ++i)
+        v[j][i] = lane + 32 * j < ng
+                      ? __ldcg(A.gpartials + (int64_t)(f.unit_begin + lane + 32 * j) * kNPart + i)
+                      : 0.0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < kNPart; ++i) s[i] += v[j][i];
-    }
-    for (; uu < ue; uu += 32) {
+      for (int i = 0; i < kNPart; ++i) s[i] += v[j][i];
+    for (int gg = lane + 128; gg < ng; gg += 32) {
 #pragma unroll
-      for (int i = 0; i < kNPart; ++i) s[i] += __ldcg(A.partials + (int64_t)uu * kNPart + i);
+      for (int i = 0; i < kNPart; ++i)
+        s[i] += __ldcg(A.gpartials + (int64_t)(f.unit_begin + gg) * kNPart + i);
     }
 #pragma unroll
     for (int i = 0; i < kNPart; ++i) s[i] = warp_allsum(s[i]);
@@ -1085,9 +1086,36 @@ __global__ void __launch_bounds__(kSolverThreads, kDiag ? 1 : 2)
         if (lane == 0) __stcg(A.partials + (int64_t)ui * kNPart + i, v);
       }
     }
+    // two-level arrival: the last unit of a group of kGroupUnits consecutive
+    // units sums the group's partials (one load per lane, a fixed butterfly)
+    // into the group's slot and arrives at the field; the field's last group
+    // completes the phase. The end-of-phase reduction then reads a few dozen
+    // group sums instead of every unit's partials.
     __threadfence();
+    const int gj = (ui - f.unit_begin) >> kGroupShift;
+    const int gslot = f.unit_begin + gj;
+    const int gfirst = f.unit_begin + (gj << kGroupShift);
+    const int gsize = min(kGroupUnits, f.unit_count - (gj << kGroupShift));
     int last = 0;
-    if (lane == 0) last = atomicAdd(A.arrive + u.field, 1) == f.unit_count - 1;
+    if (lane == 0) last = atomicAdd(A.garrive + gslot, 1) == gsize - 1;
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) continue;
+    if (lane == 0) A.garrive[gslot] = 0;
+    __threadfence();
+    if (kind == kPhaseG || kind == kPhaseI) {
+      double gv[kNPart];
+#pragma unroll
+      for (int i = 0; i < kNPart; ++i)
+        gv[i] = lane < gsize ? __ldcg(A.partials + (int64_t)(gfirst + lane) * kNPart + i) : 0.0;
+#pragma unroll
+      for (int i = 0; i < kNPart; ++i) {
+        const double v = warp_sum(gv[i]);
+        if (lane == 0) __stcg(A.gpartials + (int64_t)gslot * kNPart + i, v);
+      }
+      __threadfence();
+    }
+    const int ng = (f.unit_count + kGroupUnits - 1) >> kGroupShift;
+    if (lane == 0) last = atomicAdd(A.arrive + u.field, 1) == ng - 1;
     last = __shfl_sync(0xffffffffu, last, 0);
     if (last) {
       if (lane == 0) A.arrive[u.field] = 0;

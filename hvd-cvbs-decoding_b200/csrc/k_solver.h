@@ -9,6 +9,10 @@
 namespace hvdg {
 
 constexpr int kSolverThreads = 256;
+// Units of a field arrive in groups of kGroupUnits consecutive units: the
+// last unit of a group sums the group's partials, the last group the field's.
+constexpr int kGroupShift = 5;
+constexpr int kGroupUnits = 1 << kGroupShift;
 enum PhaseKind { kPhaseR = 0, kPhaseG = 1, kPhaseI = 2, kPhaseF = 3 };
 
 struct SolverArgs {
@@ -20,8 +24,10 @@ struct SolverArgs {
   int n_phases;                 // max phases over fields
   unsigned long long* queue;    // work counter (zeroed before launch)
   int* done_phase;              // per field, -1 before launch
-  int* arrive;                  // per field, 0 before launch
+  int* arrive;                  // per field, 0 before launch (arrived unit groups)
   double* partials;             // per unit x 5
+  int* garrive;                 // per unit group (slot unit_begin + group), 0 before launch
+  double* gpartials;            // per unit group x 5 (same slots)
   int* err;                     // set on a bounded-wait timeout
   long long phase_wait_limit;   // polls of a field's phase flag before giving up (err)
   const float* S;

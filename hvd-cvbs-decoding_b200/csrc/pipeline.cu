@@ -457,6 +457,8 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
   L.o_ctl = take(sizeof(FieldCtl) * m);
   L.o_units = take(sizeof(Unit) * b.units.size());
   L.o_partials = take(sizeof(double) * 5 * b.units.size());
+  L.o_gpart = take(sizeof(double) * 5 * b.units.size());
+  L.o_garrive = take(sizeof(int) * b.units.size());
   L.o_done = take(sizeof(int) * m);
   L.o_arrive = take(sizeof(int) * m);
   L.o_flags = take(sizeof(int) * 4);
@@ -523,6 +525,7 @@ void stage_reset(hvdg_ctx* ctx, const Staged& S) {
   mark(ctx, 0);
   cudaMemsetAsync(at<char>(ctx, L.o_ctl), 0, sizeof(FieldCtl) * n, s);
   cudaMemsetAsync(at<char>(ctx, L.o_arrive), 0, sizeof(int) * n, s);
+  cudaMemsetAsync(at<char>(ctx, L.o_garrive), 0, sizeof(int) * L.total_units, s);
   cudaMemsetAsync(at<char>(ctx, L.o_done), 0xff, sizeof(int) * n, s);
   cudaMemsetAsync(at<char>(ctx, L.o_flags), 0, sizeof(int) * 4, s);
   cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
@@ -747,6 +750,8 @@ hvdg::SolverArgs solver_args(hvdg_ctx* ctx, const Staged& S) {
   sa.done_phase = at<int>(ctx, L.o_done);
   sa.arrive = at<int>(ctx, L.o_arrive);
   sa.partials = at<double>(ctx, L.o_partials);
+  sa.garrive = at<int>(ctx, L.o_garrive);
+  sa.gpartials = at<double>(ctx, L.o_gpart);
   sa.err = at<int>(ctx, L.o_flags);
   sa.phase_wait_limit = ctx->phase_wait_limit;
   sa.S = at<float>(ctx, L.o_S);

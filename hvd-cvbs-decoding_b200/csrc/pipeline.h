@@ -184,6 +184,7 @@ struct Layout {
       o_flags, o_queue, o_lineph, o_theta, o_theta64, o_vsw, o_colph, o_khat, o_twr, o_twc,
       o_S, o_Y, o_X0, o_X1, o_G0, o_G1, o_D0, o_D1, o_Q0, o_Q1, o_W, o_rowbuf, o_itab, o_amp;
   size_t o_W2 = 0;   // (wd1, wd2) plane, only when a field has the oriented prior
+  size_t o_gpart = 0, o_garrive = 0;  // solver unit-group partials and arrival counters
   bool has_diag = false;
   size_t total;
   int64_t total_px, total_rowbuf;

@@ -620,6 +620,7 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
       // solver state reset for this colour, aniso at the current chi
       cudaMemsetAsync(at<char>(ctx, L.o_ctl), 0, sizeof(FieldCtl) * nf, s);
       cudaMemsetAsync(at<char>(ctx, L.o_arrive), 0, sizeof(int) * nf, s);
+      cudaMemsetAsync(at<char>(ctx, L.o_garrive), 0, sizeof(int) * L.total_units, s);
       cudaMemsetAsync(at<char>(ctx, L.o_done), 0xff, sizeof(int) * nf, s);
       cudaMemsetAsync(at<char>(ctx, L.o_queue), 0, sizeof(unsigned long long), s);
       if (pass == 0 && cfg.psi_init && has_temporal) {
