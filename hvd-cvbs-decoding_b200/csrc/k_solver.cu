@@ -1096,11 +1096,15 @@ __global__ void __launch_bounds__(kSolverThreads, kDiag ? 1 : 2)
     const int gslot = f.unit_begin + gj;
     const int gfirst = f.unit_begin + (gj << kGroupShift);
     const int gsize = min(kGroupUnits, f.unit_count - (gj << kGroupShift));
+    // the counters only grow (zeroed before the launch): every unit of a
+    // field arrives in a phase or none does (a phase skipped by an early
+    // exit is skipped by all), so the group's last arrival of a phase is the
+    // one that makes its count a multiple of the group size -- no reset
+    // store for the fence below to wait on
     int last = 0;
-    if (lane == 0) last = atomicAdd(A.garrive + gslot, 1) == gsize - 1;
+    if (lane == 0) last = (atomicAdd(A.garrive + gslot, 1) + 1) % gsize == 0;
     last = __shfl_sync(0xffffffffu, last, 0);
     if (!last) continue;
-    if (lane == 0) A.garrive[gslot] = 0;
     __threadfence();
     if (kind == kPhaseG || kind == kPhaseI) {
       double gv[kNPart];
@@ -1115,10 +1119,9 @@ __global__ void __launch_bounds__(kSolverThreads, kDiag ? 1 : 2)
       __threadfence();
     }
     const int ng = (f.unit_count + kGroupUnits - 1) >> kGroupShift;
-    if (lane == 0) last = atomicAdd(A.arrive + u.field, 1) == ng - 1;
+    if (lane == 0) last = (atomicAdd(A.arrive + u.field, 1) + 1) % ng == 0;
     last = __shfl_sync(0xffffffffu, last, 0);
     if (last) {
-      if (lane == 0) A.arrive[u.field] = 0;
       __threadfence();
       complete_phase(A, fg, u.field, kind, k, p, lane);
     }
