@@ -627,14 +627,21 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
     write_debug_maps(ctx->debug_dir, base_frame_id, core_begin, core_end, f1_bottom, *dg, acc_gain,
                      Yd, car, parity, h, w);
   }
-  parallel_for(core_end - core_begin, [&](int ti) {
+  // each core frame in kWeaveBands bands of frame lines, the bands on the
+  // host threads: the caller's output pages are first touched (and the
+  // planes filled) by many threads at once
+  constexpr int kWeaveBands = 8;
+  parallel_for((core_end - core_begin) * kWeaveBands, [&](int task) {
+    const int ti = task / kWeaveBands, band = task % kWeaveBands;
     const int t = core_begin + ti;
     hvdg_yc_frame& yc = out[ti];
-    const size_t sz = (size_t)fw * fh;
-    std::fill(yc.chroma, yc.chroma + sz, (int16_t)0);
-    std::fill(yc.u_plane, yc.u_plane + sz, 0.0);
-    std::fill(yc.v_plane, yc.v_plane + sz, 0.0);
-    for (int line = 0; line < fh; ++line) {
+    const int l0 = (int)((int64_t)fh * band / kWeaveBands);
+    const int l1 = (int)((int64_t)fh * (band + 1) / kWeaveBands);
+    const size_t b0 = (size_t)l0 * fw, b1 = (size_t)l1 * fw;
+    std::fill(yc.chroma + b0, yc.chroma + b1, (int16_t)0);
+    std::fill(yc.u_plane + b0, yc.u_plane + b1, 0.0);
+    std::fill(yc.v_plane + b0, yc.v_plane + b1, 0.0);
+    for (int line = l0; line < l1; ++line) {
       const int64_t src = frame_line_offset(P, line);
       std::copy(frames[t] + src, frames[t] + src + fw, yc.luma + (size_t)line * fw);
     }
@@ -650,7 +657,7 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
       const int j = use_first ? j0 : j1;
       const int fl = r / 2;
       const int flat_line = row_even ? (fal + fl) : (f1 + fal + fl);
-      if (flat_line < 0 || flat_line >= fh) continue;
+      if (flat_line < l0 || flat_line >= l1) continue;
       const double thv = (double)th[j][fal + fl];
       const float2 Lc = make_float2((float)std::cos(thv), (float)std::sin(thv));
       const bool sw = vsw && vs[j][fal + fl] < 0;

@@ -219,6 +219,131 @@ __global__ void k_nbr_assemble(const FieldDesc* __restrict__ fields,
       make_float4(sw - S[fj.px_off + o], dc.x, dc.y, cf);
 }
 
+// ---- adaptive temporal strength (sequence.cpp:526-646) ----------------------
+// Same-parity pair (j, j + stride): at y = 2, 5, 8, ... < h - 2 and x = 4, 8,
+// ... with x + 7 < w, the 4-sample means of the two fields; where they agree
+// within nr_eps, the triangle-7 demodulation of each field by its carrier and
+// e = |d_j - d_k|^2 / 4. The float operations are the reference's, one by
+// one and in its order (this translation unit is compiled without FMA
+// contraction), so every skip decision and every e is the reference
+// restatement's. E holds e (or -1 where skipped) per pair, row, column.
+__global__ void k_amb_terms(const FieldDesc* __restrict__ fields, int stride, int nyi, int nx,
+                            const float* __restrict__ S, const float4* __restrict__ lineph,
+                            const float2* __restrict__ colph, float nr_eps,
+                            double* __restrict__ E) {
+  const int xi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int yi = blockIdx.y, j = blockIdx.z;
+  if (xi >= nx) return;
+  const FieldDesc fj = fields[j], fk = fields[j + stride];
+  const int y = 2 + 3 * yi, x = 4 + 4 * xi;
+  const float* Sj = S + fj.px_off + (int64_t)y * fj.pitch;
+  const float* Sk = S + fk.px_off + (int64_t)y * fk.pitch;
+  double e = -1.0;
+  float mj = 0.f, mk = 0.f;
+  for (int q = 0; q < 4; ++q) {
+    mj += Sj[x + q];
+    mk += Sk[x + q];
+  }
+  if (!(fabsf(mj - mk) * 0.25f > nr_eps)) {
+    const float kW[7] = {1.f, 2.f, 3.f, 4.f, 3.f, 2.f, 1.f};
+    auto demod = [&](const FieldDesc& f, const float* Sf) {
+      const float4 L = lineph[f.line_off + y];
+      float dr = 0.f, di = 0.f;
+      for (int q = 0; q < 7; ++q) {
+        const float sv = kW[q] * Sf[x + q];
+        const float2 c = carrier(make_float2(L.x, L.y), colph[f.col_off + x + q], L.z);
+        dr += sv * c.x;
+        di += -sv * c.y;
+      }
+      return make_float2(dr * (1.0f / 16.0f), di * (1.0f / 16.0f));
+    };
+    const float2 dj = demod(fj, Sj), dk = demod(fk, Sk);
+    const float er = dj.x - dk.x, ei = dj.y - dk.y;
+    e = 0.25 * (double)(er * er + ei * ei);
+  }
+  E[((int64_t)j * nyi + yi) * nx + xi] = e;
+}
+
+// One warp per pair: the band sums in row order (bands of 8 rows, one lane
+// each), the p95 of the band means over bands of >= 8 terms (or the mean of
+// all terms, summed in row order, when no band has 8), its square root.
+constexpr int kAmbMaxBands = 64;
+__global__ void __launch_bounds__(32) k_amb_pairs(int nyi, int nx, const double* __restrict__ E,
+                                                  float* __restrict__ amb, int* __restrict__ ok) {
+  const int j = blockIdx.x, lane = threadIdx.x;
+  const double* Ej = E + (int64_t)j * nyi * nx;
+  const int nbands = min((nyi + 7) / 8, kAmbMaxBands);
+  __shared__ double bacc[kAmbMaxBands];
+  __shared__ int bn[kAmbMaxBands];
+  for (int b = lane; b < nbands; b += 32) {
+    double a = 0.0;
+    int n = 0;
+    for (int yi = 8 * b; yi < min(8 * b + 8, nyi); ++yi) {
+      const double* r = Ej + (int64_t)yi * nx;
+      int xi = 0;
+      // 16 terms' loads in flight, then their additions in column order
+      for (; xi + 16 <= nx; xi += 16) {
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = r[xi + q];
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (v[q] >= 0.0) {
+            a += v[q];
+            ++n;
+          }
+      }
+      for (; xi < nx; ++xi)
+        if (r[xi] >= 0.0) {
+          a += r[xi];
+          ++n;
+        }
+    }
+    bacc[b] = a;
+    bn[b] = n;
+  }
+  __syncwarp();
+  if (lane != 0) return;
+  int ntot = 0;
+  for (int b = 0; b < nbands; ++b) ntot += bn[b];
+  float a = 0.f;
+  if (ntot > 0) {
+    float brms[kAmbMaxBands];
+    int nb = 0;
+    for (int b = 0; b < nbands; ++b)
+      if (bn[b] >= 8) brms[nb++] = (float)(bacc[b] / (double)bn[b]);
+    if (nb > 0) {
+      const int k95 = min(nb - 1, (int)(0.95 * (double)nb));
+      float v = brms[0];
+      for (int i = 0; i < nb; ++i) {
+        int less = 0, eq = 0;
+        for (int t = 0; t < nb; ++t) {
+          less += brms[t] < brms[i];
+          eq += brms[t] == brms[i];
+        }
+        if (less <= k95 && k95 < less + eq) v = brms[i];
+      }
+      a = sqrtf(v);
+    } else {
+      double acc = 0.0;
+      for (int64_t i = 0; i < (int64_t)nyi * nx; ++i)
+        if (Ej[i] >= 0.0) acc += Ej[i];
+      a = sqrtf((float)(acc / (double)ntot));
+    }
+  }
+  amb[j] = a;
+  ok[j] = ntot > 0;
+}
+
+void launch_amb_pairs(const FieldDesc* d_fields, int npairs, int stride, int nyi, int nx,
+                      const float* S, const float4* lineph, const float2* colph, float nr_eps,
+                      double* E, float* amb, int* ok, cudaStream_t st) {
+  if (npairs <= 0 || nyi <= 0 || nx <= 0) return;
+  k_amb_terms<<<dim3((nx + 127) / 128, nyi, npairs), 128, 0, st>>>(d_fields, stride, nyi, nx, S,
+                                                                   lineph, colph, nr_eps, E);
+  k_amb_pairs<<<npairs, 32, 0, st>>>(nyi, nx, E, amb, ok);
+}
+
 void launch_noise(const FieldDesc* d_fields, int nf, const float* S, float* scratch,
                   const int64_t* scratch_off, float* sigma, cudaStream_t st) {
   if (nf > 0) k_noise<<<nf, 1024, 0, st>>>(d_fields, S, scratch, scratch_off, sigma);

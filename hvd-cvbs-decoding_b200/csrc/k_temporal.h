@@ -23,6 +23,14 @@ struct EnvBuffers {
   float* floor2;                              // per listed field
 };
 
+// Adaptive-strength ambiguity (sequence.cpp:526-646) of the same-parity
+// pairs (j, j + stride), j < npairs: per pair the square root of the p95 band
+// mean of the demodulation differences (amb), and whether any term was kept
+// (ok). E: npairs x nyi x nx doubles of scratch; nyi rows y = 2, 5, ... < h - 2,
+// nx columns x = 4, 8, ... with x + 7 < w.
+void launch_amb_pairs(const FieldDesc* d_fields, int npairs, int stride, int nyi, int nx,
+                      const float* S, const float4* lineph, const float2* colph, float nr_eps,
+                      double* E, float* amb, int* ok, cudaStream_t st);
 void launch_noise(const FieldDesc* d_fields, int nf, const float* S, float* scratch,
                   const int64_t* scratch_off, float* sigma, cudaStream_t st);
 void launch_envelope(const FieldDesc* d_fields, const int* d_list, int n, int max_h, int max_w,

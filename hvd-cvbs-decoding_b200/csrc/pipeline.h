@@ -304,9 +304,8 @@ hvdg_status run_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg_
 hvdg_status validate_fields(const hvdg_field_in* fields, int n, const hvdg_config* cfg,
                             hvdg_field_out* out);
 float median_mean(std::vector<float> v);
-float adaptive_strength(const std::vector<std::vector<float>>& Sh,
-                        const std::vector<std::vector<float4>>& Lh, const std::vector<float2>& P,
-                        int h, int w, int stride, float nr_eps, float* amb_out);
+float strength_from_pairs(const std::vector<float>& pair_amb, const std::vector<int>& pair_ok,
+                          float nr_eps, float* amb_out);
 hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
                              const hvdg_config* cfg_in, hvdg_field_out* out, hvdg_diag* diag,
                              const RunOpts& opt);

@@ -19,78 +19,14 @@ float median_mean(std::vector<float> v) {
   return m;
 }
 
-// Adaptive temporal strength (sequence.cpp:526-646): same-parity pair
-// ambiguity from a triangle-7 demodulation of S by each field's carrier,
-// per horizontal band, p95 of bands, median over pairs, noise-floor removal.
-float adaptive_strength(const std::vector<std::vector<float>>& Sh,
-                        const std::vector<std::vector<float4>>& Lh, const std::vector<float2>& P,
-                        int h, int w, int stride, float nr_eps, float* amb_out) {
-  static const float kW[7] = {1.f, 2.f, 3.f, 4.f, 3.f, 2.f, 1.f};
-  const int nf = (int)Sh.size();
-  auto car = [&](int f, int y, int x) {
-    const float4 L = Lh[f][y];
-    const float2 c = make_float2(L.x * P[x].x - L.y * P[x].y, L.x * P[x].y + L.y * P[x].x);
-    return L.z < 0.f ? make_float2(-c.x, c.y) : c;
-  };
-  // one value per pair, the pairs on parallel host threads
-  const int npairs = std::max(0, nf - stride);
-  std::vector<float> pair_amb(npairs, 0.0f);
-  std::vector<char> pair_ok(npairs, 0);
-  parallel_for(npairs, [&](int j) {
-    const int k = j + stride;
-    std::vector<double> band_acc;
-    std::vector<long> band_n;
-    double acc = 0.0;
-    long n = 0;
-    int yi = 0;
-    for (int y = 2; y < h - 2; y += 3, ++yi) {
-      const int band = yi / 8;
-      if (band >= (int)band_acc.size()) {
-        band_acc.push_back(0.0);
-        band_n.push_back(0);
-      }
-      for (int x = 4; x + 7 < w; x += 4) {
-        float mj = 0.f, mk = 0.f;
-        for (int q = 0; q < 4; ++q) {
-          mj += Sh[j][(size_t)y * w + x + q];
-          mk += Sh[k][(size_t)y * w + x + q];
-        }
-        if (std::fabs(mj - mk) * 0.25f > nr_eps) continue;
-        auto demod = [&](int f) {
-          float dr = 0.f, di = 0.f;
-          for (int q = 0; q < 7; ++q) {
-            const float sv = kW[q] * Sh[f][(size_t)y * w + x + q];
-            const float2 c = car(f, y, x + q);
-            dr += sv * c.x;
-            di += -sv * c.y;
-          }
-          return make_float2(dr * (1.0f / 16.0f), di * (1.0f / 16.0f));
-        };
-        const float2 dj = demod(j), dk = demod(k);
-        const float er = dj.x - dk.x, ei = dj.y - dk.y;
-        const double e = 0.25 * (double)(er * er + ei * ei);
-        acc += e;
-        ++n;
-        band_acc[band] += e;
-        ++band_n[band];
-      }
-    }
-    if (n > 0) {
-      std::vector<float> brms;
-      for (size_t b = 0; b < band_acc.size(); ++b)
-        if (band_n[b] >= 8) brms.push_back((float)(band_acc[b] / band_n[b]));
-      if (!brms.empty()) {
-        const size_t k95 = std::min(brms.size() - 1, (size_t)(0.95 * brms.size()));
-        std::nth_element(brms.begin(), brms.begin() + k95, brms.end());
-        pair_amb[j] = std::sqrt(brms[k95]);
-      } else {
-        pair_amb[j] = std::sqrt((float)(acc / n));
-      }
-      pair_ok[j] = 1;
-    }
-  });
+// Adaptive temporal strength (sequence.cpp:526-646), the host's part: the
+// median over the same-parity pairs of their ambiguities (measured on the
+// device, k_amb_terms / k_amb_pairs), the noise floor removed, mapped to a
+// strength.
+float strength_from_pairs(const std::vector<float>& pair_amb, const std::vector<int>& pair_ok,
+                          float nr_eps, float* amb_out) {
   std::vector<float> ambs;
-  for (int j = 0; j < npairs; ++j)
+  for (size_t j = 0; j < pair_amb.size(); ++j)
     if (pair_ok[j]) ambs.push_back(pair_amb[j]);
   float amb = median_mean(ambs);
   const float sigma_d = nr_eps > 0.0f ? nr_eps / 3.0f : 1.0f;
@@ -224,6 +160,16 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
                              sizeof(int) * 2 * max_pairs + 256);
   size_t x_env[5];
   for (int i = 0; i < 5; ++i) x_env[i] = take(sizeof(float) * plane * nf);
+  // adaptive strength: the demodulation terms of each same-parity pair at
+  // rows 2, 5, ... < h - 2 and columns 4, 8, ... (x + 7 < w), and the pairs'
+  // ambiguities
+  const int amb_stride = pal ? 4 : 2;
+  int amb_nyi = 0, amb_nx = 0;
+  for (int y = 2; y < h - 2; y += 3) ++amb_nyi;
+  for (int x = 4; x + 7 < w; x += 4) ++amb_nx;
+  const int amb_pairs = std::max(0, nf - amb_stride);
+  const size_t x_amb = take(sizeof(double) * (size_t)std::max(1, amb_pairs) * amb_nyi * amb_nx);
+  const size_t x_ambo = take((sizeof(float) + sizeof(int)) * (size_t)std::max(1, amb_pairs) + 256);
   const size_t env_samples = ((size_t)h * w + 6) / 7;
   const size_t x_escr = take(sizeof(float) * env_samples * nf);
   const size_t x_nscr = take(sizeof(float) * (size_t)h * std::max(1, w - 8) * nf);
@@ -286,22 +232,24 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   if (cfg.temporal_eps <= 0.0f) cfg.temporal_eps = std::min(std::max(7.0f * sigma, 4.0f), 20.0f);
   if (cfg.nr_eps <= 0.0f) cfg.nr_eps = std::min(std::max(3.0f * sigma, 3.0f), 12.0f);
   float amb = 0.0f;
-  const int amb_stride = pal ? 4 : 2;
   if (cfg.temporal_strength == 0.0f && cfg.cg_iterations > 0 && nf > amb_stride) {
-    std::vector<std::vector<float>> Sh(nf, std::vector<float>((size_t)h * w));
-    std::vector<std::vector<float4>> Lh(nf, std::vector<float4>(h));
-    for (int j = 0; j < nf; ++j) {
-      e = cudaMemcpy2DAsync(Sh[j].data(), sizeof(float) * w, at<float>(ctx, L.o_S) + b.fp[j].px_off,
-                            sizeof(float) * pitch, sizeof(float) * w, h, cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(Lh[j].data(), at<float4>(ctx, L.o_lineph) + b.fp[j].line_off,
-                            sizeof(float4) * h, cudaMemcpyDeviceToHost, s);
-      if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "D2H window state");
-    }
-    e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "D2H window state");
-    cfg.temporal_strength = adaptive_strength(Sh, Lh, b.gtabs[0]->col_phasor, h, w, amb_stride,
-                                              cfg.nr_eps, &amb);
+    float* d_amb = at<float>(ctx, X(x_ambo));
+    int* d_ambok = reinterpret_cast<int*>(align_up((size_t)(d_amb + amb_pairs), 16));
+    hvdg::launch_amb_pairs(at<FieldDesc>(ctx, L.o_fields), amb_pairs, amb_stride, amb_nyi, amb_nx,
+                           at<float>(ctx, L.o_S), at<float4>(ctx, L.o_lineph),
+                           at<float2>(ctx, L.o_colph), cfg.nr_eps, at<double>(ctx, X(x_amb)),
+                           d_amb, d_ambok, s);
+    S.launches += 2;
+    std::vector<float> pair_amb(amb_pairs);
+    std::vector<int> pair_ok(amb_pairs);
+    e = cudaMemcpyAsync(pair_amb.data(), d_amb, sizeof(float) * amb_pairs, cudaMemcpyDeviceToHost,
+                        s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(pair_ok.data(), d_ambok, sizeof(int) * amb_pairs,
+                          cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return hvdg::cuda_fail(ctx, e, "adaptive strength");
+    cfg.temporal_strength = strength_from_pairs(pair_amb, pair_ok, cfg.nr_eps, &amb);
   }
   if (cfg.temporal_strength < 0.0f) cfg.temporal_strength = 0.0f;
   if (diag) {

@@ -1299,6 +1299,77 @@ def temporal_offsets(cfg, pal):
     return [-2, -1, 1, 2] if cfg.bidirectional else [-2, -1]
 
 
+def adaptive_strength(S_list, carriers, stride, nr_eps):
+    """The adaptive temporal strength (sequence.cpp:526-646) in the
+    reference's float32 operations and order: per same-parity pair (j,
+    j + stride), at rows 2, 5, ... < h - 2 and columns 4, 8, ... (x + 7 < w)
+    where the two fields' 4-sample means agree within nr_eps, the triangle-7
+    demodulations d = sum_k w_k S conj(c) / 16 and e = |d_j - d_k|^2 / 4
+    summed in double per band of 8 rows in row order; the pair's ambiguity
+    is the sqrt of the p95 band mean (bands with >= 8 terms; else of the
+    mean of all terms); the median over pairs, the noise floor 0.29 nr_eps/3
+    removed. Returns (strength, ambiguity)."""
+    f32 = np.float32
+    kW = np.array([1, 2, 3, 4, 3, 2, 1], f32)
+    eps = f32(nr_eps)
+    ambs = []
+    for j in range(len(S_list) - stride):
+        Sj = np.asarray(S_list[j], f32)
+        Sk = np.asarray(S_list[j + stride], f32)
+        cj = np.asarray(carriers[j], np.complex64)
+        ck = np.asarray(carriers[j + stride], np.complex64)
+        h, w = Sj.shape
+        xs = np.arange(4, w - 7, 4)
+        bands = []
+        for yi, y in enumerate(range(2, h - 2, 3)):
+            if yi // 8 >= len(bands):
+                bands.append([])
+            mj = np.zeros(len(xs), f32)
+            mk = np.zeros(len(xs), f32)
+            for q in range(4):
+                mj = mj + Sj[y, xs + q]
+                mk = mk + Sk[y, xs + q]
+            keep = ~(np.abs(mj - mk) * f32(0.25) > eps)
+
+            def demod(S, c):
+                dr = np.zeros(len(xs), f32)
+                di = np.zeros(len(xs), f32)
+                for q in range(7):
+                    sv = kW[q] * S[y, xs + q]
+                    cc = c[y, xs + q]
+                    dr = dr + sv * cc.real.astype(f32)
+                    di = di + sv * (-cc.imag.astype(f32))
+                return dr * f32(1.0 / 16.0), di * f32(1.0 / 16.0)
+
+            djr, dji = demod(Sj, cj)
+            dkr, dki = demod(Sk, ck)
+            er, ei = djr - dkr, dji - dki
+            e = 0.25 * (er * er + ei * ei).astype(np.float64)
+            bands[yi // 8].append(e[keep])
+        band_e = [np.concatenate(b) if b else np.zeros(0) for b in bands]
+        n = sum(len(b) for b in band_e)
+        if n == 0:
+            continue
+        # sequential double sums (np.cumsum adds in order)
+        brms = [f32(np.cumsum(b)[-1] / len(b)) for b in band_e if len(b) >= 8]
+        if brms:
+            k95 = min(len(brms) - 1, int(0.95 * len(brms)))
+            ambs.append(np.sqrt(np.sort(np.array(brms, f32))[k95]))
+        else:
+            acc = np.cumsum(np.concatenate(band_e))[-1]
+            ambs.append(np.sqrt(f32(acc / n)))
+    amb = f32(0.0)
+    if ambs:
+        v = np.sort(np.array(ambs, f32))
+        k = len(v) // 2
+        amb = v[k] if len(v) % 2 else f32(f32(0.5) * (v[k] + v[k - 1]))
+    sigma_d = f32(eps / f32(3.0)) if eps > 0 else f32(1.0)
+    floor = sigma_d * f32(0.29)
+    amb = np.sqrt(max(f32(0.0), f32(amb * amb - floor * floor)))
+    strength = min(max(f32(f32(0.5) * amb - f32(0.05)), f32(0.0)), f32(1.5))
+    return float(strength), float(amb)
+
+
 def decode_window_temporal(fields_ire, parities, g, cfg, strength):
     """DecodeFieldWindowWithInits with a fixed temporal strength > 0, one
     pass: per field (in the reference's sweep order) EstimateMotion on the

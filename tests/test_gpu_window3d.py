@@ -173,3 +173,31 @@ def test_window_temporal_integer_sad_me_vs_oracle(ctx):
         print(f"sad-me field {j}: Y gpu {pg:.3f} oracle {po:.3f}  C gpu {cg:.3f} oracle {co:.3f}")
         assert abs(pg - po) < 0.05
         assert abs(cg - co) < 0.05
+
+
+@pytest.mark.parametrize("std,seed", [(_cabi.STD_NTSC, 61), (_cabi.STD_PAL, 62)])
+def test_window_adaptive_strength_vs_reference(ctx, std, seed):
+    """The adaptive temporal strength (sequence.cpp:526-646), measured on the
+    device (k_amb_terms / k_amb_pairs: the reference's float operations in
+    its order, band sums in row order), against the compiled reference's
+    ambiguity and resolved strength on the same fields. The planes differ in
+    the last float bits (this build's carrier comes from FP64 phases), so the
+    bar is 1e-3 relative; the oracle restatement that reproduces the
+    reference exactly is pinned in test_oracle_pins.py."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    g = _cabi.default_geometry(std)
+    nf = 6 if std == _cabi.STD_NTSC else 10
+    fs = synth.make_sequence(seed, std, nf, noise_sigma=0.8, moving=True)
+    cfg = api.default_config(irls_outer=1, cg_iterations=2, fast=1, temporal_strength=0.0,
+                             passes=1)
+    ctx.decode_field_window([api.Field(f.samples, g, parity=f.parity) for f in fs], cfg)
+    d = ctx.last_diag
+    _, _, rd = ref.decode_field_window([synth.to_ire(f.samples) for f in fs],
+                                       [f.parity for f in fs], g, cfg)
+    print(f"std={std}: device amb {d.ambiguity_ire:.7f} strength {d.resolved_strength:.7f} "
+          f"nr_eps {d.nr_eps:.7f}; reference {rd[1]:.7f} {rd[0]:.7f} {rd[4]:.7f}")
+    assert d.ambiguity_ire > 0.1
+    assert abs(d.ambiguity_ire - rd[1]) <= 1e-3 * rd[1]
+    assert abs(d.resolved_strength - rd[0]) <= 1e-3 * max(rd[0], 0.05)

@@ -412,3 +412,31 @@ def test_oracle_other_standards_match_reference(case):
     (yo, co, _), = O.decode_fields_2d([ire], [0], g, cfg)
     (yr,), (cr,) = ref.decode_fields([ire], [0], [g], [cfg], across_fields=False)
     assert np.abs(yo - yr).max() < 2e-2 and np.abs(co - cr).max() < 2e-2
+
+
+@pytest.mark.parametrize("std,seed", [(0, 61), (1, 62)])
+def test_oracle_adaptive_strength_matches_reference(std, seed):
+    """The adaptive temporal strength (sequence.cpp:526-646): the oracle's
+    float32 restatement, fed the compiled reference's own prepared S and
+    carrier planes and its calibrated nr_eps, gives the reference's
+    ambiguity and resolved strength exactly."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    from hvdg import api, synth
+    g = _cabi.default_geometry(std)
+    nf = 6 if std == _cabi.STD_NTSC else 10
+    fs = synth.make_sequence(seed, std, nf, noise_sigma=0.8, moving=True)
+    ires = [synth.to_ire(f.samples) for f in fs]
+    par = [f.parity for f in fs]
+    cfg = api.default_config(irls_outer=1, cg_iterations=2, fast=1, temporal_strength=0.0,
+                             passes=1)
+    _, _, diag = ref.decode_field_window(ires, par, g, cfg)
+    sc = [ref.prepare_field(i, g, cfg, p) for i, p in zip(ires, par)]
+    stride = 4 if O.uses_vswitch(g) else 2
+    strength, amb = O.adaptive_strength([s for s, _ in sc], [c for _, c in sc], stride,
+                                        float(diag[4]))
+    print(f"std={std}: reference amb {diag[1]!r} strength {diag[0]!r}; oracle {amb!r} {strength!r}")
+    assert amb > 0.0
+    assert np.float32(amb) == diag[1]
+    assert np.float32(strength) == diag[0]
