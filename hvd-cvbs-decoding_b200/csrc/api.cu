@@ -517,9 +517,10 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
   // cannot grow
   const int h = last_active_line(g) - g.first_active_field_line;
   const int w = g.active_video_end - g.active_video_start;
-  // each plane 256-byte aligned
+  // each plane 256-byte aligned; after the planes, the fields' burst
+  // amplitudes (a page-locked target keeps their copy asynchronous)
   const size_t n_ire = align_up((size_t)f1 * fw, 64), n_y = align_up((size_t)h * w, 64);
-  const size_t staging = (size_t)nfield * (n_ire + 3 * n_y);
+  const size_t staging = (size_t)nfield * (n_ire + 3 * n_y) + align_up((size_t)nfield, 64);
   std::vector<float> pageable;
   float* stage = nullptr;
   if (ctx->pinned.reserve(sizeof(float) * staging) == HVDG_OK) {
@@ -565,9 +566,10 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
     fo[j].theta = th[j].data();
     fo[j].vswitch = vs[j].data();
   }
-  std::vector<float> amps(nfield, 0.0f);
+  float* amps = stage + (size_t)nfield * (n_ire + 3 * n_y);
+  std::fill(amps, amps + nfield, 0.0f);
   RunOpts opt;
-  opt.amp_out = amps.data();
+  opt.amp_out = amps;
   hvdg_diag local;
   hvdg_diag* dg = diag ? diag : &local;
   if (cfg->selective_3d && cfg->cg_iterations > 0 && cfg->temporal_strength >= 0.0f) {
@@ -583,7 +585,7 @@ hvdg_status hvdg_decode_frame_sequence_window_at(hvdg_ctx* ctx, const int16_t* c
   if (st != HVDG_OK) return st;
   float acc_gain = 1.0f;
   if (cfg->acc) {
-    std::vector<float> a = amps;
+    std::vector<float> a(amps, amps + nfield);
     const size_t k = a.size() / 2;
     std::nth_element(a.begin(), a.begin() + k, a.end());
     acc_gain = std::min(std::max(nominal_burst(g) / std::max(a[k], 1.0f), 0.5f), 2.0f);
