@@ -646,15 +646,8 @@ __device__ bool phase_iter(const SolverArgs& A, const FieldDesc& f, const Unit& 
   const int nrows = yend - ybeg + 1;
   double pH = 0.0, pgd = 0.0, pgq = 0.0, pqq = 0.0, pgg = 0.0;
   bool ok = true;
+  // the first min(kNS, nrows) rows' copies were issued by the caller
   __syncwarp();
-  if (lane == 0) {
-    fence_proxy_async_global();
-    fence_proxy_async_smem();
-    for (int i = 0; i < min(kNS, nrows); ++i) {
-      const int y = ybeg + i;
-      ring_issue<kDiag>(ring, i % kNS, A, f, c, u.x0, y, first, y >= u.y0 && y < u.y1);
-    }
-  }
   auto slot_ptr = [&](int i) { return ring.slots + (i % kNS) * RingLayout<kDiag>::slot; };
   auto issue_after = [&](int i_free) {
     __syncwarp();
@@ -1045,15 +1038,6 @@ __global__ void __launch_bounds__(kSolverThreads, kDiag ? 1 : 2)
     }
     if (dp >= p) continue;  // phase skipped by an early CG exit
     __syncwarp();
-    FieldCtl c;
-    {
-      const FieldCtl* vc = A.ctl + u.field;
-      c.alpha = __ldcg(&vc->alpha);
-      c.beta = __ldcg(&vc->beta);
-      c.pending = __ldcg(&vc->pending);
-      c.sel = __ldcg(&vc->sel);
-      c.xsel = __ldcg(&vc->xsel);
-    }
     const int B = 2 + f.n_inner;
     int kind, k = 0;
     if (p == f.n_outer * B) {
@@ -1062,6 +1046,34 @@ __global__ void __launch_bounds__(kSolverThreads, kDiag ? 1 : 2)
       const int r = p % B;
       kind = r == 0 ? kPhaseR : (r == 1 ? kPhaseG : kPhaseI);
       k = r - 2;
+    }
+    // A CG sweep's plane buffers follow from its position alone: the G phase
+    // sets sel = 0 and every CG completion flips it (an early exit skips the
+    // rest of the outer), every R completion flips xsel. So its first rows'
+    // bulk copies go out before the control block's loads return, and the
+    // block only supplies alpha and beta.
+    FieldCtl ci;
+    if (kind == kPhaseI) {
+      ci.sel = k & 1;
+      ci.xsel = (p / B + 1) & 1;
+      if (lane == 0) {
+        const int ybeg = max(u.y0 - 1, 0), yend = min(u.y1, f.h - 1);
+        fence_proxy_async_global();
+        fence_proxy_async_smem();
+        for (int i = 0; i < min(kNS, yend - ybeg + 1); ++i) {
+          const int y = ybeg + i;
+          ring_issue<kDiag>(ring, i % kNS, A, f, ci, u.x0, y, k == 0, y >= u.y0 && y < u.y1);
+        }
+      }
+    }
+    FieldCtl c;
+    {
+      const FieldCtl* vc = A.ctl + u.field;
+      c.alpha = __ldcg(&vc->alpha);
+      c.beta = __ldcg(&vc->beta);
+      c.pending = __ldcg(&vc->pending);
+      c.sel = kind == kPhaseI ? ci.sel : __ldcg(&vc->sel);
+      c.xsel = kind == kPhaseI ? ci.xsel : __ldcg(&vc->xsel);
     }
     double part[kNPart] = {0.0, 0.0, 0.0, 0.0, 0.0};
     // the rarely taken phases are out of line (their registers do not

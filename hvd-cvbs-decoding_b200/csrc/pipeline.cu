@@ -218,14 +218,18 @@ std::vector<float2> twiddles(int M) {
 int auto_band_rows_hw(hvdg_ctx* ctx, const std::vector<std::pair<int, int>>& hw) {
   const int warps = ctx->sm_count * std::max(1, hvdg::solver_max_blocks_per_sm()) *
                     (hvdg::kSolverThreads / 32);
-  static const int cand[] = {32, 24, 16, 12, 8, 6, 4};
+  // a lone field (or a few) never fills the resident warps; there a CG
+  // phase costs a unit's fixed latency plus ~1 us per row, and 3-row bands
+  // measured fastest (single NTSC field: 2-row 2.82, 3-row 2.29, 4-row
+  // 2.44 ms of solver for 5 x 30)
+  static const int cand[] = {32, 24, 16, 12, 8, 6, 4, 3};
   for (int band : cand) {
     int64_t units = 0;
     for (const auto& p : hw)
       units += (int64_t)((p.second + hvdg::kStrip - 1) / hvdg::kStrip) * ((p.first + band - 1) / band);
     if (units >= warps) return band;
   }
-  return 4;
+  return 3;
 }
 
 int auto_band_rows(hvdg_ctx* ctx, const std::vector<FieldPlan>& fp) {

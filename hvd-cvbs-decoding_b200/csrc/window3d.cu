@@ -65,7 +65,13 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
   // of the sweep: every field alone in the slow temporal sweep) ----
   RunOpts o3 = opt;
   if (o3.band_rows < 0 && ctx->band_rows <= 0) {
-    const bool temporal = cfg.temporal_strength > 0.0f && cfg.cg_iterations > 0;
+    // an automatic strength (0) is measured after the batch is planned; it
+    // resolves above 0 on all but clean static content, so such a window is
+    // planned for the temporal sweep too
+    const int scan_stride = pal ? 4 : 2;
+    const bool temporal =
+        (cfg.temporal_strength > 0.0f || (cfg.temporal_strength == 0.0f && nf > scan_stride)) &&
+        cfg.cg_iterations > 0;
     int colour = nf;
     if ((cfg.fast || !temporal) && cfg.parallel_across_fields) {
       int max_off = 0;
