@@ -28,21 +28,22 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 
 // One line of BoxBlur (motion.cpp:21-55): prefix sums c_k = c_(k-1) +
 // s_(k-1) in double, in order, and out_i = (c_min(i+r+1, n) - c_max(i-r, 0))
-// * norm, from a ring of the last 2 r + 2 prefix sums; samples `ss` apart
-// in the source, outputs `ds` apart. Output i is written as soon as the
-// prefix its window ends at exists (the ones cut by the line's end last).
-// The samples are fetched kBoxChunk at a time ahead of their additions, so
-// the in-order sum waits on one memory round trip per chunk, not per
-// sample; the values are those of the sample-by-sample loop.
+// * norm; samples `ss` apart in the source, outputs `ds` apart. Output i is
+// written as soon as the prefix its window ends at exists (the ones cut by
+// the line's end last). The last 32 prefix sums of each thread live in a
+// shared-memory history (slot k & 31, one column per thread of a block of
+// at most kBoxThreads), so no step divides or touches local memory; the
+// samples are fetched kBoxChunk at a time ahead of their additions. The
+// values are those of the sample-by-sample loop. Needs 2 r + 1 <= 31.
 constexpr int kBoxChunk = 16;
+constexpr int kBoxThreads = 128;
 
 __device__ __forceinline__ void box_line(const float* __restrict__ s, int64_t ss,
                                          float* __restrict__ d, int64_t ds, int n, int r,
                                          double norm) {
-  double ring[32];
-  const int R = 2 * r + 2;
+  __shared__ double hist[32 * kBoxThreads];
+  double* h = hist + threadIdx.x;
   double c = 0.0;
-  ring[0] = 0.0;
   for (int k0 = 1; k0 <= n; k0 += kBoxChunk) {
     float v[kBoxChunk];
 #pragma unroll
@@ -52,42 +53,41 @@ __device__ __forceinline__ void box_line(const float* __restrict__ s, int64_t ss
       const int k = k0 + j;
       if (k <= n) {
         c = c + (double)v[j];
-        ring[k % R] = c;
+        h[(k & 31) * kBoxThreads] = c;
         const int i = k - r - 1;
         if (i >= 0) {
-          const int i0 = i - r > 0 ? i - r : 0;
-          d[(int64_t)i * ds] = (float)((c - ring[i0 % R]) * norm);
+          const int i0 = i - r;
+          const double c0v = i0 > 0 ? h[(i0 & 31) * kBoxThreads] : 0.0;
+          d[(int64_t)i * ds] = (float)((c - c0v) * norm);
         }
       }
     }
   }
   for (int i = n - r > 0 ? n - r : 0; i < n; ++i) {
-    const int i0 = i - r > 0 ? i - r : 0;
-    d[(int64_t)i * ds] = (float)((ring[n % R] - ring[i0 % R]) * norm);
+    const int i0 = i - r;
+    d[(int64_t)i * ds] = (float)((c - (i0 > 0 ? h[(i0 & 31) * kBoxThreads] : 0.0)) * norm);
   }
 }
 
 // box_line along rows for one warp: lane l runs row l of a 32-row band
 // (`rows` of them exist). The band's samples arrive 32 columns at a time
 // through shared memory, each load instruction reading one row's 32
-// consecutive columns, so the rows' in-order prefix sums wait on one
-// coalesced round trip per 32 columns.
+// consecutive columns. Per chunk, each lane first runs its row's prefix sums
+// (the only serial chain: one double add per column, in column order, the
+// loads and conversions ahead of it) into a 64-slot shared-memory history,
+// then forms the chunk's window sums from that history with no chain at all
+// (prefix k minus prefix k - 2 r - 1, the same doubles as a running ring),
+// and the outputs leave through a shared tile as coalesced row segments.
+// Needs 2 r + 1 <= 32.
 __device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float* __restrict__ d,
                                               int64_t pitch, int rows, int n, int r,
                                               double norm) {
   __shared__ float tile[32][33];
-  // each lane's ring of the last R = 2 r + 2 prefix sums (R <= 32); the
-  // prefix a window starts at, k - 2 r - 1, sits in the slot after prefix
-  // k's, so the slots advance by one per step without a division
-  __shared__ double sring[32][33];
+  __shared__ double pre[32][65];  // prefix k of lane l at pre[l][k & 63]
   const int lane = threadIdx.x & 31;
-  const bool live = lane < rows;
-  float* drow = d + (int64_t)lane * pitch;
-  double* ring = sring[lane];
-  const int R = 2 * r + 2;
+  double* hist = pre[lane];
   double c = 0.0;
-  ring[0] = 0.0;
-  int kr = 0;  // slot of prefix k
+  hist[0] = 0.0;
   for (int c0 = 0; c0 < n; c0 += 32) {
     {
       // all 32 loads issued before the first store
@@ -99,31 +99,46 @@ __device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float
       for (int q = 0; q < 32; ++q) tile[q][lane] = v[q];
     }
     __syncwarp();
-    if (live) {
-      for (int j = 0; j < 32; ++j) {
-        const int k = c0 + j + 1;
-        if (k > n) break;
-        c = c + (double)tile[lane][j];
-        kr = kr + 1 == R ? 0 : kr + 1;
-        ring[kr] = c;
-        const int i = k - r - 1;
-        if (i >= 0) {
-          // window start max(i - r, 0): prefix k - R + 1 (the next slot) or 0
-          const double c0v = i - r > 0 ? ring[kr + 1 == R ? 0 : kr + 1] : ring[0];
-          drow[i] = (float)((c - c0v) * norm);
+    const int m = min(32, n - c0);  // columns of this chunk
+    {
+      double v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = (double)tile[lane][j];
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < m) {
+          c = c + v[j];
+          hist[(c0 + j + 1) & 63] = c;
         }
+    }
+    __syncwarp();
+    // window sums ending at prefix k = c0 + j + 1: output column i = k - r - 1
+    // (window [max(i - r, 0), i + r]), staged in the tile at column j
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int k = c0 + j + 1, i = k - r - 1;
+      float o = 0.0f;
+      if (j < m && i >= 0) {
+        const double c0v = i - r > 0 ? hist[(i - r) & 63] : 0.0;
+        o = (float)((hist[k & 63] - c0v) * norm);
       }
+      tile[lane][j] = o;
+    }
+    __syncwarp();
+    // row q's outputs of this chunk: columns c0 - r .. c0 + m - 1 - r
+#pragma unroll 4
+    for (int q = 0; q < rows; ++q) {
+      const int i = c0 - r + lane;
+      if (lane < m && i >= 0) d[(int64_t)q * pitch + i] = tile[q][lane];
     }
     __syncwarp();
   }
-  if (!live) return;
-  // outputs whose window is cut by the end: prefix n is in slot kr
+  if (lane >= rows) return;
+  // outputs whose window is cut by the end: prefix n is c
+  float* drow = d + (int64_t)lane * pitch;
   for (int i = n - r > 0 ? n - r : 0; i < n; ++i) {
     const int i0 = i - r > 0 ? i - r : 0;
-    // slot of prefix i0: kr - (n - i0), wrapped
-    int si = kr - (n - i0) % R;
-    if (si < 0) si += R;
-    drow[i] = (float)((c - ring[i0 > 0 ? si : 0]) * norm);
+    drow[i] = (float)((c - (i0 > 0 ? hist[i0 & 63] : 0.0)) * norm);
   }
 }
 
@@ -599,7 +614,8 @@ __global__ void __launch_bounds__(256) k_me_confidence(const MeField* __restrict
 void launch_motion_blur(const MeField* d_fields, int nf, int max_h, int max_w, const MeBuffers& b,
                         cudaStream_t st) {
   if (nf <= 0) return;
-  k_blur_v<<<dim3((max_w + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.luma, b.tmp, 2, 0);
+  k_blur_v<<<dim3((max_w + kBoxThreads - 1) / kBoxThreads, nf), kBoxThreads, 0, st>>>(
+      d_fields, nf, b.luma, b.tmp, 2, 0);
   k_blur_h<<<dim3((max_h + 31) / 32, nf), 32, 0, st>>>(d_fields, nf, b.tmp, b.blur, 2);
 }
 
@@ -608,7 +624,8 @@ void launch_motion(const MeField* d_fields, int nf, int max_h, int max_w, const 
   if (nf <= 0 || npairs <= 0) return;
   const int r = 2;
   // blur every field's luma (A = blur(y_cur), B = blur(y_ref) share per field)
-  k_blur_v<<<dim3((max_w + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.luma, b.tmp, r, 0);
+  k_blur_v<<<dim3((max_w + kBoxThreads - 1) / kBoxThreads, nf), kBoxThreads, 0, st>>>(
+      d_fields, nf, b.luma, b.tmp, r, 0);
   k_blur_h<<<dim3((max_h + 31) / 32, nf), 32, 0, st>>>(d_fields, nf, b.tmp, b.blur, r);
   k_decimate<<<dim3(((max_h / 4) * (max_w / 4) + 255) / 256, nf), 256, 0, st>>>(d_fields, nf, b.blur, b.dec);
   const int ct = a.tile / 4 > 4 ? a.tile / 4 : 4;
@@ -1500,7 +1517,8 @@ void launch_vectors(const MeField* d_fields, const MePair* d_pairs, int npairs, 
   } else {
     k_conf_pixels_nearest<<<dim3((max_w + 127) / 128, max_h, npairs), 128, 0, st>>>(
         d_fields, d_pairs, npairs, a, v.conf, v.conf_tmp, v.pix_off);
-    k_pair_blur_v<<<dim3((max_w + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs,
+    k_pair_blur_v<<<dim3((max_w + kBoxThreads - 1) / kBoxThreads, npairs), kBoxThreads, 0,
+                    st>>>(d_fields, d_pairs, npairs,
                                                                      v.conf_tmp, v.conf_px,
                                                                      v.pix_off, 8);
     k_pair_blur_h<<<dim3((max_h + 31) / 32, npairs), 32, 0, st>>>(d_fields, d_pairs, npairs,
@@ -1561,7 +1579,8 @@ void launch_coherence_gate(const MeField* d_fields, const MePair* d_pairs, int n
   // ComplexCoherence's four BoxBlur(r = 6) passes (temporal.cpp:186-189)
   for (int c = 0; c < 4; ++c) {
     float* ch = b.terms + c * b.chan_stride;
-    k_pair_blur_v<<<dim3((max_w + 127) / 128, npairs), 128, 0, st>>>(d_fields, d_pairs, npairs, ch,
+    k_pair_blur_v<<<dim3((max_w + kBoxThreads - 1) / kBoxThreads, npairs), kBoxThreads, 0,
+                    st>>>(d_fields, d_pairs, npairs, ch,
                                                                     b.tmp, b.pix_off, 6);
     k_pair_blur_h<<<dim3((max_h + 31) / 32, npairs), 32, 0, st>>>(d_fields, d_pairs, npairs,
                                                                  b.tmp, ch, b.pix_off, 6);

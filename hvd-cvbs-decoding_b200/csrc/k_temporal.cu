@@ -82,11 +82,13 @@ __global__ void k_env_maps(const FieldDesc* __restrict__ fields, const int* __re
 // to the row, sqrt(mean), both maps. One warp per (field, 32-row band): lane
 // l runs row l's in-order float running sum; the band's samples arrive 32
 // columns (plus the window's 3 / 2 columns either side) at a time through
-// shared memory, one coalesced row segment per load instruction.
+// shared memory, one coalesced row segment per load instruction. The tile's
+// rows are 41 floats apart, so a lane's reads along its own row hit a
+// different bank from every other lane's.
 __global__ void k_env_smooth(const FieldDesc* __restrict__ fields, const int* __restrict__ list,
                              const float* __restrict__ gmag, const float* __restrict__ lapmag,
                              float* __restrict__ vraw, float* __restrict__ traw) {
-  __shared__ float tile[32][40];
+  __shared__ float tile[32][41];
   const FieldDesc f = fields[list[blockIdx.y]];
   const int y0 = blockIdx.x * 32;
   if (y0 >= f.h) return;
