@@ -79,12 +79,14 @@ __global__ void k_env_maps(const FieldDesc* __restrict__ fields, const int* __re
 }
 
 // (2) smooth_rows (sequence.cpp:860-889): sliding sum over [x-2, x+2] clipped
-// to the row, sqrt(mean), both maps. One warp per (field, 32-row band): lane
-// l runs row l's in-order float running sum; the band's samples arrive 32
-// columns (plus the window's 3 / 2 columns either side) at a time through
-// shared memory, one coalesced row segment per load instruction. The tile's
-// rows are 41 floats apart, so a lane's reads along its own row hit a
-// different bank from every other lane's.
+// to the row, sqrt(mean), both maps. The running sums: one warp per (field,
+// 32-row band, map): lane l runs row l's in-order float running sum (the
+// same additions and subtractions in column order); the band's samples
+// arrive 32 columns (plus the window's 3 / 2 columns either side) at a time
+// through shared memory, one coalesced row segment per load instruction, and
+// the sums leave the same way. The tile's rows are 41 floats apart, so a
+// lane's reads along its row hit a different bank from every other lane's.
+// The means and square roots, off the chain, follow in k_env_sqrt.
 __global__ void k_env_smooth(const FieldDesc* __restrict__ fields, const int* __restrict__ list,
                              const float* __restrict__ gmag, const float* __restrict__ lapmag,
                              float* __restrict__ vraw, float* __restrict__ traw) {
@@ -96,47 +98,63 @@ __global__ void k_env_smooth(const FieldDesc* __restrict__ fields, const int* __
   const int rows = min(32, f.h - y0);
   const bool live = lane < rows;
   const int ww = f.w;
-  for (int m = 0; m < 2; ++m) {
-    const float* src = (m == 0 ? gmag : lapmag) + f.px_off + (int64_t)y0 * f.pitch;
-    float* out = (m == 0 ? vraw : traw) + f.px_off + (int64_t)(y0 + lane) * f.pitch;
-    float acc = 0.0f;
-    if (live)
-      for (int x = 0; x < (ww < 3 ? ww : 3); ++x) acc += src[(int64_t)lane * f.pitch + x];
-    for (int c0 = 0; c0 < ww; c0 += 32) {
-      // columns c0 - 3 .. c0 + 34 of every row of the band
-      {
-        // all loads issued before the first store
-        float v[32], e[32];
-        const int col = c0 - 3 + lane, col2 = c0 + 29 + lane;  // second pass: lanes 0-5
-        const bool in1 = col >= 0 && col < ww, in2 = lane < 6 && col2 < ww;
+  const int m = blockIdx.z;
+  const float* src = (m == 0 ? gmag : lapmag) + f.px_off + (int64_t)y0 * f.pitch;
+  float* out = (m == 0 ? vraw : traw) + f.px_off + (int64_t)y0 * f.pitch;
+  float acc = 0.0f;
+  if (live)
+    for (int x = 0; x < (ww < 3 ? ww : 3); ++x) acc += src[(int64_t)lane * f.pitch + x];
+  for (int c0 = 0; c0 < ww; c0 += 32) {
+    // columns c0 - 3 .. c0 + 34 of every row of the band
+    {
+      // all loads issued before the first store
+      float v[32], e[32];
+      const int col = c0 - 3 + lane, col2 = c0 + 29 + lane;  // second pass: lanes 0-5
+      const bool in1 = col >= 0 && col < ww, in2 = lane < 6 && col2 < ww;
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-          v[q] = in1 && q < rows ? src[(int64_t)q * f.pitch + col] : 0.0f;
-          e[q] = in2 && q < rows ? src[(int64_t)q * f.pitch + col2] : 0.0f;
-        }
+      for (int q = 0; q < 32; ++q) {
+        v[q] = in1 && q < rows ? src[(int64_t)q * f.pitch + col] : 0.0f;
+        e[q] = in2 && q < rows ? src[(int64_t)q * f.pitch + col2] : 0.0f;
+      }
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-          tile[q][lane] = v[q];
-          if (lane < 6) tile[q][32 + lane] = e[q];
-        }
+      for (int q = 0; q < 32; ++q) {
+        tile[q][lane] = v[q];
+        if (lane < 6) tile[q][32 + lane] = e[q];
       }
-      __syncwarp();
-      if (live) {
-        for (int j = 0; j < 32; ++j) {
-          const int x = c0 + j;
-          if (x >= ww) break;
-          const int lo = x - 2, hi = x + 2;
-          if (x > 0) {
-            if (hi < ww) acc += tile[lane][j + 5];
-            if (lo - 1 >= 0) acc -= tile[lane][j];
-          }
-          const int n_taps = (hi < ww - 1 ? hi : ww - 1) - (lo > 0 ? lo : 0) + 1;
-          out[x] = sqrtf(acc / (float)n_taps);
-        }
-      }
-      __syncwarp();
     }
+    __syncwarp();
+    const int mm = min(32, ww - c0);  // columns of this chunk
+    // column j reads tile columns j and j + 5 and then holds its running
+    // sum in column j (no later column reads it)
+    for (int j = 0; j < mm; ++j) {
+      const int x = c0 + j;
+      if (x > 0) {
+        if (x + 2 < ww) acc += tile[lane][j + 5];
+        if (x - 3 >= 0) acc -= tile[lane][j];
+      }
+      tile[lane][j] = acc;
+    }
+    __syncwarp();
+#pragma unroll 4
+    for (int q = 0; q < rows; ++q)
+      if (lane < mm) out[(int64_t)q * f.pitch + c0 + lane] = tile[q][lane];
+    __syncwarp();
   }
+}
+
+// (2b) the running sums to sqrt(sum / taps), taps = |[x-2, x+2] clipped to
+// the row|, both maps, one thread per pixel
+__global__ void k_env_sqrt(const FieldDesc* __restrict__ fields, const int* __restrict__ list,
+                           float* __restrict__ vraw, float* __restrict__ traw) {
+  const FieldDesc f = fields[list[blockIdx.z]];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= f.w || y >= f.h) return;
+  const int lo = x - 2, hi = x + 2;
+  const int n_taps = (hi < f.w - 1 ? hi : f.w - 1) - (lo > 0 ? lo : 0) + 1;
+  const int64_t o = f.px_off + (int64_t)y * f.pitch + x;
+  vraw[o] = sqrtf(vraw[o] / (float)n_taps);
+  traw[o] = sqrtf(traw[o] / (float)n_taps);
 }
 
 // (3) median of every 7th envelope value (flat row-major index), per field
@@ -357,8 +375,10 @@ void launch_envelope(const FieldDesc* d_fields, const int* d_list, int n, int ma
   if (n <= 0) return;
   k_env_maps<<<dim3((max_w + 127) / 128, max_h, n), 128, 0, st>>>(d_fields, d_list, Y, X, e.gmag,
                                                                    e.lapmag);
-  k_env_smooth<<<dim3((max_h + 31) / 32, n), 32, 0, st>>>(d_fields, d_list, e.gmag, e.lapmag,
-                                                          e.vraw, e.traw);
+  k_env_smooth<<<dim3((max_h + 31) / 32, n, 2), 32, 0, st>>>(d_fields, d_list, e.gmag, e.lapmag,
+                                                             e.vraw, e.traw);
+  k_env_sqrt<<<dim3((max_w + 127) / 128, max_h, n), 128, 0, st>>>(d_fields, d_list, e.vraw,
+                                                                   e.traw);
   k_env_floor<<<n, 1024, 0, st>>>(d_fields, d_list, e.vraw, e.scratch, e.scratch_off, e.floor2);
   k_env_gate<<<dim3((max_w + 127) / 128, max_h, n), 128, 0, st>>>(
       d_fields, d_list, e.vraw, e.traw, e.floor2, e2, floor_max, e.gate);

@@ -563,7 +563,7 @@ hvdg_status decode_window_3d(hvdg_ctx* ctx, const hvdg_field_in* in, int nf,
           hvdg::launch_envelope(at<FieldDesc>(ctx, L.o_fields), d_list, (int)env_list.size(), h, w,
                                 at<float>(ctx, L.o_Y), at<float2>(ctx, L.o_X0), eb, e2, floor_max,
                                 s);
-          S.launches += 4;
+          S.launches += 5;
         }
         hvdg::launch_nbr_assemble(at<FieldDesc>(ctx, L.o_fields), d_np, npairs, h, w,
                                   at<float>(ctx, L.o_S), at<float4>(ctx, L.o_lineph),
