@@ -73,15 +73,25 @@ __device__ inline float block_select_kth(const float* v, int n, int k, unsigned*
   for (int shift = 24; shift >= 0; shift -= 8) {
     for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t key = float_key(v[i]);
-      // lanes counting into the same bin add once through their lowest lane
-      // (the keys of one selection crowd a few bins: without this the
-      // shared-memory atomics of a warp serialise)
-      const unsigned bin = (key & mask) == prefix ? (key >> shift) & 255u : 256u;
-      const unsigned peers = __match_any_sync(__activemask(), bin);
-      if (bin < 256u && (int)(__ffs(peers) - 1) == (int)(threadIdx.x & 31))
-        atomicAdd(&hist[bin], (unsigned)__popc(peers));
+    // four elements' loads in flight per thread (the values may sit in
+    // global memory), then their bins in turn; lanes counting into the same
+    // bin add once through their lowest lane (the keys of one selection
+    // crowd a few bins: without this the shared-memory atomics of a warp
+    // serialise)
+    const int step = blockDim.x;
+    for (int i0 = threadIdx.x; i0 - (int)threadIdx.x < n; i0 += 4 * step) {
+      float x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = i0 + q * step < n ? v[i0 + q * step] : 0.0f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t key = float_key(x[q]);
+        const unsigned bin = i0 + q * step < n && (key & mask) == prefix ? (key >> shift) & 255u
+                                                                         : 256u;
+        const unsigned peers = __match_any_sync(__activemask(), bin);
+        if (bin < 256u && (int)(__ffs(peers) - 1) == (int)(threadIdx.x & 31))
+          atomicAdd(&hist[bin], (unsigned)__popc(peers));
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
