@@ -577,13 +577,22 @@ __global__ void __launch_bounds__(256) k_me_confidence(const MeField* __restrict
     const int y0 = ty * tile, y1 = (ty == th - 1) ? h : (ty + 1) * tile;
     const int x0 = tx * tile, x1 = (tx == tw - 1) ? w : (tx + 1) * tile;
     float sum = 0.0f, sum2 = 0.0f, np = 0.0f;
-    for (int y = y0; y < y1; ++y)
-      for (int x = x0; x < x1; ++x) {
-        const float v = A[(int64_t)y * mc.pitch + x];
-        sum += v;
-        sum2 += v * v;
-        np += 1.0f;
+    for (int y = y0; y < y1; ++y) {
+      const float* arow = A + (int64_t)y * mc.pitch;
+      // eight samples' loads ahead of their additions, which stay in x order
+      for (int xb = x0; xb < x1; xb += 8) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = arow[xb + q < x1 ? xb + q : x1 - 1];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (xb + q < x1) {
+            sum += v[q];
+            sum2 += v[q] * v[q];
+            np += 1.0f;
+          }
       }
+    }
     const float norm = 1.0f / fmaxf(1.0f, np);
     const float tmean = sum * norm;
     const float tvar = sum2 * norm - tmean * tmean;
