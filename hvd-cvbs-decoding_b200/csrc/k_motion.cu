@@ -69,6 +69,13 @@ __device__ __forceinline__ void box_line(const float* __restrict__ s, int64_t ss
   }
 }
 
+// Shared memory of the row blur (declared once per kernel): the band's
+// 32 x 32 sample / output tile and each lane's 64-slot prefix history.
+struct RowBlurSmem {
+  float tile[32][33];
+  double hist[32][65];
+};
+
 // box_line along rows for one warp: lane l runs row l of a 32-row band
 // (`rows` of them exist). The band's samples arrive 32 columns at a time
 // through shared memory, each load instruction reading one row's 32
@@ -79,11 +86,11 @@ __device__ __forceinline__ void box_line(const float* __restrict__ s, int64_t ss
 // (prefix k minus prefix k - 2 r - 1, the same doubles as a running ring),
 // and the outputs leave through a shared tile as coalesced row segments.
 // Needs 2 r + 1 <= 32.
-__device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float* __restrict__ d,
-                                              int64_t pitch, int rows, int n, int r,
-                                              double norm) {
-  __shared__ float tile[32][33];
-  __shared__ double pre[32][65];  // prefix k of lane l at pre[l][k & 63]
+__device__ __forceinline__ void box_rows_warp_any(RowBlurSmem& sm, const float* __restrict__ s,
+                                                  float* __restrict__ d, int64_t pitch, int rows,
+                                                  int n, int r, double norm) {
+  float (&tile)[32][33] = sm.tile;
+  double (&pre)[32][65] = sm.hist;  // prefix k of lane l at pre[l][k & 63]
   const int lane = threadIdx.x & 31;
   double* hist = pre[lane];
   double c = 0.0;
@@ -140,6 +147,83 @@ __device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float
     const int i0 = i - r > 0 ? i - r : 0;
     drow[i] = (float)((c - (i0 > 0 ? hist[i0 & 63] : 0.0)) * norm);
   }
+}
+
+// The same blur for a radius known at compile time (the window's 2, 6 and
+// 8): a chunk's prefix sums and the previous chunk's stay in registers (every
+// index is a constant), so a column costs its one chained addition, a copy
+// of the sum into a shared history (read only by the windows cut by the
+// row's end) and its window sum.
+template <int R>
+__device__ __forceinline__ void box_rows_warp_r(RowBlurSmem& sm, const float* __restrict__ s,
+                                                float* __restrict__ d, int64_t pitch, int rows,
+                                                int n, double norm) {
+  constexpr int kW = 2 * R + 1;  // window: prefix k minus prefix k - kW
+  static_assert(kW <= 32, "window within two chunks");
+  float (&tile)[32][33] = sm.tile;
+  double (&hist)[32][65] = sm.hist;
+  const int lane = threadIdx.x & 31;
+  double* hrow = hist[lane];  // prefix k at slot k & 63, for the cut windows
+  double c = 0.0, prev[32], cur[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) prev[j] = 0.0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    {
+      float v[32];
+      const bool col = c0 + lane < n;
+#pragma unroll
+      for (int q = 0; q < 32; ++q) v[q] = col && q < rows ? s[(int64_t)q * pitch + c0 + lane] : 0.0f;
+#pragma unroll
+      for (int q = 0; q < 32; ++q) tile[q][lane] = v[q];
+    }
+    __syncwarp();
+    const int m = min(32, n - c0);
+    // the chain: cur[j] = prefix c0 + j + 1, in column order
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float x = tile[lane][j];
+      if (j < m) {
+        c = c + (double)x;
+        hrow[(c0 + j + 1) & 63] = c;
+      }
+      cur[j] = c;
+    }
+    __syncwarp();
+    // window sums ending at prefix k = c0 + j + 1 (output column k - R - 1),
+    // starting at prefix k - kW (0 below 1)
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int k = c0 + j + 1, i = k - R - 1;
+      const double c0v = k - kW > 0 ? (j - kW >= 0 ? cur[j - kW] : prev[j - kW + 32]) : 0.0;
+      tile[lane][j] = (j < m && i >= 0) ? (float)((cur[j] - c0v) * norm) : 0.0f;
+    }
+    __syncwarp();
+#pragma unroll 4
+    for (int q = 0; q < rows; ++q) {
+      const int i = c0 - R + lane;
+      if (lane < m && i >= 0) d[(int64_t)q * pitch + i] = tile[q][lane];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; ++j) prev[j] = cur[j];
+  }
+  if (lane >= rows) return;
+  // the windows cut by the row's end start within the last 2 R prefixes
+  float* drow = d + (int64_t)lane * pitch;
+  for (int i = n - R > 0 ? n - R : 0; i < n; ++i) {
+    const int i0 = i - R;
+    drow[i] = (float)((c - (i0 > 0 ? hrow[i0 & 63] : 0.0)) * norm);
+  }
+}
+
+__device__ __forceinline__ void box_rows_warp(const float* __restrict__ s, float* __restrict__ d,
+                                              int64_t pitch, int rows, int n, int r,
+                                              double norm) {
+  __shared__ RowBlurSmem sm;
+  if (r == 2) return box_rows_warp_r<2>(sm, s, d, pitch, rows, n, norm);
+  if (r == 6) return box_rows_warp_r<6>(sm, s, d, pitch, rows, n, norm);
+  if (r == 8) return box_rows_warp_r<8>(sm, s, d, pitch, rows, n, norm);
+  box_rows_warp_any(sm, s, d, pitch, rows, n, r, norm);
 }
 
 // ---- BoxBlur (motion.cpp:21-55): double prefix sums, constant 1/(2r+1) ----
