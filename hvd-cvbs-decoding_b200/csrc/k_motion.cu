@@ -502,12 +502,12 @@ __global__ void k_me_refine(const MeField* __restrict__ mf, const MePair* __rest
 // The same refinement with a warp per (pair, tile), for tiles of up to
 // kRefineWarpTile rows. Lane l computes the SSD of refine candidates l and
 // l + 32 (visit order) row by row in the reference's order, without the
-// bail-out, keeping the running sum after every row in shared memory. Lane
-// 0 then replays the reference's visit from those sums -- kill = best *
-// (1 / bias), the first row whose running sum reaches it ends the
-// candidate with that sum, strict-less update -- so every cost, decision
-// and vector is the per-thread kernel's; lanes 0-4 then take the four
-// CostAt sums and the zero-motion cost (full sums) at once.
+// bail-out, keeping the running sum after every row in shared memory. The
+// warp then replays the reference's visit from those sums -- kill = best *
+// (1 / bias), the first row whose running sum reaches it (a ballot over the
+// rows) ends the candidate with that sum, strict-less update -- so every
+// cost, decision and vector is the per-thread kernel's; lanes 0-4 then take
+// the four CostAt sums and the zero-motion cost (full sums) at once.
 constexpr int kRefineCands = 49;  // RangeFromCentre(-3, 3)^2
 constexpr int kRefineWarpTile = 64;
 
@@ -557,32 +557,32 @@ __global__ void k_me_refine_warp(const MeField* __restrict__ mf, const MePair* _
     }
   }
   __syncwarp();
+  // the reference's visit, the whole warp in step: for each candidate the
+  // first row whose running sum reaches kill is found by a ballot over the
+  // rows (lane r holds row r, r + 32), so every lane makes the same decisions
   float best = inf, mdy = 0.0f, mdx = 0.0f;
-  if (lane == 0) {
-    for (int c = 0; c < kRefineCands; ++c) {
-      const int dy = centre_out(c / 7), dx = centre_out(c % 7);
-      const float bias = 1.0f + 0.02f * (float)(abs(dy) + abs(dx));
-      const float inv_bias = 1.0f / bias;
-      const float kill = best * inv_bias;
-      const float* pc = part + c * tile;
-      float se = pc[rows - 1];
-      for (int r = 0; r < rows; ++r) {
-        if (pc[r] >= kill) {
-          se = pc[r];
-          break;
-        }
-      }
-      const float cost = se * bias;
-      if (cost < best) {
-        best = cost;
-        mdy = base_dy + (float)dy;
-        mdx = base_dx + (float)dx;
+  for (int c = 0; c < kRefineCands; ++c) {
+    const int dy = centre_out(c / 7), dx = centre_out(c % 7);
+    const float bias = 1.0f + 0.02f * (float)(abs(dy) + abs(dx));
+    const float inv_bias = 1.0f / bias;
+    const float kill = best * inv_bias;
+    const float* pc = part + c * tile;
+    float se = pc[rows - 1];
+    for (int r0 = 0; r0 < rows; r0 += 32) {
+      const bool hit = r0 + lane < rows && pc[r0 + lane] >= kill;
+      const unsigned b = __ballot_sync(0xffffffffu, hit);
+      if (b) {
+        se = pc[r0 + __ffs(b) - 1];
+        break;
       }
     }
+    const float cost = se * bias;
+    if (cost < best) {
+      best = cost;
+      mdy = base_dy + (float)dy;
+      mdx = base_dx + (float)dx;
+    }
   }
-  best = __shfl_sync(0xffffffffu, best, 0);
-  mdy = __shfl_sync(0xffffffffu, mdy, 0);
-  mdx = __shfl_sync(0xffffffffu, mdx, 0);
   // CostAt at (+-1, 0), (0, +-1) and the zero-motion cost: full sums
   const int iy = (int)lroundf(mdy), ix = (int)lroundf(mdx);
   float v = 0.0f;
