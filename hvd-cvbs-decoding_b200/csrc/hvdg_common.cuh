@@ -94,15 +94,36 @@ __device__ inline float block_select_kth(const float* v, int n, int k, unsigned*
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned acc = 0;
-      int b = 0;
-      for (; b < 256; ++b) {
-        if (acc + hist[b] > (unsigned)kk) break;
-        acc += hist[b];
+    if (threadIdx.x < 32) {
+      // the bin holding the kk-th key: lane l owns bins 8 l .. 8 l + 7; an
+      // exclusive scan of the lanes' totals gives each lane its base, and
+      // the lane whose bins cross kk names the bin (counts are exact)
+      const int l = threadIdx.x;
+      unsigned cnt[8], tot = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        cnt[q] = hist[8 * l + q];
+        tot += cnt[q];
       }
-      bcast[0] = (unsigned)b;
-      bcast[1] = acc;
+      unsigned incl = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (l >= o) incl += v;
+      }
+      unsigned acc = incl - tot;
+      if (acc <= (unsigned)kk && (unsigned)kk < incl) {
+        int b = 8 * l;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          if (b == 8 * l + q && acc + cnt[q] <= (unsigned)kk) {
+            acc += cnt[q];
+            ++b;
+          }
+        }
+        bcast[0] = (unsigned)b;
+        bcast[1] = acc;
+      }
     }
     __syncthreads();
     const uint32_t b = bcast[0];
