@@ -767,9 +767,12 @@ constexpr int kSadMaxBlock = 32;
 constexpr int kSadMaxRange = 22;         // (2 range + 1)^2 visit indices fit in 11 bits
 // block, window and the window's integral image at the largest block and range
 constexpr int kSadMaxWin = kSadMaxBlock + 2 * (kSadMaxRange + 1);
-constexpr int kSadMaxSmem =
-    (kSadMaxBlock * kSadMaxBlock + kSadMaxWin * kSadMaxWin + (kSadMaxWin + 1) * (kSadMaxWin + 1)) *
-    (int)sizeof(int);
+// block, window, integral image, then the packed copies (16-bit pairs) of
+// the block's rows and of the window's rows at even and odd starts
+__host__ __device__ constexpr int sad_smem_ints(int b, int ww) {
+  return b * b + ww * ww + (ww + 1) * (ww + 1) + b * (b / 2) + 2 * ww * (ww / 2 + 1);
+}
+constexpr int kSadMaxSmem = sad_smem_ints(kSadMaxBlock, kSadMaxWin) * (int)sizeof(int);
 constexpr int kSadThreads = 224;
 
 int sad_max_block() { return kSadMaxBlock; }
@@ -861,44 +864,105 @@ __device__ __forceinline__ unsigned long long warp_tile_cost(const int* As, cons
 // they read (one new load per pixel). Returns the thread's best key (biased
 // cost << 11 | centre-out visit index); the lane holding (0, 0) stores its
 // SAD in *sad0.
+// Two 16-bit lanes at once (the quantised luma is a uint16 code): the
+// per-lane maximum, and the sum of the two lanes added to an accumulator by
+// a two-way dot product with (1, 1).
+__device__ __forceinline__ unsigned vmax_u16x2(unsigned a, unsigned b) {
+  unsigned d;
+  asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+
+// Rows [yb, ye) of one item of a 16-wide block, packed: Ap holds the block's
+// rows as 8 pairs (columns 2k, 2k + 1), BpE / BpO each window row's pairs
+// starting at even / odd columns. For candidate offset dxg + g the window
+// pair under block pair k starts at column e_lo + (G - 1 - g) + 2 k, e_lo =
+// S - dxg - (G - 1); a0 = e_lo - Q (even, Q = e_lo & 1) is where this row's
+// words are loaded from, so every register index below is a constant.
+template <int G, int Q>
+__device__ __forceinline__ void sad_rows_packed(const unsigned* __restrict__ Ap,
+                                                const unsigned* __restrict__ BpE,
+                                                const unsigned* __restrict__ BpO, int hb, int wp,
+                                                int yb, int ye, int dy, int S, int a0h,
+                                                unsigned (&acc)[G]) {
+  constexpr int kWords = (Q + G - 1 + 14) / 2 + 1;
+  for (int yy = yb; yy < ye; ++yy) {
+    const unsigned* ap = Ap + yy * hb;
+    const int row = yy - dy + S;
+    const unsigned* be = BpE + row * wp + a0h;
+    const unsigned* bo = BpO + row * wp + a0h;
+    unsigned wE[kWords], wO[kWords];
+#pragma unroll
+    for (int j = 0; j < kWords; ++j) {
+      wE[j] = be[j];
+      wO[j] = bo[j];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const unsigned av = ap[k];
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int off = Q + (G - 1 - g) + 2 * k;
+        const unsigned bv = (off & 1) ? wO[off >> 1] : wE[off >> 1];
+        acc[g] = __dp2a_lo(vmax_u16x2(av, bv), 0x0101u, acc[g]);
+      }
+    }
+  }
+}
+
 template <int G, int BW>
 __device__ __forceinline__ unsigned long long sad_scan(const int* As, const int* Bs,
-                                                       const int* I, int b, int ww, int S, int bh,
-                                                       int bw, int s, unsigned sum_a,
-                                                       unsigned long long* sad0, unsigned one) {
+                                                       const int* I, const unsigned* Ap,
+                                                       const unsigned* BpE, const unsigned* BpO,
+                                                       int b, int ww, int S, int bh, int bw, int s,
+                                                       unsigned sum_a, unsigned long long* sad0,
+                                                       unsigned one) {
   const int n = 2 * s + 1;
   const int ngroups = (n + G - 1) / G;
   const int items = n * ngroups;
   const int wi = ww + 1;
   const int hsplit = (bh + 1) / 2;
   unsigned long long bestkey = ~0ull;
+  // items (dy, group of G offsets) ordered by the parity of their packed
+  // window start (odd G alternates it from group to group), so the lanes of a
+  // warp take the same packed code path
+  const int c0 = (S + s - G + 1) & 1;  // parity of group 0's start
+  const int n0 = (G & 1) ? (ngroups - c0 + 1) / 2 : (c0 == 0 ? ngroups : 0);
   for (int base = 0; base < 2 * items; base += blockDim.x) {
     const int it = base + threadIdx.x;
     const bool valid = it < 2 * items;
     const int item = it >> 1, half = it & 1;
-    const int dy = item / ngroups - s;
-    const int dxg = -s + (item % ngroups) * G;
+    int dyi, grp;
+    if (!(G & 1)) {
+      dyi = item / ngroups;
+      grp = item % ngroups;
+    } else if (item < n * n0) {
+      dyi = item / n0;
+      grp = c0 + 2 * (item % n0);
+    } else {
+      const int i1 = item - n * n0, n1 = ngroups - n0;
+      dyi = i1 / n1;
+      grp = (1 - c0) + 2 * (i1 % n1);
+    }
+    const int dy = dyi - s;
+    const int dxg = -s + grp * G;
     unsigned acc[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) acc[g] = 0u;
     if (valid) {
       const int yb = half ? hsplit : 0, ye = half ? bh : hsplit;
-      for (int yy = yb; yy < ye; ++yy) {
-        const int* ar = As + yy * b;
-        // window value under pixel xx at offset dxg + g: br[xx - g]
-        const int* br = Bs + (yy - dy + S) * ww + (S - dxg);
-        if (BW == 16) {
-          int win[16 + G - 1];  // win[j] = br[j - (G - 1)]
-#pragma unroll
-          for (int j = 0; j < 16 + G - 1; ++j) win[j] = br[j - (G - 1)];
-#pragma unroll
-          for (int xx = 0; xx < 16; ++xx) {
-            const int av = ar[xx];
-#pragma unroll
-            for (int g = 0; g < G; ++g)
-              acc[g] = (unsigned)max(av, win[xx - g + G - 1]) * one + acc[g];
-          }
-        } else {
+      if (BW == 16) {
+        const int e_lo = S - dxg - (G - 1);
+        const int a0h = (e_lo - (e_lo & 1)) >> 1;
+        if (e_lo & 1)
+          sad_rows_packed<G, 1>(Ap, BpE, BpO, b / 2, ww / 2 + 1, yb, ye, dy, S, a0h, acc);
+        else
+          sad_rows_packed<G, 0>(Ap, BpE, BpO, b / 2, ww / 2 + 1, yb, ye, dy, S, a0h, acc);
+      } else {
+        for (int yy = yb; yy < ye; ++yy) {
+          const int* ar = As + yy * b;
+          // window value under pixel xx at offset dxg + g: br[xx - g]
+          const int* br = Bs + (yy - dy + S) * ww + (S - dxg);
           for (int xx = 0; xx < bw; ++xx) {
             const int av = ar[xx];
 #pragma unroll
@@ -952,6 +1016,11 @@ __global__ void __launch_bounds__(kSadThreads, 6) k_sad_search(const MeField* __
   int* As = sad_sm;             // b x b
   int* Bs = sad_sm + b * b;     // ww x ww, B(clamp(y0 - S + wy), clamp(x0 - S + wx))
   int* I = Bs + ww * ww;        // (ww + 1)^2 integral image of Bs
+  // packed 16-bit pairs: the block's rows (b / 2 per row), the window's rows
+  // from even columns (BpE) and from odd columns (BpO), ww / 2 + 1 per row
+  unsigned* Ap = reinterpret_cast<unsigned*>(I + (ww + 1) * (ww + 1));
+  unsigned* BpE = Ap + b * (b / 2);
+  unsigned* BpO = BpE + ww * (ww / 2 + 1);
   __shared__ unsigned long long red[kSadThreads / 32];
   __shared__ unsigned long long sh_sad0, sh_best, sh_side[4], sh_ssd;
   __shared__ long long sh_s1, sh_s2;
@@ -983,6 +1052,23 @@ __global__ void __launch_bounds__(kSadThreads, 6) k_sad_search(const MeField* __
       }
     }
   }
+  {
+    // the packed copies (columns past the window's edge pack as 0)
+    const int hb = b / 2, wp = ww / 2 + 1;
+    for (int i = tid; i < b * hb; i += blockDim.x) {
+      const int r = i / hb, k = i % hb;
+      Ap[i] = (unsigned)As[r * b + 2 * k] | ((unsigned)As[r * b + 2 * k + 1] << 16);
+    }
+    for (int i = tid; i < ww * wp; i += blockDim.x) {
+      const int r = i / wp, k = i % wp;
+      const int* br = Bs + r * ww;
+      const unsigned e0 = 2 * k < ww ? (unsigned)br[2 * k] : 0u;
+      const unsigned e1 = 2 * k + 1 < ww ? (unsigned)br[2 * k + 1] : 0u;
+      const unsigned e2 = 2 * k + 2 < ww ? (unsigned)br[2 * k + 2] : 0u;
+      BpE[i] = e0 | (e1 << 16);
+      BpO[i] = e1 | (e2 << 16);
+    }
+  }
   if (warp == 0) {
     unsigned sa = 0;
     for (int i = lane; i < bh * bw; i += 32) sa += (unsigned)As[(i / bw) * b + i % bw];
@@ -1003,11 +1089,11 @@ __global__ void __launch_bounds__(kSadThreads, 6) k_sad_search(const MeField* __
   // (no wasted candidates at +-16), else 8
   unsigned long long bestkey;
   if (n % 11 == 0)
-    bestkey = bw == 16 ? sad_scan<11, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one)
-                       : sad_scan<11, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one);
+    bestkey = bw == 16 ? sad_scan<11, 16>(As, Bs, I, Ap, BpE, BpO, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one)
+                       : sad_scan<11, 0>(As, Bs, I, Ap, BpE, BpO, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one);
   else
-    bestkey = bw == 16 ? sad_scan<8, 16>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one)
-                       : sad_scan<8, 0>(As, Bs, I, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one);
+    bestkey = bw == 16 ? sad_scan<8, 16>(As, Bs, I, Ap, BpE, BpO, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one)
+                       : sad_scan<8, 0>(As, Bs, I, Ap, BpE, BpO, b, ww, S, bh, bw, s, sum_a, &sh_sad0, one);
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long v = __shfl_xor_sync(0xffffffffu, bestkey, o);
     if (v < bestkey) bestkey = v;
@@ -1144,7 +1230,7 @@ void launch_motion_sad(const MeField* d_fields, int nf, int max_h, int max_w,
   k_sad_hsum<<<dim3((max_h + 127) / 128, nf), 128, 0, st>>>(d_fields, nf, b.vsum, b.qblur);
   const int th = (max_h + a.block - 1) / a.block, tw = (max_w + a.block - 1) / a.block;
   const int ww = a.block + 2 * (a.range + 1);
-  const int smem = (a.block * a.block + ww * ww + (ww + 1) * (ww + 1)) * (int)sizeof(int);
+  const int smem = sad_smem_ints(a.block, ww) * (int)sizeof(int);
   static PerDeviceOnce sad_once;
   sad_once([] {
     cudaFuncSetAttribute(k_sad_search, cudaFuncAttributeMaxDynamicSharedMemorySize, kSadMaxSmem);
