@@ -463,7 +463,7 @@ hvdg_status decode_woven_frames(hvdg_ctx* ctx, const int16_t* const* chroma,
   if (st != HVDG_OK) return st;
   const int lines = last_active_line(g) - g.first_active_field_line;
   const int w = g.active_video_end - g.active_video_start;
-  st = check_plane(w, 2 * lines, uses_vswitch(g), hvdg::kColFftWide);
+  st = check_plane(w, 2 * lines, uses_vswitch(g));
   if (st != HVDG_OK) {
     ctx->last_error = "woven frame beyond the device-path limits";
     return st;

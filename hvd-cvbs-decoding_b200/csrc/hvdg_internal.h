@@ -17,9 +17,10 @@ namespace hvdg {
 
 constexpr int kStrip = 64;        // solver strip width (columns per warp unit)
 constexpr int kMaxLines = 1024;   // max field lines handled by the lock-in kernel
-constexpr int kRowFft = 2048;     // init: row cyclic-convolution length
+constexpr int kRowFft = 2048;     // init: row cyclic-convolution length (register FFT)
 constexpr int kColFft = 1024;     // init: column cyclic-convolution length (field planes)
 constexpr int kColFftWide = 2048; // init: column length of taller planes (woven frames)
+constexpr int kFftLong = 4096;    // init: rows / columns past the register lengths (shared-memory FFT)
 constexpr long long kSpinLimit = 4000000;  // bounded device waits: polls x ~0.5 us ~= 2 s
 constexpr int kInitPad = 16;      // init: reflect-101 row pad (holographic_init.cpp:214-222)
 
@@ -73,9 +74,10 @@ constexpr int kAdjExtB = 2;
 struct GeomDesc {
   int w, h, hp;        // active width, active lines, padded lines (h + 2 pad)
   int pad;             // row pad
-  int khat_row_off;    // offset (float2) of the 2 row kernels' spectra (2 * kRowFft)
+  int khat_row_off;    // offset (float2) of the 2 row kernels' spectra (2 * row_m)
   int khat_col_off;    // offset (float2) of the 2 column kernels' spectra (2 * col_m)
-  int col_m;           // column convolution length: kColFft or kColFftWide
+  int row_m;           // row convolution length: kRowFft or kFftLong
+  int col_m;           // column convolution length: kColFft, kColFftWide or kFftLong
   // symmetry-variant tables (offsets into the same float2 table; -1 when
   // the batch runs without the variant): Bluestein chirps exp(-i pi n^2 / N)
   // and chirp-filter spectra (1/M folded in) of the exact-length row (w)

@@ -13,7 +13,9 @@
 // power-of-two length M >= 2n - 1 (rows: 2048; columns: 1024, or 2048 for
 // woven frames) with the kernel's FFT precomputed on the host: a four-step
 // FFT held in registers (32 values per lane, one warp per 1024 points),
-// mask multiply in registers, inverse FFT, write.
+// mask multiply in registers, inverse FFT, write. Rows and columns past
+// those lengths (up to 2048 samples / padded lines) run at M = 4096 through
+// a shared-memory FFT (k_init_rows_long, k_init_cols_long).
 //   k_init_rows : one warp pair per padded row -> both row-filtered variants
 //   k_init_cols : one warp (pair) per column -> chi_1, chi_2 (x2 folded in)
 //   k_init_blend: edge-energy blend -> chi0, Y0
@@ -397,6 +399,7 @@ __global__ void __launch_bounds__(kColThreads, 3) k_init_cols(InitArgs a) {
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
+  if (gd.col_m == kFftLong) return;  // k_init_cols_long (uniform per CTA)
   if (gd.col_m == kColFftWide) {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
     const int pair = warp >> 1;
@@ -436,6 +439,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
   const int f_idx = a.prow_field[r];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
+  if (gd.row_m != kRowFft) return;  // k_init_rows_long (uniform per pair)
   const int yp = r - a.prow_first[f_idx];
   float2 v[32];
   // v[k] (natural order, x = 2 (lane + 32 k) + sub) -> out[0, pitch), zero
@@ -512,7 +516,7 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
 // field. Each exact-length 1-D DFT runs as Bluestein's chirp-z transform
 // (Bluestein 1970): with c[n] = exp(-i pi n^2 / N),
 //   X[k] = c[k] sum_n (x[n] c[n]) conj(c[k - n]),
-// a cyclic convolution of length M >= 2 N - 1 (rows 2048, columns col_m):
+// a cyclic convolution of length M >= 2 N - 1 (rows row_m, columns col_m):
 // FFT, multiply by hhat = FFT_M(conj(c), wrapped) / M, inverse FFT. The
 // inverse 2-D DFT is conj(DFT(conj(X))) / (hp w): conjugate on the column
 // pass's load and on the row pass's store. rowbuf (free once the column pass
@@ -522,15 +526,20 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_init_rows(InitArgs a, int to
 // mode 0: forward DFT of padded row yp of the demodulated field -> plane 0.
 // mode 1: last pass of the inverse, rows [pad, pad + h) of plane 1 -> chi3,
 //         x 2 / (hp w) (Fft2d::Inverse's 1 / (hp w), then the init's x2).
-// grid = total padded rows; block 256; dynamic smem 2 x kRowFft float2.
+// grid = total padded rows; block 256; dynamic smem 2 x M float2. M is the
+// geometry's row length (kRowFft, or kFftLong past 1024 active samples);
+// each instantiation takes the rows of its own length.
+template <int M>
 __global__ void __launch_bounds__(256) k_sym_rows(InitArgs a, int mode) {
   extern __shared__ float2 sm_sym[];
   float2* P = sm_sym;
-  float2* Q = P + kRowFft;
+  float2* Q = P + M;
   const int r = blockIdx.x;
   const int f_idx = a.prow_field[r];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
+  if (gd.row_m != M) return;  // uniform per CTA
+  const float2* tw = M == kRowFft ? a.tw_row : a.tw_long;
   const int yp = r - a.prow_first[f_idx];
   if (mode == 1 && (yp < gd.pad || yp >= gd.pad + f.h)) return;  // uniform per CTA
   const float2* chirp = a.khat + gd.sym_row_chirp;
@@ -540,7 +549,7 @@ __global__ void __launch_bounds__(256) k_sym_rows(InitArgs a, int mode) {
   if (mode == 0) {
     const int sy = mirror_row(yp - gd.pad, f.h);
     const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
-    for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) {
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
       float2 v = make_float2(0.f, 0.f);
       if (i < f.w) {
         const float s = S[i];
@@ -551,15 +560,15 @@ __global__ void __launch_bounds__(256) k_sym_rows(InitArgs a, int mode) {
     }
   } else {
     const float2* src = plane1 + (int64_t)yp * f.pitch;
-    for (int i = threadIdx.x; i < kRowFft; i += blockDim.x)
+    for (int i = threadIdx.x; i < M; i += blockDim.x)
       P[i] = i < f.w ? cmul(src[i], __ldg(chirp + i)) : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* spec = fft_stockham<kRowFft, false>(P, Q, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+  float2* spec = fft_stockham<M, false>(P, Q, tw, threadIdx.x, blockDim.x, BlockSync());
   float2* oth = spec == P ? Q : P;
-  for (int i = threadIdx.x; i < kRowFft; i += blockDim.x) oth[i] = cmul(spec[i], __ldg(hh + i));
+  for (int i = threadIdx.x; i < M; i += blockDim.x) oth[i] = cmul(spec[i], __ldg(hh + i));
   __syncthreads();
-  float2* res = fft_stockham<kRowFft, true>(oth, spec, a.tw_row, threadIdx.x, blockDim.x, BlockSync());
+  float2* res = fft_stockham<M, true>(oth, spec, tw, threadIdx.x, blockDim.x, BlockSync());
   if (mode == 0) {
     float2* dst = plane0 + (int64_t)yp * f.pitch;
     for (int i = threadIdx.x; i < f.pitch; i += blockDim.x)
@@ -617,6 +626,7 @@ __global__ void __launch_bounds__(kColThreads, 3) k_sym_cols(InitArgs a, int mod
   const int f_idx = a.cgrp_field[gidx];
   const FieldDesc f = a.fields[f_idx];
   const GeomDesc gd = a.geoms[f.geom];
+  if (gd.col_m == kFftLong) return;  // k_sym_cols_long (uniform per CTA)
   if (gd.col_m == kColFftWide) {
     const int x0 = (gidx - a.cgrp_first[f_idx]) * kColGroupWide;
     const int pair = warp >> 1;
@@ -657,6 +667,150 @@ __global__ void __launch_bounds__(256) k_sym_certify(InitArgs a) {
     }
     dst[x] = v;
   }
+}
+
+// ---- long rows / columns (kFftLong) -----------------------------------------
+// Planes past the register transforms' lengths (more than 1024 active
+// samples, or more than 1024 padded lines) run their cyclic convolutions at
+// length kFftLong = 4096 through the shared-memory Stockham FFT
+// (fft_stockham: six radix-4 stages, a block barrier after each), one CTA of
+// 256 threads per padded row or per column, with the same kernel spectra,
+// layouts and outputs as the register kernels. These kernels run over the
+// same padded-row / column-group grids and take only the rows / columns of
+// geometries with the long length (the register kernels skip those); a long
+// column geometry has one column per group.
+constexpr int kLongThreads = 256;
+constexpr int kLongColSmem = 2 * kFftLong * (int)sizeof(float2);  // ping-pong: 64 KiB
+constexpr int kLongRowSmem = 3 * kFftLong * (int)sizeof(float2);  // + the row's spectrum
+
+// P holds x (zero past the data, barrier taken) -> the cyclic convolution of
+// x with the kernel whose spectrum (1/M folded in) is kh; returns the buffer
+// (P or Q) holding it, barrier taken.
+__device__ __forceinline__ float2* long_conv(float2* P, float2* Q, const float2* __restrict__ kh,
+                                             const float2* __restrict__ tw) {
+  float2* spec = fft_stockham<kFftLong, false>(P, Q, tw, threadIdx.x, blockDim.x, BlockSync());
+  for (int i = threadIdx.x; i < kFftLong; i += blockDim.x) spec[i] = cmul(spec[i], __ldg(kh + i));
+  __syncthreads();
+  return fft_stockham<kFftLong, true>(spec, spec == P ? Q : P, tw, threadIdx.x, blockDim.x,
+                                      BlockSync());
+}
+
+// grid = total padded rows; block 256; dynamic smem kLongRowSmem.
+__global__ void __launch_bounds__(kLongThreads) k_init_rows_long(InitArgs a) {
+  extern __shared__ float2 sm_long[];
+  float2* P = sm_long;
+  float2* Q = P + kFftLong;
+  float2* spec = Q + kFftLong;
+  const int r = blockIdx.x;
+  const int f_idx = a.prow_field[r];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  if (gd.row_m != kFftLong) return;  // uniform per CTA
+  const int yp = r - a.prow_first[f_idx];
+  const float2 z = make_float2(0.f, 0.f);
+  // res -> out[0, pitch), zero beyond the active width; the barrier frees P / Q
+  auto store_row = [&](const float2* res, float2* out) {
+    for (int i = threadIdx.x; i < f.pitch; i += blockDim.x) out[i] = i < f.w ? res[i] : z;
+    __syncthreads();
+  };
+  if (a.adj_in) {
+    // adjoint mode: each variant filters its own input row
+    for (int var = 0; var < 2; ++var) {
+      const int64_t row = a.rowbuf_off[f_idx] + ((int64_t)var * gd.hp + yp) * f.pitch;
+      const float2* in = a.adj_in + row;
+      for (int i = threadIdx.x; i < kFftLong; i += blockDim.x) P[i] = i < f.w ? in[i] : z;
+      __syncthreads();
+      const float2* res =
+          long_conv(P, Q, a.khat + gd.khat_row_off + var * kFftLong, a.tw_long);
+      store_row(res, a.rowbuf + row);
+    }
+    return;
+  }
+  const int sy = mirror_row(yp - gd.pad, f.h);
+  const float* S = a.S + f.px_off + (int64_t)sy * f.pitch;
+  for (int i = threadIdx.x; i < kFftLong; i += blockDim.x) {
+    float2 v = z;
+    if (i < f.w) {
+      const float s = S[i];
+      const float2 c = carrier_at(a, f, sy, i);
+      v = make_float2(s * c.x, -s * c.y);  // S * conj(c)
+    }
+    P[i] = v;
+  }
+  __syncthreads();
+  const float2* X = fft_stockham<kFftLong, false>(P, Q, a.tw_long, threadIdx.x, blockDim.x,
+                                                  BlockSync());
+  for (int i = threadIdx.x; i < kFftLong; i += blockDim.x) spec[i] = X[i];
+  __syncthreads();
+  for (int var = 0; var < 2; ++var) {
+    const float2* kh = a.khat + gd.khat_row_off + var * kFftLong;
+    for (int i = threadIdx.x; i < kFftLong; i += blockDim.x) P[i] = cmul(spec[i], __ldg(kh + i));
+    __syncthreads();
+    const float2* res = fft_stockham<kFftLong, true>(P, Q, a.tw_long, threadIdx.x, blockDim.x,
+                                                     BlockSync());
+    store_row(res, a.rowbuf + a.rowbuf_off[f_idx] + ((int64_t)var * gd.hp + yp) * f.pitch);
+  }
+}
+
+// grid = total column groups; block 256; dynamic smem kLongColSmem. Column
+// x of a long geometry: rows [0, hp) of each row-filtered variant -> chi1 /
+// chi2 rows [pad, pad + h) (adjoint mode: all hp rows into adj_out).
+__global__ void __launch_bounds__(kLongThreads) k_init_cols_long(InitArgs a) {
+  extern __shared__ float2 sm_long[];
+  float2* P = sm_long;
+  float2* Q = P + kFftLong;
+  const int gidx = blockIdx.x;
+  const int f_idx = a.cgrp_field[gidx];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  if (gd.col_m != kFftLong) return;  // uniform per CTA
+  const int x = gidx - a.cgrp_first[f_idx];
+  for (int v = 0; v < 2; ++v) {
+    const int64_t plane = a.rowbuf_off[f_idx] + (int64_t)v * gd.hp * f.pitch + x;
+    const float2* src = a.rowbuf + plane;
+    for (int i = threadIdx.x; i < kFftLong; i += blockDim.x)
+      P[i] = i < gd.hp ? src[(int64_t)i * f.pitch] : make_float2(0.f, 0.f);
+    __syncthreads();
+    const float2* res = long_conv(P, Q, a.khat + gd.khat_col_off + v * kFftLong, a.tw_long);
+    if (a.adj_out) {
+      float2* dst = a.adj_out + plane;
+      for (int y = threadIdx.x; y < gd.hp; y += blockDim.x) dst[(int64_t)y * f.pitch] = res[y];
+    } else {
+      float2* dst = (v == 0 ? a.chi1 : a.chi2) + f.px_off + x;
+      for (int y = threadIdx.x; y < f.h; y += blockDim.x)
+        dst[(int64_t)y * f.pitch] = res[y + gd.pad];
+    }
+    __syncthreads();
+  }
+}
+
+// The symmetry variant's column DFTs of a long geometry (sym_cols_body at
+// length kFftLong): grid = total column groups; block 256; smem kLongColSmem.
+__global__ void __launch_bounds__(kLongThreads) k_sym_cols_long(InitArgs a, int mode) {
+  extern __shared__ float2 sm_long[];
+  float2* P = sm_long;
+  float2* Q = P + kFftLong;
+  const int gidx = blockIdx.x;
+  const int f_idx = a.cgrp_field[gidx];
+  const FieldDesc f = a.fields[f_idx];
+  const GeomDesc gd = a.geoms[f.geom];
+  if (gd.col_m != kFftLong) return;  // uniform per CTA
+  const int x = gidx - a.cgrp_first[f_idx];
+  const float2* chirp = a.khat + gd.sym_col_chirp;
+  float2* plane = a.rowbuf + a.rowbuf_off[f_idx] + (mode ? (int64_t)gd.hp * f.pitch : 0) + x;
+  for (int i = threadIdx.x; i < kFftLong; i += blockDim.x) {
+    float2 v = make_float2(0.f, 0.f);
+    if (i < gd.hp) {
+      v = plane[(int64_t)i * f.pitch];
+      if (mode) v.y = -v.y;
+      v = cmul(v, __ldg(chirp + i));
+    }
+    P[i] = v;
+  }
+  __syncthreads();
+  const float2* res = long_conv(P, Q, a.khat + gd.sym_col_hhat, a.tw_long);
+  for (int i = threadIdx.x; i < gd.hp; i += blockDim.x)
+    plane[(int64_t)i * f.pitch] = cmul(res[i], __ldg(chirp + i));
 }
 
 // ---- blend -----------------------------------------------------------------
@@ -857,6 +1011,14 @@ static void configure_init_kernels_now() {
   cudaFuncSetAttribute(k_init_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowSmem);
   cudaFuncSetAttribute(k_init_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
   cudaFuncSetAttribute(k_sym_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kColSmem);
+  cudaFuncSetAttribute(k_sym_rows<kFftLong>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kLongColSmem);
+  cudaFuncSetAttribute(k_init_rows_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kLongRowSmem);
+  cudaFuncSetAttribute(k_init_cols_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kLongColSmem);
+  cudaFuncSetAttribute(k_sym_cols_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kLongColSmem);
   cudaFuncSetAttribute(k_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, kAnisoSmem);
 }
 
@@ -866,21 +1028,40 @@ void configure_init_kernels() {
   once(configure_init_kernels_now);
 }
 
-void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
-                 cudaStream_t st) {
-  const int col_smem = kColSmem;
-  configure_init_kernels();
-  if (total_prows > 0)
+// The row and column filter passes: the register kernels, then (when the
+// batch holds a long geometry) the shared-memory ones over the same grids.
+static void launch_filter_passes(const InitArgs& a, int total_prows, int total_cgroups,
+                                 cudaStream_t st) {
+  if (total_prows > 0) {
     k_init_rows<<<(total_prows + kRowsPerCta - 1) / kRowsPerCta, kRowThreads, kRowSmem, st>>>(
         a, total_prows);
-  if (total_cgroups > 0) k_init_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a);
+    if (a.long_rows) k_init_rows_long<<<total_prows, kLongThreads, kLongRowSmem, st>>>(a);
+  }
+  if (total_cgroups > 0) {
+    k_init_cols<<<total_cgroups, kColThreads, kColSmem, st>>>(a);
+    if (a.long_cols) k_init_cols_long<<<total_cgroups, kLongThreads, kLongColSmem, st>>>(a);
+  }
+}
+
+void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int total_btiles,
+                 cudaStream_t st) {
+  configure_init_kernels();
+  launch_filter_passes(a, total_prows, total_cgroups, st);
   if (a.chi3 && total_prows > 0 && total_cgroups > 0) {
     const int sym_smem = 2 * kRowFft * sizeof(float2);
-    k_sym_rows<<<total_prows, 256, sym_smem, st>>>(a, 0);
-    k_sym_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a, 0);
+    auto sym_rows = [&](int mode) {
+      k_sym_rows<kRowFft><<<total_prows, 256, sym_smem, st>>>(a, mode);
+      if (a.long_rows) k_sym_rows<kFftLong><<<total_prows, 256, kLongColSmem, st>>>(a, mode);
+    };
+    auto sym_cols = [&](int mode) {
+      k_sym_cols<<<total_cgroups, kColThreads, kColSmem, st>>>(a, mode);
+      if (a.long_cols) k_sym_cols_long<<<total_cgroups, kLongThreads, kLongColSmem, st>>>(a, mode);
+    };
+    sym_rows(0);
+    sym_cols(0);
     k_sym_certify<<<total_prows, 256, 0, st>>>(a);
-    k_sym_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a, 1);
-    k_sym_rows<<<total_prows, 256, sym_smem, st>>>(a, 1);
+    sym_cols(1);
+    sym_rows(1);
   }
   if (total_btiles > 0) k_init_blend<<<total_btiles, 256, 0, st>>>(a);
 }
@@ -888,11 +1069,7 @@ void launch_init(const InitArgs& a, int total_prows, int total_cgroups, int tota
 void launch_init_filter_adjoint(const InitArgs& a, int total_prows, int total_cgroups,
                                 cudaStream_t st) {
   configure_init_kernels();
-  const int col_smem = kColSmem;
-  if (total_prows > 0)
-    k_init_rows<<<(total_prows + kRowsPerCta - 1) / kRowsPerCta, kRowThreads, kRowSmem, st>>>(
-        a, total_prows);
-  if (total_cgroups > 0) k_init_cols<<<total_cgroups, kColThreads, col_smem, st>>>(a);
+  launch_filter_passes(a, total_prows, total_cgroups, st);
 }
 
 void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStream_t st) {
@@ -902,7 +1079,9 @@ void launch_aniso(FieldDesc* d_fields, int n_fields, const float2* chi0, cudaStr
 }
 
 int aniso_max_samples() { return kAnisoMax; }
-int init_col_group(int col_m) { return col_m == kColFftWide ? kColGroupWide : kColGroup; }
+int init_col_group(int col_m) {
+  return col_m == kFftLong ? 1 : col_m == kColFftWide ? kColGroupWide : kColGroup;
+}
 int init_blend_tile() { return kBT; }
 
 }  // namespace hvdg

@@ -17,6 +17,9 @@ struct InitArgs {
   const float2* khat;          // kernel spectra (row / column, 2 variants each)
   const float2* tw_row;        // exp(-2 pi i k / kRowFft)
   const float2* tw_col;        // exp(-2 pi i k / kColFft) (the wide columns use tw_row)
+  const float2* tw_long = nullptr;  // exp(-2 pi i k / kFftLong)
+  int long_rows = 0;           // some geometry of the batch has row_m == kFftLong
+  int long_cols = 0;           // some geometry of the batch has col_m == kFftLong
   float2* rowbuf;              // row-filtered variants: per field 2 x hp x pitch
   const int64_t* rowbuf_off;   // per field offset into rowbuf (float2)
   float2* chi1;                // variant outputs (pitched like the planes)

@@ -155,6 +155,7 @@ extern "C" hvdg_status hvdg_holographic_init_noalloc(const float* s, const float
   gd.pad = pad;
   gd.khat_row_off = 0;
   gd.khat_col_off = 2 * hvdg::kRowFft;
+  gd.row_m = hvdg::kRowFft;
   gd.col_m = hvdg::kColFft;
   gd.sym_row_chirp = gd.sym_row_hhat = gd.sym_col_chirp = gd.sym_col_hhat = -1;
   gd.sym_gx = gd.sym_gy = -1;

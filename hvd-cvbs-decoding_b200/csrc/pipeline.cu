@@ -14,11 +14,13 @@
 namespace hvdg_pipe {
 
 // Device-path limits of one solve plane of w x h (documented in
-// include/hvdg.h): the row / column cyclic-convolution lengths of the init
-// and the auto-aniso sample buffer.
-hvdg_status check_plane(int w, int h, bool vsw, int col_max) {
+// include/hvdg.h): the longest row / column cyclic convolution of the init
+// (kFftLong: up to 2048 active samples, 2048 padded lines) and the
+// auto-aniso sample buffer.
+hvdg_status check_plane(int w, int h, bool vsw) {
   const int pad = std::min(hvdg::kInitPad, h - 1);
-  if (2 * w - 1 > hvdg::kRowFft || 2 * (h + 2 * pad) - 1 > col_max) return HVDG_ERR_UNSUPPORTED;
+  if (2 * w - 1 > hvdg::kFftLong || 2 * (h + 2 * pad) - 1 > hvdg::kFftLong)
+    return HVDG_ERR_UNSUPPORTED;
   const int group = vsw ? 4 : 2;
   const int64_t n = (int64_t)((h / group) / 2) * ((w + 1) / 3);
   if (n > hvdg::aniso_max_samples()) return HVDG_ERR_UNSUPPORTED;
@@ -44,7 +46,7 @@ hvdg_status check_geometry(const hvdg_geometry* g) {
   if (g->field_height > hvdg::kMaxLines) return HVDG_ERR_UNSUPPORTED;
   const int w = g->active_video_end - g->active_video_start;
   const int h = lal - g->first_active_field_line;
-  const hvdg_status st = check_plane(w, h, uses_vswitch(*g), hvdg::kColFft);
+  const hvdg_status st = check_plane(w, h, uses_vswitch(*g));
   if (st != HVDG_OK) return st;
   if (g->colour_burst_end - g->colour_burst_start > 64 + 3) return HVDG_ERR_UNSUPPORTED;
   return HVDG_OK;
@@ -99,7 +101,10 @@ GeomTables make_geom_tables(const hvdg_geometry& g) {
   t.h = last_active_line(g) - g.first_active_field_line;
   t.pad = std::min(hvdg::kInitPad, t.h > 1 ? t.h - 1 : 0);
   t.hp = t.h + 2 * t.pad;
-  t.col_m = 2 * t.hp - 1 <= hvdg::kColFft ? hvdg::kColFft : hvdg::kColFftWide;
+  t.row_m = 2 * t.w - 1 <= hvdg::kRowFft ? hvdg::kRowFft : hvdg::kFftLong;
+  t.col_m = 2 * t.hp - 1 <= hvdg::kColFft       ? hvdg::kColFft
+            : 2 * t.hp - 1 <= hvdg::kColFftWide ? hvdg::kColFftWide
+                                                : hvdg::kFftLong;
   for (int v = 0; v < 2; ++v) {
     std::vector<double> gx(t.w), gy(t.hp);
     const double cx = kVariants[v][0] * 1.0e6;
@@ -112,7 +117,7 @@ GeomTables make_geom_tables(const hvdg_geometry& g) {
       const double r = fftfreq(i, t.hp, 1.0) / cy;
       gy[i] = std::exp(-0.5 * r * r);
     }
-    for (const cd& c : kernel_spectrum(gx, hvdg::kRowFft, 1.0))
+    for (const cd& c : kernel_spectrum(gx, t.row_m, 1.0))
       t.khat_row.push_back(make_float2((float)c.real(), (float)c.imag()));
     // x2 of the init (holographic_init.cpp:247-251) folded into the column pass
     for (const cd& c : kernel_spectrum(gy, t.col_m, 2.0))
@@ -178,7 +183,7 @@ void bluestein_tables(int N, int M, std::vector<float2>* out) {
 // frequencies, float cutoffs, float exp.
 void make_sym_tables(GeomTables& t, const hvdg_geometry& g) {
   t.sym.clear();
-  bluestein_tables(t.w, hvdg::kRowFft, &t.sym);
+  bluestein_tables(t.w, t.row_m, &t.sym);
   bluestein_tables(t.hp, t.col_m, &t.sym);
   auto freq = [](int i, int n, double d) {
     const double inv = 1.0 / ((double)n * d);
@@ -309,7 +314,8 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     gd.hp = t.hp;
     gd.pad = t.pad;
     gd.khat_row_off = nkhat;
-    nkhat += 2 * hvdg::kRowFft;
+    gd.row_m = t.row_m;
+    nkhat += 2 * t.row_m;
     gd.khat_col_off = nkhat;
     gd.col_m = t.col_m;
     nkhat += 2 * t.col_m;
@@ -318,7 +324,7 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
     if (cfg->symmetry_variant) {
       gd.sym_row_chirp = nkhat;
       gd.sym_row_hhat = gd.sym_row_chirp + t.w;
-      gd.sym_col_chirp = gd.sym_row_hhat + hvdg::kRowFft;
+      gd.sym_col_chirp = gd.sym_row_hhat + t.row_m;
       gd.sym_col_hhat = gd.sym_col_chirp + t.hp;
       gd.sym_gx = gd.sym_col_hhat + t.col_m;
       gd.sym_gy = gd.sym_gx + t.w;
@@ -475,6 +481,7 @@ hvdg_status plan_batch(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hvdg
   L.o_khat = take(sizeof(float2) * nkhat);
   L.o_twr = take(sizeof(float2) * hvdg::kRowFft);
   L.o_twc = take(sizeof(float2) * hvdg::kColFft);
+  L.o_twl = take(sizeof(float2) * hvdg::kFftLong);
   L.o_amp = take(sizeof(float) * n);
   // index tables: itab | pitches | crop rows (int4) | px_offs (int64) | rowbuf offs (int64)
   L.o_itab = take(sizeof(int) * (b.itab.size() + b.pitches.size()) + sizeof(int4) * b.crop_rows.size() +
@@ -606,9 +613,11 @@ hvdg_status stage_upload(hvdg_ctx* ctx, const hvdg_field_in* in, int n, const hv
     }
     put(L.o_colph, col.data(), sizeof(float2) * col.size());
     put(L.o_khat, kh.data(), sizeof(float2) * kh.size());
-    static const std::vector<float2> twr = twiddles(hvdg::kRowFft), twc = twiddles(hvdg::kColFft);
+    static const std::vector<float2> twr = twiddles(hvdg::kRowFft), twc = twiddles(hvdg::kColFft),
+                                     twl = twiddles(hvdg::kFftLong);
     put(L.o_twr, twr.data(), sizeof(float2) * twr.size());
     put(L.o_twc, twc.data(), sizeof(float2) * twc.size());
+    put(L.o_twl, twl.data(), sizeof(float2) * twl.size());
   }
   size_t it = L.o_itab;
   S.it_itab = it;
@@ -655,6 +664,11 @@ hvdg::InitArgs init_args(hvdg_ctx* ctx, const Staged& S) {
   ia.khat = at<float2>(ctx, L.o_khat);
   ia.tw_row = at<float2>(ctx, L.o_twr);
   ia.tw_col = at<float2>(ctx, L.o_twc);
+  ia.tw_long = at<float2>(ctx, L.o_twl);
+  for (const GeomDesc& gd : b.geoms) {
+    ia.long_rows |= gd.row_m == hvdg::kFftLong;
+    ia.long_cols |= gd.col_m == hvdg::kFftLong;
+  }
   ia.rowbuf = at<float2>(ctx, L.o_rowbuf);
   ia.rowbuf_off = at<int64_t>(ctx, S.it_rbo);
   ia.chi1 = at<float2>(ctx, L.o_G0);

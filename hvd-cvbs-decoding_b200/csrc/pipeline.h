@@ -92,12 +92,13 @@ inline float nominal_burst(const hvdg_geometry& g) {
 
 struct GeomTables {
   int w, h, hp, pad;
-  int col_m;                     // column convolution length (kColFft or kColFftWide)
-  std::vector<float2> khat_row;  // 2 * kRowFft
+  int row_m;                     // row convolution length (kRowFft or kFftLong)
+  int col_m;                     // column convolution length (kColFft, kColFftWide or kFftLong)
+  std::vector<float2> khat_row;  // 2 * row_m
   std::vector<float2> khat_col;  // 2 * col_m
   std::vector<float2> col_phasor;
   // symmetry variant (built on first use): row chirp (w) | row chirp-filter
-  // spectrum (kRowFft) | column chirp (hp) | column filter spectrum (col_m) |
+  // spectrum (row_m) | column chirp (hp) | column filter spectrum (col_m) |
   // gx (w) | gy (hp), the last two in .x
   bool sym_ready = false;
   std::vector<float2> sym;
@@ -182,7 +183,8 @@ struct Layout {
   // byte offsets into the arena
   size_t o_raw, o_prep, o_fields, o_geoms, o_ctl, o_units, o_partials, o_done, o_arrive,
       o_flags, o_queue, o_lineph, o_theta, o_theta64, o_vsw, o_colph, o_khat, o_twr, o_twc,
-      o_S, o_Y, o_X0, o_X1, o_G0, o_G1, o_D0, o_D1, o_Q0, o_Q1, o_W, o_rowbuf, o_itab, o_amp;
+      o_twl, o_S, o_Y, o_X0, o_X1, o_G0, o_G1, o_D0, o_D1, o_Q0, o_Q1, o_W, o_rowbuf, o_itab,
+      o_amp;
   size_t o_W2 = 0;   // (wd1, wd2) plane, only when a field has the oriented prior
   size_t o_gpart = 0, o_garrive = 0;  // solver unit-group partials and arrival counters
   bool has_diag = false;
@@ -268,7 +270,7 @@ struct SelBox {
   bool valid = false;                     // an invalid single box: run full 3-D
 };
 
-hvdg_status check_plane(int w, int h, bool vsw, int col_max);
+hvdg_status check_plane(int w, int h, bool vsw);
 hvdg_status check_geometry(const hvdg_geometry* g);
 double fftfreq(int i, int n, double d);
 std::vector<cd> kernel_spectrum(const std::vector<double>& mask, int M, double scale);

@@ -466,9 +466,10 @@ hvdg_status hvdg_decode_fields_adjoint(hvdg_ctx* ctx, const hvdg_field_in* field
  * buffers, as for hvdg_holographic_init; work runs on the legacy default
  * stream of the current device and the call returns when it is done.
  * Limits: geometry is checked as for hvdg_holographic_init (same statuses);
- * fields past the init's convolution lengths (more than 1024 active samples,
- * or more than 480 active lines) are rejected with HVDG_ERR_UNSUPPORTED, and
- * every field within them fits the array. The first call on each device
+ * fields past the register transforms' lengths (more than 1024 active
+ * samples, or more than 480 active lines), which hvdg_holographic_init takes
+ * through its shared-memory transforms, are rejected here with
+ * HVDG_ERR_UNSUPPORTED, and every field within them fits the array. The first call on each device
  * looks up the array's device address and keeps it for the life of the
  * process: make that first call before any stream capture, and do not
  * cudaDeviceReset that device between calls. All calls share the one array

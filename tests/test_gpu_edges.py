@@ -1,9 +1,11 @@
 """Edge cases of the 2-D decode at the boundary, against the FP64 oracle:
 ragged geometries (odd active width and start, a line count that no solver
-band divides), a tiny plane (8 x 16), the largest planes the device path
-takes (active width 1024: row convolution 2047 <= 2048; 480 active lines:
-padded 512, column convolution 1023 <= 1024) and one past each limit
-(HVDG_ERR_UNSUPPORTED), non-finite samples (HVDG_ERR_NONFINITE_INPUT, the
+band divides), a tiny plane (8 x 16), the largest planes of the init's
+register transforms (active width 1024: row convolution 2047 <= 2048; 480
+active lines: padded 512, column convolution 1023 <= 1024) and one past
+each, which the shared-memory transforms take (test_gpu_long_planes.py
+covers those and the refusals past them), non-finite samples
+(HVDG_ERR_NONFINITE_INPUT, the
 context stays usable), the empty batch, and caller output planes that
 start off any vector boundary."""
 import ctypes as C
@@ -49,7 +51,7 @@ def test_tiny_plane(ctx):
     _vs_oracle(ctx, g, _cabi.STD_NTSC, 72)
 
 
-def test_largest_planes_and_one_past(ctx):
+def test_largest_register_planes_and_one_past(ctx):
     wide = _cabi.default_geometry(_cabi.STD_PAL)
     wide.active_video_start, wide.active_video_end = 100, 1124      # width 1024
     _vs_oracle(ctx, wide, _cabi.STD_PAL, 73)
@@ -58,12 +60,9 @@ def test_largest_planes_and_one_past(ctx):
     tall.first_active_field_line, tall.last_active_field_line = 10, 490   # 480 lines
     tall.active_video_start, tall.active_video_end = 134, 390
     _vs_oracle(ctx, tall, _cabi.STD_NTSC, 74)
-    for g, edit in ((wide, dict(active_video_end=1125)), (tall, dict(last_active_field_line=491))):
-        bad = _cabi.geometry_copy(g, **edit)
-        f = synth.make_field(75, g.standard, 0.5, geometry=g)
-        with pytest.raises(api.HvdgError) as e:
-            ctx.decode_fields([api.Field(f.samples, bad, parity=0)], _cfg())
-        assert e.value.status == _cabi.ERR_UNSUPPORTED
+    # one past each: row length 4096, column length 2048
+    _vs_oracle(ctx, _cabi.geometry_copy(wide, active_video_end=1125), _cabi.STD_PAL, 75)
+    _vs_oracle(ctx, _cabi.geometry_copy(tall, last_active_field_line=491), _cabi.STD_NTSC, 75)
 
 
 def test_nonfinite_input_and_empty_batch(ctx):

@@ -232,8 +232,9 @@ def test_frame_buffer_lossless_split(ctx):
 def test_frame_buffer_error_statuses(ctx):
     """Statuses at the boundary, as the reference's empty-result convention
     maps onto them: bad frame parameters -> BAD_GEOMETRY, a woven plane
-    beyond the device-path limits -> UNSUPPORTED, n = 0 -> OK, nothing
-    decoded; the context stays usable."""
+    beyond the device-path limits -> UNSUPPORTED (a PAL frame 1100 samples
+    wide is within them, on the long-row transforms, and matches the
+    reference), n = 0 -> OK, nothing decoded; the context stays usable."""
     frames, _ = synth.make_frames(97, _cabi.STD_NTSC, 1, noise_sigma=0.5)
     fp = api.frame_params(_cabi.STD_NTSC)
     cfg = _cfg()
@@ -249,9 +250,16 @@ def test_frame_buffer_error_statuses(ctx):
     assert out["luma"].shape == frames[0].shape
     pal_frames, _ = synth.make_frames(98, _cabi.STD_PAL, 1, noise_sigma=0.5)
     wide = api.frame_params(_cabi.STD_PAL)
-    wide.active_video_start, wide.active_video_end = 10, 1110  # 2 w - 1 > 2048
+    wide.active_video_start, wide.active_video_end = 10, 1110  # 2 w - 1 > 2048: rows of 4096
+    out = ctx.decode_frame_buffer(pal_frames[0], wide, cfg)
+    ref = _ref()
+    _compare(out, ref.decode_frame_buffer(pal_frames[0], wide, cfg), "wide PAL frame", pal=True)
+    past = api.frame_params(_cabi.STD_NTSC)
+    past.frame_width = 2100
+    past.active_video_start, past.active_video_end = 20, 2069  # 2049 samples: 2 w - 1 > 4096
+    blank = np.full((past.frame_height, past.frame_width), 16384, np.uint16)
     with pytest.raises(api.HvdgError) as e:
-        ctx.decode_frame_buffer(pal_frames[0], wide, cfg)
+        ctx.decode_frame_buffer(blank, past, cfg)
     assert e.value.status == _cabi.ERR_UNSUPPORTED
     assert ctx.decode_frame_buffers([], fp, cfg) == []
     ok = ctx.decode_frame_buffer(frames[0], fp, cfg)
