@@ -10,11 +10,13 @@
 //
 // The array is HVDG_NOALLOC_SCRATCH_BYTES (32 MiB). It is part of the
 // module, so every GPU that loads this library holds it until the process
-// exits, whether or not the entry point is ever called. The geometries the
-// init accepts at all (row convolution 2048 points: at most 1024 active
-// samples; column convolution 1024 points: at most 480 active lines) need at
-// most ~24 MiB of it (kWorstLayout below), so the array's size never limits
-// a field the context path takes. Host code cannot use the symbol itself as
+// exits, whether or not the entry point is ever called. This entry runs the
+// init's register transforms only (row convolution 2048 points: at most
+// 1024 active samples; column convolution 1024 points: at most 480 active
+// lines; larger fields, which the context path takes through its
+// shared-memory transforms, are refused here); those fields need at most
+// ~24 MiB of it (kWorstLayout below), so the array's size never limits a
+// field this entry takes. Host code cannot use the symbol itself as
 // a device address; the first call on each device looks the address up with
 // cudaGetSymbolAddress (with that device current) and caches it for the
 // life of the process, so that first call should come before any stream
@@ -69,9 +71,9 @@ hvdg_status scratch_address(void** out) {
 
 constexpr size_t up(size_t x) { return (x + 255) / 256 * 256; }
 
-// The layout below at the largest plane the init accepts (w <= 1024 active
-// samples, h + 2 pad <= 512 padded lines), tables included: the scratch
-// array holds every accepted field.
+// The layout below at the largest plane this entry accepts (w <= 1024
+// active samples, h + 2 pad <= 512 padded lines), tables included: the
+// scratch array holds every accepted field.
 constexpr size_t kMaxW = hvdg::kRowFft / 2, kMaxHp = (hvdg::kColFft + 1) / 2;
 constexpr size_t kWorstLayout =
     up(sizeof(hvdg::FieldDesc)) + up(sizeof(hvdg::GeomDesc)) + up(16 * kMaxHp) +

@@ -440,3 +440,36 @@ def test_oracle_adaptive_strength_matches_reference(std, seed):
     assert amb > 0.0
     assert np.float32(amb) == diag[1]
     assert np.float32(strength) == diag[0]
+
+
+@pytest.mark.parametrize("case", ["pal_full_line", "tall1000"])
+def test_oracle_long_planes_match_reference(case):
+    """Planes past the device init's register transforms (a whole 1135-sample
+    PAL line; 1000 lines, padded 1032): the oracle's init (plain and
+    symmetry variant) and 2-D decode against the compiled reference, whose
+    FFTs run at the plane's own size (holographic_init.cpp:214-222)."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    from hvdg import api, synth
+    if case == "pal_full_line":
+        g = _cabi.geometry_copy(_cabi.default_geometry(_cabi.STD_PAL), active_video_start=0,
+                                active_video_end=1135, first_active_field_line=22,
+                                last_active_field_line=118)
+    else:
+        g = _cabi.geometry_copy(_cabi.default_geometry(_cabi.STD_NTSC), field_height=1020,
+                                first_active_field_line=10, last_active_field_line=1010,
+                                active_video_start=134, active_video_end=230)
+    f = synth.make_field(251, g.standard, noise_sigma=0.5, geometry=g)
+    cfg = api.default_config(irls_outer=3, cg_iterations=60, fast=0, cg_tol=1e-6,
+                             temporal_strength=-1.0)
+    ire = synth.to_ire(f.samples)
+    rs, rc = ref.prepare_field(ire, g, cfg, 0)
+    for sym in (0, 1):
+        y0, chi0 = O.holographic_init(rs.astype(np.float64), rc.astype(np.complex128), g,
+                                      symmetry_variant=bool(sym))
+        ry0, rchi0 = ref.holographic_init(rs, rc, g, api.default_config(symmetry_variant=sym))
+        assert np.abs(chi0 - rchi0).max() < 1e-4 and np.abs(y0 - ry0).max() < 1e-4
+    (yo, co, _), = O.decode_fields_2d([ire], [0], g, cfg)
+    (yr,), (cr,) = ref.decode_fields([ire], [0], [g], [cfg], across_fields=False)
+    assert np.abs(yo - yr).max() < 2e-2 and np.abs(co - cr).max() < 2e-2
