@@ -75,14 +75,14 @@ def test_variational_refine_entry(ctx, std, diag_prior):
 def test_variational_refine_entry_refuses_bad_geometry(ctx):
     """A chi0 plane whose geometry the refine cannot take is refused with a
     status before any plane is read: the active width above the
-    1024-sample limit (arrays sized to the refused geometry)."""
+    2048-sample limit (arrays sized to the refused geometry)."""
     g = _cabi.default_geometry(_cabi.STD_NTSC)
-    g.field_width = g.active_video_start + 1100 + 8
-    g.active_video_end = g.active_video_start + 1100
+    g.field_width = g.active_video_start + 2049 + 8
+    g.active_video_end = g.active_video_start + 2049
     h = g.last_active_line - g.first_active_field_line
-    s = np.zeros((h, 1100), np.float32)
+    s = np.zeros((h, 2049), np.float32)
     th = np.zeros(h, np.float32)
     sw = np.zeros(h, np.int8)
     with pytest.raises(RuntimeError, match="hvdg_variational_refine"):
-        ctx.variational_refine(s, th, sw, np.zeros((h, 1100), np.complex64), g,
+        ctx.variational_refine(s, th, sw, np.zeros((h, 2049), np.complex64), g,
                                api.default_config(temporal_strength=-1.0))
