@@ -9,7 +9,8 @@ plane's own size (holographic_init.cpp:214-222), which the oracle restates.
 Cases: a full PAL line (1135 samples), the widest plane (2048 samples), a
 600-line and a 1000-line field, the init alone (and its symmetry variant)
 on long rows and long columns, one batch mixing long and standard
-geometries, the decode adjoint on a long-row field, and one past each limit
+geometries, the decode adjoint on a long-row field, the 3-D field window on
+long rows against the compiled reference, and one past each limit
 (HVDG_ERR_UNSUPPORTED)."""
 import numpy as np
 import pytest
@@ -138,6 +139,38 @@ def test_long_row_adjoint_vs_fp64_oracle(ctx):
     rel = np.linalg.norm(got - want) / np.linalg.norm(want)
     print("sample gradient rel L2", rel)
     assert rel < 1e-3
+
+
+def test_long_row_window_vs_reference(ctx):
+    """The temporal (3-D) field window -- motion search, neighbour terms,
+    envelope gate -- on PAL fields 1140 samples wide (long-row init) against
+    the compiled reference on the same fields: PSNR against ground truth
+    within 0.05 dB of the reference's, field by field."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference engine not built")
+    g = _cabi.geometry_copy(_cabi.default_geometry(_cabi.STD_PAL), field_width=1300,
+                            active_video_start=150, active_video_end=1290)
+    nf = 6
+    sc = synth.make_scene(261, _cabi.STD_PAL, n_rects=4, geometry=g)
+    seq = [synth.make_field(261, _cabi.STD_PAL, 1.0, field_index=j, parity=j % 2, scene=sc,
+                            theta_base=0.3, geometry=g) for j in range(nf)]
+    cfg = api.default_config(irls_outer=2, cg_iterations=16, fast=1, cg_tol=1e-6,
+                             temporal_strength=0.5, passes=1, nr_anchor=0.0, coherence_gate=0.0,
+                             trajectory_fit=0)
+    outs = ctx.decode_field_window([api.Field(f.samples, g, parity=f.parity) for f in seq], cfg)
+    ys, cs, _ = ref.decode_field_window([synth.to_ire(f.samples) for f in seq],
+                                        [f.parity for f in seq], g, cfg)
+
+    def psnr(a, b):
+        d = np.asarray(a, np.complex128) - np.asarray(b, np.complex128)
+        return 10 * np.log10(100.0 ** 2 / np.mean(np.abs(d) ** 2))
+
+    for j in range(nf):
+        pg, pr = psnr(outs[j].luma, seq[j].y_true), psnr(ys[j], seq[j].y_true)
+        cg, cr = psnr(outs[j].chroma, seq[j].chi_true), psnr(cs[j], seq[j].chi_true)
+        print(f"wide window field {j}: Y gpu {pg:.3f} ref {pr:.3f}  C gpu {cg:.3f} ref {cr:.3f}")
+        assert abs(pg - pr) < 0.05 and abs(cg - cr) < 0.05
 
 
 def test_one_past_each_limit(ctx):
