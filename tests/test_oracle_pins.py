@@ -285,6 +285,34 @@ def test_init_cyclic_convolution_equals_fft_crop():
         assert np.abs(got - want).max() < 1e-10
 
 
+@pytest.mark.parametrize("h,w,row_m,col_m", [(96, 1135, 4096, 1024), (600, 96, 2048, 2048),
+                                             (1000, 96, 2048, 4096), (40, 2048, 4096, 1024)])
+def test_init_cyclic_convolution_long_lengths(h, w, row_m, col_m):
+    """The same identity at the lengths of the planes past the register
+    transforms: rows of more than 1024 samples at 4096 (k_init_rows_long),
+    field columns of 513-1024 padded lines at 2048, columns of more than 1024
+    padded lines at 4096 (k_init_cols_long); the widest plane (2048 samples:
+    row convolution 4095 <= 4096)."""
+    rng = np.random.default_rng(h * 7 + w)
+    g = _cabi.default_geometry(_cabi.STD_PAL)
+    pad = min(16, h - 1)
+    hp = h + 2 * pad
+    assert 2 * w - 1 <= row_m and 2 * hp - 1 <= col_m
+    X = rng.normal(size=(hp, w)) + 1j * rng.normal(size=(hp, w))
+    for (mhz, cph) in O.INIT_VARIANTS:
+        gy, gx = O.gaussian_lpf(hp, w, g, mhz, cph, h)
+        want = np.fft.ifft2(np.fft.fft2(X) * gy[:, None] * gx[None, :])
+        xp = np.zeros((hp, row_m), complex)
+        xp[:, :w] = X
+        R = np.fft.ifft(np.fft.fft(xp, axis=1) * _khat(np.fft.ifft(gx), w, row_m)[None, :],
+                        axis=1)[:, :w] * row_m
+        cp = np.zeros((col_m, w), complex)
+        cp[:hp] = R
+        got = np.fft.ifft(np.fft.fft(cp, axis=0) * _khat(np.fft.ifft(gy), hp, col_m)[:, None],
+                          axis=0)[:hp] * col_m
+        assert np.abs(got - want).max() < 1e-10 * max(1.0, np.abs(want).max())
+
+
 def test_single_reduction_cg_recurrence():
     """k_solver: with q = g(d) - g(0), g(chi + a d) = g(chi) + a q and
     curv(d) = <d, q> / 2, so ||g + a q||^2 = gg + 2 a <g,q> + a^2 <q,q>
